@@ -1,0 +1,386 @@
+"""Benchmark of the wavefront + persistent render path (Mrays/s).
+
+Workload: the "displaced_icospheres" scene (3 level-8 displaced icospheres =
+3,932,160 triangles + ground, medium box, area light, 2048x1024 procedural sky),
+1920x1080, max depth 8, counter-based RNG. One step = one sample of every pixel
+(a full wave of 2,073,600 paths through up to 8 bounces); K steps = K spp.
+Mrays/s = (extend rays + shadow rays) / device time, rays counted on the device.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference runs the UNMODIFIED reference (oracle/_ref/libmcref.so: the
+reference's src/path_tracer.cu compiled for sm_100a) through its own
+renderWithWavefront with --persistent semantics on the same scene.
+Multi-GPU (torchrun): every rank renders its own K samples of the full image
+(weak scaling) and the accumulation buffers are summed with one NCCL
+all-reduce at the end, inside the timed region.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "monocuda-pt_b200")]
+
+WORKLOAD = {"workload": "displaced_icospheres", "triangles": 3932176, "width": 1920, "height": 1080, "max_depth": 8,
+            "env_map": "2048x1024 procedural sky", "medium": "homogeneous box, sigma_t 0.5",
+            "rng": "philox4x32-10 per (pixel, sample)", "l2": "inputs larger than L2 (BVH 252 MB + triangles 189 MB)"}
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "k_trace_displaced_icospheres.txt")
+# algorithmic bytes (roofline): node visit, primitive test, extend-ray I/O, shadow-ray I/O
+NODE_BYTES, LEAF_BYTES, EXT_IO_BYTES, SHADOW_IO_BYTES = 64, 48, 48, 72
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = the named workload)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--profile", action="store_true",
+                    help="warm-up and timed steps only (for ncu captures); prints the timed line without extras")
+    return ap.parse_args()
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if index < len(ids):
+                index = ids[index]
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        busy = [x for x in sm if mx and x > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """dram bytes (read + write) per trace launch from the committed ncu summary, or None."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def cpu_baseline(scene, args):
+    """The oracle (CPU restatement of the same integrator) on a bounded band of
+    rows of the same workload, all host threads, timed on this host."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import mcpt
+    from helpers import oracle
+    orc = oracle()
+    tris = mcpt.host_triangles(scene)
+    env = mcpt.host_env(scene)
+    h = orc.orc_scene_create(C.addressof(tris), len(tris), None, 0, env.ctypes.data, scene.env_width,
+                             scene.env_height, scene.env_intensity, 0.0)
+    W, H = scene.width, scene.height
+    threads = os.cpu_count() or 1
+    acc = np.zeros(W * H * 3, np.float64)
+    stats = np.zeros(2, np.float64)
+    cam = scene.camera
+    y0 = H // 2 - 4
+    rows = 8
+    t0 = time.perf_counter()
+    orc.orc_render(h, C.addressof(cam), W, H, 1, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
+                   stats.ctypes.data)
+    dt = time.perf_counter() - t0
+    rows = max(8, min(H, int(rows * args.cpu_seconds / max(dt, 1e-3))))
+    y0 = max(0, H // 2 - rows // 2)
+    acc[:] = 0
+    t0 = time.perf_counter()
+    orc.orc_render(h, C.addressof(cam), W, H, 1, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
+                   stats.ctypes.data)
+    dt = time.perf_counter() - t0
+    orc.orc_scene_destroy(h)
+    rays = stats[0] + stats[1]
+    return {"value": round(rays / dt / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": "%d rows x %d px x 1 spp of the same workload (FP32 oracle, %d threads, %.1f s, %d rays)"
+                      % (rows, W, threads, dt, int(rays))}
+
+
+def run_ours(args):
+    import torch
+
+    import mcpt
+    world, rank, local = dist_init(args)
+    dev = "cuda:%d" % local
+    torch.cuda.set_device(local)
+    scene = mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=args.level, seed=2)
+    tris = mcpt.host_triangles(scene)
+    env = mcpt.host_env(scene)
+    ctx = mcpt.Context(local)
+    ds = mcpt.DeviceScene(tris, env_rgba=env, env_intensity=scene.env_intensity, device=dev)
+    bvh = mcpt.Bvh(ctx, ds.view)
+    W, H = scene.width, scene.height
+    acc = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
+    K, Wm = args.steps, args.warmup
+    base = rank * (K + Wm)
+
+    def params(first, instrument=0):
+        return mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234,
+                                  first_sample=first, instrument=instrument)
+
+    st = mcpt.RenderStats()
+    for i in range(Wm):
+        p = params(base + K + i)
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
+                                               C.byref(st)))
+    acc.zero_()
+    clocks = Clocks(local) if rank == 0 else None
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rays = ext = shd = 0
+    trace_ms = 0.0
+    trace_launches = launches = 0
+    for i in range(K):
+        p = params(base + i, instrument=2)
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
+                                               C.byref(st)))
+        ext += st.extend_rays
+        shd += st.shadow_rays
+        trace_ms += st.trace_ms
+        trace_launches += st.trace_launches
+        launches += st.kernel_launches
+    if world > 1:
+        torch.distributed.all_reduce(acc)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = e0.elapsed_time(e1)
+    ck = clocks.stop() if clocks else None
+    rays = ext + shd
+    if world > 1:
+        t = torch.tensor([ms, float(rays)], dtype=torch.float64, device=dev)
+        mx = t.clone()
+        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        ms_max, rays_all = float(mx[0]), float(t[1])
+    else:
+        ms_max, rays_all = ms, float(rays)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"metric": "Mrays/s", "value": round(rays_all / (ms_max / 1e3) / 1e6, 2), "unit": "Mrays/s",
+                              "steps": K, "profile": True, "level": args.level}), flush=True)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    # untimed instrumented pass over the same samples: node visits and primitive tests
+    visits = leaves = 0
+    for i in range(K):
+        p = params(base + i, instrument=1)
+        tmp = torch.zeros_like(acc)
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), tmp.data_ptr(),
+                                               C.byref(st)))
+        visits += st.node_visits
+        leaves += st.leaf_tests
+
+    # end to end through the C ABI with host buffers: each step renders one sample
+    # and reads the accumulation buffer back into pinned host memory
+    host_acc = torch.empty(W * H * 3, dtype=torch.float32, pin_memory=True)
+    e2e_steps = K
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    e2e_rays = 0
+    for i in range(e2e_steps):
+        p = params(base + i)
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
+                                               C.byref(st)))
+        e2e_rays += st.extend_rays + st.shadow_rays
+        host_acc.copy_(acc, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+
+    # cold end to end: host triangles in, accumulation buffer out, one C-ABI call
+    host_cold = torch.zeros(W * H * 3, dtype=torch.float32, pin_memory=True)
+    pc = params(base)
+    pc.spp = K
+    cold_stats = mcpt.RenderStats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mcpt.check(ctx.lib.mc_render_host(ctx.handle, C.addressof(tris), len(tris), None, 0, C.byref(ds.env), C.byref(pc),
+                                      host_cold.data_ptr(), C.byref(cold_stats)))
+    cold_s = time.perf_counter() - t0
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    alg_bytes = visits * NODE_BYTES + leaves * LEAF_BYTES + ext * EXT_IO_BYTES + shd * SHADOW_IO_BYTES
+    per_launch_bytes = alg_bytes / max(trace_launches, 1)
+    per_launch_s = trace_ms / max(trace_launches, 1) / 1e3
+    achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+    traffic = traffic_per_launch()
+    value = rays_all / (ms_max / 1e3) / 1e6
+    out = {
+        "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": dict(WORKLOAD, spp=K * world, parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
+                       samples_per_sec=round(W * H * K * world / (ms_max / 1e3), 1),
+                       rays_per_path=round(rays_all / (W * H * K * world), 3)),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "kernel": "k_trace (persistent extend + shadow)",
+                     "launches": trace_launches, "avg_launch_ms": round(trace_ms / max(trace_launches, 1), 4),
+                     "trace_share": round(trace_ms / ms, 4),
+                     "node_visits_per_ray": round(visits / max(rays, 1), 2),
+                     "leaf_tests_per_ray": round(leaves / max(rays, 1), 2),
+                     "algorithmic_bytes_per_launch": int(per_launch_bytes)},
+        "e2e": {"value": round(e2e_rays / (e2e_ms / 1e3) / 1e6, 2), "unit": "Mrays/s",
+                "h2d_bytes_per_step": C.sizeof(mcpt.RenderParams), "d2h_bytes_per_step": W * H * 12,
+                "note": "scene and BVH resident; per step: render call with host params + accumulation read-back"},
+        "e2e_cold": {"value": round((cold_stats.extend_rays + cold_stats.shadow_rays) / cold_s / 1e6, 2), "unit": "Mrays/s",
+                     "seconds": round(cold_s, 3), "h2d_bytes": len(tris) * 224, "d2h_bytes": W * H * 12,
+                     "note": "mc_render_host: host triangles -> finalize, split, upload, BVH build, %d spp, read-back" % K},
+        "gpu_launches": launches,
+        "clocks": ck,
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(scene, args)
+    print(json.dumps(out), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import mcpt
+    import mcref
+    if not mcref.available(False):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmcref.so was not built (needs the reference sources)"}))
+        return
+    ref = mcref.load(False)
+    scene = mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=args.level, seed=2)
+    tris = mcpt.host_triangles(scene)
+    env = mcpt.host_env(scene)
+    assert ref.mcref_scene_upload(C.addressof(tris), len(tris), None, 0, env.ctypes.data, scene.env_width,
+                                  scene.env_height, scene.env_intensity, 0.0) == 0
+    W, H, K = scene.width, scene.height, args.steps
+    acc = np.zeros(W * H * 3, np.float32)
+    stats = np.zeros(3, np.float64)
+    cam = mcpt.Camera.from_buffer_copy(bytes(scene.camera))
+    for _ in range(args.warmup):
+        assert ref.mcref_render(C.addressof(cam), W, H, 1, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+    clocks = Clocks(0)
+    # timed: renderWithWavefront (PT:3757) itself, K samples, wavefront + persistent
+    assert ref.mcref_render(C.addressof(cam), W, H, K, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+    ck = clocks.stop()
+    ms = stats[2]
+    # untimed replay of the same launch sequence that also reads the shadow-queue sizes
+    assert ref.mcref_render(C.addressof(cam), W, H, K, 8, 2, 1234, 0, 0, acc.ctypes.data, stats.ctypes.data) == 0
+    rays = stats[0] + stats[1]
+    value = rays / (ms / 1e3) / 1e6
+    out = {"metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1, "steps": K, "warmup": args.warmup,
+           "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic (seeded procedural scene)", "impl": "reference",
+           "config": dict(WORKLOAD, spp=K, rng="curand XORWOW (the reference's own)", parallelism="1 GPU",
+                          note="unmodified reference renderWithWavefront --wavefront --persistent on the B200"),
+           "cpu_baseline": {"value": round(value, 2), "unit": "Mrays/s", "cores": 1, "kind": "reference",
+                            "sample": "the full workload; the reference has no CPU implementation of the path, its own "
+                                      "CUDA build runs on the GPU driven by one host thread"},
+           "e2e": {"value": round(value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "clocks": ck}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

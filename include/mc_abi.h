@@ -1,0 +1,442 @@
+/*
+ * mc_abi.h - C ABI of the B200-native MonoCUDA-PT render hot path.
+ *
+ * Plain C, plain pointers and sizes. Every pointer documented as "device" is a
+ * CUDA device pointer on the context's device; "host" pointers are ordinary
+ * host memory. No call exits the process: every entry point returns an
+ * mc_status, and mc_last_error() gives the message of the last failure on the
+ * calling thread.
+ *
+ * The structs below reproduce the byte layouts of the reference's scene surface
+ * (src/path_tracer.cu, "PT" below) so that arrays built for the reference can be
+ * handed to this library unchanged. Their sizes and field offsets are pinned by
+ * static_asserts at the end of this header (C11 or C++11).
+ */
+#ifndef MC_ABI_H
+#define MC_ABI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define MC_ALIGNAS(n) alignas(n)
+extern "C" {
+#else
+#define MC_ALIGNAS(n) _Alignas(n)
+#endif
+
+#if defined(_WIN32)
+#define MC_API __declspec(dllexport)
+#else
+#define MC_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Status codes. The reference calls exit() on any CUDA error (PT:55-69).     */
+/* ------------------------------------------------------------------------- */
+typedef enum mc_status {
+    MC_OK = 0,
+    MC_ERR_INVALID = 1,         /* bad argument (null pointer, size out of range, ...) */
+    MC_ERR_CUDA = 2,            /* a CUDA runtime call failed */
+    MC_ERR_OOM = 3,             /* device allocation failed */
+    MC_ERR_STACK_OVERFLOW = 4,  /* a traversal stack would have overflowed; the ray was abandoned */
+    MC_ERR_QUEUE_OVERFLOW = 5,  /* a queue append went past its capacity; the entry was dropped */
+    MC_ERR_TIMEOUT = 6,         /* a bounded device wait ran out */
+    MC_ERR_BUDGET = 7,          /* a request does not fit the server's HBM budget */
+    MC_ERR_CANCELLED = 8,       /* a server request was cancelled */
+    MC_ERR_NOT_FOUND = 9,       /* unknown handle / id */
+    MC_ERR_UNSUPPORTED = 10     /* feature compiled out or not available (e.g. no GPU) */
+} mc_status;
+
+/* ------------------------------------------------------------------------- */
+/* Scene surface (reference layouts).                                          */
+/* ------------------------------------------------------------------------- */
+typedef struct mc_vec3 { float x, y, z; } mc_vec3;          /* PT:105 vec3 */
+typedef struct mc_vec2 { float x, y; } mc_vec2;             /* PT:161 vec2 */
+
+/* PT:612-625 AABB: 32 bytes, 16-byte aligned (two 16-byte vector loads). */
+typedef struct mc_aabb {
+    MC_ALIGNAS(16) mc_vec3 lo;
+    float pad0;
+    mc_vec3 hi;
+    float pad1;
+} mc_aabb;
+
+/* PT:191-199 Texture */
+enum { MC_TEX_SOLID = 0, MC_TEX_CHECKER = 1, MC_TEX_IMAGE = 2 };
+typedef struct mc_texture {
+    int32_t type;
+    mc_vec3 color_a;
+    mc_vec3 color_b;
+    float scale;
+    uint64_t image;             /* cudaTextureObject_t for MC_TEX_IMAGE */
+} mc_texture;
+
+/* PT:482-496 Material */
+enum {
+    MC_MAT_LAMBERTIAN = 0,
+    MC_MAT_DIELECTRIC = 1,
+    MC_MAT_CONDUCTOR = 2,
+    MC_MAT_EMISSIVE = 3,
+    MC_MAT_ISOTROPIC = 4
+};
+typedef struct mc_material {
+    int32_t type;
+    mc_texture albedo;
+    mc_vec3 emitted;
+    float fuzz;
+    float refraction_index;
+    float density;
+    float phase_g;
+    const void* density_grid;   /* NanoVDB grid in the reference; must be NULL here */
+    float grid_max_density;
+} mc_material;
+
+/* PT:636-658 triangle (the full host record) */
+typedef struct mc_triangle {
+    mc_vec3 v0, v1, v2;
+    mc_vec2 uv0, uv1, uv2;
+    mc_vec3 n0, n1, n2;
+    mc_material mat;
+    mc_aabb aabb;
+} mc_triangle;
+
+/* PT:660-670 triangle_hot: the 36-byte stream the intersector reads */
+typedef struct mc_triangle_hot { mc_vec3 v0, v1, v2; } mc_triangle_hot;
+
+/* PT:672-680 triangle_cold */
+typedef struct mc_triangle_cold {
+    mc_vec2 uv0, uv1, uv2;
+    mc_vec3 n0, n1, n2;
+    mc_material mat;
+    mc_aabb aabb;
+} mc_triangle_cold;
+
+/* PT:845-875 sphere */
+typedef struct mc_sphere {
+    mc_vec3 center;
+    mc_vec3 center1;
+    uint8_t is_moving;
+    float radius;
+    mc_material mat;
+    mc_aabb aabb;
+} mc_sphere;
+
+/* PT:942-947 Light (one emissive triangle) */
+typedef struct mc_light {
+    mc_triangle_hot tri;
+    mc_vec3 emitted;
+    float area;
+    mc_vec3 normal;
+} mc_light;
+
+/* PT:1010-1019 BVH_Node: the reference's binary node layout, used for export
+ * and parity checks. The library traverses its own compressed layouts. */
+typedef struct mc_bvh_node {
+    mc_aabb bounds;
+    int32_t left;
+    int32_t right;
+    uint8_t left_is_leaf;
+    uint8_t right_is_leaf;
+    int32_t parent;
+    int32_t prim;
+    uint8_t is_leaf;
+} mc_bvh_node;
+
+/* PT:991-996 PackedHit */
+typedef struct mc_packed_hit {
+    MC_ALIGNAS(16) float t;
+    int32_t type;               /* 0 sphere, 1 triangle, -1 none */
+    int32_t index;
+    int32_t did_hit;
+} mc_packed_hit;
+
+/* PT:1581-1631 Camera (fields only). mc_camera_initialize() fills the derived
+ * fields exactly like Camera::initialize(). */
+typedef struct mc_camera {
+    float aspect_ratio;
+    int32_t image_width;
+    int32_t image_height;
+    int32_t samples_per_pixel;
+    int32_t max_depth;
+    float vfov;
+    mc_vec3 look_from;
+    mc_vec3 look_at;
+    mc_vec3 up;
+    mc_vec3 center;
+    mc_vec3 pixel00;
+    mc_vec3 pixel_delta_u;
+    mc_vec3 pixel_delta_v;
+    mc_vec3 u, v, w;
+    mc_vec3 background;
+    float aperture;
+    float lens_radius;
+    float focus_distance;
+    float rr_cap;
+} mc_camera;
+
+/* PT:322-333 EnvironmentMap (g_environment). Pointers are device pointers. */
+typedef struct mc_env_map {
+    uint64_t texture;           /* cudaTextureObject_t (float4, linear, wrap/clamp) */
+    int32_t enabled;
+    float intensity;
+    float rotation;             /* radians */
+    const float* row_cdf;       /* height + 1 */
+    const float* col_cdf;       /* height * (width + 1) */
+    int32_t width;
+    int32_t height;
+    float total_weight;
+} mc_env_map;
+
+/* ------------------------------------------------------------------------- */
+/* Library-side handles and parameter blocks.                                  */
+/* ------------------------------------------------------------------------- */
+typedef struct mc_context mc_context;
+typedef struct mc_bvh mc_bvh;
+
+/* Scene as the render path sees it after the reference's upload sequence
+ * (PT:4262-4303): every array is a device pointer and stays owned by the caller. */
+typedef struct mc_scene_view {
+    const mc_sphere* spheres;
+    int32_t sphere_count;
+    const mc_triangle_hot* tri_hot;
+    const mc_triangle_cold* tri_cold;
+    int32_t triangle_count;
+    const mc_light* lights;
+    int32_t light_count;
+    int32_t has_medium;         /* PT:4328-4331 sceneHasMedium */
+    mc_env_map env;
+} mc_scene_view;
+
+enum {
+    MC_BVH_LAYOUT_BINARY = 0,   /* children's boxes stored in the parent, 64 B per node */
+    MC_BVH_LAYOUT_WIDE4 = 1     /* 4-wide collapse of the binary tree, 128 B per node */
+};
+
+typedef struct mc_bvh_build_opts {
+    /* Optional device array of n = sphere_count + triangle_count ints: the
+     * primitive-reference order to use instead of the library's stable radix
+     * order (entry k = position in the sphere-then-triangle reference list of
+     * the k-th sorted primitive). Lets a caller reproduce the reference's
+     * std::sort tie order inside runs of equal Morton codes. NULL = own order. */
+    const int32_t* permutation;
+    int32_t layout;             /* MC_BVH_LAYOUT_* */
+    int32_t keep_reference_nodes; /* keep PT-layout nodes for mc_bvh_export */
+} mc_bvh_build_opts;
+
+typedef struct mc_bvh_info {
+    int32_t primitive_count;
+    int32_t internal_count;
+    int32_t depth;              /* max leaf depth (root = 0) */
+    int32_t layout;
+    int64_t node_bytes;         /* bytes of the traversal node array */
+    int64_t prim_bytes;         /* bytes of the leaf-ordered triangle stream */
+    mc_aabb scene_bounds;
+} mc_bvh_info;
+
+enum {
+    MC_RNG_PHILOX = 0,          /* counter-based Philox-4x32-10 keyed by (seed, pixel), counter (sample, draw) */
+    MC_RNG_XORWOW = 1           /* curand XORWOW per pixel, curand_init(seed, pixel, 0), state kept across samples */
+};
+
+enum {
+    MC_ISECT_REFERENCE = 0,     /* the reference's plane + edge test (PT:715-741) */
+    MC_ISECT_WATERTIGHT = 1     /* watertight test (Woop, Benthin, Wald 2013) */
+};
+
+typedef struct mc_render_params {
+    mc_camera camera;           /* initialized; image_width/height set */
+    int32_t width;
+    int32_t height;
+    int32_t spp;                /* samples rendered by this call */
+    int32_t first_sample;       /* sample index of the first one (progressive rendering) */
+    int32_t max_depth;
+    int32_t persistent;         /* PT --persistent: persistent extend kernel */
+    int32_t rng;                /* MC_RNG_* */
+    uint64_t seed;              /* PT:4297 uses 1234 */
+    int32_t intersector;        /* MC_ISECT_* */
+    int32_t disable_clamp;      /* 1 = no firefly clamp (guiding MSE studies) */
+    int32_t queue_capacity;     /* 0 = width*height */
+    int32_t refill_threshold;   /* idle lanes before a warp refills (PT:3400 uses 8); 0 = 8 */
+    int32_t use_graph;          /* capture each sample's bounce sequence in a CUDA graph */
+    int32_t instrument;         /* bit 0: count node visits / leaf tests (counting kernel variant);
+                                   bit 1: time every trace launch with CUDA events on the context stream */
+} mc_render_params;
+
+#define MC_MAX_DEPTH_STATS 64
+typedef struct mc_render_stats {
+    int64_t extend_rays;        /* sum over bounces of extend-queue sizes */
+    int64_t shadow_rays;        /* sum over bounces of shadow-queue sizes */
+    int64_t paths;              /* width*height*spp */
+    int64_t extend_per_depth[MC_MAX_DEPTH_STATS];
+    int64_t shadow_per_depth[MC_MAX_DEPTH_STATS];
+    int64_t node_visits;        /* traversal steps (instrument bit 0) */
+    int64_t leaf_tests;         /* primitive intersection tests (instrument bit 0) */
+    float render_ms;            /* device time of the sample loop (CUDA events) */
+    float trace_ms;             /* summed device time of the trace launches (instrument bit 1) */
+    int32_t trace_launches;     /* trace launches timed */
+    int32_t kernel_launches;    /* library kernels launched by the call */
+    int32_t error_flags;        /* device error word (MC_ERR_* bits) */
+} mc_render_stats;
+
+/* ------------------------------------------------------------------------- */
+/* Library, context, errors.                                                   */
+/* ------------------------------------------------------------------------- */
+MC_API const char* mc_version(void);
+MC_API const char* mc_status_string(mc_status s);
+/* Message of the last failed call on this host thread ("" if none). */
+MC_API const char* mc_last_error(void);
+
+/* A context owns the reusable wave buffers (path state, queues, RNG states) of
+ * one device and one stream. One host thread at a time per context.
+ * Replaces the per-call allocation in renderWithWavefront (PT:3757-3840). */
+MC_API mc_status mc_context_create(int device, mc_context** out);
+MC_API mc_status mc_context_destroy(mc_context* ctx);
+/* Stream (cudaStream_t) all work of this context is issued on; NULL = legacy default. */
+MC_API mc_status mc_context_set_stream(mc_context* ctx, void* stream);
+MC_API mc_status mc_context_synchronize(mc_context* ctx);
+
+/* ------------------------------------------------------------------------- */
+/* Scene helpers (host).                                                       */
+/* ------------------------------------------------------------------------- */
+/* Camera::initialize (PT:1610-1631). */
+MC_API mc_status mc_camera_initialize(mc_camera* cam);
+/* triangle::calculate_bounding_box (PT:651-655) for every triangle, then the
+ * emissive-triangle light list of finalizeScene (PT:1972-1985). lights may be
+ * NULL to only count; *light_count receives the count. Host arrays. */
+MC_API mc_status mc_scene_finalize_host(mc_triangle* tris, int32_t n, mc_light* lights, int32_t* light_count);
+/* Splits host triangles into hot/cold records (PT:4276-4281). Host arrays. */
+MC_API mc_status mc_split_triangles_host(const mc_triangle* tris, int32_t n, mc_triangle_hot* hot, mc_triangle_cold* cold);
+
+/* Environment map from a host float RGBA image (top row first), with the
+ * sampling tables of buildEnvironmentSamplingTables (PT:370-385). Creates the
+ * device texture and tables; mc_env_destroy releases them. */
+MC_API mc_status mc_env_create(const float* rgba_host, int32_t width, int32_t height, float intensity,
+                               float rotation_radians, mc_env_map* out);
+MC_API mc_status mc_env_destroy(mc_env_map* env);
+
+/* ------------------------------------------------------------------------- */
+/* Synthetic scenes (seeded, deterministic). Host output.                      */
+/* ------------------------------------------------------------------------- */
+enum {
+    MC_SCENE_CORNELL_BOXES = 1,      /* Cornell room, white floor, two rotated boxes (36 triangles) */
+    MC_SCENE_DISPLACED_ICOSPHERES = 2, /* 3 displaced level-L icospheres + ground + medium box + light + sky */
+    MC_SCENE_BATCH_MEMBER = 3,       /* one scene of the 64-scene batch (index = variant) */
+    MC_SCENE_GUIDING_ROOM = 4,       /* 10x10x4 room lit through a 0.2x0.2 aperture */
+    MC_SCENE_CORNELL_REFERENCE = 5   /* the reference's buildCornellScene geometry minus textures */
+};
+
+typedef struct mc_scene_desc {
+    int32_t kind;                /* MC_SCENE_* */
+    int32_t variant;             /* batch member index / icosphere subdivision level (0 = default) */
+    uint64_t seed;
+    int32_t triangle_target;     /* batch members: requested triangle count (0 = drawn from the seed) */
+} mc_scene_desc;
+
+typedef struct mc_scene_host {
+    mc_triangle* triangles;  int32_t triangle_count;
+    mc_sphere* spheres;      int32_t sphere_count;
+    mc_camera camera;            /* initialized for the scene's default resolution */
+    int32_t width, height, spp, max_depth;
+    int32_t has_medium;
+    float* env_rgba;             /* NULL or env_width*env_height*4 floats, top row first */
+    int32_t env_width, env_height;
+    float env_intensity;
+} mc_scene_host;
+
+MC_API mc_status mc_scene_generate(const mc_scene_desc* desc, mc_scene_host* out);
+MC_API mc_status mc_scene_free(mc_scene_host* scene);
+
+/* ------------------------------------------------------------------------- */
+/* BVH (a1-a7). Replaces the host Morton/sort (PT:1930-1987, 4223-4260) and    */
+/* BVH::generateHierarchy (PT:1063-1090).                                      */
+/* ------------------------------------------------------------------------- */
+/* Morton codes of the reference's primitive list (spheres first, then
+ * triangles; PT:1955-1971) in the scene's bounds. d_codes: device, n entries.
+ * *bounds_out (host, may be NULL) receives the scene bounds. */
+MC_API mc_status mc_morton_codes(mc_context* ctx, const mc_scene_view* scene, uint32_t* d_codes, mc_aabb* bounds_out);
+
+/* Stable LSD radix sort of 30-bit keys with their values (onesweep-style,
+ * 4 passes of 8 bits). Device arrays; in place through context scratch. */
+MC_API mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t* d_values, int32_t n, int32_t key_bits);
+
+/* Full build: bounds, Morton codes, sort, Karras hierarchy, refit, layout. */
+MC_API mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh_build_opts* opts, mc_bvh** out);
+MC_API mc_status mc_bvh_free(mc_bvh* bvh);
+MC_API mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info);
+/* Export in the reference's representation (device arrays, any may be NULL):
+ * sorted codes / primitive ids / primitive types (n each), internal nodes
+ * (n-1) and leaves (n) as mc_bvh_node. Needs keep_reference_nodes for nodes. */
+MC_API mc_status mc_bvh_export(const mc_bvh* bvh, uint32_t* d_codes, int32_t* d_ids, int32_t* d_types,
+                               mc_bvh_node* d_internal, mc_bvh_node* d_leaves);
+
+/* ------------------------------------------------------------------------- */
+/* Ray sets (a8-a15). Rays are SoA: 7 device float arrays of n entries packed  */
+/* back to back: ox[n], oy[n], oz[n], dx[n], dy[n], dz[n], time[n].            */
+/* ------------------------------------------------------------------------- */
+/* Closest hit per ray, as extendKernelPersistent writes it (PT:3402-3468). */
+MC_API mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
+                                  const float* d_rays, int32_t n, int32_t intersector, mc_packed_hit* d_hits);
+/* Any hit within (1e-4, tmax) per ray, as traverseAnyHit (PT:1152-1207).
+ * d_occluded[i] = 1 when blocked. */
+MC_API mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
+                              const float* d_rays, const float* d_tmax, int32_t n, int32_t intersector,
+                              int32_t* d_occluded);
+
+/* ------------------------------------------------------------------------- */
+/* Rendering (a16-a22). Replaces renderWithWavefront (PT:3757-3840).          */
+/* d_accum: device float3 per pixel (W*H*12 bytes, row-major, y=0 top), the   */
+/* reference's linear accumulation buffer; samples are added to it.            */
+/* ------------------------------------------------------------------------- */
+MC_API mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
+                                     const mc_render_params* params, float* d_accum, mc_render_stats* stats);
+/* Same call with host memory: copies the scene in, builds, renders, copies the
+ * accumulation buffer out (accum_host: W*H*3 floats, accumulated into). */
+MC_API mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_t n_tri,
+                                const mc_sphere* spheres, int32_t n_sph, const mc_env_map* env,
+                                const mc_render_params* params, float* accum_host, mc_render_stats* stats);
+/* Reset the per-pixel XORWOW states (PT:2865-2871 init_rng_kernel). */
+MC_API mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed);
+
+/* The params the autotuner picked for a scene size / image size class. */
+MC_API mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
+                             mc_render_params* params, int32_t budget_ms);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Layout pins (sizes measured on the reference compiled with nvcc 12.9).       */
+/* ------------------------------------------------------------------------- */
+#ifdef __cplusplus
+#define MC_STATIC_ASSERT(c, m) static_assert(c, m)
+#else
+#define MC_STATIC_ASSERT(c, m) _Static_assert(c, m)
+#endif
+MC_STATIC_ASSERT(sizeof(mc_vec3) == 12, "vec3 is 12 bytes");
+MC_STATIC_ASSERT(sizeof(mc_aabb) == 32, "AABB is 32 bytes");
+MC_STATIC_ASSERT(sizeof(mc_texture) == 40, "Texture is 40 bytes");
+MC_STATIC_ASSERT(sizeof(mc_material) == 96, "Material is 96 bytes");
+MC_STATIC_ASSERT(sizeof(mc_triangle) == 224, "triangle is 224 bytes");
+MC_STATIC_ASSERT(sizeof(mc_triangle_hot) == 36, "triangle_hot is 36 bytes");
+MC_STATIC_ASSERT(sizeof(mc_triangle_cold) == 192, "triangle_cold is 192 bytes");
+MC_STATIC_ASSERT(offsetof(mc_triangle_cold, mat) == 64, "triangle_cold.mat at 64");
+MC_STATIC_ASSERT(offsetof(mc_triangle_cold, aabb) == 160, "triangle_cold.aabb at 160");
+MC_STATIC_ASSERT(sizeof(mc_sphere) == 160, "sphere is 160 bytes");
+MC_STATIC_ASSERT(offsetof(mc_sphere, mat) == 32, "sphere.mat at 32");
+MC_STATIC_ASSERT(offsetof(mc_sphere, aabb) == 128, "sphere.aabb at 128");
+MC_STATIC_ASSERT(sizeof(mc_light) == 64, "Light is 64 bytes");
+MC_STATIC_ASSERT(sizeof(mc_bvh_node) == 64, "BVH_Node is 64 bytes");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, left) == 32, "BVH_Node.leftChild at 32");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, right) == 36, "BVH_Node.rightChild at 36");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, left_is_leaf) == 40, "BVH_Node.leftIsLeaf at 40");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, right_is_leaf) == 41, "BVH_Node.rightIsLeaf at 41");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, parent) == 44, "BVH_Node.parent at 44");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, prim) == 48, "BVH_Node.primitiveIndex at 48");
+MC_STATIC_ASSERT(offsetof(mc_bvh_node, is_leaf) == 52, "BVH_Node.isLeaf at 52");
+MC_STATIC_ASSERT(sizeof(mc_packed_hit) == 16, "PackedHit is 16 bytes");
+MC_STATIC_ASSERT(sizeof(mc_camera) == 172, "Camera is 172 bytes");
+MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
+
+#endif /* MC_ABI_H */

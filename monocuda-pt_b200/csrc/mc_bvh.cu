@@ -1,0 +1,758 @@
+// mc_bvh.cu - LBVH build on the device.
+//
+//   primitive bounds + centroids + scene bounds  (finalizeScene, PT:1930-1971)
+//   30-bit Morton codes                          (morton3D, PT:913-935; host IEEE math in the reference)
+//   stable onesweep LSD radix sort               (replaces the host std::sort, PT:4223-4226)
+//   Karras radix tree                            (delta/determineRange/findSplit, PT:1337-1447)
+//   bottom-up refit with per-node arrival counters (refitBoundsKernel, PT:1398-1415), which writes
+//   the boxes straight into the traversal layout (children's boxes stored in the parent).
+//
+// This file is compiled WITHOUT fast math and with -fmad=false: the reference
+// computes bounds and Morton codes on the host with IEEE single precision and
+// no contraction, and the codes must match bit for bit.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "mc_internal.h"
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 256;
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kTile = kSortThreads * kSortItems;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1;
+constexpr long long kSpinLimit = 1ll << 22;
+
+#define MC_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e__ = (call);                                                          \
+        if (e__ != cudaSuccess) return mc::cuda_error((int)e__, #call, __FILE__, __LINE__); \
+    } while (0)
+
+struct Box {
+    float lx, ly, lz, hx, hy, hz;
+};
+
+__device__ __forceinline__ Box merge_box(const Box& a, const Box& b) {  // PT:1456-1465 merge
+    Box m;
+    m.hx = fmaxf(a.hx, b.hx);
+    m.hy = fmaxf(a.hy, b.hy);
+    m.hz = fmaxf(a.hz, b.hz);
+    m.lx = fminf(a.lx, b.lx);
+    m.ly = fminf(a.ly, b.ly);
+    m.lz = fminf(a.lz, b.lz);
+    return m;
+}
+
+// Ordered-integer encoding so atomicMin/atomicMax on ints order floats.
+__device__ __forceinline__ int float_to_ordered(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__host__ __device__ __forceinline__ float ordered_to_float(int i) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF);
+#else
+    int j = i >= 0 ? i : i ^ 0x7FFFFFFF;
+    float f;
+    memcpy(&f, &j, 4);
+    return f;
+#endif
+}
+
+// Bounds and centroid of primitive i of the reference list (spheres first).
+// Sphere: calculate_bounding_box / calculateCentroid (PT:850-869).
+// Triangle: calculate_bounding_box with eps 1e-3 / (v0+v1+v2)/3 (PT:647-656).
+__global__ void k_prim_bounds(const mc_sphere* __restrict__ sph, int ns, const mc_triangle_hot* __restrict__ hot, int nt,
+                              mc_aabb* __restrict__ bounds, float4* __restrict__ centroids, int* __restrict__ scene) {
+    int n = ns + nt;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Box b = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    bool valid = i < n;
+    if (valid) {
+        float cx, cy, cz;
+        if (i < ns) {
+            const mc_sphere& s = sph[i];
+            float r = s.radius;
+            Box b0 = {s.center.x - r, s.center.y - r, s.center.z - r, s.center.x + r, s.center.y + r, s.center.z + r};
+            if (s.is_moving) {
+                Box b1 = {s.center1.x - r, s.center1.y - r, s.center1.z - r, s.center1.x + r, s.center1.y + r, s.center1.z + r};
+                b = merge_box(b0, b1);
+                cx = (s.center.x + s.center1.x) * 0.5f;
+                cy = (s.center.y + s.center1.y) * 0.5f;
+                cz = (s.center.z + s.center1.z) * 0.5f;
+            } else {
+                b = b0;
+                cx = s.center.x; cy = s.center.y; cz = s.center.z;
+            }
+        } else {
+            const mc_triangle_hot& t = hot[i - ns];
+            const float eps = 1e-3f;
+            b.lx = fminf(t.v0.x, fminf(t.v1.x, t.v2.x)) - eps;
+            b.ly = fminf(t.v0.y, fminf(t.v1.y, t.v2.y)) - eps;
+            b.lz = fminf(t.v0.z, fminf(t.v1.z, t.v2.z)) - eps;
+            b.hx = fmaxf(t.v0.x, fmaxf(t.v1.x, t.v2.x)) + eps;
+            b.hy = fmaxf(t.v0.y, fmaxf(t.v1.y, t.v2.y)) + eps;
+            b.hz = fmaxf(t.v0.z, fmaxf(t.v1.z, t.v2.z)) + eps;
+            cx = (t.v0.x + t.v1.x + t.v2.x) / 3.0f;
+            cy = (t.v0.y + t.v1.y + t.v2.y) / 3.0f;
+            cz = (t.v0.z + t.v1.z + t.v2.z) / 3.0f;
+        }
+        mc_aabb a;
+        a.lo = mc_vec3{b.lx, b.ly, b.lz};
+        a.pad0 = 0.f;
+        a.hi = mc_vec3{b.hx, b.hy, b.hz};
+        a.pad1 = 0.f;
+        bounds[i] = a;
+        centroids[i] = make_float4(cx, cy, cz, 0.f);
+    }
+    // warp reduction of the scene bounds (min/max are exact in any order)
+    for (int off = 16; off > 0; off >>= 1) {
+        b.lx = fminf(b.lx, __shfl_xor_sync(0xffffffffu, b.lx, off));
+        b.ly = fminf(b.ly, __shfl_xor_sync(0xffffffffu, b.ly, off));
+        b.lz = fminf(b.lz, __shfl_xor_sync(0xffffffffu, b.lz, off));
+        b.hx = fmaxf(b.hx, __shfl_xor_sync(0xffffffffu, b.hx, off));
+        b.hy = fmaxf(b.hy, __shfl_xor_sync(0xffffffffu, b.hy, off));
+        b.hz = fmaxf(b.hz, __shfl_xor_sync(0xffffffffu, b.hz, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&scene[0], float_to_ordered(b.lx));
+        atomicMin(&scene[1], float_to_ordered(b.ly));
+        atomicMin(&scene[2], float_to_ordered(b.lz));
+        atomicMax(&scene[3], float_to_ordered(b.hx));
+        atomicMax(&scene[4], float_to_ordered(b.hy));
+        atomicMax(&scene[5], float_to_ordered(b.hz));
+    }
+}
+
+// PT:913-920 expandBits: bit i of the 10-bit input moves to bit 3i.
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    uint32_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 10; i++) r |= ((v >> i) & 1u) << (3 * i);
+    return r;
+}
+
+// PT:922-925 quantize: (value - min) / (max - min) * 1023, then the host's
+// float -> unsigned conversion (x86-64: truncation through a 64-bit integer,
+// NaN -> 0, low 32 bits kept).
+__device__ __forceinline__ uint32_t quantize(float value, float lo, float hi) {
+    float normalized = __fdiv_rn(__fsub_rn(value, lo), __fsub_rn(hi, lo));
+    float scaled = __fmul_rn(normalized, 1023.0f);
+    if (scaled != scaled) return 0u;
+    long long v = __float2ll_rz(scaled);
+    return (uint32_t)v;
+}
+
+__global__ void k_morton(const float4* __restrict__ centroids, int n, const int* __restrict__ scene,
+                         uint32_t* __restrict__ codes, int32_t* __restrict__ values) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float lx = ordered_to_float(scene[0]), ly = ordered_to_float(scene[1]), lz = ordered_to_float(scene[2]);
+    float hx = ordered_to_float(scene[3]), hy = ordered_to_float(scene[4]), hz = ordered_to_float(scene[5]);
+    float4 c = centroids[i];
+    uint32_t x = expand_bits(quantize(c.x, lx, hx));
+    uint32_t y = expand_bits(quantize(c.y, ly, hy));
+    uint32_t z = expand_bits(quantize(c.z, lz, hz));
+    codes[i] = x | y << 1 | z << 2;  // PT:934
+    if (values) values[i] = i;
+}
+
+// ---------------------------------------------------------------------------
+// Onesweep radix sort (Adinets & Merrill, "Onesweep: A Faster Least
+// Significant Digit Radix Sort for GPUs", 2022): one histogram pass over the
+// keys for all digit positions, then one kernel per digit position that ranks
+// a tile, resolves its global digit offsets by decoupled look-back, and
+// scatters. Ranking inside a tile is stable (warp match + running per-warp
+// digit counts), so the sort is stable.
+// ---------------------------------------------------------------------------
+__global__ void k_radix_histogram(const uint32_t* __restrict__ keys, int n, int passes, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[4][kRadix];
+    for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t k = keys[i];
+        for (int p = 0; p < passes; p++) atomicAdd(&h[p][(k >> (p * kRadixBits)) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
+        uint32_t v = (&h[0][0])[i];
+        if (v) atomicAdd(&hist[i], v);
+    }
+}
+
+__global__ void k_radix_scan(uint32_t* __restrict__ hist, int passes) {
+    // one block of 256 threads per digit position: exclusive scan in place
+    __shared__ uint32_t s[kRadix];
+    int p = blockIdx.x;
+    if (p >= passes) return;
+    uint32_t v = hist[p * kRadix + threadIdx.x];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < kRadix; off <<= 1) {
+        uint32_t t = threadIdx.x >= (unsigned)off ? s[threadIdx.x - off] : 0u;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    hist[p * kRadix + threadIdx.x] = s[threadIdx.x] - v;
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __restrict__ keys_in, const int32_t* __restrict__ vals_in,
+                                 uint32_t* __restrict__ keys_out, int32_t* __restrict__ vals_out, int n, int shift,
+                                 const uint32_t* __restrict__ digit_offsets, uint32_t* status, int* tile_counter,
+                                 int* error) {
+    __shared__ uint32_t warp_hist[kSortWarps][kRadix];
+    __shared__ uint32_t digit_base[kRadix];
+    __shared__ int tile_s;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1);
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const int tile = tile_s;
+    const long long base = (long long)tile * kTile + (long long)warp * 32 * kSortItems;
+
+    uint32_t key[kSortItems];
+    int32_t val[kSortItems];
+    uint32_t rank[kSortItems];
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        long long idx = base + j * 32 + lane;
+        bool valid = idx < n;
+        key[j] = valid ? keys_in[idx] : 0xFFFFFFFFu;
+        val[j] = valid ? vals_in[idx] : 0;
+        uint32_t d = valid ? ((key[j] >> shift) & (kRadix - 1)) : (kRadix + lane);
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t prior = valid ? warp_hist[warp][d] : 0u;
+        __syncwarp();
+        rank[j] = prior + __popc(peers & lanemask_lt);
+        int leader = __ffs(peers) - 1;
+        if (valid && lane == leader) warp_hist[warp][d] = prior + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // exclusive scan over warps for each digit; tile total per digit
+    const int d = threadIdx.x;  // kSortThreads == kRadix
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+        uint32_t t = warp_hist[w][d];
+        warp_hist[w][d] = total;
+        total += t;
+    }
+    // decoupled look-back over the preceding tiles for this digit
+    volatile uint32_t* vstatus = status;
+    uint32_t exclusive = 0;
+    if (tile == 0) {
+        vstatus[d] = kFlagInc | total;
+    } else {
+        vstatus[(long long)tile * kRadix + d] = kFlagAgg | total;
+        int pred = tile - 1;
+        long long spins = 0;
+        while (pred >= 0) {
+            uint32_t s = vstatus[(long long)pred * kRadix + d];
+            uint32_t flag = s & ~kCountMask;
+            if (flag == 0u) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(error, MC_DEVERR_TIMEOUT);
+                    break;
+                }
+                continue;
+            }
+            exclusive += s & kCountMask;
+            if (flag == kFlagInc) break;
+            pred--;
+        }
+        __threadfence();
+        vstatus[(long long)tile * kRadix + d] = kFlagInc | (exclusive + total);
+    }
+    digit_base[d] = digit_offsets[d] + exclusive;
+    __syncthreads();
+
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        long long idx = base + j * 32 + lane;
+        if (idx < n) {
+            uint32_t dd = (key[j] >> shift) & (kRadix - 1);
+            uint32_t dst = digit_base[dd] + warp_hist[warp][dd] + rank[j];
+            if (dst < (uint32_t)n) {
+                keys_out[dst] = key[j];
+                vals_out[dst] = val[j];
+            } else {
+                atomicOr(error, MC_DEVERR_INPUT);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Karras 2012 hierarchy (PT:1337-1447).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int delta(const uint32_t* __restrict__ codes, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t ci = codes[i], cj = codes[j];
+    if (ci == cj) return 32 + __clz((unsigned int)(i ^ j));
+    return __clz(ci ^ cj);
+}
+
+// Child references: internal child c -> c; leaf child k -> ~k.
+__global__ void k_karras(const uint32_t* __restrict__ codes, int n, float4* __restrict__ nodes,
+                         int32_t* __restrict__ parents, mc_bvh_node* __restrict__ ref_internal,
+                         mc_bvh_node* __restrict__ ref_leaves) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n - 1) return;
+    int d = (delta(codes, n, idx, idx + 1) - delta(codes, n, idx, idx - 1)) >= 0 ? 1 : -1;
+    int deltaMin = delta(codes, n, idx, idx - d);
+    int lmax = 2;
+    while (delta(codes, n, idx, idx + lmax * d) > deltaMin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(codes, n, idx, idx + (l + t) * d) > deltaMin) l += t;
+    int jdx = idx + l * d;
+    int first = min(idx, jdx);
+    int last = max(idx, jdx);
+    int common = delta(codes, n, first, last);
+    int split = first;
+    int step = last - first;
+    do {
+        step = (step + 1) >> 1;
+        int ns = split + step;
+        if (ns < last && delta(codes, n, first, ns) > common) split = ns;
+    } while (step > 1);
+
+    bool leftLeaf = (split == first);
+    bool rightLeaf = (split + 1 == last);
+    int leftRef = leftLeaf ? ~split : split;
+    int rightRef = rightLeaf ? ~(split + 1) : (split + 1);
+    nodes[(long long)idx * 4 + 3] = make_float4(__int_as_float(leftRef), __int_as_float(rightRef), 0.f, 0.f);
+    // parents: internal nodes at [0, n-1), leaves at [n-1, 2n-1); value (parent << 1) | side
+    parents[leftLeaf ? (n - 1 + split) : split] = (idx << 1) | 0;
+    parents[rightLeaf ? (n - 1 + split + 1) : (split + 1)] = (idx << 1) | 1;
+    if (idx == 0) parents[0] = -1;
+    if (ref_internal) {
+        mc_bvh_node& r = ref_internal[idx];
+        r.left = split;
+        r.right = split + 1;
+        r.left_is_leaf = leftLeaf;
+        r.right_is_leaf = rightLeaf;
+        r.is_leaf = 0;
+        r.prim = -1;
+        if (idx == 0) r.parent = -1;
+        if (leftLeaf) ref_leaves[split].parent = idx; else ref_internal[split].parent = idx;
+        if (rightLeaf) ref_leaves[split + 1].parent = idx; else ref_internal[split + 1].parent = idx;
+    }
+}
+
+__device__ __forceinline__ void store_child_box(float4* nodes, int node, int side, const Box& b) {
+    float* f = reinterpret_cast<float*>(nodes + (long long)node * 4);
+    int o = side ? 6 : 0;
+    __stcg(f + o + 0, b.lx);
+    __stcg(f + o + 1, b.ly);
+    __stcg(f + o + 2, b.lz);
+    __stcg(f + o + 3, b.hx);
+    __stcg(f + o + 4, b.hy);
+    __stcg(f + o + 5, b.hz);
+}
+
+__device__ __forceinline__ Box load_child_box(const float4* nodes, int node, int side) {
+    const float* f = reinterpret_cast<const float*>(nodes + (long long)node * 4);
+    int o = side ? 6 : 0;
+    Box b;
+    b.lx = __ldcg(f + o + 0);
+    b.ly = __ldcg(f + o + 1);
+    b.lz = __ldcg(f + o + 2);
+    b.hx = __ldcg(f + o + 3);
+    b.hy = __ldcg(f + o + 4);
+    b.hz = __ldcg(f + o + 5);
+    return b;
+}
+
+// Leaves + refit (buildLeavesKernel PT:1388-1396 and refitBoundsKernel
+// PT:1398-1415): leaf k writes its primitive record and its box into the
+// parent's slot; the second thread to arrive at a node merges the two slots
+// and continues upwards.
+__global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb* __restrict__ bounds_ref, int n, int ns,
+                               const mc_sphere* __restrict__ sph, const mc_triangle_hot* __restrict__ hot,
+                               float4* __restrict__ nodes, float4* __restrict__ prims, const int32_t* __restrict__ parents,
+                               int* __restrict__ counters, int32_t* __restrict__ ids_out, int32_t* __restrict__ types_out,
+                               mc_bvh_node* __restrict__ ref_internal, mc_bvh_node* __restrict__ ref_leaves,
+                               mc_aabb* __restrict__ root_box) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int src = order[k];
+    int type = src < ns ? 0 : 1;
+    int id = src < ns ? src : src - ns;
+    float4 r0, r1, r2;
+    if (type == 1) {
+        const mc_triangle_hot t = hot[id];
+        r0 = make_float4(t.v0.x, t.v0.y, t.v0.z, t.v1.x);
+        r1 = make_float4(t.v1.y, t.v1.z, t.v2.x, t.v2.y);
+        r2 = make_float4(t.v2.z, __int_as_float(id), __int_as_float(1), 0.f);
+    } else {
+        const mc_sphere& s = sph[id];
+        r0 = make_float4(s.center.x, s.center.y, s.center.z, s.center1.x);
+        r1 = make_float4(s.center1.y, s.center1.z, s.radius, s.is_moving ? 1.f : 0.f);
+        r2 = make_float4(0.f, __int_as_float(id), __int_as_float(0), 0.f);
+    }
+    prims[(long long)k * 3 + 0] = r0;
+    prims[(long long)k * 3 + 1] = r1;
+    prims[(long long)k * 3 + 2] = r2;
+    if (ids_out) ids_out[k] = id;
+    if (types_out) types_out[k] = type;
+    mc_aabb a = bounds_ref[src];
+    Box b = {a.lo.x, a.lo.y, a.lo.z, a.hi.x, a.hi.y, a.hi.z};
+    if (ref_leaves) {
+        mc_bvh_node& r = ref_leaves[k];
+        r.bounds = a;
+        r.prim = id;
+        r.is_leaf = 1;
+        r.left = -1;
+        r.right = -1;
+        r.left_is_leaf = 0;
+        r.right_is_leaf = 0;
+    }
+    if (n == 1) {
+        *root_box = a;
+        return;
+    }
+    int p = parents[n - 1 + k];
+    while (p >= 0) {
+        int node = p >> 1, side = p & 1;
+        store_child_box(nodes, node, side, b);
+        __threadfence();
+        int old = atomicAdd(&counters[node], 1);
+        if (old == 0) return;
+        __threadfence();
+        Box other = load_child_box(nodes, node, side ^ 1);
+        b = side ? merge_box(other, b) : merge_box(b, other);
+        if (ref_internal) {
+            mc_aabb m;
+            m.lo = mc_vec3{b.lx, b.ly, b.lz};
+            m.hi = mc_vec3{b.hx, b.hy, b.hz};
+            m.pad0 = 0.f;
+            m.pad1 = 0.f;
+            ref_internal[node].bounds = m;
+        }
+        p = parents[node];
+        if (p < 0) {
+            mc_aabb m;
+            m.lo = mc_vec3{b.lx, b.ly, b.lz};
+            m.hi = mc_vec3{b.hx, b.hy, b.hz};
+            m.pad0 = 0.f;
+            m.pad1 = 0.f;
+            *root_box = m;
+        }
+    }
+}
+
+// The single-primitive tree: one node whose left child is leaf 0 and whose
+// right child is an empty box (the reference needs n >= 2).
+__global__ void k_single_root(float4* nodes, const mc_aabb* bounds) {
+    mc_aabb a = bounds[0];
+    nodes[0] = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
+    nodes[1] = make_float4(a.hi.y, a.hi.z, INFINITY, INFINITY);
+    nodes[2] = make_float4(INFINITY, -INFINITY, -INFINITY, -INFINITY);
+    nodes[3] = make_float4(__int_as_float(~0), __int_as_float(~0), 0.f, 0.f);
+}
+
+__global__ void k_leaf_depth(const int32_t* __restrict__ parents, int n, int* depth) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int dcount = 0;
+    int p = parents[n - 1 + k];
+    while (p >= 0) {
+        p = parents[p >> 1];
+        dcount++;
+        if (dcount > 4 * n + 8) break;
+    }
+    atomicMax(depth, dcount);
+}
+
+__global__ void k_gather_u32(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, int n, uint32_t* __restrict__ dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+
+int grid_for(long long n, int block) { return (int)std::max(1ll, (n + block - 1) / block); }
+
+}  // namespace
+
+namespace mc {
+
+// Sorts (keys, values) pairs of n entries stably by the low key_bits bits.
+// keys/vals are sorted in place; alt_keys/alt_vals are scratch of n entries.
+mc_status radix_sort_pairs(mc_context* ctx, uint32_t* keys, int32_t* vals, uint32_t* alt_keys, int32_t* alt_vals, int n,
+                           int key_bits) {
+    if (n <= 1) return MC_OK;
+    int passes = (key_bits + kRadixBits - 1) / kRadixBits;
+    if (passes < 1 || passes > 4) return set_error(MC_ERR_INVALID, "radix sort: key_bits must be in [1, 32]");
+    long long tiles = (n + kTile - 1) / kTile;
+    size_t statusBytes = (size_t)tiles * kRadix * sizeof(uint32_t);
+    size_t histBytes = 4 * kRadix * sizeof(uint32_t);
+    mc_status st = devbuf_reserve(ctx->scratch[6], histBytes + 16 * sizeof(int) + (size_t)passes * statusBytes);
+    if (st != MC_OK) return st;
+    char* base = (char*)ctx->scratch[6].ptr;
+    uint32_t* hist = (uint32_t*)base;
+    int* tileCounters = (int*)(base + histBytes);
+    uint32_t* status = (uint32_t*)(base + histBytes + 16 * sizeof(int));
+    MC_CUDA(cudaMemsetAsync(base, 0, histBytes + 16 * sizeof(int) + (size_t)passes * statusBytes, ctx->stream));
+    int hblocks = std::min(grid_for(n, 256), ctx->sm_count * 4);
+    k_radix_histogram<<<hblocks, 256, 0, ctx->stream>>>(keys, n, passes, hist);
+    k_radix_scan<<<passes, kRadix, 0, ctx->stream>>>(hist, passes);
+    uint32_t* kin = keys; int32_t* vin = vals; uint32_t* kout = alt_keys; int32_t* vout = alt_vals;
+    for (int p = 0; p < passes; p++) {
+        k_onesweep<<<(int)tiles, kSortThreads, 0, ctx->stream>>>(kin, vin, kout, vout, n, p * kRadixBits, hist + p * kRadix,
+                                                                 status + (size_t)p * tiles * kRadix, tileCounters + p,
+                                                                 ctx->d_error);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    if (kin != keys) {
+        MC_CUDA(cudaMemcpyAsync(keys, kin, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+        MC_CUDA(cudaMemcpyAsync(vals, vin, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    MC_CUDA(cudaGetLastError());
+    return MC_OK;
+}
+
+mc_status bvh_depth(mc_bvh* bvh) {
+    if (bvh->depth >= 0) return MC_OK;
+    if (bvh->n == 1) {
+        bvh->depth = 1;
+        return MC_OK;
+    }
+    mc_context* ctx = bvh->ctx;
+    int* d;
+    MC_CUDA(cudaMalloc(&d, sizeof(int)));
+    MC_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx->stream));
+    k_leaf_depth<<<grid_for(bvh->n, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, bvh->n, d);
+    int h = 0;
+    MC_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(d);
+    bvh->depth = h;
+    return MC_OK;
+}
+
+// Scene bounds + Morton codes (reference primitive order) into codes; the
+// primitive boxes into bounds_ref (n entries) and the raw bounds words into scene6.
+static mc_status morton_stage(mc_context* ctx, const mc_scene_view* s, uint32_t* codes, int32_t* values, mc_aabb* bounds_ref,
+                              float4* centroids, int* scene6) {
+    int n = s->sphere_count + s->triangle_count;
+    int init[6] = {0x7F800000, 0x7F800000, 0x7F800000, (int)0x807FFFFF, (int)0x807FFFFF, (int)0x807FFFFF};
+    // +inf as ordered int for mins; -inf (0xFF800000 -> ordered 0x807FFFFF) for maxes
+    MC_CUDA(cudaMemcpyAsync(scene6, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    k_prim_bounds<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(s->spheres, s->sphere_count, s->tri_hot, s->triangle_count,
+                                                                  bounds_ref, centroids, scene6);
+    k_morton<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(centroids, n, scene6, codes, values);
+    MC_CUDA(cudaGetLastError());
+    return MC_OK;
+}
+
+static mc_status check_scene(const mc_scene_view* s) {
+    if (!s) return set_error(MC_ERR_INVALID, "null scene");
+    if (s->sphere_count < 0 || s->triangle_count < 0) return set_error(MC_ERR_INVALID, "negative primitive count");
+    long long n = (long long)s->sphere_count + s->triangle_count;
+    if (n == 0) return set_error(MC_ERR_INVALID, "the scene has no primitives");
+    if (n >= (1ll << 30)) return set_error(MC_ERR_INVALID, "too many primitives (limit 2^30 - 1)");
+    if (s->sphere_count > 0 && !s->spheres) return set_error(MC_ERR_INVALID, "null sphere array");
+    if (s->triangle_count > 0 && !s->tri_hot) return set_error(MC_ERR_INVALID, "null triangle array");
+    return MC_OK;
+}
+
+}  // namespace mc
+
+extern "C" {
+
+mc_status mc_morton_codes(mc_context* ctx, const mc_scene_view* scene, uint32_t* d_codes, mc_aabb* bounds_out) {
+    if (!ctx || !d_codes) return mc::set_error(MC_ERR_INVALID, "mc_morton_codes: null argument");
+    mc_status st = mc::check_scene(scene);
+    if (st != MC_OK) return st;
+    int n = scene->sphere_count + scene->triangle_count;
+    if ((st = mc::devbuf_reserve(ctx->scratch[0], (size_t)n * sizeof(mc_aabb))) != MC_OK) return st;
+    if ((st = mc::devbuf_reserve(ctx->scratch[1], (size_t)n * sizeof(float4))) != MC_OK) return st;
+    if ((st = mc::devbuf_reserve(ctx->scratch[7], 64)) != MC_OK) return st;
+    int* scene6 = (int*)ctx->scratch[7].ptr;
+    st = mc::morton_stage(ctx, scene, d_codes, nullptr, (mc_aabb*)ctx->scratch[0].ptr, (float4*)ctx->scratch[1].ptr, scene6);
+    if (st != MC_OK) return st;
+    if (bounds_out) {
+        int h[6];
+        MC_CUDA(cudaMemcpyAsync(h, scene6, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        MC_CUDA(cudaStreamSynchronize(ctx->stream));
+        bounds_out->lo = mc_vec3{ordered_to_float(h[0]), ordered_to_float(h[1]), ordered_to_float(h[2])};
+        bounds_out->hi = mc_vec3{ordered_to_float(h[3]), ordered_to_float(h[4]), ordered_to_float(h[5])};
+        bounds_out->pad0 = bounds_out->pad1 = 0.f;
+    }
+    return MC_OK;
+}
+
+mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t* d_values, int32_t n, int32_t key_bits) {
+    if (!ctx || (n > 0 && (!d_keys || !d_values)) || n < 0) return mc::set_error(MC_ERR_INVALID, "mc_radix_sort_pairs: bad argument");
+    if (n >= (1 << 30)) return mc::set_error(MC_ERR_INVALID, "mc_radix_sort_pairs: n must be < 2^30");
+    if (key_bits < 1 || key_bits > 32) return mc::set_error(MC_ERR_INVALID, "mc_radix_sort_pairs: key_bits must be in [1, 32]");
+    mc_status st;
+    if ((st = mc::devbuf_reserve(ctx->scratch[2], (size_t)n * 4 + 16)) != MC_OK) return st;
+    if ((st = mc::devbuf_reserve(ctx->scratch[3], (size_t)n * 4 + 16)) != MC_OK) return st;
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    st = mc::radix_sort_pairs(ctx, d_keys, d_values, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, n, key_bits);
+    if (st != MC_OK) return st;
+    int flags = 0;
+    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return mc::status_from_device_flags(flags);
+}
+
+mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh_build_opts* opts, mc_bvh** out) {
+    if (!ctx || !out) return mc::set_error(MC_ERR_INVALID, "mc_bvh_build: null argument");
+    *out = nullptr;
+    mc_status st = mc::check_scene(scene);
+    if (st != MC_OK) return st;
+    mc_bvh_build_opts o = {};
+    if (opts) o = *opts;
+    if (o.layout != MC_BVH_LAYOUT_BINARY && o.layout != MC_BVH_LAYOUT_WIDE4)
+        return mc::set_error(MC_ERR_INVALID, "mc_bvh_build: unknown layout");
+    const int ns = scene->sphere_count, nt = scene->triangle_count, n = ns + nt;
+
+    mc_bvh* bvh = new mc_bvh();
+    bvh->ctx = ctx;
+    bvh->n = n; bvh->ns = ns; bvh->nt = nt;
+    bvh->layout = MC_BVH_LAYOUT_BINARY;
+    auto fail = [&](mc_status s) { mc_bvh_free(bvh); return s; };
+
+    long long nodesCount = std::max(1, n - 1);
+    size_t nodeBytes = (size_t)nodesCount * 64;
+    if (cudaMalloc(&bvh->nodes, nodeBytes) != cudaSuccess ||
+        cudaMalloc(&bvh->prims, (size_t)n * 48) != cudaSuccess ||
+        cudaMalloc(&bvh->codes, (size_t)n * 4) != cudaSuccess ||
+        cudaMalloc(&bvh->ids, (size_t)n * 4) != cudaSuccess ||
+        cudaMalloc(&bvh->types, (size_t)n * 4) != cudaSuccess ||
+        cudaMalloc(&bvh->parents, (size_t)(2 * n) * 4) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(mc::set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (n=%d)", n));
+    }
+    if (o.keep_reference_nodes) {
+        if (cudaMalloc(&bvh->ref_internal, (size_t)nodesCount * sizeof(mc_bvh_node)) != cudaSuccess ||
+            cudaMalloc(&bvh->ref_leaves, (size_t)n * sizeof(mc_bvh_node)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(mc::set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (reference nodes)"));
+        }
+        cudaMemsetAsync(bvh->ref_internal, 0, (size_t)nodesCount * sizeof(mc_bvh_node), ctx->stream);
+        cudaMemsetAsync(bvh->ref_leaves, 0, (size_t)n * sizeof(mc_bvh_node), ctx->stream);
+    }
+    bvh->node_count = nodesCount;
+    bvh->node_bytes = (long long)nodeBytes;
+
+    // scratch: [0] primitive boxes (ref order), [1] centroids, [2]/[3] sort alt buffers, [4] order, [5] counters, [7] scene6
+    if ((st = mc::devbuf_reserve(ctx->scratch[0], (size_t)n * sizeof(mc_aabb))) != MC_OK) return fail(st);
+    if ((st = mc::devbuf_reserve(ctx->scratch[1], (size_t)n * sizeof(float4))) != MC_OK) return fail(st);
+    if ((st = mc::devbuf_reserve(ctx->scratch[2], (size_t)n * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = mc::devbuf_reserve(ctx->scratch[3], (size_t)n * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = mc::devbuf_reserve(ctx->scratch[4], (size_t)n * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = mc::devbuf_reserve(ctx->scratch[5], (size_t)nodesCount * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = mc::devbuf_reserve(ctx->scratch[7], 64)) != MC_OK) return fail(st);
+    mc_aabb* boundsRef = (mc_aabb*)ctx->scratch[0].ptr;
+    float4* centroids = (float4*)ctx->scratch[1].ptr;
+    int32_t* order = (int32_t*)ctx->scratch[4].ptr;
+    int* counters = (int*)ctx->scratch[5].ptr;
+    int* scene6 = (int*)ctx->scratch[7].ptr;
+
+    if (cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream) != cudaSuccess) return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
+    if ((st = mc::morton_stage(ctx, scene, bvh->codes, order, boundsRef, centroids, scene6)) != MC_OK) return fail(st);
+    if (o.permutation) {
+        // caller-provided order (e.g. the reference's std::sort order)
+        if (cudaMemcpyAsync(order, o.permutation, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+            return fail(mc::cuda_error(cudaGetLastError(), "permutation copy", __FILE__, __LINE__));
+        uint32_t* tmp = (uint32_t*)ctx->scratch[2].ptr;
+        if (cudaMemcpyAsync(tmp, bvh->codes, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+            return fail(mc::cuda_error(cudaGetLastError(), "code copy", __FILE__, __LINE__));
+        k_gather_u32<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(tmp, order, n, bvh->codes);
+    } else {
+        st = mc::radix_sort_pairs(ctx, bvh->codes, order, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, n, 30);
+        if (st != MC_OK) return fail(st);
+    }
+    if (cudaMemsetAsync(counters, 0, (size_t)nodesCount * 4, ctx->stream) != cudaSuccess)
+        return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
+    mc_aabb* rootBox = (mc_aabb*)(scene6 + 8);
+    if (n >= 2) {
+        k_karras<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>(bvh->codes, n, (float4*)bvh->nodes, bvh->parents,
+                                                                     bvh->ref_internal, bvh->ref_leaves);
+    } else {
+        int m1 = -1;
+        cudaMemcpyAsync(bvh->parents, &m1, 4, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(bvh->parents + 1, &m1, 4, cudaMemcpyHostToDevice, ctx->stream);
+    }
+    k_leaves_refit<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(order, boundsRef, n, ns, scene->spheres, scene->tri_hot,
+                                                                   (float4*)bvh->nodes, (float4*)bvh->prims, bvh->parents,
+                                                                   counters, bvh->ids, bvh->types, bvh->ref_internal,
+                                                                   bvh->ref_leaves, rootBox);
+    if (n == 1) k_single_root<<<1, 1, 0, ctx->stream>>>((float4*)bvh->nodes, boundsRef);
+    if (cudaGetLastError() != cudaSuccess) return fail(mc::set_error(MC_ERR_CUDA, "mc_bvh_build: launch failed"));
+    int flags = 0;
+    if (cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&bvh->bounds, rootBox, sizeof(mc_aabb), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return fail(mc::cuda_error(cudaGetLastError(), "mc_bvh_build", __FILE__, __LINE__));
+    if (flags) return fail(mc::status_from_device_flags(flags));
+    *out = bvh;
+    return MC_OK;
+}
+
+mc_status mc_bvh_free(mc_bvh* bvh) {
+    if (!bvh) return MC_OK;
+    cudaFree(bvh->nodes);
+    cudaFree(bvh->prims);
+    cudaFree(bvh->codes);
+    cudaFree(bvh->ids);
+    cudaFree(bvh->types);
+    cudaFree(bvh->parents);
+    cudaFree(bvh->ref_internal);
+    cudaFree(bvh->ref_leaves);
+    delete bvh;
+    return MC_OK;
+}
+
+mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info) {
+    if (!bvh || !info) return mc::set_error(MC_ERR_INVALID, "mc_bvh_get_info: null argument");
+    mc_status st = mc::bvh_depth(const_cast<mc_bvh*>(bvh));
+    if (st != MC_OK) return st;
+    info->primitive_count = bvh->n;
+    info->internal_count = bvh->n - 1;
+    info->depth = bvh->depth;
+    info->layout = bvh->layout;
+    info->node_bytes = bvh->node_bytes;
+    info->prim_bytes = (long long)bvh->n * 48;
+    info->scene_bounds = bvh->bounds;
+    return MC_OK;
+}
+
+mc_status mc_bvh_export(const mc_bvh* bvh, uint32_t* d_codes, int32_t* d_ids, int32_t* d_types, mc_bvh_node* d_internal,
+                        mc_bvh_node* d_leaves) {
+    if (!bvh) return mc::set_error(MC_ERR_INVALID, "mc_bvh_export: null bvh");
+    cudaStream_t s = bvh->ctx->stream;
+    int n = bvh->n;
+    if (d_codes) MC_CUDA(cudaMemcpyAsync(d_codes, bvh->codes, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_ids) MC_CUDA(cudaMemcpyAsync(d_ids, bvh->ids, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_types) MC_CUDA(cudaMemcpyAsync(d_types, bvh->types, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_internal || d_leaves) {
+        if (!bvh->ref_internal) return mc::set_error(MC_ERR_INVALID, "mc_bvh_export: build with keep_reference_nodes to export nodes");
+        if (d_internal && n > 1)
+            MC_CUDA(cudaMemcpyAsync(d_internal, bvh->ref_internal, (size_t)(n - 1) * sizeof(mc_bvh_node), cudaMemcpyDeviceToDevice, s));
+        if (d_leaves) MC_CUDA(cudaMemcpyAsync(d_leaves, bvh->ref_leaves, (size_t)n * sizeof(mc_bvh_node), cudaMemcpyDeviceToDevice, s));
+    }
+    MC_CUDA(cudaStreamSynchronize(s));
+    return MC_OK;
+}
+
+}  // extern "C"

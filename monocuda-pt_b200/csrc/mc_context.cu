@@ -1,0 +1,210 @@
+// mc_context.cu - contexts, error reporting, device buffers, environment maps.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "mc_internal.h"
+
+namespace {
+thread_local char g_last_error[512] = "";
+}
+
+namespace mc {
+
+mc_status set_error(mc_status s, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return s;
+}
+
+mc_status cuda_error(int err, const char* what, const char* file, int line) {
+    cudaError_t e = (cudaError_t)err;
+    mc_status s = (e == cudaErrorMemoryAllocation) ? MC_ERR_OOM : MC_ERR_CUDA;
+    const char* base = std::strrchr(file, '/');
+    return set_error(s, "%s failed at %s:%d: %s", what, base ? base + 1 : file, line, cudaGetErrorString(e));
+}
+
+mc_status status_from_device_flags(int flags) {
+    if (flags == 0) return MC_OK;
+    if (flags & MC_DEVERR_TIMEOUT) return set_error(MC_ERR_TIMEOUT, "a bounded device wait ran out (flags 0x%x)", flags);
+    if (flags & MC_DEVERR_STACK) return set_error(MC_ERR_STACK_OVERFLOW, "a traversal stack would have overflowed (flags 0x%x)", flags);
+    if (flags & MC_DEVERR_QUEUE) return set_error(MC_ERR_QUEUE_OVERFLOW, "a queue append went past its capacity (flags 0x%x)", flags);
+    return set_error(MC_ERR_INVALID, "invalid input seen on the device (flags 0x%x)", flags);
+}
+
+mc_status devbuf_reserve(DevBuf& b, size_t bytes) {
+    if (bytes <= b.bytes && b.ptr) return MC_OK;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.ptr = nullptr;
+        return set_error(MC_ERR_OOM, "device allocation of %zu bytes failed: %s", want, cudaGetErrorString(e));
+    }
+    b.bytes = want;
+    return MC_OK;
+}
+
+void devbuf_free(DevBuf& b) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+}  // namespace mc
+
+extern "C" {
+
+const char* mc_version(void) { return "monocuda-pt-b200 0.1.0 (sm_100a)"; }
+
+const char* mc_status_string(mc_status s) {
+    switch (s) {
+        case MC_OK: return "ok";
+        case MC_ERR_INVALID: return "invalid argument";
+        case MC_ERR_CUDA: return "CUDA error";
+        case MC_ERR_OOM: return "out of device memory";
+        case MC_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+        case MC_ERR_QUEUE_OVERFLOW: return "queue overflow";
+        case MC_ERR_TIMEOUT: return "device wait timed out";
+        case MC_ERR_BUDGET: return "request exceeds the memory budget";
+        case MC_ERR_CANCELLED: return "cancelled";
+        case MC_ERR_NOT_FOUND: return "not found";
+        case MC_ERR_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+const char* mc_last_error(void) { return g_last_error; }
+
+mc_status mc_context_create(int device, mc_context** out) {
+    if (!out) return mc::set_error(MC_ERR_INVALID, "mc_context_create: null output");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return mc::set_error(MC_ERR_UNSUPPORTED, "mc_context_create: no CUDA device (%s)", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count) return mc::set_error(MC_ERR_INVALID, "mc_context_create: device %d out of range", device);
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return mc::cuda_error((int)e, "cudaSetDevice", __FILE__, __LINE__);
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return mc::cuda_error((int)e, "cudaGetDeviceProperties", __FILE__, __LINE__);
+    if (prop.major < 10) return mc::set_error(MC_ERR_UNSUPPORTED, "mc_context_create: device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+    mc_context* ctx = new mc_context();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
+    if (cudaMalloc(&ctx->d_error, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->d_counters, counterBytes) != cudaSuccess ||
+        cudaMalloc(&ctx->d_stats, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long)) != cudaSuccess) {
+        cudaGetLastError();
+        mc_context_destroy(ctx);
+        return mc::set_error(MC_ERR_OOM, "mc_context_create: device allocation failed");
+    }
+    cudaMemset(ctx->d_error, 0, sizeof(int));
+    cudaMemset(ctx->d_counters, 0, counterBytes);
+    *out = ctx;
+    return MC_OK;
+}
+
+mc_status mc_context_destroy(mc_context* ctx) {
+    if (!ctx) return MC_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream); else cudaDeviceSynchronize();
+    cudaFree(ctx->d_error);
+    cudaFree(ctx->d_counters);
+    cudaFree(ctx->d_stats);
+    for (auto& b : ctx->scratch) mc::devbuf_free(b);
+    mc::devbuf_free(ctx->wave.block);
+    cudaFree(ctx->rng_states);
+    delete ctx;
+    return MC_OK;
+}
+
+mc_status mc_context_set_stream(mc_context* ctx, void* stream) {
+    if (!ctx) return mc::set_error(MC_ERR_INVALID, "mc_context_set_stream: null context");
+    ctx->stream = (cudaStream_t)stream;
+    return MC_OK;
+}
+
+mc_status mc_context_synchronize(mc_context* ctx) {
+    if (!ctx) return mc::set_error(MC_ERR_INVALID, "mc_context_synchronize: null context");
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return mc::cuda_error((int)e, "cudaStreamSynchronize", __FILE__, __LINE__);
+    return MC_OK;
+}
+
+// PT:370-411: sampling tables (host) and a float4 texture, linear filtering,
+// wrap in u, clamp in v, element-type reads, normalized coordinates.
+mc_status mc_env_create(const float* rgba, int32_t W, int32_t H, float intensity, float rotation, mc_env_map* out) {
+    if (!out) return mc::set_error(MC_ERR_INVALID, "mc_env_create: null output");
+    std::memset(out, 0, sizeof(*out));
+    out->intensity = intensity;
+    out->rotation = rotation;
+    if (!rgba || W <= 0 || H <= 0) return MC_OK;  // disabled environment
+    std::vector<float> rowCdf, colCdf;
+    float total = 0.f;
+    mc::build_env_tables(rgba, W, H, rowCdf, colCdf, total);
+    cudaChannelFormatDesc desc = cudaCreateChannelDesc<float4>();
+    cudaArray_t arr = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocArray(&arr, &desc, W, H)) != cudaSuccess) return mc::cuda_error((int)e, "cudaMallocArray", __FILE__, __LINE__);
+    if ((e = cudaMemcpy2DToArray(arr, 0, 0, rgba, (size_t)W * sizeof(float4), (size_t)W * sizeof(float4), H, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cudaFreeArray(arr);
+        return mc::cuda_error((int)e, "cudaMemcpy2DToArray", __FILE__, __LINE__);
+    }
+    cudaResourceDesc res = {};
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = arr;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    cudaTextureObject_t tex = 0;
+    if ((e = cudaCreateTextureObject(&tex, &res, &td, nullptr)) != cudaSuccess) {
+        cudaFreeArray(arr);
+        return mc::cuda_error((int)e, "cudaCreateTextureObject", __FILE__, __LINE__);
+    }
+    float* dRow = nullptr; float* dCol = nullptr;
+    if (cudaMalloc(&dRow, rowCdf.size() * sizeof(float)) != cudaSuccess || cudaMalloc(&dCol, colCdf.size() * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaDestroyTextureObject(tex);
+        cudaFreeArray(arr);
+        cudaFree(dRow);
+        return mc::set_error(MC_ERR_OOM, "mc_env_create: device allocation failed");
+    }
+    cudaMemcpy(dRow, rowCdf.data(), rowCdf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(dCol, colCdf.data(), colCdf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    out->texture = (uint64_t)tex;
+    out->enabled = 1;
+    out->row_cdf = dRow;
+    out->col_cdf = dCol;
+    out->width = W;
+    out->height = H;
+    out->total_weight = total;
+    return MC_OK;
+}
+
+mc_status mc_env_destroy(mc_env_map* env) {
+    if (!env || !env->enabled) return MC_OK;
+    cudaResourceDesc res;
+    if (cudaGetTextureObjectResourceDesc(&res, (cudaTextureObject_t)env->texture) == cudaSuccess) {
+        cudaDestroyTextureObject((cudaTextureObject_t)env->texture);
+        if (res.resType == cudaResourceTypeArray) cudaFreeArray(res.res.array.array);
+    }
+    cudaFree((void*)env->row_cdf);
+    cudaFree((void*)env->col_cdf);
+    std::memset(env, 0, sizeof(*env));
+    return MC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+// mc_host.cu - host-memory entry point and the launch-parameter autotuner.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "mc_internal.h"
+
+#define MC_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e__ = (call);                                                          \
+        if (e__ != cudaSuccess) return mc::cuda_error((int)e__, #call, __FILE__, __LINE__); \
+    } while (0)
+
+namespace mc {
+mc_status ensure_wave(mc_context* ctx, int capacity);
+}
+
+extern "C" {
+
+// The whole reference flow from host arrays (PT:4223-4336): finalize + light
+// list, hot/cold split, upload, BVH build, render, accumulation read-back.
+mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_t n_tri, const mc_sphere* spheres, int32_t n_sph,
+                         const mc_env_map* env, const mc_render_params* params, float* accum_host, mc_render_stats* stats) {
+    if (!ctx || !params || !accum_host || n_tri < 0 || n_sph < 0 || (n_tri > 0 && !tris) || (n_sph > 0 && !spheres))
+        return mc::set_error(MC_ERR_INVALID, "mc_render_host: bad argument");
+    if (n_tri + n_sph == 0) return mc::set_error(MC_ERR_INVALID, "mc_render_host: the scene has no primitives");
+    std::vector<mc_triangle> t(tris, tris + n_tri);
+    int32_t nl = 0;
+    mc_scene_finalize_host(t.data(), n_tri, nullptr, &nl);
+    std::vector<mc_light> lights((size_t)(nl > 0 ? nl : 1));
+    mc_scene_finalize_host(t.data(), n_tri, lights.data(), &nl);
+    std::vector<mc_triangle_hot> hot((size_t)(n_tri > 0 ? n_tri : 1));
+    std::vector<mc_triangle_cold> cold((size_t)(n_tri > 0 ? n_tri : 1));
+    mc_split_triangles_host(t.data(), n_tri, hot.data(), cold.data());
+    int hasMedium = 0;
+    for (const auto& x : t) if (x.mat.type == MC_MAT_ISOTROPIC) hasMedium = 1;
+    for (int i = 0; i < n_sph; i++) if (spheres[i].mat.type == MC_MAT_ISOTROPIC) hasMedium = 1;
+
+    mc_triangle_hot* dHot = nullptr; mc_triangle_cold* dCold = nullptr; mc_sphere* dSph = nullptr; mc_light* dL = nullptr;
+    float* dAcc = nullptr;
+    size_t accBytes = (size_t)params->width * params->height * 3 * sizeof(float);
+    auto cleanup = [&]() { cudaFree(dHot); cudaFree(dCold); cudaFree(dSph); cudaFree(dL); cudaFree(dAcc); };
+    if (cudaMalloc(&dHot, hot.size() * sizeof(mc_triangle_hot)) != cudaSuccess ||
+        cudaMalloc(&dCold, cold.size() * sizeof(mc_triangle_cold)) != cudaSuccess ||
+        cudaMalloc(&dSph, (size_t)(n_sph > 0 ? n_sph : 1) * sizeof(mc_sphere)) != cudaSuccess ||
+        cudaMalloc(&dL, lights.size() * sizeof(mc_light)) != cudaSuccess || cudaMalloc(&dAcc, accBytes) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return mc::set_error(MC_ERR_OOM, "mc_render_host: device allocation failed");
+    }
+    cudaMemcpyAsync(dHot, hot.data(), (size_t)n_tri * sizeof(mc_triangle_hot), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(dCold, cold.data(), (size_t)n_tri * sizeof(mc_triangle_cold), cudaMemcpyHostToDevice, ctx->stream);
+    if (n_sph) cudaMemcpyAsync(dSph, spheres, (size_t)n_sph * sizeof(mc_sphere), cudaMemcpyHostToDevice, ctx->stream);
+    if (nl) cudaMemcpyAsync(dL, lights.data(), (size_t)nl * sizeof(mc_light), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(dAcc, accum_host, accBytes, cudaMemcpyHostToDevice, ctx->stream);
+    mc_scene_view view;
+    std::memset(&view, 0, sizeof(view));
+    view.spheres = dSph; view.sphere_count = n_sph;
+    view.tri_hot = dHot; view.tri_cold = dCold; view.triangle_count = n_tri;
+    view.lights = dL; view.light_count = nl;
+    view.has_medium = hasMedium;
+    if (env) view.env = *env;
+    mc_bvh* bvh = nullptr;
+    mc_status st = mc_bvh_build(ctx, &view, nullptr, &bvh);
+    if (st == MC_OK) st = mc_render_wavefront(ctx, bvh, &view, params, dAcc, stats);
+    if (st == MC_OK) {
+        cudaError_t e = cudaMemcpyAsync(accum_host, dAcc, accBytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = mc::cuda_error((int)e, "mc_render_host read-back", __FILE__, __LINE__);
+    }
+    mc_bvh_free(bvh);
+    cleanup();
+    return st;
+}
+
+// Picks the refill threshold and the persistent/plain trace variant by timing
+// one-sample renders at a reduced resolution with the scene's own BVH.
+// budget_ms bounds the total tuning time (0 = 2000 ms).
+mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, mc_render_params* params, int32_t budget_ms) {
+    if (!ctx || !bvh || !scene || !params) return mc::set_error(MC_ERR_INVALID, "mc_autotune: null argument");
+    if (budget_ms <= 0) budget_ms = 2000;
+    mc_render_params probe = *params;
+    int scale = 1;
+    while ((long long)(probe.width / scale) * (probe.height / scale) > 1 << 19) scale *= 2;
+    probe.width = params->width / scale > 0 ? params->width / scale : 1;
+    probe.height = params->height / scale > 0 ? params->height / scale : 1;
+    probe.camera.image_width = probe.width;
+    probe.camera.aspect_ratio = probe.width / float(probe.height);
+    mc_camera_initialize(&probe.camera);
+    probe.spp = 1;
+    probe.rng = MC_RNG_PHILOX;
+    float* dAcc = nullptr;
+    if (cudaMalloc(&dAcc, (size_t)probe.width * probe.height * 3 * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return mc::set_error(MC_ERR_OOM, "mc_autotune: allocation failed");
+    }
+    struct Cand { int persistent, refill; };
+    const Cand cands[] = {{1, 8}, {1, 4}, {1, 12}, {1, 16}, {1, 24}, {0, 8}};
+    float best = 1e30f;
+    Cand bestC = {params->persistent, params->refill_threshold > 0 ? params->refill_threshold : 8};
+    auto t0 = std::chrono::steady_clock::now();
+    mc_status st = MC_OK;
+    for (const Cand& c : cands) {
+        probe.persistent = c.persistent;
+        probe.refill_threshold = c.refill;
+        mc_render_stats rs;
+        st = mc_render_wavefront(ctx, bvh, scene, &probe, dAcc, &rs);  // warm-up
+        if (st != MC_OK) break;
+        st = mc_render_wavefront(ctx, bvh, scene, &probe, dAcc, &rs);
+        if (st != MC_OK) break;
+        if (rs.render_ms < best) {
+            best = rs.render_ms;
+            bestC = c;
+        }
+        double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (el > budget_ms) break;
+    }
+    cudaFree(dAcc);
+    if (st != MC_OK) return st;
+    params->persistent = bestC.persistent;
+    params->refill_threshold = bestC.refill;
+    return MC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+// mc_internal.h - library-internal declarations shared by the .cu/.cpp files.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "mc_abi.h"
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#else
+typedef struct CUstream_st* cudaStream_t;
+#endif
+
+// Device error word bits (written with atomicOr by kernels, read by the host).
+#define MC_DEVERR_STACK 1
+#define MC_DEVERR_QUEUE 2
+#define MC_DEVERR_TIMEOUT 4
+#define MC_DEVERR_INPUT 8
+
+// Traversal stack capacity (the reference's TRAVERSAL_STACK_CAPACITY, PT:1038).
+#define MC_STACK_CAPACITY 64
+
+namespace mc {
+
+// Records the message for mc_last_error() and returns s.
+mc_status set_error(mc_status s, const char* fmt, ...);
+mc_status cuda_error(int err, const char* what, const char* file, int line);
+mc_status status_from_device_flags(int flags);
+
+void build_env_tables(const float* rgba, int W, int H, std::vector<float>& rowCdf, std::vector<float>& colCdf,
+                      float& total);
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+mc_status devbuf_reserve(DevBuf& b, size_t bytes);
+void devbuf_free(DevBuf& b);
+
+// Per-bounce counters of one sample: [d][0] extend-queue size of bounce d,
+// [d][1] shadow-queue size of bounce d, [d][2] trace work counter,
+// [d][3] medium pass-through count.
+#define MC_COUNTERS_PER_DEPTH 4
+
+struct WaveBuffers {
+    int capacity = 0;
+    // path state, SoA (PT:3138-3163 PathStateBuffers)
+    float* ox = nullptr; float* oy = nullptr; float* oz = nullptr;
+    float* dx = nullptr; float* dy = nullptr; float* dz = nullptr;
+    float* time = nullptr;
+    float* tr = nullptr; float* tg = nullptr; float* tb = nullptr;
+    float* sr = nullptr; float* sg = nullptr; float* sb = nullptr;
+    unsigned char* spec = nullptr;
+    float* pdf = nullptr;
+    uint32_t* draw = nullptr;          // Philox draw counter per path
+    mc_packed_hit* hits = nullptr;     // PT:3165 HitResultBuffers
+    int* queue[2] = {nullptr, nullptr};  // extend queues (ping-pong)
+    // shadow-ray queue, SoA (PT:3170-3186 ShadowRayQueue)
+    float* sox = nullptr; float* soy = nullptr; float* soz = nullptr;
+    float* sdx = nullptr; float* sdy = nullptr; float* sdz = nullptr;
+    float* smax = nullptr;
+    float* scr = nullptr; float* scg = nullptr; float* scb = nullptr;
+    int* spath = nullptr;
+    DevBuf block;                      // one allocation backs all of the above
+};
+
+}  // namespace mc
+
+struct mc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    int* d_error = nullptr;            // device error word
+    int* d_counters = nullptr;         // (MC_MAX_DEPTH_STATS+1) * MC_COUNTERS_PER_DEPTH ints
+    long long* d_stats = nullptr;      // 2 * MC_MAX_DEPTH_STATS accumulated ray counts
+    mc::DevBuf scratch[8];             // build / sort scratch
+    mc::WaveBuffers wave;
+    void* rng_states = nullptr;        // curandState per pixel (XORWOW mode)
+    int rng_pixels = 0;
+    unsigned long long rng_seed = 0;
+    bool rng_ready = false;
+};
+
+struct mc_bvh {
+    mc_context* ctx = nullptr;
+    int n = 0, ns = 0, nt = 0;
+    int layout = MC_BVH_LAYOUT_BINARY;
+    int depth = -1;
+    void* nodes = nullptr;             // traversal nodes (float4 records)
+    long long node_count = 0;
+    long long node_bytes = 0;
+    void* prims = nullptr;             // leaf-ordered primitive records, 48 B each
+    // reference representation (optional)
+    uint32_t* codes = nullptr;
+    int32_t* ids = nullptr;
+    int32_t* types = nullptr;
+    mc_bvh_node* ref_internal = nullptr;
+    mc_bvh_node* ref_leaves = nullptr;
+    int32_t* parents = nullptr;        // internal parents (n-1) then leaf parents (n), encoded (p<<1)|side
+    mc_aabb bounds;
+};
+
+namespace mc {
+mc_status bvh_depth(mc_bvh* bvh);
+mc_status context_counters(mc_context* ctx);
+}

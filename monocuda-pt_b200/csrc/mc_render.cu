@@ -1,0 +1,1064 @@
+// mc_render.cu - the wavefront render path on sm_100a.
+//
+// One sample of every pixel is one wave. Per bounce d:
+//   trace(d)  persistent kernel: closest hits of the bounce-d extend queue AND
+//             the bounce-(d-1) shadow rays, pulled from one work counter by
+//             warps that refill idle lanes (PT:3416-3468 extendKernelPersistent
+//             + PT:3698-3728 shadowKernel, fused into one launch);
+//   shade(d)  grid-stride kernel (PT:3470-3696 shadeKernel) that appends to the
+//             next extend queue and to the shadow queue with one atomic per warp.
+// Queue sizes never leave the device: every kernel reads its count from the
+// per-bounce counter block, so a sample is a fixed launch sequence (no host
+// readback per bounce as in PT:3816), which also makes it graph-capturable.
+//
+// Compiled with --use_fast_math like the reference (CMakeLists.txt:94-96).
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "mc_internal.h"
+#include "mc_rng.cuh"
+#include "mc_shade.cuh"
+#include "mc_traverse.cuh"
+
+#define MC_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e__ = (call);                                                          \
+        if (e__ != cudaSuccess) return mc::cuda_error((int)e__, #call, __FILE__, __LINE__); \
+    } while (0)
+
+namespace mc {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+MC_D unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// Trace: extend rays + shadow rays in one persistent launch.
+// ---------------------------------------------------------------------------
+struct TraceArgs {
+    TraceScene ts;
+    // extend rays: path indices from queue (identity when null), rays from the path SoA
+    const int* queue;
+    const int* extCount;
+    int extN;
+    const float *ox, *oy, *oz, *dx, *dy, *dz, *time;
+    mc_packed_hit* hits;
+    // shadow rays (PT:3170-3186 layout)
+    const int* shCount;
+    int shN;
+    const float *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *scr, *scg, *scb;
+    const int* spath;
+    float *sr, *sg, *sb;   // per-path sample accumulators
+    int* occluded;         // ray-set mode: any-hit result per shadow slot instead of accumulation
+    // medium boundaries (PT:2874-2898 mediumTransmittance)
+    const mc_triangle_cold* cold;
+    const mc_sphere* spheres;
+    int* work;
+    int refill;
+    int* err;
+    unsigned long long* counts;  // [0] node visits, [1] leaf tests (counting variant)
+};
+
+// Warp-reduces the lane counters and adds them to the global pair.
+MC_D void flush_counts(const TraceArgs& a, const TravCount& c) {
+    unsigned long long v = (unsigned long long)c.visits, l = (unsigned long long)c.leaves;
+    for (int off = 16; off > 0; off >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+        l += __shfl_xor_sync(0xffffffffu, l, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&a.counts[0], v);
+        atomicAdd(&a.counts[1], l);
+    }
+}
+
+MC_D void material_medium_info(const TraceArgs& a, int type, int id, int& mtype, float& density) {
+    const mc_material* m = type == 1 ? &a.cold[id].mat : &a.spheres[id].mat;
+    mtype = m->type;
+    density = m->density;
+}
+
+// Finishes one ray. Returns true when the lane is free again.
+template <int ISECT, bool MEDIUM>
+MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int slot, float& T, float& travelled,
+                     int& crossings) {
+    if (kind == 0) {
+        mc_packed_hit h;
+        h.t = s.tmax;
+        if (s.hitLeaf >= 0) {
+            int type, id;
+            leaf_identity(a.ts, s.hitLeaf, type, id);
+            h.type = type;
+            h.index = id;
+            h.did_hit = 1;
+        } else {
+            h.type = -1;
+            h.index = -1;
+            h.did_hit = 0;
+        }
+        reinterpret_cast<int4*>(a.hits)[slot] = make_int4(__float_as_int(h.t), h.type, h.index, h.did_hit);
+        return true;
+    }
+    if (!MEDIUM) {
+        if (a.occluded) {
+            a.occluded[slot] = step == STEP_OCCLUDED ? 1 : 0;
+            return true;
+        }
+        // PT:3711-3727: unoccluded -> transmittance 1
+        if (step != STEP_OCCLUDED) {
+            int p = a.spath[slot];
+            float tr = 1.0f;
+            a.sr[p] += a.scr[slot] * tr;
+            a.sg[p] += a.scg[slot] * tr;
+            a.sb[p] += a.scb[slot] * tr;
+        }
+        return true;
+    }
+    // medium transmittance loop (at most 4 boundary crossings)
+    bool done = false;
+    bool blocked = false;
+    if (s.hitLeaf < 0) {
+        done = true;
+    } else {
+        int type, id;
+        leaf_identity(a.ts, s.hitLeaf, type, id);
+        int mtype;
+        float density;
+        material_medium_info(a, type, id, mtype, density);
+        if (mtype != MC_MAT_ISOTROPIC) {
+            blocked = true;
+            done = true;
+        } else {
+            bool front;
+            if (type == 1) {
+                const float4* rec = a.ts.prims + (long long)s.hitLeaf * 3;
+                float4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
+                V3 v0(r0.x, r0.y, r0.z), v1(r0.w, r1.x, r1.y), v2(r1.z, r1.w, r2.x);
+                V3 e1 = v1 - v0;
+                V3 e2 = v2 - v0;
+                V3 nrm = e1.cross(e2).normalize();
+                front = s.r.d.dot(nrm) < 0.0f;
+            } else {
+                const mc_sphere& sp = a.spheres[id];
+                float tt;
+                V3 outward;
+                hit_sphere_ref(v3(sp.center), v3(sp.center1), sp.is_moving != 0, sp.radius, s.r.o, s.r.d, s.time, tt, front,
+                               outward);
+            }
+            if (!front) T = T * expf(-density * s.tmax);
+            travelled = travelled + s.tmax;
+            V3 hp = s.r.o + s.r.d * s.tmax;
+            crossings++;
+            float remaining = a.smax[slot] - travelled;
+            if (crossings >= 4 || remaining <= 0.0f) {
+                done = true;
+            } else {
+                s.r.o = hp;
+                s.tmax = remaining;
+                s.hitLeaf = -1;
+                s.node = 0;
+                s.sp = 0;
+            }
+        }
+    }
+    if (!done) return false;
+    if (a.occluded) {
+        a.occluded[slot] = (blocked || !(T > 0.0f)) ? 1 : 0;
+        return true;
+    }
+    if (!blocked && T > 0.0f) {
+        int p = a.spath[slot];
+        a.sr[p] += a.scr[slot] * T;
+        a.sg[p] += a.scg[slot] * T;
+        a.sb[p] += a.scb[slot] * T;
+    }
+    return true;
+}
+
+template <int ISECT, bool MEDIUM, bool COUNT = false>
+__global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
+    TravCount cnt;
+    const int lane = threadIdx.x & 31;
+    const unsigned ltmask = lanemask_lt();
+    const int extCount = a.extCount ? *a.extCount : a.extN;
+    const int shCount = a.shCount ? *a.shCount : a.shN;
+    const int total = extCount + shCount;
+    int stack[MC_STACK_CAPACITY];
+    TravState s;
+    WatertightRay w;
+    w.kx = 0; w.ky = 1; w.kz = 2; w.sx = w.sy = w.sz = 0.f;
+    bool has = false, exhausted = total == 0;
+    int kind = 0, slot = 0, crossings = 0;
+    float T = 1.f, travelled = 0.f;
+    while (true) {
+        if (!exhausted) {
+            unsigned idle = __ballot_sync(kFull, !has);
+            int cnt = __popc(idle);
+            if (cnt >= a.refill) {
+                int leader = __ffs(idle) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(a.work, cnt);
+                base = __shfl_sync(kFull, base, leader);
+                if (!has) {
+                    int q = base + __popc(idle & ltmask);
+                    if (q < total) {
+                        V3 o, d;
+                        float time, tmax;
+                        if (q < extCount) {
+                            kind = 0;
+                            slot = a.queue ? a.queue[q] : q;
+                            o = V3(a.ox[slot], a.oy[slot], a.oz[slot]);
+                            d = V3(a.dx[slot], a.dy[slot], a.dz[slot]);
+                            time = a.time[slot];
+                            tmax = 1e30f;
+                            has = true;
+                        } else {
+                            kind = 1;
+                            slot = q - extCount;
+                            o = V3(a.sox[slot], a.soy[slot], a.soz[slot]);
+                            d = V3(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
+                            time = a.spath ? a.time[a.spath[slot]] : a.time[slot];
+                            tmax = a.smax[slot];
+                            T = 1.f;
+                            travelled = 0.f;
+                            crossings = 0;
+                            has = true;
+                            if (MEDIUM && tmax <= 0.0f) {
+                                // PT:2880-2881: nothing left to traverse, transmittance 1
+                                s.tmax = tmax;
+                                s.hitLeaf = -1;
+                                finish_ray<ISECT, MEDIUM>(a, s, STEP_DONE, kind, slot, T, travelled, crossings);
+                                has = false;
+                            }
+                        }
+                        if (has) {
+                            trav_begin(s, o, d, time, tmax);
+                            if (ISECT == MC_ISECT_WATERTIGHT) w = make_watertight(d);
+                        }
+                    }
+                }
+                if (base + cnt >= total) exhausted = true;
+            }
+        }
+        if (exhausted && __ballot_sync(kFull, has) == 0u) break;
+        if (has) {
+            int r = (kind == 1 && !MEDIUM) ? trav_step<true, ISECT, COUNT>(a.ts, s, stack, w, a.err, &cnt)
+                                           : trav_step<false, ISECT, COUNT>(a.ts, s, stack, w, a.err, &cnt);
+            if (r != STEP_CONTINUE) {
+                if (finish_ray<ISECT, MEDIUM>(a, s, r, kind, slot, T, travelled, crossings)) has = false;
+            }
+        }
+    }
+    if (COUNT) flush_counts(a, cnt);
+}
+
+// One thread per ray, no refill (the plain --wavefront extendKernel, PT:3376-3397).
+template <int ISECT, bool MEDIUM>
+__global__ void __launch_bounds__(256) k_trace_simple(TraceArgs a) {
+    const int extCount = a.extCount ? *a.extCount : a.extN;
+    const int shCount = a.shCount ? *a.shCount : a.shN;
+    const int total = extCount + shCount;
+    int stack[MC_STACK_CAPACITY];
+    WatertightRay w;
+    w.kx = 0; w.ky = 1; w.kz = 2; w.sx = w.sy = w.sz = 0.f;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        TravState s;
+        int kind, slot, crossings = 0;
+        float T = 1.f, travelled = 0.f;
+        V3 o, d;
+        float time, tmax;
+        if (q < extCount) {
+            kind = 0;
+            slot = a.queue ? a.queue[q] : q;
+            o = V3(a.ox[slot], a.oy[slot], a.oz[slot]);
+            d = V3(a.dx[slot], a.dy[slot], a.dz[slot]);
+            time = a.time[slot];
+            tmax = 1e30f;
+        } else {
+            kind = 1;
+            slot = q - extCount;
+            o = V3(a.sox[slot], a.soy[slot], a.soz[slot]);
+            d = V3(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
+            time = a.spath ? a.time[a.spath[slot]] : a.time[slot];
+            tmax = a.smax[slot];
+            if (MEDIUM && tmax <= 0.0f) {
+                s.tmax = tmax;
+                s.hitLeaf = -1;
+                finish_ray<ISECT, MEDIUM>(a, s, STEP_DONE, kind, slot, T, travelled, crossings);
+                continue;
+            }
+        }
+        trav_begin(s, o, d, time, tmax);
+        if (ISECT == MC_ISECT_WATERTIGHT) w = make_watertight(d);
+        while (true) {
+            int r = (kind == 1 && !MEDIUM) ? trav_step<true, ISECT>(a.ts, s, stack, w, a.err)
+                                           : trav_step<false, ISECT>(a.ts, s, stack, w, a.err);
+            if (r != STEP_CONTINUE && finish_ray<ISECT, MEDIUM>(a, s, r, kind, slot, T, travelled, crossings)) break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shade
+// ---------------------------------------------------------------------------
+struct ShadeArgs {
+    const mc_sphere* spheres;
+    const mc_triangle_hot* hot;
+    const mc_triangle_cold* cold;
+    const mc_light* lights;
+    int lightCount;
+    mc_env_map env;
+    float3 background;
+    float rrCap;
+    int depth;
+    float *ox, *oy, *oz, *dx, *dy, *dz;
+    const float* time;
+    float *tr, *tg, *tb, *sr, *sg, *sb;
+    unsigned char* spec;
+    float* pdf;
+    uint32_t* draw;
+    const mc_packed_hit* hits;
+    const int* queue;
+    const int* count;
+    int* nextQueue;
+    int* nextCount;
+    float *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *scr, *scg, *scb;
+    int* spath;
+    int* shCount;
+    int capacity;
+    curandState* xorwow;
+    uint32_t seedLo, seedHi, sample;
+    int* err;
+};
+
+struct ShadeOut {
+    bool next;
+    bool shadow;
+    V3 so, sd, contrib;
+    float smax;
+};
+
+template <class Rng>
+MC_D void rng_load(const ShadeArgs& a, int p, Rng& rng);
+template <>
+MC_D void rng_load<PhiloxRng>(const ShadeArgs& a, int p, PhiloxRng& rng) {
+    rng.init(a.seedLo, a.seedHi, a.sample, (uint32_t)p, a.draw[p]);
+}
+template <>
+MC_D void rng_load<XorwowRng>(const ShadeArgs& a, int p, XorwowRng& rng) {
+    rng.st = a.xorwow[p];
+}
+template <class Rng>
+MC_D void rng_store(const ShadeArgs& a, int p, const Rng& rng);
+template <>
+MC_D void rng_store<PhiloxRng>(const ShadeArgs& a, int p, const PhiloxRng& rng) {
+    a.draw[p] = rng.draw;
+}
+template <>
+MC_D void rng_store<XorwowRng>(const ShadeArgs& a, int p, const XorwowRng& rng) {
+    a.xorwow[p] = rng.st;
+}
+
+struct MatView {
+    int type;
+    mc_texture albedo;
+    V3 emitted;
+    float fuzz, ior, density, g;
+};
+
+MC_D MatView load_material(const mc_material& m) {
+    MatView v;
+    v.type = m.type;
+    v.albedo = m.albedo;
+    v.emitted = v3(m.emitted);
+    v.fuzz = m.fuzz;
+    v.ior = m.refraction_index;
+    v.density = m.density;
+    v.g = m.phase_g;
+    return v;
+}
+
+// PT:3470-3696 shadeKernel for one path.
+template <class Rng>
+MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
+    const int depth = a.depth;
+    V3 throughput(a.tr[p], a.tg[p], a.tb[p]);
+    V3 cs(a.sr[p], a.sg[p], a.sb[p]);
+    int4 hraw = reinterpret_cast<const int4*>(a.hits)[p];
+    float hitT = __int_as_float(hraw.x);
+    int ptype = hraw.y, pidx = hraw.z, didHit = hraw.w;
+    const V3 background(a.background.x, a.background.y, a.background.z);
+    if (!didHit) {
+        V3 missDir(a.dx[p], a.dy[p], a.dz[p]);
+        float envW = 1.0f;
+        float envProb = env_selection_probability(a.env, a.lightCount);
+        if (!(depth == 0 || a.spec[p] != 0) && envProb > 0.0f)
+            envW = power_heuristic(a.pdf[p], envProb * env_direction_pdf(a.env, missDir));
+        cs = cs + throughput * env_radiance(a.env, missDir, background) * envW;
+        a.sr[p] = cs.x;
+        a.sg[p] = cs.y;
+        a.sb[p] = cs.z;
+        return;
+    }
+    MatView mat = load_material(ptype == 0 ? a.spheres[pidx].mat : a.cold[pidx].mat);
+    V3 inDir(a.dx[p], a.dy[p], a.dz[p]);
+    V3 o(a.ox[p], a.oy[p], a.oz[p]);
+    float rayTime = a.time[p];
+    V3 hitPoint = o + inDir * hitT;
+    V3 hitNormal;
+    bool frontFace;
+    float hitU, hitV;
+    V3 tv0, tv1, tv2;
+    if (ptype == 0) {
+        const mc_sphere& sp = a.spheres[pidx];
+        V3 c = sphere_center_at(v3(sp.center), v3(sp.center1), sp.is_moving != 0, rayTime);
+        V3 outward = (hitPoint - c).normalize();
+        frontFace = inDir.dot(outward) < 0.0f;
+        hitNormal = frontFace ? outward : -outward;
+        V2 uv = sphere_uv(outward);
+        hitU = uv.x;
+        hitV = uv.y;
+    } else {
+        const mc_triangle_hot& h = a.hot[pidx];
+        const mc_triangle_cold& cd = a.cold[pidx];
+        tv0 = v3(h.v0); tv1 = v3(h.v1); tv2 = v3(h.v2);
+        V3 e1 = tv1 - tv0;
+        V3 e2 = tv2 - tv0;
+        V3 nrm = e1.cross(e2).normalize();
+        frontFace = inDir.dot(nrm) < 0.0f;
+        V3 shading = triangle_shading_normal(tv0, tv1, tv2, v3(cd.n0), v3(cd.n1), v3(cd.n2), hitPoint, nrm);
+        hitNormal = frontFace ? shading : -shading;
+        V2 uv = triangle_uv(tv0, tv1, tv2, V2(cd.uv0.x, cd.uv0.y), V2(cd.uv1.x, cd.uv1.y), V2(cd.uv2.x, cd.uv2.y), hitPoint);
+        hitU = uv.x;
+        hitV = uv.y;
+    }
+    if (mat.type == MC_MAT_EMISSIVE) {
+        bool prevSpec = a.spec[p] != 0;
+        float emissionWeight = 1.0f;
+        bool fromBsdf = !(depth == 0 || prevSpec);
+        if (fromBsdf && ptype == 1) {
+            float cosL = fmaxf(fabsf(inDir.dot(hitNormal)), 1e-4f);
+            float area = triangle_area(tv0, tv1, tv2);
+            float lightPdf = light_solid_angle_pdf((1.0f - env_selection_probability(a.env, a.lightCount)) / float(a.lightCount),
+                                                   hitT, cosL, area);
+            emissionWeight = power_heuristic(a.pdf[p], lightPdf);
+        }
+        cs = cs + throughput * mat.emitted * emissionWeight;
+        a.sr[p] = cs.x;
+        a.sg[p] = cs.y;
+        a.sb[p] = cs.z;
+        return;
+    }
+    Rng rng;
+    rng_load<Rng>(a, p, rng);
+    V3 scatterOrigin = hitPoint;
+    if (mat.type == MC_MAT_ISOTROPIC) {
+        float sd;
+        if (frontFace) sd = hitT;
+        else sd = -logf(1.0f - rng.uniform()) / mat.density;
+        if (sd >= hitT) {
+            a.ox[p] = hitPoint.x;
+            a.oy[p] = hitPoint.y;
+            a.oz[p] = hitPoint.z;
+            out.next = true;
+            rng_store<Rng>(a, p, rng);
+            return;
+        }
+        scatterOrigin = o + inDir * sd;
+    }
+    throughput = throughput * sample_texture(mat.albedo, hitU, hitV);
+
+    float envProb = env_selection_probability(a.env, a.lightCount);
+    if ((mat.type == MC_MAT_LAMBERTIAN || mat.type == MC_MAT_ISOTROPIC) && (a.lightCount > 0 || envProb > 0.0f)) {
+        V3 toLight, lightColor;
+        float dist, solidPdf;
+        if (envProb > 0.0f && (a.lightCount == 0 || rng.uniform() < envProb)) {
+            float dirPdf;
+            toLight = env_sample(a.env, rng, dirPdf);
+            lightColor = env_radiance(a.env, toLight, V3(0.f, 0.f, 0.f));
+            dist = 1e30f;
+            solidPdf = envProb * dirPdf;
+        } else {
+            int li = min((int)(rng.uniform() * a.lightCount), a.lightCount - 1);
+            const mc_light& L = a.lights[li];
+            float sel = (1.0f - envProb) / float(a.lightCount);
+            V3 pt = sample_triangle(v3(L.tri.v0), v3(L.tri.v1), v3(L.tri.v2), rng);
+            V3 vec = pt - scatterOrigin;
+            dist = vec.length();
+            toLight = vec / dist;
+            lightColor = v3(L.emitted);
+            float cosL = fabsf(v3(L.normal).dot(toLight));
+            solidPdf = (cosL > 1e-4f) ? sel * (dist * dist) / (cosL * L.area) : 0.0f;
+        }
+        bool iso = (mat.type == MC_MAT_ISOTROPIC);
+        float cosS = iso ? 1.0f : hitNormal.dot(toLight);
+        if (cosS > 0.0f && solidPdf > 0.0f) {
+            float phasePdf = hg_phase_pdf(inDir.dot(toLight), mat.g);
+            float scatterPdf = iso ? phasePdf : lambertian_cosine_pdf(cosS);
+            float scatterValue = iso ? phasePdf : cosS / MC_PI;
+            float neeW = power_heuristic(solidPdf, scatterPdf);
+            V3 contribution = throughput * lightColor * (scatterValue / solidPdf) * neeW;
+            out.shadow = true;
+            out.so = scatterOrigin;
+            out.sd = toLight;
+            out.smax = dist * 0.999f;
+            out.contrib = contribution;
+        }
+    }
+    bool survives = true;
+    if (depth > 3) {
+        float maxC = fmaxf(throughput.x, fmaxf(throughput.y, throughput.z));
+        float cont = fminf(maxC, a.rrCap);
+        if (rng.uniform() > cont) survives = false;
+        else throughput = throughput / cont;
+    }
+    if (survives) {
+        V3 rayDir(a.dx[p], a.dy[p], a.dz[p]);
+        V3 nd;
+        switch (mat.type) {
+            case MC_MAT_CONDUCTOR: {
+                V3 refl = specular_scatter(rayDir, hitNormal);
+                nd = (refl + random_unit_vector(rng) * mat.fuzz).normalize();
+                break;
+            }
+            case MC_MAT_DIELECTRIC: {
+                float ratio = frontFace ? 1.0f / mat.ior : mat.ior;
+                nd = dielectric_scatter(rayDir, hitNormal, ratio, rng);
+                break;
+            }
+            case MC_MAT_ISOTROPIC: nd = hg_scatter(inDir, mat.g, rng); break;
+            case MC_MAT_LAMBERTIAN:
+            default: nd = lambertian_scatter(hitNormal, rng); break;
+        }
+        a.ox[p] = scatterOrigin.x;
+        a.oy[p] = scatterOrigin.y;
+        a.oz[p] = scatterOrigin.z;
+        a.dx[p] = nd.x;
+        a.dy[p] = nd.y;
+        a.dz[p] = nd.z;
+        a.tr[p] = throughput.x;
+        a.tg[p] = throughput.y;
+        a.tb[p] = throughput.z;
+        a.spec[p] = (mat.type != MC_MAT_LAMBERTIAN && mat.type != MC_MAT_ISOTROPIC) ? 1 : 0;
+        a.pdf[p] = (mat.type == MC_MAT_ISOTROPIC) ? hg_phase_pdf(inDir.dot(nd), mat.g)
+                                                   : lambertian_cosine_pdf(fmaxf(nd.dot(hitNormal), 0.0f));
+        out.next = true;
+    }
+    rng_store<Rng>(a, p, rng);
+}
+
+// Warp-aggregated append: one atomicAdd per warp, slots in lane order.
+MC_D int warp_reserve(bool want, int* counter, unsigned ltmask) {
+    unsigned m = __ballot_sync(kFull, want);
+    if (m == 0u) return -1;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(kFull, base, leader);
+    return want ? base + __popc(m & ltmask) : -1;
+}
+
+template <class Rng>
+__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
+    const unsigned ltmask = lanemask_lt();
+    const int count = *a.count;
+    for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+        int q = base + threadIdx.x;
+        ShadeOut out;
+        out.next = false;
+        out.shadow = false;
+        int p = -1;
+        if (q < count) {
+            p = a.queue[q];
+            shade_path<Rng>(a, p, out);
+        }
+        int ns = warp_reserve(out.shadow, a.shCount, ltmask);
+        if (out.shadow) {
+            if (ns < a.capacity) {
+                a.sox[ns] = out.so.x;
+                a.soy[ns] = out.so.y;
+                a.soz[ns] = out.so.z;
+                a.sdx[ns] = out.sd.x;
+                a.sdy[ns] = out.sd.y;
+                a.sdz[ns] = out.sd.z;
+                a.smax[ns] = out.smax;
+                a.scr[ns] = out.contrib.x;
+                a.scg[ns] = out.contrib.y;
+                a.scb[ns] = out.contrib.z;
+                a.spath[ns] = p;
+            } else {
+                atomicOr(a.err, MC_DEVERR_QUEUE);
+            }
+        }
+        int nn = warp_reserve(out.next, a.nextCount, ltmask);
+        if (out.next) {
+            if (nn < a.capacity) a.nextQueue[nn] = p;
+            else atomicOr(a.err, MC_DEVERR_QUEUE);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Camera rays (PT:3342-3374) and per-sample finalize (PT:3740-3755)
+// ---------------------------------------------------------------------------
+struct CameraArgs {
+    mc_camera cam;
+    int W, H;
+    float *ox, *oy, *oz, *dx, *dy, *dz, *time;
+    float *tr, *tg, *tb, *sr, *sg, *sb;
+    unsigned char* spec;
+    float* pdf;
+    uint32_t* draw;
+    int* queue;
+    int* count;
+    curandState* xorwow;
+    uint32_t seedLo, seedHi, sample;
+};
+
+template <class Rng>
+MC_D void camera_rng(const CameraArgs& a, int p, Rng& rng);
+template <>
+MC_D void camera_rng<PhiloxRng>(const CameraArgs& a, int p, PhiloxRng& rng) {
+    rng.init(a.seedLo, a.seedHi, a.sample, (uint32_t)p, 0u);
+}
+template <>
+MC_D void camera_rng<XorwowRng>(const CameraArgs& a, int p, XorwowRng& rng) {
+    rng.st = a.xorwow[p];
+}
+
+MC_D void camera_rng_store(const CameraArgs& a, int p, const PhiloxRng& rng) { a.draw[p] = rng.draw; }
+MC_D void camera_rng_store(const CameraArgs& a, int p, const XorwowRng& rng) { a.xorwow[p] = rng.st; }
+
+template <class Rng>
+__global__ void k_camera(CameraArgs a) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    int pixels = a.W * a.H;
+    if (p == 0) *a.count = pixels;
+    if (p >= pixels) return;
+    int px = p % a.W, py = p / a.W;
+    Rng rng;
+    camera_rng<Rng>(a, p, rng);
+    V3 o, d;
+    float t;
+    camera_ray(a.cam, px, py, rng, o, d, t);
+    a.ox[p] = o.x; a.oy[p] = o.y; a.oz[p] = o.z;
+    a.dx[p] = d.x; a.dy[p] = d.y; a.dz[p] = d.z;
+    a.time[p] = t;
+    a.tr[p] = 1.0f; a.tg[p] = 1.0f; a.tb[p] = 1.0f;
+    a.sr[p] = 0.0f; a.sg[p] = 0.0f; a.sb[p] = 0.0f;
+    a.spec[p] = 1;
+    a.pdf[p] = 1.0f;
+    a.queue[p] = p;
+    camera_rng_store(a, p, rng);
+}
+
+__global__ void k_finalize(float* accum, const float* sr, const float* sg, const float* sb, int pixels, int disableClamp) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    V3 s(sr[p], sg[p], sb[p]);
+    float bright = fmaxf(s.x, fmaxf(s.y, s.z));
+    const float maxBright = 10.0f;
+    if (!disableClamp && bright > maxBright) s = s * (maxBright / bright);
+    float* acc = accum + (size_t)p * 3;
+    acc[0] = acc[0] + s.x;
+    acc[1] = acc[1] + s.y;
+    acc[2] = acc[2] + s.z;
+}
+
+__global__ void k_accumulate_counts(const int* counters, int maxDepth, long long* stats) {
+    int d = threadIdx.x;
+    if (d >= maxDepth || d >= MC_MAX_DEPTH_STATS) return;
+    stats[d] += counters[d * MC_COUNTERS_PER_DEPTH + 0];
+    stats[MC_MAX_DEPTH_STATS + d] += counters[d * MC_COUNTERS_PER_DEPTH + 1];
+}
+
+__global__ void k_init_xorwow(curandState* states, int pixels, unsigned long long seed) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < pixels) curand_init(seed, p, 0, &states[p]);  // PT:2870
+}
+
+int occupancy_blocks(const void* fn, int sms) {
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, 0);
+    if (per < 1) per = 1;
+    return per * sms;
+}
+
+}  // namespace
+
+mc_status ensure_wave(mc_context* ctx, int capacity) {
+    WaveBuffers& w = ctx->wave;
+    if (w.capacity >= capacity && w.block.ptr) return MC_OK;
+    size_t n = (size_t)capacity;
+    // 28 float/int arrays of n entries (path state 15 + draw + 2 queues + shadow 11),
+    // one byte array and the 16-byte hit records; every array 256-byte aligned.
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t f4 = al(n * 4);
+    size_t total = 29 * f4 + al(n) + al(n * 16);
+    mc_status st = devbuf_reserve(w.block, total);
+    if (st != MC_OK) return st;
+    char* b = (char*)w.block.ptr;
+    auto take = [&](size_t bytes) { char* r = b; b += bytes; return r; };
+    w.ox = (float*)take(f4); w.oy = (float*)take(f4); w.oz = (float*)take(f4);
+    w.dx = (float*)take(f4); w.dy = (float*)take(f4); w.dz = (float*)take(f4);
+    w.time = (float*)take(f4);
+    w.tr = (float*)take(f4); w.tg = (float*)take(f4); w.tb = (float*)take(f4);
+    w.sr = (float*)take(f4); w.sg = (float*)take(f4); w.sb = (float*)take(f4);
+    w.pdf = (float*)take(f4);
+    w.draw = (uint32_t*)take(f4);
+    w.queue[0] = (int*)take(f4); w.queue[1] = (int*)take(f4);
+    w.sox = (float*)take(f4); w.soy = (float*)take(f4); w.soz = (float*)take(f4);
+    w.sdx = (float*)take(f4); w.sdy = (float*)take(f4); w.sdz = (float*)take(f4);
+    w.smax = (float*)take(f4);
+    w.scr = (float*)take(f4); w.scg = (float*)take(f4); w.scb = (float*)take(f4);
+    w.spath = (int*)take(f4);
+    take(f4);  // spare
+    w.spec = (unsigned char*)take(al(n));
+    w.hits = (mc_packed_hit*)take(al(n * 16));
+    w.capacity = capacity;
+    return MC_OK;
+}
+
+namespace {
+
+TraceArgs base_trace_args(const mc_bvh* bvh, const mc_scene_view* scene, mc_context* ctx) {
+    TraceArgs t;
+    std::memset(&t, 0, sizeof(t));
+    t.ts.nodes = (const float4*)bvh->nodes;
+    t.ts.prims = (const float4*)bvh->prims;
+    t.cold = scene->tri_cold;
+    t.spheres = scene->spheres;
+    t.err = ctx->d_error;
+    t.refill = 8;  // PT:3400 minimumIdleLanesBeforeRefill
+    return t;
+}
+
+typedef void (*TraceKernel)(TraceArgs);
+
+// [persistent][count][medium][isect]
+TraceKernel trace_kernel(bool persistent, bool count, bool medium, int isect) {
+    static const TraceKernel table[2][2][2][2] = {
+        {{{k_trace_simple<0, false>, k_trace_simple<1, false>}, {k_trace_simple<0, true>, k_trace_simple<1, true>}},
+         {{k_trace_simple<0, false>, k_trace_simple<1, false>}, {k_trace_simple<0, true>, k_trace_simple<1, true>}}},
+        {{{k_trace<0, false, false>, k_trace<1, false, false>}, {k_trace<0, true, false>, k_trace<1, true, false>}},
+         {{k_trace<0, false, true>, k_trace<1, false, true>}, {k_trace<0, true, true>, k_trace<1, true, true>}}}};
+    return table[persistent ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
+}
+
+// Persistent grid: one wave of resident blocks (SMs x resident blocks per SM).
+// Plain variant: one thread per ray over the queue capacity.
+void launch_trace(mc_context* ctx, const TraceArgs& t, bool medium, int isect, bool persistent, int simpleBlocks,
+                  bool count = false) {
+    static int occ[16] = {0};
+    TraceKernel fn = trace_kernel(persistent, count && persistent, medium, isect);
+    int blocks = std::max(1, simpleBlocks);
+    if (persistent) {
+        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0);
+        if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count);
+        blocks = occ[key];
+    }
+    fn<<<blocks, 256, 0, ctx->stream>>>(t);
+}
+
+mc_status check_render_inputs(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* p) {
+    if (!ctx || !bvh || !scene || !p) return set_error(MC_ERR_INVALID, "render: null argument");
+    if (p->width <= 0 || p->height <= 0) return set_error(MC_ERR_INVALID, "render: width and height must be positive");
+    if ((long long)p->width * p->height >= (1ll << 30)) return set_error(MC_ERR_INVALID, "render: too many pixels");
+    if (p->spp < 0) return set_error(MC_ERR_INVALID, "render: spp must be >= 0");
+    if (p->max_depth < 0 || p->max_depth > MC_MAX_DEPTH_STATS) return set_error(MC_ERR_INVALID, "render: max_depth must be in [0, 64]");
+    if (p->rng != MC_RNG_PHILOX && p->rng != MC_RNG_XORWOW) return set_error(MC_ERR_INVALID, "render: unknown rng mode");
+    if (p->intersector != MC_ISECT_REFERENCE && p->intersector != MC_ISECT_WATERTIGHT) return set_error(MC_ERR_INVALID, "render: unknown intersector");
+    if (scene->light_count > 0 && !scene->lights) return set_error(MC_ERR_INVALID, "render: null light array");
+    if (scene->triangle_count > 0 && !scene->tri_cold) return set_error(MC_ERR_INVALID, "render: null cold triangle array");
+    if (scene->sphere_count + scene->triangle_count != bvh->n) return set_error(MC_ERR_INVALID, "render: the BVH was built for another scene");
+    return MC_OK;
+}
+
+}  // namespace
+
+mc_status rng_reset(mc_context* ctx, int pixels, unsigned long long seed) {
+    if (ctx->rng_pixels < pixels || !ctx->rng_states) {
+        if (ctx->rng_states) cudaFree(ctx->rng_states);
+        ctx->rng_states = nullptr;
+        ctx->rng_pixels = 0;
+        if (cudaMalloc(&ctx->rng_states, (size_t)pixels * sizeof(curandState)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(MC_ERR_OOM, "rng: allocation of %d states failed", pixels);
+        }
+        ctx->rng_pixels = pixels;
+    }
+    k_init_xorwow<<<(pixels + 255) / 256, 256, 0, ctx->stream>>>((curandState*)ctx->rng_states, pixels, seed);
+    MC_CUDA(cudaGetLastError());
+    ctx->rng_seed = seed;
+    ctx->rng_ready = true;
+    return MC_OK;
+}
+
+struct RenderTiming {
+    float ms = 0.f;
+    float trace_ms = 0.f;
+    int trace_launches = 0;
+    int kernel_launches = 0;
+};
+
+mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* p,
+                         float* accum, bool timed, RenderTiming* tm) {
+    const int W = p->width, H = p->height, pixels = W * H;
+    const int maxD = p->max_depth;
+    WaveBuffers& w = ctx->wave;
+    const bool medium = scene->has_medium != 0;
+    const int isect = p->intersector;
+    const bool philox = p->rng == MC_RNG_PHILOX;
+    curandState* xs = (curandState*)ctx->rng_states;
+    static int shadeBlocks[2] = {0, 0};
+    if (!shadeBlocks[0]) shadeBlocks[0] = occupancy_blocks((const void*)k_shade<PhiloxRng>, ctx->sm_count);
+    if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng>, ctx->sm_count);
+    const int simpleBlocks = (pixels + 255) / 256;
+
+    mc_camera cam = p->camera;
+    CameraArgs ca;
+    ca.cam = cam; ca.W = W; ca.H = H;
+    ca.ox = w.ox; ca.oy = w.oy; ca.oz = w.oz; ca.dx = w.dx; ca.dy = w.dy; ca.dz = w.dz; ca.time = w.time;
+    ca.tr = w.tr; ca.tg = w.tg; ca.tb = w.tb; ca.sr = w.sr; ca.sg = w.sg; ca.sb = w.sb;
+    ca.spec = w.spec; ca.pdf = w.pdf; ca.draw = w.draw; ca.queue = w.queue[0];
+    ca.count = ctx->d_counters;
+    ca.xorwow = xs;
+    ca.seedLo = (uint32_t)p->seed; ca.seedHi = (uint32_t)(p->seed >> 32);
+
+    ShadeArgs sa;
+    sa.spheres = scene->spheres; sa.hot = scene->tri_hot; sa.cold = scene->tri_cold;
+    sa.lights = scene->lights; sa.lightCount = scene->light_count;
+    sa.env = scene->env;
+    sa.background = make_float3(cam.background.x, cam.background.y, cam.background.z);
+    sa.rrCap = cam.rr_cap;
+    sa.ox = w.ox; sa.oy = w.oy; sa.oz = w.oz; sa.dx = w.dx; sa.dy = w.dy; sa.dz = w.dz; sa.time = w.time;
+    sa.tr = w.tr; sa.tg = w.tg; sa.tb = w.tb; sa.sr = w.sr; sa.sg = w.sg; sa.sb = w.sb;
+    sa.spec = w.spec; sa.pdf = w.pdf; sa.draw = w.draw; sa.hits = w.hits;
+    sa.sox = w.sox; sa.soy = w.soy; sa.soz = w.soz; sa.sdx = w.sdx; sa.sdy = w.sdy; sa.sdz = w.sdz; sa.smax = w.smax;
+    sa.scr = w.scr; sa.scg = w.scg; sa.scb = w.scb; sa.spath = w.spath;
+    sa.capacity = w.capacity;
+    sa.xorwow = xs;
+    sa.seedLo = ca.seedLo; sa.seedHi = ca.seedHi;
+    sa.err = ctx->d_error;
+
+    TraceArgs ta = base_trace_args(bvh, scene, ctx);
+    ta.ox = w.ox; ta.oy = w.oy; ta.oz = w.oz; ta.dx = w.dx; ta.dy = w.dy; ta.dz = w.dz; ta.time = w.time;
+    ta.hits = w.hits;
+    ta.sox = w.sox; ta.soy = w.soy; ta.soz = w.soz; ta.sdx = w.sdx; ta.sdy = w.sdy; ta.sdz = w.sdz; ta.smax = w.smax;
+    ta.scr = w.scr; ta.scg = w.scg; ta.scb = w.scb; ta.spath = w.spath;
+    ta.sr = w.sr; ta.sg = w.sg; ta.sb = w.sb;
+    if (p->refill_threshold > 0 && p->refill_threshold <= 32) ta.refill = p->refill_threshold;
+
+    const bool countVisits = (p->instrument & 1) != 0;
+    const bool timeTrace = (p->instrument & 2) != 0;
+    if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
+    int* C = ctx->d_counters;
+    const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<cudaEvent_t> traceEvents;
+    if (timed) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, ctx->stream);
+    }
+    if (tm) {
+        tm->kernel_launches = 0;
+        tm->trace_launches = 0;
+        tm->trace_ms = 0.f;
+    }
+    auto traceEvent = [&]() {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, ctx->stream);
+        traceEvents.push_back(e);
+    };
+    for (int s = 0; s < p->spp; s++) {
+        uint32_t sample = (uint32_t)(p->first_sample + s);
+        ca.sample = sample;
+        sa.sample = sample;
+        MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, ctx->stream));
+        if (philox) k_camera<PhiloxRng><<<(pixels + 255) / 256, 256, 0, ctx->stream>>>(ca);
+        else k_camera<XorwowRng><<<(pixels + 255) / 256, 256, 0, ctx->stream>>>(ca);
+        for (int d = 0; d <= maxD; d++) {
+            TraceArgs t = ta;
+            if (d < maxD) {
+                t.queue = w.queue[d & 1];
+                t.extCount = C + d * MC_COUNTERS_PER_DEPTH + 0;
+            } else {
+                t.queue = nullptr;
+                t.extCount = nullptr;
+                t.extN = 0;
+            }
+            if (d > 0) t.shCount = C + (d - 1) * MC_COUNTERS_PER_DEPTH + 1;
+            else { t.shCount = nullptr; t.shN = 0; }
+            t.work = C + d * MC_COUNTERS_PER_DEPTH + 2;
+            if (timeTrace) traceEvent();
+            launch_trace(ctx, t, medium, isect, p->persistent != 0, simpleBlocks, countVisits);
+            if (timeTrace) traceEvent();
+            if (tm) tm->kernel_launches++;
+            if (d == maxD) break;
+            ShadeArgs sd = sa;
+            sd.depth = d;
+            sd.queue = w.queue[d & 1];
+            sd.count = C + d * MC_COUNTERS_PER_DEPTH + 0;
+            sd.nextQueue = w.queue[(d + 1) & 1];
+            sd.nextCount = C + (d + 1) * MC_COUNTERS_PER_DEPTH + 0;
+            sd.shCount = C + d * MC_COUNTERS_PER_DEPTH + 1;
+            if (philox) k_shade<PhiloxRng><<<shadeBlocks[0], 256, 0, ctx->stream>>>(sd);
+            else k_shade<XorwowRng><<<shadeBlocks[1], 256, 0, ctx->stream>>>(sd);
+            if (tm) tm->kernel_launches++;
+        }
+        k_finalize<<<(pixels + 255) / 256, 256, 0, ctx->stream>>>(accum, w.sr, w.sg, w.sb, pixels, p->disable_clamp);
+        k_accumulate_counts<<<1, 64, 0, ctx->stream>>>(C, maxD, ctx->d_stats);
+        if (tm) tm->kernel_launches += 3;  // camera, finalize, count accumulation
+    }
+    MC_CUDA(cudaGetLastError());
+    if (timed) {
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (tm) tm->ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (!traceEvents.empty()) {
+        cudaEventSynchronize(traceEvents.back());
+        for (size_t i = 0; i + 1 < traceEvents.size(); i += 2) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, traceEvents[i], traceEvents[i + 1]);
+            if (tm) {
+                tm->trace_ms += ms;
+                tm->trace_launches++;
+            }
+        }
+        for (cudaEvent_t e : traceEvents) cudaEventDestroy(e);
+    }
+    return MC_OK;
+}
+
+}  // namespace mc
+
+extern "C" {
+
+mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed) {
+    if (!ctx || width <= 0 || height <= 0) return mc::set_error(MC_ERR_INVALID, "mc_rng_reset: bad argument");
+    return mc::rng_reset(ctx, width * height, seed);
+}
+
+mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* params,
+                              float* d_accum, mc_render_stats* stats) {
+    mc_status st = mc::check_render_inputs(ctx, bvh, scene, params);
+    if (st != MC_OK) return st;
+    if (!d_accum) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: null accumulation buffer");
+    int pixels = params->width * params->height;
+    int cap = params->queue_capacity > 0 ? params->queue_capacity : pixels;
+    if (cap < pixels) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: queue capacity below width*height");
+    if ((st = mc::ensure_wave(ctx, cap)) != MC_OK) return st;
+    if (params->rng == MC_RNG_XORWOW && (!ctx->rng_ready || ctx->rng_pixels < pixels || ctx->rng_seed != params->seed)) {
+        if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
+    }
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    MC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long), ctx->stream));
+    mc::RenderTiming tm;
+    st = mc::render_samples(ctx, bvh, scene, params, d_accum, stats != nullptr, &tm);
+    if (st != MC_OK) return st;
+    int flags = 0;
+    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        long long h[2 * MC_MAX_DEPTH_STATS + 8];
+        MC_CUDA(cudaMemcpyAsync(h, ctx->d_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        MC_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int d = 0; d < MC_MAX_DEPTH_STATS; d++) {
+            stats->extend_per_depth[d] = h[d];
+            stats->shadow_per_depth[d] = h[MC_MAX_DEPTH_STATS + d];
+            stats->extend_rays += h[d];
+            stats->shadow_rays += h[MC_MAX_DEPTH_STATS + d];
+        }
+        stats->node_visits = h[2 * MC_MAX_DEPTH_STATS];
+        stats->leaf_tests = h[2 * MC_MAX_DEPTH_STATS + 1];
+        stats->paths = (long long)pixels * params->spp;
+        stats->render_ms = tm.ms;
+        stats->trace_ms = tm.trace_ms;
+        stats->trace_launches = tm.trace_launches;
+        stats->kernel_launches = tm.kernel_launches;
+        stats->error_flags = flags;
+    } else {
+        MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return mc::status_from_device_flags(flags);
+}
+
+mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const float* d_rays, int32_t n,
+                           int32_t intersector, mc_packed_hit* d_hits) {
+    if (!ctx || !bvh || !scene || !d_rays || !d_hits || n < 0) return mc::set_error(MC_ERR_INVALID, "mc_trace_closest: bad argument");
+    if (intersector != MC_ISECT_REFERENCE && intersector != MC_ISECT_WATERTIGHT) return mc::set_error(MC_ERR_INVALID, "mc_trace_closest: unknown intersector");
+    if (n == 0) return MC_OK;
+    mc_status st;
+    if ((st = mc::devbuf_reserve(ctx->scratch[5], 64)) != MC_OK) return st;
+    int* work = (int*)ctx->scratch[5].ptr;
+    MC_CUDA(cudaMemsetAsync(work, 0, sizeof(int), ctx->stream));
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    mc::TraceArgs t = mc::base_trace_args(bvh, scene, ctx);
+    size_t N = (size_t)n;
+    t.queue = nullptr;
+    t.extCount = nullptr;
+    t.extN = n;
+    t.ox = d_rays; t.oy = d_rays + N; t.oz = d_rays + 2 * N;
+    t.dx = d_rays + 3 * N; t.dy = d_rays + 4 * N; t.dz = d_rays + 5 * N; t.time = d_rays + 6 * N;
+    t.hits = d_hits;
+    t.shCount = nullptr;
+    t.shN = 0;
+    t.work = work;
+    mc::launch_trace(ctx, t, false, intersector, true, 0);
+    MC_CUDA(cudaGetLastError());
+    int flags = 0;
+    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return mc::status_from_device_flags(flags);
+}
+
+mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const float* d_rays, const float* d_tmax,
+                       int32_t n, int32_t intersector, int32_t* d_occluded) {
+    if (!ctx || !bvh || !scene || !d_rays || !d_tmax || !d_occluded || n < 0) return mc::set_error(MC_ERR_INVALID, "mc_trace_any: bad argument");
+    if (intersector != MC_ISECT_REFERENCE && intersector != MC_ISECT_WATERTIGHT) return mc::set_error(MC_ERR_INVALID, "mc_trace_any: unknown intersector");
+    if (n == 0) return MC_OK;
+    mc_status st;
+    if ((st = mc::devbuf_reserve(ctx->scratch[5], 64)) != MC_OK) return st;
+    int* work = (int*)ctx->scratch[5].ptr;
+    MC_CUDA(cudaMemsetAsync(work, 0, sizeof(int), ctx->stream));
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    mc::TraceArgs t = mc::base_trace_args(bvh, scene, ctx);
+    size_t N = (size_t)n;
+    t.queue = nullptr;
+    t.extCount = nullptr;
+    t.extN = 0;
+    t.shCount = nullptr;
+    t.shN = n;
+    t.sox = d_rays; t.soy = d_rays + N; t.soz = d_rays + 2 * N;
+    t.sdx = d_rays + 3 * N; t.sdy = d_rays + 4 * N; t.sdz = d_rays + 5 * N;
+    t.time = d_rays + 6 * N;
+    t.spath = nullptr;
+    t.smax = d_tmax;
+    t.occluded = d_occluded;
+    t.work = work;
+    mc::launch_trace(ctx, t, false, intersector, true, 0);
+    MC_CUDA(cudaGetLastError());
+    int flags = 0;
+    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return mc::status_from_device_flags(flags);
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// mc_traverse.cuh - BVH traversal over the library's node layout.
+//
+// Binary layout: one 64-byte record per internal node holding BOTH children's
+// boxes and references (leaf child k -> ~k), so a traversal step is one
+// contiguous 64-byte read instead of the reference's node read plus two child
+// box reads (PT:1276-1321). Leaves are 48-byte primitive records in leaf
+// (sorted Morton) order: a triangle's three vertices plus its id and type.
+//
+// The visit order and every test follow the reference's stepTraversal /
+// traverseAnyHit (PT:1152-1321): both child boxes are tested against the
+// current closest distance, a leaf child is intersected on the spot (left then
+// right), internal children are descended left first with the right one
+// pushed. Closest hits keep the first primitive found at equal t (strict <).
+#pragma once
+#include "mc_math.cuh"
+
+namespace mc {
+
+enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_OCCLUDED = 2 };
+
+struct TraceScene {
+    const float4* __restrict__ nodes;   // binary: 4 float4 per internal node
+    const float4* __restrict__ prims;   // 3 float4 per leaf
+};
+
+// Traversal state of one ray in one lane.
+struct TravState {
+    RayInv r;
+    float time;
+    float tmax;     // closest distance so far (closest) or the segment length (any hit)
+    int hitLeaf;    // leaf slot of the closest hit, -1 none
+    int node;
+    int sp;
+};
+
+MC_D void trav_begin(TravState& s, const V3& o, const V3& d, float time, float tmax) {
+    s.r = make_ray_inv(o, d);
+    s.time = time;
+    s.tmax = tmax;
+    s.hitLeaf = -1;
+    s.node = 0;
+    s.sp = 0;
+}
+
+MC_D float4 ldg4(const float4* p) { return __ldg(p); }
+
+// Intersects leaf slot k; returns true and t when the primitive is hit with
+// t in the reference's accepted range (hit_* internal checks).
+template <int ISECT>
+MC_D bool leaf_hit(const TraceScene& sc, int k, const TravState& s, const WatertightRay& w, float& t) {
+    const float4* rec = sc.prims + (long long)k * 3;
+    float4 a = ldg4(rec + 0), b = ldg4(rec + 1), c = ldg4(rec + 2);
+    int type = __float_as_int(c.z);
+    if (type == 1) {
+        V3 v0(a.x, a.y, a.z), v1(a.w, b.x, b.y), v2(b.z, b.w, c.x);
+        if (ISECT == 0) return hit_triangle_ref(v0, v1, v2, s.r.o, s.r.d, t);
+        return hit_triangle_watertight(w, v0, v1, v2, s.r.o, t);
+    }
+    bool front;
+    V3 outward;
+    return hit_sphere_ref(V3(a.x, a.y, a.z), V3(a.w, b.x, b.y), b.w != 0.f, b.z, s.r.o, s.r.d, s.time, t, front, outward);
+}
+
+// One traversal step. ANY: any-hit semantics (PT:1152-1207): boxes are tested
+// against the fixed segment length and the first blocker in (1e-4, tmax) ends
+// the ray. Otherwise closest hit (PT:1276-1321 + testPrimitiveClosest 1537-1551).
+// Counters of the instrumented variant: node visits and primitive tests.
+struct TravCount {
+    int visits = 0;
+    int leaves = 0;
+};
+
+template <bool ANY, int ISECT, bool COUNT = false>
+MC_D int trav_step(const TraceScene& sc, TravState& s, int* stack, const WatertightRay& w, int* err,
+                   TravCount* cnt = nullptr) {
+    const float4* nd = sc.nodes + (long long)s.node * 4;
+    float4 a = ldg4(nd + 0), b = ldg4(nd + 1), c = ldg4(nd + 2), d = ldg4(nd + 3);
+    int lref = __float_as_int(d.x), rref = __float_as_int(d.y);
+    bool oL = hit_box(s.r, a.x, a.y, a.z, a.w, b.x, b.y, s.tmax);
+    bool oR = hit_box(s.r, b.z, b.w, c.x, c.y, c.z, c.w, s.tmax);
+    bool lLeaf = lref < 0, rLeaf = rref < 0;
+    if (COUNT) {
+        cnt->visits++;
+        cnt->leaves += (oL && lLeaf ? 1 : 0) + (oR && rLeaf ? 1 : 0);
+    }
+    if (oL && lLeaf) {
+        float t;
+        if (leaf_hit<ISECT>(sc, ~lref, s, w, t)) {
+            if (ANY) {
+                if (t > 0.0001f && t < s.tmax) return STEP_OCCLUDED;
+            } else if (t < s.tmax && t > 0.0001f) {
+                s.tmax = t;
+                s.hitLeaf = ~lref;
+            }
+        }
+    }
+    if (oR && rLeaf) {
+        float t;
+        if (leaf_hit<ISECT>(sc, ~rref, s, w, t)) {
+            if (ANY) {
+                if (t > 0.0001f && t < s.tmax) return STEP_OCCLUDED;
+            } else if (t < s.tmax && t > 0.0001f) {
+                s.tmax = t;
+                s.hitLeaf = ~rref;
+            }
+        }
+    }
+    bool tL = oL && !lLeaf, tR = oR && !rLeaf;
+    if (!tL && !tR) {
+        if (s.sp == 0) return STEP_DONE;
+        s.sp--;
+        s.node = stack[s.sp];
+    } else {
+        if (tL && tR) {
+            if (s.sp >= MC_STACK_CAPACITY) {
+                atomicOr(err, MC_DEVERR_STACK);
+                return STEP_DONE;
+            }
+            stack[s.sp] = rref;
+            s.sp++;
+        }
+        s.node = tL ? lref : rref;
+    }
+    return STEP_CONTINUE;
+}
+
+// The hit record fields a leaf slot stands for.
+MC_D void leaf_identity(const TraceScene& sc, int k, int& type, int& id) {
+    float4 c = ldg4(sc.prims + (long long)k * 3 + 2);
+    id = __float_as_int(c.y);
+    type = __float_as_int(c.z);
+}
+
+}  // namespace mc

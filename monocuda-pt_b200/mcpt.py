@@ -1,0 +1,412 @@
+"""ctypes binding of the C ABI in include/mc_abi.h (libmcpt.so, built in-tree).
+
+The library is the product; this module only mirrors its structs and entry
+points for Python callers (tests, bench.py, the render server driver). It
+raises McError on any non-OK status and never falls back to anything else:
+if libmcpt.so is missing or no GPU is present, the calls fail loudly.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmcpt.so")
+
+MC_OK = 0
+STATUS_NAMES = {0: "MC_OK", 1: "MC_ERR_INVALID", 2: "MC_ERR_CUDA", 3: "MC_ERR_OOM", 4: "MC_ERR_STACK_OVERFLOW",
+                5: "MC_ERR_QUEUE_OVERFLOW", 6: "MC_ERR_TIMEOUT", 7: "MC_ERR_BUDGET", 8: "MC_ERR_CANCELLED",
+                9: "MC_ERR_NOT_FOUND", 10: "MC_ERR_UNSUPPORTED"}
+MAT_LAMBERTIAN, MAT_DIELECTRIC, MAT_CONDUCTOR, MAT_EMISSIVE, MAT_ISOTROPIC = 0, 1, 2, 3, 4
+TEX_SOLID, TEX_CHECKER, TEX_IMAGE = 0, 1, 2
+RNG_PHILOX, RNG_XORWOW = 0, 1
+ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
+LAYOUT_BINARY, LAYOUT_WIDE4 = 0, 1
+SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
+MAX_DEPTH_STATS = 64
+
+
+class McError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class Vec2(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float)]
+
+
+class AABB(C.Structure):
+    _fields_ = [("lo", Vec3), ("pad0", C.c_float), ("hi", Vec3), ("pad1", C.c_float)]
+
+
+class Texture(C.Structure):
+    _fields_ = [("type", C.c_int32), ("color_a", Vec3), ("color_b", Vec3), ("scale", C.c_float), ("image", C.c_uint64)]
+
+
+class Material(C.Structure):
+    _fields_ = [("type", C.c_int32), ("albedo", Texture), ("emitted", Vec3), ("fuzz", C.c_float),
+                ("refraction_index", C.c_float), ("density", C.c_float), ("phase_g", C.c_float),
+                ("density_grid", C.c_void_p), ("grid_max_density", C.c_float)]
+
+
+class Triangle(C.Structure):
+    _fields_ = [("v0", Vec3), ("v1", Vec3), ("v2", Vec3), ("uv0", Vec2), ("uv1", Vec2), ("uv2", Vec2),
+                ("n0", Vec3), ("n1", Vec3), ("n2", Vec3), ("mat", Material), ("aabb", AABB)]
+
+
+class TriangleHot(C.Structure):
+    _fields_ = [("v0", Vec3), ("v1", Vec3), ("v2", Vec3)]
+
+
+class TriangleCold(C.Structure):
+    _fields_ = [("uv0", Vec2), ("uv1", Vec2), ("uv2", Vec2), ("n0", Vec3), ("n1", Vec3), ("n2", Vec3),
+                ("mat", Material), ("aabb", AABB)]
+
+
+class Sphere(C.Structure):
+    _fields_ = [("center", Vec3), ("center1", Vec3), ("is_moving", C.c_uint8), ("radius", C.c_float),
+                ("mat", Material), ("aabb", AABB)]
+
+
+class Light(C.Structure):
+    _fields_ = [("tri", TriangleHot), ("emitted", Vec3), ("area", C.c_float), ("normal", Vec3)]
+
+
+class BvhNode(C.Structure):
+    _fields_ = [("bounds", AABB), ("left", C.c_int32), ("right", C.c_int32), ("left_is_leaf", C.c_uint8),
+                ("right_is_leaf", C.c_uint8), ("parent", C.c_int32), ("prim", C.c_int32), ("is_leaf", C.c_uint8),
+                ("_tail", C.c_uint8 * 11)]  # the C struct is 16-byte aligned (it holds an AABB): 64 bytes
+
+
+class PackedHit(C.Structure):
+    _fields_ = [("t", C.c_float), ("type", C.c_int32), ("index", C.c_int32), ("did_hit", C.c_int32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("aspect_ratio", C.c_float), ("image_width", C.c_int32), ("image_height", C.c_int32),
+                ("samples_per_pixel", C.c_int32), ("max_depth", C.c_int32), ("vfov", C.c_float),
+                ("look_from", Vec3), ("look_at", Vec3), ("up", Vec3), ("center", Vec3), ("pixel00", Vec3),
+                ("pixel_delta_u", Vec3), ("pixel_delta_v", Vec3), ("u", Vec3), ("v", Vec3), ("w", Vec3),
+                ("background", Vec3), ("aperture", C.c_float), ("lens_radius", C.c_float),
+                ("focus_distance", C.c_float), ("rr_cap", C.c_float)]
+
+
+class EnvMap(C.Structure):
+    _fields_ = [("texture", C.c_uint64), ("enabled", C.c_int32), ("intensity", C.c_float), ("rotation", C.c_float),
+                ("row_cdf", C.c_void_p), ("col_cdf", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32),
+                ("total_weight", C.c_float)]
+
+
+class SceneView(C.Structure):
+    _fields_ = [("spheres", C.c_void_p), ("sphere_count", C.c_int32), ("tri_hot", C.c_void_p), ("tri_cold", C.c_void_p),
+                ("triangle_count", C.c_int32), ("lights", C.c_void_p), ("light_count", C.c_int32),
+                ("has_medium", C.c_int32), ("env", EnvMap)]
+
+
+class BvhBuildOpts(C.Structure):
+    _fields_ = [("permutation", C.c_void_p), ("layout", C.c_int32), ("keep_reference_nodes", C.c_int32)]
+
+
+class BvhInfo(C.Structure):
+    _fields_ = [("primitive_count", C.c_int32), ("internal_count", C.c_int32), ("depth", C.c_int32),
+                ("layout", C.c_int32), ("node_bytes", C.c_int64), ("prim_bytes", C.c_int64), ("scene_bounds", AABB)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("camera", Camera), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
+                ("first_sample", C.c_int32), ("max_depth", C.c_int32), ("persistent", C.c_int32), ("rng", C.c_int32),
+                ("seed", C.c_uint64), ("intersector", C.c_int32), ("disable_clamp", C.c_int32),
+                ("queue_capacity", C.c_int32), ("refill_threshold", C.c_int32), ("use_graph", C.c_int32),
+                ("instrument", C.c_int32)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("extend_rays", C.c_int64), ("shadow_rays", C.c_int64), ("paths", C.c_int64),
+                ("extend_per_depth", C.c_int64 * MAX_DEPTH_STATS), ("shadow_per_depth", C.c_int64 * MAX_DEPTH_STATS),
+                ("node_visits", C.c_int64), ("leaf_tests", C.c_int64), ("render_ms", C.c_float), ("trace_ms", C.c_float),
+                ("trace_launches", C.c_int32), ("kernel_launches", C.c_int32), ("error_flags", C.c_int32)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("variant", C.c_int32), ("seed", C.c_uint64), ("triangle_target", C.c_int32)]
+
+
+class SceneHost(C.Structure):
+    _fields_ = [("triangles", C.POINTER(Triangle)), ("triangle_count", C.c_int32), ("spheres", C.POINTER(Sphere)),
+                ("sphere_count", C.c_int32), ("camera", Camera), ("width", C.c_int32), ("height", C.c_int32),
+                ("spp", C.c_int32), ("max_depth", C.c_int32), ("has_medium", C.c_int32),
+                ("env_rgba", C.POINTER(C.c_float)), ("env_width", C.c_int32), ("env_height", C.c_int32),
+                ("env_intensity", C.c_float)]
+
+
+SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56}
+for _t, _s in SIZES.items():
+    assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
+
+P = C.c_void_p
+I32 = C.c_int32
+# name -> (restype, argtypes); every function declared in include/mc_abi.h
+SIGNATURES = {
+    "mc_version": (C.c_char_p, []),
+    "mc_status_string": (C.c_char_p, [I32]),
+    "mc_last_error": (C.c_char_p, []),
+    "mc_context_create": (I32, [I32, C.POINTER(P)]),
+    "mc_context_destroy": (I32, [P]),
+    "mc_context_set_stream": (I32, [P, P]),
+    "mc_context_synchronize": (I32, [P]),
+    "mc_camera_initialize": (I32, [C.POINTER(Camera)]),
+    "mc_scene_finalize_host": (I32, [P, I32, P, C.POINTER(I32)]),
+    "mc_split_triangles_host": (I32, [P, I32, P, P]),
+    "mc_env_create": (I32, [P, I32, I32, C.c_float, C.c_float, C.POINTER(EnvMap)]),
+    "mc_env_destroy": (I32, [C.POINTER(EnvMap)]),
+    "mc_scene_generate": (I32, [C.POINTER(SceneDesc), C.POINTER(SceneHost)]),
+    "mc_scene_free": (I32, [C.POINTER(SceneHost)]),
+    "mc_morton_codes": (I32, [P, C.POINTER(SceneView), P, C.POINTER(AABB)]),
+    "mc_radix_sort_pairs": (I32, [P, P, P, I32, I32]),
+    "mc_bvh_build": (I32, [P, C.POINTER(SceneView), C.POINTER(BvhBuildOpts), C.POINTER(P)]),
+    "mc_bvh_free": (I32, [P]),
+    "mc_bvh_get_info": (I32, [P, C.POINTER(BvhInfo)]),
+    "mc_bvh_export": (I32, [P, P, P, P, P, P]),
+    "mc_trace_closest": (I32, [P, P, C.POINTER(SceneView), P, I32, I32, P]),
+    "mc_trace_any": (I32, [P, P, C.POINTER(SceneView), P, P, I32, I32, P]),
+    "mc_render_wavefront": (I32, [P, P, C.POINTER(SceneView), C.POINTER(RenderParams), P, C.POINTER(RenderStats)]),
+    "mc_render_host": (I32, [P, P, I32, P, I32, C.POINTER(EnvMap), C.POINTER(RenderParams), P, C.POINTER(RenderStats)]),
+    "mc_rng_reset": (I32, [P, I32, I32, C.c_uint64]),
+    "mc_autotune": (I32, [P, P, C.POINTER(SceneView), C.POINTER(RenderParams), I32]),
+}
+
+_lib = None
+
+
+def load(path=None):
+    """Loads libmcpt.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise McError(10, "libmcpt.so not built (run monocuda-pt_b200/build.py): %s" % path)
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status):
+    if status != MC_OK:
+        msg = load().mc_last_error()
+        raise McError(status, msg.decode() if msg else "")
+    return status
+
+
+def ptr(x):
+    """Device/host address of a torch tensor, numpy array, ctypes object or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    return C.addressof(x)
+
+
+class Context:
+    def __init__(self, device=0):
+        self.lib = load()
+        h = P()
+        check(self.lib.mc_context_create(device, C.byref(h)))
+        self.handle = h
+
+    def set_stream(self, stream_ptr):
+        check(self.lib.mc_context_set_stream(self.handle, stream_ptr))
+
+    def synchronize(self):
+        check(self.lib.mc_context_synchronize(self.handle))
+
+    def close(self):
+        if self.handle:
+            self.lib.mc_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Bvh:
+    def __init__(self, ctx, view, permutation=None, layout=LAYOUT_BINARY, keep_reference_nodes=False):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        opts = BvhBuildOpts(ptr(permutation), layout, 1 if keep_reference_nodes else 0)
+        h = P()
+        check(self.lib.mc_bvh_build(ctx.handle, C.byref(view), C.byref(opts), C.byref(h)))
+        self.handle = h
+
+    def info(self):
+        i = BvhInfo()
+        check(self.lib.mc_bvh_get_info(self.handle, C.byref(i)))
+        return i
+
+    def export(self, codes=None, ids=None, types=None, internal=None, leaves=None):
+        check(self.lib.mc_bvh_export(self.handle, ptr(codes), ptr(ids), ptr(types), ptr(internal), ptr(leaves)))
+
+    def close(self):
+        if self.handle:
+            self.lib.mc_bvh_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def host_triangles(scene):
+    """The scene's triangle array as a ctypes array view (no copy)."""
+    return (Triangle * scene.triangle_count).from_address(C.addressof(scene.triangles.contents))
+
+
+def host_env(scene):
+    """The scene's environment image as a numpy (H, W, 4) view, or None."""
+    if not scene.env_rgba or scene.env_width <= 0:
+        return None
+    import numpy as np
+    n = scene.env_width * scene.env_height * 4
+    buf = (C.c_float * n).from_address(C.addressof(scene.env_rgba.contents))
+    return np.frombuffer(buf, dtype=np.float32).reshape(scene.env_height, scene.env_width, 4)
+
+
+class DeviceScene:
+    """Uploads host triangles/spheres the way the reference's main() does
+    (PT:4276-4303): hot/cold split, light list, environment texture. Device
+    memory comes from torch (plumbing only); the view is an mc_scene_view."""
+
+    def __init__(self, triangles, spheres=None, env_rgba=None, env_intensity=1.0, env_rotation=0.0, device="cuda"):
+        import numpy as np
+        import torch
+        lib = load()
+        self.lib = lib
+        n = len(triangles)
+        ns = len(spheres) if spheres is not None else 0
+        hot = (TriangleHot * max(n, 1))()
+        cold = (TriangleCold * max(n, 1))()
+        tri_addr = C.addressof(triangles) if n else None
+        check(lib.mc_split_triangles_host(tri_addr, n, C.addressof(hot), C.addressof(cold)))
+        nl = I32()
+        tcopy = (Triangle * max(n, 1))()
+        if n:
+            C.memmove(tcopy, triangles, C.sizeof(Triangle) * n)
+        check(lib.mc_scene_finalize_host(C.addressof(tcopy), n, None, C.byref(nl)))
+        lights = (Light * max(nl.value, 1))()
+        check(lib.mc_scene_finalize_host(C.addressof(tcopy), n, C.addressof(lights), C.byref(nl)))
+        self.light_count = nl.value
+
+        def up(arr, count, size):
+            b = np.frombuffer(arr, dtype=np.uint8, count=max(count, 1) * size).copy()
+            return torch.from_numpy(b).to(device)
+        self.hot = up(hot, n, 36)
+        self.cold = up(cold, n, 192)
+        self.lights = up(lights, nl.value, 64)
+        self.spheres = up(spheres, ns, 160) if ns else torch.zeros(160, dtype=torch.uint8, device=device)
+        medium = any(triangles[i].mat.type == MAT_ISOTROPIC for i in range(n)) if n < 100000 else None
+        if medium is None:
+            mt = np.frombuffer(triangles, dtype=np.uint8).reshape(n, 224)[:, 96:100].copy().view(np.int32).ravel()
+            medium = bool((mt == MAT_ISOTROPIC).any())
+        if ns and any(spheres[i].mat.type == MAT_ISOTROPIC for i in range(ns)):
+            medium = True
+        self.env = EnvMap()
+        if env_rgba is not None:
+            e = np.ascontiguousarray(env_rgba, dtype=np.float32)
+            check(lib.mc_env_create(e.ctypes.data, e.shape[1], e.shape[0], env_intensity, env_rotation, C.byref(self.env)))
+        else:
+            self.env.intensity = env_intensity
+            self.env.rotation = env_rotation
+        v = SceneView()
+        v.spheres = self.spheres.data_ptr()
+        v.sphere_count = ns
+        v.tri_hot = self.hot.data_ptr()
+        v.tri_cold = self.cold.data_ptr()
+        v.triangle_count = n
+        v.lights = self.lights.data_ptr()
+        v.light_count = nl.value
+        v.has_medium = 1 if medium else 0
+        v.env = self.env
+        self.view = v
+        self.n = n + ns
+
+    def close(self):
+        if self.env.enabled:
+            self.lib.mc_env_destroy(C.byref(self.env))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generate_scene(kind, variant=0, seed=0, triangle_target=0):
+    """Returns a SceneHost (host memory owned by the library; free with free_scene)."""
+    lib = load()
+    d = SceneDesc(kind, variant, seed, triangle_target)
+    s = SceneHost()
+    check(lib.mc_scene_generate(C.byref(d), C.byref(s)))
+    return s
+
+
+def free_scene(s):
+    load().mc_scene_free(C.byref(s))
+
+
+def camera_initialize(cam):
+    check(load().mc_camera_initialize(C.byref(cam)))
+    return cam
+
+
+def make_camera(width, height, look_from, look_at, vfov, focus, max_depth=8, spp=1, up=(0, 1, 0), aperture=0.0,
+                background=(0, 0, 0), rr_cap=0.95):
+    cam = Camera()
+    cam.aspect_ratio = width / float(height)
+    cam.image_width = width
+    cam.samples_per_pixel = spp
+    cam.max_depth = max_depth
+    cam.vfov = vfov
+    cam.look_from = Vec3(*look_from)
+    cam.look_at = Vec3(*look_at)
+    cam.up = Vec3(*up)
+    cam.aperture = aperture
+    cam.focus_distance = focus
+    cam.background = Vec3(*background)
+    cam.rr_cap = rr_cap
+    return camera_initialize(cam)
+
+
+def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RNG_PHILOX, seed=1234, first_sample=0,
+                  intersector=ISECT_REFERENCE, disable_clamp=False, refill_threshold=0, use_graph=False, instrument=0):
+    p = RenderParams()
+    p.camera = camera
+    p.width, p.height, p.spp, p.first_sample, p.max_depth = width, height, spp, first_sample, max_depth
+    p.persistent = 1 if persistent else 0
+    p.rng = rng
+    p.seed = seed
+    p.intersector = intersector
+    p.disable_clamp = 1 if disable_clamp else 0
+    p.queue_capacity = 0
+    p.refill_threshold = refill_threshold
+    p.use_graph = 1 if use_graph else 0
+    p.instrument = instrument
+    return p
