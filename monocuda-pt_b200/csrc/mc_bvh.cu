@@ -388,7 +388,7 @@ __global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb*
                                float4* __restrict__ nodes, float4* __restrict__ prims, const int32_t* __restrict__ parents,
                                int* __restrict__ counters, int32_t* __restrict__ ids_out, int32_t* __restrict__ types_out,
                                mc_bvh_node* __restrict__ ref_internal, mc_bvh_node* __restrict__ ref_leaves,
-                               mc_aabb* __restrict__ root_box) {
+                               mc_aabb* __restrict__ root_box, int* __restrict__ err) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     int src = order[k];
@@ -428,8 +428,16 @@ __global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb*
         return;
     }
     int p = parents[n - 1 + k];
-    while (p >= 0) {
+    if (p < 0) {
+        atomicOr(err, MC_DEVERR_INPUT);  // every leaf of a Karras tree over n >= 2 keys has a parent
+        return;
+    }
+    for (int level = 0; p >= 0; level++) {
         int node = p >> 1, side = p & 1;
+        if (node >= n - 1 || level > 2 * MC_STACK_CAPACITY) {
+            atomicOr(err, MC_DEVERR_INPUT);
+            return;
+        }
         store_child_box(nodes, node, side, b);
         __threadfence();
         int old = atomicAdd(&counters[node], 1);
@@ -480,9 +488,32 @@ __global__ void k_leaf_depth(const int32_t* __restrict__ parents, int n, int* de
     atomicMax(depth, dcount);
 }
 
-__global__ void k_gather_u32(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, int n, uint32_t* __restrict__ dst) {
+// dst[i] = src[idx[i]] for a caller-supplied order; out-of-range entries are
+// flagged (and read as 0) instead of being dereferenced.
+__global__ void k_gather_u32(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, int n, uint32_t* __restrict__ dst,
+                             int* err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[idx[i]];
+    if (i >= n) return;
+    int j = idx[i];
+    if (j < 0 || j >= n) {
+        atomicOr(err, MC_DEVERR_INPUT);
+        dst[i] = 0u;
+        return;
+    }
+    dst[i] = src[j];
+}
+
+// A caller-supplied order must be a permutation that sorts the codes.
+__global__ void k_check_order(const int32_t* __restrict__ order, const uint32_t* __restrict__ sorted, int n, int* seen, int* err) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int j = order[k];
+    if (j < 0 || j >= n) {
+        atomicOr(err, MC_DEVERR_INPUT);
+        return;
+    }
+    if (atomicExch(&seen[j], 1) != 0) atomicOr(err, MC_DEVERR_INPUT);
+    if (k > 0 && sorted[k] < sorted[k - 1]) atomicOr(err, MC_DEVERR_INPUT);
 }
 
 int grid_for(long long n, int block) { return (int)std::max(1ll, (n + block - 1) / block); }
@@ -677,12 +708,27 @@ mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh
         uint32_t* tmp = (uint32_t*)ctx->scratch[2].ptr;
         if (cudaMemcpyAsync(tmp, bvh->codes, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
             return fail(mc::cuda_error(cudaGetLastError(), "code copy", __FILE__, __LINE__));
-        k_gather_u32<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(tmp, order, n, bvh->codes);
+        k_gather_u32<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(tmp, order, n, bvh->codes, ctx->d_error);
+        int* seen = (int*)ctx->scratch[3].ptr;
+        if (cudaMemsetAsync(seen, 0, (size_t)n * 4, ctx->stream) != cudaSuccess)
+            return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
+        k_check_order<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(order, bvh->codes, n, seen, ctx->d_error);
     } else {
         st = mc::radix_sort_pairs(ctx, bvh->codes, order, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, n, 30);
         if (st != MC_OK) return fail(st);
     }
-    if (cudaMemsetAsync(counters, 0, (size_t)nodesCount * 4, ctx->stream) != cudaSuccess)
+    {
+        // the hierarchy is only built over a valid sorted order
+        int pre = 0;
+        if (cudaMemcpyAsync(&pre, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            return fail(mc::cuda_error(cudaGetLastError(), "mc_bvh_build", __FILE__, __LINE__));
+        if (pre & MC_DEVERR_INPUT)
+            return fail(mc::set_error(MC_ERR_INVALID, "mc_bvh_build: the permutation is not a sorting permutation of the primitives"));
+        if (pre) return fail(mc::status_from_device_flags(pre));
+    }
+    if (cudaMemsetAsync(counters, 0, (size_t)nodesCount * 4, ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(bvh->parents, 0xFF, (size_t)(2 * n) * 4, ctx->stream) != cudaSuccess)
         return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
     mc_aabb* rootBox = (mc_aabb*)(scene6 + 8);
     if (n >= 2) {
@@ -696,7 +742,7 @@ mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh
     k_leaves_refit<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(order, boundsRef, n, ns, scene->spheres, scene->tri_hot,
                                                                    (float4*)bvh->nodes, (float4*)bvh->prims, bvh->parents,
                                                                    counters, bvh->ids, bvh->types, bvh->ref_internal,
-                                                                   bvh->ref_leaves, rootBox);
+                                                                   bvh->ref_leaves, rootBox, ctx->d_error);
     if (n == 1) k_single_root<<<1, 1, 0, ctx->stream>>>((float4*)bvh->nodes, boundsRef);
     if (cudaGetLastError() != cudaSuccess) return fail(mc::set_error(MC_ERR_CUDA, "mc_bvh_build: launch failed"));
     int flags = 0;

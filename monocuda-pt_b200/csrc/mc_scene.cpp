@@ -483,7 +483,7 @@ void gen_guiding_room(mc_scene_host& s, std::vector<mc_triangle>& tris, uint64_t
         HV c((float)((rng.uniform() * 2 - 1) * 4.0), half.y, (float)((rng.uniform() * 2 - 1) * 4.0));
         add_box(tris, c, half, (float)(rng.uniform() * M_PI), make_lambertian(HV(0.4f + 0.5f * (float)rng.uniform(), 0.4f + 0.5f * (float)rng.uniform(), 0.4f + 0.5f * (float)rng.uniform())));
     }
-    const int levels[4] = {6, 5, 5, 5};
+    const int levels[4] = {6, 6, 5, 5};
     for (int i = 0; i < 4; i++) {
         Xform xf = random_rotation(rng);
         double r = 0.4 + 0.3 * rng.uniform();

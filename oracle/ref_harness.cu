@@ -189,6 +189,12 @@ int mcref_finalize_and_sort(const mc_triangle* tris, int nt, const mc_sphere* sp
 int mcref_build_bvh(const uint32_t* sorted_codes, const int32_t* sorted_ids, const int32_t* sorted_types,
                     const mc_aabb* sorted_bounds, int n, mc_bvh_node* internal_out, mc_bvh_node* leaves_out) {
     if (n < 2) return 1;
+    // The reference's kernels trust their input (an unsorted code array gives a
+    // malformed tree whose refit indexes out of bounds): check it on the host.
+    for (int i = 1; i < n; i++)
+        if (sorted_codes[i] < sorted_codes[i - 1]) return 4;
+    for (int i = 0; i < n; i++)
+        if (sorted_ids[i] < 0 || (sorted_types[i] != 0 && sorted_types[i] != 1)) return 4;
     unsigned int* d_codes = nullptr; int* d_ids = nullptr; AABB* d_bounds = nullptr; int* d_types = nullptr;
     MCREF_TRY(cudaMalloc(&d_codes, n * sizeof(unsigned int)));
     MCREF_TRY(cudaMalloc(&d_ids, n * sizeof(int)));

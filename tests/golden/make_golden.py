@@ -92,11 +92,16 @@ def gpu_part(name, kind, variant):
     tris = mcpt.host_triangles(s)
     n = len(tris)
     h = np.load(os.path.join(HERE, "%s_host.npz" % name))
+    # every NpzFile lookup makes a fresh array: hold them while the reference reads them
+    srt = np.ascontiguousarray(h["sorted"], dtype=np.uint32)
+    ids = np.ascontiguousarray(h["ids"], dtype=np.int32)
+    types = np.ascontiguousarray(h["types"], dtype=np.int32)
+    sbounds = np.ascontiguousarray(h["sorted_bounds"], dtype=np.float32)
+    assert len(srt) == n and np.all(srt[1:] >= srt[:-1]), "fixture does not match the scene"
     internal = (mcpt.BvhNode * (n - 1))()
     leaves = (mcpt.BvhNode * n)()
-    assert ref.mcref_build_bvh(h["sorted"].ctypes.data, h["ids"].ctypes.data, h["types"].ctypes.data,
-                               np.ascontiguousarray(h["sorted_bounds"]).ctypes.data, n, C.addressof(internal),
-                               C.addressof(leaves)) == 0
+    assert ref.mcref_build_bvh(srt.ctypes.data, ids.ctypes.data, types.ctypes.data, sbounds.ctypes.data, n,
+                               C.addressof(internal), C.addressof(leaves)) == 0
     env = mcpt.host_env(s)
     assert ref.mcref_scene_upload(C.addressof(tris), n, None, 0, env.ctypes.data if env is not None else None,
                                   s.env_width, s.env_height, s.env_intensity, 0.0) == 0
