@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = the named workload)")
+    ap.add_argument("--layout", default="wide4", choices=["binary", "wide4"], help="BVH node layout traversed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
@@ -184,7 +185,8 @@ def run_ours(args):
     env = mcpt.host_env(scene)
     ctx = mcpt.Context(local)
     ds = mcpt.DeviceScene(tris, env_rgba=env, env_intensity=scene.env_intensity, device=dev)
-    bvh = mcpt.Bvh(ctx, ds.view)
+    layout = mcpt.LAYOUT_WIDE4 if args.layout == "wide4" else mcpt.LAYOUT_BINARY
+    bvh = mcpt.Bvh(ctx, ds.view, layout=layout)
     W, H = scene.width, scene.height
     acc = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
     K, Wm = args.steps, args.warmup
@@ -290,7 +292,8 @@ def run_ours(args):
             torch.distributed.destroy_process_group()
         return
     peak, peak_kind = peaks()
-    alg_bytes = visits * NODE_BYTES + leaves * LEAF_BYTES + ext * EXT_IO_BYTES + shd * SHADOW_IO_BYTES
+    node_bytes = 2 * NODE_BYTES if layout == mcpt.LAYOUT_WIDE4 else NODE_BYTES  # 128-byte wide nodes
+    alg_bytes = visits * node_bytes + leaves * LEAF_BYTES + ext * EXT_IO_BYTES + shd * SHADOW_IO_BYTES
     per_launch_bytes = alg_bytes / max(trace_launches, 1)
     per_launch_s = trace_ms / max(trace_launches, 1) / 1e3
     achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
@@ -300,7 +303,8 @@ def run_ours(args):
         "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": dict(WORKLOAD, spp=K * world, parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
+        "config": dict(WORKLOAD, spp=K * world, bvh_layout=args.layout,
+                       parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
                        samples_per_sec=round(W * H * K * world / (ms_max / 1e3), 1),
                        rays_per_path=round(rays_all / (W * H * K * world), 3)),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",

@@ -243,6 +243,10 @@ enum {
     MC_ISECT_REFERENCE = 0,     /* the reference's plane + edge test (PT:715-741) */
     MC_ISECT_WATERTIGHT = 1     /* watertight test (Woop, Benthin, Wald 2013) */
 };
+/* OR into the intersector argument of mc_trace_closest / mc_trace_any: one
+ * thread per ray without refill (the reference's plain extendKernel) instead
+ * of the persistent refill loop. Results are identical; only scheduling differs. */
+#define MC_TRACE_PLAIN 0x100
 
 typedef struct mc_render_params {
     mc_camera camera;           /* initialized; image_width/height set */
@@ -323,7 +327,7 @@ enum {
     MC_SCENE_DISPLACED_ICOSPHERES = 2, /* 3 displaced level-L icospheres + ground + medium box + light + sky */
     MC_SCENE_BATCH_MEMBER = 3,       /* one scene of the 64-scene batch (index = variant) */
     MC_SCENE_GUIDING_ROOM = 4,       /* 10x10x4 room lit through a 0.2x0.2 aperture */
-    MC_SCENE_CORNELL_REFERENCE = 5   /* the reference's buildCornellScene geometry minus textures */
+    MC_SCENE_CORNELL_SPHERES = 5     /* the reference's buildCornellScene (spheres, medium, motion) minus the image texture */
 };
 
 typedef struct mc_scene_desc {

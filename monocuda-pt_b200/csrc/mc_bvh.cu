@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "mc_internal.h"
@@ -310,7 +311,7 @@ __device__ __forceinline__ int delta(const uint32_t* __restrict__ codes, int n, 
 // Child references: internal child c -> c; leaf child k -> ~k.
 __global__ void k_karras(const uint32_t* __restrict__ codes, int n, float4* __restrict__ nodes,
                          int32_t* __restrict__ parents, mc_bvh_node* __restrict__ ref_internal,
-                         mc_bvh_node* __restrict__ ref_leaves) {
+                         mc_bvh_node* __restrict__ ref_leaves, int2* __restrict__ ranges) {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n - 1) return;
     int d = (delta(codes, n, idx, idx + 1) - delta(codes, n, idx, idx - 1)) >= 0 ? 1 : -1;
@@ -334,6 +335,7 @@ __global__ void k_karras(const uint32_t* __restrict__ codes, int n, float4* __re
 
     bool leftLeaf = (split == first);
     bool rightLeaf = (split + 1 == last);
+    if (ranges) ranges[idx] = make_int2(first, last);
     int leftRef = leftLeaf ? ~split : split;
     int rightRef = rightLeaf ? ~(split + 1) : (split + 1);
     nodes[(long long)idx * 4 + 3] = make_float4(__int_as_float(leftRef), __int_as_float(rightRef), 0.f, 0.f);
@@ -475,6 +477,127 @@ __global__ void k_single_root(float4* nodes, const mc_aabb* bounds) {
     nodes[3] = make_float4(__int_as_float(~0), __int_as_float(~0), 0.f, 0.f);
 }
 
+// ---------------------------------------------------------------------------
+// 4-wide collapse.
+// Leaf rank = position of the leaf in the reference's traversal order with
+// every box overlapping (stepTraversal PT:1276-1321): at a node its leaf
+// children are tested first (left, then right), then its internal children are
+// descended left first. Walking up from a leaf, each ancestor adds the number
+// of leaves emitted before the branch that holds it.
+// ---------------------------------------------------------------------------
+__global__ void k_leaf_rank(const float4* __restrict__ nodes, const int32_t* __restrict__ parents,
+                            const int2* __restrict__ ranges, int n, int* __restrict__ rank, int* err) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (n == 1) {
+        rank[0] = 0;
+        return;
+    }
+    int r = 0;
+    int p = parents[n - 1 + k];
+    for (int level = 0; p >= 0; level++) {
+        int node = p >> 1, side = p & 1;
+        if (node >= n - 1 || level > 2 * MC_STACK_CAPACITY) {
+            atomicOr(err, MC_DEVERR_INPUT);
+            return;
+        }
+        float4 d = nodes[(long long)node * 4 + 3];
+        int lref = __float_as_int(d.x), rref = __float_as_int(d.y);
+        bool lLeaf = lref < 0, rLeaf = rref < 0;
+        if (side == 0) {
+            if (rLeaf && !lLeaf) r += 1;           // the right leaf is tested before the left subtree
+        } else {
+            if (lLeaf) r += 1;                      // the left leaf comes first
+            else if (!rLeaf) r += ranges[lref].y - ranges[lref].x + 1;  // the whole left subtree comes first
+        }
+        p = parents[node];
+    }
+    rank[k] = r;
+}
+
+// Depth parity of internal nodes: wide nodes are the binary nodes at even depth.
+__global__ void k_wide_select(const int32_t* __restrict__ parents, int n, int* __restrict__ wideId, int* counter) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int depth = 0;
+    int p = parents[i];
+    while (p >= 0 && depth <= 4 * MC_STACK_CAPACITY) {
+        depth++;
+        p = parents[p >> 1];
+    }
+    if (depth & 1) {
+        wideId[i] = -1;
+    } else {
+        wideId[i] = (i == 0) ? 0 : atomicAdd(counter, 1);
+    }
+}
+
+__device__ __forceinline__ void child_slot_box(const float4* nodes, int node, int side, float* b) {
+    const float* f = reinterpret_cast<const float*>(nodes + (long long)node * 4);
+    int o = side ? 6 : 0;
+#pragma unroll
+    for (int j = 0; j < 6; j++) b[j] = f[o + j];
+}
+
+// One wide node per selected binary node: its children, with each internal
+// child replaced by that child's two children.
+__global__ void k_wide_fill(const float4* __restrict__ nodes, const int* __restrict__ wideId, const int* __restrict__ rank,
+                            int n, float4* __restrict__ wide) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int id = wideId[i];
+    if (id < 0) return;
+    float lo[3][4], hi[3][4];
+    int ref[4];
+    int c = 0;
+    float4 d = nodes[(long long)i * 4 + 3];
+    int kids[2] = {__float_as_int(d.x), __float_as_int(d.y)};
+    for (int side = 0; side < 2; side++) {
+        int kref = kids[side];
+        if (kref < 0) {
+            float b[6];
+            child_slot_box(nodes, i, side, b);
+            lo[0][c] = b[0]; lo[1][c] = b[1]; lo[2][c] = b[2];
+            hi[0][c] = b[3]; hi[1][c] = b[4]; hi[2][c] = b[5];
+            ref[c++] = ~rank[~kref];
+        } else {
+            float4 dd = nodes[(long long)kref * 4 + 3];
+            int gk[2] = {__float_as_int(dd.x), __float_as_int(dd.y)};
+            for (int gs = 0; gs < 2; gs++) {
+                float b[6];
+                child_slot_box(nodes, kref, gs, b);
+                lo[0][c] = b[0]; lo[1][c] = b[1]; lo[2][c] = b[2];
+                hi[0][c] = b[3]; hi[1][c] = b[4]; hi[2][c] = b[5];
+                int g = gk[gs];
+                ref[c++] = g < 0 ? ~rank[~g] : wideId[g];
+            }
+        }
+    }
+    for (; c < 4; c++) {
+        lo[0][c] = lo[1][c] = lo[2][c] = INFINITY;
+        hi[0][c] = hi[1][c] = hi[2][c] = -INFINITY;
+        ref[c] = MC_WIDE_EMPTY;
+    }
+    float4* w = wide + (long long)id * 8;
+    w[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    w[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    w[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    w[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    w[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    w[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    w[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+    w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void k_reorder_prims(const float4* __restrict__ src, const int* __restrict__ rank, int n, float4* __restrict__ dst) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int r = rank[k];
+    dst[(long long)r * 3 + 0] = src[(long long)k * 3 + 0];
+    dst[(long long)r * 3 + 1] = src[(long long)k * 3 + 1];
+    dst[(long long)r * 3 + 2] = src[(long long)k * 3 + 2];
+}
+
 __global__ void k_leaf_depth(const int32_t* __restrict__ parents, int n, int* depth) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -589,6 +712,59 @@ static mc_status morton_stage(mc_context* ctx, const mc_scene_view* s, uint32_t*
                                                                   bounds_ref, centroids, scene6);
     k_morton<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(centroids, n, scene6, codes, values);
     MC_CUDA(cudaGetLastError());
+    return MC_OK;
+}
+
+// 4-wide collapse of a finished binary build (ranges of the Karras nodes are in
+// ctx->scratch[1]); fills bvh->wide_nodes / wide_prims and switches the layout.
+mc_status build_wide(mc_context* ctx, mc_bvh* bvh) {
+    const int n = bvh->n;
+    mc_status st;
+    if ((st = devbuf_reserve(ctx->scratch[2], (size_t)n * 4 + 16)) != MC_OK) return st;
+    if ((st = devbuf_reserve(ctx->scratch[3], (size_t)n * 4 + 16)) != MC_OK) return st;
+    if ((st = devbuf_reserve(ctx->scratch[5], (size_t)n * 4 + 16)) != MC_OK) return st;
+    int* rank = (int*)ctx->scratch[2].ptr;
+    int* wideId = (int*)ctx->scratch[3].ptr;
+    int* counter = (int*)ctx->scratch[5].ptr;
+    k_leaf_rank<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, bvh->parents,
+                                                                (const int2*)ctx->scratch[1].ptr, n, rank, ctx->d_error);
+    int count = 1;
+    if (n >= 2) {
+        MC_CUDA(cudaMemcpyAsync(counter, &count, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        k_wide_select<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, n, wideId, counter);
+        MC_CUDA(cudaMemcpyAsync(&count, counter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    int flags = 0;
+    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (flags) return status_from_device_flags(flags);
+    if (cudaMalloc(&bvh->wide_nodes, (size_t)count * 128) != cudaSuccess ||
+        cudaMalloc(&bvh->wide_prims, (size_t)n * 48) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MC_ERR_OOM, "mc_bvh_build: wide-node allocation failed");
+    }
+    if (n >= 2) {
+        k_wide_fill<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, wideId, rank, n,
+                                                                        (float4*)bvh->wide_nodes);
+    } else {
+        // one leaf under the root, three empty slots
+        float inf = INFINITY;
+        mc_aabb a;
+        MC_CUDA(cudaMemcpyAsync(&a, ctx->scratch[0].ptr, sizeof(a), cudaMemcpyDeviceToHost, ctx->stream));
+        MC_CUDA(cudaStreamSynchronize(ctx->stream));
+        float h[32] = {a.lo.x, inf, inf, inf, a.lo.y, inf, inf, inf, a.lo.z, inf, inf, inf,
+                       a.hi.x, -inf, -inf, -inf, a.hi.y, -inf, -inf, -inf, a.hi.z, -inf, -inf, -inf};
+        int refs[4] = {~0, MC_WIDE_EMPTY, MC_WIDE_EMPTY, MC_WIDE_EMPTY};
+        memcpy(&h[24], refs, sizeof(refs));
+        h[28] = h[29] = h[30] = h[31] = 0.f;
+        MC_CUDA(cudaMemcpyAsync(bvh->wide_nodes, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    k_reorder_prims<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->prims, rank, n,
+                                                                    (float4*)bvh->wide_prims);
+    MC_CUDA(cudaGetLastError());
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    bvh->wide_count = count;
+    bvh->layout = MC_BVH_LAYOUT_WIDE4;
     return MC_OK;
 }
 
@@ -733,7 +909,8 @@ mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh
     mc_aabb* rootBox = (mc_aabb*)(scene6 + 8);
     if (n >= 2) {
         k_karras<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>(bvh->codes, n, (float4*)bvh->nodes, bvh->parents,
-                                                                     bvh->ref_internal, bvh->ref_leaves);
+                                                                     bvh->ref_internal, bvh->ref_leaves,
+                                                                     (int2*)ctx->scratch[1].ptr);
     } else {
         int m1 = -1;
         cudaMemcpyAsync(bvh->parents, &m1, 4, cudaMemcpyHostToDevice, ctx->stream);
@@ -751,6 +928,9 @@ mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh
         cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return fail(mc::cuda_error(cudaGetLastError(), "mc_bvh_build", __FILE__, __LINE__));
     if (flags) return fail(mc::status_from_device_flags(flags));
+    if (o.layout == MC_BVH_LAYOUT_WIDE4) {
+        if ((st = mc::build_wide(ctx, bvh)) != MC_OK) return fail(st);
+    }
     *out = bvh;
     return MC_OK;
 }
@@ -759,6 +939,8 @@ mc_status mc_bvh_free(mc_bvh* bvh) {
     if (!bvh) return MC_OK;
     cudaFree(bvh->nodes);
     cudaFree(bvh->prims);
+    cudaFree(bvh->wide_nodes);
+    cudaFree(bvh->wide_prims);
     cudaFree(bvh->codes);
     cudaFree(bvh->ids);
     cudaFree(bvh->types);
@@ -777,7 +959,7 @@ mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info) {
     info->internal_count = bvh->n - 1;
     info->depth = bvh->depth;
     info->layout = bvh->layout;
-    info->node_bytes = bvh->node_bytes;
+    info->node_bytes = bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_count * 128 : bvh->node_bytes;
     info->prim_bytes = (long long)bvh->n * 48;
     info->scene_bounds = bvh->bounds;
     return MC_OK;

@@ -20,6 +20,8 @@ typedef struct CUstream_st* cudaStream_t;
 
 // Traversal stack capacity (the reference's TRAVERSAL_STACK_CAPACITY, PT:1038).
 #define MC_STACK_CAPACITY 64
+// Child reference of an unused slot in a 4-wide node.
+#define MC_WIDE_EMPTY 0x7FFFFFFF
 
 namespace mc {
 
@@ -92,6 +94,9 @@ struct mc_bvh {
     long long node_count = 0;
     long long node_bytes = 0;
     void* prims = nullptr;             // leaf-ordered primitive records, 48 B each
+    void* wide_nodes = nullptr;        // 4-wide nodes, 128 B each (layout MC_BVH_LAYOUT_WIDE4)
+    long long wide_count = 0;
+    void* wide_prims = nullptr;        // primitive records in reference visit (rank) order
     // reference representation (optional)
     uint32_t* codes = nullptr;
     int32_t* ids = nullptr;

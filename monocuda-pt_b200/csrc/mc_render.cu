@@ -66,6 +66,8 @@ struct TraceArgs {
     int refill;
     int* err;
     unsigned long long* counts;  // [0] node visits, [1] leaf tests (counting variant)
+    int wide;                    // 4-wide node layout
+    int oneShot;                 // plain mode: one ray per thread, no refill
 };
 
 // Warp-reduces the lane counters and adds them to the global pair.
@@ -184,7 +186,7 @@ MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int s
     return true;
 }
 
-template <int ISECT, bool MEDIUM, bool COUNT = false>
+template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE>
 __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
@@ -206,8 +208,13 @@ __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
             if (cnt >= a.refill) {
                 int leader = __ffs(idle) - 1;
                 int base = 0;
-                if (lane == leader) base = atomicAdd(a.work, cnt);
-                base = __shfl_sync(kFull, base, leader);
+                if (a.oneShot) {
+                    // plain wavefront (PT:3376-3397): one ray per thread, no refill
+                    base = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+                } else {
+                    if (lane == leader) base = atomicAdd(a.work, cnt);
+                    base = __shfl_sync(kFull, base, leader);
+                }
                 if (!has) {
                     int q = base + __popc(idle & ltmask);
                     if (q < total) {
@@ -246,65 +253,19 @@ __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
                         }
                     }
                 }
-                if (base + cnt >= total) exhausted = true;
+                if (a.oneShot || base + cnt >= total) exhausted = true;
             }
         }
         if (exhausted && __ballot_sync(kFull, has) == 0u) break;
         if (has) {
-            int r = (kind == 1 && !MEDIUM) ? trav_step<true, ISECT, COUNT>(a.ts, s, stack, w, a.err, &cnt)
-                                           : trav_step<false, ISECT, COUNT>(a.ts, s, stack, w, a.err, &cnt);
+            int r = (kind == 1 && !MEDIUM) ? trav_step_layout<true, ISECT, COUNT, WIDE>(a.ts, s, stack, w, a.err, &cnt)
+                                           : trav_step_layout<false, ISECT, COUNT, WIDE>(a.ts, s, stack, w, a.err, &cnt);
             if (r != STEP_CONTINUE) {
                 if (finish_ray<ISECT, MEDIUM>(a, s, r, kind, slot, T, travelled, crossings)) has = false;
             }
         }
     }
     if (COUNT) flush_counts(a, cnt);
-}
-
-// One thread per ray, no refill (the plain --wavefront extendKernel, PT:3376-3397).
-template <int ISECT, bool MEDIUM>
-__global__ void __launch_bounds__(256) k_trace_simple(TraceArgs a) {
-    const int extCount = a.extCount ? *a.extCount : a.extN;
-    const int shCount = a.shCount ? *a.shCount : a.shN;
-    const int total = extCount + shCount;
-    int stack[MC_STACK_CAPACITY];
-    WatertightRay w;
-    w.kx = 0; w.ky = 1; w.kz = 2; w.sx = w.sy = w.sz = 0.f;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
-        TravState s;
-        int kind, slot, crossings = 0;
-        float T = 1.f, travelled = 0.f;
-        V3 o, d;
-        float time, tmax;
-        if (q < extCount) {
-            kind = 0;
-            slot = a.queue ? a.queue[q] : q;
-            o = V3(a.ox[slot], a.oy[slot], a.oz[slot]);
-            d = V3(a.dx[slot], a.dy[slot], a.dz[slot]);
-            time = a.time[slot];
-            tmax = 1e30f;
-        } else {
-            kind = 1;
-            slot = q - extCount;
-            o = V3(a.sox[slot], a.soy[slot], a.soz[slot]);
-            d = V3(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
-            time = a.spath ? a.time[a.spath[slot]] : a.time[slot];
-            tmax = a.smax[slot];
-            if (MEDIUM && tmax <= 0.0f) {
-                s.tmax = tmax;
-                s.hitLeaf = -1;
-                finish_ray<ISECT, MEDIUM>(a, s, STEP_DONE, kind, slot, T, travelled, crossings);
-                continue;
-            }
-        }
-        trav_begin(s, o, d, time, tmax);
-        if (ISECT == MC_ISECT_WATERTIGHT) w = make_watertight(d);
-        while (true) {
-            int r = (kind == 1 && !MEDIUM) ? trav_step<true, ISECT>(a.ts, s, stack, w, a.err)
-                                           : trav_step<false, ISECT>(a.ts, s, stack, w, a.err);
-            if (r != STEP_CONTINUE && finish_ray<ISECT, MEDIUM>(a, s, r, kind, slot, T, travelled, crossings)) break;
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -734,8 +695,9 @@ namespace {
 TraceArgs base_trace_args(const mc_bvh* bvh, const mc_scene_view* scene, mc_context* ctx) {
     TraceArgs t;
     std::memset(&t, 0, sizeof(t));
-    t.ts.nodes = (const float4*)bvh->nodes;
-    t.ts.prims = (const float4*)bvh->prims;
+    t.wide = bvh->layout == MC_BVH_LAYOUT_WIDE4 ? 1 : 0;
+    t.ts.nodes = (const float4*)(t.wide ? bvh->wide_nodes : bvh->nodes);
+    t.ts.prims = (const float4*)(t.wide ? bvh->wide_prims : bvh->prims);
     t.cold = scene->tri_cold;
     t.spheres = scene->spheres;
     t.err = ctx->d_error;
@@ -745,25 +707,29 @@ TraceArgs base_trace_args(const mc_bvh* bvh, const mc_scene_view* scene, mc_cont
 
 typedef void (*TraceKernel)(TraceArgs);
 
-// [persistent][count][medium][isect]
-TraceKernel trace_kernel(bool persistent, bool count, bool medium, int isect) {
-    static const TraceKernel table[2][2][2][2] = {
-        {{{k_trace_simple<0, false>, k_trace_simple<1, false>}, {k_trace_simple<0, true>, k_trace_simple<1, true>}},
-         {{k_trace_simple<0, false>, k_trace_simple<1, false>}, {k_trace_simple<0, true>, k_trace_simple<1, true>}}},
-        {{{k_trace<0, false, false>, k_trace<1, false, false>}, {k_trace<0, true, false>, k_trace<1, true, false>}},
-         {{k_trace<0, false, true>, k_trace<1, false, true>}, {k_trace<0, true, true>, k_trace<1, true, true>}}}};
-    return table[persistent ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
+// [wide][count][medium][isect]
+#define MC_TK(W)                                                                                                      \
+    {{{k_trace<0, false, false, W>, k_trace<1, false, false, W>}, {k_trace<0, true, false, W>, k_trace<1, true, false, W>}}, \
+     {{k_trace<0, false, true, W>, k_trace<1, false, true, W>}, {k_trace<0, true, true, W>, k_trace<1, true, true, W>}}}
+TraceKernel trace_kernel(bool wide, bool count, bool medium, int isect) {
+    static const TraceKernel table[2][2][2][2] = {MC_TK(false), MC_TK(true)};
+    return table[wide ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
 }
 
-// Persistent grid: one wave of resident blocks (SMs x resident blocks per SM).
-// Plain variant: one thread per ray over the queue capacity.
-void launch_trace(mc_context* ctx, const TraceArgs& t, bool medium, int isect, bool persistent, int simpleBlocks,
+// Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
+// pull rays from the work counter. Plain (PT:3376-3397): the same kernel with
+// one ray per thread and no refill, over plainBlocks blocks; sharing the kernel
+// keeps the per-ray arithmetic identical between the two modes.
+void launch_trace(mc_context* ctx, const TraceArgs& t0, bool medium, int isect, bool persistent, int plainBlocks,
                   bool count = false) {
-    static int occ[16] = {0};
-    TraceKernel fn = trace_kernel(persistent, count && persistent, medium, isect);
-    int blocks = std::max(1, simpleBlocks);
+    static int occ[32] = {0};
+    TraceArgs t = t0;
+    t.oneShot = persistent ? 0 : 1;
+    const bool wide = t.wide != 0;
+    TraceKernel fn = trace_kernel(wide, count, medium, isect);
+    int blocks = std::max(1, plainBlocks);
     if (persistent) {
-        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0);
+        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0);
         if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count);
         blocks = occ[key];
     }
@@ -823,7 +789,7 @@ mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view
     static int shadeBlocks[2] = {0, 0};
     if (!shadeBlocks[0]) shadeBlocks[0] = occupancy_blocks((const void*)k_shade<PhiloxRng>, ctx->sm_count);
     if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng>, ctx->sm_count);
-    const int simpleBlocks = (pixels + 255) / 256;
+    const int simpleBlocks = (2 * pixels + 255) / 256;  // extend + shadow rays of one launch, at most one each per path
 
     mc_camera cam = p->camera;
     CameraArgs ca;
@@ -1003,6 +969,8 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
 mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const float* d_rays, int32_t n,
                            int32_t intersector, mc_packed_hit* d_hits) {
     if (!ctx || !bvh || !scene || !d_rays || !d_hits || n < 0) return mc::set_error(MC_ERR_INVALID, "mc_trace_closest: bad argument");
+    const bool plain = (intersector & MC_TRACE_PLAIN) != 0;
+    intersector &= ~MC_TRACE_PLAIN;
     if (intersector != MC_ISECT_REFERENCE && intersector != MC_ISECT_WATERTIGHT) return mc::set_error(MC_ERR_INVALID, "mc_trace_closest: unknown intersector");
     if (n == 0) return MC_OK;
     mc_status st;
@@ -1021,7 +989,7 @@ mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     t.shCount = nullptr;
     t.shN = 0;
     t.work = work;
-    mc::launch_trace(ctx, t, false, intersector, true, 0);
+    mc::launch_trace(ctx, t, false, intersector, !plain, (n + 255) / 256);
     MC_CUDA(cudaGetLastError());
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1032,6 +1000,8 @@ mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
 mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const float* d_rays, const float* d_tmax,
                        int32_t n, int32_t intersector, int32_t* d_occluded) {
     if (!ctx || !bvh || !scene || !d_rays || !d_tmax || !d_occluded || n < 0) return mc::set_error(MC_ERR_INVALID, "mc_trace_any: bad argument");
+    const bool plain = (intersector & MC_TRACE_PLAIN) != 0;
+    intersector &= ~MC_TRACE_PLAIN;
     if (intersector != MC_ISECT_REFERENCE && intersector != MC_ISECT_WATERTIGHT) return mc::set_error(MC_ERR_INVALID, "mc_trace_any: unknown intersector");
     if (n == 0) return MC_OK;
     mc_status st;
@@ -1053,7 +1023,7 @@ mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* 
     t.smax = d_tmax;
     t.occluded = d_occluded;
     t.work = work;
-    mc::launch_trace(ctx, t, false, intersector, true, 0);
+    mc::launch_trace(ctx, t, false, intersector, !plain, (n + 255) / 256);
     MC_CUDA(cudaGetLastError());
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

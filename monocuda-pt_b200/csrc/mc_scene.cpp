@@ -361,6 +361,83 @@ void gen_cornell_boxes(mc_scene_host& s, std::vector<mc_triangle>& tris) {
     set_camera(s.camera, 512, 512, HV(0, 2, 5.5f), HV(0, 2, -2), 40.0f, 7.5f, 8, 64);
 }
 
+mc_sphere make_sphere(HV c0, HV c1, bool moving, float r, const mc_material& m) {
+    mc_sphere s;
+    std::memset(&s, 0, sizeof(s));
+    s.center = c0;
+    s.center1 = c1;
+    s.is_moving = moving ? 1 : 0;
+    s.radius = r;
+    s.mat = m;
+    HV rv(r, r, r);  // PT:850-859 calculate_bounding_box
+    HV lo = c0 - rv, hi = c0 + rv;
+    if (moving) {
+        HV lo1 = c1 - rv, hi1 = c1 + rv;
+        lo = HV(fminf(lo.x, lo1.x), fminf(lo.y, lo1.y), fminf(lo.z, lo1.z));
+        hi = HV(fmaxf(hi.x, hi1.x), fmaxf(hi.y, hi1.y), fmaxf(hi.z, hi1.z));
+    }
+    s.aabb.lo = lo;
+    s.aabb.hi = hi;
+    return s;
+}
+
+// Scene "cornell_spheres": the reference's buildCornellScene (PT:1765-1822) —
+// checker floor, tall box, mirror sphere, smoke sphere (homogeneous isotropic
+// medium) and a 13x13 grid of small spheres (80% diffuse and moving, 15%
+// conductor, 5% dielectric) — with a seeded generator in place of rand() and
+// without the earth image texture. Exercises spheres, motion blur, a spherical
+// medium and checker textures.
+void gen_cornell_spheres(mc_scene_host& s, std::vector<mc_triangle>& tris, std::vector<mc_sphere>& sph, uint64_t seed) {
+    mc_material floor = base_material(MC_MAT_LAMBERTIAN);
+    floor.albedo.type = MC_TEX_CHECKER;  // PT:211-213 make_checker_texture
+    floor.albedo.color_a = srgb_to_linear(HV(0.9f, 0.9f, 0.9f));
+    floor.albedo.color_b = srgb_to_linear(HV(0.1f, 0.1f, 0.1f));
+    floor.albedo.scale = 8.f;
+    mc_material white = make_lambertian(HV(0.73f, 0.73f, 0.73f));
+    mc_material red = make_lambertian(HV(0.65f, 0.05f, 0.05f));
+    mc_material green = make_lambertian(HV(0.12f, 0.45f, 0.15f));
+    mc_material light = make_emissive(HV(15.0f, 15.0f, 15.0f));
+    const float L = -2.f, R = 2.f, B = 0.f, T = 4.f, F = -4.f, N = 0.f;
+    add_quad(tris, HV(L, B, N), HV(R, B, N), HV(R, B, F), HV(L, B, F), floor);
+    add_quad(tris, HV(L, T, N), HV(R, T, N), HV(R, T, F), HV(L, T, F), white);
+    add_quad(tris, HV(L, B, F), HV(R, B, F), HV(R, T, F), HV(L, T, F), white);
+    add_quad(tris, HV(L, B, N), HV(L, B, F), HV(L, T, F), HV(L, T, N), red);
+    add_quad(tris, HV(R, B, N), HV(R, B, F), HV(R, T, F), HV(R, T, N), green);
+    add_quad(tris, HV(-1.f, T - 0.01f, -2.6f), HV(1.f, T - 0.01f, -2.6f), HV(1.f, T - 0.01f, -1.4f),
+             HV(-1.f, T - 0.01f, -1.4f), light);
+    HV boxCenter(-0.8f, 1.1f, -2.8f);
+    add_box(tris, boxCenter, HV(0.55f, 1.1f, 0.55f), 0.3f, white);
+    HV big(0.85f, 0.7f, -1.7f);
+    sph.push_back(make_sphere(big, big, false, 0.7f, make_conductor(HV(0.9f, 0.9f, 0.9f), 0.02f)));
+    HV smoke(0.f, 2.9f, -3.0f);
+    sph.push_back(make_sphere(smoke, smoke, false, 0.6f, make_isotropic(HV(0.8f, 0.8f, 0.85f), 1.f)));
+    SplitMix rng(seed ? seed : 42);
+    const float r = 0.1f;
+    for (int a = 0; a < 13; a++) {
+        for (int b = 0; b < 13; b++) {
+            float jx = ((float)rng.uniform() - 0.5f) * 0.08f, jz = ((float)rng.uniform() - 0.5f) * 0.08f;
+            HV c(-1.8f + 0.3f * a + jx, r, -3.8f + 0.3f * b + jz);
+            if ((c - big).length() < 0.7f + r + 0.02f) continue;
+            if ((c - HV(boxCenter.x, r, boxCenter.z)).length() < 0.9f) continue;
+            float choose = (float)rng.uniform();
+            if (choose < 0.8f) {
+                mc_material m = make_lambertian(HV((float)rng.uniform(), (float)rng.uniform(), (float)rng.uniform()));
+                float h = 0.5f * (float)rng.uniform();
+                sph.push_back(make_sphere(c, c + HV(0.f, h, 0.f), true, r, m));
+            } else if (choose < 0.95f) {
+                mc_material m = make_conductor(HV(0.5f + 0.5f * (float)rng.uniform(), 0.5f + 0.5f * (float)rng.uniform(),
+                                                  0.5f + 0.5f * (float)rng.uniform()), 0.3f * (float)rng.uniform());
+                sph.push_back(make_sphere(c, c, false, r, m));
+            } else {
+                sph.push_back(make_sphere(c, c, false, r, make_dielectric(1.5f)));
+            }
+        }
+    }
+    s.width = 512; s.height = 512; s.spp = 64; s.max_depth = 8;
+    s.has_medium = 1;
+    set_camera(s.camera, 512, 512, HV(0, 2, 5.5f), HV(0, 2, -2), 40.0f, 7.5f, 8, 64);
+}
+
 // Config: "displaced_icospheres" - three level-L icospheres (L = 8 by default:
 // 1,310,720 triangles each) displaced radially by 0.05 * fbm4(value noise),
 // randomly rotated, with per-instance materials from a seeded permutation of
@@ -576,8 +653,10 @@ mc_status mc_scene_generate(const mc_scene_desc* desc, mc_scene_host* out) {
     if (!desc || !out) return mc::set_error(MC_ERR_INVALID, "mc_scene_generate: null argument");
     std::memset(out, 0, sizeof(*out));
     std::vector<mc_triangle> tris;
+    std::vector<mc_sphere> sph;
     switch (desc->kind) {
         case MC_SCENE_CORNELL_BOXES: gen_cornell_boxes(*out, tris); break;
+        case MC_SCENE_CORNELL_SPHERES: gen_cornell_spheres(*out, tris, sph, desc->seed); break;
         case MC_SCENE_DISPLACED_ICOSPHERES: {
             int level = desc->variant > 0 ? desc->variant : 8;
             if (level > 9) return mc::set_error(MC_ERR_INVALID, "mc_scene_generate: icosphere level must be <= 9");
@@ -596,8 +675,13 @@ mc_status mc_scene_generate(const mc_scene_desc* desc, mc_scene_host* out) {
     out->triangles = (mc_triangle*)std::malloc(sizeof(mc_triangle) * (tris.empty() ? 1 : tris.size()));
     if (!out->triangles) return mc::set_error(MC_ERR_OOM, "mc_scene_generate: host allocation failed");
     if (!tris.empty()) std::memcpy(out->triangles, tris.data(), sizeof(mc_triangle) * tris.size());
+    out->sphere_count = (int32_t)sph.size();
     out->spheres = nullptr;
-    out->sphere_count = 0;
+    if (!sph.empty()) {
+        out->spheres = (mc_sphere*)std::malloc(sizeof(mc_sphere) * sph.size());
+        if (!out->spheres) return mc::set_error(MC_ERR_OOM, "mc_scene_generate: host allocation failed");
+        std::memcpy(out->spheres, sph.data(), sizeof(mc_sphere) * sph.size());
+    }
     return MC_OK;
 }
 

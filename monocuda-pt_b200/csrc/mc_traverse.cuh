@@ -124,6 +124,106 @@ MC_D int trav_step(const TraceScene& sc, TravState& s, int* stack, const Waterti
     return STEP_CONTINUE;
 }
 
+// ---------------------------------------------------------------------------
+// 4-wide layout: 128 bytes per node = child boxes as six float4 (lo.x, lo.y,
+// lo.z, hi.x, hi.y, hi.z of the four children), the four child references
+// (internal: wide-node index; leaf: ~rank; empty: MC_WIDE_EMPTY) and a spare
+// float4. Leaves are stored in the reference's static visit order (their rank),
+// so "first found at equal t" becomes "smallest rank at equal t" whatever order
+// this traversal visits them in; every box is an exact box of the binary tree,
+// tested with the reference's slab arithmetic (no per-axis early exit is needed:
+// the three-axis test returns the same boolean).
+// ---------------------------------------------------------------------------
+MC_D void slab4(const RayInv& r, float lx, float ly, float lz, float hx, float hy, float hz, float tfar, float& tnear,
+                bool& hit) {
+    float e0 = (lx - r.o.x) * r.ix, x0 = (hx - r.o.x) * r.ix;
+    if (r.ix < 0.0f) { float t = e0; e0 = x0; x0 = t; }
+    float e1 = (ly - r.o.y) * r.iy, x1 = (hy - r.o.y) * r.iy;
+    if (r.iy < 0.0f) { float t = e1; e1 = x1; x1 = t; }
+    float e2 = (lz - r.o.z) * r.iz, x2 = (hz - r.o.z) * r.iz;
+    if (r.iz < 0.0f) { float t = e2; e2 = x2; x2 = t; }
+    float n = fmaxf(fmaxf(fmaxf(0.0001f, e0), e1), e2);
+    float f = fminf(fminf(fminf(tfar, x0), x1), x2);
+    hit = !(f <= n);
+    tnear = n;
+}
+
+MC_D void cswap(float& ka, int& va, float& kb, int& vb) {
+    if (kb < ka) {
+        float tk = ka; ka = kb; kb = tk;
+        int tv = va; va = vb; vb = tv;
+    }
+}
+
+template <bool ANY, int ISECT, bool COUNT = false>
+MC_D int trav_step4(const TraceScene& sc, TravState& s, int* stack, const WatertightRay& w, int* err,
+                    TravCount* cnt = nullptr) {
+    const float4* nd = sc.nodes + (long long)s.node * 8;
+    float4 lx = ldg4(nd + 0), ly = ldg4(nd + 1), lz = ldg4(nd + 2);
+    float4 hx = ldg4(nd + 3), hy = ldg4(nd + 4), hz = ldg4(nd + 5);
+    float4 rf = ldg4(nd + 6);
+    int ref[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z), __float_as_int(rf.w)};
+    float tn[4];
+    bool hit[4];
+    slab4(s.r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, s.tmax, tn[0], hit[0]);
+    slab4(s.r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, s.tmax, tn[1], hit[1]);
+    slab4(s.r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, s.tmax, tn[2], hit[2]);
+    slab4(s.r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, s.tmax, tn[3], hit[3]);
+    if (COUNT) cnt->visits++;
+    // leaf children first
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        if (hit[c] && ref[c] < 0) {
+            int k = ~ref[c];
+            float t;
+            if (COUNT) cnt->leaves++;
+            if (leaf_hit<ISECT>(sc, k, s, w, t)) {
+                if (ANY) {
+                    if (t > 0.0001f && t < s.tmax) return STEP_OCCLUDED;
+                } else if (t > 0.0001f && (t < s.tmax || (t == s.tmax && s.hitLeaf >= 0 && k < s.hitLeaf))) {
+                    s.tmax = t;
+                    s.hitLeaf = k;
+                }
+            }
+        }
+    }
+    // internal children, nearest first: sort (tnear, ref) ascending, misses as +inf
+    float k0 = (hit[0] && ref[0] >= 0 && ref[0] != MC_WIDE_EMPTY) ? tn[0] : INFINITY;
+    float k1 = (hit[1] && ref[1] >= 0 && ref[1] != MC_WIDE_EMPTY) ? tn[1] : INFINITY;
+    float k2 = (hit[2] && ref[2] >= 0 && ref[2] != MC_WIDE_EMPTY) ? tn[2] : INFINITY;
+    float k3 = (hit[3] && ref[3] >= 0 && ref[3] != MC_WIDE_EMPTY) ? tn[3] : INFINITY;
+    int v0 = ref[0], v1 = ref[1], v2 = ref[2], v3 = ref[3];
+    cswap(k0, v0, k1, v1);
+    cswap(k2, v2, k3, v3);
+    cswap(k0, v0, k2, v2);
+    cswap(k1, v1, k3, v3);
+    cswap(k1, v1, k2, v2);
+    if (k0 == INFINITY) {
+        if (s.sp == 0) return STEP_DONE;
+        s.sp--;
+        s.node = stack[s.sp];
+        return STEP_CONTINUE;
+    }
+    // push the farther ones (farthest first), continue with the nearest
+    int extra = (k1 != INFINITY) + (k2 != INFINITY) + (k3 != INFINITY);
+    if (s.sp + extra > MC_STACK_CAPACITY) {
+        atomicOr(err, MC_DEVERR_STACK);
+        return STEP_DONE;
+    }
+    if (k3 != INFINITY) stack[s.sp++] = v3;
+    if (k2 != INFINITY) stack[s.sp++] = v2;
+    if (k1 != INFINITY) stack[s.sp++] = v1;
+    s.node = v0;
+    return STEP_CONTINUE;
+}
+
+template <bool ANY, int ISECT, bool COUNT, bool WIDE>
+MC_D int trav_step_layout(const TraceScene& sc, TravState& s, int* stack, const WatertightRay& w, int* err,
+                          TravCount* cnt) {
+    if (WIDE) return trav_step4<ANY, ISECT, COUNT>(sc, s, stack, w, err, cnt);
+    return trav_step<ANY, ISECT, COUNT>(sc, s, stack, w, err, cnt);
+}
+
 // The hit record fields a leaf slot stands for.
 MC_D void leaf_identity(const TraceScene& sc, int k, int& type, int& id) {
     float4 c = ldg4(sc.prims + (long long)k * 3 + 2);

@@ -19,8 +19,10 @@ MAT_LAMBERTIAN, MAT_DIELECTRIC, MAT_CONDUCTOR, MAT_EMISSIVE, MAT_ISOTROPIC = 0, 
 TEX_SOLID, TEX_CHECKER, TEX_IMAGE = 0, 1, 2
 RNG_PHILOX, RNG_XORWOW = 0, 1
 ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
+TRACE_PLAIN = 0x100
 LAYOUT_BINARY, LAYOUT_WIDE4 = 0, 1
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
+SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64
 
 
@@ -278,6 +280,13 @@ class Bvh:
 def host_triangles(scene):
     """The scene's triangle array as a ctypes array view (no copy)."""
     return (Triangle * scene.triangle_count).from_address(C.addressof(scene.triangles.contents))
+
+
+def host_spheres(scene):
+    """The scene's sphere array as a ctypes array view (no copy), or None."""
+    if scene.sphere_count <= 0:
+        return None
+    return (Sphere * scene.sphere_count).from_address(C.addressof(scene.spheres.contents))
 
 
 def host_env(scene):
