@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
                     help="warm-up and timed steps only (for ncu captures); prints the timed line without extras")
+    ap.add_argument("--workload", default="icospheres", choices=["icospheres", "batch"],
+                    help="icospheres: the headline single-scene workload; batch: the 64-scene batched pipeline")
+    ap.add_argument("--batch-scenes", type=int, default=64)
     return ap.parse_args()
 
 
@@ -331,6 +334,67 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_batch(args):
+    """64 seeded scenes (log-normal triangle counts, median 50k, clipped to
+    [1k, 2M]; resolutions from {256^2, 512^2, 1024^2}; spp from {4, 16, 64}):
+    one batched BVH build and one batched, graph-replayed render, against
+    the same scenes built and rendered one after another."""
+    import torch
+
+    import mcpt
+    ctx = mcpt.Context(0)
+    n = args.batch_scenes
+    t0 = time.perf_counter()
+    scenes = [mcpt.generate_scene(mcpt.SCENE_BATCH_MEMBER, variant=i, seed=3) for i in range(n)]
+    gen_s = time.perf_counter() - t0
+    devs = [mcpt.DeviceScene(mcpt.host_triangles(s)) for s in scenes]
+    tris = sum(s.triangle_count for s in scenes)
+    accs = [torch.zeros(s.width * s.height * 3, dtype=torch.float32, device="cuda") for s in scenes]
+
+    def items():
+        return [mcpt.BatchItem(d.view, mcpt.render_params(s.camera, s.width, s.height, s.spp, 8, persistent=True,
+                                                           rng=mcpt.RNG_PHILOX, seed=3), a.data_ptr())
+                for s, d, a in zip(scenes, devs, accs)]
+    # warm-up
+    b = mcpt.BatchBvh(ctx, [d.view for d in devs], layout=mcpt.LAYOUT_WIDE4)
+    b.render(items(), use_graph=True)
+    b.close()
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    b = mcpt.BatchBvh(ctx, [d.view for d in devs], layout=mcpt.LAYOUT_WIDE4)
+    e1.record()
+    st = b.render(items(), use_graph=True)
+    e2.record()
+    torch.cuda.synchronize()
+    build_ms, render_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    rays = st.extend_rays + st.shadow_rays
+    # the same scenes one request at a time (plain per-request wavefront)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    seq_rays = 0
+    for s, d, a in zip(scenes, devs, accs):
+        single = mcpt.Bvh(ctx, d.view, layout=mcpt.LAYOUT_WIDE4)
+        p = mcpt.render_params(s.camera, s.width, s.height, s.spp, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=3)
+        rs = mcpt.RenderStats()
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, single.handle, C.byref(d.view), C.byref(p), a.data_ptr(),
+                                               C.byref(rs)))
+        seq_rays += rs.extend_rays + rs.shadow_rays
+        single.close()
+    f1.record()
+    torch.cuda.synchronize()
+    seq_ms = f0.elapsed_time(f1)
+    out = {"metric": "Mrays/s", "value": round(rays / ((build_ms + render_ms) / 1e3) / 1e6, 2), "unit": "Mrays/s",
+           "n_gpus": 1, "workload": "batch_%d_scenes" % n, "triangles": tris,
+           "paths": int(st.paths), "rays": int(rays), "build_ms": round(build_ms, 2), "render_ms": round(render_ms, 2),
+           "render_only_mrays": round(rays / (render_ms / 1e3) / 1e6, 2),
+           "sequential_ms": round(seq_ms, 2), "sequential_mrays": round(seq_rays / (seq_ms / 1e3) / 1e6, 2),
+           "speedup_vs_sequential": round(seq_ms / (build_ms + render_ms), 3), "generation_s": round(gen_s, 1),
+           "graph": True, "layout": "wide4"}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -382,6 +446,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -366,6 +366,12 @@ MC_API mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t*
 
 /* Full build: bounds, Morton codes, sort, Karras hierarchy, refit, layout. */
 MC_API mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh_build_opts* opts, mc_bvh** out);
+/* One build over `count` scenes in a single pass of launches: per-scene bounds
+ * and Morton codes, one stable sort by (scene, code), per-scene Karras trees,
+ * refit and collapse. The handle holds every scene's tree (scene i = the i-th
+ * view); render it with mc_render_batch. Each scene needs >= 2 primitives. */
+MC_API mc_status mc_bvh_build_batch(mc_context* ctx, const mc_scene_view* scenes, int32_t count,
+                                    const mc_bvh_build_opts* opts, mc_bvh** out);
 MC_API mc_status mc_bvh_free(mc_bvh* bvh);
 MC_API mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info);
 /* Export in the reference's representation (device arrays, any may be NULL):
@@ -394,6 +400,21 @@ MC_API mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene
 /* ------------------------------------------------------------------------- */
 MC_API mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
                                      const mc_render_params* params, float* d_accum, mc_render_stats* stats);
+/* One scene of a batched render. */
+typedef struct mc_batch_item {
+    mc_scene_view scene;        /* device arrays of this scene */
+    mc_render_params params;    /* camera, size, spp, first_sample, max depth, seed (counter-based RNG) */
+    float* d_accum;             /* this scene's accumulation buffer (W*H float3) */
+} mc_batch_item;
+
+/* Renders every item of a batch BVH (mc_bvh_build_batch, same scene order) in
+ * shared waves: each wave holds one sample of every pixel of every item that
+ * still needs samples, traced and shaded by the same persistent launches.
+ * use_graph: capture the wave's launch sequence once as a CUDA graph and
+ * replay it per wave. Layout, persistence and intersector come from items[0]. */
+MC_API mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_item* items, int32_t count,
+                                 int32_t use_graph, mc_render_stats* stats);
+
 /* Same call with host memory: copies the scene in, builds, renders, copies the
  * accumulation buffer out (accum_host: W*H*3 floats, accumulated into). */
 MC_API mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_t n_tri,

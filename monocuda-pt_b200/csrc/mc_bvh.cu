@@ -1,11 +1,18 @@
-// mc_bvh.cu - LBVH build on the device.
+// mc_bvh.cu - LBVH build on the device, for one scene or a batch of scenes.
 //
 //   primitive bounds + centroids + scene bounds  (finalizeScene, PT:1930-1971)
 //   30-bit Morton codes                          (morton3D, PT:913-935; host IEEE math in the reference)
 //   stable onesweep LSD radix sort               (replaces the host std::sort, PT:4223-4226)
 //   Karras radix tree                            (delta/determineRange/findSplit, PT:1337-1447)
 //   bottom-up refit with per-node arrival counters (refitBoundsKernel, PT:1398-1415), which writes
-//   the boxes straight into the traversal layout (children's boxes stored in the parent).
+//   the boxes straight into the traversal layout (children's boxes stored in the parent)
+//   optional 4-wide collapse.
+//
+// A batch of scenes is built by the same launches: every kernel maps a global
+// primitive / node index to its scene ("segment") and the segment-local index
+// the reference's algorithm works on; each segment gets its own root. The sort
+// orders by (segment, Morton code): a 30-bit pass sequence on the codes, then a
+// stable pass on the segment id.
 //
 // This file is compiled WITHOUT fast math and with -fmad=false: the reference
 // computes bounds and Morton codes on the host with IEEE single precision and
@@ -43,6 +50,36 @@ struct Box {
     float lx, ly, lz, hx, hy, hz;
 };
 
+// One scene of a build: its primitive arrays and where its primitives and
+// internal nodes start in the batch-wide arrays.
+struct Seg {
+    const mc_sphere* sph;
+    const mc_triangle_hot* hot;
+    int ns, nt;
+    int primOff;   // first global primitive (leaf) index
+    int intOff;    // first global internal-node index (= primOff - segment index)
+};
+
+__device__ __forceinline__ int seg_of_prim(const Seg* seg, int nseg, int g) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (seg[mid].primOff <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int seg_of_internal(const Seg* seg, int nseg, int g) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (seg[mid].intOff <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ Box merge_box(const Box& a, const Box& b) {  // PT:1456-1465 merge
     Box m;
     m.hx = fmaxf(a.hx, b.hx);
@@ -70,33 +107,36 @@ __host__ __device__ __forceinline__ float ordered_to_float(int i) {
 #endif
 }
 
-// Bounds and centroid of primitive i of the reference list (spheres first).
-// Sphere: calculate_bounding_box / calculateCentroid (PT:850-869).
-// Triangle: calculate_bounding_box with eps 1e-3 / (v0+v1+v2)/3 (PT:647-656).
-__global__ void k_prim_bounds(const mc_sphere* __restrict__ sph, int ns, const mc_triangle_hot* __restrict__ hot, int nt,
-                              mc_aabb* __restrict__ bounds, float4* __restrict__ centroids, int* __restrict__ scene) {
-    int n = ns + nt;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Bounds and centroid of every primitive (per scene: spheres first, then
+// triangles, PT:1955-1971). Sphere: calculate_bounding_box / calculateCentroid
+// (PT:850-869). Triangle: calculate_bounding_box with eps 1e-3 / (v0+v1+v2)/3
+// (PT:647-656). Scene bounds per segment (min/max are exact in any order).
+__global__ void k_prim_bounds(const Seg* __restrict__ seg, int nseg, int n, mc_aabb* __restrict__ bounds,
+                              float4* __restrict__ centroids, int* __restrict__ scene) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
     Box b = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    bool valid = i < n;
+    bool valid = g < n;
+    int s = valid ? seg_of_prim(seg, nseg, g) : 0;
     if (valid) {
+        const Seg& S = seg[s];
+        int i = g - S.primOff;
         float cx, cy, cz;
-        if (i < ns) {
-            const mc_sphere& s = sph[i];
-            float r = s.radius;
-            Box b0 = {s.center.x - r, s.center.y - r, s.center.z - r, s.center.x + r, s.center.y + r, s.center.z + r};
-            if (s.is_moving) {
-                Box b1 = {s.center1.x - r, s.center1.y - r, s.center1.z - r, s.center1.x + r, s.center1.y + r, s.center1.z + r};
+        if (i < S.ns) {
+            const mc_sphere& sp = S.sph[i];
+            float r = sp.radius;
+            Box b0 = {sp.center.x - r, sp.center.y - r, sp.center.z - r, sp.center.x + r, sp.center.y + r, sp.center.z + r};
+            if (sp.is_moving) {
+                Box b1 = {sp.center1.x - r, sp.center1.y - r, sp.center1.z - r, sp.center1.x + r, sp.center1.y + r, sp.center1.z + r};
                 b = merge_box(b0, b1);
-                cx = (s.center.x + s.center1.x) * 0.5f;
-                cy = (s.center.y + s.center1.y) * 0.5f;
-                cz = (s.center.z + s.center1.z) * 0.5f;
+                cx = (sp.center.x + sp.center1.x) * 0.5f;
+                cy = (sp.center.y + sp.center1.y) * 0.5f;
+                cz = (sp.center.z + sp.center1.z) * 0.5f;
             } else {
                 b = b0;
-                cx = s.center.x; cy = s.center.y; cz = s.center.z;
+                cx = sp.center.x; cy = sp.center.y; cz = sp.center.z;
             }
         } else {
-            const mc_triangle_hot& t = hot[i - ns];
+            const mc_triangle_hot& t = S.hot[i - S.ns];
             const float eps = 1e-3f;
             b.lx = fminf(t.v0.x, fminf(t.v1.x, t.v2.x)) - eps;
             b.ly = fminf(t.v0.y, fminf(t.v1.y, t.v2.y)) - eps;
@@ -113,26 +153,37 @@ __global__ void k_prim_bounds(const mc_sphere* __restrict__ sph, int ns, const m
         a.pad0 = 0.f;
         a.hi = mc_vec3{b.hx, b.hy, b.hz};
         a.pad1 = 0.f;
-        bounds[i] = a;
-        centroids[i] = make_float4(cx, cy, cz, 0.f);
+        bounds[g] = a;
+        centroids[g] = make_float4(cx, cy, cz, __int_as_float(s));
     }
-    // warp reduction of the scene bounds (min/max are exact in any order)
-    for (int off = 16; off > 0; off >>= 1) {
-        b.lx = fminf(b.lx, __shfl_xor_sync(0xffffffffu, b.lx, off));
-        b.ly = fminf(b.ly, __shfl_xor_sync(0xffffffffu, b.ly, off));
-        b.lz = fminf(b.lz, __shfl_xor_sync(0xffffffffu, b.lz, off));
-        b.hx = fmaxf(b.hx, __shfl_xor_sync(0xffffffffu, b.hx, off));
-        b.hy = fmaxf(b.hy, __shfl_xor_sync(0xffffffffu, b.hy, off));
-        b.hz = fmaxf(b.hz, __shfl_xor_sync(0xffffffffu, b.hz, off));
+    int* sb = scene + 6 * s;
+    int s0 = __shfl_sync(0xffffffffu, s, 0);
+    if (__all_sync(0xffffffffu, s == s0)) {
+        for (int off = 16; off > 0; off >>= 1) {
+            b.lx = fminf(b.lx, __shfl_xor_sync(0xffffffffu, b.lx, off));
+            b.ly = fminf(b.ly, __shfl_xor_sync(0xffffffffu, b.ly, off));
+            b.lz = fminf(b.lz, __shfl_xor_sync(0xffffffffu, b.lz, off));
+            b.hx = fmaxf(b.hx, __shfl_xor_sync(0xffffffffu, b.hx, off));
+            b.hy = fmaxf(b.hy, __shfl_xor_sync(0xffffffffu, b.hy, off));
+            b.hz = fmaxf(b.hz, __shfl_xor_sync(0xffffffffu, b.hz, off));
+        }
+        if ((threadIdx.x & 31) != 0) return;
+    } else if (!valid) {
+        return;
     }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMin(&scene[0], float_to_ordered(b.lx));
-        atomicMin(&scene[1], float_to_ordered(b.ly));
-        atomicMin(&scene[2], float_to_ordered(b.lz));
-        atomicMax(&scene[3], float_to_ordered(b.hx));
-        atomicMax(&scene[4], float_to_ordered(b.hy));
-        atomicMax(&scene[5], float_to_ordered(b.hz));
-    }
+    atomicMin(&sb[0], float_to_ordered(b.lx));
+    atomicMin(&sb[1], float_to_ordered(b.ly));
+    atomicMin(&sb[2], float_to_ordered(b.lz));
+    atomicMax(&sb[3], float_to_ordered(b.hx));
+    atomicMax(&sb[4], float_to_ordered(b.hy));
+    atomicMax(&sb[5], float_to_ordered(b.hz));
+}
+
+__global__ void k_init_bounds(int* scene, int nseg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nseg * 6) return;
+    // +inf as ordered int for mins; -inf (0xFF800000 -> ordered 0x807FFFFF) for maxes
+    scene[i] = (i % 6) < 3 ? 0x7F800000 : (int)0x807FFFFF;
 }
 
 // PT:913-920 expandBits: bit i of the 10-bit input moves to bit 3i.
@@ -158,14 +209,22 @@ __global__ void k_morton(const float4* __restrict__ centroids, int n, const int*
                          uint32_t* __restrict__ codes, int32_t* __restrict__ values) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float lx = ordered_to_float(scene[0]), ly = ordered_to_float(scene[1]), lz = ordered_to_float(scene[2]);
-    float hx = ordered_to_float(scene[3]), hy = ordered_to_float(scene[4]), hz = ordered_to_float(scene[5]);
     float4 c = centroids[i];
+    const int* sb = scene + 6 * __float_as_int(c.w);
+    float lx = ordered_to_float(sb[0]), ly = ordered_to_float(sb[1]), lz = ordered_to_float(sb[2]);
+    float hx = ordered_to_float(sb[3]), hy = ordered_to_float(sb[4]), hz = ordered_to_float(sb[5]);
     uint32_t x = expand_bits(quantize(c.x, lx, hx));
     uint32_t y = expand_bits(quantize(c.y, ly, hy));
     uint32_t z = expand_bits(quantize(c.z, lz, hz));
     codes[i] = x | y << 1 | z << 2;  // PT:934
     if (values) values[i] = i;
+}
+
+// Segment id of the primitive each sorted slot holds (the key of the final stable pass).
+__global__ void k_segment_keys(const float4* __restrict__ centroids, const int32_t* __restrict__ order, int n,
+                               uint32_t* __restrict__ keys) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) keys[k] = (uint32_t)__float_as_int(centroids[order[k]].w);
 }
 
 // ---------------------------------------------------------------------------
@@ -299,7 +358,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __res
 }
 
 // ---------------------------------------------------------------------------
-// Karras 2012 hierarchy (PT:1337-1447).
+// Karras 2012 hierarchy (PT:1337-1447), per segment.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int delta(const uint32_t* __restrict__ codes, int n, int i, int j) {
     if (j < 0 || j >= n) return -1;
@@ -308,42 +367,49 @@ __device__ __forceinline__ int delta(const uint32_t* __restrict__ codes, int n, 
     return __clz(ci ^ cj);
 }
 
-// Child references: internal child c -> c; leaf child k -> ~k.
-__global__ void k_karras(const uint32_t* __restrict__ codes, int n, float4* __restrict__ nodes,
-                         int32_t* __restrict__ parents, mc_bvh_node* __restrict__ ref_internal,
+// Internal node g (global) of segment s works on the segment's codes with the
+// local index g - intOff. Child references are global: internal child c ->
+// intOff + c; leaf child k -> ~(primOff + k). parents: internal nodes at
+// [0, NI), leaves at [NI, NI + N); value (global parent << 1) | side, -1 at roots.
+__global__ void k_karras(const uint32_t* __restrict__ codes, const Seg* __restrict__ seg, int nseg, int NI,
+                         float4* __restrict__ nodes, int32_t* __restrict__ parents, mc_bvh_node* __restrict__ ref_internal,
                          mc_bvh_node* __restrict__ ref_leaves, int2* __restrict__ ranges) {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n - 1) return;
-    int d = (delta(codes, n, idx, idx + 1) - delta(codes, n, idx, idx - 1)) >= 0 ? 1 : -1;
-    int deltaMin = delta(codes, n, idx, idx - d);
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= NI) return;
+    const int s = seg_of_internal(seg, nseg, g);
+    const Seg& S = seg[s];
+    const int n = S.ns + S.nt;
+    const int idx = g - S.intOff;
+    const uint32_t* c = codes + S.primOff;
+    int d = (delta(c, n, idx, idx + 1) - delta(c, n, idx, idx - 1)) >= 0 ? 1 : -1;
+    int deltaMin = delta(c, n, idx, idx - d);
     int lmax = 2;
-    while (delta(codes, n, idx, idx + lmax * d) > deltaMin) lmax *= 2;
+    while (delta(c, n, idx, idx + lmax * d) > deltaMin) lmax *= 2;
     int l = 0;
     for (int t = lmax / 2; t >= 1; t /= 2)
-        if (delta(codes, n, idx, idx + (l + t) * d) > deltaMin) l += t;
+        if (delta(c, n, idx, idx + (l + t) * d) > deltaMin) l += t;
     int jdx = idx + l * d;
     int first = min(idx, jdx);
     int last = max(idx, jdx);
-    int common = delta(codes, n, first, last);
+    int common = delta(c, n, first, last);
     int split = first;
     int step = last - first;
     do {
         step = (step + 1) >> 1;
         int ns = split + step;
-        if (ns < last && delta(codes, n, first, ns) > common) split = ns;
+        if (ns < last && delta(c, n, first, ns) > common) split = ns;
     } while (step > 1);
 
     bool leftLeaf = (split == first);
     bool rightLeaf = (split + 1 == last);
-    if (ranges) ranges[idx] = make_int2(first, last);
-    int leftRef = leftLeaf ? ~split : split;
-    int rightRef = rightLeaf ? ~(split + 1) : (split + 1);
-    nodes[(long long)idx * 4 + 3] = make_float4(__int_as_float(leftRef), __int_as_float(rightRef), 0.f, 0.f);
-    // parents: internal nodes at [0, n-1), leaves at [n-1, 2n-1); value (parent << 1) | side
-    parents[leftLeaf ? (n - 1 + split) : split] = (idx << 1) | 0;
-    parents[rightLeaf ? (n - 1 + split + 1) : (split + 1)] = (idx << 1) | 1;
-    if (idx == 0) parents[0] = -1;
-    if (ref_internal) {
+    ranges[g] = make_int2(first, last);
+    int leftRef = leftLeaf ? ~(S.primOff + split) : (S.intOff + split);
+    int rightRef = rightLeaf ? ~(S.primOff + split + 1) : (S.intOff + split + 1);
+    nodes[(long long)g * 4 + 3] = make_float4(__int_as_float(leftRef), __int_as_float(rightRef), 0.f, 0.f);
+    parents[leftLeaf ? (NI + S.primOff + split) : (S.intOff + split)] = (g << 1) | 0;
+    parents[rightLeaf ? (NI + S.primOff + split + 1) : (S.intOff + split + 1)] = (g << 1) | 1;
+    if (idx == 0) parents[g] = -1;
+    if (ref_internal) {  // single-scene builds only: the reference's node arrays
         mc_bvh_node& r = ref_internal[idx];
         r.left = split;
         r.right = split + 1;
@@ -381,31 +447,43 @@ __device__ __forceinline__ Box load_child_box(const float4* nodes, int node, int
     return b;
 }
 
+__device__ __forceinline__ mc_aabb to_aabb(const Box& b) {
+    mc_aabb m;
+    m.lo = mc_vec3{b.lx, b.ly, b.lz};
+    m.hi = mc_vec3{b.hx, b.hy, b.hz};
+    m.pad0 = 0.f;
+    m.pad1 = 0.f;
+    return m;
+}
+
 // Leaves + refit (buildLeavesKernel PT:1388-1396 and refitBoundsKernel
 // PT:1398-1415): leaf k writes its primitive record and its box into the
 // parent's slot; the second thread to arrive at a node merges the two slots
-// and continues upwards.
-__global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb* __restrict__ bounds_ref, int n, int ns,
-                               const mc_sphere* __restrict__ sph, const mc_triangle_hot* __restrict__ hot,
-                               float4* __restrict__ nodes, float4* __restrict__ prims, const int32_t* __restrict__ parents,
-                               int* __restrict__ counters, int32_t* __restrict__ ids_out, int32_t* __restrict__ types_out,
+// and continues upwards. order[k] is the global (batch) primitive index.
+__global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb* __restrict__ bounds_ref, int N, int NI,
+                               const Seg* __restrict__ seg, int nseg, float4* __restrict__ nodes,
+                               float4* __restrict__ prims, const int32_t* __restrict__ parents, int* __restrict__ counters,
+                               int32_t* __restrict__ ids_out, int32_t* __restrict__ types_out,
                                mc_bvh_node* __restrict__ ref_internal, mc_bvh_node* __restrict__ ref_leaves,
-                               mc_aabb* __restrict__ root_box, int* __restrict__ err) {
+                               mc_aabb* __restrict__ root_boxes, int* __restrict__ err) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= N) return;
     int src = order[k];
-    int type = src < ns ? 0 : 1;
-    int id = src < ns ? src : src - ns;
+    int s = seg_of_prim(seg, nseg, src);
+    const Seg& S = seg[s];
+    int local = src - S.primOff;
+    int type = local < S.ns ? 0 : 1;
+    int id = local < S.ns ? local : local - S.ns;
     float4 r0, r1, r2;
     if (type == 1) {
-        const mc_triangle_hot t = hot[id];
+        const mc_triangle_hot t = S.hot[id];
         r0 = make_float4(t.v0.x, t.v0.y, t.v0.z, t.v1.x);
         r1 = make_float4(t.v1.y, t.v1.z, t.v2.x, t.v2.y);
         r2 = make_float4(t.v2.z, __int_as_float(id), __int_as_float(1), 0.f);
     } else {
-        const mc_sphere& s = sph[id];
-        r0 = make_float4(s.center.x, s.center.y, s.center.z, s.center1.x);
-        r1 = make_float4(s.center1.y, s.center1.z, s.radius, s.is_moving ? 1.f : 0.f);
+        const mc_sphere& sp = S.sph[id];
+        r0 = make_float4(sp.center.x, sp.center.y, sp.center.z, sp.center1.x);
+        r1 = make_float4(sp.center1.y, sp.center1.z, sp.radius, sp.is_moving ? 1.f : 0.f);
         r2 = make_float4(0.f, __int_as_float(id), __int_as_float(0), 0.f);
     }
     prims[(long long)k * 3 + 0] = r0;
@@ -425,18 +503,18 @@ __global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb*
         r.left_is_leaf = 0;
         r.right_is_leaf = 0;
     }
-    if (n == 1) {
-        *root_box = a;
+    if (S.ns + S.nt == 1) {
+        root_boxes[s] = a;
         return;
     }
-    int p = parents[n - 1 + k];
+    int p = parents[NI + k];
     if (p < 0) {
         atomicOr(err, MC_DEVERR_INPUT);  // every leaf of a Karras tree over n >= 2 keys has a parent
         return;
     }
     for (int level = 0; p >= 0; level++) {
         int node = p >> 1, side = p & 1;
-        if (node >= n - 1 || level > 2 * MC_STACK_CAPACITY) {
+        if (node >= NI || level > 2 * MC_STACK_CAPACITY) {
             atomicOr(err, MC_DEVERR_INPUT);
             return;
         }
@@ -447,23 +525,9 @@ __global__ void k_leaves_refit(const int32_t* __restrict__ order, const mc_aabb*
         __threadfence();
         Box other = load_child_box(nodes, node, side ^ 1);
         b = side ? merge_box(other, b) : merge_box(b, other);
-        if (ref_internal) {
-            mc_aabb m;
-            m.lo = mc_vec3{b.lx, b.ly, b.lz};
-            m.hi = mc_vec3{b.hx, b.hy, b.hz};
-            m.pad0 = 0.f;
-            m.pad1 = 0.f;
-            ref_internal[node].bounds = m;
-        }
+        if (ref_internal) ref_internal[node - S.intOff].bounds = to_aabb(b);
         p = parents[node];
-        if (p < 0) {
-            mc_aabb m;
-            m.lo = mc_vec3{b.lx, b.ly, b.lz};
-            m.hi = mc_vec3{b.hx, b.hy, b.hz};
-            m.pad0 = 0.f;
-            m.pad1 = 0.f;
-            *root_box = m;
-        }
+        if (p < 0) root_boxes[s] = to_aabb(b);
     }
 }
 
@@ -483,21 +547,24 @@ __global__ void k_single_root(float4* nodes, const mc_aabb* bounds) {
 // every box overlapping (stepTraversal PT:1276-1321): at a node its leaf
 // children are tested first (left, then right), then its internal children are
 // descended left first. Walking up from a leaf, each ancestor adds the number
-// of leaves emitted before the branch that holds it.
+// of leaves emitted before the branch that holds it. Ranks are made global by
+// the segment's first primitive index.
 // ---------------------------------------------------------------------------
 __global__ void k_leaf_rank(const float4* __restrict__ nodes, const int32_t* __restrict__ parents,
-                            const int2* __restrict__ ranges, int n, int* __restrict__ rank, int* err) {
+                            const int2* __restrict__ ranges, const Seg* __restrict__ seg, int nseg, int N, int NI,
+                            int* __restrict__ rank, int* err) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    if (n == 1) {
-        rank[0] = 0;
+    if (k >= N) return;
+    const Seg& S = seg[seg_of_prim(seg, nseg, k)];
+    if (S.ns + S.nt == 1) {
+        rank[k] = k;
         return;
     }
     int r = 0;
-    int p = parents[n - 1 + k];
+    int p = parents[NI + k];
     for (int level = 0; p >= 0; level++) {
         int node = p >> 1, side = p & 1;
-        if (node >= n - 1 || level > 2 * MC_STACK_CAPACITY) {
+        if (node >= NI || level > 2 * MC_STACK_CAPACITY) {
             atomicOr(err, MC_DEVERR_INPUT);
             return;
         }
@@ -512,23 +579,27 @@ __global__ void k_leaf_rank(const float4* __restrict__ nodes, const int32_t* __r
         }
         p = parents[node];
     }
-    rank[k] = r;
+    rank[k] = S.primOff + r;
 }
 
-// Depth parity of internal nodes: wide nodes are the binary nodes at even depth.
-__global__ void k_wide_select(const int32_t* __restrict__ parents, int n, int* __restrict__ wideId, int* counter) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
+// Depth parity of internal nodes: wide nodes are the binary nodes at even depth
+// of their tree. Roots record their wide id per segment.
+__global__ void k_wide_select(const int32_t* __restrict__ parents, const Seg* __restrict__ seg, int nseg, int NI,
+                              int* __restrict__ wideId, int* counter, int* __restrict__ wideRoot) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= NI) return;
     int depth = 0;
-    int p = parents[i];
+    int p = parents[g];
     while (p >= 0 && depth <= 4 * MC_STACK_CAPACITY) {
         depth++;
         p = parents[p >> 1];
     }
     if (depth & 1) {
-        wideId[i] = -1;
+        wideId[g] = -1;
     } else {
-        wideId[i] = (i == 0) ? 0 : atomicAdd(counter, 1);
+        int id = atomicAdd(counter, 1);
+        wideId[g] = id;
+        if (parents[g] < 0) wideRoot[seg_of_internal(seg, nseg, g)] = id;
     }
 }
 
@@ -540,11 +611,11 @@ __device__ __forceinline__ void child_slot_box(const float4* nodes, int node, in
 }
 
 // One wide node per selected binary node: its children, with each internal
-// child replaced by that child's two children.
+// child replaced by that child's two children. Boxes are copied exactly.
 __global__ void k_wide_fill(const float4* __restrict__ nodes, const int* __restrict__ wideId, const int* __restrict__ rank,
-                            int n, float4* __restrict__ wide) {
+                            int NI, float4* __restrict__ wide) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
+    if (i >= NI) return;
     int id = wideId[i];
     if (id < 0) return;
     float lo[3][4], hi[3][4];
@@ -598,15 +669,15 @@ __global__ void k_reorder_prims(const float4* __restrict__ src, const int* __res
     dst[(long long)r * 3 + 2] = src[(long long)k * 3 + 2];
 }
 
-__global__ void k_leaf_depth(const int32_t* __restrict__ parents, int n, int* depth) {
+__global__ void k_leaf_depth(const int32_t* __restrict__ parents, int N, int NI, int* depth) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= N) return;
     int dcount = 0;
-    int p = parents[n - 1 + k];
+    int p = parents[NI + k];
     while (p >= 0) {
         p = parents[p >> 1];
         dcount++;
-        if (dcount > 4 * n + 8) break;
+        if (dcount > 4 * MC_STACK_CAPACITY) break;
     }
     atomicMax(depth, dcount);
 }
@@ -691,80 +762,12 @@ mc_status bvh_depth(mc_bvh* bvh) {
     int* d;
     MC_CUDA(cudaMalloc(&d, sizeof(int)));
     MC_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx->stream));
-    k_leaf_depth<<<grid_for(bvh->n, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, bvh->n, d);
+    k_leaf_depth<<<grid_for(bvh->n, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, bvh->n, bvh->ni, d);
     int h = 0;
     MC_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     MC_CUDA(cudaStreamSynchronize(ctx->stream));
     cudaFree(d);
     bvh->depth = h;
-    return MC_OK;
-}
-
-// Scene bounds + Morton codes (reference primitive order) into codes; the
-// primitive boxes into bounds_ref (n entries) and the raw bounds words into scene6.
-static mc_status morton_stage(mc_context* ctx, const mc_scene_view* s, uint32_t* codes, int32_t* values, mc_aabb* bounds_ref,
-                              float4* centroids, int* scene6) {
-    int n = s->sphere_count + s->triangle_count;
-    int init[6] = {0x7F800000, 0x7F800000, 0x7F800000, (int)0x807FFFFF, (int)0x807FFFFF, (int)0x807FFFFF};
-    // +inf as ordered int for mins; -inf (0xFF800000 -> ordered 0x807FFFFF) for maxes
-    MC_CUDA(cudaMemcpyAsync(scene6, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
-    k_prim_bounds<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(s->spheres, s->sphere_count, s->tri_hot, s->triangle_count,
-                                                                  bounds_ref, centroids, scene6);
-    k_morton<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(centroids, n, scene6, codes, values);
-    MC_CUDA(cudaGetLastError());
-    return MC_OK;
-}
-
-// 4-wide collapse of a finished binary build (ranges of the Karras nodes are in
-// ctx->scratch[1]); fills bvh->wide_nodes / wide_prims and switches the layout.
-mc_status build_wide(mc_context* ctx, mc_bvh* bvh) {
-    const int n = bvh->n;
-    mc_status st;
-    if ((st = devbuf_reserve(ctx->scratch[2], (size_t)n * 4 + 16)) != MC_OK) return st;
-    if ((st = devbuf_reserve(ctx->scratch[3], (size_t)n * 4 + 16)) != MC_OK) return st;
-    if ((st = devbuf_reserve(ctx->scratch[5], (size_t)n * 4 + 16)) != MC_OK) return st;
-    int* rank = (int*)ctx->scratch[2].ptr;
-    int* wideId = (int*)ctx->scratch[3].ptr;
-    int* counter = (int*)ctx->scratch[5].ptr;
-    k_leaf_rank<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, bvh->parents,
-                                                                (const int2*)ctx->scratch[1].ptr, n, rank, ctx->d_error);
-    int count = 1;
-    if (n >= 2) {
-        MC_CUDA(cudaMemcpyAsync(counter, &count, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        k_wide_select<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, n, wideId, counter);
-        MC_CUDA(cudaMemcpyAsync(&count, counter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    }
-    int flags = 0;
-    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    MC_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (flags) return status_from_device_flags(flags);
-    if (cudaMalloc(&bvh->wide_nodes, (size_t)count * 128) != cudaSuccess ||
-        cudaMalloc(&bvh->wide_prims, (size_t)n * 48) != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(MC_ERR_OOM, "mc_bvh_build: wide-node allocation failed");
-    }
-    if (n >= 2) {
-        k_wide_fill<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, wideId, rank, n,
-                                                                        (float4*)bvh->wide_nodes);
-    } else {
-        // one leaf under the root, three empty slots
-        float inf = INFINITY;
-        mc_aabb a;
-        MC_CUDA(cudaMemcpyAsync(&a, ctx->scratch[0].ptr, sizeof(a), cudaMemcpyDeviceToHost, ctx->stream));
-        MC_CUDA(cudaStreamSynchronize(ctx->stream));
-        float h[32] = {a.lo.x, inf, inf, inf, a.lo.y, inf, inf, inf, a.lo.z, inf, inf, inf,
-                       a.hi.x, -inf, -inf, -inf, a.hi.y, -inf, -inf, -inf, a.hi.z, -inf, -inf, -inf};
-        int refs[4] = {~0, MC_WIDE_EMPTY, MC_WIDE_EMPTY, MC_WIDE_EMPTY};
-        memcpy(&h[24], refs, sizeof(refs));
-        h[28] = h[29] = h[30] = h[31] = 0.f;
-        MC_CUDA(cudaMemcpyAsync(bvh->wide_nodes, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
-    }
-    k_reorder_prims<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->prims, rank, n,
-                                                                    (float4*)bvh->wide_prims);
-    MC_CUDA(cudaGetLastError());
-    MC_CUDA(cudaStreamSynchronize(ctx->stream));
-    bvh->wide_count = count;
-    bvh->layout = MC_BVH_LAYOUT_WIDE4;
     return MC_OK;
 }
 
@@ -779,6 +782,261 @@ static mc_status check_scene(const mc_scene_view* s) {
     return MC_OK;
 }
 
+static mc_status flags_now(mc_context* ctx, int* flags) {
+    MC_CUDA(cudaMemcpyAsync(flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MC_OK;
+}
+
+// Uploads the segment table of the given scenes to ctx->scratch[7] (after the
+// per-segment bounds words) and returns the device pointers.
+static mc_status upload_segments(mc_context* ctx, const mc_scene_view* views, int nseg, std::vector<Seg>& segs, Seg** dSeg,
+                                 int** dBounds, mc_aabb** dRootBoxes, int** dWideRoot) {
+    segs.resize(nseg);
+    int prim = 0;
+    for (int s = 0; s < nseg; s++) {
+        segs[s].sph = views[s].spheres;
+        segs[s].hot = views[s].tri_hot;
+        segs[s].ns = views[s].sphere_count;
+        segs[s].nt = views[s].triangle_count;
+        segs[s].primOff = prim;
+        segs[s].intOff = prim - s;
+        prim += segs[s].ns + segs[s].nt;
+    }
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t bBytes = al((size_t)nseg * 6 * sizeof(int));
+    size_t sBytes = al((size_t)nseg * sizeof(Seg));
+    size_t rBytes = al((size_t)nseg * sizeof(mc_aabb));
+    size_t wBytes = al((size_t)nseg * sizeof(int));
+    mc_status st = devbuf_reserve(ctx->scratch[7], bBytes + sBytes + rBytes + wBytes);
+    if (st != MC_OK) return st;
+    char* base = (char*)ctx->scratch[7].ptr;
+    *dBounds = (int*)base;
+    *dSeg = (Seg*)(base + bBytes);
+    *dRootBoxes = (mc_aabb*)(base + bBytes + sBytes);
+    *dWideRoot = (int*)(base + bBytes + sBytes + rBytes);
+    MC_CUDA(cudaMemcpyAsync(*dSeg, segs.data(), (size_t)nseg * sizeof(Seg), cudaMemcpyHostToDevice, ctx->stream));
+    k_init_bounds<<<grid_for(nseg * 6, kBlock), kBlock, 0, ctx->stream>>>(*dBounds, nseg);
+    return MC_OK;
+}
+
+// 4-wide collapse of a finished binary build (Karras ranges in ctx->scratch[1]).
+static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int nseg, int* dWideRoot) {
+    const int N = bvh->n, NI = bvh->ni;
+    mc_status st;
+    if ((st = devbuf_reserve(ctx->scratch[2], (size_t)N * 4 + 16)) != MC_OK) return st;
+    if ((st = devbuf_reserve(ctx->scratch[3], (size_t)N * 4 + 16)) != MC_OK) return st;
+    if ((st = devbuf_reserve(ctx->scratch[5], (size_t)N * 4 + 16)) != MC_OK) return st;
+    int* rank = (int*)ctx->scratch[2].ptr;
+    int* wideId = (int*)ctx->scratch[3].ptr;
+    int* counter = (int*)ctx->scratch[5].ptr;
+    k_leaf_rank<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, bvh->parents,
+                                                                (const int2*)ctx->scratch[1].ptr, dSeg, nseg, N, NI, rank,
+                                                                ctx->d_error);
+    int count = 1;
+    if (NI > 0) {
+        MC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
+        k_wide_select<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, dSeg, nseg, NI, wideId, counter,
+                                                                       dWideRoot);
+        MC_CUDA(cudaMemcpyAsync(&count, counter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    int flags = 0;
+    if ((st = flags_now(ctx, &flags)) != MC_OK) return st;
+    if (flags) return status_from_device_flags(flags);
+    if (cudaMalloc(&bvh->wide_nodes, (size_t)count * 128) != cudaSuccess ||
+        cudaMalloc(&bvh->wide_prims, (size_t)N * 48) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MC_ERR_OOM, "mc_bvh_build: wide-node allocation failed");
+    }
+    bvh->wide_roots.assign(nseg, 0);
+    if (NI > 0) {
+        k_wide_fill<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, wideId, rank, NI,
+                                                                     (float4*)bvh->wide_nodes);
+        MC_CUDA(cudaMemcpyAsync(bvh->wide_roots.data(), dWideRoot, (size_t)nseg * sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+    } else {
+        // one leaf under the root, three empty slots
+        float inf = INFINITY;
+        mc_aabb a;
+        MC_CUDA(cudaMemcpyAsync(&a, ctx->scratch[0].ptr, sizeof(a), cudaMemcpyDeviceToHost, ctx->stream));
+        MC_CUDA(cudaStreamSynchronize(ctx->stream));
+        float h[32] = {a.lo.x, inf, inf, inf, a.lo.y, inf, inf, inf, a.lo.z, inf, inf, inf,
+                       a.hi.x, -inf, -inf, -inf, a.hi.y, -inf, -inf, -inf, a.hi.z, -inf, -inf, -inf};
+        int refs[4] = {~0, MC_WIDE_EMPTY, MC_WIDE_EMPTY, MC_WIDE_EMPTY};
+        memcpy(&h[24], refs, sizeof(refs));
+        h[28] = h[29] = h[30] = h[31] = 0.f;
+        MC_CUDA(cudaMemcpyAsync(bvh->wide_nodes, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    k_reorder_prims<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->prims, rank, N,
+                                                                    (float4*)bvh->wide_prims);
+    MC_CUDA(cudaGetLastError());
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    bvh->wide_count = count;
+    bvh->layout = MC_BVH_LAYOUT_WIDE4;
+    return MC_OK;
+}
+
+// Builds one BVH over nseg scenes (nseg == 1: a single scene). The reference's
+// node arrays (keep_reference_nodes) and an injected permutation are single-scene only.
+mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, const mc_bvh_build_opts* opts, mc_bvh** out) {
+    if (!ctx || !out || !views || nseg < 1) return set_error(MC_ERR_INVALID, "mc_bvh_build: null argument");
+    *out = nullptr;
+    long long total = 0;
+    for (int s = 0; s < nseg; s++) {
+        mc_status st = check_scene(&views[s]);
+        if (st != MC_OK) return st;
+        long long ns = (long long)views[s].sphere_count + views[s].triangle_count;
+        if (nseg > 1 && ns < 2) return set_error(MC_ERR_INVALID, "mc_bvh_build_batch: every scene needs at least 2 primitives");
+        total += ns;
+    }
+    if (total >= (1ll << 30)) return set_error(MC_ERR_INVALID, "too many primitives in the batch (limit 2^30 - 1)");
+    mc_bvh_build_opts o = {};
+    if (opts) o = *opts;
+    if (o.layout != MC_BVH_LAYOUT_BINARY && o.layout != MC_BVH_LAYOUT_WIDE4)
+        return set_error(MC_ERR_INVALID, "mc_bvh_build: unknown layout");
+    if (nseg > 1 && (o.permutation || o.keep_reference_nodes))
+        return set_error(MC_ERR_INVALID, "mc_bvh_build_batch: permutation and reference nodes are single-scene options");
+    const int N = (int)total;
+    const int NI = N - nseg;  // every scene of n_s >= 1 primitives has n_s - 1 internal nodes
+
+    mc_bvh* bvh = new mc_bvh();
+    bvh->ctx = ctx;
+    bvh->n = N;
+    bvh->ni = NI;
+    bvh->ns = nseg == 1 ? views[0].sphere_count : 0;
+    bvh->nt = nseg == 1 ? views[0].triangle_count : 0;
+    bvh->nseg = nseg;
+    bvh->layout = MC_BVH_LAYOUT_BINARY;
+    auto fail = [&](mc_status s) { mc_bvh_free(bvh); return s; };
+
+    long long nodesCount = std::max(1, NI);
+    if (cudaMalloc(&bvh->nodes, (size_t)nodesCount * 64) != cudaSuccess ||
+        cudaMalloc(&bvh->prims, (size_t)N * 48) != cudaSuccess ||
+        cudaMalloc(&bvh->codes, (size_t)N * 4) != cudaSuccess ||
+        cudaMalloc(&bvh->ids, (size_t)N * 4) != cudaSuccess ||
+        cudaMalloc(&bvh->types, (size_t)N * 4) != cudaSuccess ||
+        cudaMalloc(&bvh->parents, (size_t)(NI + N) * 4 + 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (n=%d)", N));
+    }
+    if (o.keep_reference_nodes) {
+        if (cudaMalloc(&bvh->ref_internal, (size_t)nodesCount * sizeof(mc_bvh_node)) != cudaSuccess ||
+            cudaMalloc(&bvh->ref_leaves, (size_t)N * sizeof(mc_bvh_node)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (reference nodes)"));
+        }
+        cudaMemsetAsync(bvh->ref_internal, 0, (size_t)nodesCount * sizeof(mc_bvh_node), ctx->stream);
+        cudaMemsetAsync(bvh->ref_leaves, 0, (size_t)N * sizeof(mc_bvh_node), ctx->stream);
+    }
+    bvh->node_count = nodesCount;
+    bvh->node_bytes = nodesCount * 64;
+
+    // scratch: [0] primitive boxes, [1] centroids then Karras ranges, [2]/[3] sort buffers,
+    // [4] order, [5] refit counters, [6] sort status, [7] segment table + bounds words
+    mc_status st;
+    if ((st = devbuf_reserve(ctx->scratch[0], (size_t)N * sizeof(mc_aabb))) != MC_OK) return fail(st);
+    if ((st = devbuf_reserve(ctx->scratch[1], (size_t)N * sizeof(float4))) != MC_OK) return fail(st);
+    if ((st = devbuf_reserve(ctx->scratch[2], (size_t)N * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = devbuf_reserve(ctx->scratch[3], (size_t)N * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = devbuf_reserve(ctx->scratch[4], (size_t)N * 4 + 16)) != MC_OK) return fail(st);
+    if ((st = devbuf_reserve(ctx->scratch[5], (size_t)nodesCount * 4 + 16)) != MC_OK) return fail(st);
+    std::vector<Seg> segs;
+    Seg* dSeg;
+    int* dBounds;
+    mc_aabb* dRootBoxes;
+    int* dWideRoot;
+    if ((st = upload_segments(ctx, views, nseg, segs, &dSeg, &dBounds, &dRootBoxes, &dWideRoot)) != MC_OK) return fail(st);
+    mc_aabb* boundsRef = (mc_aabb*)ctx->scratch[0].ptr;
+    float4* centroids = (float4*)ctx->scratch[1].ptr;
+    int32_t* order = (int32_t*)ctx->scratch[4].ptr;
+    int* counters = (int*)ctx->scratch[5].ptr;
+
+    if (cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream) != cudaSuccess)
+        return fail(cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
+    k_prim_bounds<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(dSeg, nseg, N, boundsRef, centroids, dBounds);
+    k_morton<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(centroids, N, dBounds, bvh->codes, order);
+    if (o.permutation) {
+        // caller-provided order (e.g. the reference's std::sort order)
+        if (cudaMemcpyAsync(order, o.permutation, (size_t)N * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+            return fail(cuda_error(cudaGetLastError(), "permutation copy", __FILE__, __LINE__));
+        uint32_t* tmp = (uint32_t*)ctx->scratch[2].ptr;
+        if (cudaMemcpyAsync(tmp, bvh->codes, (size_t)N * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+            return fail(cuda_error(cudaGetLastError(), "code copy", __FILE__, __LINE__));
+        k_gather_u32<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(tmp, order, N, bvh->codes, ctx->d_error);
+        int* seen = (int*)ctx->scratch[3].ptr;
+        if (cudaMemsetAsync(seen, 0, (size_t)N * 4, ctx->stream) != cudaSuccess)
+            return fail(cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
+        k_check_order<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(order, bvh->codes, N, seen, ctx->d_error);
+    } else {
+        st = radix_sort_pairs(ctx, bvh->codes, order, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, N, 30);
+        if (st != MC_OK) return fail(st);
+        if (nseg > 1) {
+            // stable pass on the segment id: the order becomes (segment, code);
+            // the codes follow through a copy in ref order and a gather
+            uint32_t* segKeys = (uint32_t*)ctx->scratch[2].ptr;
+            uint32_t* codesRef = (uint32_t*)ctx->scratch[3].ptr;
+            k_morton<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(centroids, N, dBounds, codesRef, nullptr);
+            k_segment_keys<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(centroids, order, N, segKeys);
+            int bits = 1;
+            while ((1 << bits) < nseg) bits++;
+            // the sort needs its own two scratch arrays: reuse the node buffer (>= N-1 ints) is not enough, so allocate
+            uint32_t* altK = nullptr;
+            int32_t* altV = nullptr;
+            if (cudaMalloc(&altK, (size_t)N * 4) != cudaSuccess || cudaMalloc(&altV, (size_t)N * 4) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFree(altK);
+                return fail(set_error(MC_ERR_OOM, "mc_bvh_build_batch: sort scratch allocation failed"));
+            }
+            st = radix_sort_pairs(ctx, segKeys, order, altK, altV, N, bits);
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(altK);
+            cudaFree(altV);
+            if (st != MC_OK) return fail(st);
+            k_gather_u32<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(codesRef, order, N, bvh->codes, ctx->d_error);
+        }
+    }
+    {
+        // the hierarchy is only built over a valid sorted order
+        int pre = 0;
+        if ((st = flags_now(ctx, &pre)) != MC_OK) return fail(st);
+        if (pre & MC_DEVERR_INPUT)
+            return fail(set_error(MC_ERR_INVALID, "mc_bvh_build: the permutation is not a sorting permutation of the primitives"));
+        if (pre) return fail(status_from_device_flags(pre));
+    }
+    if (cudaMemsetAsync(counters, 0, (size_t)nodesCount * 4, ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(bvh->parents, 0xFF, (size_t)(NI + N) * 4, ctx->stream) != cudaSuccess)
+        return fail(cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
+    if (NI > 0)
+        k_karras<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>(bvh->codes, dSeg, nseg, NI, (float4*)bvh->nodes,
+                                                                  bvh->parents, bvh->ref_internal, bvh->ref_leaves,
+                                                                  (int2*)ctx->scratch[1].ptr);
+    k_leaves_refit<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(order, boundsRef, N, NI, dSeg, nseg, (float4*)bvh->nodes,
+                                                                   (float4*)bvh->prims, bvh->parents, counters, bvh->ids,
+                                                                   bvh->types, bvh->ref_internal, bvh->ref_leaves,
+                                                                   dRootBoxes, ctx->d_error);
+    if (N == 1) k_single_root<<<1, 1, 0, ctx->stream>>>((float4*)bvh->nodes, boundsRef);
+    if (cudaGetLastError() != cudaSuccess) return fail(set_error(MC_ERR_CUDA, "mc_bvh_build: launch failed"));
+    int flags = 0;
+    bvh->seg_bounds.resize(nseg);
+    if (cudaMemcpyAsync(bvh->seg_bounds.data(), dRootBoxes, (size_t)nseg * sizeof(mc_aabb), cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess)
+        return fail(cuda_error(cudaGetLastError(), "mc_bvh_build", __FILE__, __LINE__));
+    if ((st = flags_now(ctx, &flags)) != MC_OK) return fail(st);
+    if (flags) return fail(status_from_device_flags(flags));
+    bvh->bounds = bvh->seg_bounds[0];
+    bvh->seg_prim_off.resize(nseg);
+    bvh->bin_roots.resize(nseg);
+    for (int s = 0; s < nseg; s++) {
+        bvh->seg_prim_off[s] = segs[s].primOff;
+        bvh->bin_roots[s] = segs[s].intOff;
+    }
+    if (o.layout == MC_BVH_LAYOUT_WIDE4) {
+        if ((st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot)) != MC_OK) return fail(st);
+    }
+    *out = bvh;
+    return MC_OK;
+}
+
 }  // namespace mc
 
 extern "C" {
@@ -790,14 +1048,20 @@ mc_status mc_morton_codes(mc_context* ctx, const mc_scene_view* scene, uint32_t*
     int n = scene->sphere_count + scene->triangle_count;
     if ((st = mc::devbuf_reserve(ctx->scratch[0], (size_t)n * sizeof(mc_aabb))) != MC_OK) return st;
     if ((st = mc::devbuf_reserve(ctx->scratch[1], (size_t)n * sizeof(float4))) != MC_OK) return st;
-    if ((st = mc::devbuf_reserve(ctx->scratch[7], 64)) != MC_OK) return st;
-    int* scene6 = (int*)ctx->scratch[7].ptr;
-    st = mc::morton_stage(ctx, scene, d_codes, nullptr, (mc_aabb*)ctx->scratch[0].ptr, (float4*)ctx->scratch[1].ptr, scene6);
-    if (st != MC_OK) return st;
+    std::vector<Seg> segs;
+    Seg* dSeg;
+    int* dBounds;
+    mc_aabb* dRootBoxes;
+    int* dWideRoot;
+    if ((st = mc::upload_segments(ctx, scene, 1, segs, &dSeg, &dBounds, &dRootBoxes, &dWideRoot)) != MC_OK) return st;
+    k_prim_bounds<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(dSeg, 1, n, (mc_aabb*)ctx->scratch[0].ptr,
+                                                                  (float4*)ctx->scratch[1].ptr, dBounds);
+    k_morton<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>((const float4*)ctx->scratch[1].ptr, n, dBounds, d_codes, nullptr);
+    MC_CUDA(cudaGetLastError());
+    int h[6];
+    MC_CUDA(cudaMemcpyAsync(h, dBounds, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
     if (bounds_out) {
-        int h[6];
-        MC_CUDA(cudaMemcpyAsync(h, scene6, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-        MC_CUDA(cudaStreamSynchronize(ctx->stream));
         bounds_out->lo = mc_vec3{ordered_to_float(h[0]), ordered_to_float(h[1]), ordered_to_float(h[2])};
         bounds_out->hi = mc_vec3{ordered_to_float(h[3]), ordered_to_float(h[4]), ordered_to_float(h[5])};
         bounds_out->pad0 = bounds_out->pad1 = 0.f;
@@ -816,123 +1080,19 @@ mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t* d_valu
     st = mc::radix_sort_pairs(ctx, d_keys, d_values, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, n, key_bits);
     if (st != MC_OK) return st;
     int flags = 0;
-    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((st = mc::flags_now(ctx, &flags)) != MC_OK) return st;
     return mc::status_from_device_flags(flags);
 }
 
 mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh_build_opts* opts, mc_bvh** out) {
-    if (!ctx || !out) return mc::set_error(MC_ERR_INVALID, "mc_bvh_build: null argument");
-    *out = nullptr;
-    mc_status st = mc::check_scene(scene);
-    if (st != MC_OK) return st;
-    mc_bvh_build_opts o = {};
-    if (opts) o = *opts;
-    if (o.layout != MC_BVH_LAYOUT_BINARY && o.layout != MC_BVH_LAYOUT_WIDE4)
-        return mc::set_error(MC_ERR_INVALID, "mc_bvh_build: unknown layout");
-    const int ns = scene->sphere_count, nt = scene->triangle_count, n = ns + nt;
+    if (!scene) return mc::set_error(MC_ERR_INVALID, "mc_bvh_build: null scene");
+    return mc::build_segments(ctx, scene, 1, opts, out);
+}
 
-    mc_bvh* bvh = new mc_bvh();
-    bvh->ctx = ctx;
-    bvh->n = n; bvh->ns = ns; bvh->nt = nt;
-    bvh->layout = MC_BVH_LAYOUT_BINARY;
-    auto fail = [&](mc_status s) { mc_bvh_free(bvh); return s; };
-
-    long long nodesCount = std::max(1, n - 1);
-    size_t nodeBytes = (size_t)nodesCount * 64;
-    if (cudaMalloc(&bvh->nodes, nodeBytes) != cudaSuccess ||
-        cudaMalloc(&bvh->prims, (size_t)n * 48) != cudaSuccess ||
-        cudaMalloc(&bvh->codes, (size_t)n * 4) != cudaSuccess ||
-        cudaMalloc(&bvh->ids, (size_t)n * 4) != cudaSuccess ||
-        cudaMalloc(&bvh->types, (size_t)n * 4) != cudaSuccess ||
-        cudaMalloc(&bvh->parents, (size_t)(2 * n) * 4) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(mc::set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (n=%d)", n));
-    }
-    if (o.keep_reference_nodes) {
-        if (cudaMalloc(&bvh->ref_internal, (size_t)nodesCount * sizeof(mc_bvh_node)) != cudaSuccess ||
-            cudaMalloc(&bvh->ref_leaves, (size_t)n * sizeof(mc_bvh_node)) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(mc::set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (reference nodes)"));
-        }
-        cudaMemsetAsync(bvh->ref_internal, 0, (size_t)nodesCount * sizeof(mc_bvh_node), ctx->stream);
-        cudaMemsetAsync(bvh->ref_leaves, 0, (size_t)n * sizeof(mc_bvh_node), ctx->stream);
-    }
-    bvh->node_count = nodesCount;
-    bvh->node_bytes = (long long)nodeBytes;
-
-    // scratch: [0] primitive boxes (ref order), [1] centroids, [2]/[3] sort alt buffers, [4] order, [5] counters, [7] scene6
-    if ((st = mc::devbuf_reserve(ctx->scratch[0], (size_t)n * sizeof(mc_aabb))) != MC_OK) return fail(st);
-    if ((st = mc::devbuf_reserve(ctx->scratch[1], (size_t)n * sizeof(float4))) != MC_OK) return fail(st);
-    if ((st = mc::devbuf_reserve(ctx->scratch[2], (size_t)n * 4 + 16)) != MC_OK) return fail(st);
-    if ((st = mc::devbuf_reserve(ctx->scratch[3], (size_t)n * 4 + 16)) != MC_OK) return fail(st);
-    if ((st = mc::devbuf_reserve(ctx->scratch[4], (size_t)n * 4 + 16)) != MC_OK) return fail(st);
-    if ((st = mc::devbuf_reserve(ctx->scratch[5], (size_t)nodesCount * 4 + 16)) != MC_OK) return fail(st);
-    if ((st = mc::devbuf_reserve(ctx->scratch[7], 64)) != MC_OK) return fail(st);
-    mc_aabb* boundsRef = (mc_aabb*)ctx->scratch[0].ptr;
-    float4* centroids = (float4*)ctx->scratch[1].ptr;
-    int32_t* order = (int32_t*)ctx->scratch[4].ptr;
-    int* counters = (int*)ctx->scratch[5].ptr;
-    int* scene6 = (int*)ctx->scratch[7].ptr;
-
-    if (cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream) != cudaSuccess) return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
-    if ((st = mc::morton_stage(ctx, scene, bvh->codes, order, boundsRef, centroids, scene6)) != MC_OK) return fail(st);
-    if (o.permutation) {
-        // caller-provided order (e.g. the reference's std::sort order)
-        if (cudaMemcpyAsync(order, o.permutation, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
-            return fail(mc::cuda_error(cudaGetLastError(), "permutation copy", __FILE__, __LINE__));
-        uint32_t* tmp = (uint32_t*)ctx->scratch[2].ptr;
-        if (cudaMemcpyAsync(tmp, bvh->codes, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
-            return fail(mc::cuda_error(cudaGetLastError(), "code copy", __FILE__, __LINE__));
-        k_gather_u32<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(tmp, order, n, bvh->codes, ctx->d_error);
-        int* seen = (int*)ctx->scratch[3].ptr;
-        if (cudaMemsetAsync(seen, 0, (size_t)n * 4, ctx->stream) != cudaSuccess)
-            return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
-        k_check_order<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(order, bvh->codes, n, seen, ctx->d_error);
-    } else {
-        st = mc::radix_sort_pairs(ctx, bvh->codes, order, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, n, 30);
-        if (st != MC_OK) return fail(st);
-    }
-    {
-        // the hierarchy is only built over a valid sorted order
-        int pre = 0;
-        if (cudaMemcpyAsync(&pre, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
-            return fail(mc::cuda_error(cudaGetLastError(), "mc_bvh_build", __FILE__, __LINE__));
-        if (pre & MC_DEVERR_INPUT)
-            return fail(mc::set_error(MC_ERR_INVALID, "mc_bvh_build: the permutation is not a sorting permutation of the primitives"));
-        if (pre) return fail(mc::status_from_device_flags(pre));
-    }
-    if (cudaMemsetAsync(counters, 0, (size_t)nodesCount * 4, ctx->stream) != cudaSuccess ||
-        cudaMemsetAsync(bvh->parents, 0xFF, (size_t)(2 * n) * 4, ctx->stream) != cudaSuccess)
-        return fail(mc::cuda_error(cudaGetLastError(), "memset", __FILE__, __LINE__));
-    mc_aabb* rootBox = (mc_aabb*)(scene6 + 8);
-    if (n >= 2) {
-        k_karras<<<grid_for(n - 1, kBlock), kBlock, 0, ctx->stream>>>(bvh->codes, n, (float4*)bvh->nodes, bvh->parents,
-                                                                     bvh->ref_internal, bvh->ref_leaves,
-                                                                     (int2*)ctx->scratch[1].ptr);
-    } else {
-        int m1 = -1;
-        cudaMemcpyAsync(bvh->parents, &m1, 4, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync(bvh->parents + 1, &m1, 4, cudaMemcpyHostToDevice, ctx->stream);
-    }
-    k_leaves_refit<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(order, boundsRef, n, ns, scene->spheres, scene->tri_hot,
-                                                                   (float4*)bvh->nodes, (float4*)bvh->prims, bvh->parents,
-                                                                   counters, bvh->ids, bvh->types, bvh->ref_internal,
-                                                                   bvh->ref_leaves, rootBox, ctx->d_error);
-    if (n == 1) k_single_root<<<1, 1, 0, ctx->stream>>>((float4*)bvh->nodes, boundsRef);
-    if (cudaGetLastError() != cudaSuccess) return fail(mc::set_error(MC_ERR_CUDA, "mc_bvh_build: launch failed"));
-    int flags = 0;
-    if (cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-        cudaMemcpyAsync(&bvh->bounds, rootBox, sizeof(mc_aabb), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
-        return fail(mc::cuda_error(cudaGetLastError(), "mc_bvh_build", __FILE__, __LINE__));
-    if (flags) return fail(mc::status_from_device_flags(flags));
-    if (o.layout == MC_BVH_LAYOUT_WIDE4) {
-        if ((st = mc::build_wide(ctx, bvh)) != MC_OK) return fail(st);
-    }
-    *out = bvh;
-    return MC_OK;
+mc_status mc_bvh_build_batch(mc_context* ctx, const mc_scene_view* scenes, int32_t count, const mc_bvh_build_opts* opts,
+                             mc_bvh** out) {
+    if (!scenes || count < 1) return mc::set_error(MC_ERR_INVALID, "mc_bvh_build_batch: no scenes");
+    return mc::build_segments(ctx, scenes, count, opts, out);
 }
 
 mc_status mc_bvh_free(mc_bvh* bvh) {
@@ -956,7 +1116,7 @@ mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info) {
     mc_status st = mc::bvh_depth(const_cast<mc_bvh*>(bvh));
     if (st != MC_OK) return st;
     info->primitive_count = bvh->n;
-    info->internal_count = bvh->n - 1;
+    info->internal_count = bvh->ni;
     info->depth = bvh->depth;
     info->layout = bvh->layout;
     info->node_bytes = bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_count * 128 : bvh->node_bytes;

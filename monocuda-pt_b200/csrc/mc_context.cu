@@ -124,6 +124,16 @@ mc_status mc_context_destroy(mc_context* ctx) {
     for (auto& b : ctx->scratch) mc::devbuf_free(b);
     mc::devbuf_free(ctx->wave.block);
     cudaFree(ctx->rng_states);
+    if (ctx->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
+    if (ctx->own_stream) {
+        cudaStreamSynchronize(ctx->own_stream);
+        cudaStreamDestroy(ctx->own_stream);
+    }
+    for (void* e : ctx->table_events)
+        if (e) cudaEventDestroy((cudaEvent_t)e);
+    cudaFree(ctx->d_table);
+    if (ctx->h_tables) cudaFreeHost(ctx->h_tables);
+    cudaFree(ctx->scene_of);
     delete ctx;
     return MC_OK;
 }

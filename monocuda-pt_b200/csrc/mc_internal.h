@@ -83,11 +83,27 @@ struct mc_context {
     int rng_pixels = 0;
     unsigned long long rng_seed = 0;
     bool rng_ready = false;
+    // wave tables: device copy + a ring of pinned host tables (one per wave in flight)
+    void* d_table = nullptr;
+    void* h_tables = nullptr;
+    void* table_events[4] = {nullptr, nullptr, nullptr, nullptr};
+    int table_slot = 0;
+    unsigned short* scene_of = nullptr;  // scene id per path (batched waves)
+    int scene_of_capacity = 0;
+    cudaStream_t own_stream = nullptr;   // capture stream when the context has none
+    void* graph_exec = nullptr;          // cached per-wave CUDA graph
+    unsigned long long graph_key = 0;
 };
 
 struct mc_bvh {
     mc_context* ctx = nullptr;
     int n = 0, ns = 0, nt = 0;
+    int ni = 0;                        // internal binary nodes over all segments
+    int nseg = 1;                      // scenes in this build (a batch build has several)
+    std::vector<int> seg_prim_off;     // first leaf (primitive record) index of each scene
+    std::vector<int> bin_roots;        // binary root node of each scene
+    std::vector<int> wide_roots;       // 4-wide root node of each scene
+    std::vector<mc_aabb> seg_bounds;   // root box of each scene
     int layout = MC_BVH_LAYOUT_BINARY;
     int depth = -1;
     void* nodes = nullptr;             // traversal nodes (float4 records)

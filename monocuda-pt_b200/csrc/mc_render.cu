@@ -1,6 +1,7 @@
-// mc_render.cu - the wavefront render path on sm_100a.
+// mc_render.cu - the wavefront render path on sm_100a, for one scene or a batch.
 //
-// One sample of every pixel is one wave. Per bounce d:
+// A wave is one sample of every pixel of every scene in the wave table (a
+// single render call is a table of one scene). Per bounce d:
 //   trace(d)  persistent kernel: closest hits of the bounce-d extend queue AND
 //             the bounce-(d-1) shadow rays, pulled from one work counter by
 //             warps that refill idle lanes (PT:3416-3468 extendKernelPersistent
@@ -8,8 +9,9 @@
 //   shade(d)  grid-stride kernel (PT:3470-3696 shadeKernel) that appends to the
 //             next extend queue and to the shadow queue with one atomic per warp.
 // Queue sizes never leave the device: every kernel reads its count from the
-// per-bounce counter block, so a sample is a fixed launch sequence (no host
-// readback per bounce as in PT:3816), which also makes it graph-capturable.
+// per-bounce counter block, and camera/finalize loop over the path count the
+// table holds, so a wave is a fixed launch sequence (no host readback per
+// bounce as in PT:3816) that is captured once as a CUDA graph and replayed.
 //
 // Compiled with --use_fast_math like the reference (CMakeLists.txt:94-96).
 #include <cuda_runtime.h>
@@ -30,7 +32,41 @@
         if (e__ != cudaSuccess) return mc::cuda_error((int)e__, #call, __FILE__, __LINE__); \
     } while (0)
 
+#define MC_WAVE_MAX_SCENES 128
+
 namespace mc {
+
+// One scene of a wave: its BVH, arrays, camera, image and sample number.
+struct SceneGPU {
+    const float4* nodes;
+    const float4* prims;
+    const mc_sphere* spheres;
+    const mc_triangle_hot* hot;
+    const mc_triangle_cold* cold;
+    const mc_light* lights;
+    float* accum;
+    curandState* xorwow;
+    int root;
+    int hasMedium;
+    int lightCount;
+    int W, H;
+    int pathOffset;
+    int paths;
+    int maxDepth;
+    int disableClamp;
+    uint32_t sample;
+    uint32_t seedLo, seedHi;
+    mc_env_map env;
+    mc_camera cam;
+};
+
+struct WaveTable {
+    int nScenes;
+    int totalPaths;
+    int pad0, pad1;
+    SceneGPU scenes[MC_WAVE_MAX_SCENES];
+};
+
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -41,11 +77,16 @@ MC_D unsigned lanemask_lt() {
     return m;
 }
 
+MC_D int scene_of(const WaveTable* tab, const unsigned short* sceneOf, int path) {
+    return (tab->nScenes > 1 && sceneOf) ? (int)sceneOf[path] : 0;
+}
+
 // ---------------------------------------------------------------------------
 // Trace: extend rays + shadow rays in one persistent launch.
 // ---------------------------------------------------------------------------
 struct TraceArgs {
-    TraceScene ts;
+    const WaveTable* tab;
+    const unsigned short* sceneOf;
     // extend rays: path indices from queue (identity when null), rays from the path SoA
     const int* queue;
     const int* extCount;
@@ -59,14 +100,10 @@ struct TraceArgs {
     const int* spath;
     float *sr, *sg, *sb;   // per-path sample accumulators
     int* occluded;         // ray-set mode: any-hit result per shadow slot instead of accumulation
-    // medium boundaries (PT:2874-2898 mediumTransmittance)
-    const mc_triangle_cold* cold;
-    const mc_sphere* spheres;
     int* work;
     int refill;
     int* err;
     unsigned long long* counts;  // [0] node visits, [1] leaf tests (counting variant)
-    int wide;                    // 4-wide node layout
     int oneShot;                 // plain mode: one ray per thread, no refill
 };
 
@@ -83,34 +120,22 @@ MC_D void flush_counts(const TraceArgs& a, const TravCount& c) {
     }
 }
 
-MC_D void material_medium_info(const TraceArgs& a, int type, int id, int& mtype, float& density) {
-    const mc_material* m = type == 1 ? &a.cold[id].mat : &a.spheres[id].mat;
-    mtype = m->type;
-    density = m->density;
-}
+enum { RAY_EXTEND = 0, RAY_SHADOW_ANY = 1, RAY_SHADOW_MEDIUM = 2 };
 
 // Finishes one ray. Returns true when the lane is free again.
-template <int ISECT, bool MEDIUM>
-MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int slot, float& T, float& travelled,
-                     int& crossings) {
-    if (kind == 0) {
-        mc_packed_hit h;
-        h.t = s.tmax;
+template <int ISECT>
+MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const SceneGPU* S, TravState& s, int step, int kind,
+                     int slot, float& T, float& travelled, int& crossings) {
+    if (kind == RAY_EXTEND) {
+        int type = -1, id = -1, did = 0;
         if (s.hitLeaf >= 0) {
-            int type, id;
-            leaf_identity(a.ts, s.hitLeaf, type, id);
-            h.type = type;
-            h.index = id;
-            h.did_hit = 1;
-        } else {
-            h.type = -1;
-            h.index = -1;
-            h.did_hit = 0;
+            leaf_identity(ts, s.hitLeaf, type, id);
+            did = 1;
         }
-        reinterpret_cast<int4*>(a.hits)[slot] = make_int4(__float_as_int(h.t), h.type, h.index, h.did_hit);
+        reinterpret_cast<int4*>(a.hits)[slot] = make_int4(__float_as_int(s.tmax), type, id, did);
         return true;
     }
-    if (!MEDIUM) {
+    if (kind == RAY_SHADOW_ANY) {
         if (a.occluded) {
             a.occluded[slot] = step == STEP_OCCLUDED ? 1 : 0;
             return true;
@@ -125,24 +150,24 @@ MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int s
         }
         return true;
     }
-    // medium transmittance loop (at most 4 boundary crossings)
+    // medium transmittance loop (PT:2874-2898, at most 4 boundary crossings)
     bool done = false;
     bool blocked = false;
     if (s.hitLeaf < 0) {
         done = true;
     } else {
         int type, id;
-        leaf_identity(a.ts, s.hitLeaf, type, id);
-        int mtype;
-        float density;
-        material_medium_info(a, type, id, mtype, density);
+        leaf_identity(ts, s.hitLeaf, type, id);
+        const mc_material* m = type == 1 ? &S->cold[id].mat : &S->spheres[id].mat;
+        int mtype = m->type;
+        float density = m->density;
         if (mtype != MC_MAT_ISOTROPIC) {
             blocked = true;
             done = true;
         } else {
             bool front;
             if (type == 1) {
-                const float4* rec = a.ts.prims + (long long)s.hitLeaf * 3;
+                const float4* rec = ts.prims + (long long)s.hitLeaf * 3;
                 float4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
                 V3 v0(r0.x, r0.y, r0.z), v1(r0.w, r1.x, r1.y), v2(r1.z, r1.w, r2.x);
                 V3 e1 = v1 - v0;
@@ -150,7 +175,7 @@ MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int s
                 V3 nrm = e1.cross(e2).normalize();
                 front = s.r.d.dot(nrm) < 0.0f;
             } else {
-                const mc_sphere& sp = a.spheres[id];
+                const mc_sphere& sp = S->spheres[id];
                 float tt;
                 V3 outward;
                 hit_sphere_ref(v3(sp.center), v3(sp.center1), sp.is_moving != 0, sp.radius, s.r.o, s.r.d, s.time, tt, front,
@@ -167,7 +192,7 @@ MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int s
                 s.r.o = hp;
                 s.tmax = remaining;
                 s.hitLeaf = -1;
-                s.node = 0;
+                s.node = ts.root;
                 s.sp = 0;
             }
         }
@@ -186,8 +211,10 @@ MC_D bool finish_ray(const TraceArgs& a, TravState& s, int step, int kind, int s
     return true;
 }
 
+// MEDIUM: some scene of the launch holds a medium, so its shadow rays take the
+// closest-hit loop of mediumTransmittance instead of any-hit (PT:3711-3720).
 template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
+__global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
     const unsigned ltmask = lanemask_lt();
@@ -196,10 +223,14 @@ __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
     const int total = extCount + shCount;
     int stack[MC_STACK_CAPACITY];
     TravState s;
+    TraceScene ts;
+    ts.nodes = nullptr;
+    ts.prims = nullptr;
+    ts.root = 0;
     WatertightRay w;
     w.kx = 0; w.ky = 1; w.kz = 2; w.sx = w.sy = w.sz = 0.f;
     bool has = false, exhausted = total == 0;
-    int kind = 0, slot = 0, crossings = 0;
+    int kind = 0, slot = 0, crossings = 0, sid = 0;
     float T = 1.f, travelled = 0.f;
     while (true) {
         if (!exhausted) {
@@ -221,34 +252,40 @@ __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
                         V3 o, d;
                         float time, tmax;
                         if (q < extCount) {
-                            kind = 0;
+                            kind = RAY_EXTEND;
                             slot = a.queue ? a.queue[q] : q;
+                            sid = scene_of(a.tab, a.sceneOf, slot);
                             o = V3(a.ox[slot], a.oy[slot], a.oz[slot]);
                             d = V3(a.dx[slot], a.dy[slot], a.dz[slot]);
                             time = a.time[slot];
                             tmax = 1e30f;
-                            has = true;
                         } else {
-                            kind = 1;
                             slot = q - extCount;
+                            int path = a.spath ? a.spath[slot] : slot;
+                            sid = scene_of(a.tab, a.sceneOf, path);
+                            kind = (MEDIUM && a.tab->scenes[sid].hasMedium) ? RAY_SHADOW_MEDIUM : RAY_SHADOW_ANY;
                             o = V3(a.sox[slot], a.soy[slot], a.soz[slot]);
                             d = V3(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
-                            time = a.spath ? a.time[a.spath[slot]] : a.time[slot];
+                            time = a.time[path];
                             tmax = a.smax[slot];
                             T = 1.f;
                             travelled = 0.f;
                             crossings = 0;
-                            has = true;
-                            if (MEDIUM && tmax <= 0.0f) {
-                                // PT:2880-2881: nothing left to traverse, transmittance 1
-                                s.tmax = tmax;
-                                s.hitLeaf = -1;
-                                finish_ray<ISECT, MEDIUM>(a, s, STEP_DONE, kind, slot, T, travelled, crossings);
-                                has = false;
-                            }
+                        }
+                        const SceneGPU* S = &a.tab->scenes[sid];
+                        ts.nodes = S->nodes;
+                        ts.prims = S->prims;
+                        ts.root = S->root;
+                        has = true;
+                        if (kind == RAY_SHADOW_MEDIUM && tmax <= 0.0f) {
+                            // PT:2880-2881: nothing left to traverse, transmittance 1
+                            s.tmax = tmax;
+                            s.hitLeaf = -1;
+                            finish_ray<ISECT>(a, ts, S, s, STEP_DONE, kind, slot, T, travelled, crossings);
+                            has = false;
                         }
                         if (has) {
-                            trav_begin(s, o, d, time, tmax);
+                            trav_begin(s, o, d, time, tmax, ts.root);
                             if (ISECT == MC_ISECT_WATERTIGHT) w = make_watertight(d);
                         }
                     }
@@ -258,10 +295,10 @@ __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
         }
         if (exhausted && __ballot_sync(kFull, has) == 0u) break;
         if (has) {
-            int r = (kind == 1 && !MEDIUM) ? trav_step_layout<true, ISECT, COUNT, WIDE>(a.ts, s, stack, w, a.err, &cnt)
-                                           : trav_step_layout<false, ISECT, COUNT, WIDE>(a.ts, s, stack, w, a.err, &cnt);
+            int r = (kind == RAY_SHADOW_ANY) ? trav_step_layout<true, ISECT, COUNT, WIDE>(ts, s, stack, w, a.err, &cnt)
+                                             : trav_step_layout<false, ISECT, COUNT, WIDE>(ts, s, stack, w, a.err, &cnt);
             if (r != STEP_CONTINUE) {
-                if (finish_ray<ISECT, MEDIUM>(a, s, r, kind, slot, T, travelled, crossings)) has = false;
+                if (finish_ray<ISECT>(a, ts, &a.tab->scenes[sid], s, r, kind, slot, T, travelled, crossings)) has = false;
             }
         }
     }
@@ -272,14 +309,8 @@ __global__ void __launch_bounds__(256) k_trace(TraceArgs a) {
 // Shade
 // ---------------------------------------------------------------------------
 struct ShadeArgs {
-    const mc_sphere* spheres;
-    const mc_triangle_hot* hot;
-    const mc_triangle_cold* cold;
-    const mc_light* lights;
-    int lightCount;
-    mc_env_map env;
-    float3 background;
-    float rrCap;
+    const WaveTable* tab;
+    const unsigned short* sceneOf;
     int depth;
     float *ox, *oy, *oz, *dx, *dy, *dz;
     const float* time;
@@ -296,8 +327,6 @@ struct ShadeArgs {
     int* spath;
     int* shCount;
     int capacity;
-    curandState* xorwow;
-    uint32_t seedLo, seedHi, sample;
     int* err;
 };
 
@@ -309,24 +338,24 @@ struct ShadeOut {
 };
 
 template <class Rng>
-MC_D void rng_load(const ShadeArgs& a, int p, Rng& rng);
+MC_D void rng_load(const ShadeArgs& a, const SceneGPU& S, int p, Rng& rng);
 template <>
-MC_D void rng_load<PhiloxRng>(const ShadeArgs& a, int p, PhiloxRng& rng) {
-    rng.init(a.seedLo, a.seedHi, a.sample, (uint32_t)p, a.draw[p]);
+MC_D void rng_load<PhiloxRng>(const ShadeArgs& a, const SceneGPU& S, int p, PhiloxRng& rng) {
+    rng.init(S.seedLo, S.seedHi, S.sample, (uint32_t)(p - S.pathOffset), a.draw[p]);
 }
 template <>
-MC_D void rng_load<XorwowRng>(const ShadeArgs& a, int p, XorwowRng& rng) {
-    rng.st = a.xorwow[p];
+MC_D void rng_load<XorwowRng>(const ShadeArgs& a, const SceneGPU& S, int p, XorwowRng& rng) {
+    rng.st = S.xorwow[p - S.pathOffset];
 }
 template <class Rng>
-MC_D void rng_store(const ShadeArgs& a, int p, const Rng& rng);
+MC_D void rng_store(const ShadeArgs& a, const SceneGPU& S, int p, const Rng& rng);
 template <>
-MC_D void rng_store<PhiloxRng>(const ShadeArgs& a, int p, const PhiloxRng& rng) {
+MC_D void rng_store<PhiloxRng>(const ShadeArgs& a, const SceneGPU& S, int p, const PhiloxRng& rng) {
     a.draw[p] = rng.draw;
 }
 template <>
-MC_D void rng_store<XorwowRng>(const ShadeArgs& a, int p, const XorwowRng& rng) {
-    a.xorwow[p] = rng.st;
+MC_D void rng_store<XorwowRng>(const ShadeArgs& a, const SceneGPU& S, int p, const XorwowRng& rng) {
+    S.xorwow[p - S.pathOffset] = rng.st;
 }
 
 struct MatView {
@@ -350,27 +379,28 @@ MC_D MatView load_material(const mc_material& m) {
 
 // PT:3470-3696 shadeKernel for one path.
 template <class Rng>
-MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
+MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out) {
     const int depth = a.depth;
     V3 throughput(a.tr[p], a.tg[p], a.tb[p]);
     V3 cs(a.sr[p], a.sg[p], a.sb[p]);
     int4 hraw = reinterpret_cast<const int4*>(a.hits)[p];
     float hitT = __int_as_float(hraw.x);
     int ptype = hraw.y, pidx = hraw.z, didHit = hraw.w;
-    const V3 background(a.background.x, a.background.y, a.background.z);
+    const V3 background = v3(S.cam.background);
+    const int lightCount = S.lightCount;
     if (!didHit) {
         V3 missDir(a.dx[p], a.dy[p], a.dz[p]);
         float envW = 1.0f;
-        float envProb = env_selection_probability(a.env, a.lightCount);
+        float envProb = env_selection_probability(S.env, lightCount);
         if (!(depth == 0 || a.spec[p] != 0) && envProb > 0.0f)
-            envW = power_heuristic(a.pdf[p], envProb * env_direction_pdf(a.env, missDir));
-        cs = cs + throughput * env_radiance(a.env, missDir, background) * envW;
+            envW = power_heuristic(a.pdf[p], envProb * env_direction_pdf(S.env, missDir));
+        cs = cs + throughput * env_radiance(S.env, missDir, background) * envW;
         a.sr[p] = cs.x;
         a.sg[p] = cs.y;
         a.sb[p] = cs.z;
         return;
     }
-    MatView mat = load_material(ptype == 0 ? a.spheres[pidx].mat : a.cold[pidx].mat);
+    MatView mat = load_material(ptype == 0 ? S.spheres[pidx].mat : S.cold[pidx].mat);
     V3 inDir(a.dx[p], a.dy[p], a.dz[p]);
     V3 o(a.ox[p], a.oy[p], a.oz[p]);
     float rayTime = a.time[p];
@@ -380,7 +410,7 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
     float hitU, hitV;
     V3 tv0, tv1, tv2;
     if (ptype == 0) {
-        const mc_sphere& sp = a.spheres[pidx];
+        const mc_sphere& sp = S.spheres[pidx];
         V3 c = sphere_center_at(v3(sp.center), v3(sp.center1), sp.is_moving != 0, rayTime);
         V3 outward = (hitPoint - c).normalize();
         frontFace = inDir.dot(outward) < 0.0f;
@@ -389,8 +419,8 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
         hitU = uv.x;
         hitV = uv.y;
     } else {
-        const mc_triangle_hot& h = a.hot[pidx];
-        const mc_triangle_cold& cd = a.cold[pidx];
+        const mc_triangle_hot& h = S.hot[pidx];
+        const mc_triangle_cold& cd = S.cold[pidx];
         tv0 = v3(h.v0); tv1 = v3(h.v1); tv2 = v3(h.v2);
         V3 e1 = tv1 - tv0;
         V3 e2 = tv2 - tv0;
@@ -409,7 +439,7 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
         if (fromBsdf && ptype == 1) {
             float cosL = fmaxf(fabsf(inDir.dot(hitNormal)), 1e-4f);
             float area = triangle_area(tv0, tv1, tv2);
-            float lightPdf = light_solid_angle_pdf((1.0f - env_selection_probability(a.env, a.lightCount)) / float(a.lightCount),
+            float lightPdf = light_solid_angle_pdf((1.0f - env_selection_probability(S.env, lightCount)) / float(lightCount),
                                                    hitT, cosL, area);
             emissionWeight = power_heuristic(a.pdf[p], lightPdf);
         }
@@ -420,7 +450,7 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
         return;
     }
     Rng rng;
-    rng_load<Rng>(a, p, rng);
+    rng_load<Rng>(a, S, p, rng);
     V3 scatterOrigin = hitPoint;
     if (mat.type == MC_MAT_ISOTROPIC) {
         float sd;
@@ -430,28 +460,28 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
             a.ox[p] = hitPoint.x;
             a.oy[p] = hitPoint.y;
             a.oz[p] = hitPoint.z;
-            out.next = true;
-            rng_store<Rng>(a, p, rng);
+            out.next = depth + 1 < S.maxDepth;
+            rng_store<Rng>(a, S, p, rng);
             return;
         }
         scatterOrigin = o + inDir * sd;
     }
     throughput = throughput * sample_texture(mat.albedo, hitU, hitV);
 
-    float envProb = env_selection_probability(a.env, a.lightCount);
-    if ((mat.type == MC_MAT_LAMBERTIAN || mat.type == MC_MAT_ISOTROPIC) && (a.lightCount > 0 || envProb > 0.0f)) {
+    float envProb = env_selection_probability(S.env, lightCount);
+    if ((mat.type == MC_MAT_LAMBERTIAN || mat.type == MC_MAT_ISOTROPIC) && (lightCount > 0 || envProb > 0.0f)) {
         V3 toLight, lightColor;
         float dist, solidPdf;
-        if (envProb > 0.0f && (a.lightCount == 0 || rng.uniform() < envProb)) {
+        if (envProb > 0.0f && (lightCount == 0 || rng.uniform() < envProb)) {
             float dirPdf;
-            toLight = env_sample(a.env, rng, dirPdf);
-            lightColor = env_radiance(a.env, toLight, V3(0.f, 0.f, 0.f));
+            toLight = env_sample(S.env, rng, dirPdf);
+            lightColor = env_radiance(S.env, toLight, V3(0.f, 0.f, 0.f));
             dist = 1e30f;
             solidPdf = envProb * dirPdf;
         } else {
-            int li = min((int)(rng.uniform() * a.lightCount), a.lightCount - 1);
-            const mc_light& L = a.lights[li];
-            float sel = (1.0f - envProb) / float(a.lightCount);
+            int li = min((int)(rng.uniform() * lightCount), lightCount - 1);
+            const mc_light& L = S.lights[li];
+            float sel = (1.0f - envProb) / float(lightCount);
             V3 pt = sample_triangle(v3(L.tri.v0), v3(L.tri.v1), v3(L.tri.v2), rng);
             V3 vec = pt - scatterOrigin;
             dist = vec.length();
@@ -478,7 +508,7 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
     bool survives = true;
     if (depth > 3) {
         float maxC = fmaxf(throughput.x, fmaxf(throughput.y, throughput.z));
-        float cont = fminf(maxC, a.rrCap);
+        float cont = fminf(maxC, S.cam.rr_cap);
         if (rng.uniform() > cont) survives = false;
         else throughput = throughput / cont;
     }
@@ -512,9 +542,9 @@ MC_D void shade_path(const ShadeArgs& a, int p, ShadeOut& out) {
         a.spec[p] = (mat.type != MC_MAT_LAMBERTIAN && mat.type != MC_MAT_ISOTROPIC) ? 1 : 0;
         a.pdf[p] = (mat.type == MC_MAT_ISOTROPIC) ? hg_phase_pdf(inDir.dot(nd), mat.g)
                                                    : lambertian_cosine_pdf(fmaxf(nd.dot(hitNormal), 0.0f));
-        out.next = true;
+        out.next = depth + 1 < S.maxDepth;  // the scene's max depth ends the path (PT:3793)
     }
-    rng_store<Rng>(a, p, rng);
+    rng_store<Rng>(a, S, p, rng);
 }
 
 // Warp-aggregated append: one atomicAdd per warp, slots in lane order.
@@ -541,7 +571,8 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
         int p = -1;
         if (q < count) {
             p = a.queue[q];
-            shade_path<Rng>(a, p, out);
+            const SceneGPU& S = a.tab->scenes[scene_of(a.tab, a.sceneOf, p)];
+            shade_path<Rng>(a, S, p, out);
         }
         int ns = warp_reserve(out.shadow, a.shCount, ltmask);
         if (out.shadow) {
@@ -573,8 +604,8 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
 // Camera rays (PT:3342-3374) and per-sample finalize (PT:3740-3755)
 // ---------------------------------------------------------------------------
 struct CameraArgs {
-    mc_camera cam;
-    int W, H;
+    const WaveTable* tab;
+    unsigned short* sceneOf;
     float *ox, *oy, *oz, *dx, *dy, *dz, *time;
     float *tr, *tg, *tb, *sr, *sg, *sb;
     unsigned char* spec;
@@ -582,58 +613,64 @@ struct CameraArgs {
     uint32_t* draw;
     int* queue;
     int* count;
-    curandState* xorwow;
-    uint32_t seedLo, seedHi, sample;
 };
 
-template <class Rng>
-MC_D void camera_rng(const CameraArgs& a, int p, Rng& rng);
-template <>
-MC_D void camera_rng<PhiloxRng>(const CameraArgs& a, int p, PhiloxRng& rng) {
-    rng.init(a.seedLo, a.seedHi, a.sample, (uint32_t)p, 0u);
-}
-template <>
-MC_D void camera_rng<XorwowRng>(const CameraArgs& a, int p, XorwowRng& rng) {
-    rng.st = a.xorwow[p];
+MC_D int find_scene(const WaveTable* tab, int p) {
+    int lo = 0, hi = tab->nScenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (tab->scenes[mid].pathOffset <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
-MC_D void camera_rng_store(const CameraArgs& a, int p, const PhiloxRng& rng) { a.draw[p] = rng.draw; }
-MC_D void camera_rng_store(const CameraArgs& a, int p, const XorwowRng& rng) { a.xorwow[p] = rng.st; }
+MC_D void camera_rng(const SceneGPU& S, int pixel, PhiloxRng& rng) { rng.init(S.seedLo, S.seedHi, S.sample, (uint32_t)pixel, 0u); }
+MC_D void camera_rng(const SceneGPU& S, int pixel, XorwowRng& rng) { rng.st = S.xorwow[pixel]; }
+MC_D void camera_rng_store(const CameraArgs& a, const SceneGPU& S, int p, int pixel, const PhiloxRng& rng) { a.draw[p] = rng.draw; }
+MC_D void camera_rng_store(const CameraArgs& a, const SceneGPU& S, int p, int pixel, const XorwowRng& rng) { S.xorwow[pixel] = rng.st; }
 
 template <class Rng>
 __global__ void k_camera(CameraArgs a) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    int pixels = a.W * a.H;
-    if (p == 0) *a.count = pixels;
-    if (p >= pixels) return;
-    int px = p % a.W, py = p / a.W;
-    Rng rng;
-    camera_rng<Rng>(a, p, rng);
-    V3 o, d;
-    float t;
-    camera_ray(a.cam, px, py, rng, o, d, t);
-    a.ox[p] = o.x; a.oy[p] = o.y; a.oz[p] = o.z;
-    a.dx[p] = d.x; a.dy[p] = d.y; a.dz[p] = d.z;
-    a.time[p] = t;
-    a.tr[p] = 1.0f; a.tg[p] = 1.0f; a.tb[p] = 1.0f;
-    a.sr[p] = 0.0f; a.sg[p] = 0.0f; a.sb[p] = 0.0f;
-    a.spec[p] = 1;
-    a.pdf[p] = 1.0f;
-    a.queue[p] = p;
-    camera_rng_store(a, p, rng);
+    const int total = a.tab->totalPaths;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.count = total;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+        int sid = a.tab->nScenes > 1 ? find_scene(a.tab, p) : 0;
+        const SceneGPU& S = a.tab->scenes[sid];
+        if (a.tab->nScenes > 1) a.sceneOf[p] = (unsigned short)sid;
+        int pixel = p - S.pathOffset;
+        int px = pixel % S.W, py = pixel / S.W;
+        Rng rng;
+        camera_rng(S, pixel, rng);
+        V3 o, d;
+        float t;
+        camera_ray(S.cam, px, py, rng, o, d, t);
+        a.ox[p] = o.x; a.oy[p] = o.y; a.oz[p] = o.z;
+        a.dx[p] = d.x; a.dy[p] = d.y; a.dz[p] = d.z;
+        a.time[p] = t;
+        a.tr[p] = 1.0f; a.tg[p] = 1.0f; a.tb[p] = 1.0f;
+        a.sr[p] = 0.0f; a.sg[p] = 0.0f; a.sb[p] = 0.0f;
+        a.spec[p] = 1;
+        a.pdf[p] = 1.0f;
+        a.queue[p] = p;
+        camera_rng_store(a, S, p, pixel, rng);
+    }
 }
 
-__global__ void k_finalize(float* accum, const float* sr, const float* sg, const float* sb, int pixels, int disableClamp) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= pixels) return;
-    V3 s(sr[p], sg[p], sb[p]);
-    float bright = fmaxf(s.x, fmaxf(s.y, s.z));
-    const float maxBright = 10.0f;
-    if (!disableClamp && bright > maxBright) s = s * (maxBright / bright);
-    float* acc = accum + (size_t)p * 3;
-    acc[0] = acc[0] + s.x;
-    acc[1] = acc[1] + s.y;
-    acc[2] = acc[2] + s.z;
+__global__ void k_finalize(const WaveTable* tab, const unsigned short* sceneOf, const float* sr, const float* sg,
+                           const float* sb) {
+    const int total = tab->totalPaths;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+        const SceneGPU& S = tab->scenes[scene_of(tab, sceneOf, p)];
+        V3 s(sr[p], sg[p], sb[p]);
+        float bright = fmaxf(s.x, fmaxf(s.y, s.z));
+        const float maxBright = 10.0f;
+        if (!S.disableClamp && bright > maxBright) s = s * (maxBright / bright);
+        float* acc = S.accum + (size_t)(p - S.pathOffset) * 3;
+        acc[0] = acc[0] + s.x;
+        acc[1] = acc[1] + s.y;
+        acc[2] = acc[2] + s.z;
+    }
 }
 
 __global__ void k_accumulate_counts(const int* counters, int maxDepth, long long* stats) {
@@ -655,8 +692,41 @@ int occupancy_blocks(const void* fn, int sms) {
     return per * sms;
 }
 
+typedef void (*TraceKernel)(TraceArgs);
+
+// [wide][count][medium][isect]
+#define MC_TK(W)                                                                                                      \
+    {{{k_trace<0, false, false, W>, k_trace<1, false, false, W>}, {k_trace<0, true, false, W>, k_trace<1, true, false, W>}}, \
+     {{k_trace<0, false, true, W>, k_trace<1, false, true, W>}, {k_trace<0, true, true, W>, k_trace<1, true, true, W>}}}
+TraceKernel trace_kernel(bool wide, bool count, bool medium, int isect) {
+    static const TraceKernel table[2][2][2][2] = {MC_TK(false), MC_TK(true)};
+    return table[wide ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
+}
+
+// Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
+// pull rays from the work counter. Plain (PT:3376-3397): the same kernel with
+// one ray per thread and no refill, over plainBlocks blocks; sharing the kernel
+// keeps the per-ray arithmetic identical between the two modes.
+void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, bool wide, bool medium, int isect,
+                  bool persistent, int plainBlocks, bool count = false) {
+    static int occ[32] = {0};
+    TraceArgs t = t0;
+    t.oneShot = persistent ? 0 : 1;
+    TraceKernel fn = trace_kernel(wide, count, medium, isect);
+    int blocks = std::max(1, plainBlocks);
+    if (persistent) {
+        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0);
+        if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count);
+        blocks = occ[key];
+    }
+    fn<<<blocks, 256, 0, stream>>>(t);
+}
+
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
 mc_status ensure_wave(mc_context* ctx, int capacity) {
     WaveBuffers& w = ctx->wave;
     if (w.capacity >= capacity && w.block.ptr) return MC_OK;
@@ -687,70 +757,44 @@ mc_status ensure_wave(mc_context* ctx, int capacity) {
     w.spec = (unsigned char*)take(al(n));
     w.hits = (mc_packed_hit*)take(al(n * 16));
     w.capacity = capacity;
-    return MC_OK;
-}
-
-namespace {
-
-TraceArgs base_trace_args(const mc_bvh* bvh, const mc_scene_view* scene, mc_context* ctx) {
-    TraceArgs t;
-    std::memset(&t, 0, sizeof(t));
-    t.wide = bvh->layout == MC_BVH_LAYOUT_WIDE4 ? 1 : 0;
-    t.ts.nodes = (const float4*)(t.wide ? bvh->wide_nodes : bvh->nodes);
-    t.ts.prims = (const float4*)(t.wide ? bvh->wide_prims : bvh->prims);
-    t.cold = scene->tri_cold;
-    t.spheres = scene->spheres;
-    t.err = ctx->d_error;
-    t.refill = 8;  // PT:3400 minimumIdleLanesBeforeRefill
-    return t;
-}
-
-typedef void (*TraceKernel)(TraceArgs);
-
-// [wide][count][medium][isect]
-#define MC_TK(W)                                                                                                      \
-    {{{k_trace<0, false, false, W>, k_trace<1, false, false, W>}, {k_trace<0, true, false, W>, k_trace<1, true, false, W>}}, \
-     {{k_trace<0, false, true, W>, k_trace<1, false, true, W>}, {k_trace<0, true, true, W>, k_trace<1, true, true, W>}}}
-TraceKernel trace_kernel(bool wide, bool count, bool medium, int isect) {
-    static const TraceKernel table[2][2][2][2] = {MC_TK(false), MC_TK(true)};
-    return table[wide ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
-}
-
-// Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
-// pull rays from the work counter. Plain (PT:3376-3397): the same kernel with
-// one ray per thread and no refill, over plainBlocks blocks; sharing the kernel
-// keeps the per-ray arithmetic identical between the two modes.
-void launch_trace(mc_context* ctx, const TraceArgs& t0, bool medium, int isect, bool persistent, int plainBlocks,
-                  bool count = false) {
-    static int occ[32] = {0};
-    TraceArgs t = t0;
-    t.oneShot = persistent ? 0 : 1;
-    const bool wide = t.wide != 0;
-    TraceKernel fn = trace_kernel(wide, count, medium, isect);
-    int blocks = std::max(1, plainBlocks);
-    if (persistent) {
-        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0);
-        if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count);
-        blocks = occ[key];
+    // the graph captured for the old buffers is stale
+    if (ctx->graph_exec) {
+        cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        ctx->graph_key = 0;
     }
-    fn<<<blocks, 256, 0, ctx->stream>>>(t);
-}
-
-mc_status check_render_inputs(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* p) {
-    if (!ctx || !bvh || !scene || !p) return set_error(MC_ERR_INVALID, "render: null argument");
-    if (p->width <= 0 || p->height <= 0) return set_error(MC_ERR_INVALID, "render: width and height must be positive");
-    if ((long long)p->width * p->height >= (1ll << 30)) return set_error(MC_ERR_INVALID, "render: too many pixels");
-    if (p->spp < 0) return set_error(MC_ERR_INVALID, "render: spp must be >= 0");
-    if (p->max_depth < 0 || p->max_depth > MC_MAX_DEPTH_STATS) return set_error(MC_ERR_INVALID, "render: max_depth must be in [0, 64]");
-    if (p->rng != MC_RNG_PHILOX && p->rng != MC_RNG_XORWOW) return set_error(MC_ERR_INVALID, "render: unknown rng mode");
-    if (p->intersector != MC_ISECT_REFERENCE && p->intersector != MC_ISECT_WATERTIGHT) return set_error(MC_ERR_INVALID, "render: unknown intersector");
-    if (scene->light_count > 0 && !scene->lights) return set_error(MC_ERR_INVALID, "render: null light array");
-    if (scene->triangle_count > 0 && !scene->tri_cold) return set_error(MC_ERR_INVALID, "render: null cold triangle array");
-    if (scene->sphere_count + scene->triangle_count != bvh->n) return set_error(MC_ERR_INVALID, "render: the BVH was built for another scene");
     return MC_OK;
 }
 
-}  // namespace
+static mc_status ensure_tables(mc_context* ctx, int capacity) {
+    if (!ctx->d_table) {
+        MC_CUDA(cudaMalloc(&ctx->d_table, sizeof(WaveTable)));
+        MC_CUDA(cudaMallocHost(&ctx->h_tables, 4 * sizeof(WaveTable)));
+        for (int i = 0; i < 4; i++) MC_CUDA(cudaEventCreateWithFlags((cudaEvent_t*)&ctx->table_events[i], cudaEventDisableTiming));
+    }
+    if (ctx->scene_of_capacity < capacity) {
+        if (ctx->scene_of) cudaFree(ctx->scene_of);
+        ctx->scene_of = nullptr;
+        ctx->scene_of_capacity = 0;
+        MC_CUDA(cudaMalloc(&ctx->scene_of, (size_t)capacity * sizeof(unsigned short)));
+        ctx->scene_of_capacity = capacity;
+        if (ctx->graph_exec) {
+            cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+            ctx->graph_key = 0;
+        }
+    }
+    return MC_OK;
+}
+
+// A pinned host table that no copy in flight reads any more.
+static WaveTable* next_host_table(mc_context* ctx, int* slot) {
+    int s = ctx->table_slot;
+    ctx->table_slot = (s + 1) & 3;
+    cudaEventSynchronize((cudaEvent_t)ctx->table_events[s]);
+    *slot = s;
+    return (WaveTable*)ctx->h_tables + s;
+}
 
 mc_status rng_reset(mc_context* ctx, int pixels, unsigned long long seed) {
     if (ctx->rng_pixels < pixels || !ctx->rng_states) {
@@ -777,84 +821,129 @@ struct RenderTiming {
     int kernel_launches = 0;
 };
 
-mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* p,
-                         float* accum, bool timed, RenderTiming* tm) {
-    const int W = p->width, H = p->height, pixels = W * H;
-    const int maxD = p->max_depth;
+struct WaveItem {
+    const mc_scene_view* view;
+    const mc_render_params* p;
+    float* accum;
+    int root;
+    int segment;
+};
+
+static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* bvh, const WaveItem& it, int pathOffset, uint32_t sample) {
+    SceneGPU g;
+    std::memset(&g, 0, sizeof(g));
+    const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
+    g.nodes = (const float4*)(wide ? bvh->wide_nodes : bvh->nodes);
+    g.prims = (const float4*)(wide ? bvh->wide_prims : bvh->prims);
+    g.root = it.root;
+    g.spheres = it.view->spheres;
+    g.hot = it.view->tri_hot;
+    g.cold = it.view->tri_cold;
+    g.lights = it.view->lights;
+    g.lightCount = it.view->light_count;
+    g.hasMedium = it.view->has_medium;
+    g.env = it.view->env;
+    g.cam = it.p->camera;
+    g.W = it.p->width;
+    g.H = it.p->height;
+    g.pathOffset = pathOffset;
+    g.paths = it.p->width * it.p->height;
+    g.maxDepth = it.p->max_depth;
+    g.disableClamp = it.p->disable_clamp;
+    g.sample = sample;
+    g.seedLo = (uint32_t)it.p->seed;
+    g.seedHi = (uint32_t)(it.p->seed >> 32);
+    g.accum = it.accum;
+    g.xorwow = (curandState*)ctx->rng_states;
+    return g;
+}
+
+// Runs waves until every item has rendered its spp samples. All items share
+// the launch configuration of items[0] (layout, persistence, RNG, intersector).
+mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph, bool timed,
+                    RenderTiming* tm) {
+    const mc_render_params& p0 = *items[0].p;
+    const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
+    const bool philox = p0.rng == MC_RNG_PHILOX;
+    const int isect = p0.intersector;
+    const bool persistent = p0.persistent != 0;
+    const bool countVisits = (p0.instrument & 1) != 0;
+    const bool timeTrace = (p0.instrument & 2) != 0;
+    int capacity = 0, maxD = 0, waves = 0;
+    bool medium = false;
+    for (int i = 0; i < n; i++) {
+        capacity += items[i].p->width * items[i].p->height;
+        maxD = std::max(maxD, items[i].p->max_depth);
+        waves = std::max(waves, items[i].p->spp);
+        medium = medium || items[i].view->has_medium;
+    }
+    mc_status st;
+    if ((st = ensure_wave(ctx, capacity)) != MC_OK) return st;
+    if ((st = ensure_tables(ctx, capacity)) != MC_OK) return st;
     WaveBuffers& w = ctx->wave;
-    const bool medium = scene->has_medium != 0;
-    const int isect = p->intersector;
-    const bool philox = p->rng == MC_RNG_PHILOX;
-    curandState* xs = (curandState*)ctx->rng_states;
+    if (timeTrace || countVisits) useGraph = false;
+    cudaStream_t stream = ctx->stream;
+    if (useGraph && !stream) {
+        if (!ctx->own_stream) MC_CUDA(cudaStreamCreate(&ctx->own_stream));
+        stream = ctx->own_stream;
+    }
     static int shadeBlocks[2] = {0, 0};
     if (!shadeBlocks[0]) shadeBlocks[0] = occupancy_blocks((const void*)k_shade<PhiloxRng>, ctx->sm_count);
     if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng>, ctx->sm_count);
-    const int simpleBlocks = (2 * pixels + 255) / 256;  // extend + shadow rays of one launch, at most one each per path
+    const int plainBlocks = (2 * capacity + 255) / 256;
+    const int loopBlocks = ctx->sm_count * 8;
+    const WaveTable* dtab = (const WaveTable*)ctx->d_table;
+    unsigned short* sceneOf = n > 1 ? ctx->scene_of : nullptr;
 
-    mc_camera cam = p->camera;
     CameraArgs ca;
-    ca.cam = cam; ca.W = W; ca.H = H;
+    ca.tab = dtab;
+    ca.sceneOf = sceneOf;
     ca.ox = w.ox; ca.oy = w.oy; ca.oz = w.oz; ca.dx = w.dx; ca.dy = w.dy; ca.dz = w.dz; ca.time = w.time;
     ca.tr = w.tr; ca.tg = w.tg; ca.tb = w.tb; ca.sr = w.sr; ca.sg = w.sg; ca.sb = w.sb;
     ca.spec = w.spec; ca.pdf = w.pdf; ca.draw = w.draw; ca.queue = w.queue[0];
     ca.count = ctx->d_counters;
-    ca.xorwow = xs;
-    ca.seedLo = (uint32_t)p->seed; ca.seedHi = (uint32_t)(p->seed >> 32);
 
     ShadeArgs sa;
-    sa.spheres = scene->spheres; sa.hot = scene->tri_hot; sa.cold = scene->tri_cold;
-    sa.lights = scene->lights; sa.lightCount = scene->light_count;
-    sa.env = scene->env;
-    sa.background = make_float3(cam.background.x, cam.background.y, cam.background.z);
-    sa.rrCap = cam.rr_cap;
+    std::memset(&sa, 0, sizeof(sa));
+    sa.tab = dtab;
+    sa.sceneOf = sceneOf;
     sa.ox = w.ox; sa.oy = w.oy; sa.oz = w.oz; sa.dx = w.dx; sa.dy = w.dy; sa.dz = w.dz; sa.time = w.time;
     sa.tr = w.tr; sa.tg = w.tg; sa.tb = w.tb; sa.sr = w.sr; sa.sg = w.sg; sa.sb = w.sb;
     sa.spec = w.spec; sa.pdf = w.pdf; sa.draw = w.draw; sa.hits = w.hits;
     sa.sox = w.sox; sa.soy = w.soy; sa.soz = w.soz; sa.sdx = w.sdx; sa.sdy = w.sdy; sa.sdz = w.sdz; sa.smax = w.smax;
     sa.scr = w.scr; sa.scg = w.scg; sa.scb = w.scb; sa.spath = w.spath;
     sa.capacity = w.capacity;
-    sa.xorwow = xs;
-    sa.seedLo = ca.seedLo; sa.seedHi = ca.seedHi;
     sa.err = ctx->d_error;
 
-    TraceArgs ta = base_trace_args(bvh, scene, ctx);
+    TraceArgs ta;
+    std::memset(&ta, 0, sizeof(ta));
+    ta.tab = dtab;
+    ta.sceneOf = sceneOf;
     ta.ox = w.ox; ta.oy = w.oy; ta.oz = w.oz; ta.dx = w.dx; ta.dy = w.dy; ta.dz = w.dz; ta.time = w.time;
     ta.hits = w.hits;
     ta.sox = w.sox; ta.soy = w.soy; ta.soz = w.soz; ta.sdx = w.sdx; ta.sdy = w.sdy; ta.sdz = w.sdz; ta.smax = w.smax;
     ta.scr = w.scr; ta.scg = w.scg; ta.scb = w.scb; ta.spath = w.spath;
     ta.sr = w.sr; ta.sg = w.sg; ta.sb = w.sb;
-    if (p->refill_threshold > 0 && p->refill_threshold <= 32) ta.refill = p->refill_threshold;
-
-    const bool countVisits = (p->instrument & 1) != 0;
-    const bool timeTrace = (p->instrument & 2) != 0;
+    ta.err = ctx->d_error;
+    ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
+
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::vector<cudaEvent_t> traceEvents;
-    if (timed) {
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, ctx->stream);
-    }
-    if (tm) {
-        tm->kernel_launches = 0;
-        tm->trace_launches = 0;
-        tm->trace_ms = 0.f;
-    }
     auto traceEvent = [&]() {
         cudaEvent_t e;
         cudaEventCreate(&e);
-        cudaEventRecord(e, ctx->stream);
+        cudaEventRecord(e, stream);
         traceEvents.push_back(e);
     };
-    for (int s = 0; s < p->spp; s++) {
-        uint32_t sample = (uint32_t)(p->first_sample + s);
-        ca.sample = sample;
-        sa.sample = sample;
-        MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, ctx->stream));
-        if (philox) k_camera<PhiloxRng><<<(pixels + 255) / 256, 256, 0, ctx->stream>>>(ca);
-        else k_camera<XorwowRng><<<(pixels + 255) / 256, 256, 0, ctx->stream>>>(ca);
+    int launches = 0;
+    // the launch sequence of one wave (device table already holds the wave)
+    auto enqueue_wave = [&]() -> mc_status {
+        MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, stream));
+        if (philox) k_camera<PhiloxRng><<<loopBlocks, 256, 0, stream>>>(ca);
+        else k_camera<XorwowRng><<<loopBlocks, 256, 0, stream>>>(ca);
+        launches++;
         for (int d = 0; d <= maxD; d++) {
             TraceArgs t = ta;
             if (d < maxD) {
@@ -869,9 +958,9 @@ mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view
             else { t.shCount = nullptr; t.shN = 0; }
             t.work = C + d * MC_COUNTERS_PER_DEPTH + 2;
             if (timeTrace) traceEvent();
-            launch_trace(ctx, t, medium, isect, p->persistent != 0, simpleBlocks, countVisits);
+            launch_trace(ctx, stream, t, wide, medium, isect, persistent, plainBlocks, countVisits);
             if (timeTrace) traceEvent();
-            if (tm) tm->kernel_launches++;
+            launches++;
             if (d == maxD) break;
             ShadeArgs sd = sa;
             sd.depth = d;
@@ -880,17 +969,75 @@ mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view
             sd.nextQueue = w.queue[(d + 1) & 1];
             sd.nextCount = C + (d + 1) * MC_COUNTERS_PER_DEPTH + 0;
             sd.shCount = C + d * MC_COUNTERS_PER_DEPTH + 1;
-            if (philox) k_shade<PhiloxRng><<<shadeBlocks[0], 256, 0, ctx->stream>>>(sd);
-            else k_shade<XorwowRng><<<shadeBlocks[1], 256, 0, ctx->stream>>>(sd);
-            if (tm) tm->kernel_launches++;
+            if (philox) k_shade<PhiloxRng><<<shadeBlocks[0], 256, 0, stream>>>(sd);
+            else k_shade<XorwowRng><<<shadeBlocks[1], 256, 0, stream>>>(sd);
+            launches++;
         }
-        k_finalize<<<(pixels + 255) / 256, 256, 0, ctx->stream>>>(accum, w.sr, w.sg, w.sb, pixels, p->disable_clamp);
-        k_accumulate_counts<<<1, 64, 0, ctx->stream>>>(C, maxD, ctx->d_stats);
-        if (tm) tm->kernel_launches += 3;  // camera, finalize, count accumulation
+        k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb);
+        k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
+        launches += 2;
+        MC_CUDA(cudaGetLastError());
+        return MC_OK;
+    };
+
+    cudaGraphExec_t exec = nullptr;
+    if (useGraph) {
+        unsigned long long key = ((unsigned long long)(uintptr_t)bvh->nodes) ^ ((unsigned long long)capacity << 20) ^
+                                 ((unsigned long long)maxD << 1) ^ (wide ? 0x100000000ull : 0) ^ (medium ? 0x200000000ull : 0) ^
+                                 (philox ? 0x400000000ull : 0) ^ ((unsigned long long)isect << 35) ^
+                                 (persistent ? 0x1000000000ull : 0) ^ ((unsigned long long)ta.refill << 40) ^
+                                 ((unsigned long long)(n > 1) << 50) ^ ((unsigned long long)(uintptr_t)stream << 8);
+        if (ctx->graph_exec && ctx->graph_key == key) {
+            exec = (cudaGraphExec_t)ctx->graph_exec;
+        } else {
+            if (ctx->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+            cudaGraph_t graph;
+            MC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            mc_status cs = enqueue_wave();
+            cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+            if (cs != MC_OK) return cs;
+            if (ce != cudaSuccess) return cuda_error((int)ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+            ce = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ce != cudaSuccess) return cuda_error((int)ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+            ctx->graph_exec = exec;
+            ctx->graph_key = key;
+        }
+        launches = 0;
     }
-    MC_CUDA(cudaGetLastError());
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (timed) {
-        cudaEventRecord(e1, ctx->stream);
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, stream);
+    }
+    int perWave = 0;
+    for (int wv = 0; wv < waves; wv++) {
+        int slot;
+        WaveTable* h = next_host_table(ctx, &slot);
+        int off = 0, k = 0;
+        for (int i = 0; i < n; i++) {
+            if (items[i].p->spp <= wv) continue;
+            h->scenes[k++] = scene_gpu(ctx, bvh, items[i], off, (uint32_t)(items[i].p->first_sample + wv));
+            off += items[i].p->width * items[i].p->height;
+        }
+        h->nScenes = k;
+        h->totalPaths = off;
+        size_t bytes = offsetof(WaveTable, scenes) + (size_t)std::max(k, 1) * sizeof(SceneGPU);
+        MC_CUDA(cudaMemcpyAsync(ctx->d_table, h, bytes, cudaMemcpyHostToDevice, stream));
+        MC_CUDA(cudaEventRecord((cudaEvent_t)ctx->table_events[slot], stream));
+        if (useGraph) {
+            MC_CUDA(cudaGraphLaunch(exec, stream));
+            perWave = 3 + 2 * maxD;
+        } else {
+            if ((st = enqueue_wave()) != MC_OK) return st;
+        }
+    }
+    if (useGraph) launches = perWave * waves;
+    if (timed) {
+        cudaEventRecord(e1, stream);
         cudaEventSynchronize(e1);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
@@ -898,6 +1045,7 @@ mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
+    if (tm) tm->kernel_launches = launches;
     if (!traceEvents.empty()) {
         cudaEventSynchronize(traceEvents.back());
         for (size_t i = 0; i + 1 < traceEvents.size(); i += 2) {
@@ -910,35 +1058,24 @@ mc_status render_samples(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view
         }
         for (cudaEvent_t e : traceEvents) cudaEventDestroy(e);
     }
+    if (stream != ctx->stream) MC_CUDA(cudaStreamSynchronize(stream));
     return MC_OK;
 }
 
-}  // namespace mc
-
-extern "C" {
-
-mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed) {
-    if (!ctx || width <= 0 || height <= 0) return mc::set_error(MC_ERR_INVALID, "mc_rng_reset: bad argument");
-    return mc::rng_reset(ctx, width * height, seed);
+static mc_status check_params(const mc_render_params* p, const mc_scene_view* v) {
+    if (!p || !v) return set_error(MC_ERR_INVALID, "render: null argument");
+    if (p->width <= 0 || p->height <= 0) return set_error(MC_ERR_INVALID, "render: width and height must be positive");
+    if ((long long)p->width * p->height >= (1ll << 30)) return set_error(MC_ERR_INVALID, "render: too many pixels");
+    if (p->spp < 0) return set_error(MC_ERR_INVALID, "render: spp must be >= 0");
+    if (p->max_depth < 0 || p->max_depth > MC_MAX_DEPTH_STATS) return set_error(MC_ERR_INVALID, "render: max_depth must be in [0, 64]");
+    if (p->rng != MC_RNG_PHILOX && p->rng != MC_RNG_XORWOW) return set_error(MC_ERR_INVALID, "render: unknown rng mode");
+    if (p->intersector != MC_ISECT_REFERENCE && p->intersector != MC_ISECT_WATERTIGHT) return set_error(MC_ERR_INVALID, "render: unknown intersector");
+    if (v->light_count > 0 && !v->lights) return set_error(MC_ERR_INVALID, "render: null light array");
+    if (v->triangle_count > 0 && !v->tri_cold) return set_error(MC_ERR_INVALID, "render: null cold triangle array");
+    return MC_OK;
 }
 
-mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* params,
-                              float* d_accum, mc_render_stats* stats) {
-    mc_status st = mc::check_render_inputs(ctx, bvh, scene, params);
-    if (st != MC_OK) return st;
-    if (!d_accum) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: null accumulation buffer");
-    int pixels = params->width * params->height;
-    int cap = params->queue_capacity > 0 ? params->queue_capacity : pixels;
-    if (cap < pixels) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: queue capacity below width*height");
-    if ((st = mc::ensure_wave(ctx, cap)) != MC_OK) return st;
-    if (params->rng == MC_RNG_XORWOW && (!ctx->rng_ready || ctx->rng_pixels < pixels || ctx->rng_seed != params->seed)) {
-        if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
-    }
-    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
-    MC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long), ctx->stream));
-    mc::RenderTiming tm;
-    st = mc::render_samples(ctx, bvh, scene, params, d_accum, stats != nullptr, &tm);
-    if (st != MC_OK) return st;
+static mc_status finish_stats(mc_context* ctx, const RenderTiming& tm, long long paths, mc_render_stats* stats) {
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     if (stats) {
@@ -954,7 +1091,7 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
         }
         stats->node_visits = h[2 * MC_MAX_DEPTH_STATS];
         stats->leaf_tests = h[2 * MC_MAX_DEPTH_STATS + 1];
-        stats->paths = (long long)pixels * params->spp;
+        stats->paths = paths;
         stats->render_ms = tm.ms;
         stats->trace_ms = tm.trace_ms;
         stats->trace_launches = tm.trace_launches;
@@ -963,7 +1100,87 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
     } else {
         MC_CUDA(cudaStreamSynchronize(ctx->stream));
     }
-    return mc::status_from_device_flags(flags);
+    return status_from_device_flags(flags);
+}
+
+mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph,
+                       mc_render_stats* stats) {
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    MC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long), ctx->stream));
+    RenderTiming tm;
+    mc_status st = run_waves(ctx, bvh, items, n, useGraph, stats != nullptr, &tm);
+    if (st != MC_OK) return st;
+    long long paths = 0;
+    for (int i = 0; i < n; i++) paths += (long long)items[i].p->width * items[i].p->height * items[i].p->spp;
+    return finish_stats(ctx, tm, paths, stats);
+}
+
+// A one-scene wave table for the ray-set entry points.
+static mc_status ray_set_table(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene) {
+    mc_status st;
+    if ((st = ensure_tables(ctx, 1)) != MC_OK) return st;
+    int slot;
+    WaveTable* h = next_host_table(ctx, &slot);
+    mc_render_params p;
+    std::memset(&p, 0, sizeof(p));
+    p.width = p.height = 1;
+    WaveItem it{scene, &p, nullptr, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
+    h->nScenes = 1;
+    h->totalPaths = 0;
+    h->scenes[0] = scene_gpu(ctx, bvh, it, 0, 0);
+    MC_CUDA(cudaMemcpyAsync(ctx->d_table, h, offsetof(WaveTable, scenes) + sizeof(SceneGPU), cudaMemcpyHostToDevice, ctx->stream));
+    MC_CUDA(cudaEventRecord((cudaEvent_t)ctx->table_events[slot], ctx->stream));
+    return MC_OK;
+}
+
+}  // namespace mc
+
+extern "C" {
+
+mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed) {
+    if (!ctx || width <= 0 || height <= 0) return mc::set_error(MC_ERR_INVALID, "mc_rng_reset: bad argument");
+    return mc::rng_reset(ctx, width * height, seed);
+}
+
+mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* params,
+                              float* d_accum, mc_render_stats* stats) {
+    if (!ctx || !bvh) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: null argument");
+    mc_status st = mc::check_params(params, scene);
+    if (st != MC_OK) return st;
+    if (!d_accum) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: null accumulation buffer");
+    if (bvh->nseg != 1) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: a batch BVH renders with mc_render_batch");
+    if (scene->sphere_count + scene->triangle_count != bvh->n) return mc::set_error(MC_ERR_INVALID, "render: the BVH was built for another scene");
+    int pixels = params->width * params->height;
+    if (params->queue_capacity > 0 && params->queue_capacity < pixels)
+        return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: queue capacity below width*height");
+    if (params->rng == MC_RNG_XORWOW && (!ctx->rng_ready || ctx->rng_pixels < pixels || ctx->rng_seed != params->seed)) {
+        if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
+    }
+    mc::WaveItem it{scene, params, d_accum, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
+    return mc::render_items(ctx, bvh, &it, 1, params->use_graph != 0, stats);
+}
+
+mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_item* items, int32_t count, int32_t use_graph,
+                          mc_render_stats* stats) {
+    if (!ctx || !bvh || !items || count < 1) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: bad argument");
+    if (count > MC_WAVE_MAX_SCENES) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: at most %d scenes per batch", MC_WAVE_MAX_SCENES);
+    if (count != bvh->nseg) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: %d items for a BVH of %d scenes", count, bvh->nseg);
+    std::vector<mc::WaveItem> its((size_t)count);
+    long long capacity = 0;
+    for (int i = 0; i < count; i++) {
+        mc_status st = mc::check_params(&items[i].params, &items[i].scene);
+        if (st != MC_OK) return st;
+        if (!items[i].d_accum) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: null accumulation buffer (item %d)", i);
+        if (items[i].params.rng != MC_RNG_PHILOX) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: batches use the counter-based RNG");
+        int prims = items[i].scene.sphere_count + items[i].scene.triangle_count;
+        int segPrims = (i + 1 < bvh->nseg ? bvh->seg_prim_off[i + 1] : bvh->n) - bvh->seg_prim_off[i];
+        if (prims != segPrims) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: item %d does not match scene %d of the BVH", i, i);
+        capacity += (long long)items[i].params.width * items[i].params.height;
+        its[i] = mc::WaveItem{&items[i].scene, &items[i].params, items[i].d_accum,
+                              bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[i] : bvh->bin_roots[i], i};
+    }
+    if (capacity >= (1ll << 30)) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: too many paths per wave");
+    return mc::render_items(ctx, bvh, its.data(), count, use_graph != 0, stats);
 }
 
 mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const float* d_rays, int32_t n,
@@ -972,24 +1189,26 @@ mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     const bool plain = (intersector & MC_TRACE_PLAIN) != 0;
     intersector &= ~MC_TRACE_PLAIN;
     if (intersector != MC_ISECT_REFERENCE && intersector != MC_ISECT_WATERTIGHT) return mc::set_error(MC_ERR_INVALID, "mc_trace_closest: unknown intersector");
+    if (bvh->nseg != 1) return mc::set_error(MC_ERR_INVALID, "mc_trace_closest: needs a single-scene BVH");
     if (n == 0) return MC_OK;
     mc_status st;
     if ((st = mc::devbuf_reserve(ctx->scratch[5], 64)) != MC_OK) return st;
+    if ((st = mc::ray_set_table(ctx, bvh, scene)) != MC_OK) return st;
     int* work = (int*)ctx->scratch[5].ptr;
     MC_CUDA(cudaMemsetAsync(work, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
-    mc::TraceArgs t = mc::base_trace_args(bvh, scene, ctx);
+    mc::TraceArgs t;
+    std::memset(&t, 0, sizeof(t));
+    t.tab = (const mc::WaveTable*)ctx->d_table;
+    t.err = ctx->d_error;
+    t.refill = 8;
     size_t N = (size_t)n;
-    t.queue = nullptr;
-    t.extCount = nullptr;
     t.extN = n;
     t.ox = d_rays; t.oy = d_rays + N; t.oz = d_rays + 2 * N;
     t.dx = d_rays + 3 * N; t.dy = d_rays + 4 * N; t.dz = d_rays + 5 * N; t.time = d_rays + 6 * N;
     t.hits = d_hits;
-    t.shCount = nullptr;
-    t.shN = 0;
     t.work = work;
-    mc::launch_trace(ctx, t, false, intersector, !plain, (n + 255) / 256);
+    mc::launch_trace(ctx, ctx->stream, t, bvh->layout == MC_BVH_LAYOUT_WIDE4, false, intersector, !plain, (n + 255) / 256);
     MC_CUDA(cudaGetLastError());
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1003,27 +1222,28 @@ mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* 
     const bool plain = (intersector & MC_TRACE_PLAIN) != 0;
     intersector &= ~MC_TRACE_PLAIN;
     if (intersector != MC_ISECT_REFERENCE && intersector != MC_ISECT_WATERTIGHT) return mc::set_error(MC_ERR_INVALID, "mc_trace_any: unknown intersector");
+    if (bvh->nseg != 1) return mc::set_error(MC_ERR_INVALID, "mc_trace_any: needs a single-scene BVH");
     if (n == 0) return MC_OK;
     mc_status st;
     if ((st = mc::devbuf_reserve(ctx->scratch[5], 64)) != MC_OK) return st;
+    if ((st = mc::ray_set_table(ctx, bvh, scene)) != MC_OK) return st;
     int* work = (int*)ctx->scratch[5].ptr;
     MC_CUDA(cudaMemsetAsync(work, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
-    mc::TraceArgs t = mc::base_trace_args(bvh, scene, ctx);
+    mc::TraceArgs t;
+    std::memset(&t, 0, sizeof(t));
+    t.tab = (const mc::WaveTable*)ctx->d_table;
+    t.err = ctx->d_error;
+    t.refill = 8;
     size_t N = (size_t)n;
-    t.queue = nullptr;
-    t.extCount = nullptr;
-    t.extN = 0;
-    t.shCount = nullptr;
     t.shN = n;
     t.sox = d_rays; t.soy = d_rays + N; t.soz = d_rays + 2 * N;
     t.sdx = d_rays + 3 * N; t.sdy = d_rays + 4 * N; t.sdz = d_rays + 5 * N;
     t.time = d_rays + 6 * N;
-    t.spath = nullptr;
     t.smax = d_tmax;
     t.occluded = d_occluded;
     t.work = work;
-    mc::launch_trace(ctx, t, false, intersector, !plain, (n + 255) / 256);
+    mc::launch_trace(ctx, ctx->stream, t, bvh->layout == MC_BVH_LAYOUT_WIDE4, false, intersector, !plain, (n + 255) / 256);
     MC_CUDA(cudaGetLastError());
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

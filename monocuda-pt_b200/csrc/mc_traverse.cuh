@@ -19,8 +19,9 @@ namespace mc {
 enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_OCCLUDED = 2 };
 
 struct TraceScene {
-    const float4* __restrict__ nodes;   // binary: 4 float4 per internal node
+    const float4* __restrict__ nodes;   // binary: 4 float4 per internal node; wide: 8
     const float4* __restrict__ prims;   // 3 float4 per leaf
+    int root;                           // root node of this scene (batched builds share the arrays)
 };
 
 // Traversal state of one ray in one lane.
@@ -33,12 +34,12 @@ struct TravState {
     int sp;
 };
 
-MC_D void trav_begin(TravState& s, const V3& o, const V3& d, float time, float tmax) {
+MC_D void trav_begin(TravState& s, const V3& o, const V3& d, float time, float tmax, int root) {
     s.r = make_ray_inv(o, d);
     s.time = time;
     s.tmax = tmax;
     s.hitLeaf = -1;
-    s.node = 0;
+    s.node = root;
     s.sp = 0;
 }
 

@@ -132,6 +132,10 @@ class RenderStats(C.Structure):
                 ("trace_launches", C.c_int32), ("kernel_launches", C.c_int32), ("error_flags", C.c_int32)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("scene", SceneView), ("params", RenderParams), ("d_accum", C.c_void_p)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("variant", C.c_int32), ("seed", C.c_uint64), ("triangle_target", C.c_int32)]
 
@@ -170,6 +174,8 @@ SIGNATURES = {
     "mc_morton_codes": (I32, [P, C.POINTER(SceneView), P, C.POINTER(AABB)]),
     "mc_radix_sort_pairs": (I32, [P, P, P, I32, I32]),
     "mc_bvh_build": (I32, [P, C.POINTER(SceneView), C.POINTER(BvhBuildOpts), C.POINTER(P)]),
+    "mc_bvh_build_batch": (I32, [P, P, I32, C.POINTER(BvhBuildOpts), C.POINTER(P)]),
+    "mc_render_batch": (I32, [P, P, P, I32, I32, C.POINTER(RenderStats)]),
     "mc_bvh_free": (I32, [P]),
     "mc_bvh_get_info": (I32, [P, C.POINTER(BvhInfo)]),
     "mc_bvh_export": (I32, [P, P, P, P, P, P]),
@@ -264,6 +270,38 @@ class Bvh:
 
     def export(self, codes=None, ids=None, types=None, internal=None, leaves=None):
         check(self.lib.mc_bvh_export(self.handle, ptr(codes), ptr(ids), ptr(types), ptr(internal), ptr(leaves)))
+
+    def close(self):
+        if self.handle:
+            self.lib.mc_bvh_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchBvh:
+    """One build over several device scenes (mc_bvh_build_batch)."""
+
+    def __init__(self, ctx, views, layout=LAYOUT_WIDE4):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        arr = (SceneView * len(views))(*views)
+        opts = BvhBuildOpts(None, layout, 0)
+        h = P()
+        check(self.lib.mc_bvh_build_batch(ctx.handle, C.addressof(arr), len(views), C.byref(opts), C.byref(h)))
+        self.handle = h
+        self.count = len(views)
+
+    def render(self, items, use_graph=False):
+        arr = (BatchItem * len(items))(*items)
+        st = RenderStats()
+        check(self.lib.mc_render_batch(self.ctx.handle, self.handle, C.addressof(arr), len(items), 1 if use_graph else 0,
+                                       C.byref(st)))
+        return st
 
     def close(self):
         if self.handle:
