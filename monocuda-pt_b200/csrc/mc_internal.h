@@ -92,7 +92,7 @@ struct mc_context {
     int scene_of_capacity = 0;
     cudaStream_t own_stream = nullptr;   // capture stream when the context has none
     void* graph_exec = nullptr;          // cached per-wave CUDA graph
-    unsigned long long graph_key = 0;
+    unsigned long long graph_key[16] = {};  // every value the captured launches bake in
 };
 
 struct mc_bvh {

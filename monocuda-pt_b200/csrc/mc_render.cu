@@ -87,6 +87,11 @@ MC_D int scene_of(const WaveTable* tab, const unsigned short* sceneOf, int path)
 struct TraceArgs {
     const WaveTable* tab;
     const unsigned short* sceneOf;
+    // single-scene launches: the scene's BVH as kernel parameters (constant bank, no registers)
+    TraceScene ts0;
+    int medium0;
+    const mc_sphere* spheres0;
+    const mc_triangle_cold* cold0;
     // extend rays: path indices from queue (identity when null), rays from the path SoA
     const int* queue;
     const int* extCount;
@@ -124,8 +129,8 @@ enum { RAY_EXTEND = 0, RAY_SHADOW_ANY = 1, RAY_SHADOW_MEDIUM = 2 };
 
 // Finishes one ray. Returns true when the lane is free again.
 template <int ISECT>
-MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const SceneGPU* S, TravState& s, int step, int kind,
-                     int slot, float& T, float& travelled, int& crossings) {
+MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle_cold* cold, const mc_sphere* spheres,
+                     TravState& s, int step, int kind, int slot, float& T, float& travelled, int& crossings) {
     if (kind == RAY_EXTEND) {
         int type = -1, id = -1, did = 0;
         if (s.hitLeaf >= 0) {
@@ -158,7 +163,7 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const SceneGPU* S
     } else {
         int type, id;
         leaf_identity(ts, s.hitLeaf, type, id);
-        const mc_material* m = type == 1 ? &S->cold[id].mat : &S->spheres[id].mat;
+        const mc_material* m = type == 1 ? &cold[id].mat : &spheres[id].mat;
         int mtype = m->type;
         float density = m->density;
         if (mtype != MC_MAT_ISOTROPIC) {
@@ -175,7 +180,7 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const SceneGPU* S
                 V3 nrm = e1.cross(e2).normalize();
                 front = s.r.d.dot(nrm) < 0.0f;
             } else {
-                const mc_sphere& sp = S->spheres[id];
+                const mc_sphere& sp = spheres[id];
                 float tt;
                 V3 outward;
                 hit_sphere_ref(v3(sp.center), v3(sp.center1), sp.is_moving != 0, sp.radius, s.r.o, s.r.d, s.time, tt, front,
@@ -213,7 +218,10 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const SceneGPU* S
 
 // MEDIUM: some scene of the launch holds a medium, so its shadow rays take the
 // closest-hit loop of mediumTransmittance instead of any-hit (PT:3711-3720).
-template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE>
+// BATCH: rays of several scenes share the launch; each lane reads its ray's
+// scene from the wave table. A single-scene launch reads the scene from the
+// kernel parameters instead, which costs no registers.
+template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE, bool BATCH>
 __global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
@@ -223,10 +231,11 @@ __global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
     const int total = extCount + shCount;
     int stack[MC_STACK_CAPACITY];
     TravState s;
-    TraceScene ts;
-    ts.nodes = nullptr;
-    ts.prims = nullptr;
-    ts.root = 0;
+    TraceScene tsLane;
+    tsLane.nodes = nullptr;
+    tsLane.prims = nullptr;
+    tsLane.root = 0;
+    const TraceScene& ts = BATCH ? tsLane : a.ts0;
     WatertightRay w;
     w.kx = 0; w.ky = 1; w.kz = 2; w.sx = w.sy = w.sz = 0.f;
     bool has = false, exhausted = total == 0;
@@ -254,7 +263,7 @@ __global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
                         if (q < extCount) {
                             kind = RAY_EXTEND;
                             slot = a.queue ? a.queue[q] : q;
-                            sid = scene_of(a.tab, a.sceneOf, slot);
+                            if (BATCH) sid = scene_of(a.tab, a.sceneOf, slot);
                             o = V3(a.ox[slot], a.oy[slot], a.oz[slot]);
                             d = V3(a.dx[slot], a.dy[slot], a.dz[slot]);
                             time = a.time[slot];
@@ -262,8 +271,9 @@ __global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
                         } else {
                             slot = q - extCount;
                             int path = a.spath ? a.spath[slot] : slot;
-                            sid = scene_of(a.tab, a.sceneOf, path);
-                            kind = (MEDIUM && a.tab->scenes[sid].hasMedium) ? RAY_SHADOW_MEDIUM : RAY_SHADOW_ANY;
+                            if (BATCH) sid = scene_of(a.tab, a.sceneOf, path);
+                            const bool med = MEDIUM && (BATCH ? a.tab->scenes[sid].hasMedium != 0 : a.medium0 != 0);
+                            kind = med ? RAY_SHADOW_MEDIUM : RAY_SHADOW_ANY;
                             o = V3(a.sox[slot], a.soy[slot], a.soz[slot]);
                             d = V3(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
                             time = a.time[path];
@@ -272,16 +282,19 @@ __global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
                             travelled = 0.f;
                             crossings = 0;
                         }
-                        const SceneGPU* S = &a.tab->scenes[sid];
-                        ts.nodes = S->nodes;
-                        ts.prims = S->prims;
-                        ts.root = S->root;
+                        if (BATCH) {
+                            const SceneGPU* S = &a.tab->scenes[sid];
+                            tsLane.nodes = S->nodes;
+                            tsLane.prims = S->prims;
+                            tsLane.root = S->root;
+                        }
                         has = true;
                         if (kind == RAY_SHADOW_MEDIUM && tmax <= 0.0f) {
                             // PT:2880-2881: nothing left to traverse, transmittance 1
+                            // (no leaf, so the material arrays are not read)
                             s.tmax = tmax;
                             s.hitLeaf = -1;
-                            finish_ray<ISECT>(a, ts, S, s, STEP_DONE, kind, slot, T, travelled, crossings);
+                            finish_ray<ISECT>(a, ts, nullptr, nullptr, s, STEP_DONE, kind, slot, T, travelled, crossings);
                             has = false;
                         }
                         if (has) {
@@ -298,7 +311,13 @@ __global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
             int r = (kind == RAY_SHADOW_ANY) ? trav_step_layout<true, ISECT, COUNT, WIDE>(ts, s, stack, w, a.err, &cnt)
                                              : trav_step_layout<false, ISECT, COUNT, WIDE>(ts, s, stack, w, a.err, &cnt);
             if (r != STEP_CONTINUE) {
-                if (finish_ray<ISECT>(a, ts, &a.tab->scenes[sid], s, r, kind, slot, T, travelled, crossings)) has = false;
+                const mc_triangle_cold* cold = a.cold0;
+                const mc_sphere* spheres = a.spheres0;
+                if (BATCH && MEDIUM && kind == RAY_SHADOW_MEDIUM) {
+                    cold = a.tab->scenes[sid].cold;
+                    spheres = a.tab->scenes[sid].spheres;
+                }
+                if (finish_ray<ISECT>(a, ts, cold, spheres, s, r, kind, slot, T, travelled, crossings)) has = false;
             }
         }
     }
@@ -694,28 +713,31 @@ int occupancy_blocks(const void* fn, int sms) {
 
 typedef void (*TraceKernel)(TraceArgs);
 
-// [wide][count][medium][isect]
-#define MC_TK(W)                                                                                                      \
-    {{{k_trace<0, false, false, W>, k_trace<1, false, false, W>}, {k_trace<0, true, false, W>, k_trace<1, true, false, W>}}, \
-     {{k_trace<0, false, true, W>, k_trace<1, false, true, W>}, {k_trace<0, true, true, W>, k_trace<1, true, true, W>}}}
-TraceKernel trace_kernel(bool wide, bool count, bool medium, int isect) {
-    static const TraceKernel table[2][2][2][2] = {MC_TK(false), MC_TK(true)};
-    return table[wide ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
+// [batch][wide][count][medium][isect]
+#define MC_TK(W, B)                                                                                                           \
+    {{{k_trace<0, false, false, W, B>, k_trace<1, false, false, W, B>}, {k_trace<0, true, false, W, B>, k_trace<1, true, false, W, B>}}, \
+     {{k_trace<0, false, true, W, B>, k_trace<1, false, true, W, B>}, {k_trace<0, true, true, W, B>, k_trace<1, true, true, W, B>}}}
+TraceKernel trace_kernel(bool batch, bool wide, bool count, bool medium, int isect) {
+    static const TraceKernel table[2][2][2][2][2] = {{MC_TK(false, false), MC_TK(true, false)},
+                                                     {MC_TK(false, true), MC_TK(true, true)}};
+    return table[batch ? 1 : 0][wide ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
 }
 
 // Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
 // pull rays from the work counter. Plain (PT:3376-3397): the same kernel with
 // one ray per thread and no refill, over plainBlocks blocks; sharing the kernel
-// keeps the per-ray arithmetic identical between the two modes.
+// keeps the per-ray arithmetic identical between the two modes. A launch is a
+// batch launch when it carries a per-path scene map.
 void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, bool wide, bool medium, int isect,
                   bool persistent, int plainBlocks, bool count = false) {
-    static int occ[32] = {0};
+    static int occ[64] = {0};
     TraceArgs t = t0;
     t.oneShot = persistent ? 0 : 1;
-    TraceKernel fn = trace_kernel(wide, count, medium, isect);
+    const bool batch = t.sceneOf != nullptr;
+    TraceKernel fn = trace_kernel(batch, wide, count, medium, isect);
     int blocks = std::max(1, plainBlocks);
     if (persistent) {
-        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0);
+        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0) + (batch ? 16 : 0);
         if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count);
         blocks = occ[key];
     }
@@ -761,7 +783,7 @@ mc_status ensure_wave(mc_context* ctx, int capacity) {
     if (ctx->graph_exec) {
         cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
         ctx->graph_exec = nullptr;
-        ctx->graph_key = 0;
+        std::memset(ctx->graph_key, 0, sizeof(ctx->graph_key));
     }
     return MC_OK;
 }
@@ -781,7 +803,7 @@ static mc_status ensure_tables(mc_context* ctx, int capacity) {
         if (ctx->graph_exec) {
             cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
             ctx->graph_exec = nullptr;
-            ctx->graph_key = 0;
+            std::memset(ctx->graph_key, 0, sizeof(ctx->graph_key));
         }
     }
     return MC_OK;
@@ -858,6 +880,17 @@ static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* bvh, const WaveItem& it
     return g;
 }
 
+// The scene of a single-scene trace launch, passed as kernel parameters.
+static void set_single_scene(TraceArgs& t, const mc_bvh* bvh, int root, const mc_scene_view* v) {
+    const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
+    t.ts0.nodes = (const float4*)(wide ? bvh->wide_nodes : bvh->nodes);
+    t.ts0.prims = (const float4*)(wide ? bvh->wide_prims : bvh->prims);
+    t.ts0.root = root;
+    t.medium0 = v->has_medium;
+    t.cold0 = v->tri_cold;
+    t.spheres0 = v->spheres;
+}
+
 // Runs waves until every item has rendered its spp samples. All items share
 // the launch configuration of items[0] (layout, persistence, RNG, intersector).
 mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph, bool timed,
@@ -927,6 +960,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.err = ctx->d_error;
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
+    if (n == 1) set_single_scene(ta, bvh, items[0].root, items[0].view);
 
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
@@ -982,16 +1016,30 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
 
     cudaGraphExec_t exec = nullptr;
     if (useGraph) {
-        unsigned long long key = ((unsigned long long)(uintptr_t)bvh->nodes) ^ ((unsigned long long)capacity << 20) ^
-                                 ((unsigned long long)maxD << 1) ^ (wide ? 0x100000000ull : 0) ^ (medium ? 0x200000000ull : 0) ^
-                                 (philox ? 0x400000000ull : 0) ^ ((unsigned long long)isect << 35) ^
-                                 (persistent ? 0x1000000000ull : 0) ^ ((unsigned long long)ta.refill << 40) ^
-                                 ((unsigned long long)(n > 1) << 50) ^ ((unsigned long long)(uintptr_t)stream << 8);
-        if (ctx->graph_exec && ctx->graph_key == key) {
+        // the captured launches bake in these values; any change needs a new capture
+        unsigned long long key[16] = {(unsigned long long)(uintptr_t)stream,
+                                      (unsigned long long)capacity,
+                                      (unsigned long long)maxD,
+                                      (unsigned long long)((wide ? 1 : 0) | (medium ? 2 : 0) | (philox ? 4 : 0) |
+                                                           (persistent ? 8 : 0) | (n > 1 ? 16 : 0)),
+                                      (unsigned long long)isect,
+                                      (unsigned long long)ta.refill,
+                                      (unsigned long long)(uintptr_t)ta.ts0.nodes,
+                                      (unsigned long long)(uintptr_t)ta.ts0.prims,
+                                      (unsigned long long)ta.ts0.root,
+                                      (unsigned long long)ta.medium0,
+                                      (unsigned long long)(uintptr_t)ta.cold0,
+                                      (unsigned long long)(uintptr_t)ta.spheres0,
+                                      (unsigned long long)(uintptr_t)w.block.ptr,
+                                      (unsigned long long)(uintptr_t)sceneOf,
+                                      (unsigned long long)(uintptr_t)dtab,
+                                      1ull};
+        if (ctx->graph_exec && std::memcmp(ctx->graph_key, key, sizeof(key)) == 0) {
             exec = (cudaGraphExec_t)ctx->graph_exec;
         } else {
             if (ctx->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
             ctx->graph_exec = nullptr;
+            std::memset(ctx->graph_key, 0, sizeof(ctx->graph_key));
             cudaGraph_t graph;
             MC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             mc_status cs = enqueue_wave();
@@ -1002,7 +1050,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             cudaGraphDestroy(graph);
             if (ce != cudaSuccess) return cuda_error((int)ce, "cudaGraphInstantiate", __FILE__, __LINE__);
             ctx->graph_exec = exec;
-            ctx->graph_key = key;
+            std::memcpy(ctx->graph_key, key, sizeof(key));
         }
         launches = 0;
     }
@@ -1115,22 +1163,9 @@ mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items
     return finish_stats(ctx, tm, paths, stats);
 }
 
-// A one-scene wave table for the ray-set entry points.
-static mc_status ray_set_table(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene) {
-    mc_status st;
-    if ((st = ensure_tables(ctx, 1)) != MC_OK) return st;
-    int slot;
-    WaveTable* h = next_host_table(ctx, &slot);
-    mc_render_params p;
-    std::memset(&p, 0, sizeof(p));
-    p.width = p.height = 1;
-    WaveItem it{scene, &p, nullptr, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
-    h->nScenes = 1;
-    h->totalPaths = 0;
-    h->scenes[0] = scene_gpu(ctx, bvh, it, 0, 0);
-    MC_CUDA(cudaMemcpyAsync(ctx->d_table, h, offsetof(WaveTable, scenes) + sizeof(SceneGPU), cudaMemcpyHostToDevice, ctx->stream));
-    MC_CUDA(cudaEventRecord((cudaEvent_t)ctx->table_events[slot], ctx->stream));
-    return MC_OK;
+// The single-scene trace arguments of the ray-set entry points.
+static void ray_set_scene(TraceArgs& t, const mc_bvh* bvh, const mc_scene_view* scene) {
+    set_single_scene(t, bvh, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], scene);
 }
 
 }  // namespace mc
@@ -1193,13 +1228,12 @@ mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     if (n == 0) return MC_OK;
     mc_status st;
     if ((st = mc::devbuf_reserve(ctx->scratch[5], 64)) != MC_OK) return st;
-    if ((st = mc::ray_set_table(ctx, bvh, scene)) != MC_OK) return st;
     int* work = (int*)ctx->scratch[5].ptr;
     MC_CUDA(cudaMemsetAsync(work, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
     mc::TraceArgs t;
     std::memset(&t, 0, sizeof(t));
-    t.tab = (const mc::WaveTable*)ctx->d_table;
+    mc::ray_set_scene(t, bvh, scene);
     t.err = ctx->d_error;
     t.refill = 8;
     size_t N = (size_t)n;
@@ -1226,13 +1260,12 @@ mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* 
     if (n == 0) return MC_OK;
     mc_status st;
     if ((st = mc::devbuf_reserve(ctx->scratch[5], 64)) != MC_OK) return st;
-    if ((st = mc::ray_set_table(ctx, bvh, scene)) != MC_OK) return st;
     int* work = (int*)ctx->scratch[5].ptr;
     MC_CUDA(cudaMemsetAsync(work, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
     mc::TraceArgs t;
     std::memset(&t, 0, sizeof(t));
-    t.tab = (const mc::WaveTable*)ctx->d_table;
+    mc::ray_set_scene(t, bvh, scene);
     t.err = ctx->d_error;
     t.refill = 8;
     size_t N = (size_t)n;
