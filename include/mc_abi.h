@@ -364,6 +364,42 @@ MC_API mc_status mc_morton_codes(mc_context* ctx, const mc_scene_view* scene, ui
  * 4 passes of 8 bits). Device arrays; in place through context scratch. */
 MC_API mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t* d_values, int32_t n, int32_t key_bits);
 
+/* Largest n that mc_radix_sort_pairs_static accepts. */
+#define MC_SORT_STATIC_MAX_PAIRS (1 << 20)
+
+/* The same stable radix sort as mc_radix_sort_pairs, with the same results,
+ * for callers that must not allocate device memory when they sort. This entry
+ * point has no counterpart in the reference (whose sort is a host std::sort).
+ *
+ * Who needs it: a caller whose device memory is fully handed out ahead of time
+ * (a render server that admits jobs up to a fixed HBM budget has nothing left
+ * to allocate from at request time), a caller whose memory belongs to another
+ * allocator (a caching allocator such as PyTorch's, which a direct cudaMalloc
+ * would bypass and fragment), and a latency-bound loop that cannot take the
+ * device-wide synchronisation cudaFree implies. This call allocates nothing:
+ * no cudaMalloc/cudaFree and no allocating library routine.
+ *
+ * Scratch: a fixed device array inside the library (about 9 MiB: the
+ * alternate key/value arrays for MC_SORT_STATIC_MAX_PAIRS pairs, the digit
+ * histograms, tile counters and look-back status), one per device, reserved
+ * when the library's device code loads. n > MC_SORT_STATIC_MAX_PAIRS returns
+ * MC_ERR_INVALID without touching the arrays; sort larger arrays with
+ * mc_radix_sort_pairs. The histograms, counters and status words are cleared
+ * on ctx's stream by every call.
+ *
+ * Set-up: the first call on a device looks up that device's scratch address
+ * (with the device made current for the look-up) and loads the sort kernels.
+ * If that first call may happen inside a stream capture, make it earlier
+ * instead: a call with n = 0 (keys and values may be NULL) does the set-up
+ * and nothing else.
+ *
+ * Overlapping calls race: every call on one device shares the one scratch
+ * array, so two calls whose work overlaps in time (from two threads, or on two
+ * streams) corrupt each other's results. Issue them one after another, on one
+ * stream or with the earlier one finished. */
+MC_API mc_status mc_radix_sort_pairs_static(mc_context* ctx, uint32_t* d_keys, int32_t* d_values, int32_t n,
+                                            int32_t key_bits);
+
 /* Full build: bounds, Morton codes, sort, Karras hierarchy, refit, layout. */
 MC_API mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const mc_bvh_build_opts* opts, mc_bvh** out);
 /* One build over `count` scenes in a single pass of launches: per-scene bounds

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "mc_internal.h"
@@ -752,6 +753,100 @@ mc_status radix_sort_pairs(mc_context* ctx, uint32_t* keys, int32_t* vals, uint3
     return MC_OK;
 }
 
+}  // namespace mc
+
+// ---------------------------------------------------------------------------
+// Radix sort over a fixed scratch array (no device allocation).
+// Byte layout of the array, every part 256-byte aligned:
+//   [alternate keys: MAX u32][alternate values: MAX i32]
+//   [histograms: 4 x 256 u32][tile counters: 64 i32][status: 4 x tiles x 256 u32]
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kStaticPairs = MC_SORT_STATIC_MAX_PAIRS;
+constexpr size_t kStaticTiles = (kStaticPairs + kTile - 1) / kTile;
+constexpr size_t kStaticValsOff = kStaticPairs * sizeof(uint32_t);
+constexpr size_t kStaticHistOff = kStaticValsOff + kStaticPairs * sizeof(int32_t);
+constexpr size_t kStaticCounterOff = kStaticHistOff + 4 * kRadix * sizeof(uint32_t);
+constexpr size_t kStaticStatusOff = kStaticCounterOff + 64 * sizeof(int);
+constexpr size_t kStaticBytes = kStaticStatusOff + 4 * kStaticTiles * kRadix * sizeof(uint32_t);
+static_assert(kStaticValsOff % 256 == 0 && kStaticHistOff % 256 == 0 && kStaticCounterOff % 256 == 0 &&
+                  kStaticStatusOff % 256 == 0,
+              "scratch parts must stay 256-byte aligned");
+constexpr int kStaticMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_sort_scratch[kStaticBytes];
+
+namespace mc {
+namespace {
+
+std::mutex g_static_mu;
+void* g_static_scratch[kStaticMaxDevices] = {};
+
+// Address of this device's scratch array; looked up once per device with the
+// device current. Also loads the sort kernels, so later calls load nothing.
+mc_status static_sort_scratch(int device, char** out) {
+    if (device < 0 || device >= kStaticMaxDevices) return set_error(MC_ERR_INVALID, "static sort: device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_scratch[device]) {
+        int cur = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e != cudaSuccess) return cuda_error((int)e, "cudaGetDevice", __FILE__, __LINE__);
+        if (cur != device && (e = cudaSetDevice(device)) != cudaSuccess) return cuda_error((int)e, "cudaSetDevice", __FILE__, __LINE__);
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_sort_scratch);
+        cudaFuncAttributes fa;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_radix_histogram);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_radix_scan);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_onesweep);
+        if (cur != device) cudaSetDevice(cur);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_error((int)e, "static sort set-up (cudaGetSymbolAddress)", __FILE__, __LINE__);
+        }
+        if (!p) return set_error(MC_ERR_CUDA, "static sort: null scratch address");
+        g_static_scratch[device] = p;
+    }
+    *out = (char*)g_static_scratch[device];
+    return MC_OK;
+}
+
+}  // namespace
+
+mc_status radix_sort_pairs_static(mc_context* ctx, uint32_t* keys, int32_t* vals, int n, int key_bits) {
+    char* base = nullptr;
+    mc_status st = static_sort_scratch(ctx->device, &base);
+    if (st != MC_OK) return st;
+    if (n <= 1) return MC_OK;
+    const int passes = (key_bits + kRadixBits - 1) / kRadixBits;
+    const long long tiles = (n + kTile - 1) / kTile;
+    uint32_t* altKeys = (uint32_t*)base;
+    int32_t* altVals = (int32_t*)(base + kStaticValsOff);
+    uint32_t* hist = (uint32_t*)(base + kStaticHistOff);
+    int* tileCounters = (int*)(base + kStaticCounterOff);
+    uint32_t* status = (uint32_t*)(base + kStaticStatusOff);
+    // histograms, tile counters and the status words of the used passes start at zero
+    const size_t zeroBytes = (kStaticStatusOff - kStaticHistOff) + (size_t)passes * tiles * kRadix * sizeof(uint32_t);
+    MC_CUDA(cudaMemsetAsync(base + kStaticHistOff, 0, zeroBytes, ctx->stream));
+    int hblocks = std::min(grid_for(n, 256), ctx->sm_count * 4);
+    k_radix_histogram<<<hblocks, 256, 0, ctx->stream>>>(keys, n, passes, hist);
+    k_radix_scan<<<passes, kRadix, 0, ctx->stream>>>(hist, passes);
+    uint32_t* kin = keys; int32_t* vin = vals; uint32_t* kout = altKeys; int32_t* vout = altVals;
+    for (int p = 0; p < passes; p++) {
+        k_onesweep<<<(int)tiles, kSortThreads, 0, ctx->stream>>>(kin, vin, kout, vout, n, p * kRadixBits, hist + p * kRadix,
+                                                                 status + (size_t)p * tiles * kRadix, tileCounters + p,
+                                                                 ctx->d_error);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    if (kin != keys) {
+        MC_CUDA(cudaMemcpyAsync(keys, kin, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+        MC_CUDA(cudaMemcpyAsync(vals, vin, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    MC_CUDA(cudaGetLastError());
+    return MC_OK;
+}
+
 mc_status bvh_depth(mc_bvh* bvh) {
     if (bvh->depth >= 0) return MC_OK;
     if (bvh->n == 1) {
@@ -1079,6 +1174,20 @@ mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t* d_valu
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
     st = mc::radix_sort_pairs(ctx, d_keys, d_values, (uint32_t*)ctx->scratch[2].ptr, (int32_t*)ctx->scratch[3].ptr, n, key_bits);
     if (st != MC_OK) return st;
+    int flags = 0;
+    if ((st = mc::flags_now(ctx, &flags)) != MC_OK) return st;
+    return mc::status_from_device_flags(flags);
+}
+
+mc_status mc_radix_sort_pairs_static(mc_context* ctx, uint32_t* d_keys, int32_t* d_values, int32_t n, int32_t key_bits) {
+    if (!ctx || (n > 0 && (!d_keys || !d_values)) || n < 0) return mc::set_error(MC_ERR_INVALID, "mc_radix_sort_pairs_static: bad argument");
+    if (key_bits < 1 || key_bits > 32) return mc::set_error(MC_ERR_INVALID, "mc_radix_sort_pairs_static: key_bits must be in [1, 32]");
+    if (n > MC_SORT_STATIC_MAX_PAIRS)
+        return mc::set_error(MC_ERR_INVALID, "mc_radix_sort_pairs_static: n = %d exceeds the fixed scratch of %d pairs (use mc_radix_sort_pairs)",
+                             n, MC_SORT_STATIC_MAX_PAIRS);
+    if (n > 1) MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    mc_status st = mc::radix_sort_pairs_static(ctx, d_keys, d_values, n, key_bits);
+    if (st != MC_OK || n <= 1) return st;
     int flags = 0;
     if ((st = mc::flags_now(ctx, &flags)) != MC_OK) return st;
     return mc::status_from_device_flags(flags);

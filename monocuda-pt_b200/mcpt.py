@@ -24,6 +24,7 @@ LAYOUT_BINARY, LAYOUT_WIDE4 = 0, 1
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
 SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64
+SORT_STATIC_MAX_PAIRS = 1 << 20
 
 
 class McError(RuntimeError):
@@ -173,6 +174,7 @@ SIGNATURES = {
     "mc_scene_free": (I32, [C.POINTER(SceneHost)]),
     "mc_morton_codes": (I32, [P, C.POINTER(SceneView), P, C.POINTER(AABB)]),
     "mc_radix_sort_pairs": (I32, [P, P, P, I32, I32]),
+    "mc_radix_sort_pairs_static": (I32, [P, P, P, I32, I32]),
     "mc_bvh_build": (I32, [P, C.POINTER(SceneView), C.POINTER(BvhBuildOpts), C.POINTER(P)]),
     "mc_bvh_build_batch": (I32, [P, P, I32, C.POINTER(BvhBuildOpts), C.POINTER(P)]),
     "mc_render_batch": (I32, [P, P, P, I32, I32, C.POINTER(RenderStats)]),
