@@ -180,6 +180,7 @@ def run_ours(args):
     import torch
 
     import mcpt
+    import sharding
     world, rank, local = dist_init(args)
     dev = "cuda:%d" % local
     torch.cuda.set_device(local)
@@ -193,15 +194,15 @@ def run_ours(args):
     W, H = scene.width, scene.height
     acc = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
     K, Wm = args.steps, args.warmup
-    base = rank * (K + Wm)
+    timed_samples, warm_samples = sharding.sample_ranges(rank, world, K, Wm)
 
     def params(first, instrument=0):
         return mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234,
                                   first_sample=first, instrument=instrument)
 
     st = mcpt.RenderStats()
-    for i in range(Wm):
-        p = params(base + K + i)
+    for s in warm_samples:
+        p = params(s)
         mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
                                                C.byref(st)))
     acc.zero_()
@@ -215,8 +216,8 @@ def run_ours(args):
     rays = ext = shd = 0
     trace_ms = 0.0
     trace_launches = launches = 0
-    for i in range(K):
-        p = params(base + i, instrument=2)
+    for s in timed_samples:
+        p = params(s, instrument=2)
         mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
                                                C.byref(st)))
         ext += st.extend_rays
@@ -224,8 +225,7 @@ def run_ours(args):
         trace_ms += st.trace_ms
         trace_launches += st.trace_launches
         launches += st.kernel_launches
-    if world > 1:
-        torch.distributed.all_reduce(acc)
+    sharding.reduce_accumulation(acc, world)
     e1.record()
     torch.cuda.synchronize()
     if world > 1:
@@ -251,8 +251,8 @@ def run_ours(args):
 
     # untimed instrumented pass over the same samples: node visits and primitive tests
     visits = leaves = 0
-    for i in range(K):
-        p = params(base + i, instrument=1)
+    for s in timed_samples:
+        p = params(s, instrument=1)
         tmp = torch.zeros_like(acc)
         mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), tmp.data_ptr(),
                                                C.byref(st)))
@@ -268,8 +268,8 @@ def run_ours(args):
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record()
     e2e_rays = 0
-    for i in range(e2e_steps):
-        p = params(base + i)
+    for s in timed_samples[:e2e_steps]:
+        p = params(s)
         mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
                                                C.byref(st)))
         e2e_rays += st.extend_rays + st.shadow_rays
@@ -281,7 +281,7 @@ def run_ours(args):
 
     # cold end to end: host triangles in, accumulation buffer out, one C-ABI call
     host_cold = torch.zeros(W * H * 3, dtype=torch.float32, pin_memory=True)
-    pc = params(base)
+    pc = params(timed_samples.start)
     pc.spp = K
     cold_stats = mcpt.RenderStats()
     torch.cuda.synchronize()
