@@ -1,0 +1,237 @@
+// monocuda - command-line driver over the C ABI.
+//
+// Mirrors the reference executable's render flags (parseCommandLine,
+// src/path_tracer.cu:3908-3964): --wavefront, --persistent, --scene NAME,
+// --spp N, plus the settings the reference fixes in main() (resolution
+// PT:4080-4081, max depth PT:4117, seed PT:4297) and this library's own
+// choices (RNG, intersector, CUDA graph). The scenes are the
+// library's seeded generators; the output is the averaged linear radiance as a
+// PFM (tone mapping and PNG stay out of this path).
+//
+// Exit status: 0 on success, 1 on a library error (message on stderr), 2 on a
+// usage error.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mc_abi.h"
+
+namespace {
+
+struct Options {
+    bool wavefront = false;
+    bool persistent = false;
+    std::string scene = "cornell_boxes";
+    int variant = 0;
+    uint64_t sceneSeed = 0;
+    int spp = 0;
+    int width = 0;
+    int height = 0;
+    int maxDepth = 0;
+    uint64_t seed = 1234;
+    int rng = MC_RNG_PHILOX;
+    int intersector = MC_ISECT_REFERENCE;
+    bool graph = false;
+    std::string out;
+    bool stats = false;
+};
+
+const struct {
+    const char* name;
+    int kind;
+} kScenes[] = {{"cornell_boxes", MC_SCENE_CORNELL_BOXES},
+               {"cornell_spheres", MC_SCENE_CORNELL_SPHERES},
+               {"displaced_icospheres", MC_SCENE_DISPLACED_ICOSPHERES},
+               {"guiding_room", MC_SCENE_GUIDING_ROOM},
+               {"batch_member", MC_SCENE_BATCH_MEMBER}};
+
+void usage(FILE* f) {
+    std::fprintf(f,
+                 "usage: monocuda [--wavefront] [--persistent] [--scene NAME] [--spp N]\n"
+                 "                [--width W] [--height H] [--depth D] [--seed S] [--variant V] [--scene-seed S]\n"
+                 "                [--rng philox|xorwow] [--watertight] [--graph]\n"
+                 "                [--out FILE.pfm] [--stats]\n"
+                 "scenes:");
+    for (const auto& s : kScenes) std::fprintf(f, " %s", s.name);
+    std::fprintf(f, "\n");
+}
+
+bool parse(int argc, char** argv, Options& o) {
+    for (int i = 1; i < argc; i++) {
+        const char* a = argv[i];
+        auto next = [&](const char* flag) -> const char* {
+            if (i + 1 >= argc) {
+                std::fprintf(stderr, "%s needs a value\n", flag);
+                return nullptr;
+            }
+            return argv[++i];
+        };
+        const char* v = nullptr;
+        if (!std::strcmp(a, "--wavefront")) o.wavefront = true;
+        else if (!std::strcmp(a, "--persistent")) o.persistent = true;
+        else if (!std::strcmp(a, "--watertight")) o.intersector = MC_ISECT_WATERTIGHT;
+        else if (!std::strcmp(a, "--graph")) o.graph = true;
+        else if (!std::strcmp(a, "--stats")) o.stats = true;
+        else if (!std::strcmp(a, "--help") || !std::strcmp(a, "-h")) {
+            usage(stdout);
+            std::exit(0);
+        } else if (!std::strcmp(a, "--scene")) {
+            if (!(v = next(a))) return false;
+            o.scene = v;
+        } else if (!std::strcmp(a, "--spp")) {
+            if (!(v = next(a))) return false;
+            o.spp = std::atoi(v);
+        } else if (!std::strcmp(a, "--width")) {
+            if (!(v = next(a))) return false;
+            o.width = std::atoi(v);
+        } else if (!std::strcmp(a, "--height")) {
+            if (!(v = next(a))) return false;
+            o.height = std::atoi(v);
+        } else if (!std::strcmp(a, "--depth")) {
+            if (!(v = next(a))) return false;
+            o.maxDepth = std::atoi(v);
+        } else if (!std::strcmp(a, "--seed")) {
+            if (!(v = next(a))) return false;
+            o.seed = std::strtoull(v, nullptr, 10);
+        } else if (!std::strcmp(a, "--scene-seed")) {
+            if (!(v = next(a))) return false;
+            o.sceneSeed = std::strtoull(v, nullptr, 10);
+        } else if (!std::strcmp(a, "--variant")) {
+            if (!(v = next(a))) return false;
+            o.variant = std::atoi(v);
+        } else if (!std::strcmp(a, "--rng")) {
+            if (!(v = next(a))) return false;
+            if (!std::strcmp(v, "philox")) o.rng = MC_RNG_PHILOX;
+            else if (!std::strcmp(v, "xorwow")) o.rng = MC_RNG_XORWOW;
+            else {
+                std::fprintf(stderr, "unknown rng '%s'\n", v);
+                return false;
+            }
+        } else if (!std::strcmp(a, "--out")) {
+            if (!(v = next(a))) return false;
+            o.out = v;
+        } else {
+            std::fprintf(stderr, "unknown argument '%s'\n", a);
+            return false;
+        }
+    }
+    if (o.persistent && !o.wavefront) {
+        // as the reference (PT:4051-4053): --persistent alone is ignored
+        std::printf("--persistent only applies to the wavefront path tracer, ignoring it (add --wavefront)\n");
+        o.persistent = false;
+    }
+    return true;
+}
+
+int fail(const char* what, mc_status s) {
+    std::fprintf(stderr, "%s: %s: %s\n", what, mc_status_string(s), mc_last_error());
+    return 1;
+}
+
+// Little-endian PFM (negative scale), bottom row first as the format wants.
+bool write_pfm(const std::string& path, const std::vector<float>& rgb, int W, int H) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return false;
+    std::fprintf(f, "PF\n%d %d\n-1.0\n", W, H);
+    for (int y = H - 1; y >= 0; y--) std::fwrite(&rgb[(size_t)y * W * 3], sizeof(float), (size_t)W * 3, f);
+    return std::fclose(f) == 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    Options o;
+    if (!parse(argc, argv, o)) {
+        usage(stderr);
+        return 2;
+    }
+    int kind = 0;
+    for (const auto& s : kScenes)
+        if (o.scene == s.name) kind = s.kind;
+    if (!kind) {
+        std::fprintf(stderr, "unknown scene '%s'\n", o.scene.c_str());
+        usage(stderr);
+        return 2;
+    }
+    if (!o.wavefront)
+        std::fprintf(stderr, "note: this library has only the wavefront path; rendering with it (the megakernel is not part of it)\n");
+
+    mc_scene_desc desc = {};
+    desc.kind = kind;
+    desc.variant = o.variant;
+    desc.seed = o.sceneSeed;
+    mc_scene_host scene = {};
+    mc_status st = mc_scene_generate(&desc, &scene);
+    if (st != MC_OK) return fail("mc_scene_generate", st);
+
+    const int W = o.width > 0 ? o.width : scene.width;
+    const int H = o.height > 0 ? o.height : (o.width > 0 ? (int)((long long)scene.height * W / scene.width) : scene.height);
+    mc_camera cam = scene.camera;
+    if (W != scene.width || H != scene.height) {
+        cam.image_width = W;
+        cam.aspect_ratio = (float)W / (float)H;
+        if ((st = mc_camera_initialize(&cam)) != MC_OK) return fail("mc_camera_initialize", st);
+    }
+
+    mc_context* ctx = nullptr;
+    if ((st = mc_context_create(0, &ctx)) != MC_OK) {
+        mc_scene_free(&scene);
+        return fail("mc_context_create", st);
+    }
+    mc_env_map env = {};
+    if (scene.env_rgba && (st = mc_env_create(scene.env_rgba, scene.env_width, scene.env_height, scene.env_intensity, 0.f, &env)) != MC_OK) {
+        mc_context_destroy(ctx);
+        mc_scene_free(&scene);
+        return fail("mc_env_create", st);
+    }
+
+    mc_render_params p = {};
+    p.camera = cam;
+    p.width = W;
+    p.height = H;
+    p.spp = o.spp > 0 ? o.spp : scene.spp;
+    p.max_depth = o.maxDepth > 0 ? o.maxDepth : scene.max_depth;
+    p.persistent = o.persistent ? 1 : 0;
+    p.rng = o.rng;
+    p.seed = o.seed;
+    p.intersector = o.intersector;
+    p.use_graph = o.graph ? 1 : 0;
+    p.refill_threshold = 0;
+
+    std::vector<float> accum((size_t)W * H * 3, 0.f);
+    mc_render_stats stats = {};
+    st = mc_render_host(ctx, scene.triangles, scene.triangle_count, scene.spheres, scene.sphere_count, &env, &p,
+                        accum.data(), &stats);
+    int rc = 0;
+    if (st != MC_OK) {
+        rc = fail("mc_render_host", st);
+    } else {
+        long long rays = stats.extend_rays + stats.shadow_rays;
+        std::printf("%s: %dx%d, %d spp, depth %d, %d triangles, %d spheres\n", o.scene.c_str(), W, H, p.spp, p.max_depth,
+                    scene.triangle_count, scene.sphere_count);
+        std::printf("render %.3f ms, %lld rays, %.1f Mrays/s\n", stats.render_ms, rays,
+                    stats.render_ms > 0 ? rays / (stats.render_ms * 1e3) : 0.0);
+        if (o.stats) {
+            for (int d = 0; d < MC_MAX_DEPTH_STATS && (stats.extend_per_depth[d] || stats.shadow_per_depth[d]); d++)
+                std::printf("  bounce %d: %lld extend, %lld shadow\n", d, (long long)stats.extend_per_depth[d],
+                            (long long)stats.shadow_per_depth[d]);
+        }
+        if (!o.out.empty()) {
+            std::vector<float> avg(accum.size());
+            for (size_t i = 0; i < accum.size(); i++) avg[i] = accum[i] / (float)p.spp;
+            if (!write_pfm(o.out, avg, W, H)) {
+                std::fprintf(stderr, "could not write '%s'\n", o.out.c_str());
+                rc = 1;
+            } else {
+                std::printf("wrote %s\n", o.out.c_str());
+            }
+        }
+    }
+    mc_env_destroy(&env);
+    mc_context_destroy(ctx);
+    mc_scene_free(&scene);
+    return rc;
+}

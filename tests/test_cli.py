@@ -1,0 +1,63 @@
+"""The `monocuda` command-line driver (reference flags over the C ABI)."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import mcpt
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "monocuda-pt_b200", "monocuda")
+
+
+def _run(*args):
+    return subprocess.run([CLI] + list(args), capture_output=True, text=True, timeout=300)
+
+
+def _read_pfm(path):
+    with open(path, "rb") as f:
+        assert f.readline().strip() == b"PF"
+        w, h = map(int, f.readline().split())
+        scale = float(f.readline())
+        data = np.frombuffer(f.read(), dtype="<f4" if scale < 0 else ">f4")
+    return data.reshape(h, w, 3)[::-1]  # PFM stores the bottom row first
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="CLI not built")
+def test_usage_errors_exit_2():
+    r = _run("--bogus")
+    assert r.returncode == 2 and "unknown argument" in r.stderr
+    r = _run("--scene", "no_such_scene")
+    assert r.returncode == 2 and "unknown scene" in r.stderr
+    r = _run("--help")
+    assert r.returncode == 0 and "--persistent" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cli_render_equals_library_call(tmp_path):
+    out = os.path.join(tmp_path, "c.pfm")
+    r = _run("--wavefront", "--persistent", "--scene", "cornell_boxes", "--width", "64", "--spp", "2", "--stats",
+             "--out", out)
+    assert r.returncode == 0, r.stderr
+    assert "Mrays/s" in r.stdout and "bounce 0" in r.stdout
+    img = _read_pfm(out)
+    assert img.shape == (64, 64, 3) and float(img.sum()) > 0
+
+    s = mcpt.generate_scene(mcpt.SCENE_CORNELL_BOXES)
+    cam = mcpt.Camera.from_buffer_copy(bytes(s.camera))
+    cam.image_width = 64
+    cam.aspect_ratio = 1.0
+    mcpt.camera_initialize(cam)
+    p = mcpt.render_params(cam, 64, 64, 2, s.max_depth, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234)
+    ctx = mcpt.Context(0)
+    tris = mcpt.host_triangles(s)
+    acc = np.zeros(64 * 64 * 3, np.float32)
+    env = mcpt.EnvMap()
+    st = mcpt.RenderStats()
+    mcpt.check(ctx.lib.mc_render_host(ctx.handle, C.addressof(tris), len(tris), None, 0, C.byref(env), C.byref(p),
+                                      acc.ctypes.data, C.byref(st)))
+    ctx.close()
+    mcpt.free_scene(s)
+    np.testing.assert_array_equal(img.reshape(-1), acc / np.float32(2))
