@@ -463,6 +463,71 @@ MC_API mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, ui
 MC_API mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
                              mc_render_params* params, int32_t budget_ms);
 
+/* ------------------------------------------------------------------------- */
+/* Learned path guiding. No counterpart in the reference: its shade kernel    */
+/* samples the BSDF only (PT:3645-3690).                                      */
+/*                                                                           */
+/* A small MLP maps an encoded (position, ray direction) to a mixture of 8   */
+/* von Mises-Fisher lobes over the next direction. Input: each of the 6      */
+/* coordinates (position normalized to the guide's box, direction) encoded   */
+/* as sin/cos(pi * 2^f * x), f = 0..11 (144 inputs); three hidden layers of  */
+/* 64 ReLU units; 40 outputs (8 logits, 8 x 3 unnormalized means, 8 log      */
+/* concentrations). BF16 weights and activations, FP32 accumulation on the   */
+/* tensor cores (tcgen05), FP32 master weights updated by Adam.              */
+/* ------------------------------------------------------------------------- */
+#define MC_GUIDE_INPUTS 144
+#define MC_GUIDE_HIDDEN 64
+#define MC_GUIDE_LOBES 8
+#define MC_GUIDE_OUTPUTS 40
+/* Flat FP32 parameter vector: W1[64][144] b1[64] W2[64][64] b2[64] W3[64][64]
+ * b3[64] W4[40][64] b4[40] (W[out][in], row-major). */
+#define MC_GUIDE_PARAM_COUNT 20200
+/* Per query: x, y, z, dx, dy, dz (world position, ray direction). */
+#define MC_GUIDE_QUERY_FLOATS 6
+/* Per training record: position, ray direction at the vertex, the sampled
+ * next direction, and the record's weight (the radiance estimate carried back
+ * through that direction divided by its sampling density, a luminance). */
+#define MC_GUIDE_RECORD_FLOATS 10
+/* Per query output: lobe weights[8] (sum 1), unit means[8][3], kappa[8]. */
+#define MC_GUIDE_MIXTURE_FLOATS 40
+
+typedef struct mc_guide mc_guide;
+
+typedef struct mc_guide_config {
+    mc_aabb bounds;             /* positions are normalized to this box */
+    float learning_rate;        /* Adam; 0 = 1e-3 */
+    float beta1, beta2, epsilon;/* 0 = 0.9, 0.999, 1e-8 */
+    uint64_t seed;              /* weight initialization */
+    int32_t batch_capacity;     /* records per training step in guided renders; 0 = 65536 */
+    float guide_fraction;       /* one-sample MIS mix: probability of sampling the guide; 0 = 0.5 */
+} mc_guide_config;
+
+MC_API mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_guide** out);
+MC_API mc_status mc_guide_destroy(mc_guide* guide);
+/* FP32 master parameters (host arrays of MC_GUIDE_PARAM_COUNT floats). */
+MC_API mc_status mc_guide_get_params(const mc_guide* guide, float* params);
+MC_API mc_status mc_guide_set_params(mc_guide* guide, const float* params);
+/* Mixtures for n queries (device arrays). */
+MC_API mc_status mc_guide_infer(mc_guide* guide, const float* d_queries, int32_t n, float* d_mixtures);
+/* Gradient of sum_i weight_i * -log q(next_i | position_i, direction_i) over
+ * n records, w.r.t. the flat parameters (d_grad: device, PARAM_COUNT floats);
+ * *loss (host, may be NULL) receives the loss. No parameter update. */
+MC_API mc_status mc_guide_gradient(mc_guide* guide, const float* d_records, int32_t n, float* d_grad, double* loss);
+/* One Adam step on n records, with the weights normalized to sum 1. */
+MC_API mc_status mc_guide_train(mc_guide* guide, const float* d_records, int32_t n);
+/* Adam steps taken so far. */
+MC_API int32_t mc_guide_steps(const mc_guide* guide);
+
+/* Guided wavefront render: at diffuse vertices the next direction comes from
+ * the guide with probability guide_fraction and from the cosine BSDF
+ * otherwise, weighted by the mixed density (one-sample MIS, unbiased); NEE's
+ * MIS weights use the same mixed density. With train != 0 every sample's
+ * primary vertices become training records and the guide takes one Adam step
+ * after each sample. Needs the counter-based RNG and a single-scene BVH. */
+MC_API mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
+                                  const mc_render_params* params, mc_guide* guide, int32_t train, float* d_accum,
+                                  mc_render_stats* stats);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

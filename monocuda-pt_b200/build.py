@@ -34,7 +34,7 @@ UNITS = {
     "mc_context.cu": ["-O3"],
     "mc_host.cu": ["-O3"],
     "mc_batch.cu": ["-O3", "--use_fast_math"],
-    "mc_guide.cu": ["-O3", "--use_fast_math"],
+    "mc_guide.cu": ["-O3"],
     "mc_server.cu": ["-O3"],
 }
 HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"]}

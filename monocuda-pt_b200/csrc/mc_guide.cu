@@ -1,0 +1,924 @@
+// mc_guide.cu - the path-guiding MLP on the sm_100a tensor cores.
+//
+// Network: 144 encoded inputs -> 64 -> 64 -> 64 (ReLU) -> 40 outputs (an
+// 8-lobe vMF mixture). Every layer is a tcgen05.mma (kind::f16, BF16 operands
+// from shared memory, FP32 accumulators in tensor memory) over a tile of 128
+// queries, issued by one thread; the 128 threads of the CTA each own one
+// query row for the epilogues (TMEM -> registers -> bias/ReLU -> BF16 ->
+// shared memory as the next layer's operand).
+//
+// Training (one kernel, forward + backward per tile of 128 records):
+//   forward   Z_l = H_{l-1} W_l^T + b_l          (A = activations, B = W_l)
+//   loss      -w log q(next) of the vMF mixture, gradient dY per row (FP32)
+//   backward  dH_{l-1} = dZ_l W_l                (A = dZ_l, B = W_l^T copy)
+//             dW_l += dZ_l^T [H_{l-1} | 1]       (A = dZ_l^T, rows padded to
+//                                                 128; B = H^T plus a row of
+//                                                 ones, so the last column is
+//                                                 the bias gradient)
+// The weight gradients accumulate in tensor memory over all tiles a CTA
+// processes (464 of the 512 columns) and are written once per CTA as FP32
+// partials; the Adam kernel sums the partials in a fixed order
+// (deterministic) and updates FP32 master weights, from which the BF16
+// operand copies are regenerated.
+//
+// Compiled without fast math: the encoding and the loss are compared with an
+// FP64 restatement.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mc_guide.cuh"
+#include "mc_internal.h"
+#include "mc_umma.cuh"
+
+#define MC_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e__ = (call);                                                          \
+        if (e__ != cudaSuccess) return mc::cuda_error((int)e__, #call, __FILE__, __LINE__); \
+    } while (0)
+
+namespace {
+
+using namespace mc::guide;
+using namespace mc::umma;
+typedef __nv_bfloat16 bf16;
+
+constexpr int kTile = 128;
+constexpr long long kWaitLimit = 1ll << 20;
+
+// ---- shared-memory layouts (bytes) ----
+// inference
+constexpr int iW1 = 0;
+constexpr int iW2 = iW1 + kHid * kIn * 2;
+constexpr int iW3 = iW2 + kHid * kHid * 2;
+constexpr int iW4 = iW3 + kHid * kHid * 2;
+constexpr int iE = iW4 + kOutPad * kHid * 2;
+constexpr int iH = iE + kTile * kIn * 2;
+constexpr int iBias = iH + kTile * kHid * 2;
+constexpr int kInferSmem = iBias + (3 * kHid + kOutPad) * 4;
+// training
+constexpr int tW1 = 0;
+constexpr int tW2 = tW1 + kHid * kIn * 2;
+constexpr int tW3 = tW2 + kHid * kHid * 2;
+constexpr int tW4 = tW3 + kHid * kHid * 2;
+constexpr int tW2t = tW4 + kOutPad * kHid * 2;
+constexpr int tW3t = tW2t + kHid * kHid * 2;
+constexpr int tW4t = tW3t + kHid * kHid * 2;
+constexpr int tE = tW4t + kHid * kOutPad * 2;           // X0 (128 x 144) or X0^T + ones row (160 x 128)
+constexpr int tH1 = tE + 160 * kTile * 2;
+constexpr int tH2 = tH1 + kTile * kHid * 2;
+constexpr int tH3 = tH2 + kTile * kHid * 2;
+constexpr int tHt = tH3 + kTile * kHid * 2;             // H^T + ones row (80 x 128)
+constexpr int tD = tHt + 80 * kTile * 2;                // dZ (128 x 64) or dY (128 x 48)
+constexpr int tDt = tD + kTile * kHid * 2;              // dZ^T padded to 128 rows (128 x 128)
+constexpr int tBias = tDt + kTile * kTile * 2;
+constexpr int kTrainSmem = tBias + (3 * kHid + kOutPad) * 4;
+static_assert(kTrainSmem <= 232448, "training tile exceeds the shared memory of one CTA");
+static_assert(kTile * kIn * 2 <= 160 * kTile * 2, "X0 must fit the transposed buffer");
+
+// TMEM columns of the training kernel
+constexpr uint32_t cR = 0, cG1 = 64, cG2 = 224, cG3 = 304, cG4 = 384, kTrainCols = 512;
+constexpr uint32_t kInferCols = 64;
+
+struct GuideInferArgs {
+    const bf16* blob;
+    const float* master;
+    float lox, loy, loz, invx, invy, invz;
+    int n;
+    const int* count;
+    int capacity;
+    const float* queries;                   // API: n x 6
+    const int* queue;                       // render: path per slot
+    const float *ox, *oy, *oz, *dx, *dy, *dz;
+    const mc_packed_hit* hits;
+    float* mix;
+    int* err;
+};
+
+struct GuideTrainArgs {
+    const bf16* blob;
+    const float* master;
+    float lox, loy, loz, invx, invy, invz;
+    const float* records;
+    int n;
+    const int* count;
+    int capacity;
+    const float* scale;
+    float* partials;
+    double* loss;
+    int* err;
+};
+
+__device__ __forceinline__ void sync_operands() {
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+}
+
+// Thread 0 waits for the committed MMAs; every thread learns the outcome.
+__device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t& phase, int* sFlag, int* err) {
+    if (threadIdx.x == 0) {
+        bool ok = mbar_wait(bar, phase, kWaitLimit);
+        *sFlag = ok ? 0 : 1;
+        if (!ok) atomicOr(err, MC_DEVERR_TIMEOUT);
+    }
+    __syncthreads();
+    fence_after_sync();
+    if (*sFlag) return false;
+    phase ^= 1u;
+    return true;
+}
+
+__device__ __forceinline__ void load_kmaj(unsigned char* dst, const bf16* src, int rows, int K) {
+    const int per = K / 8;
+    for (int c = threadIdx.x; c < rows * per; c += blockDim.x) {
+        int r = c / per, k8 = (c % per) * 8;
+        *reinterpret_cast<uint4*>(dst + kmaj_off(r, k8, K)) = *reinterpret_cast<const uint4*>(src + (size_t)r * K + k8);
+    }
+}
+
+__device__ __forceinline__ void load_bias(float* sb, const float* master) {
+    for (int i = threadIdx.x; i < 3 * kHid + kOutPad; i += blockDim.x) {
+        float v = 0.f;
+        if (i < kHid) v = master[oB1 + i];
+        else if (i < 2 * kHid) v = master[oB2 + i - kHid];
+        else if (i < 3 * kHid) v = master[oB3 + i - 2 * kHid];
+        else if (i - 3 * kHid < kOut) v = master[oB4 + i - 3 * kHid];
+        sb[i] = v;
+    }
+}
+
+// TMEM address of column c of this warp's 32-lane slice.
+__device__ __forceinline__ uint32_t tcol(uint32_t base, uint32_t c) {
+    return base + ((uint32_t)(threadIdx.x & ~31) << 16) + c;
+}
+
+// Encodes one query row into the K-major X0 operand.
+__device__ __forceinline__ void encode_row(unsigned char* sE, int row, const float* coord6) {
+#pragma unroll 1
+    for (int ch = 0; ch < kIn / 8; ch++) {
+        float f[8];
+        encode_chunk(coord6, ch, f);
+        *reinterpret_cast<uint4*>(sE + kmaj_off(row, ch * 8, kIn)) = pack8_bf16(f);
+    }
+}
+
+// Hidden-layer epilogue: 64 accumulator columns + bias, ReLU, BF16 row.
+__device__ __forceinline__ void epi_hidden(uint32_t tR, const float* bias, unsigned char* sOut, int row) {
+#pragma unroll 1
+    for (int c = 0; c < kHid; c += 16) {
+        float v[16];
+        tmem_ld16(tcol(tR, c), v);
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = fmaxf(v[j] + bias[c + j], 0.0f);
+        *reinterpret_cast<uint4*>(sOut + kmaj_off(row, c, kHid)) = pack8_bf16(v);
+        *reinterpret_cast<uint4*>(sOut + kmaj_off(row, c + 8, kHid)) = pack8_bf16(v + 8);
+    }
+}
+
+// Raw outputs -> mixture (weights, unit means, kappa).
+__device__ __forceinline__ void raw_to_mixture(const float* y, float* m) {
+    float mx = y[0];
+#pragma unroll
+    for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, y[k]);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) {
+        m[k] = expf(y[k] - mx);
+        s += m[k];
+    }
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) {
+        m[k] = m[k] / s;
+        float a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
+        float len = sqrtf(a * a + b * b + c * c);
+        if (len > 1e-20f) {
+            m[8 + 3 * k] = a / len; m[9 + 3 * k] = b / len; m[10 + 3 * k] = c / len;
+        } else {
+            m[8 + 3 * k] = 0.f; m[9 + 3 * k] = 0.f; m[10 + 3 * k] = 1.f;
+        }
+        m[32 + k] = expf(fminf(fmaxf(y[32 + k], kLogKappaMin), kLogKappaMax));
+    }
+}
+
+// Loss -W log q(w) of one record and its gradient w.r.t. the 40 raw outputs.
+__device__ float loss_grad(const float* y, float wx, float wy, float wz, float W, float* dy) {
+    float mx = y[0];
+    for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, y[k]);
+    float e[kLobes], s = 0.f;
+    for (int k = 0; k < kLobes; k++) {
+        e[k] = expf(y[k] - mx);
+        s += e[k];
+    }
+    float wk[kLobes], vk[kLobes], kap[kLobes], cs[kLobes], len[kLobes], mu[3 * kLobes];
+    bool clamped[kLobes];
+    float q = 0.f;
+    for (int k = 0; k < kLobes; k++) {
+        wk[k] = e[k] / s;
+        float a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
+        float l = sqrtf(a * a + b * b + c * c);
+        if (l > 1e-20f) {
+            mu[3 * k] = a / l; mu[3 * k + 1] = b / l; mu[3 * k + 2] = c / l;
+        } else {
+            mu[3 * k] = 0.f; mu[3 * k + 1] = 0.f; mu[3 * k + 2] = 1.f;
+            l = 0.f;
+        }
+        len[k] = l;
+        float lk = y[32 + k];
+        clamped[k] = lk < kLogKappaMin || lk > kLogKappaMax;
+        kap[k] = expf(fminf(fmaxf(lk, kLogKappaMin), kLogKappaMax));
+        cs[k] = mu[3 * k] * wx + mu[3 * k + 1] * wy + mu[3 * k + 2] * wz;
+        vk[k] = vmf_pdf(kap[k], cs[k]);
+        q += wk[k] * vk[k];
+    }
+    q = fmaxf(q, 1e-30f);
+    for (int k = 0; k < kLobes; k++) {
+        float r = wk[k] * vk[k] / q;
+        dy[k] = -W * (r - wk[k]);
+        float dlogv = 1.0f / kap[k] - 2.0f / expm1f(2.0f * kap[k]) + cs[k] - 1.0f;
+        dy[32 + k] = clamped[k] ? 0.f : -W * r * kap[k] * dlogv;
+        float g = len[k] > 0.f ? -W * r * kap[k] / len[k] : 0.f;
+        dy[8 + 3 * k] = g * (wx - cs[k] * mu[3 * k]);
+        dy[9 + 3 * k] = g * (wy - cs[k] * mu[3 * k + 1]);
+        dy[10 + 3 * k] = g * (wz - cs[k] * mu[3 * k + 2]);
+    }
+    return W != 0.f ? -W * logf(q) : 0.f;
+}
+
+__device__ __forceinline__ void store_bf16(unsigned char* base, uint32_t off, float v) {
+    *reinterpret_cast<bf16*>(base + off) = __float2bfloat16_rn(v);
+}
+
+// ---------------------------------------------------------------------------
+// Inference
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_guide_infer(GuideInferArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tbase;
+    __shared__ int sFlag;
+    const int tid = threadIdx.x, row = tid;
+    if ((tid >> 5) == 0) tmem_alloc(&tbase, kInferCols);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        sFlag = 0;
+    }
+    load_kmaj(sm + iW1, a.blob + bW1, kHid, kIn);
+    load_kmaj(sm + iW2, a.blob + bW2, kHid, kHid);
+    load_kmaj(sm + iW3, a.blob + bW3, kHid, kHid);
+    load_kmaj(sm + iW4, a.blob + bW4, kOutPad, kHid);
+    float* sb = reinterpret_cast<float*>(sm + iBias);
+    load_bias(sb, a.master);
+    sync_operands();
+    const uint32_t R = tbase;
+    const uint32_t s0 = smem_u32(sm);
+    const uint32_t id64 = idesc_bf16(128, kHid), id48 = idesc_bf16(128, kOutPad);
+    const int n = a.count ? min(*a.count, a.capacity) : a.n;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile * kTile < n; tile += gridDim.x) {
+        const int q = tile * kTile + row;
+        const bool valid = q < n;
+        float coord[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int out = -1;
+        if (valid) {
+            float px, py, pz, dx, dy, dz;
+            if (a.queue) {
+                const int p = a.queue[q];
+                const int4 h = reinterpret_cast<const int4*>(a.hits)[p];
+                const float t = h.w ? __int_as_float(h.x) : 0.f;
+                dx = a.dx[p]; dy = a.dy[p]; dz = a.dz[p];
+                px = a.ox[p] + dx * t; py = a.oy[p] + dy * t; pz = a.oz[p] + dz * t;
+                out = p;
+            } else {
+                const float* Q = a.queries + (size_t)q * 6;
+                px = Q[0]; py = Q[1]; pz = Q[2]; dx = Q[3]; dy = Q[4]; dz = Q[5];
+                out = q;
+            }
+            coord[0] = (px - a.lox) * a.invx;
+            coord[1] = (py - a.loy) * a.invy;
+            coord[2] = (pz - a.loz) * a.invz;
+            coord[3] = dx; coord[4] = dy; coord[5] = dz;
+        }
+        encode_row(sm + iE, row, coord);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(R, s0 + iE, s0 + iW1, kIn, id64, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        epi_hidden(R, sb, sm + iH, row);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(R, s0 + iH, s0 + iW2, kHid, id64, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        epi_hidden(R, sb + kHid, sm + iH, row);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(R, s0 + iH, s0 + iW3, kHid, id64, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        epi_hidden(R, sb + 2 * kHid, sm + iH, row);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(R, s0 + iH, s0 + iW4, kHid, id48, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        float y[kOutPad];
+        tmem_ld16(tcol(R, 0), y);
+        tmem_ld16(tcol(R, 16), y + 16);
+        tmem_ld16(tcol(R, 32), y + 32);
+        if (valid) {
+            for (int k = 0; k < kOut; k++) y[k] += sb[3 * kHid + k];
+            float m[kOut];
+            raw_to_mixture(y, m);
+            float4* dst = reinterpret_cast<float4*>(a.mix + (size_t)out * kOut);
+            for (int i = 0; i < kOut / 4; i++) dst[i] = make_float4(m[4 * i], m[4 * i + 1], m[4 * i + 2], m[4 * i + 3]);
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (!ok && tid == 0) mbar_wait(&bar, phase, kWaitLimit);  // let an overdue MMA finish before TMEM goes back
+    __syncthreads();
+    if ((tid >> 5) == 0) tmem_dealloc(tbase, kInferCols);
+}
+
+// ---------------------------------------------------------------------------
+// Training: forward + loss + backward, weight gradients accumulated in TMEM
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tbase;
+    __shared__ int sFlag;
+    const int tid = threadIdx.x, warp = tid >> 5, row = tid;
+    if (warp == 0) tmem_alloc(&tbase, kTrainCols);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        sFlag = 0;
+    }
+    load_kmaj(sm + tW1, a.blob + bW1, kHid, kIn);
+    load_kmaj(sm + tW2, a.blob + bW2, kHid, kHid);
+    load_kmaj(sm + tW3, a.blob + bW3, kHid, kHid);
+    load_kmaj(sm + tW4, a.blob + bW4, kOutPad, kHid);
+    load_kmaj(sm + tW2t, a.blob + bW2t, kHid, kHid);
+    load_kmaj(sm + tW3t, a.blob + bW3t, kHid, kHid);
+    load_kmaj(sm + tW4t, a.blob + bW4t, kHid, kOutPad);
+    float* sb = reinterpret_cast<float*>(sm + tBias);
+    load_bias(sb, a.master);
+    // constant operand rows: the ones row (bias gradient) and zero padding
+    for (int i = tid; i < 16 * kTile; i += blockDim.x) {
+        const int r = i / kTile, c = i % kTile;
+        const float v = r == 0 ? 1.f : 0.f;
+        store_bf16(sm + tE, kmaj_off(kIn + r, c, kTile), v);
+        store_bf16(sm + tHt, kmaj_off(kHid + r, c, kTile), v);
+    }
+    for (int i = tid; i < 64 * kTile; i += blockDim.x) store_bf16(sm + tDt, kmaj_off(64 + i / kTile, i % kTile, kTile), 0.f);
+    sync_operands();
+
+    const uint32_t T = tbase;
+    const uint32_t s0 = smem_u32(sm);
+    const uint32_t id64 = idesc_bf16(128, kHid), id48 = idesc_bf16(128, kOutPad);
+    const uint32_t id80 = idesc_bf16(128, 80), id160 = idesc_bf16(128, 160);
+    const int n = a.count ? min(*a.count, a.capacity) : a.n;
+    const float scale = a.scale ? *a.scale : 1.0f;
+    uint32_t phase = 0;
+    bool ok = true;
+    int done = 0;
+    float lossAcc = 0.f;
+    for (int tile = blockIdx.x; tile * kTile < n; tile += gridDim.x) {
+        const int q = tile * kTile + row;
+        const bool valid = q < n;
+        float rec[MC_GUIDE_RECORD_FLOATS];
+        for (int i = 0; i < MC_GUIDE_RECORD_FLOATS; i++) rec[i] = valid ? a.records[(size_t)q * MC_GUIDE_RECORD_FLOATS + i] : 0.f;
+        float coord[6];
+        coord[0] = (rec[0] - a.lox) * a.invx;
+        coord[1] = (rec[1] - a.loy) * a.invy;
+        coord[2] = (rec[2] - a.loz) * a.invz;
+        coord[3] = rec[3]; coord[4] = rec[4]; coord[5] = rec[5];
+        if (!valid) for (int i = 0; i < 6; i++) coord[i] = 0.f;
+        encode_row(sm + tE, row, coord);
+        sync_operands();
+        // ---- forward ----
+        if (tid == 0) {
+            gemm_k(T + cR, s0 + tE, s0 + tW1, kIn, id64, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        epi_hidden(T + cR, sb, sm + tH1, row);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(T + cR, s0 + tH1, s0 + tW2, kHid, id64, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        epi_hidden(T + cR, sb + kHid, sm + tH2, row);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(T + cR, s0 + tH2, s0 + tW3, kHid, id64, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        epi_hidden(T + cR, sb + 2 * kHid, sm + tH3, row);
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(T + cR, s0 + tH3, s0 + tW4, kHid, id48, 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        // ---- loss and dY ----
+        {
+            float y[kOutPad];
+            tmem_ld16(tcol(T + cR, 0), y);
+            tmem_ld16(tcol(T + cR, 16), y + 16);
+            tmem_ld16(tcol(T + cR, 32), y + 32);
+            for (int k = 0; k < kOut; k++) y[k] += sb[3 * kHid + k];
+            float dy[kOutPad];
+            for (int k = kOut; k < kOutPad; k++) dy[k] = 0.f;
+            const float W = valid ? rec[9] * scale : 0.f;
+            float nx = rec[6], ny = rec[7], nz = rec[8];
+            lossAcc += loss_grad(y, nx, ny, nz, W, dy);
+            for (int c = 0; c < kOutPad; c += 8)
+                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c, kOutPad)) = pack8_bf16(dy + c);
+            for (int o = 0; o < kHid; o++) store_bf16(sm + tDt, kmaj_off(o, row, kTile), o < kOut ? dy[o] : 0.f);
+        }
+        // H3^T
+        for (int c = 0; c < kHid; c += 8) {
+            float h[8];
+            unpack8_bf16(*reinterpret_cast<const uint4*>(sm + tH3 + kmaj_off(row, c, kHid)), h);
+            for (int j = 0; j < 8; j++) store_bf16(sm + tHt, kmaj_off(c + j, row, kTile), h[j]);
+        }
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(T + cR, s0 + tD, s0 + tW4t, kOutPad, id64, 0);            // dH3 = dY W4
+            gemm_k(T + cG4, s0 + tDt, s0 + tHt, kTile, id80, done > 0);      // dW4 | db4
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        // ---- layers 3, 2: dZ = dH * relu'(Z), then the next data / weight gradients ----
+        const int hOff[3] = {tH3, tH2, tH1};
+        const int wtOff[2] = {tW3t, tW2t};
+        const uint32_t gOff[2] = {cG3, cG2};
+        for (int l = 0; l < 2; l++) {
+            for (int c = 0; c < kHid; c += 16) {
+                float v[16], h[16];
+                tmem_ld16(tcol(T + cR, c), v);
+                unpack8_bf16(*reinterpret_cast<const uint4*>(sm + hOff[l] + kmaj_off(row, c, kHid)), h);
+                unpack8_bf16(*reinterpret_cast<const uint4*>(sm + hOff[l] + kmaj_off(row, c + 8, kHid)), h + 8);
+                for (int j = 0; j < 16; j++) v[j] = h[j] > 0.f ? v[j] : 0.f;
+                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c, kHid)) = pack8_bf16(v);
+                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c + 8, kHid)) = pack8_bf16(v + 8);
+                for (int j = 0; j < 16; j++) store_bf16(sm + tDt, kmaj_off(c + j, row, kTile), v[j]);
+            }
+            for (int c = 0; c < kHid; c += 8) {
+                float h[8];
+                unpack8_bf16(*reinterpret_cast<const uint4*>(sm + hOff[l + 1] + kmaj_off(row, c, kHid)), h);
+                for (int j = 0; j < 8; j++) store_bf16(sm + tHt, kmaj_off(c + j, row, kTile), h[j]);
+            }
+            sync_operands();
+            if (tid == 0) {
+                gemm_k(T + cR, s0 + tD, s0 + wtOff[l], kHid, id64, 0);
+                gemm_k(T + gOff[l], s0 + tDt, s0 + tHt, kTile, id80, done > 0);
+                commit(&bar);
+            }
+            if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        }
+        if (!ok) break;
+        // ---- layer 1: dZ1 and dW1 | db1 against X0^T ----
+        for (int c = 0; c < kHid; c += 16) {
+            float v[16], h[16];
+            tmem_ld16(tcol(T + cR, c), v);
+            unpack8_bf16(*reinterpret_cast<const uint4*>(sm + tH1 + kmaj_off(row, c, kHid)), h);
+            unpack8_bf16(*reinterpret_cast<const uint4*>(sm + tH1 + kmaj_off(row, c + 8, kHid)), h + 8);
+            for (int j = 0; j < 16; j++) store_bf16(sm + tDt, kmaj_off(c + j, row, kTile), h[j] > 0.f ? v[j] : 0.f);
+        }
+        __syncthreads();  // every thread is done with the X0 operand layout before it is overwritten
+        for (int ch = 0; ch < kIn / 8; ch++) {
+            float f[8];
+            encode_chunk(coord, ch, f);
+            for (int j = 0; j < 8; j++) store_bf16(sm + tE, kmaj_off(ch * 8 + j, row, kTile), f[j]);
+        }
+        sync_operands();
+        if (tid == 0) {
+            gemm_k(T + cG1, s0 + tDt, s0 + tE, kTile, id160, done > 0);
+            commit(&bar);
+        }
+        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        done++;
+    }
+    // loss
+    for (int off = 16; off > 0; off >>= 1) lossAcc += __shfl_xor_sync(0xffffffffu, lossAcc, off);
+    if ((tid & 31) == 0 && a.loss && lossAcc != 0.f) atomicAdd(a.loss, (double)lossAcc);
+    // per-CTA partial gradients (rows = output units, lanes 0..63)
+    if (warp < 2) {
+        const int o = row;
+        float* P = a.partials + (size_t)blockIdx.x * kParams;
+        const bool have = ok && done > 0;
+        for (int c = 0; c < 160; c += 16) {
+            float v[16];
+            if (have) tmem_ld16(tcol(T + cG1, c), v);
+            for (int j = 0; j < 16; j++) {
+                const int i = c + j;
+                const float g = have ? v[j] : 0.f;
+                if (i < kIn) P[oW1 + o * kIn + i] = g;
+                else if (i == kIn) P[oB1 + o] = g;
+            }
+        }
+        const uint32_t gc[3] = {cG2, cG3, cG4};
+        const int ow[3] = {oW2, oW3, oW4}, ob[3] = {oB2, oB3, oB4};
+        for (int l = 0; l < 3; l++) {
+            const bool rowUsed = l < 2 || o < kOut;
+            for (int c = 0; c < 80; c += 16) {
+                float v[16];
+                if (have) tmem_ld16(tcol(T + gc[l], c), v);
+                if (!rowUsed) continue;
+                for (int j = 0; j < 16; j++) {
+                    const int i = c + j;
+                    const float g = have ? v[j] : 0.f;
+                    if (i < kHid) P[ow[l] + o * kHid + i] = g;
+                    else if (i == kHid) P[ob[l] + o] = g;
+                }
+            }
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (!ok && tid == 0) mbar_wait(&bar, phase, kWaitLimit);
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tbase, kTrainCols);
+}
+
+// ---------------------------------------------------------------------------
+// Parameter maintenance
+// ---------------------------------------------------------------------------
+__global__ void k_guide_prepare(const float* master, bf16* blob) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kBlob; e += gridDim.x * blockDim.x) {
+        float v = 0.f;
+        if (e < bW2) v = master[oW1 + e];
+        else if (e < bW3) v = master[oW2 + (e - bW2)];
+        else if (e < bW4) v = master[oW3 + (e - bW3)];
+        else if (e < bW2t) {
+            int o = (e - bW4) / kHid, i = (e - bW4) % kHid;
+            v = o < kOut ? master[oW4 + o * kHid + i] : 0.f;
+        } else if (e < bW3t) {
+            int i = (e - bW2t) / kHid, o = (e - bW2t) % kHid;
+            v = master[oW2 + o * kHid + i];
+        } else if (e < bW4t) {
+            int i = (e - bW3t) / kHid, o = (e - bW3t) % kHid;
+            v = master[oW3 + o * kHid + i];
+        } else {
+            int i = (e - bW4t) / kOutPad, o = (e - bW4t) % kOutPad;
+            v = o < kOut ? master[oW4 + o * kHid + i] : 0.f;
+        }
+        blob[e] = __float2bfloat16_rn(v);
+    }
+}
+
+__global__ void k_guide_reduce(const float* partials, int parts, float* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int c = 0; c < parts; c++) s += partials[(size_t)c * kParams + i];
+        out[i] = s;
+    }
+}
+
+__global__ void k_guide_adam(float* master, float* m, float* v, const float* partials, int parts, float lr, float b1,
+                             float b2, float eps, float c1, float c2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        float g = 0.f;
+        for (int c = 0; c < parts; c++) g += partials[(size_t)c * kParams + i];
+        float mi = b1 * m[i] + (1.f - b1) * g;
+        float vi = b2 * v[i] + (1.f - b2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        master[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// 1 / (sum of the records' weights), or 0 when the sum is not positive.
+__global__ void k_guide_weight_scale(const float* records, int n, const int* count, int capacity, float* scale) {
+    __shared__ float part[32];
+    const int cnt = count ? min(*count, capacity) : n;
+    float s = 0.f;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) s += records[(size_t)i * MC_GUIDE_RECORD_FLOATS + 9];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (int)(blockDim.x >> 5) ? part[threadIdx.x] : 0.f;
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (threadIdx.x == 0) *scale = s > 0.f ? 1.0f / s : 0.f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct SplitMix {
+    uint64_t s;
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+// He-uniform weights (bound sqrt(6 / fan_in)), the output layer scaled by 0.1,
+// zero biases (kappa starts at 1).
+void init_params(std::vector<float>& p, uint64_t seed) {
+    SplitMix r{seed ^ 0x6A09E667F3BCC909ull};
+    p.assign(kParams, 0.f);
+    auto fill = [&](int off, int out, int in, double gain) {
+        double b = std::sqrt(6.0 / in) * gain;
+        for (int i = 0; i < out * in; i++) p[off + i] = (float)((2.0 * r.uniform() - 1.0) * b);
+    };
+    fill(oW1, kHid, kIn, 1.0);
+    fill(oW2, kHid, kHid, 1.0);
+    fill(oW3, kHid, kHid, 1.0);
+    fill(oW4, kOut, kHid, 0.1);
+}
+
+bool g_attr_done = false;
+
+mc_status set_attrs() {
+    if (g_attr_done) return MC_OK;
+    MC_CUDA(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
+    MC_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
+    g_attr_done = true;
+    return MC_OK;
+}
+
+void box(const mc_guide* g, float* lo, float* inv) {
+    const mc_aabb& b = g->cfg.bounds;
+    const float l[3] = {b.lo.x, b.lo.y, b.lo.z}, h[3] = {b.hi.x, b.hi.y, b.hi.z};
+    for (int i = 0; i < 3; i++) {
+        lo[i] = l[i];
+        float ext = h[i] - l[i];
+        inv[i] = ext > 0.f ? 1.0f / ext : 1.0f;
+    }
+}
+
+mc_status prepare(mc_guide* g, cudaStream_t s) {
+    k_guide_prepare<<<64, 256, 0, s>>>(g->master, (bf16*)g->blob);
+    MC_CUDA(cudaGetLastError());
+    return MC_OK;
+}
+
+template <class Args>
+void fill_box(const mc_guide* g, Args& a) {
+    float lo[3], inv[3];
+    box(g, lo, inv);
+    a.lox = lo[0]; a.loy = lo[1]; a.loz = lo[2];
+    a.invx = inv[0]; a.invy = inv[1]; a.invz = inv[2];
+}
+
+mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n, const int* count, int capacity,
+                       const float* scale, int* gridOut) {
+    mc_status st = set_attrs();
+    if (st != MC_OK) return st;
+    GuideTrainArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.blob = (const bf16*)g->blob;
+    a.master = g->master;
+    fill_box(g, a);
+    a.records = records;
+    a.n = n;
+    a.count = count;
+    a.capacity = capacity;
+    a.scale = scale;
+    a.partials = g->partials;
+    a.loss = g->loss;
+    a.err = g->ctx->d_error;
+    const int sms = g->ctx->sm_count;
+    int grid = count ? sms : std::max(1, std::min(sms, (n + kTile - 1) / kTile));
+    k_guide_train<<<grid, kTile, kTrainSmem, s>>>(a);
+    MC_CUDA(cudaGetLastError());
+    *gridOut = grid;
+    return MC_OK;
+}
+
+mc_status adam_step(mc_guide* g, cudaStream_t s, int parts) {
+    const int t = g->steps + 1;
+    const float b1 = g->cfg.beta1, b2 = g->cfg.beta2;
+    const float c1 = (float)(1.0 - std::pow((double)b1, t)), c2 = (float)(1.0 - std::pow((double)b2, t));
+    k_guide_adam<<<80, 256, 0, s>>>(g->master, g->adam_m, g->adam_v, g->partials, parts, g->cfg.learning_rate, b1, b2,
+                                    g->cfg.epsilon, c1, c2);
+    MC_CUDA(cudaGetLastError());
+    g->steps = t;
+    return prepare(g, s);
+}
+
+mc_status flags_of(mc_context* ctx) {
+    int flags = 0;
+    MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return mc::status_from_device_flags(flags);
+}
+
+}  // namespace
+
+namespace mc {
+
+mc_status guide_reserve_paths(mc_guide* g, int paths) {
+    if (g->mixture_capacity >= paths) return MC_OK;
+    cudaFree(g->mixtures);
+    cudaFree(g->records);
+    cudaFree(g->nee0);
+    g->mixtures = g->records = g->nee0 = nullptr;
+    g->mixture_capacity = g->record_capacity = 0;
+    if (cudaMalloc(&g->mixtures, (size_t)paths * kOut * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&g->records, (size_t)paths * 12 * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&g->nee0, (size_t)paths * 3 * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MC_ERR_OOM, "guide: allocation of per-path buffers failed");
+    }
+    g->mixture_capacity = g->record_capacity = paths;
+    return MC_OK;
+}
+
+mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
+                            const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
+                            const float* dz, const mc_packed_hit* hits, float* mixtures) {
+    mc_status st = set_attrs();
+    if (st != MC_OK) return st;
+    GuideInferArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.blob = (const bf16*)g->blob;
+    a.master = g->master;
+    fill_box(g, a);
+    a.count = count;
+    a.capacity = capacity;
+    a.queue = queue;
+    a.ox = ox; a.oy = oy; a.oz = oz; a.dx = dx; a.dy = dy; a.dz = dz;
+    a.hits = hits;
+    a.mix = mixtures;
+    a.err = g->ctx->d_error;
+    k_guide_infer<<<2 * g->ctx->sm_count, kTile, kInferSmem, s>>>(a);
+    MC_CUDA(cudaGetLastError());
+    return MC_OK;
+}
+
+mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity) {
+    k_guide_weight_scale<<<1, 1024, 0, s>>>(records, 0, count, capacity, g->scale);
+    MC_CUDA(cudaGetLastError());
+    int grid = 0;
+    mc_status st = launch_train(g, s, records, 0, count, capacity, g->scale, &grid);
+    if (st != MC_OK) return st;
+    return adam_step(g, s, grid);
+}
+
+}  // namespace mc
+
+extern "C" {
+
+mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_guide** out) {
+    if (!ctx || !config || !out) return mc::set_error(MC_ERR_INVALID, "mc_guide_create: null argument");
+    *out = nullptr;
+    mc_guide* g = new mc_guide();
+    g->ctx = ctx;
+    g->cfg = *config;
+    if (g->cfg.learning_rate <= 0.f) g->cfg.learning_rate = 1e-3f;
+    if (g->cfg.beta1 <= 0.f) g->cfg.beta1 = 0.9f;
+    if (g->cfg.beta2 <= 0.f) g->cfg.beta2 = 0.999f;
+    if (g->cfg.epsilon <= 0.f) g->cfg.epsilon = 1e-8f;
+    if (g->cfg.batch_capacity <= 0) g->cfg.batch_capacity = 65536;
+    if (!(g->cfg.guide_fraction > 0.f && g->cfg.guide_fraction < 1.f)) g->cfg.guide_fraction = 0.5f;
+    const size_t P = (size_t)kParams * sizeof(float);
+    bool okAlloc = cudaMalloc(&g->master, P) == cudaSuccess && cudaMalloc(&g->adam_m, P) == cudaSuccess &&
+                   cudaMalloc(&g->adam_v, P) == cudaSuccess && cudaMalloc(&g->blob, (size_t)kBlob * 2) == cudaSuccess &&
+                   cudaMalloc(&g->partials, (size_t)ctx->sm_count * P) == cudaSuccess &&
+                   cudaMalloc(&g->scale, sizeof(float)) == cudaSuccess && cudaMalloc(&g->loss, sizeof(double)) == cudaSuccess &&
+                   cudaMalloc(&g->batch, (size_t)g->cfg.batch_capacity * MC_GUIDE_RECORD_FLOATS * sizeof(float)) == cudaSuccess &&
+                   cudaMalloc(&g->batch_count, sizeof(int)) == cudaSuccess;
+    if (!okAlloc) {
+        cudaGetLastError();
+        mc_guide_destroy(g);
+        return mc::set_error(MC_ERR_OOM, "mc_guide_create: device allocation failed");
+    }
+    std::vector<float> p;
+    init_params(p, g->cfg.seed);
+    cudaMemcpy(g->master, p.data(), P, cudaMemcpyHostToDevice);
+    cudaMemset(g->adam_m, 0, P);
+    cudaMemset(g->adam_v, 0, P);
+    mc_status st = prepare(g, ctx->stream);
+    if (st == MC_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = mc::cuda_error((int)e, "mc_guide_create", __FILE__, __LINE__);
+    }
+    if (st != MC_OK) {
+        mc_guide_destroy(g);
+        return st;
+    }
+    *out = g;
+    return MC_OK;
+}
+
+// Does not touch the guide's context (which may be gone already): cudaFree
+// waits for the device work that uses the buffers.
+mc_status mc_guide_destroy(mc_guide* g) {
+    if (!g) return MC_OK;
+    cudaFree(g->master);
+    cudaFree(g->adam_m);
+    cudaFree(g->adam_v);
+    cudaFree(g->blob);
+    cudaFree(g->partials);
+    cudaFree(g->scale);
+    cudaFree(g->loss);
+    cudaFree(g->batch);
+    cudaFree(g->batch_count);
+    cudaFree(g->records);
+    cudaFree(g->mixtures);
+    cudaFree(g->nee0);
+    delete g;
+    return MC_OK;
+}
+
+mc_status mc_guide_get_params(const mc_guide* g, float* params) {
+    if (!g || !params) return mc::set_error(MC_ERR_INVALID, "mc_guide_get_params: null argument");
+    MC_CUDA(cudaMemcpyAsync(params, g->master, (size_t)kParams * sizeof(float), cudaMemcpyDeviceToHost, g->ctx->stream));
+    MC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return MC_OK;
+}
+
+mc_status mc_guide_set_params(mc_guide* g, const float* params) {
+    if (!g || !params) return mc::set_error(MC_ERR_INVALID, "mc_guide_set_params: null argument");
+    MC_CUDA(cudaMemcpyAsync(g->master, params, (size_t)kParams * sizeof(float), cudaMemcpyHostToDevice, g->ctx->stream));
+    mc_status st = prepare(g, g->ctx->stream);
+    if (st != MC_OK) return st;
+    MC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return MC_OK;
+}
+
+mc_status mc_guide_infer(mc_guide* g, const float* d_queries, int32_t n, float* d_mixtures) {
+    if (!g || n < 0 || (n > 0 && (!d_queries || !d_mixtures))) return mc::set_error(MC_ERR_INVALID, "mc_guide_infer: bad argument");
+    if (n == 0) return MC_OK;
+    mc_status st = set_attrs();
+    if (st != MC_OK) return st;
+    mc_context* ctx = g->ctx;
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    GuideInferArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.blob = (const bf16*)g->blob;
+    a.master = g->master;
+    fill_box(g, a);
+    a.n = n;
+    a.queries = d_queries;
+    a.mix = d_mixtures;
+    a.err = ctx->d_error;
+    int tiles = (n + kTile - 1) / kTile;
+    k_guide_infer<<<std::min(tiles, 2 * ctx->sm_count), kTile, kInferSmem, ctx->stream>>>(a);
+    MC_CUDA(cudaGetLastError());
+    return flags_of(ctx);
+}
+
+mc_status mc_guide_gradient(mc_guide* g, const float* d_records, int32_t n, float* d_grad, double* loss) {
+    if (!g || n < 0 || !d_grad || (n > 0 && !d_records)) return mc::set_error(MC_ERR_INVALID, "mc_guide_gradient: bad argument");
+    mc_context* ctx = g->ctx;
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    MC_CUDA(cudaMemsetAsync(g->loss, 0, sizeof(double), ctx->stream));
+    if (n == 0) {
+        MC_CUDA(cudaMemsetAsync(d_grad, 0, (size_t)kParams * sizeof(float), ctx->stream));
+        if (loss) *loss = 0.0;
+        return flags_of(ctx);
+    }
+    int grid = 0;
+    mc_status st = launch_train(g, ctx->stream, d_records, n, nullptr, 0, nullptr, &grid);
+    if (st != MC_OK) return st;
+    k_guide_reduce<<<80, 256, 0, ctx->stream>>>(g->partials, grid, d_grad);
+    MC_CUDA(cudaGetLastError());
+    double l = 0.0;
+    MC_CUDA(cudaMemcpyAsync(&l, g->loss, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    st = flags_of(ctx);
+    if (loss) *loss = l;
+    return st;
+}
+
+mc_status mc_guide_train(mc_guide* g, const float* d_records, int32_t n) {
+    if (!g || n < 0 || (n > 0 && !d_records)) return mc::set_error(MC_ERR_INVALID, "mc_guide_train: bad argument");
+    if (n == 0) return MC_OK;
+    mc_context* ctx = g->ctx;
+    MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    MC_CUDA(cudaMemsetAsync(g->loss, 0, sizeof(double), ctx->stream));
+    k_guide_weight_scale<<<1, 1024, 0, ctx->stream>>>(d_records, n, nullptr, 0, g->scale);
+    MC_CUDA(cudaGetLastError());
+    int grid = 0;
+    mc_status st = launch_train(g, ctx->stream, d_records, n, nullptr, 0, g->scale, &grid);
+    if (st != MC_OK) return st;
+    if ((st = adam_step(g, ctx->stream, grid)) != MC_OK) return st;
+    return flags_of(ctx);
+}
+
+int32_t mc_guide_steps(const mc_guide* g) { return g ? g->steps : 0; }
+
+}  // extern "C"

@@ -123,7 +123,33 @@ struct mc_bvh {
     mc_aabb bounds;
 };
 
+struct mc_guide {
+    mc_context* ctx = nullptr;
+    mc_guide_config cfg;
+    float* master = nullptr;           // FP32 parameters
+    float* adam_m = nullptr;
+    float* adam_v = nullptr;
+    void* blob = nullptr;              // BF16 weights (forward and transposed copies)
+    float* partials = nullptr;         // per-CTA gradient partials [sm_count][PARAM_COUNT]
+    float* scale = nullptr;            // device: weight normalization of the current step
+    double* loss = nullptr;            // device: loss accumulator
+    float* batch = nullptr;            // training records of guided renders
+    int* batch_count = nullptr;
+    float* records = nullptr;          // per-path primary-vertex records of guided renders
+    int record_capacity = 0;
+    float* mixtures = nullptr;         // per-path mixtures of the current bounce
+    int mixture_capacity = 0;
+    float* nee0 = nullptr;             // per-path NEE of the primary vertex (kept out of the records' weights)
+    int steps = 0;
+};
+
 namespace mc {
 mc_status bvh_depth(mc_bvh* bvh);
 mc_status context_counters(mc_context* ctx);
+// Guide kernels driven by device-side counts (guided renders).
+mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
+                            const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
+                            const float* dz, const mc_packed_hit* hits, float* mixtures);
+mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity);
+mc_status guide_reserve_paths(mc_guide* g, int paths);
 }

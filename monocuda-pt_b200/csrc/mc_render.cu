@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 
+#include "mc_guide.cuh"
 #include "mc_internal.h"
 #include "mc_rng.cuh"
 #include "mc_shade.cuh"
@@ -347,7 +348,16 @@ struct ShadeArgs {
     int* shCount;
     int capacity;
     int* err;
+    // guided shading: per-path mixtures of this bounce, the guide's share of
+    // the one-sample MIS, and the primary-vertex training records
+    const float* mix;
+    float guideFrac;
+    float* rec;
 };
+
+// Per-path training record of the primary vertex: position, ray direction,
+// sampled direction, weight, valid flag, spare.
+constexpr int kRecFloats = 12;
 
 struct ShadeOut {
     bool next;
@@ -396,8 +406,16 @@ MC_D MatView load_material(const mc_material& m) {
     return v;
 }
 
-// PT:3470-3696 shadeKernel for one path.
-template <class Rng>
+// Density of the guided direction sampler at a diffuse vertex: the cosine
+// lobe with probability 1 - frac, the guide's mixture with probability frac.
+MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w) {
+    float c = fmaxf(n.dot(w), 0.0f);
+    return (1.0f - frac) * (c / MC_PI) + frac * guide::mixture_pdf(m, w.x, w.y, w.z);
+}
+
+// PT:3470-3696 shadeKernel for one path. GUIDED: diffuse vertices sample the
+// next direction by one-sample MIS of the cosine lobe and the guide.
+template <class Rng, bool GUIDED>
 MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out) {
     const int depth = a.depth;
     V3 throughput(a.tr[p], a.tg[p], a.tb[p]);
@@ -514,6 +532,8 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         if (cosS > 0.0f && solidPdf > 0.0f) {
             float phasePdf = hg_phase_pdf(inDir.dot(toLight), mat.g);
             float scatterPdf = iso ? phasePdf : lambertian_cosine_pdf(cosS);
+            if (GUIDED && !iso && mat.type == MC_MAT_LAMBERTIAN)
+                scatterPdf = guided_pdf(a.mix + (size_t)p * guide::kOut, a.guideFrac, hitNormal, toLight);
             float scatterValue = iso ? phasePdf : cosS / MC_PI;
             float neeW = power_heuristic(solidPdf, scatterPdf);
             V3 contribution = throughput * lightColor * (scatterValue / solidPdf) * neeW;
@@ -531,9 +551,10 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         if (rng.uniform() > cont) survives = false;
         else throughput = throughput / cont;
     }
+    float guidedPdf = 0.0f;
+    V3 nd;
     if (survives) {
         V3 rayDir(a.dx[p], a.dy[p], a.dz[p]);
-        V3 nd;
         switch (mat.type) {
             case MC_MAT_CONDUCTOR: {
                 V3 refl = specular_scatter(rayDir, hitNormal);
@@ -547,8 +568,38 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             }
             case MC_MAT_ISOTROPIC: nd = hg_scatter(inDir, mat.g, rng); break;
             case MC_MAT_LAMBERTIAN:
-            default: nd = lambertian_scatter(hitNormal, rng); break;
+            default:
+                if (GUIDED) {
+                    const float* m = a.mix + (size_t)p * guide::kOut;
+                    if (rng.uniform() < a.guideFrac) {
+                        float u0 = rng.uniform(), u1 = rng.uniform(), u2 = rng.uniform();
+                        float d3[3];
+                        guide::mixture_sample(m, u0, u1, u2, d3);
+                        nd = V3(d3[0], d3[1], d3[2]);
+                    } else {
+                        nd = lambertian_scatter(hitNormal, rng);
+                    }
+                    const float c = nd.dot(hitNormal);
+                    if (!(c > 0.0f)) {
+                        survives = false;  // below the surface: the BSDF is zero
+                        break;
+                    }
+                    guidedPdf = guided_pdf(m, a.guideFrac, hitNormal, nd);
+                    throughput = throughput * ((c / MC_PI) / guidedPdf);
+                    if (a.rec && depth == 0) {
+                        float* r = a.rec + (size_t)p * kRecFloats;
+                        r[0] = scatterOrigin.x; r[1] = scatterOrigin.y; r[2] = scatterOrigin.z;
+                        r[3] = inDir.x; r[4] = inDir.y; r[5] = inDir.z;
+                        r[6] = nd.x; r[7] = nd.y; r[8] = nd.z;
+                        r[10] = 1.0f;
+                    }
+                } else {
+                    nd = lambertian_scatter(hitNormal, rng);
+                }
+                break;
         }
+    }
+    if (survives) {
         a.ox[p] = scatterOrigin.x;
         a.oy[p] = scatterOrigin.y;
         a.oz[p] = scatterOrigin.z;
@@ -560,7 +611,8 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         a.tb[p] = throughput.z;
         a.spec[p] = (mat.type != MC_MAT_LAMBERTIAN && mat.type != MC_MAT_ISOTROPIC) ? 1 : 0;
         a.pdf[p] = (mat.type == MC_MAT_ISOTROPIC) ? hg_phase_pdf(inDir.dot(nd), mat.g)
-                                                   : lambertian_cosine_pdf(fmaxf(nd.dot(hitNormal), 0.0f));
+                   : (GUIDED && mat.type == MC_MAT_LAMBERTIAN) ? guidedPdf
+                                                               : lambertian_cosine_pdf(fmaxf(nd.dot(hitNormal), 0.0f));
         out.next = depth + 1 < S.maxDepth;  // the scene's max depth ends the path (PT:3793)
     }
     rng_store<Rng>(a, S, p, rng);
@@ -578,7 +630,7 @@ MC_D int warp_reserve(bool want, int* counter, unsigned ltmask) {
     return want ? base + __popc(m & ltmask) : -1;
 }
 
-template <class Rng>
+template <class Rng, bool GUIDED>
 __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
     const unsigned ltmask = lanemask_lt();
     const int count = *a.count;
@@ -591,7 +643,8 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
         if (q < count) {
             p = a.queue[q];
             const SceneGPU& S = a.tab->scenes[scene_of(a.tab, a.sceneOf, p)];
-            shade_path<Rng>(a, S, p, out);
+            if (GUIDED && a.rec && a.depth == 0) a.rec[(size_t)p * kRecFloats + 10] = 0.0f;
+            shade_path<Rng, GUIDED>(a, S, p, out);
         }
         int ns = warp_reserve(out.shadow, a.shCount, ltmask);
         if (out.shadow) {
@@ -689,6 +742,51 @@ __global__ void k_finalize(const WaveTable* tab, const unsigned short* sceneOf, 
         acc[0] = acc[0] + s.x;
         acc[1] = acc[1] + s.y;
         acc[2] = acc[2] + s.z;
+    }
+}
+
+// Guided renders (one scene): the sample plus the primary vertex's NEE goes
+// to the image; a primary-vertex record takes the sample without that NEE
+// (the radiance carried back through its sampled direction over that
+// direction's density) as its weight, and records of positive weight are
+// appended to the training batch.
+__global__ void k_finalize_guided(const WaveTable* tab, const float* sr, const float* sg, const float* sb, const float* nr,
+                                  const float* ng, const float* nb, const float* rec, float* batch, int* batchCount,
+                                  int capacity) {
+    const unsigned ltmask = lanemask_lt();
+    const SceneGPU& S = tab->scenes[0];
+    const int total = tab->totalPaths;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        const int p = base + threadIdx.x;
+        bool emit = false;
+        float w = 0.f;
+        if (p < total) {
+            V3 smp(sr[p], sg[p], sb[p]);
+            V3 s = smp + V3(nr[p], ng[p], nb[p]);
+            float bright = fmaxf(s.x, fmaxf(s.y, s.z));
+            if (!S.disableClamp && bright > 10.0f) s = s * (10.0f / bright);
+            float* acc = S.accum + (size_t)p * 3;
+            acc[0] = acc[0] + s.x;
+            acc[1] = acc[1] + s.y;
+            acc[2] = acc[2] + s.z;
+            if (rec && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
+                w = (smp.x + smp.y + smp.z) * (1.0f / 3.0f);
+                emit = w > 0.0f && w < 1e30f;
+            }
+        }
+        unsigned m = __ballot_sync(kFull, emit);
+        if (m) {
+            int leader = __ffs(m) - 1, slot = 0;
+            if ((int)(threadIdx.x & 31) == leader) slot = atomicAdd(batchCount, __popc(m));
+            slot = __shfl_sync(kFull, slot, leader) + __popc(m & ltmask);
+            if (emit && slot < capacity) {
+                const float* r = rec + (size_t)p * kRecFloats;
+                float* b = batch + (size_t)slot * MC_GUIDE_RECORD_FLOATS;
+                for (int i = 0; i < 9; i++) b[i] = r[i];
+                b[9] = w;
+            }
+        }
     }
 }
 
@@ -894,7 +992,7 @@ static void set_single_scene(TraceArgs& t, const mc_bvh* bvh, int root, const mc
 // Runs waves until every item has rendered its spp samples. All items share
 // the launch configuration of items[0] (layout, persistence, RNG, intersector).
 mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph, bool timed,
-                    RenderTiming* tm) {
+                    RenderTiming* tm, mc_guide* guide = nullptr, bool train = false) {
     const mc_render_params& p0 = *items[0].p;
     const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
     const bool philox = p0.rng == MC_RNG_PHILOX;
@@ -914,15 +1012,17 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     if ((st = ensure_wave(ctx, capacity)) != MC_OK) return st;
     if ((st = ensure_tables(ctx, capacity)) != MC_OK) return st;
     WaveBuffers& w = ctx->wave;
-    if (timeTrace || countVisits) useGraph = false;
+    if (timeTrace || countVisits || guide) useGraph = false;
     cudaStream_t stream = ctx->stream;
     if (useGraph && !stream) {
         if (!ctx->own_stream) MC_CUDA(cudaStreamCreate(&ctx->own_stream));
         stream = ctx->own_stream;
     }
     static int shadeBlocks[2] = {0, 0};
-    if (!shadeBlocks[0]) shadeBlocks[0] = occupancy_blocks((const void*)k_shade<PhiloxRng>, ctx->sm_count);
-    if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng>, ctx->sm_count);
+    if (!shadeBlocks[0]) shadeBlocks[0] = occupancy_blocks((const void*)k_shade<PhiloxRng, false>, ctx->sm_count);
+    if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng, false>, ctx->sm_count);
+    static int guidedBlocks = 0;
+    if (guide && !guidedBlocks) guidedBlocks = occupancy_blocks((const void*)k_shade<PhiloxRng, true>, ctx->sm_count);
     const int plainBlocks = (2 * capacity + 255) / 256;
     const int loopBlocks = ctx->sm_count * 8;
     const WaveTable* dtab = (const WaveTable*)ctx->d_table;
@@ -973,8 +1073,18 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     };
     int launches = 0;
     // the launch sequence of one wave (device table already holds the wave)
+    float* nee0[3] = {nullptr, nullptr, nullptr};
+    if (guide) {
+        nee0[0] = guide->nee0;
+        nee0[1] = guide->nee0 + capacity;
+        nee0[2] = guide->nee0 + 2 * (size_t)capacity;
+    }
     auto enqueue_wave = [&]() -> mc_status {
         MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, stream));
+        if (guide) {
+            MC_CUDA(cudaMemsetAsync(guide->nee0, 0, (size_t)capacity * 3 * sizeof(float), stream));
+            MC_CUDA(cudaMemsetAsync(guide->batch_count, 0, sizeof(int), stream));
+        }
         if (philox) k_camera<PhiloxRng><<<loopBlocks, 256, 0, stream>>>(ca);
         else k_camera<XorwowRng><<<loopBlocks, 256, 0, stream>>>(ca);
         launches++;
@@ -991,11 +1101,22 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             if (d > 0) t.shCount = C + (d - 1) * MC_COUNTERS_PER_DEPTH + 1;
             else { t.shCount = nullptr; t.shN = 0; }
             t.work = C + d * MC_COUNTERS_PER_DEPTH + 2;
+            if (guide && d == 1) {
+                // the primary vertex's NEE lands apart from the sample so that
+                // its training records see only the light through the sampled direction
+                t.sr = nee0[0]; t.sg = nee0[1]; t.sb = nee0[2];
+            }
             if (timeTrace) traceEvent();
             launch_trace(ctx, stream, t, wide, medium, isect, persistent, plainBlocks, countVisits);
             if (timeTrace) traceEvent();
             launches++;
             if (d == maxD) break;
+            if (guide) {
+                mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], C + d * MC_COUNTERS_PER_DEPTH + 0, capacity,
+                                                 w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.hits, guide->mixtures);
+                if (gs != MC_OK) return gs;
+                launches++;
+            }
             ShadeArgs sd = sa;
             sd.depth = d;
             sd.queue = w.queue[d & 1];
@@ -1003,13 +1124,32 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             sd.nextQueue = w.queue[(d + 1) & 1];
             sd.nextCount = C + (d + 1) * MC_COUNTERS_PER_DEPTH + 0;
             sd.shCount = C + d * MC_COUNTERS_PER_DEPTH + 1;
-            if (philox) k_shade<PhiloxRng><<<shadeBlocks[0], 256, 0, stream>>>(sd);
-            else k_shade<XorwowRng><<<shadeBlocks[1], 256, 0, stream>>>(sd);
+            if (guide) {
+                sd.mix = guide->mixtures;
+                sd.guideFrac = guide->cfg.guide_fraction;
+                sd.rec = train ? guide->records : nullptr;
+                k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
+            } else if (philox) {
+                k_shade<PhiloxRng, false><<<shadeBlocks[0], 256, 0, stream>>>(sd);
+            } else {
+                k_shade<XorwowRng, false><<<shadeBlocks[1], 256, 0, stream>>>(sd);
+            }
             launches++;
         }
-        k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb);
+        if (guide) {
+            k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
+                                                              train ? guide->records : nullptr, guide->batch,
+                                                              guide->batch_count, guide->cfg.batch_capacity);
+        } else {
+            k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb);
+        }
         k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
         launches += 2;
+        if (guide && train) {
+            mc_status gs = guide_train_device(guide, stream, guide->batch, guide->batch_count, guide->cfg.batch_capacity);
+            if (gs != MC_OK) return gs;
+            launches += 4;
+        }
         MC_CUDA(cudaGetLastError());
         return MC_OK;
     };
@@ -1152,11 +1292,11 @@ static mc_status finish_stats(mc_context* ctx, const RenderTiming& tm, long long
 }
 
 mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph,
-                       mc_render_stats* stats) {
+                       mc_render_stats* stats, mc_guide* guide = nullptr, bool train = false) {
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long), ctx->stream));
     RenderTiming tm;
-    mc_status st = run_waves(ctx, bvh, items, n, useGraph, stats != nullptr, &tm);
+    mc_status st = run_waves(ctx, bvh, items, n, useGraph, stats != nullptr, &tm, guide, train);
     if (st != MC_OK) return st;
     long long paths = 0;
     for (int i = 0; i < n; i++) paths += (long long)items[i].p->width * items[i].p->height * items[i].p->spp;
@@ -1216,6 +1356,24 @@ mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_ite
     }
     if (capacity >= (1ll << 30)) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: too many paths per wave");
     return mc::render_items(ctx, bvh, its.data(), count, use_graph != 0, stats);
+}
+
+mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const mc_render_params* params,
+                           mc_guide* guide, int32_t train, float* d_accum, mc_render_stats* stats) {
+    if (!ctx || !bvh || !guide) return mc::set_error(MC_ERR_INVALID, "mc_render_guided: null argument");
+    mc_status st = mc::check_params(params, scene);
+    if (st != MC_OK) return st;
+    if (!d_accum) return mc::set_error(MC_ERR_INVALID, "mc_render_guided: null accumulation buffer");
+    if (bvh->nseg != 1) return mc::set_error(MC_ERR_INVALID, "mc_render_guided: needs a single-scene BVH");
+    if (scene->sphere_count + scene->triangle_count != bvh->n) return mc::set_error(MC_ERR_INVALID, "render: the BVH was built for another scene");
+    if (params->rng != MC_RNG_PHILOX) return mc::set_error(MC_ERR_INVALID, "mc_render_guided: guided renders use the counter-based RNG");
+    if (guide->ctx != ctx) return mc::set_error(MC_ERR_INVALID, "mc_render_guided: the guide belongs to another context");
+    const int pixels = params->width * params->height;
+    if (params->queue_capacity > 0 && params->queue_capacity < pixels)
+        return mc::set_error(MC_ERR_INVALID, "mc_render_guided: queue capacity below width*height");
+    if ((st = mc::guide_reserve_paths(guide, pixels)) != MC_OK) return st;
+    mc::WaveItem it{scene, params, d_accum, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
+    return mc::render_items(ctx, bvh, &it, 1, false, stats, guide, train != 0);
 }
 
 mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, const float* d_rays, int32_t n,

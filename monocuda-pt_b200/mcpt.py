@@ -25,6 +25,8 @@ SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDI
 SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64
 SORT_STATIC_MAX_PAIRS = 1 << 20
+GUIDE_PARAM_COUNT = 20200
+GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_OUTPUTS, GUIDE_LOBES = 144, 64, 40, 8
 
 
 class McError(RuntimeError):
@@ -126,6 +128,12 @@ class RenderParams(C.Structure):
                 ("instrument", C.c_int32)]
 
 
+class GuideConfig(C.Structure):
+    _fields_ = [("bounds", AABB), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
+                ("guide_fraction", C.c_float)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("extend_rays", C.c_int64), ("shadow_rays", C.c_int64), ("paths", C.c_int64),
                 ("extend_per_depth", C.c_int64 * MAX_DEPTH_STATS), ("shadow_per_depth", C.c_int64 * MAX_DEPTH_STATS),
@@ -150,7 +158,7 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56}
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
 
@@ -187,6 +195,16 @@ SIGNATURES = {
     "mc_render_host": (I32, [P, P, I32, P, I32, C.POINTER(EnvMap), C.POINTER(RenderParams), P, C.POINTER(RenderStats)]),
     "mc_rng_reset": (I32, [P, I32, I32, C.c_uint64]),
     "mc_autotune": (I32, [P, P, C.POINTER(SceneView), C.POINTER(RenderParams), I32]),
+    "mc_guide_create": (I32, [P, C.POINTER(GuideConfig), C.POINTER(P)]),
+    "mc_guide_destroy": (I32, [P]),
+    "mc_guide_get_params": (I32, [P, P]),
+    "mc_guide_set_params": (I32, [P, P]),
+    "mc_guide_infer": (I32, [P, P, I32, P]),
+    "mc_guide_gradient": (I32, [P, P, I32, P, C.POINTER(C.c_double)]),
+    "mc_guide_train": (I32, [P, P, I32]),
+    "mc_guide_steps": (I32, [P]),
+    "mc_render_guided": (I32, [P, P, C.POINTER(SceneView), C.POINTER(RenderParams), P, I32, P,
+                               C.POINTER(RenderStats)]),
 }
 
 _lib = None
@@ -459,3 +477,58 @@ def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RN
     p.use_graph = 1 if use_graph else 0
     p.instrument = instrument
     return p
+
+
+class Guide:
+    """The path-guiding MLP (mc_guide_*): FP32 master weights on the device,
+    BF16 tensor-core inference and training."""
+
+    def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        cfg = GuideConfig()
+        cfg.bounds.lo = Vec3(*bounds_lo)
+        cfg.bounds.hi = Vec3(*bounds_hi)
+        cfg.learning_rate = learning_rate
+        cfg.seed = seed
+        cfg.batch_capacity = batch_capacity
+        cfg.guide_fraction = guide_fraction
+        self.config = cfg
+        h = P()
+        check(self.lib.mc_guide_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h
+
+    def box(self):
+        """(lo, 1/extent) as the kernels form them (float32)."""
+        import numpy as np
+        lo = np.array([self.config.bounds.lo.x, self.config.bounds.lo.y, self.config.bounds.lo.z], np.float32)
+        hi = np.array([self.config.bounds.hi.x, self.config.bounds.hi.y, self.config.bounds.hi.z], np.float32)
+        ext = hi - lo
+        inv = np.where(ext > 0, np.float32(1.0) / np.where(ext > 0, ext, np.float32(1)), np.float32(1)).astype(np.float32)
+        return lo, inv
+
+    def get_params(self):
+        import numpy as np
+        out = np.zeros(GUIDE_PARAM_COUNT, np.float32)
+        check(self.lib.mc_guide_get_params(self.handle, out.ctypes.data))
+        return out
+
+    def set_params(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == GUIDE_PARAM_COUNT
+        check(self.lib.mc_guide_set_params(self.handle, p.ctypes.data))
+
+    def steps(self):
+        return self.lib.mc_guide_steps(self.handle)
+
+    def close(self):
+        if self.handle:
+            self.lib.mc_guide_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -28,6 +28,8 @@ def oracle():
         lib.orc_scene_destroy.argtypes = [P]
         lib.orc_render.argtypes = [P, P, I, I, I, I, I, C.c_uint64, I, I, I, I, I, I, I, P, P]
         lib.orc_philox4x32_10.argtypes = [P, P, P]
+        lib.orc_guide_forward.argtypes = [P, P, I, P, P, I, P]
+        lib.orc_guide_loss_grad.argtypes = [P, P, I, P, P, I, P, P]
         _orc = lib
     return _orc
 
