@@ -49,9 +49,16 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
                     help="warm-up and timed steps only (for ncu captures); prints the timed line without extras")
-    ap.add_argument("--workload", default="icospheres", choices=["icospheres", "batch"],
-                    help="icospheres: the headline single-scene workload; batch: the 64-scene batched pipeline")
+    ap.add_argument("--workload", default="icospheres", choices=["icospheres", "batch", "guiding", "mlp"],
+                    help="icospheres: the headline single-scene workload; batch: the 64-scene batched pipeline; "
+                         "guiding: guided vs plain time to a fixed RMSE on the aperture room")
     ap.add_argument("--batch-scenes", type=int, default=64)
+    ap.add_argument("--guide-ref-spp", type=int, default=1024)
+    ap.add_argument("--guide-plain-spp", type=int, default=64)
+    ap.add_argument("--guide-chunk", type=int, default=8)
+    ap.add_argument("--guide-lr", type=float, default=1e-3)
+    ap.add_argument("--guide-steps", type=int, default=4, help="Adam steps per sample, each on 65536 records")
+    ap.add_argument("--mlp-items", type=int, default=1 << 20)
     return ap.parse_args()
 
 
@@ -102,13 +109,14 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def peaks():
+def peaks(key="hbm_gbs"):
+    """A measured peak from MEASURED_PEAKS.json (HBM GB/s or bf16 TFLOP/s), else the fallback."""
     try:
         with open(PEAKS_FILE) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+        return float(p[key]), "measured"
     except (OSError, KeyError, ValueError):
-        return 6650.0, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}.get(key, 0.0), "fallback"
 
 
 def traffic_per_launch():
@@ -395,6 +403,169 @@ def run_batch(args):
     print(json.dumps(out), flush=True)
 
 
+def mlp_throughput(ctx, guide, n=1 << 20):
+    """Guide MLP kernels on n queries (inference) and n records (forward +
+    backward + weight gradients), useful tensor-core FLOPs per item (padding
+    excluded) over CUDA-event time."""
+    import torch
+
+    import mcpt
+    q = torch.rand(n, 6, device="cuda")
+    mix = torch.empty(n * 40, device="cuda")
+    recs = torch.rand(n, 10, device="cuda")
+    grad = torch.empty(mcpt.GUIDE_PARAM_COUNT, device="cuda")
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    infer_ms = timed(lambda: mcpt.check(ctx.lib.mc_guide_infer(guide.handle, q.data_ptr(), n, mix.data_ptr())))
+    loss = C.c_double()
+    train_ms = timed(lambda: mcpt.check(ctx.lib.mc_guide_gradient(guide.handle, recs.data_ptr(), n, grad.data_ptr(),
+                                                                   C.byref(loss))))
+    # useful FLOPs (padding excluded): forward, backward data, backward weights
+    fwd_flop = 2 * (144 * 64 + 64 * 64 + 64 * 64 + 64 * 40)
+    bwd_flop = 2 * (40 * 64 + 64 * 64 + 64 * 64) + 2 * (40 * 64 + 64 * 64 + 64 * 64 + 64 * 144)
+    peak, peak_kind = peaks("bf16_tflops")
+    infer_tf = n * fwd_flop / (infer_ms / 1e3) / 1e12
+    train_tf = n * (fwd_flop + bwd_flop) / (train_ms / 1e3) / 1e12
+    return {"items": n, "infer_ms": round(infer_ms, 3), "infer_queries_per_s": round(n / (infer_ms / 1e3)),
+            "infer_tflops": round(infer_tf, 2), "train_ms": round(train_ms, 3),
+            "train_records_per_s": round(n / (train_ms / 1e3)), "train_tflops": round(train_tf, 2),
+            "peak_tflops": peak, "peak_kind": peak_kind, "infer_frac": round(infer_tf / peak, 4) if peak else None,
+            "train_frac": round(train_tf / peak, 4) if peak else None, "flop_per_query": fwd_flop,
+            "flop_per_record": fwd_flop + bwd_flop}
+
+
+def run_mlp(args):
+    """The guide MLP kernels alone (a small, self-contained case for profiling)."""
+    import mcpt
+    ctx = mcpt.Context(0)
+    guide = mcpt.Guide(ctx, [-1.0, -1.0, -1.0], [1.0, 1.0, 1.0], seed=1)
+    out = mlp_throughput(ctx, guide, n=args.mlp_items)
+    out["metric"] = "guide MLP throughput"
+    print(json.dumps(out), flush=True)
+    guide.close()
+
+
+def run_guiding(args):
+    """Time to a fixed RMSE, guided vs plain wavefront, on the aperture room
+    (about 200k triangles, 1024x1024, light only through a 0.2 x 0.2 hole).
+    The target RMSE is plain wavefront's at --guide-plain-spp; the guided
+    renderer starts from an untrained guide, trains online (one Adam step per
+    sample) and counts every sample and every training step in its time. The
+    reference image is a plain render at --guide-ref-spp (its own noise adds
+    the same amount to both MSEs). Firefly clamp off in all three (the clamp
+    biases the estimators differently). Times are CUDA events around the
+    render calls; the RMSE evaluation between chunks is not timed."""
+    import numpy as np
+    import torch
+
+    import mcpt
+    ctx = mcpt.Context(0)
+    s = mcpt.generate_scene(mcpt.SCENE_GUIDING_ROOM)
+    tris = mcpt.host_triangles(s)
+    ds = mcpt.DeviceScene(tris)
+    bvh = mcpt.Bvh(ctx, ds.view, layout=mcpt.LAYOUT_WIDE4)
+    W, H = s.width, s.height
+    raw = np.frombuffer(tris, dtype=np.uint8).reshape(len(tris), 224)
+    verts = raw[:, :36].copy().view(np.float32).reshape(-1, 3)
+    lo, hi = verts.min(0), verts.max(0)
+    chunk = args.guide_chunk
+
+    def params(spp, first):
+        return mcpt.render_params(s.camera, W, H, spp, s.max_depth, persistent=True, rng=mcpt.RNG_PHILOX, seed=4,
+                                  first_sample=first, disable_clamp=True)
+
+    def render(acc, spp, first, guide=None, train=0):
+        st = mcpt.RenderStats()
+        p = params(spp, first)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if guide is None:
+            mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
+                                                   C.byref(st)))
+        else:
+            mcpt.check(ctx.lib.mc_render_guided(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), guide.handle,
+                                                train, acc.data_ptr(), C.byref(st)))
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), st
+
+    # warm-up of both paths (kernels loaded, buffers reserved)
+    tmp = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    render(tmp, 1, 999999)
+    warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1)
+    render(tmp, 1, 999998, warm_guide, 1)
+    warm_guide.close()
+    # reference image
+    ref = torch.zeros_like(tmp)
+    ref_ms = 0.0
+    for c in range(0, args.guide_ref_spp, 64):
+        ms, _ = render(ref, min(64, args.guide_ref_spp - c), 10_000_000 + c)
+        ref_ms += ms
+    ref /= args.guide_ref_spp
+
+    def rmse(acc, spp):
+        return float(torch.sqrt(torch.mean((acc / spp - ref) ** 2)))
+
+    # plain: the target
+    acc = torch.zeros_like(tmp)
+    plain_ms, plain_curve, rays_plain = 0.0, [], 0
+    for c in range(0, args.guide_plain_spp, chunk):
+        ms, st = render(acc, chunk, 20_000_000 + c)
+        plain_ms += ms
+        rays_plain += st.extend_rays + st.shadow_rays
+        plain_curve.append((c + chunk, round(plain_ms, 1), rmse(acc, c + chunk)))
+    target = plain_curve[-1][2]
+    # guided, trained online from scratch
+    guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
+                       train_steps=args.guide_steps)
+    acc = torch.zeros_like(tmp)
+    g_ms, g_curve, reached, rays_g = 0.0, [], None, 0
+    spp = 0
+    while spp < args.guide_plain_spp * 4:
+        ms, st = render(acc, chunk, 30_000_000 + spp, guide, 1)
+        prev_ms, prev_err = g_ms, (g_curve[-1][2] if g_curve else None)
+        g_ms += ms
+        spp += chunk
+        rays_g += st.extend_rays + st.shadow_rays
+        err = rmse(acc, spp)
+        g_curve.append((spp, round(g_ms, 1), err))
+        if err <= target:
+            # interpolate the crossing inside the last chunk (error ~ 1/sqrt(time))
+            if prev_err is not None and prev_err > target:
+                f = (1 / prev_err ** 2 - 1 / target ** 2) / (1 / prev_err ** 2 - 1 / err ** 2)
+                reached = prev_ms + f * (g_ms - prev_ms)
+            else:
+                reached = g_ms
+            break
+    steps = guide.steps()
+
+    mlp = mlp_throughput(ctx, guide)
+    guide.close()
+    ratio = reached / plain_ms if reached is not None else None
+    out = {"metric": "time to fixed RMSE vs plain wavefront", "value": round(ratio, 4) if ratio is not None else None,
+           "unit": "guided time / plain time (lower is better)", "higher_is_better": False, "n_gpus": 1,
+           "workload": "guiding_room", "triangles": int(len(tris)), "width": W, "height": H, "max_depth": s.max_depth,
+           "target_rmse": round(target, 6), "plain_spp": args.guide_plain_spp, "plain_ms": round(plain_ms, 1),
+           "guided_ms_to_target": round(reached, 1) if reached is not None else None,
+           "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
+           "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
+           "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
+           "plain_curve": plain_curve, "guided_curve": g_curve,
+           "mlp": mlp,
+           "data": "synthetic (seeded procedural room)", "dtype": "bf16 MLP / f32 tracer"}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -448,6 +619,10 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "guiding":
+        run_guiding(args)
+    elif args.workload == "mlp":
+        run_mlp(args)
     else:
         run_ours(args)
 

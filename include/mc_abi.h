@@ -500,6 +500,8 @@ typedef struct mc_guide_config {
     uint64_t seed;              /* weight initialization */
     int32_t batch_capacity;     /* records per training step in guided renders; 0 = 65536 */
     float guide_fraction;       /* one-sample MIS mix: probability of sampling the guide; 0 = 0.5 */
+    int32_t train_steps;        /* Adam steps per sample in guided renders, each on its own
+                                   batch_capacity records of that sample; 0 = 1 */
 } mc_guide_config;
 
 MC_API mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_guide** out);
@@ -564,5 +566,7 @@ MC_STATIC_ASSERT(offsetof(mc_bvh_node, is_leaf) == 52, "BVH_Node.isLeaf at 52");
 MC_STATIC_ASSERT(sizeof(mc_packed_hit) == 16, "PackedHit is 16 bytes");
 MC_STATIC_ASSERT(sizeof(mc_camera) == 172, "Camera is 172 bytes");
 MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
+/* this library's own structs (bindings mirror these sizes) */
+MC_STATIC_ASSERT(sizeof(mc_guide_config) == 80, "mc_guide_config is 80 bytes");
 
 #endif /* MC_ABI_H */

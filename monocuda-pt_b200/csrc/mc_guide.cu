@@ -103,10 +103,12 @@ struct GuideTrainArgs {
     const bf16* blob;
     const float* master;
     float lox, loy, loz, invx, invy, invz;
-    const float* records;
+    const float* records;                   // already advanced to this step's slice
     int n;
-    const int* count;
-    int capacity;
+    const int* count;                       // device count of the whole batch (or null: n records)
+    int offset;                             // this step's first record in the batch
+    int capacity;                           // records the batch holds
+    int stepCap;                            // records one step takes
     const float* scale;
     float* partials;
     double* loss;
@@ -389,7 +391,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
     const uint32_t s0 = smem_u32(sm);
     const uint32_t id64 = idesc_bf16(128, kHid), id48 = idesc_bf16(128, kOutPad);
     const uint32_t id80 = idesc_bf16(128, 80), id160 = idesc_bf16(128, 160);
-    const int n = a.count ? min(*a.count, a.capacity) : a.n;
+    const int n = a.count ? max(0, min(min(*a.count, a.capacity) - a.offset, a.stepCap)) : a.n;
     const float scale = a.scale ? *a.scale : 1.0f;
     uint32_t phase = 0;
     bool ok = true;
@@ -605,9 +607,10 @@ __global__ void k_guide_adam(float* master, float* m, float* v, const float* par
 }
 
 // 1 / (sum of the records' weights), or 0 when the sum is not positive.
-__global__ void k_guide_weight_scale(const float* records, int n, const int* count, int capacity, float* scale) {
+__global__ void k_guide_weight_scale(const float* records, int n, const int* count, int offset, int capacity, int stepCap,
+                                     float* scale) {
     __shared__ float part[32];
-    const int cnt = count ? min(*count, capacity) : n;
+    const int cnt = count ? max(0, min(min(*count, capacity) - offset, stepCap)) : n;
     float s = 0.f;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) s += records[(size_t)i * MC_GUIDE_RECORD_FLOATS + 9];
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
@@ -683,8 +686,8 @@ void fill_box(const mc_guide* g, Args& a) {
     a.invx = inv[0]; a.invy = inv[1]; a.invz = inv[2];
 }
 
-mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n, const int* count, int capacity,
-                       const float* scale, int* gridOut) {
+mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n, const int* count, int offset,
+                       int capacity, int stepCap, const float* scale, int* gridOut) {
     mc_status st = set_attrs();
     if (st != MC_OK) return st;
     GuideTrainArgs a;
@@ -695,7 +698,9 @@ mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n,
     a.records = records;
     a.n = n;
     a.count = count;
+    a.offset = offset;
     a.capacity = capacity;
+    a.stepCap = stepCap;
     a.scale = scale;
     a.partials = g->partials;
     a.loss = g->loss;
@@ -770,12 +775,18 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
 }
 
 mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity) {
-    k_guide_weight_scale<<<1, 1024, 0, s>>>(records, 0, count, capacity, g->scale);
-    MC_CUDA(cudaGetLastError());
-    int grid = 0;
-    mc_status st = launch_train(g, s, records, 0, count, capacity, g->scale, &grid);
-    if (st != MC_OK) return st;
-    return adam_step(g, s, grid);
+    const int B = g->cfg.batch_capacity;
+    for (int i = 0; i < g->cfg.train_steps; i++) {
+        const int off = i * B;
+        const float* r = records + (size_t)off * MC_GUIDE_RECORD_FLOATS;
+        k_guide_weight_scale<<<1, 1024, 0, s>>>(r, 0, count, off, capacity, B, g->scale);
+        MC_CUDA(cudaGetLastError());
+        int grid = 0;
+        mc_status st = launch_train(g, s, r, 0, count, off, capacity, B, g->scale, &grid);
+        if (st != MC_OK) return st;
+        if ((st = adam_step(g, s, grid)) != MC_OK) return st;
+    }
+    return MC_OK;
 }
 
 }  // namespace mc
@@ -793,13 +804,15 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     if (g->cfg.beta2 <= 0.f) g->cfg.beta2 = 0.999f;
     if (g->cfg.epsilon <= 0.f) g->cfg.epsilon = 1e-8f;
     if (g->cfg.batch_capacity <= 0) g->cfg.batch_capacity = 65536;
+    if (g->cfg.train_steps <= 0) g->cfg.train_steps = 1;
     if (!(g->cfg.guide_fraction > 0.f && g->cfg.guide_fraction < 1.f)) g->cfg.guide_fraction = 0.5f;
     const size_t P = (size_t)kParams * sizeof(float);
     bool okAlloc = cudaMalloc(&g->master, P) == cudaSuccess && cudaMalloc(&g->adam_m, P) == cudaSuccess &&
                    cudaMalloc(&g->adam_v, P) == cudaSuccess && cudaMalloc(&g->blob, (size_t)kBlob * 2) == cudaSuccess &&
                    cudaMalloc(&g->partials, (size_t)ctx->sm_count * P) == cudaSuccess &&
                    cudaMalloc(&g->scale, sizeof(float)) == cudaSuccess && cudaMalloc(&g->loss, sizeof(double)) == cudaSuccess &&
-                   cudaMalloc(&g->batch, (size_t)g->cfg.batch_capacity * MC_GUIDE_RECORD_FLOATS * sizeof(float)) == cudaSuccess &&
+                   cudaMalloc(&g->batch, (size_t)g->cfg.batch_capacity * g->cfg.train_steps * MC_GUIDE_RECORD_FLOATS *
+                                             sizeof(float)) == cudaSuccess &&
                    cudaMalloc(&g->batch_count, sizeof(int)) == cudaSuccess;
     if (!okAlloc) {
         cudaGetLastError();
@@ -893,7 +906,7 @@ mc_status mc_guide_gradient(mc_guide* g, const float* d_records, int32_t n, floa
         return flags_of(ctx);
     }
     int grid = 0;
-    mc_status st = launch_train(g, ctx->stream, d_records, n, nullptr, 0, nullptr, &grid);
+    mc_status st = launch_train(g, ctx->stream, d_records, n, nullptr, 0, 0, 0, nullptr, &grid);
     if (st != MC_OK) return st;
     k_guide_reduce<<<80, 256, 0, ctx->stream>>>(g->partials, grid, d_grad);
     MC_CUDA(cudaGetLastError());
@@ -910,10 +923,10 @@ mc_status mc_guide_train(mc_guide* g, const float* d_records, int32_t n) {
     mc_context* ctx = g->ctx;
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(g->loss, 0, sizeof(double), ctx->stream));
-    k_guide_weight_scale<<<1, 1024, 0, ctx->stream>>>(d_records, n, nullptr, 0, g->scale);
+    k_guide_weight_scale<<<1, 1024, 0, ctx->stream>>>(d_records, n, nullptr, 0, 0, 0, g->scale);
     MC_CUDA(cudaGetLastError());
     int grid = 0;
-    mc_status st = launch_train(g, ctx->stream, d_records, n, nullptr, 0, g->scale, &grid);
+    mc_status st = launch_train(g, ctx->stream, d_records, n, nullptr, 0, 0, 0, g->scale, &grid);
     if (st != MC_OK) return st;
     if ((st = adam_step(g, ctx->stream, grid)) != MC_OK) return st;
     return flags_of(ctx);

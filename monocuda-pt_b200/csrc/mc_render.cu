@@ -1139,16 +1139,18 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         if (guide) {
             k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
                                                               train ? guide->records : nullptr, guide->batch,
-                                                              guide->batch_count, guide->cfg.batch_capacity);
+                                                              guide->batch_count,
+                                                              guide->cfg.batch_capacity * guide->cfg.train_steps);
         } else {
             k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb);
         }
         k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
         launches += 2;
         if (guide && train) {
-            mc_status gs = guide_train_device(guide, stream, guide->batch, guide->batch_count, guide->cfg.batch_capacity);
+            mc_status gs = guide_train_device(guide, stream, guide->batch, guide->batch_count,
+                                              guide->cfg.batch_capacity * guide->cfg.train_steps);
             if (gs != MC_OK) return gs;
-            launches += 4;
+            launches += 4 * guide->cfg.train_steps;
         }
         MC_CUDA(cudaGetLastError());
         return MC_OK;

@@ -131,7 +131,7 @@ class RenderParams(C.Structure):
 class GuideConfig(C.Structure):
     _fields_ = [("bounds", AABB), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
-                ("guide_fraction", C.c_float)]
+                ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("_pad", C.c_int32 * 3)]
 
 
 class RenderStats(C.Structure):
@@ -158,7 +158,7 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 64}
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 80}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
 
@@ -483,7 +483,8 @@ class Guide:
     """The path-guiding MLP (mc_guide_*): FP32 master weights on the device,
     BF16 tensor-core inference and training."""
 
-    def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5):
+    def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5,
+                 train_steps=1):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = GuideConfig()
@@ -493,6 +494,7 @@ class Guide:
         cfg.seed = seed
         cfg.batch_capacity = batch_capacity
         cfg.guide_fraction = guide_fraction
+        cfg.train_steps = train_steps
         self.config = cfg
         h = P()
         check(self.lib.mc_guide_create(ctx.handle, C.byref(cfg), C.byref(h)))
