@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
                     help="warm-up and timed steps only (for ncu captures); prints the timed line without extras")
-    ap.add_argument("--workload", default="icospheres", choices=["icospheres", "batch", "guiding", "mlp"],
+    ap.add_argument("--workload", default="icospheres", choices=["icospheres", "batch", "guiding", "mlp", "server"],
                     help="icospheres: the headline single-scene workload; batch: the 64-scene batched pipeline; "
                          "guiding: guided vs plain time to a fixed RMSE on the aperture room")
     ap.add_argument("--batch-scenes", type=int, default=64)
@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--guide-lr", type=float, default=1e-3)
     ap.add_argument("--guide-steps", type=int, default=4, help="Adam steps per sample, each on 65536 records")
     ap.add_argument("--mlp-items", type=int, default=1 << 20)
+    ap.add_argument("--server-rates", type=float, nargs="+", default=[1, 4, 16, 64], help="arrival rates (requests/s)")
+    ap.add_argument("--server-requests", type=int, default=24, help="requests per arrival rate")
+    ap.add_argument("--server-sps", type=int, default=4, help="samples per server step")
+    ap.add_argument("--server-wave-paths", type=int, default=0, help="paths per server wave (0 = 4M)")
     return ap.parse_args()
 
 
@@ -566,6 +570,136 @@ def run_guiding(args):
     print(json.dumps(out), flush=True)
 
 
+def run_server(args):
+    """Render server under Poisson load. Scenes: 16 members of the 64-scene
+    batch (seeded, 1k-2M triangles) and a level-7 displaced-icosphere scene
+    (983k triangles), resident with their BVHs. Requests (seed 5): scene
+    uniform, resolution uniform over {256^2, 512^2, 1024^2, 1920x1080}, spp
+    log-uniform in [1, 256], guided for half of them. For each arrival rate
+    the same request trace runs through the server (shared waves, HBM budget
+    150 GB) and through the plain per-request wavefront tracer (one request
+    at a time, arrival order). Latency = completion - scheduled arrival."""
+    import math
+    import random
+
+    import torch
+
+    import mcpt
+    ctx = mcpt.Context(0)
+    scenes = [mcpt.generate_scene(mcpt.SCENE_BATCH_MEMBER, variant=i, seed=3) for i in range(16)]
+    scenes.append(mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=7, seed=2))
+    devs = []
+    for s in scenes:
+        env = mcpt.host_env(s) if s.env_width > 0 else None
+        devs.append(mcpt.DeviceScene(mcpt.host_triangles(s), env_rgba=env, env_intensity=s.env_intensity))
+    srv = mcpt.Server(ctx, samples_per_step=args.server_sps, wave_paths=args.server_wave_paths)
+    sids = [srv.add_scene(d) for d in devs]
+    bvhs = [mcpt.Bvh(ctx, d.view, layout=mcpt.LAYOUT_WIDE4) for d in devs]
+    sizes = [(256, 256), (512, 512), (1024, 1024), (1920, 1080)]
+
+    def trace(rate, n, seed):
+        rnd = random.Random(seed)
+        t, out = 0.0, []
+        for _ in range(n):
+            t += rnd.expovariate(rate)
+            k = rnd.randrange(len(scenes))
+            W, H = sizes[rnd.randrange(len(sizes))]
+            spp = max(1, min(256, int(math.exp(rnd.uniform(0.0, math.log(256.0))))))
+            out.append((t, k, W, H, spp, rnd.random() < 0.5))
+        return out
+
+    def params(k, W, H, spp, first=0):
+        s = scenes[k]
+        cam = mcpt.Camera.from_buffer_copy(bytes(s.camera))
+        cam.image_width = W
+        cam.aspect_ratio = W / float(H)
+        mcpt.camera_initialize(cam)
+        return mcpt.render_params(cam, W, H, spp, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=5, first_sample=first)
+
+    def pct(xs, q):
+        xs = sorted(xs)
+        return xs[min(len(xs) - 1, int(math.ceil(q * len(xs))) - 1)]
+
+    def serve(tr):
+        t0 = srv.now()
+        base_rays = srv.stats().rays
+        pending = list(tr)
+        ids = []
+        while pending or srv.stats().active or srv.stats().pending:
+            now = srv.now() - t0
+            while pending and pending[0][0] <= now:
+                t, k, W, H, spp, guided = pending.pop(0)
+                ids.append((t, srv.submit(sids[k], params(k, W, H, spp), guided=guided)))
+            st = srv.stats()
+            if st.active or st.pending:
+                srv.step()
+                for t, rid in ids:
+                    r = srv.result(rid)
+                    if r.state == mcpt.REQ_DONE:
+                        srv.release(rid)
+            elif pending:
+                time.sleep(max(0.0, min(0.002, pending[0][0] - now)))
+        lat, last = [], 0.0
+        for t, rid in ids:
+            r = srv.result(rid)
+            lat.append(r.done_s - t0 - t)
+            last = max(last, r.done_s - t0)
+        rays = srv.stats().rays - base_rays
+        return lat, rays / last / 1e6
+
+    def baseline(tr):
+        acc = {}
+        t0 = time.perf_counter()
+        lat, rays, last = [], 0, 0.0
+        for t, k, W, H, spp, guided in tr:
+            now = time.perf_counter() - t0
+            if now < t:
+                time.sleep(t - now)
+            a = acc.get((W, H))
+            if a is None:
+                a = acc[(W, H)] = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+            a.zero_()
+            p = params(k, W, H, spp)
+            st = mcpt.RenderStats()
+            mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvhs[k].handle, C.byref(devs[k].view), C.byref(p),
+                                                   a.data_ptr(), C.byref(st)))
+            done = time.perf_counter() - t0
+            lat.append(done - t)
+            rays += st.extend_rays + st.shadow_rays
+            last = done
+        return lat, rays / last / 1e6
+
+    # warm-up: one small request of each scene through both
+    warm = [(0.0, k, 256, 256, 1, k % 2 == 0) for k in range(len(scenes))]
+    serve(warm)
+    baseline([(0.0, k, 256, 256, 1, False) for k in range(len(scenes))])
+    points = []
+    for i, rate in enumerate(args.server_rates):
+        tr = trace(rate, args.server_requests, 5 + i)
+        lat, mr = serve(tr)
+        plain_tr = [(t, k, W, H, spp, False) for t, k, W, H, spp, _ in tr]
+        plat, pmr = serve(plain_tr)
+        blat, bmr = baseline(tr)
+        points.append({"lambda_per_s": rate, "requests": len(tr), "guided_requests": sum(1 for x in tr if x[5]),
+                       "p50_s": round(pct(lat, 0.5), 4), "p99_s": round(pct(lat, 0.99), 4), "mrays": round(mr, 1),
+                       "plain_only_p50_s": round(pct(plat, 0.5), 4), "plain_only_p99_s": round(pct(plat, 0.99), 4),
+                       "plain_only_mrays": round(pmr, 1),
+                       "baseline_p50_s": round(pct(blat, 0.5), 4), "baseline_p99_s": round(pct(blat, 0.99), 4),
+                       "baseline_mrays": round(bmr, 1)})
+    st = srv.stats()
+    out = {"metric": "served-render p50/p99 latency", "unit": "s", "higher_is_better": False, "n_gpus": 1,
+           "workload": "render_server", "scenes": len(scenes),
+           "scene_triangles": [int(s.triangle_count) for s in scenes], "budget_gb": st.budget_bytes / 1e9,
+           "resident_scene_gb": round(st.scene_bytes / 1e9, 3), "samples_per_step": args.server_sps,
+           "wave_paths": args.server_wave_paths or 4194304,
+           "points": points, "data": "synthetic (seeded scenes and request trace)",
+           "baseline": "plain per-request wavefront tracer, one request at a time in arrival order"}
+    print(json.dumps(out), flush=True)
+    srv.close()
+    for s in scenes:
+        mcpt.free_scene(s)
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -623,6 +757,8 @@ def main():
         run_guiding(args)
     elif args.workload == "mlp":
         run_mlp(args)
+    elif args.workload == "server":
+        run_server(args)
     else:
         run_ours(args)
 

@@ -530,6 +530,75 @@ MC_API mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_s
                                   const mc_render_params* params, mc_guide* guide, int32_t train, float* d_accum,
                                   mc_render_stats* stats);
 
+/* ------------------------------------------------------------------------- */
+/* Render server. No counterpart in the reference (one scene per process).   */
+/*                                                                           */
+/* Scenes are registered once; their BVHs stay resident. Requests (scene,    */
+/* camera, size, spp, seed, guided or not) are admitted in arrival order     */
+/* while their memory fits the HBM budget (accumulation buffer, their share  */
+/* of the wave buffers and, for guided requests, the guide's per-path        */
+/* buffers); a request that could never fit is refused with MC_ERR_BUDGET.   */
+/* Each mc_server_step renders samples_per_step samples of the active        */
+/* requests it schedules (the oldest, then least remaining work first, up to */
+/* wave_paths paths): the plain ones of all scenes share the same waves (one */
+/* persistent trace launch and one shade launch per bounce for all of them), */
+/* guided ones run their scene's guided render. A request is done when it    */
+/* has all its samples; its accumulation buffer stays until released.        */
+/* Times are host seconds since the server was created.                      */
+/* ------------------------------------------------------------------------- */
+typedef struct mc_server mc_server;
+
+typedef struct mc_server_config {
+    int64_t hbm_budget_bytes;   /* 0 = 150 GB */
+    int32_t max_active;         /* requests admitted at a time (<= 128); 0 = 128 */
+    int32_t samples_per_step;   /* 0 = 1 */
+    int64_t wave_paths;         /* paths a step renders per sample: the oldest active request,
+                                   then the ones with the least remaining work while they fit;
+                                   0 = 4194304 */
+} mc_server_config;
+
+typedef struct mc_server_request {
+    int64_t scene_id;
+    mc_render_params params;    /* camera, size, spp, seed, max depth (counter-based RNG) */
+    int32_t guided;             /* render with the scene's guide (trained online) */
+} mc_server_request;
+
+enum { MC_REQ_PENDING = 0, MC_REQ_ACTIVE = 1, MC_REQ_DONE = 2, MC_REQ_RELEASED = 3 };
+
+typedef struct mc_server_result {
+    int64_t request_id;
+    int32_t state;              /* MC_REQ_* */
+    int32_t spp_done;
+    double submit_s, admit_s, done_s;
+    int64_t bytes;              /* memory charged to the budget until released */
+    const float* d_accum;       /* W*H float3 accumulation (valid until released) */
+} mc_server_result;
+
+typedef struct mc_server_stats {
+    int64_t budget_bytes, used_bytes, scene_bytes;
+    int32_t scenes, pending, active, done;
+    int64_t steps, waves, rays;
+} mc_server_stats;
+
+MC_API mc_status mc_server_create(mc_context* ctx, const mc_server_config* config, mc_server** out);
+MC_API mc_status mc_server_destroy(mc_server* server);
+/* Builds the scene's 4-wide BVH; the scene arrays stay owned by the caller
+ * and must outlive the server. *scene_id: the id requests refer to. */
+MC_API mc_status mc_server_add_scene(mc_server* server, const mc_scene_view* scene, int64_t* scene_id);
+MC_API mc_status mc_server_submit(mc_server* server, const mc_server_request* request, int64_t* request_id);
+/* Admits what fits, renders one step, retires finished requests.
+ * *active (may be NULL): requests active after the step. */
+MC_API mc_status mc_server_step(mc_server* server, int32_t* active);
+MC_API mc_status mc_server_get_result(mc_server* server, int64_t request_id, mc_server_result* result);
+/* Copies a request's accumulation buffer (W*H float3, the sum over its
+ * samples so far) into host memory. */
+MC_API mc_status mc_server_read(mc_server* server, int64_t request_id, float* host_rgb);
+/* Frees a finished request's accumulation buffer. */
+MC_API mc_status mc_server_release(mc_server* server, int64_t request_id);
+MC_API mc_status mc_server_get_stats(const mc_server* server, mc_server_stats* stats);
+/* Host seconds since the server was created (the clock of the results). */
+MC_API double mc_server_now(const mc_server* server);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
@@ -568,5 +637,10 @@ MC_STATIC_ASSERT(sizeof(mc_camera) == 172, "Camera is 172 bytes");
 MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
 /* this library's own structs (bindings mirror these sizes) */
 MC_STATIC_ASSERT(sizeof(mc_guide_config) == 80, "mc_guide_config is 80 bytes");
+MC_STATIC_ASSERT(sizeof(mc_render_params) == 232, "mc_render_params is 232 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_config) == 24, "mc_server_config is 24 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_request) == 248, "mc_server_request is 248 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_result) == 56, "mc_server_result is 56 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_stats) == 64, "mc_server_stats is 64 bytes");
 
 #endif /* MC_ABI_H */

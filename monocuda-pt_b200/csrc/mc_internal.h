@@ -144,6 +144,34 @@ struct mc_guide {
 };
 
 namespace mc {
+
+struct RenderTiming {
+    float ms = 0.f;
+    float trace_ms = 0.f;
+    int trace_launches = 0;
+    int kernel_launches = 0;
+};
+
+// One image of a wave sequence: its scene arrays, parameters, accumulation
+// buffer and BVH root; bvh, when set, is this item's own BVH (the server's
+// per-scene trees) instead of the segment of the shared one.
+struct WaveItem {
+    const mc_scene_view* view;
+    const mc_render_params* p;
+    float* accum;
+    int root;
+    int segment;
+    const mc_bvh* bvh = nullptr;
+};
+
+// Renders the items' samples in shared waves (mc_render.cu).
+mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph, bool timed,
+                    RenderTiming* tm, mc_guide* guide = nullptr, bool train = false);
+// run_waves with the error word and ray statistics reset before and read after.
+mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph,
+                       mc_render_stats* stats, mc_guide* guide = nullptr, bool train = false);
+mc_status check_params(const mc_render_params* p, const mc_scene_view* v);
+
 mc_status bvh_depth(mc_bvh* bvh);
 mc_status context_counters(mc_context* ctx);
 // Guide kernels driven by device-side counts (guided renders).

@@ -934,24 +934,10 @@ mc_status rng_reset(mc_context* ctx, int pixels, unsigned long long seed) {
     return MC_OK;
 }
 
-struct RenderTiming {
-    float ms = 0.f;
-    float trace_ms = 0.f;
-    int trace_launches = 0;
-    int kernel_launches = 0;
-};
-
-struct WaveItem {
-    const mc_scene_view* view;
-    const mc_render_params* p;
-    float* accum;
-    int root;
-    int segment;
-};
-
-static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* bvh, const WaveItem& it, int pathOffset, uint32_t sample) {
+static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* shared, const WaveItem& it, int pathOffset, uint32_t sample) {
     SceneGPU g;
     std::memset(&g, 0, sizeof(g));
+    const mc_bvh* bvh = it.bvh ? it.bvh : shared;
     const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
     g.nodes = (const float4*)(wide ? bvh->wide_nodes : bvh->nodes);
     g.prims = (const float4*)(wide ? bvh->wide_prims : bvh->prims);
@@ -992,7 +978,7 @@ static void set_single_scene(TraceArgs& t, const mc_bvh* bvh, int root, const mc
 // Runs waves until every item has rendered its spp samples. All items share
 // the launch configuration of items[0] (layout, persistence, RNG, intersector).
 mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph, bool timed,
-                    RenderTiming* tm, mc_guide* guide = nullptr, bool train = false) {
+                    RenderTiming* tm, mc_guide* guide, bool train) {
     const mc_render_params& p0 = *items[0].p;
     const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
     const bool philox = p0.rng == MC_RNG_PHILOX;
@@ -1060,7 +1046,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.err = ctx->d_error;
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
-    if (n == 1) set_single_scene(ta, bvh, items[0].root, items[0].view);
+    if (n == 1) set_single_scene(ta, items[0].bvh ? items[0].bvh : bvh, items[0].root, items[0].view);
 
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
@@ -1252,7 +1238,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     return MC_OK;
 }
 
-static mc_status check_params(const mc_render_params* p, const mc_scene_view* v) {
+mc_status check_params(const mc_render_params* p, const mc_scene_view* v) {
     if (!p || !v) return set_error(MC_ERR_INVALID, "render: null argument");
     if (p->width <= 0 || p->height <= 0) return set_error(MC_ERR_INVALID, "render: width and height must be positive");
     if ((long long)p->width * p->height >= (1ll << 30)) return set_error(MC_ERR_INVALID, "render: too many pixels");
@@ -1294,7 +1280,7 @@ static mc_status finish_stats(mc_context* ctx, const RenderTiming& tm, long long
 }
 
 mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph,
-                       mc_render_stats* stats, mc_guide* guide = nullptr, bool train = false) {
+                       mc_render_stats* stats, mc_guide* guide, bool train) {
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
     MC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long), ctx->stream));
     RenderTiming tm;

@@ -1,0 +1,343 @@
+// mc_server.cu - a render server over the wavefront path: resident scenes and
+// BVHs, admission by an HBM budget, and shared waves for all active requests.
+//
+// Each step renders samples_per_step samples of every active request. Plain
+// requests of every scene go into the same waves: the wave table holds one
+// entry per request (its own BVH, scene arrays, camera, image and sample
+// number), so one persistent trace launch and one shade launch per bounce
+// serve all of them. Guided requests render with their scene's guide, which
+// keeps training online across requests of that scene.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "mc_internal.h"
+
+namespace {
+
+// Wave-buffer bytes per path (path state, queues, shadow queue, hits, scene id)
+// and the guide's per-path buffers (mixture, record, primary NEE).
+constexpr long long kWaveBytesPerPath = 29 * 4 + 1 + 16 + 2;
+constexpr long long kGuideBytesPerPath = (40 + 12 + 3) * 4;
+
+struct ServerScene {
+    mc_scene_view view;
+    mc_bvh* bvh = nullptr;
+    mc_guide* guide = nullptr;
+    long long bytes = 0;
+};
+
+struct ServerRequest {
+    long long id = 0;
+    long long scene = 0;
+    mc_render_params params;
+    bool guided = false;
+    int state = MC_REQ_PENDING;
+    int done = 0;
+    float* accum = nullptr;
+    long long bytes = 0;
+    double submit_s = 0, admit_s = 0, done_s = 0;
+};
+
+long long bvh_bytes(const mc_bvh* b) {
+    long long n = b->n;
+    long long s = b->node_bytes + n * 48 + b->wide_count * 128 + n * 48 + 3 * n * 4 + (2 * n) * 4;
+    if (b->ref_internal) s += (2 * n) * (long long)sizeof(mc_bvh_node);
+    return s;
+}
+
+}  // namespace
+
+struct mc_server {
+    mc_context* ctx = nullptr;
+    mc_server_config cfg;
+    std::chrono::steady_clock::time_point t0;
+    std::vector<ServerScene> scenes;
+    std::map<long long, ServerRequest> requests;
+    std::deque<long long> pending;
+    std::vector<long long> active;
+    long long next_id = 1;
+    long long used = 0;
+    long long scene_bytes = 0;
+    long long steps = 0, waves = 0, rays = 0;
+    int done = 0;
+
+    double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+namespace {
+
+long long request_bytes(const mc_render_params& p, bool guided) {
+    long long px = (long long)p.width * p.height;
+    return px * 12 + px * kWaveBytesPerPath + (guided ? px * kGuideBytesPerPath : 0);
+}
+
+mc_status admit(mc_server* s) {
+    const double t = s->now();
+    while (!s->pending.empty() && (int)s->active.size() < s->cfg.max_active) {
+        ServerRequest& r = s->requests[s->pending.front()];
+        if (s->used + r.bytes > s->cfg.hbm_budget_bytes) break;  // arrival order: the head waits for room
+        size_t accBytes = (size_t)r.params.width * r.params.height * 3 * sizeof(float);
+        if (cudaMalloc(&r.accum, accBytes) != cudaSuccess) {
+            cudaGetLastError();
+            return mc::set_error(MC_ERR_OOM, "mc_server_step: accumulation buffer allocation failed");
+        }
+        cudaMemsetAsync(r.accum, 0, accBytes, s->ctx->stream);
+        s->used += r.bytes;
+        r.state = MC_REQ_ACTIVE;
+        r.admit_s = t;
+        s->active.push_back(r.id);
+        s->pending.pop_front();
+    }
+    return MC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mc_status mc_server_create(mc_context* ctx, const mc_server_config* config, mc_server** out) {
+    if (!ctx || !out) return mc::set_error(MC_ERR_INVALID, "mc_server_create: null argument");
+    mc_server* s = new mc_server();
+    s->ctx = ctx;
+    if (config) s->cfg = *config;
+    else std::memset(&s->cfg, 0, sizeof(s->cfg));
+    if (s->cfg.hbm_budget_bytes <= 0) s->cfg.hbm_budget_bytes = 150ll * 1000 * 1000 * 1000;
+    if (s->cfg.max_active <= 0) s->cfg.max_active = 128;
+    if (s->cfg.max_active > 128) s->cfg.max_active = 128;
+    if (s->cfg.samples_per_step <= 0) s->cfg.samples_per_step = 1;
+    if (s->cfg.wave_paths <= 0) s->cfg.wave_paths = 4194304;
+    s->t0 = std::chrono::steady_clock::now();
+    *out = s;
+    return MC_OK;
+}
+
+// Does not touch the server's context (which may be gone already): cudaFree
+// waits for the device work that uses the buffers.
+mc_status mc_server_destroy(mc_server* s) {
+    if (!s) return MC_OK;
+    for (auto& kv : s->requests) cudaFree(kv.second.accum);
+    for (auto& sc : s->scenes) {
+        mc_bvh_free(sc.bvh);
+        mc_guide_destroy(sc.guide);
+    }
+    delete s;
+    return MC_OK;
+}
+
+mc_status mc_server_add_scene(mc_server* s, const mc_scene_view* scene, int64_t* scene_id) {
+    if (!s || !scene || !scene_id) return mc::set_error(MC_ERR_INVALID, "mc_server_add_scene: null argument");
+    mc_bvh_build_opts opts;
+    std::memset(&opts, 0, sizeof(opts));
+    opts.layout = MC_BVH_LAYOUT_WIDE4;
+    ServerScene sc;
+    sc.view = *scene;
+    mc_status st = mc_bvh_build(s->ctx, scene, &opts, &sc.bvh);
+    if (st != MC_OK) return st;
+    sc.bytes = bvh_bytes(sc.bvh);
+    if (s->used + sc.bytes > s->cfg.hbm_budget_bytes) {
+        mc_bvh_free(sc.bvh);
+        return mc::set_error(MC_ERR_BUDGET, "mc_server_add_scene: the scene's BVH (%lld bytes) does not fit the budget",
+                             sc.bytes);
+    }
+    s->used += sc.bytes;
+    s->scene_bytes += sc.bytes;
+    s->scenes.push_back(sc);
+    *scene_id = (int64_t)s->scenes.size() - 1;
+    return MC_OK;
+}
+
+mc_status mc_server_submit(mc_server* s, const mc_server_request* req, int64_t* request_id) {
+    if (!s || !req || !request_id) return mc::set_error(MC_ERR_INVALID, "mc_server_submit: null argument");
+    if (req->scene_id < 0 || req->scene_id >= (int64_t)s->scenes.size())
+        return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_submit: unknown scene %lld", (long long)req->scene_id);
+    const ServerScene& sc = s->scenes[(size_t)req->scene_id];
+    mc_status st = mc::check_params(&req->params, &sc.view);
+    if (st != MC_OK) return st;
+    if (req->params.rng != MC_RNG_PHILOX) return mc::set_error(MC_ERR_INVALID, "mc_server_submit: requests use the counter-based RNG");
+    if (req->params.spp < 1) return mc::set_error(MC_ERR_INVALID, "mc_server_submit: spp must be >= 1");
+    ServerRequest r;
+    r.id = s->next_id++;
+    r.scene = req->scene_id;
+    r.params = req->params;
+    r.guided = req->guided != 0;
+    r.bytes = request_bytes(r.params, r.guided);
+    if (r.bytes + s->scene_bytes > s->cfg.hbm_budget_bytes)
+        return mc::set_error(MC_ERR_BUDGET, "mc_server_submit: the request needs %lld bytes, more than the budget leaves",
+                             r.bytes);
+    r.submit_s = s->now();
+    s->requests[r.id] = r;
+    s->pending.push_back(r.id);
+    *request_id = r.id;
+    return MC_OK;
+}
+
+mc_status mc_server_step(mc_server* s, int32_t* active_out) {
+    if (!s) return mc::set_error(MC_ERR_INVALID, "mc_server_step: null server");
+    mc_status st = admit(s);
+    if (st != MC_OK) return st;
+    s->steps++;
+    const int sps = s->cfg.samples_per_step;
+    // schedule: the oldest active request (no starvation), then least remaining
+    // work first while the step's paths stay within wave_paths
+    std::vector<long long> order(s->active.begin(), s->active.end());
+    if (order.size() > 1) {
+        std::stable_sort(order.begin() + 1, order.end(), [&](long long a, long long b) {
+            const ServerRequest& ra = s->requests[a];
+            const ServerRequest& rb = s->requests[b];
+            long long wa = (long long)ra.params.width * ra.params.height * (ra.params.spp - ra.done);
+            long long wb = (long long)rb.params.width * rb.params.height * (rb.params.spp - rb.done);
+            return wa < wb;
+        });
+    }
+    std::vector<long long> chosen;
+    long long paths = 0;
+    for (long long id : order) {
+        const ServerRequest& r = s->requests[id];
+        long long px = (long long)r.params.width * r.params.height;
+        if (!chosen.empty() && paths + px > s->cfg.wave_paths) continue;
+        chosen.push_back(id);
+        paths += px;
+    }
+    // plain requests of every scene share the waves
+    std::vector<mc_render_params> params;
+    std::vector<mc::WaveItem> items;
+    std::vector<long long> ids;
+    params.reserve(chosen.size());
+    for (long long id : chosen) {
+        ServerRequest& r = s->requests[id];
+        if (r.guided) continue;
+        mc_render_params p = r.params;
+        p.first_sample = r.params.first_sample + r.done;
+        p.spp = std::min(sps, r.params.spp - r.done);
+        p.use_graph = 0;
+        p.instrument = 0;
+        params.push_back(p);
+        ids.push_back(id);
+    }
+    for (size_t i = 0; i < ids.size(); i++) {
+        ServerRequest& r = s->requests[ids[i]];
+        const ServerScene& sc = s->scenes[(size_t)r.scene];
+        mc::WaveItem it{&sc.view, &params[i], r.accum, sc.bvh->wide_roots[0], 0};
+        it.bvh = sc.bvh;
+        items.push_back(it);
+    }
+    if (!items.empty()) {
+        mc_render_stats rs;
+        st = mc::render_items(s->ctx, items[0].bvh, items.data(), (int)items.size(), false, &rs);
+        if (st != MC_OK) return st;
+        s->rays += rs.extend_rays + rs.shadow_rays;
+        int w = 0;
+        for (const auto& p : params) w = std::max(w, p.spp);
+        s->waves += w;
+        for (size_t i = 0; i < ids.size(); i++) s->requests[ids[i]].done += params[i].spp;
+    }
+    // guided requests: their scene's guided render, training the scene's guide
+    for (long long id : chosen) {
+        ServerRequest& r = s->requests[id];
+        if (!r.guided) continue;
+        ServerScene& sc = s->scenes[(size_t)r.scene];
+        if (!sc.guide) {
+            mc_guide_config gc;
+            std::memset(&gc, 0, sizeof(gc));
+            gc.bounds = sc.bvh->bounds;
+            gc.seed = (uint64_t)r.scene + 1;
+            if ((st = mc_guide_create(s->ctx, &gc, &sc.guide)) != MC_OK) return st;
+        }
+        mc_render_params p = r.params;
+        p.first_sample = r.params.first_sample + r.done;
+        p.spp = std::min(sps, r.params.spp - r.done);
+        p.use_graph = 0;
+        p.instrument = 0;
+        mc_render_stats rs;
+        if ((st = mc_render_guided(s->ctx, sc.bvh, &sc.view, &p, sc.guide, 1, r.accum, &rs)) != MC_OK) return st;
+        s->rays += rs.extend_rays + rs.shadow_rays;
+        s->waves += p.spp;
+        r.done += p.spp;
+    }
+    // retire finished requests (their buffers stay until released)
+    const double t = s->now();
+    std::vector<long long> still;
+    for (long long id : s->active) {
+        ServerRequest& r = s->requests[id];
+        if (r.done >= r.params.spp) {
+            r.state = MC_REQ_DONE;
+            r.done_s = t;
+            s->done++;
+        } else {
+            still.push_back(id);
+        }
+    }
+    s->active.swap(still);
+    if (active_out) *active_out = (int32_t)s->active.size();
+    return MC_OK;
+}
+
+mc_status mc_server_get_result(mc_server* s, int64_t request_id, mc_server_result* out) {
+    if (!s || !out) return mc::set_error(MC_ERR_INVALID, "mc_server_get_result: null argument");
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_get_result: unknown request %lld", (long long)request_id);
+    const ServerRequest& r = it->second;
+    std::memset(out, 0, sizeof(*out));
+    out->request_id = r.id;
+    out->state = r.state;
+    out->spp_done = r.done;
+    out->submit_s = r.submit_s;
+    out->admit_s = r.admit_s;
+    out->done_s = r.done_s;
+    out->bytes = r.bytes;
+    out->d_accum = r.accum;
+    return MC_OK;
+}
+
+mc_status mc_server_read(mc_server* s, int64_t request_id, float* host_rgb) {
+    if (!s || !host_rgb) return mc::set_error(MC_ERR_INVALID, "mc_server_read: null argument");
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_read: unknown request %lld", (long long)request_id);
+    const ServerRequest& r = it->second;
+    if (!r.accum) return mc::set_error(MC_ERR_INVALID, "mc_server_read: request %lld holds no image", (long long)request_id);
+    const size_t bytes = (size_t)r.params.width * r.params.height * 3 * sizeof(float);
+    cudaError_t e = cudaMemcpyAsync(host_rgb, r.accum, bytes, cudaMemcpyDeviceToHost, s->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->ctx->stream);
+    if (e != cudaSuccess) return mc::cuda_error((int)e, "mc_server_read", __FILE__, __LINE__);
+    return MC_OK;
+}
+
+mc_status mc_server_release(mc_server* s, int64_t request_id) {
+    if (!s) return mc::set_error(MC_ERR_INVALID, "mc_server_release: null server");
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_release: unknown request %lld", (long long)request_id);
+    ServerRequest& r = it->second;
+    if (r.state != MC_REQ_DONE) return mc::set_error(MC_ERR_INVALID, "mc_server_release: request %lld is not done", (long long)request_id);
+    cudaFree(r.accum);
+    r.accum = nullptr;
+    r.state = MC_REQ_RELEASED;
+    s->used -= r.bytes;
+    return MC_OK;
+}
+
+mc_status mc_server_get_stats(const mc_server* s, mc_server_stats* out) {
+    if (!s || !out) return mc::set_error(MC_ERR_INVALID, "mc_server_get_stats: null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->budget_bytes = s->cfg.hbm_budget_bytes;
+    out->used_bytes = s->used;
+    out->scene_bytes = s->scene_bytes;
+    out->scenes = (int32_t)s->scenes.size();
+    out->pending = (int32_t)s->pending.size();
+    out->active = (int32_t)s->active.size();
+    out->done = s->done;
+    out->steps = s->steps;
+    out->waves = s->waves;
+    out->rays = s->rays;
+    return MC_OK;
+}
+
+double mc_server_now(const mc_server* s) { return s ? s->now() : 0.0; }
+
+}  // extern "C"

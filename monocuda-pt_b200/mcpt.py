@@ -24,6 +24,7 @@ LAYOUT_BINARY, LAYOUT_WIDE4 = 0, 1
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
 SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64
+REQ_PENDING, REQ_ACTIVE, REQ_DONE, REQ_RELEASED = 0, 1, 2, 3
 SORT_STATIC_MAX_PAIRS = 1 << 20
 GUIDE_PARAM_COUNT = 20200
 GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_OUTPUTS, GUIDE_LOBES = 144, 64, 40, 8
@@ -134,6 +135,26 @@ class GuideConfig(C.Structure):
                 ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("_pad", C.c_int32 * 3)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_active", C.c_int32), ("samples_per_step", C.c_int32),
+                ("wave_paths", C.c_int64)]
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [("scene_id", C.c_int64), ("params", RenderParams), ("guided", C.c_int32)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("request_id", C.c_int64), ("state", C.c_int32), ("spp_done", C.c_int32), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double), ("bytes", C.c_int64), ("d_accum", C.c_void_p)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("budget_bytes", C.c_int64), ("used_bytes", C.c_int64), ("scene_bytes", C.c_int64),
+                ("scenes", C.c_int32), ("pending", C.c_int32), ("active", C.c_int32), ("done", C.c_int32),
+                ("steps", C.c_int64), ("waves", C.c_int64), ("rays", C.c_int64)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("extend_rays", C.c_int64), ("shadow_rays", C.c_int64), ("paths", C.c_int64),
                 ("extend_per_depth", C.c_int64 * MAX_DEPTH_STATS), ("shadow_per_depth", C.c_int64 * MAX_DEPTH_STATS),
@@ -158,7 +179,8 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 80}
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 80, RenderParams: 232,
+         ServerConfig: 24, ServerRequest: 248, ServerResult: 56, ServerStats: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
 
@@ -205,6 +227,16 @@ SIGNATURES = {
     "mc_guide_steps": (I32, [P]),
     "mc_render_guided": (I32, [P, P, C.POINTER(SceneView), C.POINTER(RenderParams), P, I32, P,
                                C.POINTER(RenderStats)]),
+    "mc_server_create": (I32, [P, C.POINTER(ServerConfig), C.POINTER(P)]),
+    "mc_server_destroy": (I32, [P]),
+    "mc_server_add_scene": (I32, [P, C.POINTER(SceneView), C.POINTER(C.c_int64)]),
+    "mc_server_submit": (I32, [P, C.POINTER(ServerRequest), C.POINTER(C.c_int64)]),
+    "mc_server_step": (I32, [P, C.POINTER(I32)]),
+    "mc_server_get_result": (I32, [P, C.c_int64, C.POINTER(ServerResult)]),
+    "mc_server_release": (I32, [P, C.c_int64]),
+    "mc_server_read": (I32, [P, C.c_int64, P]),
+    "mc_server_get_stats": (I32, [P, C.POINTER(ServerStats)]),
+    "mc_server_now": (C.c_double, [P]),
 }
 
 _lib = None
@@ -527,6 +559,71 @@ class Guide:
     def close(self):
         if self.handle:
             self.lib.mc_guide_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The render server (mc_server_*): resident scenes, HBM-budget admission,
+    shared waves for all active requests."""
+
+    def __init__(self, ctx, budget_bytes=0, max_active=0, samples_per_step=1, wave_paths=0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        cfg = ServerConfig(budget_bytes, max_active, samples_per_step, wave_paths)
+        h = P()
+        check(self.lib.mc_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self.views = []  # the scene views must outlive the server
+
+    def add_scene(self, device_scene):
+        sid = C.c_int64()
+        check(self.lib.mc_server_add_scene(self.handle, C.byref(device_scene.view), C.byref(sid)))
+        self.views.append(device_scene)
+        return sid.value
+
+    def submit(self, scene_id, params, guided=False):
+        req = ServerRequest(scene_id, params, 1 if guided else 0)
+        rid = C.c_int64()
+        check(self.lib.mc_server_submit(self.handle, C.byref(req), C.byref(rid)))
+        return rid.value
+
+    def step(self):
+        a = I32()
+        check(self.lib.mc_server_step(self.handle, C.byref(a)))
+        return a.value
+
+    def result(self, rid):
+        r = ServerResult()
+        check(self.lib.mc_server_get_result(self.handle, rid, C.byref(r)))
+        return r
+
+    def read(self, rid, width, height):
+        """The request's accumulation buffer (sum over its samples) as a host array."""
+        import numpy as np
+        out = np.zeros(width * height * 3, np.float32)
+        check(self.lib.mc_server_read(self.handle, rid, out.ctypes.data))
+        return out
+
+    def release(self, rid):
+        check(self.lib.mc_server_release(self.handle, rid))
+
+    def stats(self):
+        st = ServerStats()
+        check(self.lib.mc_server_get_stats(self.handle, C.byref(st)))
+        return st
+
+    def now(self):
+        return self.lib.mc_server_now(self.handle)
+
+    def close(self):
+        if self.handle:
+            self.lib.mc_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
