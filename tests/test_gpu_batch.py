@@ -110,3 +110,26 @@ def test_batch_rejects_mismatched_items(ctx):
             batch.render(swapped)
     for s in scenes:
         mcpt.free_scene(s)
+
+
+def test_autotune_returns_params_that_leave_the_image_unchanged(ctx):
+    s = mcpt.generate_scene(mcpt.SCENE_CORNELL_SPHERES)
+    d = mcpt.DeviceScene(mcpt.host_triangles(s), spheres=mcpt.host_spheres(s))
+    b = mcpt.Bvh(ctx, d.view, layout=mcpt.LAYOUT_WIDE4)
+    p = small_params(s, 96, 4)
+    tuned = mcpt.RenderParams.from_buffer_copy(bytes(p))
+    mcpt.check(ctx.lib.mc_autotune(ctx.handle, b.handle, C.byref(d.view), C.byref(tuned), 3000))
+    assert tuned.persistent in (0, 1) and 1 <= tuned.refill_threshold <= 32 and tuned.use_graph in (0, 1)
+    again = mcpt.RenderParams.from_buffer_copy(bytes(p))
+    mcpt.check(ctx.lib.mc_autotune(ctx.handle, b.handle, C.byref(d.view), C.byref(again), 3000))  # cached
+    assert (again.persistent, again.refill_threshold, again.use_graph) == \
+        (tuned.persistent, tuned.refill_threshold, tuned.use_graph)
+    imgs = []
+    for q in (p, tuned):
+        acc = torch.zeros(96 * 96 * 3, dtype=torch.float32, device="cuda")
+        st = mcpt.RenderStats()
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, b.handle, C.byref(d.view), C.byref(q), acc.data_ptr(),
+                                               C.byref(st)))
+        imgs.append(acc.cpu().numpy())
+    assert np.array_equal(imgs[0], imgs[1])
+    mcpt.free_scene(s)
