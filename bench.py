@@ -208,9 +208,15 @@ def run_ours(args):
     K, Wm = args.steps, args.warmup
     timed_samples, warm_samples = sharding.sample_ranges(rank, world, K, Wm)
 
+    # the library's autotuner picks the trace variant and refill threshold for
+    # this scene / image size class (untimed; the choice does not change the image)
+    tuned = mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234)
+    mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
+
     def params(first, instrument=0):
-        return mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234,
-                                  first_sample=first, instrument=instrument)
+        return mcpt.render_params(scene.camera, W, H, 1, 8, persistent=bool(tuned.persistent), rng=mcpt.RNG_PHILOX,
+                                  seed=1234, first_sample=first, instrument=instrument,
+                                  refill_threshold=tuned.refill_threshold)
 
     st = mcpt.RenderStats()
     for s in warm_samples:
@@ -319,6 +325,7 @@ def run_ours(args):
         "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "config": dict(WORKLOAD, spp=K * world, bvh_layout=args.layout,
+                       autotuned={"persistent": int(tuned.persistent), "refill_threshold": int(tuned.refill_threshold)},
                        parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
                        samples_per_sec=round(W * H * K * world / (ms_max / 1e3), 1),
                        rays_per_path=round(rays_all / (W * H * K * world), 3)),

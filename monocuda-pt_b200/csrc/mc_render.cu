@@ -223,7 +223,10 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 // scene from the wave table. A single-scene launch reads the scene from the
 // kernel parameters instead, which costs no registers.
 template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE, bool BATCH>
-__global__ void __launch_bounds__(256, 4) k_trace(TraceArgs a) {
+#ifndef MC_TRACE_MIN_BLOCKS
+#define MC_TRACE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(256, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
     const unsigned ltmask = lanemask_lt();

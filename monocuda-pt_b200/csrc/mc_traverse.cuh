@@ -14,6 +14,12 @@
 #pragma once
 #include "mc_math.cuh"
 
+// Leaf children of a 4-wide node: one loop over the lane's hit leaves (1) or
+// one predicated block per child slot (0).
+#ifndef MC_LEAF_LOOP
+#define MC_LEAF_LOOP 1
+#endif
+
 namespace mc {
 
 enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_OCCLUDED = 2 };
@@ -172,6 +178,27 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, int* stack, const Watert
     slab4(s.r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, s.tmax, tn[3], hit[3]);
     if (COUNT) cnt->visits++;
     // leaf children first
+#if MC_LEAF_LOOP
+    // one loop over this lane's hit leaf children: a warp runs as many
+    // iterations as its busiest lane, not one predicated block per child slot
+    unsigned lm = (hit[0] && ref[0] < 0 ? 1u : 0u) | (hit[1] && ref[1] < 0 ? 2u : 0u) |
+                  (hit[2] && ref[2] < 0 ? 4u : 0u) | (hit[3] && ref[3] < 0 ? 8u : 0u);
+    while (lm) {
+        const int c = __ffs(lm) - 1;
+        lm &= lm - 1;
+        const int k = ~(c == 0 ? ref[0] : c == 1 ? ref[1] : c == 2 ? ref[2] : ref[3]);
+        float t;
+        if (COUNT) cnt->leaves++;
+        if (leaf_hit<ISECT>(sc, k, s, w, t)) {
+            if (ANY) {
+                if (t > 0.0001f && t < s.tmax) return STEP_OCCLUDED;
+            } else if (t > 0.0001f && (t < s.tmax || (t == s.tmax && s.hitLeaf >= 0 && k < s.hitLeaf))) {
+                s.tmax = t;
+                s.hitLeaf = k;
+            }
+        }
+    }
+#else
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         if (hit[c] && ref[c] < 0) {
@@ -188,6 +215,7 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, int* stack, const Watert
             }
         }
     }
+#endif
     // internal children, nearest first: sort (tnear, ref) ascending, misses as +inf
     float k0 = (hit[0] && ref[0] >= 0 && ref[0] != MC_WIDE_EMPTY) ? tn[0] : INFINITY;
     float k1 = (hit[1] && ref[1] >= 0 && ref[1] != MC_WIDE_EMPTY) ? tn[1] : INFINITY;

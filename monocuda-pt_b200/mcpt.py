@@ -247,7 +247,7 @@ def load(path=None):
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    path = path or os.environ.get("MCPT_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         raise McError(10, "libmcpt.so not built (run monocuda-pt_b200/build.py): %s" % path)
     lib = C.CDLL(path)
