@@ -222,18 +222,26 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 // BATCH: rays of several scenes share the launch; each lane reads its ray's
 // scene from the wave table. A single-scene launch reads the scene from the
 // kernel parameters instead, which costs no registers.
-template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE, bool BATCH>
 #ifndef MC_TRACE_MIN_BLOCKS
 #define MC_TRACE_MIN_BLOCKS 3
 #endif
-__global__ void __launch_bounds__(256, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
+constexpr int kTraceThreads = 256;
+constexpr int kTraceSmem = MC_SMEM_STACK ? kTraceThreads * MC_STACK_CAPACITY * (int)sizeof(int) : 0;
+template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE, bool BATCH>
+__global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
     const unsigned ltmask = lanemask_lt();
     const int extCount = a.extCount ? *a.extCount : a.extN;
     const int shCount = a.shCount ? *a.shCount : a.shN;
     const int total = extCount + shCount;
-    int stack[MC_STACK_CAPACITY];
+#if MC_SMEM_STACK
+    extern __shared__ int traceStack[];
+    const SharedStack<kTraceThreads> stack{traceStack + threadIdx.x};
+#else
+    int stackMem[MC_STACK_CAPACITY];
+    const LocalStack stack{stackMem};
+#endif
     TravState s;
     TraceScene tsLane;
     tsLane.nodes = nullptr;
@@ -805,9 +813,9 @@ __global__ void k_init_xorwow(curandState* states, int pixels, unsigned long lon
     if (p < pixels) curand_init(seed, p, 0, &states[p]);  // PT:2870
 }
 
-int occupancy_blocks(const void* fn, int sms) {
+int occupancy_blocks(const void* fn, int sms, size_t smem = 0) {
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem);
     if (per < 1) per = 1;
     return per * sms;
 }
@@ -832,17 +840,22 @@ TraceKernel trace_kernel(bool batch, bool wide, bool count, bool medium, int ise
 void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, bool wide, bool medium, int isect,
                   bool persistent, int plainBlocks, bool count = false) {
     static int occ[64] = {0};
+    static bool attr[64] = {false};
     TraceArgs t = t0;
     t.oneShot = persistent ? 0 : 1;
     const bool batch = t.sceneOf != nullptr;
     TraceKernel fn = trace_kernel(batch, wide, count, medium, isect);
+    const int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0) + (batch ? 16 : 0);
+    if (kTraceSmem > 48 * 1024 && !attr[key]) {
+        cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kTraceSmem);
+        attr[key] = true;
+    }
     int blocks = std::max(1, plainBlocks);
     if (persistent) {
-        int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0) + (batch ? 16 : 0);
-        if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count);
+        if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count, kTraceSmem);
         blocks = occ[key];
     }
-    fn<<<blocks, 256, 0, stream>>>(t);
+    fn<<<blocks, kTraceThreads, kTraceSmem, stream>>>(t);
 }
 
 }  // namespace

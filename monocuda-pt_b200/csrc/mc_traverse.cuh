@@ -19,6 +19,11 @@
 #ifndef MC_LEAF_LOOP
 #define MC_LEAF_LOOP 1
 #endif
+// Traversal stack of the trace kernel: shared memory (1; 64 KB per 256-thread
+// block, measured 2 % faster on B200) or local memory (0).
+#ifndef MC_SMEM_STACK
+#define MC_SMEM_STACK 1
+#endif
 
 namespace mc {
 
@@ -28,6 +33,19 @@ struct TraceScene {
     const float4* __restrict__ nodes;   // binary: 4 float4 per internal node; wide: 8
     const float4* __restrict__ prims;   // 3 float4 per leaf
     int root;                           // root node of this scene (batched builds share the arrays)
+};
+
+// A lane's traversal stack in local memory.
+struct LocalStack {
+    int* p;
+    MC_D int& operator[](int i) const { return p[i]; }
+};
+// A lane's traversal stack in shared memory: entry i of the block's thread t at
+// base[i * STRIDE + t], so a warp's accesses fall in 32 distinct banks at any depths.
+template <int STRIDE>
+struct SharedStack {
+    int* p;  // base + threadIdx.x
+    MC_D int& operator[](int i) const { return p[i * STRIDE]; }
 };
 
 // Traversal state of one ray in one lane.
@@ -77,8 +95,8 @@ struct TravCount {
     int leaves = 0;
 };
 
-template <bool ANY, int ISECT, bool COUNT = false>
-MC_D int trav_step(const TraceScene& sc, TravState& s, int* stack, const WatertightRay& w, int* err,
+template <bool ANY, int ISECT, bool COUNT = false, class Stack = LocalStack>
+MC_D int trav_step(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
                    TravCount* cnt = nullptr) {
     const float4* nd = sc.nodes + (long long)s.node * 4;
     float4 a = ldg4(nd + 0), b = ldg4(nd + 1), c = ldg4(nd + 2), d = ldg4(nd + 3);
@@ -162,8 +180,8 @@ MC_D void cswap(float& ka, int& va, float& kb, int& vb) {
     }
 }
 
-template <bool ANY, int ISECT, bool COUNT = false>
-MC_D int trav_step4(const TraceScene& sc, TravState& s, int* stack, const WatertightRay& w, int* err,
+template <bool ANY, int ISECT, bool COUNT = false, class Stack = LocalStack>
+MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
                     TravCount* cnt = nullptr) {
     const float4* nd = sc.nodes + (long long)s.node * 8;
     float4 lx = ldg4(nd + 0), ly = ldg4(nd + 1), lz = ldg4(nd + 2);
@@ -246,11 +264,11 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, int* stack, const Watert
     return STEP_CONTINUE;
 }
 
-template <bool ANY, int ISECT, bool COUNT, bool WIDE>
-MC_D int trav_step_layout(const TraceScene& sc, TravState& s, int* stack, const WatertightRay& w, int* err,
+template <bool ANY, int ISECT, bool COUNT, bool WIDE, class Stack>
+MC_D int trav_step_layout(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
                           TravCount* cnt) {
-    if (WIDE) return trav_step4<ANY, ISECT, COUNT>(sc, s, stack, w, err, cnt);
-    return trav_step<ANY, ISECT, COUNT>(sc, s, stack, w, err, cnt);
+    if (WIDE) return trav_step4<ANY, ISECT, COUNT, Stack>(sc, s, stack, w, err, cnt);
+    return trav_step<ANY, ISECT, COUNT, Stack>(sc, s, stack, w, err, cnt);
 }
 
 // The hit record fields a leaf slot stands for.
