@@ -604,6 +604,123 @@ __global__ void k_wide_select(const int32_t* __restrict__ parents, const Seg* __
     }
 }
 
+// Surface-area-greedy collapse: a wide node rooted at binary node B starts
+// with B's two children and repeatedly opens its internal slot of largest
+// surface area (ties: lowest slot) until it holds four slots or only leaves.
+// Every slot is a node of the binary tree, so every box stays exact.
+struct WideSlots {
+    int n;
+    int ref[4];   // binary child reference (internal index, or ~leaf)
+    int par[4];   // binary node whose record holds the slot's box
+    int side[4];
+};
+
+__device__ __forceinline__ float slot_area(const float4* nodes, int par, int side) {
+    const float* f = reinterpret_cast<const float*>(nodes + (long long)par * 4) + (side ? 6 : 0);
+    float dx = f[3] - f[0], dy = f[4] - f[1], dz = f[5] - f[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ void greedy_slots(const float4* nodes, int B, WideSlots& w) {
+    float4 d = nodes[(long long)B * 4 + 3];
+    w.n = 2;
+    w.ref[0] = __float_as_int(d.x); w.par[0] = B; w.side[0] = 0;
+    w.ref[1] = __float_as_int(d.y); w.par[1] = B; w.side[1] = 1;
+    while (w.n < 4) {
+        int best = -1;
+        float bestA = -1.0f;
+        for (int j = 0; j < w.n; j++) {
+            if (w.ref[j] < 0) continue;
+            float a = slot_area(nodes, w.par[j], w.side[j]);
+            if (a > bestA) {
+                bestA = a;
+                best = j;
+            }
+        }
+        if (best < 0) break;
+        const int X = w.ref[best];
+        float4 dx = nodes[(long long)X * 4 + 3];
+        w.ref[best] = __float_as_int(dx.x); w.par[best] = X; w.side[best] = 0;
+        w.ref[w.n] = __float_as_int(dx.y); w.par[w.n] = X; w.side[w.n] = 1;
+        w.n++;
+    }
+}
+
+// Wide id i for the i-th scene root.
+__global__ void k_scatter_ids(const int* __restrict__ roots, int n, int* __restrict__ wideId) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) wideId[roots[i]] = i;
+}
+
+// One level of the collapse: every wide node of the frontier picks its slots
+// and gives its internal slots consecutive wide ids (the next frontier).
+__global__ void k_wide_greedy_level(const float4* __restrict__ nodes, const int* __restrict__ frontier,
+                                    const int* __restrict__ count, int capacity, int* __restrict__ next,
+                                    int* __restrict__ nextCount, int* __restrict__ wideId, int* __restrict__ rootOf,
+                                    int* counter, int* err) {
+    const int n = min(*count, capacity);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int B = frontier[i];
+        const int w = wideId[B];
+        if (w < 0 || w >= capacity) {
+            atomicOr(err, MC_DEVERR_INPUT);
+            continue;
+        }
+        rootOf[w] = B;
+        WideSlots s;
+        greedy_slots(nodes, B, s);
+        int nInt = 0;
+        for (int j = 0; j < s.n; j++) nInt += s.ref[j] >= 0 ? 1 : 0;
+        if (nInt == 0) continue;
+        const int base = atomicAdd(counter, nInt);
+        const int out = atomicAdd(nextCount, nInt);
+        int k = 0;
+        for (int j = 0; j < s.n; j++) {
+            if (s.ref[j] < 0) continue;
+            if (base + k >= capacity || out + k >= capacity) {
+                atomicOr(err, MC_DEVERR_INPUT);
+                break;
+            }
+            wideId[s.ref[j]] = base + k;
+            next[out + k] = s.ref[j];
+            k++;
+        }
+    }
+}
+
+// Writes every wide node of the greedy collapse from its slots.
+__global__ void k_wide_fill_greedy(const float4* __restrict__ nodes, const int* __restrict__ rootOf,
+                                   const int* __restrict__ wideId, const int* __restrict__ rank, int count,
+                                   float4* __restrict__ wide) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= count) return;
+    WideSlots s;
+    greedy_slots(nodes, rootOf[id], s);
+    float lo[3][4], hi[3][4];
+    int ref[4];
+    for (int c = 0; c < 4; c++) {
+        if (c < s.n) {
+            const float* f = reinterpret_cast<const float*>(nodes + (long long)s.par[c] * 4) + (s.side[c] ? 6 : 0);
+            lo[0][c] = f[0]; lo[1][c] = f[1]; lo[2][c] = f[2];
+            hi[0][c] = f[3]; hi[1][c] = f[4]; hi[2][c] = f[5];
+            ref[c] = s.ref[c] < 0 ? ~rank[~s.ref[c]] : wideId[s.ref[c]];
+        } else {
+            lo[0][c] = lo[1][c] = lo[2][c] = INFINITY;
+            hi[0][c] = hi[1][c] = hi[2][c] = -INFINITY;
+            ref[c] = MC_WIDE_EMPTY;
+        }
+    }
+    float4* w = wide + (long long)id * 8;
+    w[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    w[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    w[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    w[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    w[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    w[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    w[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+    w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 __device__ __forceinline__ void child_slot_box(const float4* nodes, int node, int side, float* b) {
     const float* f = reinterpret_cast<const float*>(nodes + (long long)node * 4);
     int o = side ? 6 : 0;
@@ -929,22 +1046,76 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
                                                                 (const int2*)ctx->scratch[1].ptr, dSeg, nseg, N, NI, rank,
                                                                 ctx->d_error);
     int count = 1;
+    int* rootOf = nullptr;   // greedy collapse: binary root of each wide node
+    bool greedy = false;
     if (NI > 0) {
-        MC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-        k_wide_select<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, dSeg, nseg, NI, wideId, counter,
-                                                                       dWideRoot);
-        MC_CUDA(cudaMemcpyAsync(&count, counter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        // surface-area-greedy collapse, level by level from the scene roots
+        int* front[2] = {nullptr, nullptr};
+        int* cnt = nullptr;  // [0], [1]: frontier sizes, [2]: wide-id counter
+        auto release = [&]() { cudaFree(front[0]); cudaFree(front[1]); cudaFree(cnt); };
+        if (cudaMalloc(&rootOf, (size_t)NI * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&front[0], (size_t)NI * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&front[1], (size_t)NI * sizeof(int)) != cudaSuccess || cudaMalloc(&cnt, 4 * sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            release();
+            cudaFree(rootOf);
+            return set_error(MC_ERR_OOM, "mc_bvh_build: wide-collapse scratch allocation failed");
+        }
+        MC_CUDA(cudaMemsetAsync(wideId, 0xFF, (size_t)NI * sizeof(int), ctx->stream));
+        std::vector<int> roots(bvh->bin_roots.begin(), bvh->bin_roots.end());
+        MC_CUDA(cudaMemcpyAsync(front[0], roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        k_scatter_ids<<<grid_for(nseg, kBlock), kBlock, 0, ctx->stream>>>(front[0], nseg, wideId);
+        int h[3] = {nseg, 0, nseg};
+        MC_CUDA(cudaMemcpyAsync(cnt, h, 3 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        int levels = 0, cur = 0, n = nseg;
+        while (n > 0 && levels <= 4 * MC_STACK_CAPACITY) {
+            MC_CUDA(cudaMemsetAsync(cnt + (1 - cur), 0, sizeof(int), ctx->stream));
+            k_wide_greedy_level<<<std::max(1, std::min(grid_for(n, kBlock), ctx->sm_count * 8)), kBlock, 0, ctx->stream>>>(
+                (const float4*)bvh->nodes, front[cur], cnt + cur, NI, front[1 - cur], cnt + (1 - cur), wideId, rootOf,
+                cnt + 2, ctx->d_error);
+            MC_CUDA(cudaMemcpyAsync(&n, cnt + (1 - cur), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            MC_CUDA(cudaStreamSynchronize(ctx->stream));
+            cur = 1 - cur;
+            levels++;
+        }
+        MC_CUDA(cudaMemcpyAsync(&count, cnt + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        int flags = 0;
+        if ((st = flags_now(ctx, &flags)) != MC_OK || flags) {
+            release();
+            cudaFree(rootOf);
+            return st != MC_OK ? st : status_from_device_flags(flags);
+        }
+        release();
+        // a visit pushes at most 3 siblings: the traversal stack must hold 3 per level
+        greedy = n == 0 && 3 * levels <= MC_STACK_CAPACITY;
+        if (!greedy) {
+            cudaFree(rootOf);
+            rootOf = nullptr;
+            MC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
+            k_wide_select<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, dSeg, nseg, NI, wideId, counter,
+                                                                           dWideRoot);
+            MC_CUDA(cudaMemcpyAsync(&count, counter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        }
     }
     int flags = 0;
-    if ((st = flags_now(ctx, &flags)) != MC_OK) return st;
-    if (flags) return status_from_device_flags(flags);
+    if ((st = flags_now(ctx, &flags)) != MC_OK || flags) {
+        cudaFree(rootOf);
+        return st != MC_OK ? st : status_from_device_flags(flags);
+    }
     if (cudaMalloc(&bvh->wide_nodes, (size_t)count * 128) != cudaSuccess ||
         cudaMalloc(&bvh->wide_prims, (size_t)N * 48) != cudaSuccess) {
         cudaGetLastError();
+        cudaFree(rootOf);
         return set_error(MC_ERR_OOM, "mc_bvh_build: wide-node allocation failed");
     }
     bvh->wide_roots.assign(nseg, 0);
-    if (NI > 0) {
+    if (NI > 0 && greedy) {
+        k_wide_fill_greedy<<<grid_for(count, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, rootOf, wideId,
+                                                                              rank, count, (float4*)bvh->wide_nodes);
+        for (int s = 0; s < nseg; s++) bvh->wide_roots[s] = s;
+        MC_CUDA(cudaStreamSynchronize(ctx->stream));
+        cudaFree(rootOf);
+    } else if (NI > 0) {
         k_wide_fill<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, wideId, rank, NI,
                                                                      (float4*)bvh->wide_nodes);
         MC_CUDA(cudaMemcpyAsync(bvh->wide_roots.data(), dWideRoot, (size_t)nseg * sizeof(int), cudaMemcpyDeviceToHost,
