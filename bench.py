@@ -44,7 +44,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = the named workload)")
-    ap.add_argument("--layout", default="wide4", choices=["binary", "wide4"], help="BVH node layout traversed")
+    ap.add_argument("--layout", default="wide4", choices=["binary", "wide4", "wide4q"], help="BVH node layout traversed")
+    ap.add_argument("--refill", type=int, default=0,
+                    help="trace refill threshold; 0 = the library autotuner's choice (a fixed value keeps profiles "
+                         "free of the autotuner's probe launches)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
@@ -201,7 +204,7 @@ def run_ours(args):
     env = mcpt.host_env(scene)
     ctx = mcpt.Context(local)
     ds = mcpt.DeviceScene(tris, env_rgba=env, env_intensity=scene.env_intensity, device=dev)
-    layout = mcpt.LAYOUT_WIDE4 if args.layout == "wide4" else mcpt.LAYOUT_BINARY
+    layout = {"binary": mcpt.LAYOUT_BINARY, "wide4": mcpt.LAYOUT_WIDE4, "wide4q": mcpt.LAYOUT_WIDE4Q}[args.layout]
     bvh = mcpt.Bvh(ctx, ds.view, layout=layout)
     W, H = scene.width, scene.height
     acc = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
@@ -210,8 +213,10 @@ def run_ours(args):
 
     # the library's autotuner picks the trace variant and refill threshold for
     # this scene / image size class (untimed; the choice does not change the image)
-    tuned = mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234)
-    mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
+    tuned = mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234,
+                               refill_threshold=args.refill)
+    if args.refill <= 0:
+        mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
 
     def params(first, instrument=0):
         return mcpt.render_params(scene.camera, W, H, 1, 8, persistent=bool(tuned.persistent), rng=mcpt.RNG_PHILOX,
@@ -313,7 +318,7 @@ def run_ours(args):
             torch.distributed.destroy_process_group()
         return
     peak, peak_kind = peaks()
-    node_bytes = 2 * NODE_BYTES if layout == mcpt.LAYOUT_WIDE4 else NODE_BYTES  # 128-byte wide nodes
+    node_bytes = 2 * NODE_BYTES if layout == mcpt.LAYOUT_WIDE4 else NODE_BYTES  # 128-byte wide, 64-byte binary / quantised
     alg_bytes = visits * node_bytes + leaves * LEAF_BYTES + ext * EXT_IO_BYTES + shd * SHADOW_IO_BYTES
     per_launch_bytes = alg_bytes / max(trace_launches, 1)
     per_launch_s = trace_ms / max(trace_launches, 1) / 1e3

@@ -210,7 +210,9 @@ typedef struct mc_scene_view {
 
 enum {
     MC_BVH_LAYOUT_BINARY = 0,   /* children's boxes stored in the parent, 64 B per node */
-    MC_BVH_LAYOUT_WIDE4 = 1     /* 4-wide collapse of the binary tree, 128 B per node */
+    MC_BVH_LAYOUT_WIDE4 = 1,    /* 4-wide collapse of the binary tree, exact boxes, 128 B per node */
+    MC_BVH_LAYOUT_WIDE4Q = 2    /* the same tree with child boxes quantised to 8 bits per plane
+                                   against a per-node frame, rounded outward, 64 B per node */
 };
 
 typedef struct mc_bvh_build_opts {

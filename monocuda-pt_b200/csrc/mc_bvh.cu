@@ -721,6 +721,72 @@ __global__ void k_wide_fill_greedy(const float4* __restrict__ nodes, const int* 
     w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// Quantised 4-wide node (64 bytes), from an exact one (128 bytes):
+//   float4 0: frame origin (x, y, z) = the union's low corner; w = the three
+//             scale exponents (e + 128, one byte per axis)
+//   float4 1: lo.x, lo.y, lo.z, hi.x of the 4 children, one byte per child
+//   float4 2: hi.y, hi.z of the 4 children; two spare words
+//   float4 3: the 4 child references (as in the exact layout)
+// A plane decodes as origin + q * 2^e. q is chosen so that this decode, which
+// is exact up to one rounding of the sum (q * 2^e is exact), lies at or
+// outside the exact plane: low planes round down, high planes round up.
+// Exponents stay >= -100 so no decode term is subnormal.
+__device__ __forceinline__ float q_decode(float origin, int q, int e) {
+    return origin + (float)q * __int_as_float((e + 127) << 23);
+}
+
+__global__ void k_quantize_wide(const float4* __restrict__ exact, int count, float4* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float4* n = exact + (size_t)i * 8;
+    const float4 lx = n[0], ly = n[1], lz = n[2], hx = n[3], hy = n[4], hz = n[5], rf = n[6];
+    const float lo[3][4] = {{lx.x, lx.y, lx.z, lx.w}, {ly.x, ly.y, ly.z, ly.w}, {lz.x, lz.y, lz.z, lz.w}};
+    const float hi[3][4] = {{hx.x, hx.y, hx.z, hx.w}, {hy.x, hy.y, hy.z, hy.w}, {hz.x, hz.y, hz.z, hz.w}};
+    const int ref[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z), __float_as_int(rf.w)};
+    float origin[3];
+    int ex[3];
+    unsigned qlo[3][4], qhi[3][4];
+    for (int a = 0; a < 3; a++) {
+        float ulo = INFINITY, uhi = -INFINITY;
+        for (int c = 0; c < 4; c++) {
+            if (ref[c] == MC_WIDE_EMPTY) continue;
+            ulo = fminf(ulo, lo[a][c]);
+            uhi = fmaxf(uhi, hi[a][c]);
+        }
+        if (!(ulo <= uhi)) { ulo = 0.f; uhi = 0.f; }
+        origin[a] = ulo;
+        int e = -100;
+        const double ext = (double)uhi - (double)ulo;
+        if (ext > 0.0) e = max(-100, (int)ceil(log2(ext / 255.0)));
+        while (e < 127 && q_decode(ulo, 255, e) < uhi) e++;
+        ex[a] = e;
+        for (int c = 0; c < 4; c++) {
+            if (ref[c] == MC_WIDE_EMPTY) {
+                qlo[a][c] = 255;  // empty: low above high
+                qhi[a][c] = 0;
+                continue;
+            }
+            const double s = ldexp(1.0, e);
+            int ql = (int)floor(((double)lo[a][c] - (double)ulo) / s);
+            ql = min(255, max(0, ql));
+            while (ql > 0 && q_decode(ulo, ql, e) > lo[a][c]) ql--;
+            int qh = (int)ceil(((double)hi[a][c] - (double)ulo) / s);
+            qh = min(255, max(0, qh));
+            while (qh < 255 && q_decode(ulo, qh, e) < hi[a][c]) qh++;
+            qlo[a][c] = (unsigned)ql;
+            qhi[a][c] = (unsigned)qh;
+        }
+    }
+    auto pack = [](const unsigned* v) { return v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24); };
+    const unsigned exps = (unsigned)(ex[0] + 128) | ((unsigned)(ex[1] + 128) << 8) | ((unsigned)(ex[2] + 128) << 16);
+    float4* o = out + (size_t)i * 4;
+    o[0] = make_float4(origin[0], origin[1], origin[2], __int_as_float((int)exps));
+    o[1] = make_float4(__int_as_float((int)pack(qlo[0])), __int_as_float((int)pack(qlo[1])),
+                       __int_as_float((int)pack(qlo[2])), __int_as_float((int)pack(qhi[0])));
+    o[2] = make_float4(__int_as_float((int)pack(qhi[1])), __int_as_float((int)pack(qhi[2])), 0.f, 0.f);
+    o[3] = rf;
+}
+
 __device__ __forceinline__ void child_slot_box(const float4* nodes, int node, int side, float* b) {
     const float* f = reinterpret_cast<const float*>(nodes + (long long)node * 4);
     int o = side ? 6 : 0;
@@ -1158,7 +1224,7 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
     if (total >= (1ll << 30)) return set_error(MC_ERR_INVALID, "too many primitives in the batch (limit 2^30 - 1)");
     mc_bvh_build_opts o = {};
     if (opts) o = *opts;
-    if (o.layout != MC_BVH_LAYOUT_BINARY && o.layout != MC_BVH_LAYOUT_WIDE4)
+    if (o.layout != MC_BVH_LAYOUT_BINARY && o.layout != MC_BVH_LAYOUT_WIDE4 && o.layout != MC_BVH_LAYOUT_WIDE4Q)
         return set_error(MC_ERR_INVALID, "mc_bvh_build: unknown layout");
     if (nseg > 1 && (o.permutation || o.keep_reference_nodes))
         return set_error(MC_ERR_INVALID, "mc_bvh_build_batch: permutation and reference nodes are single-scene options");
@@ -1296,8 +1362,24 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
         bvh->seg_prim_off[s] = segs[s].primOff;
         bvh->bin_roots[s] = segs[s].intOff;
     }
-    if (o.layout == MC_BVH_LAYOUT_WIDE4) {
+    if (o.layout == MC_BVH_LAYOUT_WIDE4 || o.layout == MC_BVH_LAYOUT_WIDE4Q) {
         if ((st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot)) != MC_OK) return fail(st);
+    }
+    if (o.layout == MC_BVH_LAYOUT_WIDE4Q) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, (size_t)bvh->wide_count * 64) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(set_error(MC_ERR_OOM, "mc_bvh_build: quantised-node allocation failed"));
+        }
+        k_quantize_wide<<<grid_for((int)bvh->wide_count, kBlock), kBlock, 0, ctx->stream>>>(
+            (const float4*)bvh->wide_nodes, (int)bvh->wide_count, (float4*)q);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            cudaFree(q);
+            return fail(cuda_error(cudaGetLastError(), "mc_bvh_build (quantise)", __FILE__, __LINE__));
+        }
+        cudaFree(bvh->wide_nodes);
+        bvh->wide_nodes = q;
+        bvh->layout = MC_BVH_LAYOUT_WIDE4Q;
     }
     *out = bvh;
     return MC_OK;
@@ -1399,7 +1481,9 @@ mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info) {
     info->internal_count = bvh->ni;
     info->depth = bvh->depth;
     info->layout = bvh->layout;
-    info->node_bytes = bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_count * 128 : bvh->node_bytes;
+    info->node_bytes = bvh->layout == MC_BVH_LAYOUT_WIDE4    ? bvh->wide_count * 128
+                       : bvh->layout == MC_BVH_LAYOUT_WIDE4Q ? bvh->wide_count * 64
+                                                             : bvh->node_bytes;
     info->prim_bytes = (long long)bvh->n * 48;
     info->scene_bounds = bvh->bounds;
     return MC_OK;

@@ -227,7 +227,7 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 #endif
 constexpr int kTraceThreads = 256;
 constexpr int kTraceSmem = MC_SMEM_STACK ? kTraceThreads * MC_STACK_CAPACITY * (int)sizeof(int) : 0;
-template <int ISECT, bool MEDIUM, bool COUNT, bool WIDE, bool BATCH>
+template <int ISECT, bool MEDIUM, bool COUNT, int LAY, bool BATCH>
 __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
@@ -320,8 +320,8 @@ __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(Tr
         }
         if (exhausted && __ballot_sync(kFull, has) == 0u) break;
         if (has) {
-            int r = (kind == RAY_SHADOW_ANY) ? trav_step_layout<true, ISECT, COUNT, WIDE>(ts, s, stack, w, a.err, &cnt)
-                                             : trav_step_layout<false, ISECT, COUNT, WIDE>(ts, s, stack, w, a.err, &cnt);
+            int r = (kind == RAY_SHADOW_ANY) ? trav_step_layout<true, ISECT, COUNT, LAY>(ts, s, stack, w, a.err, &cnt)
+                                             : trav_step_layout<false, ISECT, COUNT, LAY>(ts, s, stack, w, a.err, &cnt);
             if (r != STEP_CONTINUE) {
                 const mc_triangle_cold* cold = a.cold0;
                 const mc_sphere* spheres = a.spheres0;
@@ -822,14 +822,14 @@ int occupancy_blocks(const void* fn, int sms, size_t smem = 0) {
 
 typedef void (*TraceKernel)(TraceArgs);
 
-// [batch][wide][count][medium][isect]
-#define MC_TK(W, B)                                                                                                           \
-    {{{k_trace<0, false, false, W, B>, k_trace<1, false, false, W, B>}, {k_trace<0, true, false, W, B>, k_trace<1, true, false, W, B>}}, \
-     {{k_trace<0, false, true, W, B>, k_trace<1, false, true, W, B>}, {k_trace<0, true, true, W, B>, k_trace<1, true, true, W, B>}}}
-TraceKernel trace_kernel(bool batch, bool wide, bool count, bool medium, int isect) {
-    static const TraceKernel table[2][2][2][2][2] = {{MC_TK(false, false), MC_TK(true, false)},
-                                                     {MC_TK(false, true), MC_TK(true, true)}};
-    return table[batch ? 1 : 0][wide ? 1 : 0][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
+// [batch][layout][count][medium][isect]
+#define MC_TK(L, B)                                                                                                           \
+    {{{k_trace<0, false, false, L, B>, k_trace<1, false, false, L, B>}, {k_trace<0, true, false, L, B>, k_trace<1, true, false, L, B>}}, \
+     {{k_trace<0, false, true, L, B>, k_trace<1, false, true, L, B>}, {k_trace<0, true, true, L, B>, k_trace<1, true, true, L, B>}}}
+TraceKernel trace_kernel(bool batch, int layout, bool count, bool medium, int isect) {
+    static const TraceKernel table[2][3][2][2][2] = {{MC_TK(0, false), MC_TK(1, false), MC_TK(2, false)},
+                                                     {MC_TK(0, true), MC_TK(1, true), MC_TK(2, true)}};
+    return table[batch ? 1 : 0][layout][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
 }
 
 // Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
@@ -837,15 +837,15 @@ TraceKernel trace_kernel(bool batch, bool wide, bool count, bool medium, int ise
 // one ray per thread and no refill, over plainBlocks blocks; sharing the kernel
 // keeps the per-ray arithmetic identical between the two modes. A launch is a
 // batch launch when it carries a per-path scene map.
-void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, bool wide, bool medium, int isect,
+void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, int layout, bool medium, int isect,
                   bool persistent, int plainBlocks, bool count = false) {
     static int occ[64] = {0};
     static bool attr[64] = {false};
     TraceArgs t = t0;
     t.oneShot = persistent ? 0 : 1;
     const bool batch = t.sceneOf != nullptr;
-    TraceKernel fn = trace_kernel(batch, wide, count, medium, isect);
-    const int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (wide ? 8 : 0) + (batch ? 16 : 0);
+    TraceKernel fn = trace_kernel(batch, layout, count, medium, isect);
+    const int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (batch ? 8 : 0) + 16 * layout;  // < 48
     if (kTraceSmem > 48 * 1024 && !attr[key]) {
         cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kTraceSmem);
         attr[key] = true;
@@ -954,7 +954,7 @@ static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* shared, const WaveItem&
     SceneGPU g;
     std::memset(&g, 0, sizeof(g));
     const mc_bvh* bvh = it.bvh ? it.bvh : shared;
-    const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
+    const bool wide = bvh->layout != MC_BVH_LAYOUT_BINARY;
     g.nodes = (const float4*)(wide ? bvh->wide_nodes : bvh->nodes);
     g.prims = (const float4*)(wide ? bvh->wide_prims : bvh->prims);
     g.root = it.root;
@@ -982,7 +982,7 @@ static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* shared, const WaveItem&
 
 // The scene of a single-scene trace launch, passed as kernel parameters.
 static void set_single_scene(TraceArgs& t, const mc_bvh* bvh, int root, const mc_scene_view* v) {
-    const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
+    const bool wide = bvh->layout != MC_BVH_LAYOUT_BINARY;
     t.ts0.nodes = (const float4*)(wide ? bvh->wide_nodes : bvh->nodes);
     t.ts0.prims = (const float4*)(wide ? bvh->wide_prims : bvh->prims);
     t.ts0.root = root;
@@ -996,7 +996,7 @@ static void set_single_scene(TraceArgs& t, const mc_bvh* bvh, int root, const mc
 mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, int n, bool useGraph, bool timed,
                     RenderTiming* tm, mc_guide* guide, bool train) {
     const mc_render_params& p0 = *items[0].p;
-    const bool wide = bvh->layout == MC_BVH_LAYOUT_WIDE4;
+    const int layout = bvh->layout;
     const bool philox = p0.rng == MC_RNG_PHILOX;
     const int isect = p0.intersector;
     const bool persistent = p0.persistent != 0;
@@ -1109,7 +1109,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 t.sr = nee0[0]; t.sg = nee0[1]; t.sb = nee0[2];
             }
             if (timeTrace) traceEvent();
-            launch_trace(ctx, stream, t, wide, medium, isect, persistent, plainBlocks, countVisits);
+            launch_trace(ctx, stream, t, layout, medium, isect, persistent, plainBlocks, countVisits);
             if (timeTrace) traceEvent();
             launches++;
             if (d == maxD) break;
@@ -1164,7 +1164,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         unsigned long long key[16] = {(unsigned long long)(uintptr_t)stream,
                                       (unsigned long long)capacity,
                                       (unsigned long long)maxD,
-                                      (unsigned long long)((wide ? 1 : 0) | (medium ? 2 : 0) | (philox ? 4 : 0) |
+                                      (unsigned long long)((layout << 6) | (medium ? 2 : 0) | (philox ? 4 : 0) |
                                                            (persistent ? 8 : 0) | (n > 1 ? 16 : 0)),
                                       (unsigned long long)isect,
                                       (unsigned long long)ta.refill,
@@ -1309,7 +1309,7 @@ mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items
 
 // The single-scene trace arguments of the ray-set entry points.
 static void ray_set_scene(TraceArgs& t, const mc_bvh* bvh, const mc_scene_view* scene) {
-    set_single_scene(t, bvh, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], scene);
+    set_single_scene(t, bvh, bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0], scene);
 }
 
 }  // namespace mc
@@ -1335,7 +1335,7 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
     if (params->rng == MC_RNG_XORWOW && (!ctx->rng_ready || ctx->rng_pixels < pixels || ctx->rng_seed != params->seed)) {
         if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
     }
-    mc::WaveItem it{scene, params, d_accum, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
+    mc::WaveItem it{scene, params, d_accum, bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
     return mc::render_items(ctx, bvh, &it, 1, params->use_graph != 0, stats);
 }
 
@@ -1356,7 +1356,7 @@ mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_ite
         if (prims != segPrims) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: item %d does not match scene %d of the BVH", i, i);
         capacity += (long long)items[i].params.width * items[i].params.height;
         its[i] = mc::WaveItem{&items[i].scene, &items[i].params, items[i].d_accum,
-                              bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[i] : bvh->bin_roots[i], i};
+                              bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[i] : bvh->bin_roots[i], i};
     }
     if (capacity >= (1ll << 30)) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: too many paths per wave");
     return mc::render_items(ctx, bvh, its.data(), count, use_graph != 0, stats);
@@ -1376,7 +1376,7 @@ mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     if (params->queue_capacity > 0 && params->queue_capacity < pixels)
         return mc::set_error(MC_ERR_INVALID, "mc_render_guided: queue capacity below width*height");
     if ((st = mc::guide_reserve_paths(guide, pixels)) != MC_OK) return st;
-    mc::WaveItem it{scene, params, d_accum, bvh->layout == MC_BVH_LAYOUT_WIDE4 ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
+    mc::WaveItem it{scene, params, d_accum, bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
     return mc::render_items(ctx, bvh, &it, 1, false, stats, guide, train != 0);
 }
 
@@ -1404,7 +1404,7 @@ mc_status mc_trace_closest(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     t.dx = d_rays + 3 * N; t.dy = d_rays + 4 * N; t.dz = d_rays + 5 * N; t.time = d_rays + 6 * N;
     t.hits = d_hits;
     t.work = work;
-    mc::launch_trace(ctx, ctx->stream, t, bvh->layout == MC_BVH_LAYOUT_WIDE4, false, intersector, !plain, (n + 255) / 256);
+    mc::launch_trace(ctx, ctx->stream, t, bvh->layout, false, intersector, !plain, (n + 255) / 256);
     MC_CUDA(cudaGetLastError());
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1438,7 +1438,7 @@ mc_status mc_trace_any(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* 
     t.smax = d_tmax;
     t.occluded = d_occluded;
     t.work = work;
-    mc::launch_trace(ctx, ctx->stream, t, bvh->layout == MC_BVH_LAYOUT_WIDE4, false, intersector, !plain, (n + 255) / 256);
+    mc::launch_trace(ctx, ctx->stream, t, bvh->layout, false, intersector, !plain, (n + 255) / 256);
     MC_CUDA(cudaGetLastError());
     int flags = 0;
     MC_CUDA(cudaMemcpyAsync(&flags, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

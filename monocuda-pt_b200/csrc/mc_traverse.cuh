@@ -180,13 +180,42 @@ MC_D void cswap(float& ka, int& va, float& kb, int& vb) {
     }
 }
 
-template <bool ANY, int ISECT, bool COUNT = false, class Stack = LocalStack>
+// Child planes of a quantised node (MC_BVH_LAYOUT_WIDE4Q): plane = origin +
+// byte * 2^e, one byte per child in each word.
+MC_D float4 q_planes(float origin, float scale, unsigned bytes) {
+    return make_float4(fmaf((float)(bytes & 0xFFu), scale, origin), fmaf((float)((bytes >> 8) & 0xFFu), scale, origin),
+                       fmaf((float)((bytes >> 16) & 0xFFu), scale, origin), fmaf((float)(bytes >> 24), scale, origin));
+}
+
+MC_D float q_scale(unsigned exps, int axis) {
+    const int e = (int)((exps >> (8 * axis)) & 0xFFu) - 128;
+    return __int_as_float((e + 127) << 23);
+}
+
+// QUANT: 64-byte quantised nodes with conservative boxes (more boxes pass; the
+// leaf tests and the rank rule decide the hit as with exact boxes).
+template <bool ANY, int ISECT, bool COUNT = false, class Stack = LocalStack, bool QUANT = false>
 MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
                     TravCount* cnt = nullptr) {
-    const float4* nd = sc.nodes + (long long)s.node * 8;
-    float4 lx = ldg4(nd + 0), ly = ldg4(nd + 1), lz = ldg4(nd + 2);
-    float4 hx = ldg4(nd + 3), hy = ldg4(nd + 4), hz = ldg4(nd + 5);
-    float4 rf = ldg4(nd + 6);
+    float4 lx, ly, lz, hx, hy, hz, rf;
+    if (QUANT) {
+        const float4* nd = sc.nodes + (long long)s.node * 4;
+        const float4 h = ldg4(nd + 0), q0 = ldg4(nd + 1), q1 = ldg4(nd + 2);
+        rf = ldg4(nd + 3);
+        const unsigned ex = (unsigned)__float_as_int(h.w);
+        const float sx = q_scale(ex, 0), sy = q_scale(ex, 1), sz = q_scale(ex, 2);
+        lx = q_planes(h.x, sx, (unsigned)__float_as_int(q0.x));
+        ly = q_planes(h.y, sy, (unsigned)__float_as_int(q0.y));
+        lz = q_planes(h.z, sz, (unsigned)__float_as_int(q0.z));
+        hx = q_planes(h.x, sx, (unsigned)__float_as_int(q0.w));
+        hy = q_planes(h.y, sy, (unsigned)__float_as_int(q1.x));
+        hz = q_planes(h.z, sz, (unsigned)__float_as_int(q1.y));
+    } else {
+        const float4* nd = sc.nodes + (long long)s.node * 8;
+        lx = ldg4(nd + 0); ly = ldg4(nd + 1); lz = ldg4(nd + 2);
+        hx = ldg4(nd + 3); hy = ldg4(nd + 4); hz = ldg4(nd + 5);
+        rf = ldg4(nd + 6);
+    }
     int ref[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z), __float_as_int(rf.w)};
     float tn[4];
     bool hit[4];
@@ -264,10 +293,12 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, cons
     return STEP_CONTINUE;
 }
 
-template <bool ANY, int ISECT, bool COUNT, bool WIDE, class Stack>
+// LAY: MC_BVH_LAYOUT_BINARY, _WIDE4 or _WIDE4Q.
+template <bool ANY, int ISECT, bool COUNT, int LAY, class Stack>
 MC_D int trav_step_layout(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
                           TravCount* cnt) {
-    if (WIDE) return trav_step4<ANY, ISECT, COUNT, Stack>(sc, s, stack, w, err, cnt);
+    if (LAY == MC_BVH_LAYOUT_WIDE4Q) return trav_step4<ANY, ISECT, COUNT, Stack, true>(sc, s, stack, w, err, cnt);
+    if (LAY == MC_BVH_LAYOUT_WIDE4) return trav_step4<ANY, ISECT, COUNT, Stack, false>(sc, s, stack, w, err, cnt);
     return trav_step<ANY, ISECT, COUNT, Stack>(sc, s, stack, w, err, cnt);
 }
 

@@ -20,7 +20,7 @@ TEX_SOLID, TEX_CHECKER, TEX_IMAGE = 0, 1, 2
 RNG_PHILOX, RNG_XORWOW = 0, 1
 ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
 TRACE_PLAIN = 0x100
-LAYOUT_BINARY, LAYOUT_WIDE4 = 0, 1
+LAYOUT_BINARY, LAYOUT_WIDE4, LAYOUT_WIDE4Q = 0, 1, 2
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
 SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64

@@ -20,7 +20,7 @@ torch = pytest.importorskip("torch")
 
 CORNELL, ICO, SPHERES = mcpt.SCENE_CORNELL_BOXES, mcpt.SCENE_DISPLACED_ICOSPHERES, mcpt.SCENE_CORNELL_SPHERES
 CASES = [(CORNELL, 0), (ICO, 5), (SPHERES, 0)]
-LAYOUTS = [mcpt.LAYOUT_BINARY, mcpt.LAYOUT_WIDE4]
+LAYOUTS = [mcpt.LAYOUT_BINARY, mcpt.LAYOUT_WIDE4, mcpt.LAYOUT_WIDE4Q]
 
 
 @pytest.fixture(scope="module")
@@ -287,20 +287,23 @@ def test_full_size_wide_matches_binary(ctx):
     perm = dev(r["perm"])
     b2 = mcpt.Bvh(ctx, ds.view, permutation=perm, layout=mcpt.LAYOUT_BINARY)
     b4 = mcpt.Bvh(ctx, ds.view, permutation=perm, layout=mcpt.LAYOUT_WIDE4)
-    i4 = b4.info()
+    bq = mcpt.Bvh(ctx, ds.view, permutation=perm, layout=mcpt.LAYOUT_WIDE4Q)
+    i4, iq = b4.info(), bq.info()
     assert i4.layout == mcpt.LAYOUT_WIDE4 and i4.node_bytes <= 1.05 * b2.info().node_bytes
+    assert iq.layout == mcpt.LAYOUT_WIDE4Q and 2 * iq.node_bytes == i4.node_bytes
     rays = np.ascontiguousarray(np.concatenate([primary_rays(s.camera, s.width, s.height, stride=1),
                                                 random_rays(1000000, -3.0, 3.0, seed=5)], axis=1))
     n = rays.shape[1]
     d_rays = dev(rays)
     res = []
-    for b, flags in ((b2, 0), (b4, 0), (b4, mcpt.TRACE_PLAIN)):
+    for b, flags in ((b2, 0), (b4, 0), (b4, mcpt.TRACE_PLAIN), (bq, 0)):
         h = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
         mcpt.check(ctx.lib.mc_trace_closest(ctx.handle, b.handle, C.byref(ds.view), d_rays.data_ptr(), n,
                                             mcpt.ISECT_REFERENCE | flags, h.data_ptr()))
         res.append(h.cpu().numpy())
     assert np.array_equal(res[0], res[1])
     assert np.array_equal(res[1], res[2])
+    assert np.array_equal(res[1], res[3]), "quantised boxes changed %d hits" % int((res[1] != res[3]).any(axis=1).sum())
 
 
 def test_edge_case_scenes(ctx):
