@@ -367,7 +367,7 @@ struct ShadeArgs {
 };
 
 // Per-path training record of the primary vertex: position, ray direction,
-// sampled direction, weight, valid flag, spare.
+// sampled direction, weight, valid flag, MIS remainder of depth-1 emission.
 constexpr int kRecFloats = 12;
 
 struct ShadeOut {
@@ -424,6 +424,19 @@ MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w) {
     return (1.0f - frac) * (c / MC_PI) + frac * guide::mixture_pdf(m, w.x, w.y, w.z);
 }
 
+// Guided renders: a primary-vertex record must see all the light that arrives
+// along its sampled direction. Emission (or environment) found at depth 1 by
+// that direction enters the image with its MIS weight w; the part (1 - w) that
+// NEE's side of the MIS carries instead is kept in the record's spare slot and
+// added to its weight. Without it a broad early guide, whose density is tiny
+// next to the light's, would never be pulled toward a small light.
+MC_D void train_remainder(const ShadeArgs& a, int p, const V3& L, float w) {
+    if (w >= 1.0f) return;
+    float* r = a.rec + (size_t)p * kRecFloats;
+    if (r[10] == 0.0f) return;
+    r[11] = (L.x + L.y + L.z) * (1.0f / 3.0f) * (1.0f - w);
+}
+
 // PT:3470-3696 shadeKernel for one path. GUIDED: diffuse vertices sample the
 // next direction by one-sample MIS of the cosine lobe and the guide.
 template <class Rng, bool GUIDED>
@@ -442,7 +455,9 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         float envProb = env_selection_probability(S.env, lightCount);
         if (!(depth == 0 || a.spec[p] != 0) && envProb > 0.0f)
             envW = power_heuristic(a.pdf[p], envProb * env_direction_pdf(S.env, missDir));
-        cs = cs + throughput * env_radiance(S.env, missDir, background) * envW;
+        const V3 envL = throughput * env_radiance(S.env, missDir, background);
+        cs = cs + envL * envW;
+        if (GUIDED && a.rec && depth == 1) train_remainder(a, p, envL, envW);
         a.sr[p] = cs.x;
         a.sg[p] = cs.y;
         a.sb[p] = cs.z;
@@ -492,6 +507,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             emissionWeight = power_heuristic(a.pdf[p], lightPdf);
         }
         cs = cs + throughput * mat.emitted * emissionWeight;
+        if (GUIDED && a.rec && depth == 1) train_remainder(a, p, throughput * mat.emitted, emissionWeight);
         a.sr[p] = cs.x;
         a.sg[p] = cs.y;
         a.sb[p] = cs.z;
@@ -654,7 +670,10 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
         if (q < count) {
             p = a.queue[q];
             const SceneGPU& S = a.tab->scenes[scene_of(a.tab, a.sceneOf, p)];
-            if (GUIDED && a.rec && a.depth == 0) a.rec[(size_t)p * kRecFloats + 10] = 0.0f;
+            if (GUIDED && a.rec && a.depth == 0) {
+                a.rec[(size_t)p * kRecFloats + 10] = 0.0f;
+                a.rec[(size_t)p * kRecFloats + 11] = 0.0f;
+            }
             shade_path<Rng, GUIDED>(a, S, p, out);
         }
         int ns = warp_reserve(out.shadow, a.shCount, ltmask);
@@ -782,7 +801,7 @@ __global__ void k_finalize_guided(const WaveTable* tab, const float* sr, const f
             acc[1] = acc[1] + s.y;
             acc[2] = acc[2] + s.z;
             if (rec && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
-                w = (smp.x + smp.y + smp.z) * (1.0f / 3.0f);
+                w = (smp.x + smp.y + smp.z) * (1.0f / 3.0f) + rec[(size_t)p * kRecFloats + 11];
                 emit = w > 0.0f && w < 1e30f;
             }
         }
