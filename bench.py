@@ -3,7 +3,8 @@
 Workload: the "displaced_icospheres" scene (3 level-8 displaced icospheres =
 3,932,160 triangles + ground, medium box, area light, 2048x1024 procedural sky),
 1920x1080, max depth 8, counter-based RNG. One step = one sample of every pixel
-(a full wave of 2,073,600 paths through up to 8 bounces); K steps = K spp.
+(a full wave of 2,073,600 paths through up to 8 bounces); K steps = K spp
+(default 64, about half a second of timed work).
 Mrays/s = (extend rays + shadow rays) / device time, rays counted on the device.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -40,7 +41,7 @@ NODE_BYTES, LEAF_BYTES, EXT_IO_BYTES, SHADOW_IO_BYTES = 64, 48, 48, 72
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = the named workload)")
@@ -84,7 +85,7 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
@@ -177,18 +178,21 @@ def cpu_baseline(scene, args):
     orc.orc_render(h, C.addressof(cam), W, H, 1, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
                    stats.ctypes.data)
     dt = time.perf_counter() - t0
-    rows = max(8, min(H, int(rows * args.cpu_seconds / max(dt, 1e-3))))
+    # size the sample to about --cpu-seconds: more rows first, then more samples per pixel
+    per_row = max(dt, 1e-4) / rows
+    rows = max(8, min(H, int(args.cpu_seconds / per_row)))
+    spp = max(1, int(round(args.cpu_seconds / (per_row * rows)))) if rows == H else 1
     y0 = max(0, H // 2 - rows // 2)
     acc[:] = 0
     t0 = time.perf_counter()
-    orc.orc_render(h, C.addressof(cam), W, H, 1, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
+    orc.orc_render(h, C.addressof(cam), W, H, spp, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
                    stats.ctypes.data)
     dt = time.perf_counter() - t0
     orc.orc_scene_destroy(h)
     rays = stats[0] + stats[1]
     return {"value": round(rays / dt / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "port",
-            "sample": "%d rows x %d px x 1 spp of the same workload (FP32 oracle, %d threads, %.1f s, %d rays)"
-                      % (rows, W, threads, dt, int(rays))}
+            "sample": "%d rows x %d px x %d spp of the same workload (FP32 oracle, %d threads, %.1f s, %d rays)"
+                      % (rows, W, spp, threads, dt, int(rays))}
 
 
 def run_ours(args):
