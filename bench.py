@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--guide-steps", type=int, default=4, help="Adam steps per sample, each on 65536 records")
     ap.add_argument("--mlp-items", type=int, default=1 << 20)
     ap.add_argument("--server-rates", type=float, nargs="+", default=[1, 4, 16, 64], help="arrival rates (requests/s)")
-    ap.add_argument("--server-requests", type=int, default=24, help="requests per arrival rate")
+    ap.add_argument("--server-requests", type=int, default=64,
+                    help="requests per arrival rate (at most; max(24, 16 x rate) at low rates)")
     ap.add_argument("--server-sps", type=int, default=4, help="samples per server step")
     ap.add_argument("--server-wave-paths", type=int, default=0, help="paths per server wave (0 = 4M)")
     return ap.parse_args()
@@ -690,8 +691,11 @@ def run_server(args):
     serve(warm)
     baseline([(0.0, k, 256, 256, 1, False) for k in range(len(scenes))])
     points = []
-    for i, rate in enumerate(args.server_rates):
-        tr = trace(rate, args.server_requests, 5 + i)
+    for rate in args.server_rates:
+        # the same trace for a rate whatever else is swept; fewer requests at low
+        # rates, where the arrivals themselves take wall-clock time
+        n_req = max(24, min(args.server_requests, int(16 * rate)))
+        tr = trace(rate, n_req, 5 + int(round(rate * 1000)))
         lat, mr = serve(tr)
         plain_tr = [(t, k, W, H, spp, False) for t, k, W, H, spp, _ in tr]
         plat, pmr = serve(plain_tr)

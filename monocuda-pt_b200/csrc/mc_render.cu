@@ -775,16 +775,15 @@ __global__ void k_finalize(const WaveTable* tab, const unsigned short* sceneOf, 
     }
 }
 
-// Guided renders (one scene): the sample plus the primary vertex's NEE goes
+// Guided renders (one scene, one or more images): the sample plus the primary vertex's NEE goes
 // to the image; a primary-vertex record takes the sample without that NEE
 // (the radiance carried back through its sampled direction over that
 // direction's density) as its weight, and records of positive weight are
 // appended to the training batch.
-__global__ void k_finalize_guided(const WaveTable* tab, const float* sr, const float* sg, const float* sb, const float* nr,
-                                  const float* ng, const float* nb, const float* rec, float* batch, int* batchCount,
-                                  int capacity) {
+__global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sceneOf, const float* sr, const float* sg,
+                                  const float* sb, const float* nr, const float* ng, const float* nb, const float* rec,
+                                  float* batch, int* batchCount, int capacity) {
     const unsigned ltmask = lanemask_lt();
-    const SceneGPU& S = tab->scenes[0];
     const int total = tab->totalPaths;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -792,11 +791,12 @@ __global__ void k_finalize_guided(const WaveTable* tab, const float* sr, const f
         bool emit = false;
         float w = 0.f;
         if (p < total) {
+            const SceneGPU& S = tab->scenes[scene_of(tab, sceneOf, p)];
             V3 smp(sr[p], sg[p], sb[p]);
             V3 s = smp + V3(nr[p], ng[p], nb[p]);
             float bright = fmaxf(s.x, fmaxf(s.y, s.z));
             if (!S.disableClamp && bright > 10.0f) s = s * (10.0f / bright);
-            float* acc = S.accum + (size_t)p * 3;
+            float* acc = S.accum + (size_t)(p - S.pathOffset) * 3;
             acc[0] = acc[0] + s.x;
             acc[1] = acc[1] + s.y;
             acc[2] = acc[2] + s.z;
@@ -1158,7 +1158,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             launches++;
         }
         if (guide) {
-            k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
+            k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
                                                               train ? guide->records : nullptr, guide->batch,
                                                               guide->batch_count,
                                                               guide->cfg.batch_capacity * guide->cfg.train_steps);

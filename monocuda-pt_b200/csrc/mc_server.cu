@@ -238,28 +238,48 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
         s->waves += w;
         for (size_t i = 0; i < ids.size(); i++) s->requests[ids[i]].done += params[i].spp;
     }
-    // guided requests: their scene's guided render, training the scene's guide
-    for (long long id : chosen) {
-        ServerRequest& r = s->requests[id];
-        if (!r.guided) continue;
-        ServerScene& sc = s->scenes[(size_t)r.scene];
+    // guided requests: the ones of each scene share waves and the scene's
+    // guide, which trains on all of their primary vertices
+    std::map<long long, std::vector<long long>> guidedByScene;
+    for (long long id : chosen)
+        if (s->requests[id].guided) guidedByScene[s->requests[id].scene].push_back(id);
+    for (auto& kv : guidedByScene) {
+        ServerScene& sc = s->scenes[(size_t)kv.first];
         if (!sc.guide) {
             mc_guide_config gc;
             std::memset(&gc, 0, sizeof(gc));
             gc.bounds = sc.bvh->bounds;
-            gc.seed = (uint64_t)r.scene + 1;
+            gc.seed = (uint64_t)kv.first + 1;
             if ((st = mc_guide_create(s->ctx, &gc, &sc.guide)) != MC_OK) return st;
         }
-        mc_render_params p = r.params;
-        p.first_sample = r.params.first_sample + r.done;
-        p.spp = std::min(sps, r.params.spp - r.done);
-        p.use_graph = 0;
-        p.instrument = 0;
+        std::vector<mc_render_params> gp;
+        std::vector<mc::WaveItem> gi;
+        gp.reserve(kv.second.size());
+        int paths = 0, w = 0;
+        for (long long id : kv.second) {
+            ServerRequest& r = s->requests[id];
+            mc_render_params p = r.params;
+            p.first_sample = r.params.first_sample + r.done;
+            p.spp = std::min(sps, r.params.spp - r.done);
+            p.use_graph = 0;
+            p.instrument = 0;
+            gp.push_back(p);
+            paths += p.width * p.height;
+            w = std::max(w, p.spp);
+        }
+        for (size_t i = 0; i < kv.second.size(); i++) {
+            ServerRequest& r = s->requests[kv.second[i]];
+            mc::WaveItem it{&sc.view, &gp[i], r.accum, sc.bvh->wide_roots[0], 0};
+            it.bvh = sc.bvh;
+            gi.push_back(it);
+        }
+        if ((st = mc::guide_reserve_paths(sc.guide, paths)) != MC_OK) return st;
         mc_render_stats rs;
-        if ((st = mc_render_guided(s->ctx, sc.bvh, &sc.view, &p, sc.guide, 1, r.accum, &rs)) != MC_OK) return st;
+        st = mc::render_items(s->ctx, sc.bvh, gi.data(), (int)gi.size(), false, &rs, sc.guide, true);
+        if (st != MC_OK) return st;
         s->rays += rs.extend_rays + rs.shadow_rays;
-        s->waves += p.spp;
-        r.done += p.spp;
+        s->waves += w;
+        for (size_t i = 0; i < kv.second.size(); i++) s->requests[kv.second[i]].done += gp[i].spp;
     }
     // retire finished requests (their buffers stay until released)
     const double t = s->now();

@@ -102,12 +102,13 @@ def test_guided_and_plain_requests_together(ctx):
     srv = mcpt.Server(ctx, samples_per_step=4)
     sid = srv.add_scene(d)
     g = srv.submit(sid, _params(s, 64, 8), guided=True)
+    g2 = srv.submit(sid, _params(s, 48, 6), guided=True)  # shares the first one's waves and guide
     p = srv.submit(sid, _params(s, 64, 8))
     _drain(srv)
-    for rid in (g, p):
+    for rid, W, spp in ((g, 64, 8), (g2, 48, 6), (p, 64, 8)):
         r = srv.result(rid)
-        assert r.state == mcpt.REQ_DONE and r.spp_done == 8
-        host = srv.read(rid, 64, 64)
+        assert r.state == mcpt.REQ_DONE and r.spp_done == spp
+        host = srv.read(rid, W, W)
         assert np.isfinite(host).all() and host.sum() > 0
     assert srv.stats().rays > 0
     srv.close()
