@@ -313,6 +313,19 @@ MC_API mc_status mc_camera_initialize(mc_camera* cam);
 MC_API mc_status mc_scene_finalize_host(mc_triangle* tris, int32_t n, mc_light* lights, int32_t* light_count);
 /* Splits host triangles into hot/cold records (PT:4276-4281). Host arrays. */
 MC_API mc_status mc_split_triangles_host(const mc_triangle* tris, int32_t n, mc_triangle_hot* hot, mc_triangle_cold* cold);
+/* Scene ingestion on the device: the triangle bounds and emissive-triangle
+ * light list of finalizeScene (PT:1930-1987) and main()'s hot/cold split
+ * (PT:4276-4289) as kernels, byte-identical to mc_scene_finalize_host followed
+ * by mc_split_triangles_host. tris (n AoS records), hot and cold are device
+ * arrays, 16-byte aligned; tris is not modified. lights: device array with
+ * room for every emissive triangle (n is always enough), or NULL to only count.
+ * spheres (device, n_sph records, may be NULL when n_sph is 0) are scanned for
+ * media. light_count and has_medium (a material of type MC_MAT_ISOTROPIC on any
+ * primitive) are host outputs and may be NULL; the call synchronizes the
+ * context's stream to read them. */
+MC_API mc_status mc_scene_ingest(mc_context* ctx, const mc_triangle* tris, int32_t n, const mc_sphere* spheres,
+                                 int32_t n_sph, mc_triangle_hot* hot, mc_triangle_cold* cold, mc_light* lights,
+                                 int32_t* light_count, int32_t* has_medium);
 
 /* Environment map from a host float RGBA image (top row first), with the
  * sampling tables of buildEnvironmentSamplingTables (PT:370-385). Creates the

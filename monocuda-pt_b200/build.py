@@ -4,6 +4,8 @@
 Per-file flags:
   mc_bvh.cu     -O3 -fmad=false, IEEE division: the Morton codes must equal the
                 reference's host (IEEE, no contraction) computation bit for bit.
+  mc_ingest.cu  the same IEEE flags: light areas and normals equal the
+                reference's host computation bit for bit.
   mc_render.cu  -O3 --use_fast_math: the reference's release flags
                 (CMakeLists.txt:88-96), which the per-ray arithmetic must match.
   other .cu     -O3
@@ -36,6 +38,7 @@ UNITS = {
     "mc_batch.cu": ["-O3", "--use_fast_math"],
     "mc_guide.cu": ["-O3"],
     "mc_server.cu": ["-O3"],
+    "mc_ingest.cu": ["-O3", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
 }
 HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"]}
 

@@ -22,42 +22,40 @@ mc_status ensure_wave(mc_context* ctx, int capacity);
 
 extern "C" {
 
-// The whole reference flow from host arrays (PT:4223-4336): finalize + light
-// list, hot/cold split, upload, BVH build, render, accumulation read-back.
+// The whole reference flow from host arrays (PT:4223-4336): upload of the AoS
+// triangles, then on the device finalize + light list + hot/cold split
+// (mc_scene_ingest), BVH build, render, accumulation read-back.
 mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_t n_tri, const mc_sphere* spheres, int32_t n_sph,
                          const mc_env_map* env, const mc_render_params* params, float* accum_host, mc_render_stats* stats) {
     if (!ctx || !params || !accum_host || n_tri < 0 || n_sph < 0 || (n_tri > 0 && !tris) || (n_sph > 0 && !spheres))
         return mc::set_error(MC_ERR_INVALID, "mc_render_host: bad argument");
     if (n_tri + n_sph == 0) return mc::set_error(MC_ERR_INVALID, "mc_render_host: the scene has no primitives");
-    std::vector<mc_triangle> t(tris, tris + n_tri);
-    int32_t nl = 0;
-    mc_scene_finalize_host(t.data(), n_tri, nullptr, &nl);
-    std::vector<mc_light> lights((size_t)(nl > 0 ? nl : 1));
-    mc_scene_finalize_host(t.data(), n_tri, lights.data(), &nl);
-    std::vector<mc_triangle_hot> hot((size_t)(n_tri > 0 ? n_tri : 1));
-    std::vector<mc_triangle_cold> cold((size_t)(n_tri > 0 ? n_tri : 1));
-    mc_split_triangles_host(t.data(), n_tri, hot.data(), cold.data());
-    int hasMedium = 0;
-    for (const auto& x : t) if (x.mat.type == MC_MAT_ISOTROPIC) hasMedium = 1;
-    for (int i = 0; i < n_sph; i++) if (spheres[i].mat.type == MC_MAT_ISOTROPIC) hasMedium = 1;
-
+    const size_t nt = (size_t)(n_tri > 0 ? n_tri : 1);
+    mc_triangle* dTri = nullptr;
     mc_triangle_hot* dHot = nullptr; mc_triangle_cold* dCold = nullptr; mc_sphere* dSph = nullptr; mc_light* dL = nullptr;
     float* dAcc = nullptr;
     size_t accBytes = (size_t)params->width * params->height * 3 * sizeof(float);
-    auto cleanup = [&]() { cudaFree(dHot); cudaFree(dCold); cudaFree(dSph); cudaFree(dL); cudaFree(dAcc); };
-    if (cudaMalloc(&dHot, hot.size() * sizeof(mc_triangle_hot)) != cudaSuccess ||
-        cudaMalloc(&dCold, cold.size() * sizeof(mc_triangle_cold)) != cudaSuccess ||
+    auto cleanup = [&]() { cudaFree(dTri); cudaFree(dHot); cudaFree(dCold); cudaFree(dSph); cudaFree(dL); cudaFree(dAcc); };
+    if (cudaMalloc(&dTri, nt * sizeof(mc_triangle)) != cudaSuccess ||
+        cudaMalloc(&dHot, nt * sizeof(mc_triangle_hot)) != cudaSuccess ||
+        cudaMalloc(&dCold, nt * sizeof(mc_triangle_cold)) != cudaSuccess ||
         cudaMalloc(&dSph, (size_t)(n_sph > 0 ? n_sph : 1) * sizeof(mc_sphere)) != cudaSuccess ||
-        cudaMalloc(&dL, lights.size() * sizeof(mc_light)) != cudaSuccess || cudaMalloc(&dAcc, accBytes) != cudaSuccess) {
+        cudaMalloc(&dL, nt * sizeof(mc_light)) != cudaSuccess || cudaMalloc(&dAcc, accBytes) != cudaSuccess) {
         cudaGetLastError();
         cleanup();
         return mc::set_error(MC_ERR_OOM, "mc_render_host: device allocation failed");
     }
-    cudaMemcpyAsync(dHot, hot.data(), (size_t)n_tri * sizeof(mc_triangle_hot), cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(dCold, cold.data(), (size_t)n_tri * sizeof(mc_triangle_cold), cudaMemcpyHostToDevice, ctx->stream);
+    if (n_tri) cudaMemcpyAsync(dTri, tris, (size_t)n_tri * sizeof(mc_triangle), cudaMemcpyHostToDevice, ctx->stream);
     if (n_sph) cudaMemcpyAsync(dSph, spheres, (size_t)n_sph * sizeof(mc_sphere), cudaMemcpyHostToDevice, ctx->stream);
-    if (nl) cudaMemcpyAsync(dL, lights.data(), (size_t)nl * sizeof(mc_light), cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(dAcc, accum_host, accBytes, cudaMemcpyHostToDevice, ctx->stream);
+    int32_t nl = 0, hasMedium = 0;
+    mc_status st0 = mc_scene_ingest(ctx, dTri, n_tri, dSph, n_sph, dHot, dCold, dL, &nl, &hasMedium);
+    cudaFree(dTri);  // the AoS records are not needed past the split
+    dTri = nullptr;
+    if (st0 != MC_OK) {
+        cleanup();
+        return st0;
+    }
     mc_scene_view view;
     std::memset(&view, 0, sizeof(view));
     view.spheres = dSph; view.sphere_count = n_sph;

@@ -198,6 +198,7 @@ SIGNATURES = {
     "mc_camera_initialize": (I32, [C.POINTER(Camera)]),
     "mc_scene_finalize_host": (I32, [P, I32, P, C.POINTER(I32)]),
     "mc_split_triangles_host": (I32, [P, I32, P, P]),
+    "mc_scene_ingest": (I32, [P, P, I32, P, I32, P, P, P, C.POINTER(I32), C.POINTER(I32)]),
     "mc_env_create": (I32, [P, I32, I32, C.c_float, C.c_float, C.POINTER(EnvMap)]),
     "mc_env_destroy": (I32, [C.POINTER(EnvMap)]),
     "mc_scene_generate": (I32, [C.POINTER(SceneDesc), C.POINTER(SceneHost)]),
@@ -392,15 +393,41 @@ def host_env(scene):
 class DeviceScene:
     """Uploads host triangles/spheres the way the reference's main() does
     (PT:4276-4303): hot/cold split, light list, environment texture. Device
-    memory comes from torch (plumbing only); the view is an mc_scene_view."""
+    memory comes from torch (plumbing only); the view is an mc_scene_view.
 
-    def __init__(self, triangles, spheres=None, env_rgba=None, env_intensity=1.0, env_rotation=0.0, device="cuda"):
+    With a Context (`ctx`), the AoS triangles are uploaded as they are and the
+    bounds, light list and split run on the device (mc_scene_ingest); without
+    one they run on the host (mc_scene_finalize_host, mc_split_triangles_host).
+    Both give the same bytes."""
+
+    def __init__(self, triangles, spheres=None, env_rgba=None, env_intensity=1.0, env_rotation=0.0, device="cuda",
+                 ctx=None):
         import numpy as np
         import torch
         lib = load()
         self.lib = lib
         n = len(triangles)
         ns = len(spheres) if spheres is not None else 0
+
+        def up(arr, count, size):
+            b = np.frombuffer(arr, dtype=np.uint8, count=max(count, 1) * size).copy()
+            return torch.from_numpy(b).to(device)
+        self.spheres = up(spheres, ns, 160) if ns else torch.zeros(160, dtype=torch.uint8, device=device)
+        if ctx is not None:
+            src = torch.frombuffer(triangles, dtype=torch.uint8, count=n * 224) if n else torch.zeros(224, dtype=torch.uint8)
+            aos = src.to(device)
+            self.hot = torch.empty(max(n, 1) * 36, dtype=torch.uint8, device=device)
+            self.cold = torch.empty(max(n, 1) * 192, dtype=torch.uint8, device=device)
+            self.lights = torch.empty(max(n, 1) * 64, dtype=torch.uint8, device=device)
+            nl, med = I32(), I32()
+            torch.cuda.synchronize()
+            check(lib.mc_scene_ingest(ctx.handle, aos.data_ptr(), n, self.spheres.data_ptr() if ns else None, ns,
+                                      self.hot.data_ptr(), self.cold.data_ptr(), self.lights.data_ptr(),
+                                      C.byref(nl), C.byref(med)))
+            del aos
+            self.light_count = nl.value
+            self._finish(n, ns, nl.value, bool(med.value), env_rgba, env_intensity, env_rotation)
+            return
         hot = (TriangleHot * max(n, 1))()
         cold = (TriangleCold * max(n, 1))()
         tri_addr = C.addressof(triangles) if n else None
@@ -414,19 +441,20 @@ class DeviceScene:
         check(lib.mc_scene_finalize_host(C.addressof(tcopy), n, C.addressof(lights), C.byref(nl)))
         self.light_count = nl.value
 
-        def up(arr, count, size):
-            b = np.frombuffer(arr, dtype=np.uint8, count=max(count, 1) * size).copy()
-            return torch.from_numpy(b).to(device)
         self.hot = up(hot, n, 36)
         self.cold = up(cold, n, 192)
         self.lights = up(lights, nl.value, 64)
-        self.spheres = up(spheres, ns, 160) if ns else torch.zeros(160, dtype=torch.uint8, device=device)
         medium = any(triangles[i].mat.type == MAT_ISOTROPIC for i in range(n)) if n < 100000 else None
         if medium is None:
             mt = np.frombuffer(triangles, dtype=np.uint8).reshape(n, 224)[:, 96:100].copy().view(np.int32).ravel()
             medium = bool((mt == MAT_ISOTROPIC).any())
         if ns and any(spheres[i].mat.type == MAT_ISOTROPIC for i in range(ns)):
             medium = True
+        self._finish(n, ns, nl.value, medium, env_rgba, env_intensity, env_rotation)
+
+    def _finish(self, n, ns, nl, medium, env_rgba, env_intensity, env_rotation):
+        import numpy as np
+        lib = self.lib
         self.env = EnvMap()
         if env_rgba is not None:
             e = np.ascontiguousarray(env_rgba, dtype=np.float32)
@@ -441,7 +469,7 @@ class DeviceScene:
         v.tri_cold = self.cold.data_ptr()
         v.triangle_count = n
         v.lights = self.lights.data_ptr()
-        v.light_count = nl.value
+        v.light_count = nl
         v.has_medium = 1 if medium else 0
         v.env = self.env
         self.view = v

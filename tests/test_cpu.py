@@ -297,3 +297,31 @@ def test_primary_rays_helper_matches_camera():
     assert r.shape == (7, 64)
     assert np.allclose(np.linalg.norm(r[3:6], axis=0), 1.0, atol=1e-6)
     mcpt.free_scene(s)
+
+
+def test_host_finalize_matches_reference_on_random_soup():
+    """mc_scene_finalize_host against the reference's finalizeScene on 5,000
+    random triangles, 30 % emissive: bounds and the light list bit-exact."""
+    rng = np.random.default_rng(11)
+    s = _scene("ico3")
+    src = np.frombuffer(mcpt.host_triangles(s), np.uint8).reshape(-1, 224)
+    n = 5000
+    a = src[rng.integers(0, len(src), n)].copy()
+    a[:, 0:36] = rng.uniform(-1, 1, (n, 9)).astype(np.float32).view(np.uint8)
+    a[:, 96:100] = np.where(rng.random(n) < 0.3, mcpt.MAT_EMISSIVE, 0).astype(np.int32).view(np.uint8).reshape(n, 4)
+    mcpt.free_scene(s)
+    tris = (mcpt.Triangle * n)()
+    C.memmove(tris, a.ctypes.data, n * 224)
+    tb = np.zeros(n * 8, np.float32)
+    rl = np.zeros(n * 16, np.float32)
+    rn = C.c_int32()
+    assert mcref.load(False).mcref_finalize_and_sort(C.addressof(tris), n, None, 0, None, None, None, None, None, None,
+                                                     None, tb.ctypes.data, rl.ctypes.data, C.byref(rn)) == 0
+    hl = (mcpt.Light * n)()
+    hn = C.c_int32()
+    mcpt.check(mcpt.load().mc_scene_finalize_host(C.addressof(tris), n, C.addressof(hl), C.byref(hn)))
+    assert hn.value == rn.value > 1000
+    assert np.frombuffer(hl, np.uint8)[:hn.value * 64].tobytes() == rl.view(np.uint8)[:rn.value * 64].tobytes()
+    boxes = np.frombuffer(tris, np.uint8).reshape(n, 224)[:, 192:224].copy().view(np.float32)
+    lanes = [0, 1, 2, 4, 5, 6]
+    assert np.array_equal(boxes[:, lanes].view(np.uint32), tb.reshape(n, 8)[:, lanes].view(np.uint32))
