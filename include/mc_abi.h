@@ -326,6 +326,12 @@ MC_API mc_status mc_split_triangles_host(const mc_triangle* tris, int32_t n, mc_
 MC_API mc_status mc_scene_ingest(mc_context* ctx, const mc_triangle* tris, int32_t n, const mc_sphere* spheres,
                                  int32_t n_sph, mc_triangle_hot* hot, mc_triangle_cold* cold, mc_light* lights,
                                  int32_t* light_count, int32_t* has_medium);
+/* mc_scene_ingest from a HOST array of AoS triangles (pageable or pinned):
+ * uploads it (large pageable arrays through pinned staging filled by several
+ * host threads), then ingests on the device. Other arguments as above. */
+MC_API mc_status mc_scene_ingest_host(mc_context* ctx, const mc_triangle* tris, int32_t n, const mc_sphere* spheres,
+                                      int32_t n_sph, mc_triangle_hot* hot, mc_triangle_cold* cold, mc_light* lights,
+                                      int32_t* light_count, int32_t* has_medium);
 
 /* Environment map from a host float RGBA image (top row first), with the
  * sampling tables of buildEnvironmentSamplingTables (PT:370-385). Creates the

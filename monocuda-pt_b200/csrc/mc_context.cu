@@ -134,6 +134,7 @@ mc_status mc_context_destroy(mc_context* ctx) {
     cudaFree(ctx->d_table);
     if (ctx->h_tables) cudaFreeHost(ctx->h_tables);
     cudaFree(ctx->scene_of);
+    if (ctx->staging) cudaFreeHost(ctx->staging);
     delete ctx;
     return MC_OK;
 }

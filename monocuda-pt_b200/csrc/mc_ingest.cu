@@ -248,3 +248,19 @@ extern "C" mc_status mc_scene_ingest(mc_context* ctx, const mc_triangle* tris, i
     if (has_medium) *has_medium = h[0] & 1;
     return MC_OK;
 }
+
+extern "C" mc_status mc_scene_ingest_host(mc_context* ctx, const mc_triangle* tris, int32_t n, const mc_sphere* spheres,
+                                          int32_t n_sph, mc_triangle_hot* hot, mc_triangle_cold* cold, mc_light* lights,
+                                          int32_t* light_count, int32_t* has_medium) {
+    using namespace mc;
+    if (!ctx || n < 0 || (n > 0 && !tris)) return set_error(MC_ERR_INVALID, "mc_scene_ingest_host: bad arguments");
+    mc_triangle* dTri = nullptr;
+    if (n > 0 && cudaMalloc(&dTri, (size_t)n * sizeof(mc_triangle)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MC_ERR_OOM, "mc_scene_ingest_host: device allocation failed");
+    }
+    mc_status st = upload_host(ctx, dTri, tris, (size_t)n * sizeof(mc_triangle));
+    if (st == MC_OK) st = mc_scene_ingest(ctx, dTri, n, spheres, n_sph, hot, cold, lights, light_count, has_medium);
+    cudaFree(dTri);
+    return st;
+}

@@ -41,6 +41,11 @@ struct DevBuf {
 mc_status devbuf_reserve(DevBuf& b, size_t bytes);
 void devbuf_free(DevBuf& b);
 
+// Copies `bytes` of host memory to the device; complete when the call returns.
+// Large copies from pageable memory go through the context's pinned staging
+// buffers, filled by several host threads while earlier pieces are in flight.
+mc_status upload_host(mc_context* ctx, void* dst, const void* src, size_t bytes);
+
 // Per-bounce counters of one sample: [d][0] extend-queue size of bounce d,
 // [d][1] shadow-queue size of bounce d, [d][2] trace work counter,
 // [d][3] medium pass-through count.
@@ -93,6 +98,8 @@ struct mc_context {
     cudaStream_t own_stream = nullptr;   // capture stream when the context has none
     void* graph_exec = nullptr;          // cached per-wave CUDA graph
     unsigned long long graph_key[16] = {};  // every value the captured launches bake in
+    void* staging = nullptr;             // pinned host staging for large pageable uploads
+    size_t staging_bytes = 0;
 };
 
 struct mc_bvh {

@@ -199,6 +199,7 @@ SIGNATURES = {
     "mc_scene_finalize_host": (I32, [P, I32, P, C.POINTER(I32)]),
     "mc_split_triangles_host": (I32, [P, I32, P, P]),
     "mc_scene_ingest": (I32, [P, P, I32, P, I32, P, P, P, C.POINTER(I32), C.POINTER(I32)]),
+    "mc_scene_ingest_host": (I32, [P, P, I32, P, I32, P, P, P, C.POINTER(I32), C.POINTER(I32)]),
     "mc_env_create": (I32, [P, I32, I32, C.c_float, C.c_float, C.POINTER(EnvMap)]),
     "mc_env_destroy": (I32, [C.POINTER(EnvMap)]),
     "mc_scene_generate": (I32, [C.POINTER(SceneDesc), C.POINTER(SceneHost)]),
@@ -396,7 +397,7 @@ class DeviceScene:
     memory comes from torch (plumbing only); the view is an mc_scene_view.
 
     With a Context (`ctx`), the AoS triangles are uploaded as they are and the
-    bounds, light list and split run on the device (mc_scene_ingest); without
+    bounds, light list and split run on the device (mc_scene_ingest_host); without
     one they run on the host (mc_scene_finalize_host, mc_split_triangles_host).
     Both give the same bytes."""
 
@@ -414,17 +415,14 @@ class DeviceScene:
             return torch.from_numpy(b).to(device)
         self.spheres = up(spheres, ns, 160) if ns else torch.zeros(160, dtype=torch.uint8, device=device)
         if ctx is not None:
-            src = torch.frombuffer(triangles, dtype=torch.uint8, count=n * 224) if n else torch.zeros(224, dtype=torch.uint8)
-            aos = src.to(device)
             self.hot = torch.empty(max(n, 1) * 36, dtype=torch.uint8, device=device)
             self.cold = torch.empty(max(n, 1) * 192, dtype=torch.uint8, device=device)
             self.lights = torch.empty(max(n, 1) * 64, dtype=torch.uint8, device=device)
             nl, med = I32(), I32()
             torch.cuda.synchronize()
-            check(lib.mc_scene_ingest(ctx.handle, aos.data_ptr(), n, self.spheres.data_ptr() if ns else None, ns,
-                                      self.hot.data_ptr(), self.cold.data_ptr(), self.lights.data_ptr(),
-                                      C.byref(nl), C.byref(med)))
-            del aos
+            check(lib.mc_scene_ingest_host(ctx.handle, C.addressof(triangles) if n else None, n,
+                                           self.spheres.data_ptr() if ns else None, ns, self.hot.data_ptr(),
+                                           self.cold.data_ptr(), self.lights.data_ptr(), C.byref(nl), C.byref(med)))
             self.light_count = nl.value
             self._finish(n, ns, nl.value, bool(med.value), env_rgba, env_intensity, env_rotation)
             return

@@ -27,21 +27,29 @@ def ctx():
     c.close()
 
 
-def ingest(ctx, tris, spheres=None):
-    """Runs mc_scene_ingest on a host triangle array; returns numpy views of
-    hot (n, 36), cold (n, 192), lights (count, 64) bytes and has_medium."""
+def ingest(ctx, tris, spheres=None, via_host=False, src_ptr=None):
+    """Runs mc_scene_ingest on a device copy of a host triangle array (or
+    mc_scene_ingest_host on the host array itself, or on src_ptr); returns
+    numpy views of hot (n, 36), cold (n, 192), lights (count, 64) bytes and
+    has_medium."""
     n = len(tris)
     ns = len(spheres) if spheres is not None else 0
-    aos = torch.frombuffer(tris, dtype=torch.uint8, count=n * 224).cuda() if n else None
+    aos = torch.frombuffer(tris, dtype=torch.uint8, count=n * 224).cuda() if n and not via_host else None
     sph = torch.frombuffer(spheres, dtype=torch.uint8, count=ns * 160).cuda() if ns else None
     hot = torch.full((max(n, 1) * 36,), 0xAB, dtype=torch.uint8, device="cuda")
     cold = torch.full((max(n, 1) * 192,), 0xAB, dtype=torch.uint8, device="cuda")
     lights = torch.full((max(n, 1) * 64,), 0xAB, dtype=torch.uint8, device="cuda")
     nl, med = C.c_int32(-1), C.c_int32(-1)
     torch.cuda.synchronize()
-    mcpt.check(mcpt.load().mc_scene_ingest(ctx.handle, aos.data_ptr() if n else None, n,
-                                           sph.data_ptr() if ns else None, ns, hot.data_ptr(), cold.data_ptr(),
-                                           lights.data_ptr(), C.byref(nl), C.byref(med)))
+    if via_host:
+        src = src_ptr if src_ptr is not None else (C.addressof(tris) if n else None)
+        mcpt.check(mcpt.load().mc_scene_ingest_host(ctx.handle, src, n, sph.data_ptr() if ns else None, ns,
+                                                    hot.data_ptr(), cold.data_ptr(), lights.data_ptr(), C.byref(nl),
+                                                    C.byref(med)))
+    else:
+        mcpt.check(mcpt.load().mc_scene_ingest(ctx.handle, aos.data_ptr() if n else None, n,
+                                               sph.data_ptr() if ns else None, ns, hot.data_ptr(), cold.data_ptr(),
+                                               lights.data_ptr(), C.byref(nl), C.byref(med)))
     return (hot.cpu().numpy()[:n * 36].reshape(n, 36), cold.cpu().numpy()[:n * 192].reshape(n, 192),
             lights.cpu().numpy()[:nl.value * 64].reshape(nl.value, 64), med.value)
 
@@ -72,8 +80,8 @@ def reference_finalize(tris, spheres=None):
     return tb[:n * 8].reshape(n, 8), lights.view(np.uint8)[:nl.value * 64].reshape(nl.value, 64)
 
 
-def check_against_reference(ctx, tris, spheres=None, expect_medium=None):
-    hot, cold, lights, med = ingest(ctx, tris, spheres)
+def check_against_reference(ctx, tris, spheres=None, expect_medium=None, via_host=False):
+    hot, cold, lights, med = ingest(ctx, tris, spheres, via_host=via_host)
     h_hot, h_cold = host_split(tris)
     assert np.array_equal(hot, h_hot), "hot records differ from the host split"
     assert np.array_equal(cold, h_cold), "cold records differ from the host split"
@@ -121,18 +129,33 @@ def soup(n, seed, emissive_frac=0.1, medium_frac=0.0):
 
 
 @pytest.mark.parametrize("n", [1, 127, 128, 129, 1000, 4097])
-def test_ingest_ragged_sizes(ctx, n):
+@pytest.mark.parametrize("via_host", [False, True])
+def test_ingest_ragged_sizes(ctx, n, via_host):
     tris, types = soup(n, seed=n, emissive_frac=0.3)
-    nl = check_against_reference(ctx, tris, expect_medium=False)
+    nl = check_against_reference(ctx, tris, expect_medium=False, via_host=via_host)
     assert nl == int((types == mcpt.MAT_EMISSIVE).sum())
 
 
-def test_ingest_many_lights_over_many_tiles(ctx):
+@pytest.mark.parametrize("via_host", [False, True])
+def test_ingest_many_lights_over_many_tiles(ctx, via_host):
     """300,000 triangles = 2,344 tiles (the offset scan runs three rounds),
-    about 10 % emissive, spread over every tile; a few isotropic ones."""
+    about 10 % emissive, spread over every tile; a few isotropic ones. From a
+    host array of 67 MB the upload goes through the pinned staging threads."""
     tris, types = soup(300000, seed=7, emissive_frac=0.1, medium_frac=0.001)
-    nl = check_against_reference(ctx, tris, expect_medium=True)
+    nl = check_against_reference(ctx, tris, expect_medium=True, via_host=via_host)
     assert nl == int((types == mcpt.MAT_EMISSIVE).sum()) > 25000
+
+
+def test_ingest_host_from_pinned_memory(ctx):
+    """A pinned host array is copied directly (no staging); same bytes."""
+    tris, types = soup(200000, seed=9, emissive_frac=0.05)
+    pinned = torch.empty(len(tris) * 224, dtype=torch.uint8, pin_memory=True)
+    pinned.copy_(torch.frombuffer(tris, dtype=torch.uint8, count=len(tris) * 224))
+    a = ingest(ctx, tris)
+    b = ingest(ctx, tris, via_host=True, src_ptr=pinned.data_ptr())
+    for x, y in zip(a[:3], b[:3]):
+        assert np.array_equal(x, y)
+    assert a[3] == b[3]
 
 
 def test_ingest_no_triangles_spheres_only(ctx):
@@ -152,6 +175,8 @@ def test_ingest_full_scene(ctx):
     hot, cold, lights, med = ingest(ctx, tris)
     h_hot, h_cold = host_split(tris)
     assert np.array_equal(hot, h_hot) and np.array_equal(cold, h_cold)
+    via = ingest(ctx, tris, via_host=True)
+    assert all(np.array_equal(x, y) for x, y in zip((hot, cold, lights), via[:3])) and via[3] == med
     tcopy = (mcpt.Triangle * len(tris))()
     C.memmove(tcopy, tris, C.sizeof(mcpt.Triangle) * len(tris))
     nl = C.c_int32()
