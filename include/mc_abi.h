@@ -552,6 +552,44 @@ MC_API mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_s
                                   mc_render_stats* stats);
 
 /* ------------------------------------------------------------------------- */
+/* Resolve and output encoding.                                                */
+/* ------------------------------------------------------------------------- */
+/* PT:3073 ToneMapOption */
+enum { MC_TONEMAP_NONE = 0, MC_TONEMAP_REINHARD = 1, MC_TONEMAP_ACES = 2 };
+enum {
+    MC_IMAGE_RGB8 = 0,      /* W*H*3 bytes, top row first: the pixels main() writes to the PNG (PT:4363-4380) */
+    MC_IMAGE_RGB_F32 = 1,   /* W*H float3: resolve_kernel's frame buffer (PT:3092-3100), sRGB-encoded */
+    MC_IMAGE_PFM = 2,       /* a little-endian PFM file: "PF\n<W> <H>\n-1.0\n" and W*H float3 of linear
+                               radiance (average x exposure, no tone map), bottom row first */
+    MC_IMAGE_PNG = 3        /* a PNG file of the MC_IMAGE_RGB8 pixels (stored deflate blocks) */
+};
+typedef struct mc_image_options {
+    int32_t format;         /* MC_IMAGE_* */
+    int32_t tonemap;        /* MC_TONEMAP_* (RGB8, RGB_F32, PNG) */
+    float exposure;         /* > 0: multiplier; <= 0: automatic, computeAutoExposure (PT:3121-3132) */
+    int32_t device_output;  /* 1: out is device memory (RGB8 and RGB_F32 only) */
+} mc_image_options;
+
+/* Resolves an accumulation buffer once (the reference resolves after every
+ * sample, PT:3823) and encodes it: average over `samples`, exposure, tone map,
+ * sRGB, 8-bit quantisation with main()'s NaN shield, in one pass over the
+ * buffer. accum: device, W*H float3. out: host memory (or device memory with
+ * opts.device_output, RGB8 and RGB_F32 only) of at least *bytes; out NULL only reports the size in
+ * *bytes. chosen_exposure (host, may be NULL): the exposure applied. An
+ * automatic exposure sums ln(1e-4 + luminance) in a fixed order in FP64 (the
+ * reference adds FP32 warp sums with atomics, in no fixed order). */
+MC_API mc_status mc_image_encode(mc_context* ctx, const float* accum, int32_t width, int32_t height, int32_t samples,
+                                 const mc_image_options* opts, void* out, int64_t* bytes, float* chosen_exposure);
+/* mc_image_encode of a HOST accumulation buffer (uploaded first); out is host
+ * memory. */
+MC_API mc_status mc_image_encode_host(mc_context* ctx, const float* accum_host, int32_t width, int32_t height,
+                                      int32_t samples, const mc_image_options* opts, void* out, int64_t* bytes,
+                                      float* chosen_exposure);
+/* Host: a PNG file (8-bit RGB, no interlace, stored deflate blocks) of
+ * W*H*3 bytes of pixels, top row first. out NULL only reports *bytes. */
+MC_API mc_status mc_png_encode(const uint8_t* rgb, int32_t width, int32_t height, uint8_t* out, int64_t* bytes);
+
+/* ------------------------------------------------------------------------- */
 /* Render server. No counterpart in the reference (one scene per process).   */
 /*                                                                           */
 /* Scenes are registered once; their BVHs stay resident. Requests (scene,    */
@@ -614,6 +652,10 @@ MC_API mc_status mc_server_get_result(mc_server* server, int64_t request_id, mc_
 /* Copies a request's accumulation buffer (W*H float3, the sum over its
  * samples so far) into host memory. */
 MC_API mc_status mc_server_read(mc_server* server, int64_t request_id, float* host_rgb);
+/* Encodes a request's image as mc_image_encode does (samples = the samples
+ * accumulated so far) into host memory; out NULL only reports *bytes. */
+MC_API mc_status mc_server_encode(mc_server* server, int64_t request_id, const mc_image_options* opts, void* out,
+                                  int64_t* bytes, float* chosen_exposure);
 /* Frees a finished request's accumulation buffer. */
 MC_API mc_status mc_server_release(mc_server* server, int64_t request_id);
 MC_API mc_status mc_server_get_stats(const mc_server* server, mc_server_stats* stats);
@@ -663,5 +705,6 @@ MC_STATIC_ASSERT(sizeof(mc_server_config) == 24, "mc_server_config is 24 bytes")
 MC_STATIC_ASSERT(sizeof(mc_server_request) == 248, "mc_server_request is 248 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_result) == 56, "mc_server_result is 56 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_stats) == 64, "mc_server_stats is 64 bytes");
+MC_STATIC_ASSERT(sizeof(mc_image_options) == 16, "mc_image_options is 16 bytes");
 
 #endif /* MC_ABI_H */

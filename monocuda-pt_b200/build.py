@@ -6,7 +6,7 @@ Per-file flags:
                 reference's host (IEEE, no contraction) computation bit for bit.
   mc_ingest.cu  the same IEEE flags: light areas and normals equal the
                 reference's host computation bit for bit.
-  mc_render.cu  -O3 --use_fast_math: the reference's release flags
+  mc_render.cu, mc_resolve.cu  -O3 --use_fast_math: the reference's release flags
                 (CMakeLists.txt:88-96), which the per-ray arithmetic must match.
   other .cu     -O3
   mc_scene.cpp  g++ -O2 -ffp-contract=off (host scene/camera math as the reference's host code).
@@ -39,8 +39,9 @@ UNITS = {
     "mc_guide.cu": ["-O3"],
     "mc_server.cu": ["-O3"],
     "mc_ingest.cu": ["-O3", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
+    "mc_resolve.cu": ["-O3", "--use_fast_math"],
 }
-HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"]}
+HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_image.cpp": ["-O2"]}
 
 
 def headers():

@@ -5,8 +5,11 @@
 // --spp N, plus the settings the reference fixes in main() (resolution
 // PT:4080-4081, max depth PT:4117, seed PT:4297) and this library's own
 // choices (RNG, intersector, CUDA graph). The scenes are the
-// library's seeded generators; the output is the averaged linear radiance as a
-// PFM (tone mapping and PNG stay out of this path).
+// library's seeded generators. --tonemap and --exposure follow the reference's
+// flags; the image is resolved once after the last sample (mc_image_encode)
+// and written by the extension of --out: .png (the reference's output: tone
+// mapped, sRGB, 8-bit), .ppm (the same pixels), .pfm (linear radiance times
+// the exposure).
 //
 // Exit status: 0 on success, 1 on a library error (message on stderr), 2 on a
 // usage error.
@@ -37,6 +40,8 @@ struct Options {
     bool graph = false;
     std::string out;
     bool stats = false;
+    int tonemap = MC_TONEMAP_NONE;
+    float exposure = 1.0f;  // <= 0: automatic
 };
 
 const struct {
@@ -53,7 +58,8 @@ void usage(FILE* f) {
                  "usage: monocuda [--wavefront] [--persistent] [--scene NAME] [--spp N]\n"
                  "                [--width W] [--height H] [--depth D] [--seed S] [--variant V] [--scene-seed S]\n"
                  "                [--rng philox|xorwow] [--watertight] [--graph]\n"
-                 "                [--out FILE.pfm] [--stats]\n"
+                 "                [--tonemap none|reinhard|aces] [--exposure X|auto]\n"
+                 "                [--out FILE.png|FILE.ppm|FILE.pfm] [--stats]\n"
                  "scenes:");
     for (const auto& s : kScenes) std::fprintf(f, " %s", s.name);
     std::fprintf(f, "\n");
@@ -110,6 +116,16 @@ bool parse(int argc, char** argv, Options& o) {
                 std::fprintf(stderr, "unknown rng '%s'\n", v);
                 return false;
             }
+        } else if (!std::strcmp(a, "--tonemap")) {
+            // PT:3933-3936: unknown names leave the default (none)
+            if (!(v = next(a))) return false;
+            if (!std::strcmp(v, "reinhard")) o.tonemap = MC_TONEMAP_REINHARD;
+            else if (!std::strcmp(v, "aces")) o.tonemap = MC_TONEMAP_ACES;
+        } else if (!std::strcmp(a, "--exposure")) {
+            // PT:3937-3944: "auto", or a positive multiplier (others are ignored)
+            if (!(v = next(a))) return false;
+            if (!std::strcmp(v, "auto")) o.exposure = 0.0f;
+            else if ((float)std::atof(v) > 0.0f) o.exposure = (float)std::atof(v);
         } else if (!std::strcmp(a, "--out")) {
             if (!(v = next(a))) return false;
             o.out = v;
@@ -131,13 +147,16 @@ int fail(const char* what, mc_status s) {
     return 1;
 }
 
-// Little-endian PFM (negative scale), bottom row first as the format wants.
-bool write_pfm(const std::string& path, const std::vector<float>& rgb, int W, int H) {
+bool ends_with(const std::string& s, const char* suffix) {
+    const size_t n = std::strlen(suffix);
+    return s.size() >= n && s.compare(s.size() - n, n, suffix) == 0;
+}
+
+bool write_file(const std::string& path, const void* head, size_t headBytes, const void* data, size_t bytes) {
     FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) return false;
-    std::fprintf(f, "PF\n%d %d\n-1.0\n", W, H);
-    for (int y = H - 1; y >= 0; y--) std::fwrite(&rgb[(size_t)y * W * 3], sizeof(float), (size_t)W * 3, f);
-    return std::fclose(f) == 0;
+    bool ok = std::fwrite(head, 1, headBytes, f) == headBytes && std::fwrite(data, 1, bytes, f) == bytes;
+    return (std::fclose(f) == 0) && ok;
 }
 
 }  // namespace
@@ -220,13 +239,31 @@ int main(int argc, char** argv) {
                             (long long)stats.shadow_per_depth[d]);
         }
         if (!o.out.empty()) {
-            std::vector<float> avg(accum.size());
-            for (size_t i = 0; i < accum.size(); i++) avg[i] = accum[i] / (float)p.spp;
-            if (!write_pfm(o.out, avg, W, H)) {
-                std::fprintf(stderr, "could not write '%s'\n", o.out.c_str());
-                rc = 1;
+            mc_image_options io = {};
+            io.format = ends_with(o.out, ".pfm") ? MC_IMAGE_PFM : ends_with(o.out, ".png") ? MC_IMAGE_PNG : MC_IMAGE_RGB8;
+            io.tonemap = o.tonemap;
+            io.exposure = o.exposure;
+            int64_t bytes = 0;
+            float chosen = 0.f;
+            std::vector<uint8_t> img;
+            st = mc_image_encode_host(ctx, accum.data(), W, H, p.spp, &io, nullptr, &bytes, nullptr);
+            if (st == MC_OK) {
+                img.resize((size_t)bytes);
+                st = mc_image_encode_host(ctx, accum.data(), W, H, p.spp, &io, img.data(), &bytes, &chosen);
+            }
+            if (st != MC_OK) {
+                rc = fail("mc_image_encode_host", st);
             } else {
-                std::printf("wrote %s\n", o.out.c_str());
+                if (o.exposure <= 0.f) std::printf("Auto exposure: %.3f\n", chosen);  // PT:4358
+                char head[64];
+                size_t headBytes = 0;
+                if (io.format == MC_IMAGE_RGB8) headBytes = (size_t)std::snprintf(head, sizeof(head), "P6\n%d %d\n255\n", W, H);
+                if (!write_file(o.out, head, headBytes, img.data(), img.size())) {
+                    std::fprintf(stderr, "could not write '%s'\n", o.out.c_str());
+                    rc = 1;
+                } else {
+                    std::printf("wrote %s\n", o.out.c_str());
+                }
             }
         }
     }

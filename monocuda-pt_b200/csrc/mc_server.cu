@@ -329,6 +329,18 @@ mc_status mc_server_read(mc_server* s, int64_t request_id, float* host_rgb) {
     return MC_OK;
 }
 
+mc_status mc_server_encode(mc_server* s, int64_t request_id, const mc_image_options* opts, void* out, int64_t* bytes,
+                           float* chosen_exposure) {
+    if (!s || !opts || !bytes) return mc::set_error(MC_ERR_INVALID, "mc_server_encode: null argument");
+    if (opts->device_output) return mc::set_error(MC_ERR_INVALID, "mc_server_encode: the response goes to host memory");
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_encode: unknown request %lld", (long long)request_id);
+    const ServerRequest& r = it->second;
+    if (!r.accum) return mc::set_error(MC_ERR_INVALID, "mc_server_encode: request %lld holds no image", (long long)request_id);
+    if (r.done <= 0) return mc::set_error(MC_ERR_INVALID, "mc_server_encode: request %lld has no samples yet", (long long)request_id);
+    return mc_image_encode(s->ctx, r.accum, r.params.width, r.params.height, r.done, opts, out, bytes, chosen_exposure);
+}
+
 mc_status mc_server_release(mc_server* s, int64_t request_id) {
     if (!s) return mc::set_error(MC_ERR_INVALID, "mc_server_release: null server");
     auto it = s->requests.find(request_id);

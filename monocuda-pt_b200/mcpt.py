@@ -21,6 +21,8 @@ RNG_PHILOX, RNG_XORWOW = 0, 1
 ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
 TRACE_PLAIN = 0x100
 LAYOUT_BINARY, LAYOUT_WIDE4, LAYOUT_WIDE4Q = 0, 1, 2
+TONEMAP_NONE, TONEMAP_REINHARD, TONEMAP_ACES = 0, 1, 2
+IMAGE_RGB8, IMAGE_RGB_F32, IMAGE_PFM, IMAGE_PNG = 0, 1, 2, 3
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
 SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64
@@ -149,6 +151,10 @@ class ServerResult(C.Structure):
                 ("admit_s", C.c_double), ("done_s", C.c_double), ("bytes", C.c_int64), ("d_accum", C.c_void_p)]
 
 
+class ImageOptions(C.Structure):
+    _fields_ = [("format", C.c_int32), ("tonemap", C.c_int32), ("exposure", C.c_float), ("device_output", C.c_int32)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("used_bytes", C.c_int64), ("scene_bytes", C.c_int64),
                 ("scenes", C.c_int32), ("pending", C.c_int32), ("active", C.c_int32), ("done", C.c_int32),
@@ -237,6 +243,12 @@ SIGNATURES = {
     "mc_server_get_result": (I32, [P, C.c_int64, C.POINTER(ServerResult)]),
     "mc_server_release": (I32, [P, C.c_int64]),
     "mc_server_read": (I32, [P, C.c_int64, P]),
+    "mc_server_encode": (I32, [P, C.c_int64, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64), C.POINTER(C.c_float)]),
+    "mc_image_encode": (I32, [P, P, I32, I32, I32, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64),
+                              C.POINTER(C.c_float)]),
+    "mc_png_encode": (I32, [P, I32, I32, P, C.POINTER(C.c_int64)]),
+    "mc_image_encode_host": (I32, [P, P, I32, I32, I32, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_float)]),
     "mc_server_get_stats": (I32, [P, C.POINTER(ServerStats)]),
     "mc_server_now": (C.c_double, [P]),
 }
@@ -484,6 +496,37 @@ class DeviceScene:
             pass
 
 
+def image_encode(ctx, accum_ptr, width, height, samples, fmt=IMAGE_RGB8, tonemap=TONEMAP_NONE, exposure=1.0,
+                 device_out=None):
+    """Resolves and encodes a device accumulation buffer once (mc_image_encode).
+    Returns (bytes or None when device_out is given, exposure applied)."""
+    lib = load()
+    opts = ImageOptions(fmt, tonemap, exposure, 1 if device_out is not None else 0)
+    n = C.c_int64()
+    check(lib.mc_image_encode(ctx.handle, accum_ptr, width, height, samples, C.byref(opts), None, C.byref(n), None))
+    chosen = C.c_float()
+    if device_out is not None:
+        check(lib.mc_image_encode(ctx.handle, accum_ptr, width, height, samples, C.byref(opts), device_out,
+                                  C.byref(n), C.byref(chosen)))
+        return None, chosen.value
+    buf = (C.c_uint8 * n.value)()
+    check(lib.mc_image_encode(ctx.handle, accum_ptr, width, height, samples, C.byref(opts), buf, C.byref(n),
+                              C.byref(chosen)))
+    return bytes(buf), chosen.value
+
+
+def png_encode(rgb8, width, height):
+    """A PNG file (bytes) of W*H*3 8-bit RGB pixels, top row first (mc_png_encode)."""
+    import numpy as np
+    lib = load()
+    px = np.ascontiguousarray(rgb8, dtype=np.uint8)
+    n = C.c_int64()
+    check(lib.mc_png_encode(None, width, height, None, C.byref(n)))
+    buf = (C.c_uint8 * n.value)()
+    check(lib.mc_png_encode(px.ctypes.data, width, height, buf, C.byref(n)))
+    return bytes(buf)[:n.value]
+
+
 def generate_scene(kind, variant=0, seed=0, triangle_target=0):
     """Returns a SceneHost (host memory owned by the library; free with free_scene)."""
     lib = load()
@@ -635,6 +678,17 @@ class Server:
         out = np.zeros(width * height * 3, np.float32)
         check(self.lib.mc_server_read(self.handle, rid, out.ctypes.data))
         return out
+
+    def encode(self, rid, fmt=IMAGE_RGB8, tonemap=TONEMAP_NONE, exposure=1.0):
+        """The request's image encoded once (mc_server_encode): bytes, and the
+        exposure applied (exposure <= 0: automatic)."""
+        opts = ImageOptions(fmt, tonemap, exposure, 0)
+        n = C.c_int64()
+        check(self.lib.mc_server_encode(self.handle, rid, C.byref(opts), None, C.byref(n), None))
+        buf = (C.c_uint8 * n.value)()
+        chosen = C.c_float()
+        check(self.lib.mc_server_encode(self.handle, rid, C.byref(opts), buf, C.byref(n), C.byref(chosen)))
+        return bytes(buf), chosen.value
 
     def release(self, rid):
         check(self.lib.mc_server_release(self.handle, rid))

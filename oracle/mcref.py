@@ -20,6 +20,7 @@ _SIGS = {
     "mcref_scene_release": (I32, []),
     "mcref_trace": (I32, [P, I32, I32, P, P, P]),
     "mcref_render": (I32, [P, I32, I32, I32, I32, I32, C.c_ulonglong, I32, I32, P, P]),
+    "mcref_resolve": (I32, [P, I32, I32, I32, I32, C.c_float, I32, P, P, P]),
 }
 _libs = {}
 

@@ -537,4 +537,47 @@ int mcref_render(const mc_camera* cam_in, int W, int H, int spp, int max_depth, 
     return 0;
 }
 
+// resolve_kernel (path_tracer.cu:3092-3100) on a host accumulation buffer,
+// with the exposure of computeAutoExposure (3121-3132) when auto_exposure is
+// set, launched with main()'s wavefront block and grid shapes (4101-4103),
+// then the 8-bit encoding main() applies before writing the PNG (4363-4380,
+// restated here: it is inline in main()). Outputs (host, may be NULL):
+// frame W*H*3 floats, rgb8 W*H*3 bytes, *chosen the exposure used.
+int mcref_resolve(const float* accum_in, int W, int H, int samples, int tonemap, float exposure, int auto_exposure,
+                  float* frame_out, unsigned char* rgb8_out, float* chosen) {
+    if (W <= 0 || H <= 0 || samples <= 0 || tonemap < 0 || tonemap > 2) return 1;
+    QuietStdout quiet;
+    int dev = 0;
+    cudaDeviceProp props;
+    MCREF_TRY(cudaGetDevice(&dev));
+    MCREF_TRY(cudaGetDeviceProperties(&props, dev));
+    dim3 block = chooseImageBlockShape(generateCameraRaysKernel, props);
+    dim3 grid = chooseImageGridShape(block, W, H, props);
+    const size_t pixels = (size_t)W * H;
+    vec3* d_accum; vec3* d_frame;
+    MCREF_TRY(cudaMalloc(&d_accum, pixels * sizeof(vec3)));
+    MCREF_TRY(cudaMalloc(&d_frame, pixels * sizeof(vec3)));
+    MCREF_TRY(cudaMemcpy(d_accum, accum_in, pixels * sizeof(vec3), cudaMemcpyHostToDevice));
+    float e = exposure;
+    if (auto_exposure) e = computeAutoExposure(d_accum, W, H, samples, grid, block);
+    resolve_kernel<<<grid, block>>>(d_accum, d_frame, W, H, samples, (ToneMapOption)tonemap, e);
+    MCREF_TRY(cudaGetLastError());
+    std::vector<vec3> frame(pixels);
+    MCREF_TRY(cudaMemcpy(frame.data(), d_frame, pixels * sizeof(vec3), cudaMemcpyDeviceToHost));
+    cudaFree(d_accum);
+    cudaFree(d_frame);
+    if (frame_out) std::memcpy(frame_out, frame.data(), pixels * sizeof(vec3));
+    if (rgb8_out) {
+        for (size_t p = 0; p < pixels; p++) {
+            const float c[3] = {frame[p].x, frame[p].y, frame[p].z};
+            for (int k = 0; k < 3; k++) {
+                float f = std::isfinite(c[k]) ? fminf(fmaxf(c[k], 0.0f), 1.0f) : 0.0f;
+                rgb8_out[3 * p + k] = (unsigned char)(255.99f * f);
+            }
+        }
+    }
+    if (chosen) *chosen = e;
+    return 0;
+}
+
 }  // extern "C"

@@ -60,4 +60,41 @@ def test_cli_render_equals_library_call(tmp_path):
                                       acc.ctypes.data, C.byref(st)))
     ctx.close()
     mcpt.free_scene(s)
-    np.testing.assert_array_equal(img.reshape(-1), acc / np.float32(2))
+    np.testing.assert_allclose(img.reshape(-1), acc / np.float32(2), rtol=4e-7, atol=0)
+
+
+@pytest.mark.gpu
+def test_cli_png_and_ppm_match_reference_resolve(tmp_path):
+    """--tonemap aces --exposure 0.8: the PNG and PPM pixels equal the
+    reference's resolve_kernel + 8-bit encoding of the same accumulation."""
+    import mcref
+    from test_cpu import _png_pixels
+    outs = [os.path.join(tmp_path, "c.png"), os.path.join(tmp_path, "c.ppm")]
+    for out in outs:
+        r = _run("--wavefront", "--persistent", "--scene", "cornell_boxes", "--width", "48", "--spp", "3",
+                 "--tonemap", "aces", "--exposure", "0.8", "--out", out)
+        assert r.returncode == 0, r.stderr
+    w, h, png = _png_pixels(open(outs[0], "rb").read())
+    assert (w, h) == (48, 48)
+    ppm = open(outs[1], "rb").read()
+    assert ppm.startswith(b"P6\n48 48\n255\n")
+    assert ppm[len(b"P6\n48 48\n255\n"):] == png.tobytes()
+
+    s = mcpt.generate_scene(mcpt.SCENE_CORNELL_BOXES)
+    cam = mcpt.Camera.from_buffer_copy(bytes(s.camera))
+    cam.image_width = 48
+    cam.aspect_ratio = 1.0
+    mcpt.camera_initialize(cam)
+    p = mcpt.render_params(cam, 48, 48, 3, s.max_depth, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234)
+    ctx = mcpt.Context(0)
+    tris = mcpt.host_triangles(s)
+    acc = np.zeros(48 * 48 * 3, np.float32)
+    env = mcpt.EnvMap()
+    mcpt.check(ctx.lib.mc_render_host(ctx.handle, C.addressof(tris), len(tris), None, 0, C.byref(env), C.byref(p),
+                                      acc.ctypes.data, None))
+    ctx.close()
+    mcpt.free_scene(s)
+    rgb8 = np.zeros(48 * 48 * 3, np.uint8)
+    assert mcref.load(False).mcref_resolve(acc.ctypes.data, 48, 48, 3, mcpt.TONEMAP_ACES, 0.8, 0, None,
+                                           rgb8.ctypes.data, None) == 0
+    assert np.array_equal(png.reshape(-1), rgb8)

@@ -325,3 +325,53 @@ def test_host_finalize_matches_reference_on_random_soup():
     boxes = np.frombuffer(tris, np.uint8).reshape(n, 224)[:, 192:224].copy().view(np.float32)
     lanes = [0, 1, 2, 4, 5, 6]
     assert np.array_equal(boxes[:, lanes].view(np.uint32), tb.reshape(n, 8)[:, lanes].view(np.uint32))
+
+
+def _png_pixels(png):
+    """Decodes a PNG of 8-bit RGB with filter type 0 rows: checks the chunk
+    CRCs and returns (width, height, pixels)."""
+    import struct
+    import zlib
+    assert png[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, ihdr = 8, b"", None
+    while pos < len(png):
+        (length,) = struct.unpack(">I", png[pos:pos + 4])
+        ctype, data = png[pos + 4:pos + 8], png[pos + 8:pos + 8 + length]
+        (crc,) = struct.unpack(">I", png[pos + 8 + length:pos + 12 + length])
+        assert crc == zlib.crc32(ctype + data) & 0xFFFFFFFF, ctype
+        if ctype == b"IHDR":
+            ihdr = struct.unpack(">IIBBBBB", data)
+        elif ctype == b"IDAT":
+            idat += data
+        pos += 12 + length
+        if ctype == b"IEND":
+            break
+    assert pos == len(png)
+    w, h, depth, colour, comp, filt, interlace = ihdr
+    assert (depth, colour, comp, filt, interlace) == (8, 2, 0, 0, 0)
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + 3 * w)
+    assert (raw[:, 0] == 0).all()
+    return w, h, raw[:, 1:].reshape(h, w, 3)
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (37, 23), (300, 250), (1920, 12)])
+def test_png_encoder_round_trip(w, h):
+    """mc_png_encode: valid chunks and CRCs, a zlib stream (stored blocks,
+    more than one once a row set passes 65,535 bytes) that decodes to the
+    same pixels."""
+    rng = np.random.default_rng(w * 1000 + h)
+    px = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+    png = mcpt.png_encode(px, w, h)
+    gw, gh, got = _png_pixels(png)
+    assert (gw, gh) == (w, h)
+    assert np.array_equal(got, px)
+
+
+def test_png_encoder_rejects_bad_sizes():
+    n = C.c_int64(0)
+    assert mcpt.load().mc_png_encode(None, 0, 5, None, C.byref(n)) == 1
+    assert mcpt.load().mc_png_encode(None, 4, 4, None, None) == 1
+    n = C.c_int64(10)
+    buf = (C.c_uint8 * 10)()
+    px = np.zeros(48, np.uint8)
+    assert mcpt.load().mc_png_encode(px.ctypes.data, 4, 4, buf, C.byref(n)) == 1
