@@ -372,6 +372,38 @@ typedef struct mc_scene_host {
 MC_API mc_status mc_scene_generate(const mc_scene_desc* desc, mc_scene_host* out);
 MC_API mc_status mc_scene_free(mc_scene_host* scene);
 
+/* OBJ/MTL loading: loadObject (PT:2644-2859) with loadMtlFile (PT:2614-2680).
+ * Appends the file's triangles to scene->triangles (reallocated; free with
+ * mc_scene_free). The model is centred on x/z with its lowest point at y = 0
+ * and its largest side 1, then scaled by `scale`, rotated by rotation_y
+ * radians about y and moved by `translation`. Faces are fan-triangulated;
+ * faces with a bad index or zero area are skipped; without vn the normals are
+ * area-weighted vertex averages. Materials: newmtl/Kd/Ke/map_Kd, emissive when
+ * Ke has a positive component, else lambertian (with the map_Kd image read
+ * from a .ppm beside the named file when load_textures is set and it loads);
+ * faces without a known material get *fallback. Errors: MC_ERR_NOT_FOUND (no
+ * such file), MC_ERR_INVALID (no vertices, faces or triangles). */
+typedef struct mc_obj_info {
+    int32_t triangles_added;
+    int32_t faces_skipped;
+    int32_t materials;
+    int32_t textures_loaded;
+    int32_t textures_missing;   /* materials whose map_Kd image was not loaded */
+    int32_t unknown_materials;  /* usemtl names the libraries do not define */
+    uint64_t* textures;         /* the textures_loaded textures created (mc_image_texture_destroy each,
+                                   then mc_obj_info_free) */
+} mc_obj_info;
+MC_API mc_status mc_obj_load(const char* path, const mc_material* fallback, mc_vec3 translation, float scale,
+                             float rotation_y, int32_t load_textures, mc_scene_host* scene, mc_obj_info* info);
+MC_API mc_status mc_obj_info_free(mc_obj_info* info);
+/* loadPpmAsRgba8 (PT:236-294): a binary PPM (P6, maximum 255) as RGBA8 with
+ * alpha 255. rgba NULL only reads the size. */
+MC_API mc_status mc_ppm_read(const char* path, int32_t* width, int32_t* height, uint8_t* rgba);
+/* createImageTextureObject (PT:296-316): an RGBA8 image texture (sRGB,
+ * bilinear, wrapped) for mc_texture.image; mc_image_texture_destroy frees it. */
+MC_API mc_status mc_image_texture_create(const uint8_t* rgba, int32_t width, int32_t height, uint64_t* texture);
+MC_API mc_status mc_image_texture_destroy(uint64_t texture);
+
 /* ------------------------------------------------------------------------- */
 /* BVH (a1-a7). Replaces the host Morton/sort (PT:1930-1987, 4223-4260) and    */
 /* BVH::generateHierarchy (PT:1063-1090).                                      */
@@ -706,5 +738,6 @@ MC_STATIC_ASSERT(sizeof(mc_server_request) == 248, "mc_server_request is 248 byt
 MC_STATIC_ASSERT(sizeof(mc_server_result) == 56, "mc_server_result is 56 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_stats) == 64, "mc_server_stats is 64 bytes");
 MC_STATIC_ASSERT(sizeof(mc_image_options) == 16, "mc_image_options is 16 bytes");
+MC_STATIC_ASSERT(sizeof(mc_obj_info) == 32, "mc_obj_info is 32 bytes");
 
 #endif /* MC_ABI_H */

@@ -154,6 +154,49 @@ mc_status mc_context_synchronize(mc_context* ctx) {
 
 // PT:370-411: sampling tables (host) and a float4 texture, linear filtering,
 // wrap in u, clamp in v, element-type reads, normalized coordinates.
+// createImageTextureObject (PT:296-316): RGBA8 array, sRGB, bilinear,
+// wrapped, normalised coordinates.
+mc_status mc_image_texture_create(const uint8_t* rgba, int32_t width, int32_t height, uint64_t* texture) {
+    if (!rgba || !texture || width <= 0 || height <= 0) return mc::set_error(MC_ERR_INVALID, "mc_image_texture_create: bad arguments");
+    cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();
+    cudaArray_t arr = nullptr;
+    cudaError_t e = cudaMallocArray(&arr, &fmt, (size_t)width, (size_t)height);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DToArray(arr, 0, 0, rgba, (size_t)width * 4, (size_t)width * 4, (size_t)height, cudaMemcpyHostToDevice);
+    cudaTextureObject_t tex = 0;
+    if (e == cudaSuccess) {
+        cudaResourceDesc res;
+        std::memset(&res, 0, sizeof(res));
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = arr;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = cudaAddressModeWrap;
+        td.addressMode[1] = cudaAddressModeWrap;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeNormalizedFloat;
+        td.normalizedCoords = 1;
+        td.sRGB = 1;
+        e = cudaCreateTextureObject(&tex, &res, &td, nullptr);
+    }
+    if (e != cudaSuccess) {
+        if (arr) cudaFreeArray(arr);
+        return mc::cuda_error((int)e, "mc_image_texture_create", __FILE__, __LINE__);
+    }
+    *texture = (uint64_t)tex;
+    return MC_OK;
+}
+
+mc_status mc_image_texture_destroy(uint64_t texture) {
+    if (!texture) return MC_OK;
+    cudaResourceDesc res;
+    cudaError_t e = cudaGetTextureObjectResourceDesc(&res, (cudaTextureObject_t)texture);
+    if (e != cudaSuccess) return mc::cuda_error((int)e, "mc_image_texture_destroy", __FILE__, __LINE__);
+    cudaDestroyTextureObject((cudaTextureObject_t)texture);
+    if (res.resType == cudaResourceTypeArray && res.res.array.array) cudaFreeArray(res.res.array.array);
+    return MC_OK;
+}
+
 mc_status mc_env_create(const float* rgba, int32_t W, int32_t H, float intensity, float rotation, mc_env_map* out) {
     if (!out) return mc::set_error(MC_ERR_INVALID, "mc_env_create: null output");
     std::memset(out, 0, sizeof(*out));

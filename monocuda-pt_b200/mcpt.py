@@ -155,6 +155,12 @@ class ImageOptions(C.Structure):
     _fields_ = [("format", C.c_int32), ("tonemap", C.c_int32), ("exposure", C.c_float), ("device_output", C.c_int32)]
 
 
+class ObjInfo(C.Structure):
+    _fields_ = [("triangles_added", C.c_int32), ("faces_skipped", C.c_int32), ("materials", C.c_int32),
+                ("textures_loaded", C.c_int32), ("textures_missing", C.c_int32), ("unknown_materials", C.c_int32),
+                ("textures", C.POINTER(C.c_uint64))]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("used_bytes", C.c_int64), ("scene_bytes", C.c_int64),
                 ("scenes", C.c_int32), ("pending", C.c_int32), ("active", C.c_int32), ("done", C.c_int32),
@@ -247,6 +253,12 @@ SIGNATURES = {
     "mc_image_encode": (I32, [P, P, I32, I32, I32, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64),
                               C.POINTER(C.c_float)]),
     "mc_png_encode": (I32, [P, I32, I32, P, C.POINTER(C.c_int64)]),
+    "mc_obj_load": (I32, [C.c_char_p, C.POINTER(Material), Vec3, C.c_float, C.c_float, I32, C.POINTER(SceneHost),
+                          C.POINTER(ObjInfo)]),
+    "mc_obj_info_free": (I32, [C.POINTER(ObjInfo)]),
+    "mc_ppm_read": (I32, [C.c_char_p, C.POINTER(I32), C.POINTER(I32), P]),
+    "mc_image_texture_create": (I32, [P, I32, I32, C.POINTER(C.c_uint64)]),
+    "mc_image_texture_destroy": (I32, [C.c_uint64]),
     "mc_image_encode_host": (I32, [P, P, I32, I32, I32, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64),
                                    C.POINTER(C.c_float)]),
     "mc_server_get_stats": (I32, [P, C.POINTER(ServerStats)]),
@@ -525,6 +537,28 @@ def png_encode(rgb8, width, height):
     buf = (C.c_uint8 * n.value)()
     check(lib.mc_png_encode(px.ctypes.data, width, height, buf, C.byref(n)))
     return bytes(buf)[:n.value]
+
+
+def obj_load(path, fallback, translation=(0.0, 0.0, 0.0), scale=1.0, rotation_y=0.0, load_textures=False, scene=None):
+    """Appends an OBJ file's triangles to a SceneHost (a new, empty one when
+    scene is None) with mc_obj_load. Returns (scene, ObjInfo); free the scene
+    with free_scene and the info with obj_info_free (after destroying its
+    textures when the scene is no longer rendered)."""
+    lib = load()
+    if scene is None:
+        scene = SceneHost()
+    info = ObjInfo()
+    check(lib.mc_obj_load(os.fsencode(path), C.byref(fallback), Vec3(*translation), scale, rotation_y,
+                          1 if load_textures else 0, C.byref(scene), C.byref(info)))
+    return scene, info
+
+
+def obj_info_free(info, destroy_textures=True):
+    lib = load()
+    if destroy_textures:
+        for i in range(info.textures_loaded):
+            lib.mc_image_texture_destroy(info.textures[i])
+    lib.mc_obj_info_free(C.byref(info))
 
 
 def generate_scene(kind, variant=0, seed=0, triangle_target=0):

@@ -580,4 +580,21 @@ int mcref_resolve(const float* accum_in, int W, int H, int samples, int tonemap,
     return 0;
 }
 
+// loadObject (path_tracer.cu:2644-2859) into an empty scene; copies up to
+// `capacity` triangles out, *count = the number loaded. Returns 0 when the
+// reference reports success, 3 when it returns false.
+int mcref_load_object(const char* path, const mc_material* mat, float tx, float ty, float tz, float scale, float rot,
+                      mc_triangle* out, int capacity, int* count) {
+    QuietStdout quiet;
+    hostScene scene;
+    Material m;
+    static_assert(sizeof(Material) == sizeof(mc_material), "Material layout");
+    std::memcpy(&m, mat, sizeof(Material));
+    bool ok = loadObject(scene, path, m, vec3(tx, ty, tz), scale, rot);
+    const int n = (int)scene.triangles.size();
+    if (count) *count = n;
+    for (int i = 0; i < n && i < capacity; i++) std::memcpy(&out[i], &scene.triangles[i], sizeof(triangle));
+    return ok ? 0 : 3;
+}
+
 }  // extern "C"
