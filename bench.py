@@ -2,9 +2,10 @@
 
 Workload: the "displaced_icospheres" scene (3 level-8 displaced icospheres =
 3,932,160 triangles + ground, medium box, area light, 2048x1024 procedural sky),
-1920x1080, max depth 8, counter-based RNG. One step = one sample of every pixel
-(a full wave of 2,073,600 paths through up to 8 bounces); K steps = K spp
-(default 64, about half a second of timed work).
+1920x1080, max depth 8, counter-based RNG. One step = one frame of the
+workload's 16 samples per pixel (--spp-per-step), rendered by one C-ABI call
+that traces several samples per wave (the library's automatic wave size);
+K steps = 16 K spp (default K = 16, about a second of timed work).
 Mrays/s = (extend rays + shadow rays) / device time, rays counted on the device.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -12,7 +13,7 @@ Mrays/s = (extend rays + shadow rays) / device time, rays counted on the device.
 --impl reference runs the UNMODIFIED reference (oracle/_ref/libmcref.so: the
 reference's src/path_tracer.cu compiled for sm_100a) through its own
 renderWithWavefront with --persistent semantics on the same scene.
-Multi-GPU (torchrun): every rank renders its own K samples of the full image
+Multi-GPU (torchrun): every rank renders its own K frames of the full image
 (weak scaling) and the accumulation buffers are summed with one NCCL
 all-reduce at the end, inside the timed region.
 """
@@ -42,7 +43,10 @@ INGEST_BYTES = 224 + 36 + 192  # per triangle: AoS record read, hot and cold rec
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--spp-per-step", type=int, default=16, help="samples per pixel of one step (one frame)")
+    ap.add_argument("--samples-per-wave", type=int, default=0,
+                    help="samples traced together per wave (0 = the library's automatic choice, 1 = one per wave)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = the named workload)")
@@ -214,7 +218,8 @@ def run_ours(args):
     bvh = mcpt.Bvh(ctx, ds.view, layout=layout)
     W, H = scene.width, scene.height
     acc = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
-    K, Wm = args.steps, args.warmup
+    K, Wm, S = args.steps, args.warmup, args.spp_per_step
+    # step indices; step s renders samples [s * S, (s + 1) * S)
     timed_samples, warm_samples = sharding.sample_ranges(rank, world, K, Wm)
 
     # the library's autotuner picks the trace variant and refill threshold for
@@ -224,10 +229,10 @@ def run_ours(args):
     if args.refill <= 0:
         mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
 
-    def params(first, instrument=0):
-        return mcpt.render_params(scene.camera, W, H, 1, 8, persistent=bool(tuned.persistent), rng=mcpt.RNG_PHILOX,
-                                  seed=1234, first_sample=first, instrument=instrument,
-                                  refill_threshold=tuned.refill_threshold)
+    def params(step, instrument=0):
+        return mcpt.render_params(scene.camera, W, H, S, 8, persistent=bool(tuned.persistent), rng=mcpt.RNG_PHILOX,
+                                  seed=1234, first_sample=step * S, instrument=instrument,
+                                  refill_threshold=tuned.refill_threshold, samples_per_wave=args.samples_per_wave)
 
     st = mcpt.RenderStats()
     for s in warm_samples:
@@ -311,7 +316,6 @@ def run_ours(args):
     # cold end to end: host triangles in, accumulation buffer out, one C-ABI call
     host_cold = torch.zeros(W * H * 3, dtype=torch.float32, pin_memory=True)
     pc = params(timed_samples.start)
-    pc.spp = K
     cold_stats = mcpt.RenderStats()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -370,11 +374,12 @@ def run_ours(args):
         "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": dict(WORKLOAD, spp=K * world, bvh_layout=args.layout,
+        "config": dict(WORKLOAD, spp=K * S * world, spp_per_step=S, bvh_layout=args.layout,
                        autotuned={"persistent": int(tuned.persistent), "refill_threshold": int(tuned.refill_threshold)},
                        parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
-                       samples_per_sec=round(W * H * K * world / (ms_max / 1e3), 1),
-                       rays_per_path=round(rays_all / (W * H * K * world), 3)),
+                       samples_per_wave=args.samples_per_wave or "automatic",
+                       samples_per_sec=round(W * H * K * S * world / (ms_max / 1e3), 1),
+                       rays_per_path=round(rays_all / (W * H * K * S * world), 3)),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic, "kernel": "k_trace (persistent extend + shadow)",
@@ -390,7 +395,7 @@ def run_ours(args):
                      "seconds": round(cold_s, 3), "h2d_bytes": len(tris) * 224, "d2h_bytes": W * H * 12,
                      "stages": stages,
                      "note": "mc_render_host: host triangles -> upload, device ingestion (bounds, lights, split), "
-                             "BVH build, %d spp, read-back" % K},
+                             "BVH build, %d spp, read-back" % S},
         "gpu_launches": launches,
         "clocks": ck,
     }
@@ -777,25 +782,25 @@ def run_reference(args):
     env = mcpt.host_env(scene)
     assert ref.mcref_scene_upload(C.addressof(tris), len(tris), None, 0, env.ctypes.data, scene.env_width,
                                   scene.env_height, scene.env_intensity, 0.0) == 0
-    W, H, K = scene.width, scene.height, args.steps
+    W, H, K, S = scene.width, scene.height, args.steps, args.spp_per_step
     acc = np.zeros(W * H * 3, np.float32)
     stats = np.zeros(3, np.float64)
     cam = mcpt.Camera.from_buffer_copy(bytes(scene.camera))
     for _ in range(args.warmup):
         assert ref.mcref_render(C.addressof(cam), W, H, 1, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
     clocks = Clocks(0)
-    # timed: renderWithWavefront (PT:3757) itself, K samples, wavefront + persistent
-    assert ref.mcref_render(C.addressof(cam), W, H, K, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+    # timed: renderWithWavefront (PT:3757) itself, K steps of S samples, wavefront + persistent
+    assert ref.mcref_render(C.addressof(cam), W, H, K * S, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
     ck = clocks.stop()
     ms = stats[2]
     # untimed replay of the same launch sequence that also reads the shadow-queue sizes
-    assert ref.mcref_render(C.addressof(cam), W, H, K, 8, 2, 1234, 0, 0, acc.ctypes.data, stats.ctypes.data) == 0
+    assert ref.mcref_render(C.addressof(cam), W, H, K * S, 8, 2, 1234, 0, 0, acc.ctypes.data, stats.ctypes.data) == 0
     rays = stats[0] + stats[1]
     value = rays / (ms / 1e3) / 1e6
     out = {"metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1, "steps": K, "warmup": args.warmup,
            "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic (seeded procedural scene)", "impl": "reference",
-           "config": dict(WORKLOAD, spp=K, rng="curand XORWOW (the reference's own)", parallelism="1 GPU",
+           "config": dict(WORKLOAD, spp=K * S, spp_per_step=S, rng="curand XORWOW (the reference's own)", parallelism="1 GPU",
                           note="unmodified reference renderWithWavefront --wavefront --persistent on the B200"),
            "cpu_baseline": {"value": round(value, 2), "unit": "Mrays/s", "cores": 1, "kind": "reference",
                             "sample": "the full workload; the reference has no CPU implementation of the path, its own "

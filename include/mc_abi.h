@@ -267,6 +267,10 @@ typedef struct mc_render_params {
     int32_t use_graph;          /* capture each sample's bounce sequence in a CUDA graph */
     int32_t instrument;         /* bit 0: count node visits / leaf tests (counting kernel variant);
                                    bit 1: time every trace launch with CUDA events on the context stream */
+    int32_t samples_per_wave;   /* samples traced together in one wave (counter-based RNG only; the XORWOW
+                                   states advance sample by sample): 0 = automatic (up to 16, at most about
+                                   32M paths per wave), 1 = one sample per wave. Images do not depend on it:
+                                   each pixel adds its samples in sample order. */
 } mc_render_params;
 
 #define MC_MAX_DEPTH_STATS 64
@@ -732,9 +736,9 @@ MC_STATIC_ASSERT(sizeof(mc_camera) == 172, "Camera is 172 bytes");
 MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
 /* this library's own structs (bindings mirror these sizes) */
 MC_STATIC_ASSERT(sizeof(mc_guide_config) == 80, "mc_guide_config is 80 bytes");
-MC_STATIC_ASSERT(sizeof(mc_render_params) == 232, "mc_render_params is 232 bytes");
+MC_STATIC_ASSERT(sizeof(mc_render_params) == 240, "mc_render_params is 240 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_config) == 24, "mc_server_config is 24 bytes");
-MC_STATIC_ASSERT(sizeof(mc_server_request) == 248, "mc_server_request is 248 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_request) == 256, "mc_server_request is 256 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_result) == 56, "mc_server_result is 56 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_stats) == 64, "mc_server_stats is 64 bytes");
 MC_STATIC_ASSERT(sizeof(mc_image_options) == 16, "mc_image_options is 16 bytes");

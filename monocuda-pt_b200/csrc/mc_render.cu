@@ -775,6 +775,32 @@ __global__ void k_finalize(const WaveTable* tab, const unsigned short* sceneOf, 
     }
 }
 
+// Several samples of one image in one wave (items 0..n-1 of equal size, in
+// sample order): each pixel adds its samples in that order, as consecutive
+// one-sample waves would, so the sums are the same to the bit.
+__global__ void k_finalize_samples(const WaveTable* tab, const float* sr, const float* sg, const float* sb) {
+    const int pixels = tab->scenes[0].paths;
+    const int n = tab->nScenes;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pixels; q += gridDim.x * blockDim.x) {
+        float* acc = tab->scenes[0].accum + (size_t)q * 3;
+        float a0 = acc[0], a1 = acc[1], a2 = acc[2];
+        for (int j = 0; j < n; j++) {
+            const SceneGPU& S = tab->scenes[j];
+            const int p = S.pathOffset + q;
+            V3 s(sr[p], sg[p], sb[p]);
+            float bright = fmaxf(s.x, fmaxf(s.y, s.z));
+            const float maxBright = 10.0f;
+            if (!S.disableClamp && bright > maxBright) s = s * (maxBright / bright);
+            a0 = a0 + s.x;
+            a1 = a1 + s.y;
+            a2 = a2 + s.z;
+        }
+        acc[0] = a0;
+        acc[1] = a1;
+        acc[2] = a2;
+    }
+}
+
 // Guided renders (one scene, one or more images): the sample plus the primary vertex's NEE goes
 // to the image; a primary-vertex record takes the sample without that NEE
 // (the radiance carried back through its sampled direction over that
@@ -1023,11 +1049,19 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     const bool timeTrace = (p0.instrument & 2) != 0;
     int capacity = 0, maxD = 0, waves = 0;
     bool medium = false;
+    auto item_waves = [&](int i) { return items[i].waves >= 0 ? items[i].waves : items[i].p->spp; };
+    // items that are samples of one image of one scene: single-scene trace
+    // launches and the ordered per-pixel finalize
+    bool samples = n > 1;
     for (int i = 0; i < n; i++) {
         capacity += items[i].p->width * items[i].p->height;
         maxD = std::max(maxD, items[i].p->max_depth);
-        waves = std::max(waves, items[i].p->spp);
+        waves = std::max(waves, item_waves(i));
         medium = medium || items[i].view->has_medium;
+        if (items[i].accum != items[0].accum || items[i].view != items[0].view || items[i].bvh != items[0].bvh ||
+            items[i].root != items[0].root || items[i].p->width != items[0].p->width ||
+            items[i].p->height != items[0].p->height || items[i].sample0 != i)
+            samples = false;
     }
     mc_status st;
     if ((st = ensure_wave(ctx, capacity)) != MC_OK) return st;
@@ -1081,7 +1115,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.err = ctx->d_error;
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
-    if (n == 1) set_single_scene(ta, items[0].bvh ? items[0].bvh : bvh, items[0].root, items[0].view);
+    if (n == 1 || samples) set_single_scene(ta, items[0].bvh ? items[0].bvh : bvh, items[0].root, items[0].view);
+    if (samples) ta.sceneOf = nullptr;  // one scene: the trace reads it from kernel parameters
 
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
@@ -1162,6 +1197,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                                                               train ? guide->records : nullptr, guide->batch,
                                                               guide->batch_count,
                                                               guide->cfg.batch_capacity * guide->cfg.train_steps);
+        } else if (samples) {
+            k_finalize_samples<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         } else {
             k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb);
         }
@@ -1184,7 +1221,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                                       (unsigned long long)capacity,
                                       (unsigned long long)maxD,
                                       (unsigned long long)((layout << 6) | (medium ? 2 : 0) | (philox ? 4 : 0) |
-                                                           (persistent ? 8 : 0) | (n > 1 ? 16 : 0)),
+                                                           (persistent ? 8 : 0) | (n > 1 ? 16 : 0) |
+                                                           (samples ? 32 : 0)),
                                       (unsigned long long)isect,
                                       (unsigned long long)ta.refill,
                                       (unsigned long long)(uintptr_t)ta.ts0.nodes,
@@ -1230,8 +1268,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         WaveTable* h = next_host_table(ctx, &slot);
         int off = 0, k = 0;
         for (int i = 0; i < n; i++) {
-            if (items[i].p->spp <= wv) continue;
-            h->scenes[k++] = scene_gpu(ctx, bvh, items[i], off, (uint32_t)(items[i].p->first_sample + wv));
+            if (item_waves(i) <= wv) continue;
+            const int sample = items[i].p->first_sample + items[i].sample0 + wv * items[i].stride;
+            h->scenes[k++] = scene_gpu(ctx, bvh, items[i], off, (uint32_t)sample);
             off += items[i].p->width * items[i].p->height;
         }
         h->nScenes = k;
@@ -1322,7 +1361,8 @@ mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items
     mc_status st = run_waves(ctx, bvh, items, n, useGraph, stats != nullptr, &tm, guide, train);
     if (st != MC_OK) return st;
     long long paths = 0;
-    for (int i = 0; i < n; i++) paths += (long long)items[i].p->width * items[i].p->height * items[i].p->spp;
+    for (int i = 0; i < n; i++)
+        paths += (long long)items[i].p->width * items[i].p->height * (items[i].waves >= 0 ? items[i].waves : items[i].p->spp);
     return finish_stats(ctx, tm, paths, stats);
 }
 
@@ -1354,8 +1394,32 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
     if (params->rng == MC_RNG_XORWOW && (!ctx->rng_ready || ctx->rng_pixels < pixels || ctx->rng_seed != params->seed)) {
         if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
     }
-    mc::WaveItem it{scene, params, d_accum, bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
-    return mc::render_items(ctx, bvh, &it, 1, params->use_graph != 0, stats);
+    const int root = bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0];
+    // samples per wave: the tail bounces (few rays, a few long traversals set
+    // the launch time) and the launch sequence are then paid once per wave
+    int k = 1;
+    if (params->rng == MC_RNG_PHILOX && params->spp > 1) {
+        if (params->samples_per_wave > 0) {
+            k = std::min(params->samples_per_wave, params->spp);
+        } else if (params->samples_per_wave == 0) {
+            // up to 32M paths per wave (about 4.5 GB of path and queue state)
+            const long long perWave = 32ll << 20;
+            k = (int)std::max(1ll, std::min<long long>({perWave / pixels, 16ll, (long long)params->spp}));
+        }
+    }
+    k = std::min(k, MC_WAVE_MAX_SCENES);
+    if (params->queue_capacity > 0 && k > 1) k = 1;  // a fixed queue capacity is one image's paths
+    if ((long long)k * pixels >= (1ll << 30)) k = 1;
+    std::vector<mc::WaveItem> items((size_t)k);
+    for (int j = 0; j < k; j++) {
+        items[j] = mc::WaveItem{scene, params, d_accum, root, 0};
+        if (k > 1) {
+            items[j].sample0 = j;
+            items[j].stride = k;
+            items[j].waves = (params->spp - j + k - 1) / k;
+        }
+    }
+    return mc::render_items(ctx, bvh, items.data(), k, params->use_graph != 0, stats);
 }
 
 mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_item* items, int32_t count, int32_t use_graph,

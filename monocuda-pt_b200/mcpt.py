@@ -128,7 +128,7 @@ class RenderParams(C.Structure):
                 ("first_sample", C.c_int32), ("max_depth", C.c_int32), ("persistent", C.c_int32), ("rng", C.c_int32),
                 ("seed", C.c_uint64), ("intersector", C.c_int32), ("disable_clamp", C.c_int32),
                 ("queue_capacity", C.c_int32), ("refill_threshold", C.c_int32), ("use_graph", C.c_int32),
-                ("instrument", C.c_int32)]
+                ("instrument", C.c_int32), ("samples_per_wave", C.c_int32)]
 
 
 class GuideConfig(C.Structure):
@@ -191,8 +191,8 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 80, RenderParams: 232,
-         ServerConfig: 24, ServerRequest: 248, ServerResult: 56, ServerStats: 64}
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 80, RenderParams: 240,
+         ServerConfig: 24, ServerRequest: 256, ServerResult: 56, ServerStats: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
 
@@ -598,7 +598,8 @@ def make_camera(width, height, look_from, look_at, vfov, focus, max_depth=8, spp
 
 
 def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RNG_PHILOX, seed=1234, first_sample=0,
-                  intersector=ISECT_REFERENCE, disable_clamp=False, refill_threshold=0, use_graph=False, instrument=0):
+                  intersector=ISECT_REFERENCE, disable_clamp=False, refill_threshold=0, use_graph=False, instrument=0,
+                  samples_per_wave=0):
     p = RenderParams()
     p.camera = camera
     p.width, p.height, p.spp, p.first_sample, p.max_depth = width, height, spp, first_sample, max_depth
@@ -611,6 +612,7 @@ def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RN
     p.refill_threshold = refill_threshold
     p.use_graph = 1 if use_graph else 0
     p.instrument = instrument
+    p.samples_per_wave = samples_per_wave
     return p
 
 
