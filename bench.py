@@ -189,11 +189,17 @@ def cpu_baseline(scene, args):
     rows = max(8, min(H, int(args.cpu_seconds / per_row)))
     spp = max(1, int(round(args.cpu_seconds / (per_row * rows)))) if rows == H else 1
     y0 = max(0, H // 2 - rows // 2)
-    acc[:] = 0
-    t0 = time.perf_counter()
-    orc.orc_render(h, C.addressof(cam), W, H, spp, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
-                   stats.ctypes.data)
-    dt = time.perf_counter() - t0
+    for attempt in range(2):
+        acc[:] = 0
+        t0 = time.perf_counter()
+        orc.orc_render(h, C.addressof(cam), W, H, spp, 0, 8, 1234, 0, 0, 0, y0, W, y0 + rows, threads, acc.ctypes.data,
+                       stats.ctypes.data)
+        dt = time.perf_counter() - t0
+        # the middle rows cost more than the average row: when the whole image
+        # ran well short of the budget, rescale the samples once
+        if rows < H or dt >= 0.5 * args.cpu_seconds:
+            break
+        spp = max(spp + 1, int(round(spp * args.cpu_seconds / max(dt, 1e-3))))
     orc.orc_scene_destroy(h)
     rays = stats[0] + stats[1]
     return {"value": round(rays / dt / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "port",
@@ -322,6 +328,11 @@ def run_ours(args):
     mcpt.check(ctx.lib.mc_render_host(ctx.handle, C.addressof(tris), len(tris), None, 0, C.byref(ds.env), C.byref(pc),
                                       host_cold.data_ptr(), C.byref(cold_stats)))
     cold_s = time.perf_counter() - t0
+    # the same call again: the context's pinned staging and wave state exist now
+    t0 = time.perf_counter()
+    mcpt.check(ctx.lib.mc_render_host(ctx.handle, C.addressof(tris), len(tris), None, 0, C.byref(ds.env), C.byref(pc),
+                                      host_cold.data_ptr(), None))
+    cold2_s = time.perf_counter() - t0
 
     # the cold call's stages one by one, from the same pageable host array:
     # mc_scene_ingest_host (upload through the context's pinned staging, which
@@ -392,7 +403,8 @@ def run_ours(args):
                 "h2d_bytes_per_step": C.sizeof(mcpt.RenderParams), "d2h_bytes_per_step": W * H * 12,
                 "note": "scene and BVH resident; per step: render call with host params + accumulation read-back"},
         "e2e_cold": {"value": round((cold_stats.extend_rays + cold_stats.shadow_rays) / cold_s / 1e6, 2), "unit": "Mrays/s",
-                     "seconds": round(cold_s, 3), "h2d_bytes": len(tris) * 224, "d2h_bytes": W * H * 12,
+                     "seconds": round(cold_s, 3), "seconds_second_call": round(cold2_s, 3),
+                     "h2d_bytes": len(tris) * 224, "d2h_bytes": W * H * 12,
                      "stages": stages,
                      "note": "mc_render_host: host triangles -> upload, device ingestion (bounds, lights, split), "
                              "BVH build, %d spp, read-back" % S},
