@@ -34,6 +34,9 @@
     } while (0)
 
 #define MC_WAVE_MAX_SCENES 128
+#ifndef MC_WAVE_INTERLEAVE
+#define MC_WAVE_INTERLEAVE 1
+#endif
 
 namespace mc {
 
@@ -52,6 +55,7 @@ struct SceneGPU {
     int lightCount;
     int W, H;
     int pathOffset;
+    int pathStride;  // paths of this item are pathOffset + pixel * pathStride
     int paths;
     int maxDepth;
     int disableClamp;
@@ -64,7 +68,8 @@ struct SceneGPU {
 struct WaveTable {
     int nScenes;
     int totalPaths;
-    int pad0, pad1;
+    int interleave;  // > 0: the items are samples of one image, path = pixel * interleave + item
+    int pad1;
     SceneGPU scenes[MC_WAVE_MAX_SCENES];
 };
 
@@ -79,7 +84,13 @@ MC_D unsigned lanemask_lt() {
 }
 
 MC_D int scene_of(const WaveTable* tab, const unsigned short* sceneOf, int path) {
+    if (tab->interleave > 0) return path % tab->interleave;
     return (tab->nScenes > 1 && sceneOf) ? (int)sceneOf[path] : 0;
+}
+
+MC_D int pixel_of(const SceneGPU& S, int path) {
+    const int r = path - S.pathOffset;
+    return S.pathStride == 1 ? r : r / S.pathStride;
 }
 
 // ---------------------------------------------------------------------------
@@ -381,11 +392,11 @@ template <class Rng>
 MC_D void rng_load(const ShadeArgs& a, const SceneGPU& S, int p, Rng& rng);
 template <>
 MC_D void rng_load<PhiloxRng>(const ShadeArgs& a, const SceneGPU& S, int p, PhiloxRng& rng) {
-    rng.init(S.seedLo, S.seedHi, S.sample, (uint32_t)(p - S.pathOffset), a.draw[p]);
+    rng.init(S.seedLo, S.seedHi, S.sample, (uint32_t)pixel_of(S, p), a.draw[p]);
 }
 template <>
 MC_D void rng_load<XorwowRng>(const ShadeArgs& a, const SceneGPU& S, int p, XorwowRng& rng) {
-    rng.st = S.xorwow[p - S.pathOffset];
+    rng.st = S.xorwow[pixel_of(S, p)];
 }
 template <class Rng>
 MC_D void rng_store(const ShadeArgs& a, const SceneGPU& S, int p, const Rng& rng);
@@ -395,7 +406,7 @@ MC_D void rng_store<PhiloxRng>(const ShadeArgs& a, const SceneGPU& S, int p, con
 }
 template <>
 MC_D void rng_store<XorwowRng>(const ShadeArgs& a, const SceneGPU& S, int p, const XorwowRng& rng) {
-    S.xorwow[p - S.pathOffset] = rng.st;
+    S.xorwow[pixel_of(S, p)] = rng.st;
 }
 
 struct MatView {
@@ -657,8 +668,11 @@ MC_D int warp_reserve(bool want, int* counter, unsigned ltmask) {
     return want ? base + __popc(m & ltmask) : -1;
 }
 
+// 4 resident blocks (64 registers, a few spills) beat 2 blocks of 113
+// registers by 5 %: shading waits on scattered loads (hit, material, light,
+// texture) and more warps hide more of that latency.
 template <class Rng, bool GUIDED>
-__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
+__global__ void __launch_bounds__(256, GUIDED ? 2 : 4) k_shade(ShadeArgs a) {
     const unsigned ltmask = lanemask_lt();
     const int count = *a.count;
     for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
@@ -737,10 +751,10 @@ __global__ void k_camera(CameraArgs a) {
     const int total = a.tab->totalPaths;
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.count = total;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
-        int sid = a.tab->nScenes > 1 ? find_scene(a.tab, p) : 0;
+        int sid = a.tab->interleave > 0 ? p % a.tab->interleave : (a.tab->nScenes > 1 ? find_scene(a.tab, p) : 0);
         const SceneGPU& S = a.tab->scenes[sid];
-        if (a.tab->nScenes > 1) a.sceneOf[p] = (unsigned short)sid;
-        int pixel = p - S.pathOffset;
+        if (a.tab->nScenes > 1 && a.sceneOf) a.sceneOf[p] = (unsigned short)sid;
+        int pixel = pixel_of(S, p);
         int px = pixel % S.W, py = pixel / S.W;
         Rng rng;
         camera_rng(S, pixel, rng);
@@ -768,7 +782,7 @@ __global__ void k_finalize(const WaveTable* tab, const unsigned short* sceneOf, 
         float bright = fmaxf(s.x, fmaxf(s.y, s.z));
         const float maxBright = 10.0f;
         if (!S.disableClamp && bright > maxBright) s = s * (maxBright / bright);
-        float* acc = S.accum + (size_t)(p - S.pathOffset) * 3;
+        float* acc = S.accum + (size_t)pixel_of(S, p) * 3;
         acc[0] = acc[0] + s.x;
         acc[1] = acc[1] + s.y;
         acc[2] = acc[2] + s.z;
@@ -786,7 +800,7 @@ __global__ void k_finalize_samples(const WaveTable* tab, const float* sr, const 
         float a0 = acc[0], a1 = acc[1], a2 = acc[2];
         for (int j = 0; j < n; j++) {
             const SceneGPU& S = tab->scenes[j];
-            const int p = S.pathOffset + q;
+            const int p = S.pathOffset + q * S.pathStride;
             V3 s(sr[p], sg[p], sb[p]);
             float bright = fmaxf(s.x, fmaxf(s.y, s.z));
             const float maxBright = 10.0f;
@@ -822,7 +836,7 @@ __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sc
             V3 s = smp + V3(nr[p], ng[p], nb[p]);
             float bright = fmaxf(s.x, fmaxf(s.y, s.z));
             if (!S.disableClamp && bright > 10.0f) s = s * (10.0f / bright);
-            float* acc = S.accum + (size_t)(p - S.pathOffset) * 3;
+            float* acc = S.accum + (size_t)pixel_of(S, p) * 3;
             acc[0] = acc[0] + s.x;
             acc[1] = acc[1] + s.y;
             acc[2] = acc[2] + s.z;
@@ -1014,6 +1028,7 @@ static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* shared, const WaveItem&
     g.W = it.p->width;
     g.H = it.p->height;
     g.pathOffset = pathOffset;
+    g.pathStride = 1;
     g.paths = it.p->width * it.p->height;
     g.maxDepth = it.p->max_depth;
     g.disableClamp = it.p->disable_clamp;
@@ -1081,7 +1096,10 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     const int plainBlocks = (2 * capacity + 255) / 256;
     const int loopBlocks = ctx->sm_count * 8;
     const WaveTable* dtab = (const WaveTable*)ctx->d_table;
-    unsigned short* sceneOf = n > 1 ? ctx->scene_of : nullptr;
+    // samples of one image: pixel-major paths (the samples of a pixel share
+    // a warp), the item is the path index modulo the samples in the wave
+    const bool interleave = samples && MC_WAVE_INTERLEAVE;
+    unsigned short* sceneOf = n > 1 && !interleave ? ctx->scene_of : nullptr;
 
     CameraArgs ca;
     ca.tab = dtab;
@@ -1275,6 +1293,15 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         }
         h->nScenes = k;
         h->totalPaths = off;
+        h->interleave = 0;
+        h->pad1 = 0;
+        if (interleave) {
+            h->interleave = k;
+            for (int j = 0; j < k; j++) {
+                h->scenes[j].pathOffset = j;
+                h->scenes[j].pathStride = k;
+            }
+        }
         size_t bytes = offsetof(WaveTable, scenes) + (size_t)std::max(k, 1) * sizeof(SceneGPU);
         MC_CUDA(cudaMemcpyAsync(ctx->d_table, h, bytes, cudaMemcpyHostToDevice, stream));
         MC_CUDA(cudaEventRecord((cudaEvent_t)ctx->table_events[slot], stream));
