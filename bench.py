@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--server-rates", type=float, nargs="+", default=[1, 4, 16, 64], help="arrival rates (requests/s)")
     ap.add_argument("--server-requests", type=int, default=64,
                     help="requests per arrival rate (at most; max(24, 16 x rate) at low rates)")
-    ap.add_argument("--server-sps", type=int, default=4, help="samples per server step")
+    ap.add_argument("--server-sps", type=int, default=16, help="samples per server step")
     ap.add_argument("--server-wave-paths", type=int, default=0, help="paths per server wave (0 = 4M)")
     return ap.parse_args()
 

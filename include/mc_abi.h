@@ -646,7 +646,7 @@ typedef struct mc_server mc_server;
 typedef struct mc_server_config {
     int64_t hbm_budget_bytes;   /* 0 = 150 GB */
     int32_t max_active;         /* requests admitted at a time (<= 128); 0 = 128 */
-    int32_t samples_per_step;   /* 0 = 1 */
+    int32_t samples_per_step;   /* 0 = 16 (traced in one wave per step for plain requests) */
     int64_t wave_paths;         /* paths a step renders per sample: the oldest active request,
                                    then the ones with the least remaining work while they fit;
                                    0 = 4194304 */

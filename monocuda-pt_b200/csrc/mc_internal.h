@@ -169,12 +169,9 @@ struct WaveItem {
     int root;
     int segment;
     const mc_bvh* bvh = nullptr;
-    // Samples of the item: p->first_sample + sample0 + wave * stride for its
-    // first `waves` waves (waves < 0: p->spp waves of stride 1). Several items
-    // of one image with strides k and offsets 0..k-1 trace k samples per wave.
-    int sample0 = 0;
-    int stride = 1;
-    int waves = -1;
+    // Samples of this item traced together in one wave (pixel-major: the
+    // samples of a pixel are neighbouring paths). Counter-based RNG only.
+    int spw = 1;
 };
 
 // Renders the items' samples in shared waves (mc_render.cu).

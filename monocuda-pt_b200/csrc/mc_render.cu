@@ -34,9 +34,6 @@
     } while (0)
 
 #define MC_WAVE_MAX_SCENES 128
-#ifndef MC_WAVE_INTERLEAVE
-#define MC_WAVE_INTERLEAVE 1
-#endif
 
 namespace mc {
 
@@ -54,8 +51,12 @@ struct SceneGPU {
     int hasMedium;
     int lightCount;
     int W, H;
+    // This item's paths in the wave: pathOffset + pixel * pathStride + j for its
+    // j = 0..pathStride-1 samples of the wave (sample index `sample` + j):
+    // the samples of a pixel are neighbours, so they share warps.
     int pathOffset;
-    int pathStride;  // paths of this item are pathOffset + pixel * pathStride
+    int pathStride;
+    int pixelOffset;  // first pixel of this item among the wave's pixels
     int paths;
     int maxDepth;
     int disableClamp;
@@ -68,7 +69,7 @@ struct SceneGPU {
 struct WaveTable {
     int nScenes;
     int totalPaths;
-    int interleave;  // > 0: the items are samples of one image, path = pixel * interleave + item
+    int totalPixels;  // pixels of all items (each holds pathStride paths)
     int pad1;
     SceneGPU scenes[MC_WAVE_MAX_SCENES];
 };
@@ -84,13 +85,16 @@ MC_D unsigned lanemask_lt() {
 }
 
 MC_D int scene_of(const WaveTable* tab, const unsigned short* sceneOf, int path) {
-    if (tab->interleave > 0) return path % tab->interleave;
     return (tab->nScenes > 1 && sceneOf) ? (int)sceneOf[path] : 0;
 }
 
 MC_D int pixel_of(const SceneGPU& S, int path) {
     const int r = path - S.pathOffset;
     return S.pathStride == 1 ? r : r / S.pathStride;
+}
+
+MC_D uint32_t sample_of(const SceneGPU& S, int path) {
+    return S.pathStride == 1 ? S.sample : S.sample + (uint32_t)((path - S.pathOffset) % S.pathStride);
 }
 
 // ---------------------------------------------------------------------------
@@ -392,7 +396,7 @@ template <class Rng>
 MC_D void rng_load(const ShadeArgs& a, const SceneGPU& S, int p, Rng& rng);
 template <>
 MC_D void rng_load<PhiloxRng>(const ShadeArgs& a, const SceneGPU& S, int p, PhiloxRng& rng) {
-    rng.init(S.seedLo, S.seedHi, S.sample, (uint32_t)pixel_of(S, p), a.draw[p]);
+    rng.init(S.seedLo, S.seedHi, sample_of(S, p), (uint32_t)pixel_of(S, p), a.draw[p]);
 }
 template <>
 MC_D void rng_load<XorwowRng>(const ShadeArgs& a, const SceneGPU& S, int p, XorwowRng& rng) {
@@ -741,8 +745,8 @@ MC_D int find_scene(const WaveTable* tab, int p) {
     return lo;
 }
 
-MC_D void camera_rng(const SceneGPU& S, int pixel, PhiloxRng& rng) { rng.init(S.seedLo, S.seedHi, S.sample, (uint32_t)pixel, 0u); }
-MC_D void camera_rng(const SceneGPU& S, int pixel, XorwowRng& rng) { rng.st = S.xorwow[pixel]; }
+MC_D void camera_rng(const SceneGPU& S, int pixel, uint32_t sample, PhiloxRng& rng) { rng.init(S.seedLo, S.seedHi, sample, (uint32_t)pixel, 0u); }
+MC_D void camera_rng(const SceneGPU& S, int pixel, uint32_t, XorwowRng& rng) { rng.st = S.xorwow[pixel]; }
 MC_D void camera_rng_store(const CameraArgs& a, const SceneGPU& S, int p, int pixel, const PhiloxRng& rng) { a.draw[p] = rng.draw; }
 MC_D void camera_rng_store(const CameraArgs& a, const SceneGPU& S, int p, int pixel, const XorwowRng& rng) { S.xorwow[pixel] = rng.st; }
 
@@ -751,13 +755,13 @@ __global__ void k_camera(CameraArgs a) {
     const int total = a.tab->totalPaths;
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.count = total;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
-        int sid = a.tab->interleave > 0 ? p % a.tab->interleave : (a.tab->nScenes > 1 ? find_scene(a.tab, p) : 0);
+        int sid = a.tab->nScenes > 1 ? find_scene(a.tab, p) : 0;
         const SceneGPU& S = a.tab->scenes[sid];
         if (a.tab->nScenes > 1 && a.sceneOf) a.sceneOf[p] = (unsigned short)sid;
         int pixel = pixel_of(S, p);
         int px = pixel % S.W, py = pixel / S.W;
         Rng rng;
-        camera_rng(S, pixel, rng);
+        camera_rng(S, pixel, sample_of(S, p), rng);
         V3 o, d;
         float t;
         camera_ray(S.cam, px, py, rng, o, d, t);
@@ -773,34 +777,28 @@ __global__ void k_camera(CameraArgs a) {
     }
 }
 
-__global__ void k_finalize(const WaveTable* tab, const unsigned short* sceneOf, const float* sr, const float* sg,
-                           const float* sb) {
-    const int total = tab->totalPaths;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
-        const SceneGPU& S = tab->scenes[scene_of(tab, sceneOf, p)];
-        V3 s(sr[p], sg[p], sb[p]);
-        float bright = fmaxf(s.x, fmaxf(s.y, s.z));
-        const float maxBright = 10.0f;
-        if (!S.disableClamp && bright > maxBright) s = s * (maxBright / bright);
-        float* acc = S.accum + (size_t)pixel_of(S, p) * 3;
-        acc[0] = acc[0] + s.x;
-        acc[1] = acc[1] + s.y;
-        acc[2] = acc[2] + s.z;
+MC_D int find_scene_by_pixel(const WaveTable* tab, int u) {
+    int lo = 0, hi = tab->nScenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (tab->scenes[mid].pixelOffset <= u) lo = mid;
+        else hi = mid - 1;
     }
+    return lo;
 }
 
-// Several samples of one image in one wave (items 0..n-1 of equal size, in
-// sample order): each pixel adds its samples in that order, as consecutive
-// one-sample waves would, so the sums are the same to the bit.
-__global__ void k_finalize_samples(const WaveTable* tab, const float* sr, const float* sg, const float* sb) {
-    const int pixels = tab->scenes[0].paths;
-    const int n = tab->nScenes;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pixels; q += gridDim.x * blockDim.x) {
-        float* acc = tab->scenes[0].accum + (size_t)q * 3;
+// PT:3740-3755 per-sample clamp and accumulation. One thread per pixel adds the
+// pixel's samples of the wave in sample order, as consecutive one-sample waves
+// would, so the sums are the same to the bit.
+__global__ void k_finalize(const WaveTable* tab, const float* sr, const float* sg, const float* sb) {
+    const int pixels = tab->totalPixels;
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < pixels; u += gridDim.x * blockDim.x) {
+        const SceneGPU& S = tab->scenes[tab->nScenes > 1 ? find_scene_by_pixel(tab, u) : 0];
+        const int q = u - S.pixelOffset;
+        float* acc = S.accum + (size_t)q * 3;
         float a0 = acc[0], a1 = acc[1], a2 = acc[2];
-        for (int j = 0; j < n; j++) {
-            const SceneGPU& S = tab->scenes[j];
-            const int p = S.pathOffset + q * S.pathStride;
+        for (int j = 0; j < S.pathStride; j++) {
+            const int p = S.pathOffset + q * S.pathStride + j;
             V3 s(sr[p], sg[p], sb[p]);
             float bright = fmaxf(s.x, fmaxf(s.y, s.z));
             const float maxBright = 10.0f;
@@ -1064,19 +1062,17 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     const bool timeTrace = (p0.instrument & 2) != 0;
     int capacity = 0, maxD = 0, waves = 0;
     bool medium = false;
-    auto item_waves = [&](int i) { return items[i].waves >= 0 ? items[i].waves : items[i].p->spp; };
-    // items that are samples of one image of one scene: single-scene trace
-    // launches and the ordered per-pixel finalize
-    bool samples = n > 1;
+    auto item_spw = [&](int i) { return std::max(1, std::min(items[i].spw, std::max(1, items[i].p->spp))); };
+    auto item_waves = [&](int i) { return (items[i].p->spp + item_spw(i) - 1) / item_spw(i); };
+    // every item on one scene: single-scene trace launches
+    bool sameScene = true;
     for (int i = 0; i < n; i++) {
-        capacity += items[i].p->width * items[i].p->height;
+        capacity += items[i].p->width * items[i].p->height * item_spw(i);
         maxD = std::max(maxD, items[i].p->max_depth);
         waves = std::max(waves, item_waves(i));
         medium = medium || items[i].view->has_medium;
-        if (items[i].accum != items[0].accum || items[i].view != items[0].view || items[i].bvh != items[0].bvh ||
-            items[i].root != items[0].root || items[i].p->width != items[0].p->width ||
-            items[i].p->height != items[0].p->height || items[i].sample0 != i)
-            samples = false;
+        if (items[i].view != items[0].view || items[i].bvh != items[0].bvh || items[i].root != items[0].root)
+            sameScene = false;
     }
     mc_status st;
     if ((st = ensure_wave(ctx, capacity)) != MC_OK) return st;
@@ -1096,10 +1092,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     const int plainBlocks = (2 * capacity + 255) / 256;
     const int loopBlocks = ctx->sm_count * 8;
     const WaveTable* dtab = (const WaveTable*)ctx->d_table;
-    // samples of one image: pixel-major paths (the samples of a pixel share
-    // a warp), the item is the path index modulo the samples in the wave
-    const bool interleave = samples && MC_WAVE_INTERLEAVE;
-    unsigned short* sceneOf = n > 1 && !interleave ? ctx->scene_of : nullptr;
+    unsigned short* sceneOf = n > 1 ? ctx->scene_of : nullptr;
 
     CameraArgs ca;
     ca.tab = dtab;
@@ -1133,8 +1126,11 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.err = ctx->d_error;
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
-    if (n == 1 || samples) set_single_scene(ta, items[0].bvh ? items[0].bvh : bvh, items[0].root, items[0].view);
-    if (samples) ta.sceneOf = nullptr;  // one scene: the trace reads it from kernel parameters
+    if (sameScene) {
+        // one scene: the trace reads it from kernel parameters
+        set_single_scene(ta, items[0].bvh ? items[0].bvh : bvh, items[0].root, items[0].view);
+        ta.sceneOf = nullptr;
+    }
 
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
@@ -1215,10 +1211,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                                                               train ? guide->records : nullptr, guide->batch,
                                                               guide->batch_count,
                                                               guide->cfg.batch_capacity * guide->cfg.train_steps);
-        } else if (samples) {
-            k_finalize_samples<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         } else {
-            k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb);
+            k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         }
         k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
         launches += 2;
@@ -1240,7 +1234,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                                       (unsigned long long)maxD,
                                       (unsigned long long)((layout << 6) | (medium ? 2 : 0) | (philox ? 4 : 0) |
                                                            (persistent ? 8 : 0) | (n > 1 ? 16 : 0) |
-                                                           (samples ? 32 : 0)),
+                                                           (sameScene ? 32 : 0)),
                                       (unsigned long long)isect,
                                       (unsigned long long)ta.refill,
                                       (unsigned long long)(uintptr_t)ta.ts0.nodes,
@@ -1284,24 +1278,23 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     for (int wv = 0; wv < waves; wv++) {
         int slot;
         WaveTable* h = next_host_table(ctx, &slot);
-        int off = 0, k = 0;
+        int off = 0, pix = 0, k = 0;
         for (int i = 0; i < n; i++) {
             if (item_waves(i) <= wv) continue;
-            const int sample = items[i].p->first_sample + items[i].sample0 + wv * items[i].stride;
-            h->scenes[k++] = scene_gpu(ctx, bvh, items[i], off, (uint32_t)sample);
-            off += items[i].p->width * items[i].p->height;
+            const int m = item_spw(i);
+            const int r = std::min(m, items[i].p->spp - wv * m);
+            const int px = items[i].p->width * items[i].p->height;
+            SceneGPU g = scene_gpu(ctx, bvh, items[i], off, (uint32_t)(items[i].p->first_sample + wv * m));
+            g.pathStride = r;
+            g.pixelOffset = pix;
+            h->scenes[k++] = g;
+            off += px * r;
+            pix += px;
         }
         h->nScenes = k;
         h->totalPaths = off;
-        h->interleave = 0;
+        h->totalPixels = pix;
         h->pad1 = 0;
-        if (interleave) {
-            h->interleave = k;
-            for (int j = 0; j < k; j++) {
-                h->scenes[j].pathOffset = j;
-                h->scenes[j].pathStride = k;
-            }
-        }
         size_t bytes = offsetof(WaveTable, scenes) + (size_t)std::max(k, 1) * sizeof(SceneGPU);
         MC_CUDA(cudaMemcpyAsync(ctx->d_table, h, bytes, cudaMemcpyHostToDevice, stream));
         MC_CUDA(cudaEventRecord((cudaEvent_t)ctx->table_events[slot], stream));
@@ -1388,8 +1381,7 @@ mc_status render_items(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items
     mc_status st = run_waves(ctx, bvh, items, n, useGraph, stats != nullptr, &tm, guide, train);
     if (st != MC_OK) return st;
     long long paths = 0;
-    for (int i = 0; i < n; i++)
-        paths += (long long)items[i].p->width * items[i].p->height * (items[i].waves >= 0 ? items[i].waves : items[i].p->spp);
+    for (int i = 0; i < n; i++) paths += (long long)items[i].p->width * items[i].p->height * items[i].p->spp;
     return finish_stats(ctx, tm, paths, stats);
 }
 
@@ -1434,19 +1426,11 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
             k = (int)std::max(1ll, std::min<long long>({perWave / pixels, 16ll, (long long)params->spp}));
         }
     }
-    k = std::min(k, MC_WAVE_MAX_SCENES);
     if (params->queue_capacity > 0 && k > 1) k = 1;  // a fixed queue capacity is one image's paths
     if ((long long)k * pixels >= (1ll << 30)) k = 1;
-    std::vector<mc::WaveItem> items((size_t)k);
-    for (int j = 0; j < k; j++) {
-        items[j] = mc::WaveItem{scene, params, d_accum, root, 0};
-        if (k > 1) {
-            items[j].sample0 = j;
-            items[j].stride = k;
-            items[j].waves = (params->spp - j + k - 1) / k;
-        }
-    }
-    return mc::render_items(ctx, bvh, items.data(), k, params->use_graph != 0, stats);
+    mc::WaveItem it{scene, params, d_accum, root, 0};
+    it.spw = k;
+    return mc::render_items(ctx, bvh, &it, 1, params->use_graph != 0, stats);
 }
 
 mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_item* items, int32_t count, int32_t use_graph,
@@ -1469,6 +1453,14 @@ mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_ite
                               bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[i] : bvh->bin_roots[i], i};
     }
     if (capacity >= (1ll << 30)) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: too many paths per wave");
+    // samples per wave: an item's own setting, else one for all items that
+    // keeps a wave within about 32M paths (at most 16)
+    const long long autoSpw = std::max(1ll, std::min(16ll, (32ll << 20) / std::max(1ll, capacity)));
+    for (int i = 0; i < count; i++) {
+        const int want = items[i].params.samples_per_wave;
+        its[i].spw = want > 0 ? want : want == 0 ? (int)autoSpw : 1;
+        if ((long long)items[i].params.width * items[i].params.height * its[i].spw >= (1ll << 30)) its[i].spw = 1;
+    }
     return mc::render_items(ctx, bvh, its.data(), count, use_graph != 0, stats);
 }
 

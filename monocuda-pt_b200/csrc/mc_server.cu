@@ -73,9 +73,12 @@ struct mc_server {
 
 namespace {
 
-long long request_bytes(const mc_render_params& p, bool guided) {
+// A plain request traces its step's samples in one wave (one path per pixel
+// and sample); a guided one a sample per wave.
+long long request_bytes(const mc_render_params& p, bool guided, int sps) {
     long long px = (long long)p.width * p.height;
-    return px * 12 + px * kWaveBytesPerPath + (guided ? px * kGuideBytesPerPath : 0);
+    long long spw = guided ? 1 : std::max(1, std::min(sps, p.spp));
+    return px * 12 + px * spw * kWaveBytesPerPath + (guided ? px * kGuideBytesPerPath : 0);
 }
 
 mc_status admit(mc_server* s) {
@@ -111,7 +114,7 @@ mc_status mc_server_create(mc_context* ctx, const mc_server_config* config, mc_s
     if (s->cfg.hbm_budget_bytes <= 0) s->cfg.hbm_budget_bytes = 150ll * 1000 * 1000 * 1000;
     if (s->cfg.max_active <= 0) s->cfg.max_active = 128;
     if (s->cfg.max_active > 128) s->cfg.max_active = 128;
-    if (s->cfg.samples_per_step <= 0) s->cfg.samples_per_step = 1;
+    if (s->cfg.samples_per_step <= 0) s->cfg.samples_per_step = 16;
     if (s->cfg.wave_paths <= 0) s->cfg.wave_paths = 4194304;
     s->t0 = std::chrono::steady_clock::now();
     *out = s;
@@ -167,7 +170,7 @@ mc_status mc_server_submit(mc_server* s, const mc_server_request* req, int64_t* 
     r.scene = req->scene_id;
     r.params = req->params;
     r.guided = req->guided != 0;
-    r.bytes = request_bytes(r.params, r.guided);
+    r.bytes = request_bytes(r.params, r.guided, s->cfg.samples_per_step);
     if (r.bytes + s->scene_bytes > s->cfg.hbm_budget_bytes)
         return mc::set_error(MC_ERR_BUDGET, "mc_server_submit: the request needs %lld bytes, more than the budget leaves",
                              r.bytes);
@@ -226,6 +229,7 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
         const ServerScene& sc = s->scenes[(size_t)r.scene];
         mc::WaveItem it{&sc.view, &params[i], r.accum, sc.bvh->wide_roots[0], 0};
         it.bvh = sc.bvh;
+        it.spw = params[i].spp;  // the step's samples in one wave, pixel-major
         items.push_back(it);
     }
     if (!items.empty()) {
@@ -233,9 +237,7 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
         st = mc::render_items(s->ctx, items[0].bvh, items.data(), (int)items.size(), false, &rs);
         if (st != MC_OK) return st;
         s->rays += rs.extend_rays + rs.shadow_rays;
-        int w = 0;
-        for (const auto& p : params) w = std::max(w, p.spp);
-        s->waves += w;
+        s->waves += 1;  // each request's step samples share the one wave
         for (size_t i = 0; i < ids.size(); i++) s->requests[ids[i]].done += params[i].spp;
     }
     // guided requests: the ones of each scene share waves and the scene's

@@ -677,7 +677,7 @@ class Server:
     """The render server (mc_server_*): resident scenes, HBM-budget admission,
     shared waves for all active requests."""
 
-    def __init__(self, ctx, budget_bytes=0, max_active=0, samples_per_step=1, wave_paths=0):
+    def __init__(self, ctx, budget_bytes=0, max_active=0, samples_per_step=0, wave_paths=0):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = ServerConfig(budget_bytes, max_active, samples_per_step, wave_paths)

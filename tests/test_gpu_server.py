@@ -73,9 +73,10 @@ def test_admission_follows_the_budget(ctx):
     scene_bytes = probe.stats().scene_bytes
     probe.close()
     W = 64
+    # one sample per step: a request's share of the wave buffers is one path per pixel
     per_request = W * W * (12 + 29 * 4 + 1 + 16 + 2)
     # room for the scene and one request at a time
-    srv = mcpt.Server(ctx, budget_bytes=scene_bytes + per_request + per_request // 2)
+    srv = mcpt.Server(ctx, budget_bytes=scene_bytes + per_request + per_request // 2, samples_per_step=1)
     sid = srv.add_scene(d)
     a = srv.submit(sid, _params(s, W, 3))
     b = srv.submit(sid, _params(s, W, 2))
