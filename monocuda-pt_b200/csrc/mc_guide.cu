@@ -774,9 +774,22 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
     return MC_OK;
 }
 
-mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity) {
+mc_status guide_reserve_batch(mc_guide* g, int records) {
+    if (g->batch_records >= records) return MC_OK;
+    float* nb = nullptr;
+    if (cudaMalloc(&nb, (size_t)records * MC_GUIDE_RECORD_FLOATS * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MC_ERR_OOM, "guide: allocation of the training batch failed");
+    }
+    cudaFree(g->batch);
+    g->batch = nb;
+    g->batch_records = records;
+    return MC_OK;
+}
+
+mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps) {
     const int B = g->cfg.batch_capacity;
-    for (int i = 0; i < g->cfg.train_steps; i++) {
+    for (int i = 0; i < steps; i++) {
         const int off = i * B;
         const float* r = records + (size_t)off * MC_GUIDE_RECORD_FLOATS;
         k_guide_weight_scale<<<1, 1024, 0, s>>>(r, 0, count, off, capacity, B, g->scale);
@@ -813,6 +826,7 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
                    cudaMalloc(&g->scale, sizeof(float)) == cudaSuccess && cudaMalloc(&g->loss, sizeof(double)) == cudaSuccess &&
                    cudaMalloc(&g->batch, (size_t)g->cfg.batch_capacity * g->cfg.train_steps * MC_GUIDE_RECORD_FLOATS *
                                              sizeof(float)) == cudaSuccess &&
+                   (g->batch_records = g->cfg.batch_capacity * g->cfg.train_steps) > 0 &&
                    cudaMalloc(&g->batch_count, sizeof(int)) == cudaSuccess;
     if (!okAlloc) {
         cudaGetLastError();

@@ -141,6 +141,7 @@ struct mc_guide {
     float* scale = nullptr;            // device: weight normalization of the current step
     double* loss = nullptr;            // device: loss accumulator
     float* batch = nullptr;            // training records of guided renders
+    int batch_records = 0;             // records the batch buffer holds
     int* batch_count = nullptr;
     float* records = nullptr;          // per-path primary-vertex records of guided renders
     int record_capacity = 0;
@@ -188,6 +189,9 @@ mc_status context_counters(mc_context* ctx);
 mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
                             const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
                             const float* dz, const mc_packed_hit* hits, float* mixtures);
-mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity);
+// `steps` Adam steps, each on cfg.batch_capacity of the records.
+mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps);
+// Grows the training batch buffer to hold `records` records.
+mc_status guide_reserve_batch(mc_guide* g, int records);
 mc_status guide_reserve_paths(mc_guide* g, int paths);
 }

@@ -821,6 +821,28 @@ __global__ void k_finalize(const WaveTable* tab, const float* sr, const float* s
 __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sceneOf, const float* sr, const float* sg,
                                   const float* sb, const float* nr, const float* ng, const float* nb, const float* rec,
                                   float* batch, int* batchCount, int capacity) {
+    // the image: each pixel adds its samples of the wave in sample order
+    const int pixels = tab->totalPixels;
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < pixels; u += gridDim.x * blockDim.x) {
+        const SceneGPU& S = tab->scenes[tab->nScenes > 1 ? find_scene_by_pixel(tab, u) : 0];
+        const int q = u - S.pixelOffset;
+        float* acc = S.accum + (size_t)q * 3;
+        float a0 = acc[0], a1 = acc[1], a2 = acc[2];
+        for (int j = 0; j < S.pathStride; j++) {
+            const int p = S.pathOffset + q * S.pathStride + j;
+            V3 s = V3(sr[p], sg[p], sb[p]) + V3(nr[p], ng[p], nb[p]);
+            float bright = fmaxf(s.x, fmaxf(s.y, s.z));
+            if (!S.disableClamp && bright > 10.0f) s = s * (10.0f / bright);
+            a0 = a0 + s.x;
+            a1 = a1 + s.y;
+            a2 = a2 + s.z;
+        }
+        acc[0] = a0;
+        acc[1] = a1;
+        acc[2] = a2;
+    }
+    if (!rec) return;
+    // the training records, one per path with a primary-vertex record
     const unsigned ltmask = lanemask_lt();
     const int total = tab->totalPaths;
     const int stride = gridDim.x * blockDim.x;
@@ -828,20 +850,9 @@ __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sc
         const int p = base + threadIdx.x;
         bool emit = false;
         float w = 0.f;
-        if (p < total) {
-            const SceneGPU& S = tab->scenes[scene_of(tab, sceneOf, p)];
-            V3 smp(sr[p], sg[p], sb[p]);
-            V3 s = smp + V3(nr[p], ng[p], nb[p]);
-            float bright = fmaxf(s.x, fmaxf(s.y, s.z));
-            if (!S.disableClamp && bright > 10.0f) s = s * (10.0f / bright);
-            float* acc = S.accum + (size_t)pixel_of(S, p) * 3;
-            acc[0] = acc[0] + s.x;
-            acc[1] = acc[1] + s.y;
-            acc[2] = acc[2] + s.z;
-            if (rec && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
-                w = (smp.x + smp.y + smp.z) * (1.0f / 3.0f) + rec[(size_t)p * kRecFloats + 11];
-                emit = w > 0.0f && w < 1e30f;
-            }
+        if (p < total && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
+            w = (sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) + rec[(size_t)p * kRecFloats + 11];
+            emit = w > 0.0f && w < 1e30f;
         }
         unsigned m = __ballot_sync(kFull, emit);
         if (m) {
@@ -1142,6 +1153,12 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         traceEvents.push_back(e);
     };
     int launches = 0;
+    int waveR = 1;  // samples per pixel in the current wave (the most any item traces)
+    if (guide && train) {
+        int maxR = 1;
+        for (int i = 0; i < n; i++) maxR = std::max(maxR, item_spw(i));
+        if ((st = guide_reserve_batch(guide, guide->cfg.batch_capacity * guide->cfg.train_steps * maxR)) != MC_OK) return st;
+    }
     // the launch sequence of one wave (device table already holds the wave)
     float* nee0[3] = {nullptr, nullptr, nullptr};
     if (guide) {
@@ -1210,17 +1227,19 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
                                                               train ? guide->records : nullptr, guide->batch,
                                                               guide->batch_count,
-                                                              guide->cfg.batch_capacity * guide->cfg.train_steps);
+                                                              guide->cfg.batch_capacity * guide->cfg.train_steps * waveR);
         } else {
             k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         }
         k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
         launches += 2;
         if (guide && train) {
+            // as many Adam steps per sample as with one sample per wave
             mc_status gs = guide_train_device(guide, stream, guide->batch, guide->batch_count,
-                                              guide->cfg.batch_capacity * guide->cfg.train_steps);
+                                              guide->cfg.batch_capacity * guide->cfg.train_steps * waveR,
+                                              guide->cfg.train_steps * waveR);
             if (gs != MC_OK) return gs;
-            launches += 4 * guide->cfg.train_steps;
+            launches += 4 * guide->cfg.train_steps * waveR;
         }
         MC_CUDA(cudaGetLastError());
         return MC_OK;
@@ -1279,10 +1298,12 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         int slot;
         WaveTable* h = next_host_table(ctx, &slot);
         int off = 0, pix = 0, k = 0;
+        waveR = 1;
         for (int i = 0; i < n; i++) {
             if (item_waves(i) <= wv) continue;
             const int m = item_spw(i);
             const int r = std::min(m, items[i].p->spp - wv * m);
+            waveR = std::max(waveR, r);
             const int px = items[i].p->width * items[i].p->height;
             SceneGPU g = scene_gpu(ctx, bvh, items[i], off, (uint32_t)(items[i].p->first_sample + wv * m));
             g.pathStride = r;
@@ -1477,8 +1498,18 @@ mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     const int pixels = params->width * params->height;
     if (params->queue_capacity > 0 && params->queue_capacity < pixels)
         return mc::set_error(MC_ERR_INVALID, "mc_render_guided: queue capacity below width*height");
-    if ((st = mc::guide_reserve_paths(guide, pixels)) != MC_OK) return st;
+    // samples per wave as for plain renders; the guide then trains once per
+    // wave with as many Adam steps per sample as with one sample per wave
+    int k = 1;
+    if (params->spp > 1) {
+        if (params->samples_per_wave > 0) k = std::min(params->samples_per_wave, params->spp);
+        else if (params->samples_per_wave == 0)
+            k = (int)std::max(1ll, std::min<long long>({(32ll << 20) / pixels, 16ll, (long long)params->spp}));
+    }
+    if (params->queue_capacity > 0) k = 1;
+    if ((st = mc::guide_reserve_paths(guide, pixels * k)) != MC_OK) return st;
     mc::WaveItem it{scene, params, d_accum, bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0], 0};
+    it.spw = k;
     return mc::render_items(ctx, bvh, &it, 1, false, stats, guide, train != 0);
 }
 
