@@ -575,11 +575,11 @@ def run_guiding(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), st
 
-    # warm-up of both paths (kernels loaded, buffers reserved)
+    # warm-up of both paths (kernels loaded, wave buffers reserved for a chunk)
     tmp = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
-    render(tmp, 1, 999999)
+    render(tmp, chunk, 999999)
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1)
-    render(tmp, 1, 999998, warm_guide, 1)
+    render(tmp, chunk, 999998, warm_guide, 1)
     warm_guide.close()
     # reference image
     ref = torch.zeros_like(tmp)
@@ -604,6 +604,9 @@ def run_guiding(args):
     # guided, trained online from scratch
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
                        train_steps=args.guide_steps)
+    # an untimed render without training sizes the new guide's buffers; its
+    # weights stay as initialised
+    render(tmp, chunk, 999997, guide, 0)
     acc = torch.zeros_like(tmp)
     g_ms, g_curve, reached, rays_g = 0.0, [], None, 0
     spp = 0

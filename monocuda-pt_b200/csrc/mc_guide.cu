@@ -787,8 +787,9 @@ mc_status guide_reserve_batch(mc_guide* g, int records) {
     return MC_OK;
 }
 
-mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps) {
-    const int B = g->cfg.batch_capacity;
+mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps,
+                             int stepRecords) {
+    const int B = stepRecords > 0 ? std::min(stepRecords, g->cfg.batch_capacity) : g->cfg.batch_capacity;
     for (int i = 0; i < steps; i++) {
         const int off = i * B;
         const float* r = records + (size_t)off * MC_GUIDE_RECORD_FLOATS;

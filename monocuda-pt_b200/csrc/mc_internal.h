@@ -189,8 +189,10 @@ mc_status context_counters(mc_context* ctx);
 mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
                             const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
                             const float* dz, const mc_packed_hit* hits, float* mixtures);
-// `steps` Adam steps, each on cfg.batch_capacity of the records.
-mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps);
+// `steps` Adam steps, each on the next min(stepRecords, cfg.batch_capacity)
+// of the records (stepRecords <= 0: cfg.batch_capacity).
+mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps,
+                             int stepRecords);
 // Grows the training batch buffer to hold `records` records.
 mc_status guide_reserve_batch(mc_guide* g, int records);
 mc_status guide_reserve_paths(mc_guide* g, int paths);

@@ -820,7 +820,7 @@ __global__ void k_finalize(const WaveTable* tab, const float* sr, const float* s
 // appended to the training batch.
 __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sceneOf, const float* sr, const float* sg,
                                   const float* sb, const float* nr, const float* ng, const float* nb, const float* rec,
-                                  float* batch, int* batchCount, int capacity) {
+                                  float* batch, int* batchCount, int capacity, int recStride, int recPhase) {
     // the image: each pixel adds its samples of the wave in sample order
     const int pixels = tab->totalPixels;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < pixels; u += gridDim.x * blockDim.x) {
@@ -842,7 +842,10 @@ __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sc
         acc[2] = a2;
     }
     if (!rec) return;
-    // the training records, one per path with a primary-vertex record
+    // the training records, one per path with a primary-vertex record; when
+    // the wave has more paths than the batch holds, every recStride-th path
+    // (from recPhase, which the host rotates) so that records come from the
+    // whole image rather than its first rows
     const unsigned ltmask = lanemask_lt();
     const int total = tab->totalPaths;
     const int stride = gridDim.x * blockDim.x;
@@ -850,7 +853,7 @@ __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sc
         const int p = base + threadIdx.x;
         bool emit = false;
         float w = 0.f;
-        if (p < total && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
+        if (p < total && (p + recPhase) % recStride == 0 && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
             w = (sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) + rec[(size_t)p * kRecFloats + 11];
             emit = w > 0.0f && w < 1e30f;
         }
@@ -1153,7 +1156,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         traceEvents.push_back(e);
     };
     int launches = 0;
-    int waveR = 1;  // samples per pixel in the current wave (the most any item traces)
+    int waveR = 1;       // samples per pixel in the current wave (the most any item traces)
+    int wavePixels = 0;  // pixels of the current wave
+    int recStride = 1, recPhase = 0;  // training-record subsampling of the current wave
     if (guide && train) {
         int maxR = 1;
         for (int i = 0; i < n; i++) maxR = std::max(maxR, item_spw(i));
@@ -1227,17 +1232,19 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
                                                               train ? guide->records : nullptr, guide->batch,
                                                               guide->batch_count,
-                                                              guide->cfg.batch_capacity * guide->cfg.train_steps * waveR);
+                                                              guide->cfg.batch_capacity * guide->cfg.train_steps * waveR,
+                                                              recStride, recPhase);
         } else {
             k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         }
         k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
         launches += 2;
         if (guide && train) {
-            // as many Adam steps per sample as with one sample per wave
+            // as many Adam steps per sample, on as many records each, as with
+            // one sample per wave (a sample holds at most a record per pixel)
             mc_status gs = guide_train_device(guide, stream, guide->batch, guide->batch_count,
                                               guide->cfg.batch_capacity * guide->cfg.train_steps * waveR,
-                                              guide->cfg.train_steps * waveR);
+                                              guide->cfg.train_steps * waveR, wavePixels);
             if (gs != MC_OK) return gs;
             launches += 4 * guide->cfg.train_steps * waveR;
         }
@@ -1315,6 +1322,12 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         h->nScenes = k;
         h->totalPaths = off;
         h->totalPixels = pix;
+        wavePixels = pix;
+        if (guide) {
+            const long long cap = (long long)guide->cfg.batch_capacity * guide->cfg.train_steps * waveR;
+            recStride = (int)std::max(1ll, (off + cap - 1) / cap);
+            recPhase = wv % recStride;
+        }
         h->pad1 = 0;
         size_t bytes = offsetof(WaveTable, scenes) + (size_t)std::max(k, 1) * sizeof(SceneGPU);
         MC_CUDA(cudaMemcpyAsync(ctx->d_table, h, bytes, cudaMemcpyHostToDevice, stream));
@@ -1498,13 +1511,15 @@ mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_scene_vi
     const int pixels = params->width * params->height;
     if (params->queue_capacity > 0 && params->queue_capacity < pixels)
         return mc::set_error(MC_ERR_INVALID, "mc_render_guided: queue capacity below width*height");
-    // samples per wave as for plain renders; the guide then trains once per
-    // wave with as many Adam steps per sample as with one sample per wave
+    // several samples per wave as for plain renders, but at most 4 by
+    // default: the guide trains once per wave (with as many Adam steps per
+    // sample as with one sample per wave), and every record of a wave comes
+    // from the same weights, so shorter waves keep the feedback tighter
     int k = 1;
     if (params->spp > 1) {
         if (params->samples_per_wave > 0) k = std::min(params->samples_per_wave, params->spp);
         else if (params->samples_per_wave == 0)
-            k = (int)std::max(1ll, std::min<long long>({(32ll << 20) / pixels, 16ll, (long long)params->spp}));
+            k = (int)std::max(1ll, std::min<long long>({(32ll << 20) / pixels, 4ll, (long long)params->spp}));
     }
     if (params->queue_capacity > 0) k = 1;
     if ((st = mc::guide_reserve_paths(guide, pixels * k)) != MC_OK) return st;
