@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = the named workload)")
     ap.add_argument("--layout", default="wide4", choices=["binary", "wide4", "wide4q"], help="BVH node layout traversed")
+    ap.add_argument("--builder", default="clustered", choices=["clustered", "lbvh"],
+                    help="binary tree the wide layouts collapse: clustered (PLOC) or the reference's LBVH")
     ap.add_argument("--refill", type=int, default=0,
                     help="trace refill threshold; 0 = the library autotuner's choice (a fixed value keeps profiles "
                          "free of the autotuner's probe launches)")
@@ -221,7 +223,8 @@ def run_ours(args):
     ctx = mcpt.Context(local)
     ds = mcpt.DeviceScene(tris, env_rgba=env, env_intensity=scene.env_intensity, device=dev)
     layout = {"binary": mcpt.LAYOUT_BINARY, "wide4": mcpt.LAYOUT_WIDE4, "wide4q": mcpt.LAYOUT_WIDE4Q}[args.layout]
-    bvh = mcpt.Bvh(ctx, ds.view, layout=layout)
+    builder = {"clustered": mcpt.BUILDER_CLUSTERED, "lbvh": mcpt.BUILDER_LBVH}[args.builder]
+    bvh = mcpt.Bvh(ctx, ds.view, layout=layout, builder=builder)
     W, H = scene.width, scene.height
     acc = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
     K, Wm, S = args.steps, args.warmup, args.spp_per_step
@@ -385,7 +388,7 @@ def run_ours(args):
         "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": dict(WORKLOAD, spp=K * S * world, spp_per_step=S, bvh_layout=args.layout,
+        "config": dict(WORKLOAD, spp=K * S * world, spp_per_step=S, bvh_layout=args.layout, bvh_builder=args.builder,
                        autotuned={"persistent": int(tuned.persistent), "refill_threshold": int(tuned.refill_threshold)},
                        parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
                        samples_per_wave=args.samples_per_wave or "automatic",

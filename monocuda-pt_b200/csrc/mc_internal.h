@@ -112,6 +112,7 @@ struct mc_bvh {
     std::vector<int> wide_roots;       // 4-wide root node of each scene
     std::vector<mc_aabb> seg_bounds;   // root box of each scene
     int layout = MC_BVH_LAYOUT_BINARY;
+    int builder = MC_BVH_BUILDER_LBVH;  // the binary tree the wide layout collapses
     int depth = -1;
     void* nodes = nullptr;             // traversal nodes (float4 records)
     long long node_count = 0;

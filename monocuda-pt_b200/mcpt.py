@@ -21,6 +21,7 @@ RNG_PHILOX, RNG_XORWOW = 0, 1
 ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
 TRACE_PLAIN = 0x100
 LAYOUT_BINARY, LAYOUT_WIDE4, LAYOUT_WIDE4Q = 0, 1, 2
+BUILDER_CLUSTERED, BUILDER_LBVH = 0, 1
 TONEMAP_NONE, TONEMAP_REINHARD, TONEMAP_ACES = 0, 1, 2
 IMAGE_RGB8, IMAGE_RGB_F32, IMAGE_PFM, IMAGE_PNG = 0, 1, 2, 3
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
@@ -115,7 +116,8 @@ class SceneView(C.Structure):
 
 
 class BvhBuildOpts(C.Structure):
-    _fields_ = [("permutation", C.c_void_p), ("layout", C.c_int32), ("keep_reference_nodes", C.c_int32)]
+    _fields_ = [("permutation", C.c_void_p), ("layout", C.c_int32), ("keep_reference_nodes", C.c_int32),
+                ("builder", C.c_int32), ("pad0", C.c_int32)]
 
 
 class BvhInfo(C.Structure):
@@ -333,10 +335,11 @@ class Context:
 
 
 class Bvh:
-    def __init__(self, ctx, view, permutation=None, layout=LAYOUT_BINARY, keep_reference_nodes=False):
+    def __init__(self, ctx, view, permutation=None, layout=LAYOUT_BINARY, keep_reference_nodes=False,
+                 builder=BUILDER_CLUSTERED):
         self.ctx = ctx
         self.lib = ctx.lib
-        opts = BvhBuildOpts(ptr(permutation), layout, 1 if keep_reference_nodes else 0)
+        opts = BvhBuildOpts(ptr(permutation), layout, 1 if keep_reference_nodes else 0, builder, 0)
         h = P()
         check(self.lib.mc_bvh_build(ctx.handle, C.byref(view), C.byref(opts), C.byref(h)))
         self.handle = h
@@ -364,11 +367,11 @@ class Bvh:
 class BatchBvh:
     """One build over several device scenes (mc_bvh_build_batch)."""
 
-    def __init__(self, ctx, views, layout=LAYOUT_WIDE4):
+    def __init__(self, ctx, views, layout=LAYOUT_WIDE4, builder=BUILDER_CLUSTERED):
         self.ctx = ctx
         self.lib = ctx.lib
         arr = (SceneView * len(views))(*views)
-        opts = BvhBuildOpts(None, layout, 0)
+        opts = BvhBuildOpts(None, layout, 0, builder, 0)
         h = P()
         check(self.lib.mc_bvh_build_batch(ctx.handle, C.addressof(arr), len(views), C.byref(opts), C.byref(h)))
         self.handle = h

@@ -1,0 +1,107 @@
+"""The wide layouts' binary tree (mc_bvh_build_opts.builder): the clustered
+tree (PLOC over the Morton-sorted leaves) and the reference's LBVH give the
+same closest hits to the bit (t and primitive), the same any-hit answers and
+the same images, because leaves keep the reference's rank for ties; the
+clustered tree needs fewer node visits."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import mcpt
+from helpers import random_rays
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = mcpt.Context(0)
+    yield c
+    c.close()
+
+
+CASES = [(mcpt.SCENE_CORNELL_BOXES, 0), (mcpt.SCENE_DISPLACED_ICOSPHERES, 5), (mcpt.SCENE_CORNELL_SPHERES, 0)]
+
+
+def _scene(kind, variant):
+    s = mcpt.generate_scene(kind, variant=variant, seed=2)
+    ds = mcpt.DeviceScene(mcpt.host_triangles(s), spheres=mcpt.host_spheres(s))
+    return s, ds
+
+
+@pytest.mark.parametrize("layout", [mcpt.LAYOUT_WIDE4, mcpt.LAYOUT_WIDE4Q])
+@pytest.mark.parametrize("kind,variant", CASES)
+def test_clustered_tree_gives_the_same_hits(ctx, kind, variant, layout):
+    s, ds = _scene(kind, variant)
+    v = np.frombuffer(mcpt.host_triangles(s), np.uint8).reshape(-1, 224)[:, :36].copy().view(np.float32).reshape(-1, 3)
+    rays = random_rays(200000, v.min(0), v.max(0), seed=variant + 11)
+    out = {}
+    for b in (mcpt.BUILDER_LBVH, mcpt.BUILDER_CLUSTERED):
+        bvh = mcpt.Bvh(ctx, ds.view, layout=layout, builder=b)
+        d_rays = torch.from_numpy(np.ascontiguousarray(rays)).cuda()
+        hits = torch.zeros(rays.shape[1] * 4, dtype=torch.int32, device="cuda")
+        mcpt.check(ctx.lib.mc_trace_closest(ctx.handle, bvh.handle, C.byref(ds.view), d_rays.data_ptr(), rays.shape[1], 0,
+                                            hits.data_ptr()))
+        occ = torch.zeros(rays.shape[1], dtype=torch.int32, device="cuda")
+        tmax = torch.full((rays.shape[1],), 2.0, dtype=torch.float32, device="cuda")
+        mcpt.check(ctx.lib.mc_trace_any(ctx.handle, bvh.handle, C.byref(ds.view), d_rays.data_ptr(), tmax.data_ptr(),
+                                        rays.shape[1], 0, occ.data_ptr()))
+        out[b] = (hits.cpu().numpy(), occ.cpu().numpy())
+        bvh.close()
+    assert np.array_equal(out[mcpt.BUILDER_LBVH][0], out[mcpt.BUILDER_CLUSTERED][0])
+    assert np.array_equal(out[mcpt.BUILDER_LBVH][1], out[mcpt.BUILDER_CLUSTERED][1])
+    mcpt.free_scene(s)
+
+
+def test_clustered_tree_same_image_fewer_visits(ctx):
+    s, ds = _scene(mcpt.SCENE_DISPLACED_ICOSPHERES, 6)
+    W, H = 320, 180
+    cam = mcpt.Camera.from_buffer_copy(bytes(s.camera))
+    cam.image_width = W
+    cam.aspect_ratio = W / H
+    mcpt.camera_initialize(cam)
+    res = {}
+    for b in (mcpt.BUILDER_LBVH, mcpt.BUILDER_CLUSTERED):
+        bvh = mcpt.Bvh(ctx, ds.view, layout=mcpt.LAYOUT_WIDE4, builder=b)
+        acc = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+        p = mcpt.render_params(cam, W, H, 4, 8, instrument=1)
+        st = mcpt.RenderStats()
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
+                                               C.byref(st)))
+        res[b] = (acc.cpu().numpy(), st.node_visits, st.extend_rays + st.shadow_rays)
+        bvh.close()
+    assert res[mcpt.BUILDER_LBVH][0].tobytes() == res[mcpt.BUILDER_CLUSTERED][0].tobytes()
+    assert res[mcpt.BUILDER_LBVH][2] == res[mcpt.BUILDER_CLUSTERED][2]
+    assert res[mcpt.BUILDER_CLUSTERED][1] < 0.8 * res[mcpt.BUILDER_LBVH][1], (res[1][1], res[0][1])
+    mcpt.free_scene(s)
+
+
+def test_batch_build_uses_clustered_trees_per_scene(ctx):
+    scenes = [_scene(mcpt.SCENE_BATCH_MEMBER, v) for v in (1, 2, 3)]
+    views = [d.view for _, d in scenes]
+    hits = {}
+    for b in (mcpt.BUILDER_LBVH, mcpt.BUILDER_CLUSTERED):
+        bb = mcpt.BatchBvh(ctx, views, layout=mcpt.LAYOUT_WIDE4, builder=b)
+        items = []
+        accs = []
+        for s, d in scenes:
+            cam = mcpt.Camera.from_buffer_copy(bytes(s.camera))
+            cam.image_width = 64
+            cam.aspect_ratio = 1.0
+            mcpt.camera_initialize(cam)
+            acc = torch.zeros(64 * 64 * 3, dtype=torch.float32, device="cuda")
+            accs.append(acc)
+            it = mcpt.BatchItem()
+            it.scene = d.view
+            it.params = mcpt.render_params(cam, 64, 64, 3, 8)
+            it.d_accum = acc.data_ptr()
+            items.append(it)
+        bb.render(items)
+        torch.cuda.synchronize()
+        hits[b] = [a.cpu().numpy().tobytes() for a in accs]
+        bb.close()
+    assert hits[mcpt.BUILDER_LBVH] == hits[mcpt.BUILDER_CLUSTERED]
+    for s, _ in scenes:
+        mcpt.free_scene(s)
