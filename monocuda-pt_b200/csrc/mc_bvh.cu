@@ -1141,9 +1141,12 @@ __device__ __forceinline__ float merged_area(float4 alo, float4 ahi, float4 blo,
 
 // nn[i] = the position j != i, |i - j| <= kPlocRadius, same scene, of least
 // merged area (ties: the lower j); -1 when no cluster of its scene is near.
-__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float4* __restrict__ cbox, int n, int* __restrict__ nn) {
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float4* __restrict__ cbox, const int* __restrict__ nPtr,
+                                                         int* __restrict__ nn) {
     __shared__ float4 sLo[kPlocBlock + 2 * kPlocRadius], sHi[kPlocBlock + 2 * kPlocRadius];
+    const int n = *nPtr;
     const int b0 = blockIdx.x * kPlocBlock;
+    if (b0 >= n) return;
     for (int t = threadIdx.x; t < kPlocBlock + 2 * kPlocRadius; t += blockDim.x) {
         const int g = b0 - kPlocRadius + t;
         if (g >= 0 && g < n) {
@@ -1178,7 +1181,8 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float4* __restrict
 
 // (merge, alive) per cluster: a mutual pair merges at its lower position and
 // the higher one disappears; every other cluster stays.
-__global__ void k_ploc_flags(const int* __restrict__ nn, int n, int2* __restrict__ flags) {
+__global__ void k_ploc_flags(const int* __restrict__ nn, const int* __restrict__ nPtr, int2* __restrict__ flags) {
+    const int n = *nPtr;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int j = nn[i];
         const bool mutual = j >= 0 && nn[j] == i;
@@ -1188,9 +1192,10 @@ __global__ void k_ploc_flags(const int* __restrict__ nn, int n, int2* __restrict
 
 // Exclusive scan of int2 values: per block of kPlocBlock * kScanItems items,
 // then the block sums (one block), then the offsets.
-__global__ void __launch_bounds__(kPlocBlock) k_scan2_blocks(const int2* __restrict__ in, int n, int2* __restrict__ out,
-                                                              int2* __restrict__ sums) {
+__global__ void __launch_bounds__(kPlocBlock) k_scan2_blocks(const int2* __restrict__ in, const int* __restrict__ nPtr,
+                                                              int2* __restrict__ out, int2* __restrict__ sums) {
     __shared__ int2 warpSum[kPlocBlock / 32];
+    const int n = *nPtr;
     const long long base = ((long long)blockIdx.x * kPlocBlock + threadIdx.x) * kScanItems;
     int2 v[kScanItems];
     int2 acc = make_int2(0, 0);
@@ -1260,9 +1265,9 @@ __global__ void __launch_bounds__(1024) k_scan2_sums(int2* __restrict__ sums, in
     if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void k_scan2_add(int2* __restrict__ out, int n, const int2* __restrict__ sums) {
+__global__ void k_scan2_add(int2* __restrict__ out, const int* __restrict__ nPtr, const int2* __restrict__ sums) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
+    if (g >= *nPtr) return;
     const int2 off = sums[g / (kPlocBlock * kScanItems)];
     const int2 v = out[g];
     out[g] = make_int2(v.x + off.x, v.y + off.y);
@@ -1271,9 +1276,10 @@ __global__ void k_scan2_add(int2* __restrict__ out, int n, const int2* __restric
 // Writes the round's new internal nodes (binary layout: left box, right box,
 // references) and the compacted clusters.
 __global__ void k_ploc_emit(const int* __restrict__ cref, const float4* __restrict__ cbox, const int* __restrict__ nn,
-                            const int2* __restrict__ flags, const int2* __restrict__ pos, int n, int nodeBase, int nodeCap,
-                            float4* __restrict__ nodes, int* __restrict__ crefOut, float4* __restrict__ cboxOut,
+                            const int2* __restrict__ flags, const int2* __restrict__ pos, const int* __restrict__ state,
+                            int nodeCap, float4* __restrict__ nodes, int* __restrict__ crefOut, float4* __restrict__ cboxOut,
                             int* __restrict__ err) {
+    const int n = state[0], nodeBase = state[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int2 f = flags[i];
         if (!f.y) continue;
@@ -1303,6 +1309,19 @@ __global__ void k_ploc_emit(const int* __restrict__ cref, const float4* __restri
     }
 }
 
+// End of a round: the cluster count and the next node id move on; a round
+// without a merge while a scene still has two clusters is an error (it
+// cannot happen: the closest pair is mutual).
+__global__ void k_ploc_advance(const int2* __restrict__ total, int* __restrict__ state, int nseg, int* __restrict__ err) {
+    const int2 t = *total;
+    if (t.x == 0) {
+        if (state[0] > nseg) atomicOr(err, MC_DEVERR_INPUT);
+        return;
+    }
+    state[1] += t.x;
+    state[0] = t.y;
+}
+
 // Builds the clustered tree into tree->nodes (NI internal nodes) and its
 // scene roots; MC_ERR_UNSUPPORTED when a scene has fewer than two primitives
 // (the caller keeps the LBVH then).
@@ -1318,7 +1337,7 @@ static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg,
     const int per = kPlocBlock * kScanItems;
     const long long nbMax = (N + per - 1) / per;
     const size_t bytes = (size_t)NI * 64 + 2 * (size_t)N * 4 + 4 * (size_t)N * 16 + (size_t)N * 4 + 2 * (size_t)N * 8 +
-                         (size_t)(nbMax + 1) * 8 + 16 + 16 * 16;  // + the 16-byte rounding of each part
+                         (size_t)(nbMax + 1) * 8 + 32 + 16 * 16;  // + the 16-byte rounding of each part
     char* mem = nullptr;
     if (cudaMalloc(&mem, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -1333,33 +1352,45 @@ static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg,
     int2* flags = (int2*)take((size_t)N * 8);
     int2* pos = (int2*)take((size_t)N * 8);
     int2* sums = (int2*)take((size_t)(nbMax + 1) * 8);
-    int2* total = (int2*)take(16);
+    int2* total = (int2*)take(32);  // the round's totals, then [2..3] as ints: clusters, next node id
     auto fail = [&](mc_status s) {
         cudaFree(mem);
         tree.nodes = nullptr;
         return s;
     };
     const int loop = ctx->sm_count * 8;
+    int* state = (int*)(total + 2);  // [0] clusters, [1] next node id
     k_ploc_init<<<std::min(grid_for(N, kBlock), loop), kBlock, 0, ctx->stream>>>(order, bounds, dSeg, nseg, N, cref[0], cbox[0]);
+    const int h0[2] = {N, 0};
+    if (cudaMemcpyAsync(state, h0, sizeof(h0), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        return fail(cuda_error(cudaGetLastError(), "mc_bvh_build (clustering)", __FILE__, __LINE__));
+    // rounds run in batches between host checks; every launch reads the
+    // cluster count from the device and is sized for the last count seen
     int n = N, nodeBase = 0, cur = 0, rounds = 0;
+    const int kBatch = 8;
     while (n > nseg) {
-        if (++rounds > 4096) return fail(set_error(MC_ERR_INVALID, "mc_bvh_build: clustering did not converge"));
-        k_ploc_nn<<<(n + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, ctx->stream>>>(cbox[cur], n, nn);
-        k_ploc_flags<<<std::min(grid_for(n, kBlock), loop), kBlock, 0, ctx->stream>>>(nn, n, flags);
+        if (rounds > 4096) return fail(set_error(MC_ERR_INVALID, "mc_bvh_build: clustering did not converge"));
         const int nb = (n + per - 1) / per;
-        k_scan2_blocks<<<nb, kPlocBlock, 0, ctx->stream>>>(flags, n, pos, sums);
-        k_scan2_sums<<<1, 1024, 0, ctx->stream>>>(sums, nb, total);
-        k_scan2_add<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(pos, n, sums);
-        int2 h;
-        if (cudaMemcpyAsync(&h, total, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        for (int r = 0; r < kBatch; r++, rounds++) {
+            k_ploc_nn<<<(n + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, ctx->stream>>>(cbox[cur], state, nn);
+            k_ploc_flags<<<std::min(grid_for(n, kBlock), loop), kBlock, 0, ctx->stream>>>(nn, state, flags);
+            k_scan2_blocks<<<nb, kPlocBlock, 0, ctx->stream>>>(flags, state, pos, sums);
+            k_scan2_sums<<<1, 1024, 0, ctx->stream>>>(sums, nb, total);
+            k_scan2_add<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(pos, state, sums);
+            k_ploc_emit<<<std::min(grid_for(n, kBlock), loop), kBlock, 0, ctx->stream>>>(
+                cref[cur], cbox[cur], nn, flags, pos, state, NI, tree.nodes, cref[1 - cur], cbox[1 - cur], ctx->d_error);
+            k_ploc_advance<<<1, 1, 0, ctx->stream>>>(total, state, nseg, ctx->d_error);
+            cur = 1 - cur;
+        }
+        int h[2];
+        if (cudaMemcpyAsync(h, state, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
             cudaStreamSynchronize(ctx->stream) != cudaSuccess)
             return fail(cuda_error(cudaGetLastError(), "mc_bvh_build (clustering)", __FILE__, __LINE__));
-        if (h.x <= 0 || nodeBase + h.x > NI) return fail(set_error(MC_ERR_INVALID, "mc_bvh_build: clustering made no progress"));
-        k_ploc_emit<<<std::min(grid_for(n, kBlock), loop), kBlock, 0, ctx->stream>>>(
-            cref[cur], cbox[cur], nn, flags, pos, n, nodeBase, NI, tree.nodes, cref[1 - cur], cbox[1 - cur], ctx->d_error);
-        nodeBase += h.x;
-        n = h.y;
-        cur = 1 - cur;
+        int fl = 0;
+        mc_status fs = flags_now(ctx, &fl);
+        if (fs != MC_OK || fl) return fail(fs != MC_OK ? fs : status_from_device_flags(fl));
+        n = h[0];
+        nodeBase = h[1];
     }
     tree.roots.assign((size_t)nseg, -1);
     if (cudaMemcpyAsync(tree.roots.data(), cref[cur], (size_t)nseg * 4, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
