@@ -1116,7 +1116,7 @@ static mc_status upload_segments(mc_context* ctx, const mc_scene_view* views, in
 // ranks: leaves keep their reference-rank slots, so the tie rule, and with
 // it every hit, is the same with either tree.
 // ---------------------------------------------------------------------------
-constexpr int kPlocRadius = 16;
+constexpr int kPlocRadius = 8;  // 8, 16, 32 measured within 1 % of each other; 8 builds fastest
 constexpr int kPlocBlock = 256;
 constexpr int kScanItems = 4;  // items per thread of the block scans
 
