@@ -105,3 +105,64 @@ def test_batch_build_uses_clustered_trees_per_scene(ctx):
     assert hits[mcpt.BUILDER_LBVH] == hits[mcpt.BUILDER_CLUSTERED]
     for s, _ in scenes:
         mcpt.free_scene(s)
+
+
+def _tiny_scene(n_tris, seed):
+    """n_tris random triangles with the default material, as a DeviceScene."""
+    rng = np.random.default_rng(seed)
+    arr = (mcpt.Triangle * n_tris)()
+    for i in range(n_tris):
+        c = rng.uniform(-1, 1, 3)
+        for k, name in enumerate(("v0", "v1", "v2")):
+            p = c + rng.uniform(-0.3, 0.3, 3)
+            setattr(arr[i], name, mcpt.Vec3(*p.astype(np.float32)))
+    return arr, mcpt.DeviceScene(arr)
+
+
+@pytest.mark.parametrize("n_tris", [1, 2, 3, 17])
+def test_tiny_scenes_build_and_agree(ctx, n_tris):
+    """One primitive has no tree to cluster (the build keeps the LBVH's
+    collapse); two or more cluster. Either way the hits equal the LBVH's."""
+    tris, ds = _tiny_scene(n_tris, seed=n_tris)
+    rays = random_rays(5000, np.full(3, -1.5), np.full(3, 1.5), seed=3)
+    out = []
+    for b in (mcpt.BUILDER_LBVH, mcpt.BUILDER_CLUSTERED):
+        bvh = mcpt.Bvh(ctx, ds.view, layout=mcpt.LAYOUT_WIDE4, builder=b)
+        d_rays = torch.from_numpy(rays).cuda()
+        hits = torch.zeros(rays.shape[1] * 4, dtype=torch.int32, device="cuda")
+        mcpt.check(ctx.lib.mc_trace_closest(ctx.handle, bvh.handle, C.byref(ds.view), d_rays.data_ptr(), rays.shape[1], 0,
+                                            hits.data_ptr()))
+        out.append(hits.cpu().numpy())
+        bvh.close()
+    assert np.array_equal(out[0], out[1])
+    assert (out[0].reshape(-1, 4)[:, 3] == 1).any()
+
+
+def test_batch_with_a_one_primitive_scene(ctx):
+    """A batch holding a one-primitive scene falls back to the LBVH's collapse
+    for the whole batch; the images still equal the LBVH build's."""
+    small = _tiny_scene(1, seed=5)
+    big = _scene(mcpt.SCENE_BATCH_MEMBER, 4)
+    views = [small[1].view, big[1].view]
+    imgs = {}
+    for b in (mcpt.BUILDER_LBVH, mcpt.BUILDER_CLUSTERED):
+        bb = mcpt.BatchBvh(ctx, views, layout=mcpt.LAYOUT_WIDE4, builder=b)
+        cam = mcpt.Camera.from_buffer_copy(bytes(big[0].camera))
+        cam.image_width = 48
+        cam.aspect_ratio = 1.0
+        mcpt.camera_initialize(cam)
+        accs, items = [], []
+        for v in views:
+            acc = torch.zeros(48 * 48 * 3, dtype=torch.float32, device="cuda")
+            it = mcpt.BatchItem()
+            it.scene = v
+            it.params = mcpt.render_params(cam, 48, 48, 2, 8)
+            it.d_accum = acc.data_ptr()
+            accs.append(acc)
+            items.append(it)
+        bb.render(items)
+        torch.cuda.synchronize()
+        imgs[b] = [a.cpu().numpy().tobytes() for a in accs]
+        bb.close()
+    assert imgs[mcpt.BUILDER_LBVH] == imgs[mcpt.BUILDER_CLUSTERED]
+    mcpt.free_scene(big[0])
