@@ -787,6 +787,19 @@ mc_status guide_reserve_batch(mc_guide* g, int records) {
     return MC_OK;
 }
 
+mc_status guide_reserve_tiles(mc_guide* g, int tiles) {
+    if (g->rec_tile_capacity >= tiles) return MC_OK;
+    int* nt = nullptr;
+    if (cudaMalloc(&nt, (size_t)std::max(tiles, 1) * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MC_ERR_OOM, "guide: allocation of the record tile counts failed");
+    }
+    cudaFree(g->rec_tiles);
+    g->rec_tiles = nt;
+    g->rec_tile_capacity = tiles;
+    return MC_OK;
+}
+
 mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps,
                              int stepRecords) {
     const int B = stepRecords > 0 ? std::min(stepRecords, g->cfg.batch_capacity) : g->cfg.batch_capacity;
@@ -865,6 +878,7 @@ mc_status mc_guide_destroy(mc_guide* g) {
     cudaFree(g->loss);
     cudaFree(g->batch);
     cudaFree(g->batch_count);
+    cudaFree(g->rec_tiles);
     cudaFree(g->records);
     cudaFree(g->mixtures);
     cudaFree(g->nee0);

@@ -144,6 +144,8 @@ struct mc_guide {
     float* batch = nullptr;            // training records of guided renders
     int batch_records = 0;             // records the batch buffer holds
     int* batch_count = nullptr;
+    int* rec_tiles = nullptr;          // per-tile record counts, then first batch slots, of a wave
+    int rec_tile_capacity = 0;
     float* records = nullptr;          // per-path primary-vertex records of guided renders
     int record_capacity = 0;
     float* mixtures = nullptr;         // per-path mixtures of the current bounce
@@ -196,5 +198,6 @@ mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, 
                              int stepRecords);
 // Grows the training batch buffer to hold `records` records.
 mc_status guide_reserve_batch(mc_guide* g, int records);
+mc_status guide_reserve_tiles(mc_guide* g, int tiles);
 mc_status guide_reserve_paths(mc_guide* g, int paths);
 }

@@ -813,14 +813,47 @@ __global__ void k_finalize(const WaveTable* tab, const float* sr, const float* s
     }
 }
 
-// Guided renders (one scene, one or more images): the sample plus the primary vertex's NEE goes
-// to the image; a primary-vertex record takes the sample without that NEE
-// (the radiance carried back through its sampled direction over that
-// direction's density) as its weight, and records of positive weight are
-// appended to the training batch.
-__global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sceneOf, const float* sr, const float* sg,
-                                  const float* sb, const float* nr, const float* ng, const float* nb, const float* rec,
-                                  float* batch, int* batchCount, int capacity, int recStride, int recPhase) {
+// A guided wave's training batch holds its records in (sample, pixel) order:
+// sample j of every pixel before sample j + 1 of any, so that an Adam step on
+// a pixel count of records sees about one sample of the whole image, as with
+// one sample per wave, and the batch (and so the trained guide) is the same
+// on every run. Entry v of that order is sample v / totalPixels of wave pixel
+// v % totalPixels. When the wave has more paths than the batch holds, only
+// entries with (pixel + sample + recPhase) % recStride == 0 are kept, the host
+// rotating recPhase between waves, so that records come from the whole image.
+// A kept entry is a record when its path has a primary-vertex record of
+// positive, finite weight: the sample without the primary vertex's NEE (the
+// radiance carried back through the sampled direction over that direction's
+// density).
+constexpr int kRecThreads = 256;
+constexpr int kRecTileChunks = 8;
+constexpr int kRecTile = kRecThreads * kRecTileChunks;  // entries per tile
+
+MC_D bool rec_entry(const WaveTable* tab, long long v, int recStride, int recPhase, const float* sr, const float* sg,
+                    const float* sb, const float* rec, int* path, float* weight) {
+    const int pixels = tab->totalPixels;
+    const int j = (int)(v / pixels);
+    const int u = (int)(v - (long long)j * pixels);
+    if ((u + j + recPhase) % recStride != 0) return false;
+    const SceneGPU& S = tab->scenes[tab->nScenes > 1 ? find_scene_by_pixel(tab, u) : 0];
+    if (j >= S.pathStride) return false;
+    const int p = S.pathOffset + (u - S.pixelOffset) * S.pathStride + j;
+    const float* r = rec + (size_t)p * kRecFloats;
+    if (r[10] == 0.0f) return false;
+    const float w = (sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) + r[11];
+    *path = p;
+    *weight = w;
+    return w > 0.0f && w < 1e30f;
+}
+
+// Guided renders (one scene, one or more images): the sample plus the primary
+// vertex's NEE goes to the image, and each tile of the wave's training entries
+// (`entries` of them, none when not training) counts its records.
+__global__ void __launch_bounds__(kRecThreads) k_finalize_guided(const WaveTable* tab, const unsigned short* sceneOf,
+                                                                 const float* sr, const float* sg, const float* sb,
+                                                                 const float* nr, const float* ng, const float* nb,
+                                                                 const float* rec, int* tileCounts, long long entries,
+                                                                 int recStride, int recPhase) {
     // the image: each pixel adds its samples of the wave in sample order
     const int pixels = tab->totalPixels;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < pixels; u += gridDim.x * blockDim.x) {
@@ -842,32 +875,91 @@ __global__ void k_finalize_guided(const WaveTable* tab, const unsigned short* sc
         acc[2] = a2;
     }
     if (!rec) return;
-    // the training records, one per path with a primary-vertex record; when
-    // the wave has more paths than the batch holds, every recStride-th path
-    // (from recPhase, which the host rotates) so that records come from the
-    // whole image rather than its first rows
-    const unsigned ltmask = lanemask_lt();
-    const int total = tab->totalPaths;
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
-        const int p = base + threadIdx.x;
-        bool emit = false;
-        float w = 0.f;
-        if (p < total && (p + recPhase) % recStride == 0 && rec[(size_t)p * kRecFloats + 10] != 0.0f) {
-            w = (sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) + rec[(size_t)p * kRecFloats + 11];
-            emit = w > 0.0f && w < 1e30f;
+    // the training records: each tile's count (k_rec_scan and k_rec_write place them)
+    const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        int c = 0;
+        for (int i = 0; i < kRecTileChunks; i++) {
+            const long long v = (long long)t * kRecTile + i * kRecThreads + threadIdx.x;
+            int p;
+            float w;
+            c += __syncthreads_count(v < entries && rec_entry(tab, v, recStride, recPhase, sr, sg, sb, rec, &p, &w));
         }
-        unsigned m = __ballot_sync(kFull, emit);
-        if (m) {
-            int leader = __ffs(m) - 1, slot = 0;
-            if ((int)(threadIdx.x & 31) == leader) slot = atomicAdd(batchCount, __popc(m));
-            slot = __shfl_sync(kFull, slot, leader) + __popc(m & ltmask);
-            if (emit && slot < capacity) {
+        if (threadIdx.x == 0) tileCounts[t] = c;
+    }
+}
+
+// Exclusive scan of the wave's tile counts by one block of 1024 threads: each
+// tile's first batch slot, and the wave's record count in *batchCount.
+__global__ void __launch_bounds__(1024) k_rec_scan(int* tileCounts, int tiles, int* batchCount) {
+    __shared__ int warpSums[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < tiles; base += 1024) {
+        const int t = base + threadIdx.x;
+        const int c = t < tiles ? tileCounts[t] : 0;
+        int x = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSums[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int s = warpSums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, s, o);
+                if (lane >= o) s += y;
+            }
+            warpSums[lane] = s;
+        }
+        __syncthreads();
+        const int before = carry + (wid > 0 ? warpSums[wid - 1] : 0) + x - c;
+        if (t < tiles) tileCounts[t] = before;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = before + c;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *batchCount = carry;
+}
+
+// Writes each kept record to its slot in (sample, pixel) order: the tile's
+// first slot (k_rec_scan) plus the kept entries before it in the tile.
+__global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab, const float* sr, const float* sg,
+                                                           const float* sb, const float* rec, const int* tileFirst,
+                                                           long long entries, int recStride, int recPhase, float* batch,
+                                                           int capacity) {
+    __shared__ int warpCount[kRecThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned ltmask = lanemask_lt();
+    const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        int next = tileFirst[t];
+        for (int i = 0; i < kRecTileChunks; i++) {
+            const long long v = (long long)t * kRecTile + i * kRecThreads + threadIdx.x;
+            int p = 0;
+            float w = 0.f;
+            const bool e = v < entries && rec_entry(tab, v, recStride, recPhase, sr, sg, sb, rec, &p, &w);
+            const unsigned m = __ballot_sync(kFull, e);
+            if (lane == 0) warpCount[wid] = __popc(m);
+            __syncthreads();
+            int before = next, all = 0;
+            for (int k = 0; k < kRecThreads / 32; k++) {
+                const int c = warpCount[k];
+                if (k < wid) before += c;
+                all += c;
+            }
+            const int slot = before + __popc(m & ltmask);
+            if (e && slot < capacity) {
                 const float* r = rec + (size_t)p * kRecFloats;
                 float* b = batch + (size_t)slot * MC_GUIDE_RECORD_FLOATS;
-                for (int i = 0; i < 9; i++) b[i] = r[i];
+                for (int k = 0; k < 9; k++) b[k] = r[k];
                 b[9] = w;
             }
+            next += all;
+            __syncthreads();
         }
     }
 }
@@ -1163,6 +1255,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         int maxR = 1;
         for (int i = 0; i < n; i++) maxR = std::max(maxR, item_spw(i));
         if ((st = guide_reserve_batch(guide, guide->cfg.batch_capacity * guide->cfg.train_steps * maxR)) != MC_OK) return st;
+        long long pixelsAll = 0;
+        for (int i = 0; i < n; i++) pixelsAll += (long long)items[i].p->width * items[i].p->height;
+        if ((st = guide_reserve_tiles(guide, (int)((pixelsAll * maxR + kRecTile - 1) / kRecTile))) != MC_OK) return st;
     }
     // the launch sequence of one wave (device table already holds the wave)
     float* nee0[3] = {nullptr, nullptr, nullptr};
@@ -1229,11 +1324,19 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             launches++;
         }
         if (guide) {
-            k_finalize_guided<<<loopBlocks, 256, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2],
-                                                              train ? guide->records : nullptr, guide->batch,
-                                                              guide->batch_count,
-                                                              guide->cfg.batch_capacity * guide->cfg.train_steps * waveR,
-                                                              recStride, recPhase);
+            const long long entries = train ? (long long)waveR * wavePixels : 0;
+            k_finalize_guided<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1],
+                                                                      nee0[2], train ? guide->records : nullptr,
+                                                                      guide->rec_tiles, entries, recStride, recPhase);
+            if (train) {
+                const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
+                k_rec_scan<<<1, 1024, 0, stream>>>(guide->rec_tiles, tiles, guide->batch_count);
+                k_rec_write<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, w.sr, w.sg, w.sb, guide->records, guide->rec_tiles,
+                                                                    entries, recStride, recPhase, guide->batch,
+                                                                    guide->cfg.batch_capacity * guide->cfg.train_steps *
+                                                                        waveR);
+                launches += 2;
+            }
         } else {
             k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         }

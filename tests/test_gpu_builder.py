@@ -138,10 +138,11 @@ def test_tiny_scenes_build_and_agree(ctx, n_tris):
     assert (out[0].reshape(-1, 4)[:, 3] == 1).any()
 
 
-def test_batch_with_a_one_primitive_scene(ctx):
-    """A batch holding a one-primitive scene falls back to the LBVH's collapse
-    for the whole batch; the images still equal the LBVH build's."""
-    small = _tiny_scene(1, seed=5)
+def test_batch_with_the_smallest_scenes(ctx):
+    """A batch whose smallest scene has two primitives clusters it like the
+    others and gives the images of the LBVH build. A one-primitive scene in a
+    batch is rejected with MC_ERR_INVALID by either builder."""
+    small = _tiny_scene(2, seed=5)
     big = _scene(mcpt.SCENE_BATCH_MEMBER, 4)
     views = [small[1].view, big[1].view]
     imgs = {}
@@ -165,4 +166,9 @@ def test_batch_with_a_one_primitive_scene(ctx):
         imgs[b] = [a.cpu().numpy().tobytes() for a in accs]
         bb.close()
     assert imgs[mcpt.BUILDER_LBVH] == imgs[mcpt.BUILDER_CLUSTERED]
+    one = _tiny_scene(1, seed=6)
+    for b in (mcpt.BUILDER_LBVH, mcpt.BUILDER_CLUSTERED):
+        with pytest.raises(mcpt.McError) as e:
+            mcpt.BatchBvh(ctx, [one[1].view, big[1].view], layout=mcpt.LAYOUT_WIDE4, builder=b)
+        assert e.value.status == 1  # MC_ERR_INVALID
     mcpt.free_scene(big[0])

@@ -81,14 +81,15 @@ def test_guided_estimator_is_unbiased(ctx):
     mcpt.free_scene(s)
 
 
-@pytest.mark.parametrize("samples_per_wave,bar", [(1, 0.85), (0, 0.95)])
+@pytest.mark.parametrize("samples_per_wave,bar", [(1, 0.85), (0, 0.88)])
 def test_trained_guide_lowers_error_in_the_aperture_room(ctx, samples_per_wave, bar):
     """Online training on the renderer's own primary-vertex samples, then
     guided vs plain MSE at equal spp. One sample per wave trains after every
-    sample (measured ratios 0.75-0.80); the default several samples per wave
-    train once per wave on records of the same weights (0.80-0.87). The order
-    in which records enter a batch varies from run to run; the bars leave
-    room for that."""
+    sample; the default several samples per wave train once per wave, one
+    Adam step per sample of the wave, on records of the same weights. Training
+    is reproducible, so each case gives one ratio; over guide seeds 1-5 and 9
+    they measured 0.77-0.82 (one sample per wave) and 0.79-0.86 (default),
+    0.81 for seed 9 in both."""
     W = 96
     s, tris, d, bvh, cam = _setup(ctx, mcpt.SCENE_GUIDING_ROOM, W)
     lo, hi = _bounds(tris)
@@ -103,4 +104,27 @@ def test_trained_guide_lowers_error_in_the_aperture_room(ctx, samples_per_wave, 
     mse_g = float(((guided - ref) ** 2).mean())
     assert np.isfinite(mse_g) and mse_g < bar * mse_p, (mse_g, mse_p)
     guide.close()
+    mcpt.free_scene(s)
+
+
+@pytest.mark.parametrize("samples_per_wave", [1, 3, 0])
+def test_guided_training_is_reproducible(ctx, samples_per_wave):
+    """The training batch holds each wave's records in (sample, pixel) order,
+    whatever order the shading queues reached them in, so two trainings from
+    the same seed end with the same weights to the bit and render the same
+    image."""
+    W = 64
+    s, tris, d, bvh, cam = _setup(ctx, mcpt.SCENE_GUIDING_ROOM, W)
+    lo, hi = _bounds(tris)
+    runs = []
+    for _ in range(2):
+        guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=4, learning_rate=3e-3)
+        trained, _ = _guided(ctx, bvh, d, cam, W, 24, 1000, guide, 1, samples_per_wave=samples_per_wave)
+        assert guide.steps() == 24
+        after, _ = _guided(ctx, bvh, d, cam, W, 8, 9000, guide, 0)
+        runs.append((guide.get_params(), trained, after))
+        guide.close()
+    assert runs[0][0].tobytes() == runs[1][0].tobytes()
+    assert runs[0][1].tobytes() == runs[1][1].tobytes()
+    assert runs[0][2].tobytes() == runs[1][2].tobytes()
     mcpt.free_scene(s)
