@@ -578,11 +578,14 @@ def run_guiding(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), st
 
-    # warm-up of both paths (kernels loaded, wave buffers reserved for a chunk)
+    # warm-up of both paths (kernels loaded, wave buffers reserved for a chunk),
+    # the guided one with the timed guide's configuration
     tmp = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
     render(tmp, chunk, 999999)
-    warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1)
+    warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
+                            train_steps=args.guide_steps)
     render(tmp, chunk, 999998, warm_guide, 1)
+    render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
     # reference image
     ref = torch.zeros_like(tmp)
