@@ -231,10 +231,10 @@ def run_ours(args):
     # step indices; step s renders samples [s * S, (s + 1) * S)
     timed_samples, warm_samples = sharding.sample_ranges(rank, world, K, Wm)
 
-    # the library's autotuner picks the trace variant and refill threshold for
-    # this scene / image size class (untimed; the choice does not change the image)
-    tuned = mcpt.render_params(scene.camera, W, H, 1, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234,
-                               refill_threshold=args.refill)
+    # the library's autotuner picks the trace variant and refill threshold by
+    # timing the wave that each step traces (untimed; the choice does not change the image)
+    tuned = mcpt.render_params(scene.camera, W, H, S, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234,
+                               refill_threshold=args.refill, samples_per_wave=args.samples_per_wave)
     if args.refill <= 0:
         mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
 

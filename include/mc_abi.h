@@ -88,7 +88,7 @@ typedef struct mc_material {
     float refraction_index;
     float density;
     float phase_g;
-    const void* density_grid;   /* NanoVDB grid in the reference; must be NULL here */
+    const void* density_grid;   /* device mc_volume_grid (a NanoVDB FloatGrid in the reference) or NULL */
     float grid_max_density;
 } mc_material;
 
@@ -204,7 +204,7 @@ typedef struct mc_scene_view {
     int32_t triangle_count;
     const mc_light* lights;
     int32_t light_count;
-    int32_t has_medium;         /* PT:4328-4331 sceneHasMedium */
+    int32_t has_medium;         /* PT:4328-4331 sceneHasMedium: MC_MEDIUM_ANY, | MC_MEDIUM_GRID with density grids */
     mc_env_map env;
 } mc_scene_view;
 
@@ -335,8 +335,9 @@ MC_API mc_status mc_split_triangles_host(const mc_triangle* tris, int32_t n, mc_
  * arrays, 16-byte aligned; tris is not modified. lights: device array with
  * room for every emissive triangle (n is always enough), or NULL to only count.
  * spheres (device, n_sph records, may be NULL when n_sph is 0) are scanned for
- * media. light_count and has_medium (a material of type MC_MAT_ISOTROPIC on any
- * primitive) are host outputs and may be NULL; the call synchronizes the
+ * media. light_count and has_medium (MC_MEDIUM_ANY when a primitive has a
+ * material of type MC_MAT_ISOTROPIC, | MC_MEDIUM_GRID when one of those has a
+ * density grid) are host outputs and may be NULL; the call synchronizes the
  * context's stream to read them. */
 MC_API mc_status mc_scene_ingest(mc_context* ctx, const mc_triangle* tris, int32_t n, const mc_sphere* spheres,
                                  int32_t n_sph, mc_triangle_hot* hot, mc_triangle_cold* cold, mc_light* lights,
@@ -354,6 +355,58 @@ MC_API mc_status mc_scene_ingest_host(mc_context* ctx, const mc_triangle* tris, 
 MC_API mc_status mc_env_create(const float* rgba_host, int32_t width, int32_t height, float intensity,
                                float rotation_radians, mc_env_map* out);
 MC_API mc_status mc_env_destroy(mc_env_map* env);
+
+/* ------------------------------------------------------------------------- */
+/* Heterogeneous media (PT:784-838). An isotropic material whose density_grid  */
+/* is set scatters by delta tracking and attenuates shadow rays by ratio       */
+/* tracking, with extinction density x grid value and majorant density x      */
+/* grid_max_density; without a grid it stays homogeneous (PT:3559-3566).       */
+/* ------------------------------------------------------------------------- */
+/* The reference's grid is a NanoVDB FloatGrid (openvdb v12.0.1, nanovdb/
+ * subtree, not vendored), read through its world-to-index map and a
+ * trilinear sampler (PT:784-789). This grid is dense: FP32 voxels, x fastest,
+ * voxel (i,j,k) centred at origin + voxel_size * (i,j,k), value 0 outside.
+ * Index coordinates are (p - origin) * inv_voxel_size; the sample at index
+ * point x interpolates the 8 voxels around floor(x), z first, then y, then x,
+ * each step a + w * (b - a) as one fused multiply-add. The device copy is
+ * self-contained: this 64-byte header, then the voxels. */
+typedef struct mc_volume_grid {
+    MC_ALIGNAS(16) float origin[3];
+    float voxel_size;
+    float inv_voxel_size;
+    int32_t dims[3];
+    float maximum_density;      /* largest voxel value: the majorant (root().maximum() in NanoVDB) */
+    float world_min[3];         /* centre of voxel (0,0,0) */
+    float world_max[3];         /* centre of the last voxel */
+    int32_t pad0;
+} mc_volume_grid;
+
+enum {
+    MC_MEDIUM_ANY = 1,          /* mc_scene_view.has_medium bits: an isotropic material (PT:4328-4331) */
+    MC_MEDIUM_GRID = 2          /* ... of which at least one carries a density grid */
+};
+
+/* Copies nx*ny*nz host densities (x fastest; finite, >= 0) to a device grid.
+ * *d_grid receives the device pointer that mc_material.density_grid takes;
+ * *header (optional) the header, whose maximum_density goes into
+ * mc_material.grid_max_density. mc_volume_grid_destroy frees it. */
+MC_API mc_status mc_volume_grid_create(mc_context* ctx, const float* density_host, int32_t nx, int32_t ny, int32_t nz,
+                                       const float origin[3], float voxel_size, const mc_volume_grid** d_grid,
+                                       mc_volume_grid* header);
+MC_API mc_status mc_volume_grid_destroy(const mc_volume_grid* d_grid);
+/* The fog sphere of createFogSphereGrid (src/volume_io.cpp:53-64, nanovdb's
+ * createFogVolumeSphere) centred at the origin: a narrow band of half_width
+ * voxels (nanovdb's default 3) inside the surface ramps the density linearly
+ * from 0 at the surface to 1, the interior is 1, the outside 0. Voxel values
+ * are clamp((radius - |p|) / (half_width * voxel_size), 0, 1) at the voxel
+ * centres p, computed in double. The grid spans ceil(radius / voxel_size) + 1
+ * voxels on each side of the centre voxel. With density_host NULL only dims
+ * and origin are returned. */
+MC_API mc_status mc_volume_fog_sphere(float radius, float voxel_size, float half_width, float* density_host,
+                                      int32_t dims[3], float origin[3]);
+/* Grid values at n world points (device, xyz packed) as the media sample them. */
+MC_API mc_status mc_volume_density(mc_context* ctx, const mc_volume_grid* d_grid, const float* d_points, int32_t n,
+                                   float* d_out);
 
 /* ------------------------------------------------------------------------- */
 /* Synthetic scenes (seeded, deterministic). Host output.                      */
@@ -527,7 +580,11 @@ MC_API mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_
 /* Reset the per-pixel XORWOW states (PT:2865-2871 init_rng_kernel). */
 MC_API mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed);
 
-/* The params the autotuner picked for a scene size / image size class. */
+/* Sets params' trace variant (persistent), refill_threshold and use_graph to
+ * the fastest for the first wave that rendering params traces (its size,
+ * samples per wave and spp as given), timed on this scene and BVH. Cached per
+ * (device, layout, scene size class, wave size class); the image does not
+ * depend on the choice. budget_ms bounds the tuning time (0 = 2000). */
 MC_API mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
                              mc_render_params* params, int32_t budget_ms);
 

@@ -6,7 +6,7 @@ Per-file flags:
                 reference's host (IEEE, no contraction) computation bit for bit.
   mc_ingest.cu  the same IEEE flags: light areas and normals equal the
                 reference's host computation bit for bit.
-  mc_render.cu, mc_resolve.cu  -O3 --use_fast_math: the reference's release flags
+  mc_render.cu, mc_resolve.cu, mc_volume.cu  -O3 --use_fast_math: the reference's release flags
                 (CMakeLists.txt:88-96), which the per-ray arithmetic must match.
   other .cu     -O3
   mc_scene.cpp, mc_obj.cpp  g++ -O2 -ffp-contract=off (host scene, camera and OBJ
@@ -41,6 +41,7 @@ UNITS = {
     "mc_server.cu": ["-O3"],
     "mc_ingest.cu": ["-O3", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "mc_resolve.cu": ["-O3", "--use_fast_math"],
+    "mc_volume.cu": ["-O3", "--use_fast_math"],
 }
 HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_image.cpp": ["-O2"],
               "mc_obj.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"]}

@@ -652,39 +652,111 @@ __global__ void k_scatter_ids(const int* __restrict__ roots, int n, int* __restr
     if (i < n) wideId[roots[i]] = i;
 }
 
-// One level of the collapse: every wide node of the frontier picks its slots
-// and gives its internal slots consecutive wide ids (the next frontier).
-__global__ void k_wide_greedy_level(const float4* __restrict__ nodes, const int* __restrict__ frontier,
-                                    const int* __restrict__ count, int capacity, int* __restrict__ next,
-                                    int* __restrict__ nextCount, int* __restrict__ wideId, int* __restrict__ rootOf,
-                                    int* counter, int* err) {
-    const int n = min(*count, capacity);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// One level of the collapse, in three launches so that wide ids follow the
+// frontier's order (the same layout on every build: breadth first, the
+// internal children of a wide node consecutive, in slot order).
+// Count: every wide node of the frontier picks its slots, keeps its internal
+// ones in slot order and adds their number to its block's total.
+__global__ void __launch_bounds__(kBlock) k_wide_level_count(const float4* __restrict__ nodes,
+                                                             const int* __restrict__ frontier, int n, int capacity,
+                                                             const int* __restrict__ wideId, int* __restrict__ rootOf,
+                                                             int4* __restrict__ internal, int* __restrict__ blockTotals,
+                                                             int* err) {
+    __shared__ int warpSum[kBlock / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int nInt = 0;
+    if (i < n) {
         const int B = frontier[i];
         const int w = wideId[B];
+        int r[4] = {-1, -1, -1, -1};
         if (w < 0 || w >= capacity) {
             atomicOr(err, MC_DEVERR_INPUT);
-            continue;
+        } else {
+            rootOf[w] = B;
+            WideSlots s;
+            greedy_slots(nodes, B, s);
+            for (int j = 0; j < s.n; j++)
+                if (s.ref[j] >= 0) r[nInt++] = s.ref[j];
         }
-        rootOf[w] = B;
-        WideSlots s;
-        greedy_slots(nodes, B, s);
-        int nInt = 0;
-        for (int j = 0; j < s.n; j++) nInt += s.ref[j] >= 0 ? 1 : 0;
-        if (nInt == 0) continue;
-        const int base = atomicAdd(counter, nInt);
-        const int out = atomicAdd(nextCount, nInt);
-        int k = 0;
-        for (int j = 0; j < s.n; j++) {
-            if (s.ref[j] < 0) continue;
-            if (base + k >= capacity || out + k >= capacity) {
-                atomicOr(err, MC_DEVERR_INPUT);
-                break;
+        internal[i] = make_int4(r[0], r[1], r[2], r[3]);
+    }
+    int v = nInt;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warpSum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int k = 0; k < kBlock / 32; k++) t += warpSum[k];
+        blockTotals[blockIdx.x] = t;
+    }
+}
+
+// Scan: exclusive prefix of the block totals by one block of 1024 threads;
+// the level's total (the next frontier's size) goes to *total.
+__global__ void __launch_bounds__(1024) k_wide_level_scan(int* blockTotals, int blocks, int* total) {
+    __shared__ int warpSums[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < blocks; base += 1024) {
+        const int t = base + threadIdx.x;
+        const int c = t < blocks ? blockTotals[t] : 0;
+        int x = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSums[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int s = warpSums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
             }
-            wideId[s.ref[j]] = base + k;
-            next[out + k] = s.ref[j];
-            k++;
+            warpSums[lane] = s;
         }
+        __syncthreads();
+        const int before = carry + (wid > 0 ? warpSums[wid - 1] : 0) + x - c;
+        if (t < blocks) blockTotals[t] = before;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = before + c;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// Write: the internal children of frontier node i take wide ids idBase + o,
+// o = (internal children of the nodes before i), and the same places of the
+// next frontier.
+__global__ void __launch_bounds__(kBlock) k_wide_level_write(const int4* __restrict__ internal, int n,
+                                                             const int* __restrict__ blockFirst, int idBase,
+                                                             int capacity, int* __restrict__ next,
+                                                             int* __restrict__ wideId, int* err) {
+    __shared__ int warpSum[kBlock / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int4 r = make_int4(-1, -1, -1, -1);
+    if (i < n) r = internal[i];
+    const int nInt = (r.x >= 0) + (r.y >= 0) + (r.z >= 0) + (r.w >= 0);
+    int x = nInt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSum[wid] = x;
+    __syncthreads();
+    int off = blockFirst[blockIdx.x] + x - nInt;
+    for (int k = 0; k < wid; k++) off += warpSum[k];
+    const int refs[4] = {r.x, r.y, r.z, r.w};
+    for (int k = 0; k < nInt; k++) {
+        if (off + k >= capacity || idBase + off + k >= capacity) {
+            atomicOr(err, MC_DEVERR_INPUT);
+            break;
+        }
+        wideId[refs[k]] = idBase + off + k;
+        next[off + k] = refs[k];
     }
 }
 
@@ -1431,11 +1503,21 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
     if (NI > 0) {
         // surface-area-greedy collapse, level by level from the scene roots
         int* front[2] = {nullptr, nullptr};
-        int* cnt = nullptr;  // [0], [1]: frontier sizes, [2]: wide-id counter
-        auto release = [&]() { cudaFree(front[0]); cudaFree(front[1]); cudaFree(cnt); };
+        int* cnt = nullptr;  // [0]: next frontier size
+        int4* internal = nullptr;  // per frontier node: its internal slots
+        int* blockTotals = nullptr;
+        auto release = [&]() {
+            cudaFree(front[0]);
+            cudaFree(front[1]);
+            cudaFree(cnt);
+            cudaFree(internal);
+            cudaFree(blockTotals);
+        };
         if (cudaMalloc(&rootOf, (size_t)NI * sizeof(int)) != cudaSuccess ||
             cudaMalloc(&front[0], (size_t)NI * sizeof(int)) != cudaSuccess ||
-            cudaMalloc(&front[1], (size_t)NI * sizeof(int)) != cudaSuccess || cudaMalloc(&cnt, 4 * sizeof(int)) != cudaSuccess) {
+            cudaMalloc(&front[1], (size_t)NI * sizeof(int)) != cudaSuccess || cudaMalloc(&cnt, 4 * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&internal, (size_t)NI * sizeof(int4)) != cudaSuccess ||
+            cudaMalloc(&blockTotals, (size_t)(grid_for(NI, kBlock) + 1) * sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             release();
             cudaFree(rootOf);
@@ -1445,20 +1527,28 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         const std::vector<int> rootList = roots ? *roots : std::vector<int>(bvh->bin_roots.begin(), bvh->bin_roots.end());
         MC_CUDA(cudaMemcpyAsync(front[0], rootList.data(), rootList.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
         k_scatter_ids<<<grid_for(nseg, kBlock), kBlock, 0, ctx->stream>>>(front[0], nseg, wideId);
-        int h[3] = {nseg, 0, nseg};
-        MC_CUDA(cudaMemcpyAsync(cnt, h, 3 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        int levels = 0, cur = 0, n = nseg;
+        // wide ids 0..nseg-1 are the roots; each level's children follow in frontier order
+        int levels = 0, cur = 0, n = nseg, idBase = nseg;
         while (n > 0 && levels <= 4 * MC_STACK_CAPACITY) {
-            MC_CUDA(cudaMemsetAsync(cnt + (1 - cur), 0, sizeof(int), ctx->stream));
-            k_wide_greedy_level<<<std::max(1, std::min(grid_for(n, kBlock), ctx->sm_count * 8)), kBlock, 0, ctx->stream>>>(
-                bin, front[cur], cnt + cur, NI, front[1 - cur], cnt + (1 - cur), wideId, rootOf,
-                cnt + 2, ctx->d_error);
-            MC_CUDA(cudaMemcpyAsync(&n, cnt + (1 - cur), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            const int blocks = grid_for(n, kBlock);
+            k_wide_level_count<<<blocks, kBlock, 0, ctx->stream>>>(bin, front[cur], n, NI, wideId, rootOf, internal,
+                                                                   blockTotals, ctx->d_error);
+            k_wide_level_scan<<<1, 1024, 0, ctx->stream>>>(blockTotals, blocks, cnt);
+            k_wide_level_write<<<blocks, kBlock, 0, ctx->stream>>>(internal, n, blockTotals, idBase, NI, front[1 - cur],
+                                                                   wideId, ctx->d_error);
+            MC_CUDA(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
             MC_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (n < 0 || (long long)idBase + n > NI) {
+                // more wide nodes than internal nodes: not a binary tree over these leaves
+                release();
+                cudaFree(rootOf);
+                return set_error(MC_ERR_INVALID, "mc_bvh_build: the collapse found %d nodes past %d", n, idBase);
+            }
+            idBase += n;
             cur = 1 - cur;
             levels++;
         }
-        MC_CUDA(cudaMemcpyAsync(&count, cnt + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        count = idBase;
         int flags = 0;
         if ((st = flags_now(ctx, &flags)) != MC_OK || flags) {
             release();

@@ -123,6 +123,7 @@ mc_status mc_context_destroy(mc_context* ctx) {
     cudaFree(ctx->d_stats);
     for (auto& b : ctx->scratch) mc::devbuf_free(b);
     mc::devbuf_free(ctx->wave.block);
+    mc::devbuf_free(ctx->volume);
     cudaFree(ctx->rng_states);
     if (ctx->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)ctx->graph_exec);
     if (ctx->own_stream) {

@@ -156,19 +156,24 @@ mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_t n_tri
 }
 
 // Picks the trace variant (persistent or plain), the refill threshold and CUDA
-// graph replay by timing one-sample renders at a reduced resolution with the
-// scene's own BVH. Results are cached per (device, layout, scene size class,
-// image size class): later calls in the same class return at once. None of
-// the choices changes the image. budget_ms bounds the tuning time (0 = 2000).
+// graph replay by timing the first wave that a render of these params traces
+// (full resolution, the wave's samples per pixel, the scene's own BVH): every
+// candidate once untimed, then three timed rounds taken in turn, each
+// candidate keeping its fastest time. Results are cached per (device, layout,
+// scene size class, wave size class): later calls in the same class return at
+// once. None of the choices changes the image. budget_ms bounds the tuning
+// time (0 = 2000); candidates not timed by then are not chosen.
 mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, mc_render_params* params, int32_t budget_ms) {
     if (!ctx || !bvh || !scene || !params) return mc::set_error(MC_ERR_INVALID, "mc_autotune: null argument");
+    if (params->width < 1 || params->height < 1) return mc::set_error(MC_ERR_INVALID, "mc_autotune: empty image");
     if (budget_ms <= 0) budget_ms = 2000;
     struct Choice { int persistent, refill, graph; };
     static std::mutex mu;
     static std::map<std::array<long long, 4>, Choice> cache;
     auto log2c = [](long long v) { int b = 0; while (v > 1) { v >>= 1; b++; } return (long long)b; };
-    const std::array<long long, 4> key = {(long long)ctx->device, (long long)bvh->layout, log2c(bvh->n),
-                                          log2c((long long)params->width * params->height)};
+    const int k = mc::wave_samples(params);
+    const long long pixels = (long long)params->width * params->height;
+    const std::array<long long, 4> key = {(long long)ctx->device, (long long)bvh->layout, log2c(bvh->n), log2c(pixels * k)};
     {
         std::lock_guard<std::mutex> lock(mu);
         auto it = cache.find(key);
@@ -180,58 +185,59 @@ mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* s
         }
     }
     mc_render_params probe = *params;
-    int scale = 1;
-    while ((long long)(probe.width / scale) * (probe.height / scale) > 1 << 19) scale *= 2;
-    probe.width = params->width / scale > 0 ? params->width / scale : 1;
-    probe.height = params->height / scale > 0 ? params->height / scale : 1;
-    probe.camera.image_width = probe.width;
-    probe.camera.aspect_ratio = probe.width / float(probe.height);
-    mc_camera_initialize(&probe.camera);
-    probe.spp = 1;
-    probe.rng = MC_RNG_PHILOX;
+    probe.spp = k;
+    probe.samples_per_wave = k;
+    probe.first_sample = 0;
     probe.instrument = 0;
     float* dAcc = nullptr;
-    if (cudaMalloc(&dAcc, (size_t)probe.width * probe.height * 3 * sizeof(float)) != cudaSuccess) {
+    if (cudaMalloc(&dAcc, (size_t)pixels * 3 * sizeof(float)) != cudaSuccess) {
         cudaGetLastError();
         return mc::set_error(MC_ERR_OOM, "mc_autotune: allocation failed");
     }
-    const Choice cands[] = {{1, 8, 0}, {1, 4, 0}, {1, 12, 0}, {1, 16, 0}, {1, 24, 0}, {0, 8, 0}};
-    float best = 1e30f;
-    Choice bestC = {params->persistent, params->refill_threshold > 0 ? params->refill_threshold : 8, params->use_graph};
+    std::vector<Choice> cands = {{1, 8, 0}, {1, 4, 0}, {1, 12, 0}, {1, 16, 0}, {1, 24, 0}, {0, 8, 0}};
     auto t0 = std::chrono::steady_clock::now();
-    auto timeOne = [&](const Choice& c, float* ms) -> mc_status {
+    auto elapsed = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
+    auto run = [&](const Choice& c, float* ms) -> mc_status {
         probe.persistent = c.persistent;
         probe.refill_threshold = c.refill;
         probe.use_graph = c.graph;
         mc_render_stats rs;
-        mc_status st = mc_render_wavefront(ctx, bvh, scene, &probe, dAcc, &rs);  // warm-up (and graph capture)
-        if (st != MC_OK) return st;
-        // graph replays are not timed by the render's own events: time the call
         auto a = std::chrono::steady_clock::now();
-        st = mc_render_wavefront(ctx, bvh, scene, &probe, dAcc, &rs);
-        cudaStreamSynchronize(ctx->stream);
-        *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - a).count();
+        mc_status st = mc_render_wavefront(ctx, bvh, scene, &probe, dAcc, &rs);
+        if (cudaDeviceSynchronize() != cudaSuccess && st == MC_OK) st = mc::set_error(MC_ERR_CUDA, "mc_autotune: render failed");
+        if (ms) *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - a).count();
         return st;
     };
-    mc_status st = MC_OK;
-    for (const Choice& c : cands) {
-        float ms = 0.f;
-        if ((st = timeOne(c, &ms)) != MC_OK) break;
-        if (ms < best) {
-            best = ms;
-            bestC = c;
+    // warm-up of every candidate (kernel loads, buffers, graph capture), then timed rounds
+    auto tune = [&](std::vector<Choice>& cs, std::vector<float>& best) -> mc_status {
+        best.assign(cs.size(), 1e30f);
+        for (const Choice& c : cs) {
+            mc_status st = run(c, nullptr);
+            if (st != MC_OK) return st;
         }
-        double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        if (el > budget_ms) break;
-    }
+        for (int round = 0; round < 3 && elapsed() < budget_ms; round++) {
+            for (size_t i = 0; i < cs.size(); i++) {
+                float ms = 0.f;
+                mc_status st = run(cs[i], &ms);
+                if (st != MC_OK) return st;
+                best[i] = std::min(best[i], ms);
+            }
+        }
+        return MC_OK;
+    };
+    std::vector<float> best;
+    mc_status st = tune(cands, best);
+    Choice bestC = {params->persistent, params->refill_threshold > 0 ? params->refill_threshold : 8, params->use_graph};
     if (st == MC_OK) {
-        Choice g = bestC;
-        g.graph = 1;
-        float ms = 0.f;
-        if ((st = timeOne(g, &ms)) == MC_OK && ms < best) {
-            best = ms;
-            bestC = g;
-        }
+        size_t b = 0;
+        for (size_t i = 1; i < cands.size(); i++)
+            if (best[i] < best[b]) b = i;
+        if (best[b] < 1e30f) bestC = cands[b];
+        // graph replay of the winner against the winner as launched
+        std::vector<Choice> pair = {bestC, bestC};
+        pair[1].graph = 1;
+        std::vector<float> bp;
+        if ((st = tune(pair, bp)) == MC_OK && bp[1] < bp[0]) bestC = pair[1];
     }
     cudaFree(dAcc);
     if (st != MC_OK) return st;

@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kThreads) k_ingest_split(const mc_triangle* __
     __syncthreads();
 
     // PT:651-655 calculate_bounding_box: min/max of the vertices -/+ 1e-3.
-    bool emissive = false, medium = false;
+    bool emissive = false, medium = false, grid = false;
     if (threadIdx.x < cnt) {
         const mc_triangle& t = *reinterpret_cast<const mc_triangle*>(sTri + threadIdx.x * kTriWords);
         const float eps = 1e-3f;
@@ -83,12 +83,14 @@ __global__ void __launch_bounds__(kThreads) k_ingest_split(const mc_triangle* __
         b[7] = 0.f;
         emissive = t.mat.type == MC_MAT_EMISSIVE;
         medium = t.mat.type == MC_MAT_ISOTROPIC;
+        grid = medium && t.mat.density_grid != nullptr;
     }
     const int lights = __syncthreads_count(emissive);
     const int anyMedium = __syncthreads_or(medium);
+    const int anyGrid = __syncthreads_or(grid);
     if (threadIdx.x == 0) {
         tileCount[blockIdx.x] = lights;
-        if (anyMedium) atomicOr(flags, 1);
+        if (anyMedium) atomicOr(flags, anyGrid ? MC_MEDIUM_ANY | MC_MEDIUM_GRID : MC_MEDIUM_ANY);
     }
 
     // Hot records: the first 9 words of each triangle.
@@ -196,7 +198,8 @@ __global__ void __launch_bounds__(kTile) k_ingest_lights(const mc_triangle* __re
 
 __global__ void k_ingest_spheres(const mc_sphere* __restrict__ sph, int ns, int* __restrict__ flags) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x)
-        if (sph[i].mat.type == MC_MAT_ISOTROPIC) atomicOr(flags, 1);
+        if (sph[i].mat.type == MC_MAT_ISOTROPIC)
+            atomicOr(flags, sph[i].mat.density_grid ? MC_MEDIUM_ANY | MC_MEDIUM_GRID : MC_MEDIUM_ANY);
 }
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
@@ -245,7 +248,7 @@ extern "C" mc_status mc_scene_ingest(mc_context* ctx, const mc_triangle* tris, i
     MC_CUDA(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     MC_CUDA(cudaStreamSynchronize(ctx->stream));
     if (light_count) *light_count = h[1];
-    if (has_medium) *has_medium = h[0] & 1;
+    if (has_medium) *has_medium = h[0] & (MC_MEDIUM_ANY | MC_MEDIUM_GRID);
     return MC_OK;
 }
 

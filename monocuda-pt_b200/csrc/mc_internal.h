@@ -84,6 +84,7 @@ struct mc_context {
     long long* d_stats = nullptr;      // 2 * MC_MAX_DEPTH_STATS accumulated ray counts
     mc::DevBuf scratch[8];             // build / sort scratch
     mc::WaveBuffers wave;
+    mc::DevBuf volume;                 // per shadow slot: medium crossings (scenes with density grids)
     void* rng_states = nullptr;        // curandState per pixel (XORWOW mode)
     int rng_pixels = 0;
     unsigned long long rng_seed = 0;
@@ -199,5 +200,7 @@ mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, 
 // Grows the training batch buffer to hold `records` records.
 mc_status guide_reserve_batch(mc_guide* g, int records);
 mc_status guide_reserve_tiles(mc_guide* g, int tiles);
+// Samples per pixel in one wave of a single-image render of these params.
+int wave_samples(const mc_render_params* params);
 mc_status guide_reserve_paths(mc_guide* g, int paths);
 }

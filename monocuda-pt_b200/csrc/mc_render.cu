@@ -26,6 +26,7 @@
 #include "mc_rng.cuh"
 #include "mc_shade.cuh"
 #include "mc_traverse.cuh"
+#include "mc_volume.cuh"
 
 #define MC_CUDA(call)                                                                      \
     do {                                                                                   \
@@ -126,6 +127,14 @@ struct TraceArgs {
     int* err;
     unsigned long long* counts;  // [0] node visits, [1] leaf tests (counting variant)
     int oneShot;                 // plain mode: one ray per thread, no refill
+    // launches with gridded media (MC_MEDIUM_GRID): per shadow slot, the
+    // distance of each medium crossing and, for back faces, the homogeneous
+    // factor or the crossed primitive of a grid; rays that crossed a grid are
+    // listed (count in vdefer[0]) for k_ratio_track, which draws their random numbers
+    float4* vsegT;
+    int4* vsegX;
+    int* vmeta;
+    int* vdefer;
 };
 
 // Warp-reduces the lane counters and adds them to the global pair.
@@ -143,8 +152,10 @@ MC_D void flush_counts(const TraceArgs& a, const TravCount& c) {
 
 enum { RAY_EXTEND = 0, RAY_SHADOW_ANY = 1, RAY_SHADOW_MEDIUM = 2 };
 
-// Finishes one ray. Returns true when the lane is free again.
-template <int ISECT>
+// Finishes one ray. Returns true when the lane is free again. GRID: the
+// launch's scenes hold density grids (the crossing bookkeeping for
+// k_ratio_track is compiled in only then).
+template <int ISECT, bool GRID>
 MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle_cold* cold, const mc_sphere* spheres,
                      TravState& s, int step, int kind, int slot, float& T, float& travelled, int& crossings) {
     if (kind == RAY_EXTEND) {
@@ -202,12 +213,30 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
                 hit_sphere_ref(v3(sp.center), v3(sp.center1), sp.is_moving != 0, sp.radius, s.r.o, s.r.d, s.time, tt, front,
                                outward);
             }
-            if (!front) T = T * expf(-density * s.tmax);
+            const int c = GRID ? crossings & 15 : crossings;
+            if (!front) {
+                if (GRID && m->density_grid) {
+                    // ratio tracking draws random numbers: deferred to k_ratio_track.
+                    // Ray-set queries (occluded output) draw none and skip the grid.
+                    if (a.vsegT) {
+                        (&a.vsegX[slot].x)[c] = type == 1 ? id : -1 - id;
+                        crossings |= 1 << (4 + c);
+                    }
+                } else {
+                    const float f = expf(-density * s.tmax);
+                    T = T * f;
+                    if (GRID && a.vsegT) {
+                        (&a.vsegX[slot].x)[c] = __float_as_int(f);
+                        crossings |= 1 << (8 + c);
+                    }
+                }
+            }
+            if (GRID && a.vsegT) (&a.vsegT[slot].x)[c] = s.tmax;
             travelled = travelled + s.tmax;
             V3 hp = s.r.o + s.r.d * s.tmax;
             crossings++;
             float remaining = a.smax[slot] - travelled;
-            if (crossings >= 4 || remaining <= 0.0f) {
+            if ((GRID ? crossings & 15 : crossings) >= 4 || remaining <= 0.0f) {
                 done = true;
             } else {
                 s.r.o = hp;
@@ -223,6 +252,12 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
         a.occluded[slot] = (blocked || !(T > 0.0f)) ? 1 : 0;
         return true;
     }
+    if (GRID && (crossings & 0xf0)) {
+        // a grid was crossed: k_ratio_track finishes the ray in crossing order
+        a.vmeta[slot] = crossings | (blocked ? 1 << 12 : 0);
+        a.vdefer[1 + atomicAdd(a.vdefer, 1)] = slot;
+        return true;
+    }
     if (!blocked && T > 0.0f) {
         int p = a.spath[slot];
         a.sr[p] += a.scr[slot] * T;
@@ -232,8 +267,9 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
     return true;
 }
 
-// MEDIUM: some scene of the launch holds a medium, so its shadow rays take the
-// closest-hit loop of mediumTransmittance instead of any-hit (PT:3711-3720).
+// MED: 1 when some scene of the launch holds a medium, so its shadow rays take
+// the closest-hit loop of mediumTransmittance instead of any-hit
+// (PT:3711-3720); 2 when some medium also has a density grid.
 // BATCH: rays of several scenes share the launch; each lane reads its ray's
 // scene from the wave table. A single-scene launch reads the scene from the
 // kernel parameters instead, which costs no registers.
@@ -242,7 +278,7 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 #endif
 constexpr int kTraceThreads = 256;
 constexpr int kTraceSmem = MC_SMEM_STACK ? kTraceThreads * MC_STACK_CAPACITY * (int)sizeof(int) : 0;
-template <int ISECT, bool MEDIUM, bool COUNT, int LAY, bool BATCH>
+template <int ISECT, int MED, bool COUNT, int LAY, bool BATCH>
 __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
@@ -299,7 +335,7 @@ __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(Tr
                             slot = q - extCount;
                             int path = a.spath ? a.spath[slot] : slot;
                             if (BATCH) sid = scene_of(a.tab, a.sceneOf, path);
-                            const bool med = MEDIUM && (BATCH ? a.tab->scenes[sid].hasMedium != 0 : a.medium0 != 0);
+                            const bool med = MED != 0 && (BATCH ? a.tab->scenes[sid].hasMedium != 0 : a.medium0 != 0);
                             kind = med ? RAY_SHADOW_MEDIUM : RAY_SHADOW_ANY;
                             o = V3(a.sox[slot], a.soy[slot], a.soz[slot]);
                             d = V3(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
@@ -321,7 +357,7 @@ __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(Tr
                             // (no leaf, so the material arrays are not read)
                             s.tmax = tmax;
                             s.hitLeaf = -1;
-                            finish_ray<ISECT>(a, ts, nullptr, nullptr, s, STEP_DONE, kind, slot, T, travelled, crossings);
+                            finish_ray<ISECT, MED == 2>(a, ts, nullptr, nullptr, s, STEP_DONE, kind, slot, T, travelled, crossings);
                             has = false;
                         }
                         if (has) {
@@ -340,11 +376,11 @@ __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(Tr
             if (r != STEP_CONTINUE) {
                 const mc_triangle_cold* cold = a.cold0;
                 const mc_sphere* spheres = a.spheres0;
-                if (BATCH && MEDIUM && kind == RAY_SHADOW_MEDIUM) {
+                if (BATCH && MED != 0 && kind == RAY_SHADOW_MEDIUM) {
                     cold = a.tab->scenes[sid].cold;
                     spheres = a.tab->scenes[sid].spheres;
                 }
-                if (finish_ray<ISECT>(a, ts, cold, spheres, s, r, kind, slot, T, travelled, crossings)) has = false;
+                if (finish_ray<ISECT, MED == 2>(a, ts, cold, spheres, s, r, kind, slot, T, travelled, crossings)) has = false;
             }
         }
     }
@@ -533,7 +569,13 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
     V3 scatterOrigin = hitPoint;
     if (mat.type == MC_MAT_ISOTROPIC) {
         float sd;
-        if (frontFace) sd = hitT;
+        const mc_material& M = ptype == 0 ? S.spheres[pidx].mat : S.cold[pidx].mat;
+        const mc_volume_grid* grid = static_cast<const mc_volume_grid*>(M.density_grid);
+        // a grid in a scene whose flags lack MC_MEDIUM_GRID: its shadow rays were
+        // traced without grid bookkeeping
+        if (grid && !(S.hasMedium & MC_MEDIUM_GRID)) atomicOr(a.err, MC_DEVERR_INPUT);
+        if (frontFace) sd = hitT;  // this hit only enters the medium
+        else if (grid) sd = volume_free_flight(grid, mat.density, M.grid_max_density, o, inDir, hitT, rng);  // PT:3562-3564
         else sd = -logf(1.0f - rng.uniform()) / mat.density;
         if (sd >= hitT) {
             a.ox[p] = hitPoint.x;
@@ -964,6 +1006,58 @@ __global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab,
     }
 }
 
+// Finishes the shadow rays that crossed a density grid (k_trace lists them),
+// as mediumTransmittance does (PT:2874-2898): each crossing's segment starts
+// where the previous one ended; a back face multiplies the transmittance, in
+// crossing order, by its homogeneous factor or by ratio tracking through the
+// grid on the path's random numbers, which are stored back (PT:3712-3716).
+// Runs after the trace launch and before the next shade, the reference's
+// order of draws (shade, then shadow, then the next shade).
+struct RatioArgs {
+    const float4* segT;
+    const int4* segX;
+    const int* meta;
+    const int* list;       // [0] count, then shadow slots
+    float *sr, *sg, *sb;   // the sample accumulators of the trace launch
+};
+
+template <class Rng>
+__global__ void __launch_bounds__(256) k_ratio_track(ShadeArgs a, RatioArgs v) {
+    const int n = min(v.list[0], a.capacity);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = v.list[1 + i];
+        const int p = a.spath[slot];
+        const SceneGPU& S = a.tab->scenes[scene_of(a.tab, a.sceneOf, p)];
+        const int meta = v.meta[slot];
+        const float4 ts = v.segT[slot];
+        const int4 xs = v.segX[slot];
+        V3 o(a.sox[slot], a.soy[slot], a.soz[slot]);
+        const V3 d(a.sdx[slot], a.sdy[slot], a.sdz[slot]);
+        Rng rng;
+        rng_load<Rng>(a, S, p, rng);
+        float T = 1.0f;
+        const int count = meta & 15;
+        for (int c = 0; c < count; c++) {
+            const float t = (&ts.x)[c];
+            const int x = (&xs.x)[c];
+            if (meta & (1 << (4 + c))) {
+                const mc_material& m = x >= 0 ? S.cold[x].mat : S.spheres[-1 - x].mat;
+                T = T * volume_transmittance(static_cast<const mc_volume_grid*>(m.density_grid), m.density,
+                                             m.grid_max_density, o, d, t, rng);
+            } else if (meta & (1 << (8 + c))) {
+                T = T * __int_as_float(x);
+            }
+            o = o + d * t;
+        }
+        rng_store<Rng>(a, S, p, rng);
+        if (!(meta & (1 << 12)) && T > 0.0f) {
+            v.sr[p] += a.scr[slot] * T;
+            v.sg[p] += a.scg[slot] * T;
+            v.sb[p] += a.scb[slot] * T;
+        }
+    }
+}
+
 __global__ void k_accumulate_counts(const int* counters, int maxDepth, long long* stats) {
     int d = threadIdx.x;
     if (d >= maxDepth || d >= MC_MAX_DEPTH_STATS) return;
@@ -985,14 +1079,16 @@ int occupancy_blocks(const void* fn, int sms, size_t smem = 0) {
 
 typedef void (*TraceKernel)(TraceArgs);
 
-// [batch][layout][count][medium][isect]
-#define MC_TK(L, B)                                                                                                           \
-    {{{k_trace<0, false, false, L, B>, k_trace<1, false, false, L, B>}, {k_trace<0, true, false, L, B>, k_trace<1, true, false, L, B>}}, \
-     {{k_trace<0, false, true, L, B>, k_trace<1, false, true, L, B>}, {k_trace<0, true, true, L, B>, k_trace<1, true, true, L, B>}}}
-TraceKernel trace_kernel(bool batch, int layout, bool count, bool medium, int isect) {
-    static const TraceKernel table[2][3][2][2][2] = {{MC_TK(0, false), MC_TK(1, false), MC_TK(2, false)},
+// [batch][layout][count][medium kind][isect]
+#define MC_TKM(C, L, B)                                                                                   \
+    {{k_trace<0, 0, C, L, B>, k_trace<1, 0, C, L, B>}, {k_trace<0, 1, C, L, B>, k_trace<1, 1, C, L, B>}, \
+     {k_trace<0, 2, C, L, B>, k_trace<1, 2, C, L, B>}}
+#define MC_TK(L, B) {MC_TKM(false, L, B), MC_TKM(true, L, B)}
+// medium: 0 none, 1 homogeneous media only, 2 media with density grids
+TraceKernel trace_kernel(bool batch, int layout, bool count, int medium, int isect) {
+    static const TraceKernel table[2][3][2][3][2] = {{MC_TK(0, false), MC_TK(1, false), MC_TK(2, false)},
                                                      {MC_TK(0, true), MC_TK(1, true), MC_TK(2, true)}};
-    return table[batch ? 1 : 0][layout][count ? 1 : 0][medium ? 1 : 0][isect ? 1 : 0];
+    return table[batch ? 1 : 0][layout][count ? 1 : 0][medium][isect ? 1 : 0];
 }
 
 // Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
@@ -1000,15 +1096,15 @@ TraceKernel trace_kernel(bool batch, int layout, bool count, bool medium, int is
 // one ray per thread and no refill, over plainBlocks blocks; sharing the kernel
 // keeps the per-ray arithmetic identical between the two modes. A launch is a
 // batch launch when it carries a per-path scene map.
-void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, int layout, bool medium, int isect,
+void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, int layout, int medium, int isect,
                   bool persistent, int plainBlocks, bool count = false) {
-    static int occ[64] = {0};
-    static bool attr[64] = {false};
+    static int occ[128] = {0};
+    static bool attr[128] = {false};
     TraceArgs t = t0;
     t.oneShot = persistent ? 0 : 1;
     const bool batch = t.sceneOf != nullptr;
     TraceKernel fn = trace_kernel(batch, layout, count, medium, isect);
-    const int key = (medium ? 1 : 0) + (isect ? 2 : 0) + (count ? 4 : 0) + (batch ? 8 : 0) + 16 * layout;  // < 48
+    const int key = medium + 3 * (isect ? 1 : 0) + 6 * (count ? 1 : 0) + 12 * (batch ? 1 : 0) + 24 * layout;  // < 72
     if (kTraceSmem > 48 * 1024 && !attr[key]) {
         cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kTraceSmem);
         attr[key] = true;
@@ -1167,7 +1263,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     const bool countVisits = (p0.instrument & 1) != 0;
     const bool timeTrace = (p0.instrument & 2) != 0;
     int capacity = 0, maxD = 0, waves = 0;
-    bool medium = false;
+    bool medium = false, grid = false;
     auto item_spw = [&](int i) { return std::max(1, std::min(items[i].spw, std::max(1, items[i].p->spp))); };
     auto item_waves = [&](int i) { return (items[i].p->spp + item_spw(i) - 1) / item_spw(i); };
     // every item on one scene: single-scene trace launches
@@ -1177,6 +1273,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         maxD = std::max(maxD, items[i].p->max_depth);
         waves = std::max(waves, item_waves(i));
         medium = medium || items[i].view->has_medium;
+        grid = grid || (items[i].view->has_medium & MC_MEDIUM_GRID) != 0;
         if (items[i].view != items[0].view || items[i].bvh != items[0].bvh || items[i].root != items[0].root)
             sameScene = false;
     }
@@ -1238,6 +1335,24 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         ta.sceneOf = nullptr;
     }
 
+    RatioArgs ra;
+    std::memset(&ra, 0, sizeof(ra));
+    if (grid) {
+        // per shadow slot: crossing distances (float4), factors / grid primitives
+        // (int4), the crossing mask (int); then the list of deferred slots
+        const size_t cap = (size_t)capacity;
+        if ((st = devbuf_reserve(ctx->volume, cap * 36 + (cap + 1) * sizeof(int))) != MC_OK) return st;
+        char* base = (char*)ctx->volume.ptr;
+        ta.vsegT = (float4*)base;
+        ta.vsegX = (int4*)(base + cap * 16);
+        ta.vmeta = (int*)(base + cap * 32);
+        ta.vdefer = (int*)(base + cap * 36);
+        ra.segT = ta.vsegT;
+        ra.segX = ta.vsegX;
+        ra.meta = ta.vmeta;
+        ra.list = ta.vdefer;
+    }
+
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
     std::vector<cudaEvent_t> traceEvents;
@@ -1293,10 +1408,18 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 // its training records see only the light through the sampled direction
                 t.sr = nee0[0]; t.sg = nee0[1]; t.sb = nee0[2];
             }
+            if (grid && d > 0) MC_CUDA(cudaMemsetAsync(ta.vdefer, 0, sizeof(int), stream));
             if (timeTrace) traceEvent();
-            launch_trace(ctx, stream, t, layout, medium, isect, persistent, plainBlocks, countVisits);
+            launch_trace(ctx, stream, t, layout, grid ? 2 : medium ? 1 : 0, isect, persistent, plainBlocks, countVisits);
             if (timeTrace) traceEvent();
             launches++;
+            if (grid && d > 0) {
+                RatioArgs r = ra;
+                r.sr = t.sr; r.sg = t.sg; r.sb = t.sb;
+                if (philox || guide) k_ratio_track<PhiloxRng><<<loopBlocks, 256, 0, stream>>>(sa, r);
+                else k_ratio_track<XorwowRng><<<loopBlocks, 256, 0, stream>>>(sa, r);
+                launches++;
+            }
             if (d == maxD) break;
             if (guide) {
                 mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], C + d * MC_COUNTERS_PER_DEPTH + 0, capacity,
@@ -1363,7 +1486,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                                       (unsigned long long)maxD,
                                       (unsigned long long)((layout << 6) | (medium ? 2 : 0) | (philox ? 4 : 0) |
                                                            (persistent ? 8 : 0) | (n > 1 ? 16 : 0) |
-                                                           (sameScene ? 32 : 0)),
+                                                           (sameScene ? 32 : 0) | (grid ? 1024 : 0)),
                                       (unsigned long long)isect,
                                       (unsigned long long)ta.refill,
                                       (unsigned long long)(uintptr_t)ta.ts0.nodes,
@@ -1437,7 +1560,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         MC_CUDA(cudaEventRecord((cudaEvent_t)ctx->table_events[slot], stream));
         if (useGraph) {
             MC_CUDA(cudaGraphLaunch(exec, stream));
-            perWave = 3 + 2 * maxD;
+            perWave = 3 + 2 * maxD + (grid ? maxD : 0);
         } else {
             if ((st = enqueue_wave()) != MC_OK) return st;
         }
@@ -1529,6 +1652,28 @@ static void ray_set_scene(TraceArgs& t, const mc_bvh* bvh, const mc_scene_view* 
 
 }  // namespace mc
 
+namespace mc {
+// Samples per pixel in one wave of a single-image render: the tail bounces
+// (few rays, a few long traversals set the launch time) and the launch
+// sequence are then paid once per wave.
+int wave_samples(const mc_render_params* params) {
+    const long long pixels = (long long)params->width * params->height;
+    int k = 1;
+    if (params->rng == MC_RNG_PHILOX && params->spp > 1) {
+        if (params->samples_per_wave > 0) {
+            k = std::min(params->samples_per_wave, params->spp);
+        } else if (params->samples_per_wave == 0) {
+            // up to 32M paths per wave (about 4.5 GB of path and queue state)
+            const long long perWave = 32ll << 20;
+            k = (int)std::max(1ll, std::min<long long>({perWave / std::max(pixels, 1ll), 16ll, (long long)params->spp}));
+        }
+    }
+    if (params->queue_capacity > 0 && k > 1) k = 1;  // a fixed queue capacity is one image's paths
+    if ((long long)k * pixels >= (1ll << 30)) k = 1;
+    return k;
+}
+}  // namespace mc
+
 extern "C" {
 
 mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed) {
@@ -1551,22 +1696,8 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
         if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
     }
     const int root = bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[0] : bvh->bin_roots[0];
-    // samples per wave: the tail bounces (few rays, a few long traversals set
-    // the launch time) and the launch sequence are then paid once per wave
-    int k = 1;
-    if (params->rng == MC_RNG_PHILOX && params->spp > 1) {
-        if (params->samples_per_wave > 0) {
-            k = std::min(params->samples_per_wave, params->spp);
-        } else if (params->samples_per_wave == 0) {
-            // up to 32M paths per wave (about 4.5 GB of path and queue state)
-            const long long perWave = 32ll << 20;
-            k = (int)std::max(1ll, std::min<long long>({perWave / pixels, 16ll, (long long)params->spp}));
-        }
-    }
-    if (params->queue_capacity > 0 && k > 1) k = 1;  // a fixed queue capacity is one image's paths
-    if ((long long)k * pixels >= (1ll << 30)) k = 1;
     mc::WaveItem it{scene, params, d_accum, root, 0};
-    it.spw = k;
+    it.spw = mc::wave_samples(params);
     return mc::render_items(ctx, bvh, &it, 1, params->use_graph != 0, stats);
 }
 

@@ -103,6 +103,15 @@ class Camera(C.Structure):
                 ("focus_distance", C.c_float), ("rr_cap", C.c_float)]
 
 
+class VolumeGrid(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("voxel_size", C.c_float), ("inv_voxel_size", C.c_float),
+                ("dims", C.c_int32 * 3), ("maximum_density", C.c_float), ("world_min", C.c_float * 3),
+                ("world_max", C.c_float * 3), ("pad0", C.c_int32)]
+
+
+MEDIUM_ANY, MEDIUM_GRID = 1, 2
+
+
 class EnvMap(C.Structure):
     _fields_ = [("texture", C.c_uint64), ("enabled", C.c_int32), ("intensity", C.c_float), ("rotation", C.c_float),
                 ("row_cdf", C.c_void_p), ("col_cdf", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32),
@@ -193,7 +202,7 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, GuideConfig: 80, RenderParams: 240,
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, VolumeGrid: 64, GuideConfig: 80, RenderParams: 240,
          ServerConfig: 24, ServerRequest: 256, ServerResult: 56, ServerStats: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
@@ -263,6 +272,10 @@ SIGNATURES = {
     "mc_image_texture_destroy": (I32, [C.c_uint64]),
     "mc_image_encode_host": (I32, [P, P, I32, I32, I32, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64),
                                    C.POINTER(C.c_float)]),
+    "mc_volume_grid_create": (I32, [P, P, I32, I32, I32, P, C.c_float, C.POINTER(C.c_void_p), C.POINTER(VolumeGrid)]),
+    "mc_volume_grid_destroy": (I32, [P]),
+    "mc_volume_fog_sphere": (I32, [C.c_float, C.c_float, C.c_float, P, P, P]),
+    "mc_volume_density": (I32, [P, P, P, I32, P]),
     "mc_server_get_stats": (I32, [P, C.POINTER(ServerStats)]),
     "mc_server_now": (C.c_double, [P]),
 }
@@ -418,6 +431,24 @@ def host_env(scene):
     return np.frombuffer(buf, dtype=np.float32).reshape(scene.env_height, scene.env_width, 4)
 
 
+def _medium_flags(records, count, record_type):
+    """MEDIUM_ANY when a record's material is isotropic, | MEDIUM_GRID when
+    one of those has a density grid (what mc_scene_ingest reports)."""
+    import numpy as np
+    if not count:
+        return 0
+    size = C.sizeof(record_type)
+    raw = np.frombuffer(records, dtype=np.uint8, count=count * size).reshape(count, size)
+    mat = record_type.mat.offset
+    t = mat + Material.type.offset
+    g = mat + Material.density_grid.offset
+    iso = raw[:, t:t + 4].copy().view(np.int32).ravel() == MAT_ISOTROPIC
+    if not iso.any():
+        return 0
+    grid = raw[:, g:g + 8].copy().view(np.uint64).ravel() != 0
+    return MEDIUM_ANY | (MEDIUM_GRID if (iso & grid).any() else 0)
+
+
 class DeviceScene:
     """Uploads host triangles/spheres the way the reference's main() does
     (PT:4276-4303): hot/cold split, light list, environment texture. Device
@@ -451,7 +482,7 @@ class DeviceScene:
                                            self.spheres.data_ptr() if ns else None, ns, self.hot.data_ptr(),
                                            self.cold.data_ptr(), self.lights.data_ptr(), C.byref(nl), C.byref(med)))
             self.light_count = nl.value
-            self._finish(n, ns, nl.value, bool(med.value), env_rgba, env_intensity, env_rotation)
+            self._finish(n, ns, nl.value, med.value, env_rgba, env_intensity, env_rotation)
             return
         hot = (TriangleHot * max(n, 1))()
         cold = (TriangleCold * max(n, 1))()
@@ -469,12 +500,7 @@ class DeviceScene:
         self.hot = up(hot, n, 36)
         self.cold = up(cold, n, 192)
         self.lights = up(lights, nl.value, 64)
-        medium = any(triangles[i].mat.type == MAT_ISOTROPIC for i in range(n)) if n < 100000 else None
-        if medium is None:
-            mt = np.frombuffer(triangles, dtype=np.uint8).reshape(n, 224)[:, 96:100].copy().view(np.int32).ravel()
-            medium = bool((mt == MAT_ISOTROPIC).any())
-        if ns and any(spheres[i].mat.type == MAT_ISOTROPIC for i in range(ns)):
-            medium = True
+        medium = _medium_flags(triangles, n, Triangle) | _medium_flags(spheres, ns, Sphere)
         self._finish(n, ns, nl.value, medium, env_rgba, env_intensity, env_rotation)
 
     def _finish(self, n, ns, nl, medium, env_rgba, env_intensity, env_rotation):
@@ -495,7 +521,7 @@ class DeviceScene:
         v.triangle_count = n
         v.lights = self.lights.data_ptr()
         v.light_count = nl
-        v.has_medium = 1 if medium else 0
+        v.has_medium = int(medium)
         v.env = self.env
         self.view = v
         self.n = n + ns
@@ -509,6 +535,42 @@ class DeviceScene:
             self.close()
         except Exception:
             pass
+
+
+def volume_grid_create(ctx, density, origin, voxel_size):
+    """Uploads a dense density grid, numpy (nz, ny, nx) (x fastest). Returns
+    (device pointer for Material.density_grid, VolumeGrid header); the
+    header's maximum_density is the Material's grid_max_density."""
+    import numpy as np
+    d = np.ascontiguousarray(density, dtype=np.float32)
+    assert d.ndim == 3
+    o = (C.c_float * 3)(*[float(x) for x in origin])
+    g = C.c_void_p()
+    h = VolumeGrid()
+    check(load().mc_volume_grid_create(ctx.handle, d.ctypes.data, d.shape[2], d.shape[1], d.shape[0], o,
+                                       float(voxel_size), C.byref(g), C.byref(h)))
+    return g.value, h
+
+
+def volume_grid_destroy(grid):
+    check(load().mc_volume_grid_destroy(grid))
+
+
+def fog_sphere(radius, voxel_size, half_width=3.0):
+    """The fog sphere grid (mc_volume_fog_sphere): (density (n, n, n) float32, origin)."""
+    import numpy as np
+    lib = load()
+    dims = (I32 * 3)()
+    org = (C.c_float * 3)()
+    check(lib.mc_volume_fog_sphere(radius, voxel_size, half_width, None, dims, org))
+    out = np.zeros((dims[2], dims[1], dims[0]), np.float32)
+    check(lib.mc_volume_fog_sphere(radius, voxel_size, half_width, out.ctypes.data, dims, org))
+    return out, tuple(org)
+
+
+def volume_density(ctx, grid, d_points, n, d_out):
+    """Grid values at n device points (xyz packed) into d_out, as the media sample them."""
+    check(load().mc_volume_density(ctx.handle, grid, ptr(d_points), n, ptr(d_out)))
 
 
 def image_encode(ctx, accum_ptr, width, height, samples, fmt=IMAGE_RGB8, tonemap=TONEMAP_NONE, exposure=1.0,
