@@ -25,6 +25,9 @@ namespace {
 // and the guide's per-path buffers (mixture, record, primary NEE).
 constexpr long long kWaveBytesPerPath = 29 * 4 + 1 + 16 + 2;
 constexpr long long kGuideBytesPerPath = (40 + 12 + 3) * 4;
+// scenes with density grids: per shadow slot the medium crossings (36 B) and
+// a place in the list of rays that crossed a grid (4 B)
+constexpr long long kGridBytesPerPath = 40;
 
 struct ServerScene {
     mc_scene_view view;
@@ -75,10 +78,11 @@ namespace {
 
 // A plain request traces its step's samples in one wave (one path per pixel
 // and sample); a guided one a sample per wave.
-long long request_bytes(const mc_render_params& p, bool guided, int sps) {
+long long request_bytes(const mc_render_params& p, bool guided, int sps, bool grid) {
     long long px = (long long)p.width * p.height;
     long long spw = guided ? 1 : std::max(1, std::min(sps, p.spp));
-    return px * 12 + px * spw * kWaveBytesPerPath + (guided ? px * kGuideBytesPerPath : 0);
+    return px * 12 + px * spw * (kWaveBytesPerPath + (grid ? kGridBytesPerPath : 0)) +
+           (guided ? px * kGuideBytesPerPath : 0);
 }
 
 mc_status admit(mc_server* s) {
@@ -170,7 +174,7 @@ mc_status mc_server_submit(mc_server* s, const mc_server_request* req, int64_t* 
     r.scene = req->scene_id;
     r.params = req->params;
     r.guided = req->guided != 0;
-    r.bytes = request_bytes(r.params, r.guided, s->cfg.samples_per_step);
+    r.bytes = request_bytes(r.params, r.guided, s->cfg.samples_per_step, (sc.view.has_medium & MC_MEDIUM_GRID) != 0);
     if (r.bytes + s->scene_bytes > s->cfg.hbm_budget_bytes)
         return mc::set_error(MC_ERR_BUDGET, "mc_server_submit: the request needs %lld bytes, more than the budget leaves",
                              r.bytes);
