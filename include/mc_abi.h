@@ -267,7 +267,7 @@ typedef struct mc_render_params {
     int32_t height;
     int32_t spp;                /* samples rendered by this call */
     int32_t first_sample;       /* sample index of the first one (progressive rendering) */
-    int32_t max_depth;
+    int32_t max_depth;          /* bounces, 0..MC_MAX_DEPTH (the cloud scene uses 1000, PT:4166) */
     int32_t persistent;         /* PT --persistent: persistent extend kernel */
     int32_t rng;                /* MC_RNG_* */
     uint64_t seed;              /* PT:4297 uses 1234 */
@@ -284,12 +284,13 @@ typedef struct mc_render_params {
                                    each pixel adds its samples in sample order. */
 } mc_render_params;
 
+#define MC_MAX_DEPTH 65536
 #define MC_MAX_DEPTH_STATS 64
 typedef struct mc_render_stats {
     int64_t extend_rays;        /* sum over bounces of extend-queue sizes */
     int64_t shadow_rays;        /* sum over bounces of shadow-queue sizes */
     int64_t paths;              /* width*height*spp */
-    int64_t extend_per_depth[MC_MAX_DEPTH_STATS];
+    int64_t extend_per_depth[MC_MAX_DEPTH_STATS];   /* the last entry: depth 63 and deeper */
     int64_t shadow_per_depth[MC_MAX_DEPTH_STATS];
     int64_t node_visits;        /* traversal steps (instrument bit 0) */
     int64_t leaf_tests;         /* primitive intersection tests (instrument bit 0) */

@@ -1058,6 +1058,32 @@ __global__ void __launch_bounds__(256) k_ratio_track(ShadeArgs a, RatioArgs v) {
     }
 }
 
+// Renders deeper than the counter block (max_depth > MC_MAX_DEPTH_STATS) use
+// its MC_MAX_DEPTH_STATS + 1 slots as a ring: bounce d's counters live in
+// slot d % kRingSlots. Before bounce d + kRingSlots reuses a slot, its counts
+// go to the statistics (the last bucket holds depth 63 and deeper) and it is
+// cleared.
+constexpr int kRingSlots = MC_MAX_DEPTH_STATS + 1;
+
+__global__ void k_recycle_slot(int* slot, int depth, long long* stats) {
+    if (threadIdx.x != 0) return;
+    const int b = min(depth, MC_MAX_DEPTH_STATS - 1);
+    stats[b] += slot[0];
+    stats[MC_MAX_DEPTH_STATS + b] += slot[1];
+    for (int k = 0; k < MC_COUNTERS_PER_DEPTH; k++) slot[k] = 0;
+}
+
+// The depths [lo, hi) still in the ring at the end of a deep wave.
+__global__ void k_accumulate_ring(const int* counters, int lo, int hi, long long* stats) {
+    if (threadIdx.x != 0) return;  // one thread: several depths share the last bucket
+    for (int d = lo; d < hi; d++) {
+        const int* c = counters + (d % kRingSlots) * MC_COUNTERS_PER_DEPTH;
+        const int b = min(d, MC_MAX_DEPTH_STATS - 1);
+        stats[b] += c[0];
+        stats[MC_MAX_DEPTH_STATS + b] += c[1];
+    }
+}
+
 __global__ void k_accumulate_counts(const int* counters, int maxDepth, long long* stats) {
     int d = threadIdx.x;
     if (d >= maxDepth || d >= MC_MAX_DEPTH_STATS) return;
@@ -1281,7 +1307,10 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     if ((st = ensure_wave(ctx, capacity)) != MC_OK) return st;
     if ((st = ensure_tables(ctx, capacity)) != MC_OK) return st;
     WaveBuffers& w = ctx->wave;
-    if (timeTrace || countVisits || guide) useGraph = false;
+    // deeper than the counter block: ring slots, a stop once a bounce has no
+    // paths left (read back every 8 bounces), no graph
+    const bool deep = maxD > MC_MAX_DEPTH_STATS;
+    if (timeTrace || countVisits || guide || deep) useGraph = false;
     cudaStream_t stream = ctx->stream;
     if (useGraph && !stream) {
         if (!ctx->own_stream) MC_CUDA(cudaStreamCreate(&ctx->own_stream));
@@ -1381,6 +1410,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         nee0[1] = guide->nee0 + capacity;
         nee0[2] = guide->nee0 + 2 * (size_t)capacity;
     }
+    auto slot = [&](int d) { return C + (deep ? d % kRingSlots : d) * MC_COUNTERS_PER_DEPTH; };
     auto enqueue_wave = [&]() -> mc_status {
         MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, stream));
         if (guide) {
@@ -1390,19 +1420,22 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         if (philox) k_camera<PhiloxRng><<<loopBlocks, 256, 0, stream>>>(ca);
         else k_camera<XorwowRng><<<loopBlocks, 256, 0, stream>>>(ca);
         launches++;
+        int dEnd = maxD;
+        bool stop = false;
         for (int d = 0; d <= maxD; d++) {
+            const bool last = d == maxD || stop;  // shadow rays of the previous bounce only
             TraceArgs t = ta;
-            if (d < maxD) {
+            if (!last) {
                 t.queue = w.queue[d & 1];
-                t.extCount = C + d * MC_COUNTERS_PER_DEPTH + 0;
+                t.extCount = slot(d) + 0;
             } else {
                 t.queue = nullptr;
                 t.extCount = nullptr;
                 t.extN = 0;
             }
-            if (d > 0) t.shCount = C + (d - 1) * MC_COUNTERS_PER_DEPTH + 1;
+            if (d > 0) t.shCount = slot(d - 1) + 1;
             else { t.shCount = nullptr; t.shN = 0; }
-            t.work = C + d * MC_COUNTERS_PER_DEPTH + 2;
+            t.work = slot(d) + 2;
             if (guide && d == 1) {
                 // the primary vertex's NEE lands apart from the sample so that
                 // its training records see only the light through the sampled direction
@@ -1420,20 +1453,29 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 else k_ratio_track<XorwowRng><<<loopBlocks, 256, 0, stream>>>(sa, r);
                 launches++;
             }
-            if (d == maxD) break;
+            if (last) {
+                dEnd = d;
+                break;
+            }
             if (guide) {
-                mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], C + d * MC_COUNTERS_PER_DEPTH + 0, capacity,
+                mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], slot(d) + 0, capacity,
                                                  w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.hits, guide->mixtures);
                 if (gs != MC_OK) return gs;
+                launches++;
+            }
+            if (deep && d + 1 >= kRingSlots) {
+                // slot(d + 1) still holds bounce d + 1 - kRingSlots (last read by its
+                // shadow rays' trace, long done): count it and clear it for shade(d)
+                k_recycle_slot<<<1, 32, 0, stream>>>(slot(d + 1), d + 1 - kRingSlots, ctx->d_stats);
                 launches++;
             }
             ShadeArgs sd = sa;
             sd.depth = d;
             sd.queue = w.queue[d & 1];
-            sd.count = C + d * MC_COUNTERS_PER_DEPTH + 0;
+            sd.count = slot(d) + 0;
             sd.nextQueue = w.queue[(d + 1) & 1];
-            sd.nextCount = C + (d + 1) * MC_COUNTERS_PER_DEPTH + 0;
-            sd.shCount = C + d * MC_COUNTERS_PER_DEPTH + 1;
+            sd.nextCount = slot(d + 1) + 0;
+            sd.shCount = slot(d) + 1;
             if (guide) {
                 sd.mix = guide->mixtures;
                 sd.guideFrac = guide->cfg.guide_fraction;
@@ -1445,6 +1487,13 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 k_shade<XorwowRng, false><<<shadeBlocks[1], 256, 0, stream>>>(sd);
             }
             launches++;
+            if (deep && (d & 7) == 7 && d + 1 < maxD) {
+                // no path continues: the next bounce traces the last shadow rays only
+                int next = 0;
+                MC_CUDA(cudaMemcpyAsync(&next, slot(d + 1), sizeof(int), cudaMemcpyDeviceToHost, stream));
+                MC_CUDA(cudaStreamSynchronize(stream));
+                stop = next == 0;
+            }
         }
         if (guide) {
             const long long entries = train ? (long long)waveR * wavePixels : 0;
@@ -1463,7 +1512,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         } else {
             k_finalize<<<loopBlocks, 256, 0, stream>>>(dtab, w.sr, w.sg, w.sb);
         }
-        k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
+        if (deep) k_accumulate_ring<<<1, 32, 0, stream>>>(C, std::max(0, dEnd - (kRingSlots - 1)), dEnd, ctx->d_stats);
+        else k_accumulate_counts<<<1, 64, 0, stream>>>(C, maxD, ctx->d_stats);
         launches += 2;
         if (guide && train) {
             // as many Adam steps per sample, on as many records each, as with
@@ -1597,7 +1647,7 @@ mc_status check_params(const mc_render_params* p, const mc_scene_view* v) {
     if (p->width <= 0 || p->height <= 0) return set_error(MC_ERR_INVALID, "render: width and height must be positive");
     if ((long long)p->width * p->height >= (1ll << 30)) return set_error(MC_ERR_INVALID, "render: too many pixels");
     if (p->spp < 0) return set_error(MC_ERR_INVALID, "render: spp must be >= 0");
-    if (p->max_depth < 0 || p->max_depth > MC_MAX_DEPTH_STATS) return set_error(MC_ERR_INVALID, "render: max_depth must be in [0, 64]");
+    if (p->max_depth < 0 || p->max_depth > MC_MAX_DEPTH) return set_error(MC_ERR_INVALID, "render: max_depth must be in [0, %d]", MC_MAX_DEPTH);
     if (p->rng != MC_RNG_PHILOX && p->rng != MC_RNG_XORWOW) return set_error(MC_ERR_INVALID, "render: unknown rng mode");
     if (p->intersector != MC_ISECT_REFERENCE && p->intersector != MC_ISECT_WATERTIGHT) return set_error(MC_ERR_INVALID, "render: unknown intersector");
     if (v->light_count > 0 && !v->lights) return set_error(MC_ERR_INVALID, "render: null light array");

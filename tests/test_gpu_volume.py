@@ -225,6 +225,34 @@ def test_constant_grid_equals_homogeneous_medium_in_expectation(ctx):
     mcpt.free_scene(grid)
 
 
+@pytest.mark.parametrize("grid", [True, False])
+def test_paths_deeper_than_the_counter_block(ctx, grid):
+    """Renders deeper than the 64 per-bounce counter slots (the cloud scene's
+    max_depth is 1000, PT:4166): a dense medium with roulette capped at 0.95
+    and max_depth 300 gives the reference's image and ray counts, and the
+    deepest statistics bucket (depth 63 and deeper) is reached."""
+    if grid:
+        s = gridded_spheres(ctx, scale=60.0)
+    else:
+        s = mcpt.generate_scene(mcpt.SCENE_CORNELL_SPHERES, seed=2)
+        mcpt.host_spheres(s)[1].mat.density = 40.0
+    sp = mcpt.host_spheres(s)[1]
+    sp.mat.albedo.color_a = mcpt.Vec3(1.0, 1.0, 1.0)
+    s.camera.rr_cap = 0.95
+    mine, st = render_mine(ctx, s, 128, 128, 2, 300, mcpt.RNG_PHILOX, layout=mcpt.LAYOUT_WIDE4)
+    ref, rs = render_ref(s, 128, 128, 2, 300, 2, philox=True)
+    frac = pixel_agreement(mine, ref)
+    print("deep (grid %s): pixel agreement %.6f, rays %d+%d (reference %d+%d), depth 63+ extend %d"
+          % (grid, frac, st.extend_rays, st.shadow_rays, rs[0], rs[1], st.extend_per_depth[63]))
+    assert st.error_flags == 0
+    assert frac >= 0.999
+    assert abs(st.extend_rays - rs[0]) <= 0.001 * rs[0]
+    assert st.extend_per_depth[63] > 0
+    assert st.extend_rays == sum(st.extend_per_depth[i] for i in range(64))
+    mcpt.free_scene(s)
+
+
+
 def test_release_grids(ctx):
     while _grids:
         mcpt.volume_grid_destroy(_grids.pop())
