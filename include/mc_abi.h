@@ -405,6 +405,14 @@ MC_API mc_status mc_volume_grid_destroy(const mc_volume_grid* d_grid);
  * and origin are returned. */
 MC_API mc_status mc_volume_fog_sphere(float radius, float voxel_size, float half_width, float* density_host,
                                       int32_t dims[3], float origin[3]);
+/* A dense grid file (the --volume file of the command-line driver): one
+ * text line "MCVOL nx ny nz voxel_size origin_x origin_y origin_z" and a
+ * newline, then nx*ny*nz little-endian float32 densities, x fastest.
+ * density_host NULL only reads the header. */
+MC_API mc_status mc_volume_file_read(const char* path, int32_t dims[3], float origin[3], float* voxel_size,
+                                     float* density_host);
+MC_API mc_status mc_volume_file_write(const char* path, const int32_t dims[3], const float origin[3], float voxel_size,
+                                      const float* density_host);
 /* Grid values at n world points (device, xyz packed) as the media sample them. */
 MC_API mc_status mc_volume_density(mc_context* ctx, const mc_volume_grid* d_grid, const float* d_points, int32_t n,
                                    float* d_out);
@@ -468,6 +476,11 @@ MC_API mc_status mc_obj_info_free(mc_obj_info* info);
 /* loadPpmAsRgba8 (PT:236-294): a binary PPM (P6, maximum 255) as RGBA8 with
  * alpha 255. rgba NULL only reads the size. */
 MC_API mc_status mc_ppm_read(const char* path, int32_t* width, int32_t* height, uint8_t* rgba);
+/* loadPfmAsRgba32f (PT:335-368): a little-endian colour PFM ("PF", negative
+ * scale) as float RGBA, top row first, alpha 1; the environment maps of
+ * --env. The header's four fields are whitespace-separated and exactly one
+ * byte follows them. rgba NULL only reads the size. */
+MC_API mc_status mc_pfm_read(const char* path, int32_t* width, int32_t* height, float* rgba);
 /* createImageTextureObject (PT:296-316): an RGBA8 image texture (sRGB,
  * bilinear, wrapped) for mc_texture.image; mc_image_texture_destroy frees it. */
 MC_API mc_status mc_image_texture_create(const uint8_t* rgba, int32_t width, int32_t height, uint64_t* texture);

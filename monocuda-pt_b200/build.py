@@ -44,7 +44,7 @@ UNITS = {
     "mc_volume.cu": ["-O3", "--use_fast_math"],
 }
 HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_image.cpp": ["-O2"],
-              "mc_obj.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"]}
+              "mc_obj.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_files.cpp": ["-O2"]}
 
 
 def headers():

@@ -9,10 +9,17 @@
 // flags; the image is resolved once after the last sample (mc_image_encode)
 // and written by the extension of --out: .png (the reference's output: tone
 // mapped, sRGB, 8-bit), .ppm (the same pixels), .pfm (linear radiance times
-// the exposure).
+// the exposure). --env / --env-intensity / --env-rotation load a PFM
+// environment map as the reference does (PT:4186-4221; its EXR/HDR readers
+// belong to image libraries this build does not include), --phase-g sets the
+// Henyey-Greenstein g of every medium (PT:4059, 2505-2508) and --volume fills
+// every medium with a dense density grid file (the reference's .nvdb grid,
+// PT:4066-4076, 2509-2520; see mc_volume_file_read). --pbrt and
+// --max-triangles (pbrt scene import) are refused.
 //
 // Exit status: 0 on success, 1 on a library error (message on stderr), 2 on a
 // usage error.
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -42,7 +49,16 @@ struct Options {
     bool stats = false;
     int tonemap = MC_TONEMAP_NONE;
     float exposure = 1.0f;  // <= 0: automatic
+    std::string envPath;
+    float envIntensity = 1.0f;
+    bool envIntensitySet = false;
+    float envRotationDegrees = 0.0f;
+    float phaseG = 0.0f;
+    bool phaseGSet = false;
+    std::string volumePath;
 };
+
+constexpr float kPi = 3.14159265358979323846f;
 
 const struct {
     const char* name;
@@ -60,6 +76,8 @@ void usage(FILE* f) {
                  "                [--rng philox|xorwow] [--watertight] [--graph]\n"
                  "                [--tonemap none|reinhard|aces] [--exposure X|auto]\n"
                  "                [--out FILE.png|FILE.ppm|FILE.pfm] [--stats]\n"
+                 "                [--env FILE.pfm] [--env-intensity X] [--env-rotation DEGREES] [--phase-g G]\n"
+                 "                [--volume FILE]\n"
                  "scenes:");
     for (const auto& s : kScenes) std::fprintf(f, " %s", s.name);
     std::fprintf(f, "\n");
@@ -129,6 +147,26 @@ bool parse(int argc, char** argv, Options& o) {
         } else if (!std::strcmp(a, "--out")) {
             if (!(v = next(a))) return false;
             o.out = v;
+        } else if (!std::strcmp(a, "--env")) {
+            if (!(v = next(a))) return false;
+            o.envPath = v;
+        } else if (!std::strcmp(a, "--env-intensity")) {
+            if (!(v = next(a))) return false;
+            o.envIntensity = (float)std::atof(v);
+            o.envIntensitySet = true;
+        } else if (!std::strcmp(a, "--env-rotation")) {
+            if (!(v = next(a))) return false;
+            o.envRotationDegrees = (float)std::atof(v);
+        } else if (!std::strcmp(a, "--phase-g")) {
+            if (!(v = next(a))) return false;
+            o.phaseG = (float)std::atof(v);
+            o.phaseGSet = true;
+        } else if (!std::strcmp(a, "--volume")) {
+            if (!(v = next(a))) return false;
+            o.volumePath = v;
+        } else if (!std::strcmp(a, "--pbrt") || !std::strcmp(a, "--max-triangles")) {
+            std::fprintf(stderr, "%s: pbrt scene import is not part of this build\n", a);
+            return false;
         } else {
             std::fprintf(stderr, "unknown argument '%s'\n", a);
             return false;
@@ -177,6 +215,33 @@ int main(int argc, char** argv) {
     }
     if (!o.wavefront)
         std::fprintf(stderr, "note: this library has only the wavefront path; rendering with it (the megakernel is not part of it)\n");
+    // the environment map and the grid are read before any device work
+    std::vector<float> envPixels;
+    int envW = 0, envH = 0;
+    if (!o.envPath.empty()) {
+        mc_status es = MC_OK;
+        if (!ends_with(o.envPath, ".pfm")) {
+            std::fprintf(stderr, "could not load environment map '%s': only PFM files are read (EXR and HDR need image "
+                                 "libraries this build does not include)\n", o.envPath.c_str());
+            return 1;
+        }
+        if ((es = mc_pfm_read(o.envPath.c_str(), &envW, &envH, nullptr)) == MC_OK) {
+            envPixels.resize((size_t)envW * envH * 4);
+            es = mc_pfm_read(o.envPath.c_str(), &envW, &envH, envPixels.data());
+        }
+        if (es != MC_OK) return fail("could not load environment map", es);
+    }
+    std::vector<float> density;
+    int32_t gridDims[3] = {0, 0, 0};
+    float gridOrigin[3] = {0, 0, 0}, voxel = 0.f;
+    if (!o.volumePath.empty()) {
+        mc_status vs = mc_volume_file_read(o.volumePath.c_str(), gridDims, gridOrigin, &voxel, nullptr);
+        if (vs == MC_OK) {
+            density.resize((size_t)gridDims[0] * gridDims[1] * gridDims[2]);
+            vs = mc_volume_file_read(o.volumePath.c_str(), gridDims, gridOrigin, &voxel, density.data());
+        }
+        if (vs != MC_OK) return fail("could not load volume", vs);
+    }
 
     mc_scene_desc desc = {};
     desc.kind = kind;
@@ -185,6 +250,18 @@ int main(int argc, char** argv) {
     mc_scene_host scene = {};
     mc_status st = mc_scene_generate(&desc, &scene);
     if (st != MC_OK) return fail("mc_scene_generate", st);
+    auto forEachMedium = [&](auto&& fn) {
+        int n = 0;
+        for (int i = 0; i < scene.sphere_count; i++)
+            if (scene.spheres[i].mat.type == MC_MAT_ISOTROPIC) fn(scene.spheres[i].mat), n++;
+        for (int i = 0; i < scene.triangle_count; i++)
+            if (scene.triangles[i].mat.type == MC_MAT_ISOTROPIC) fn(scene.triangles[i].mat), n++;
+        return n;
+    };
+    if (o.phaseGSet) {
+        const float g = std::fmin(std::fmax(o.phaseG, -0.99f), 0.99f);
+        forEachMedium([&](mc_material& m) { m.phase_g = g; });
+    }
 
     const int W = o.width > 0 ? o.width : scene.width;
     const int H = o.height > 0 ? o.height : (o.width > 0 ? (int)((long long)scene.height * W / scene.width) : scene.height);
@@ -201,10 +278,38 @@ int main(int argc, char** argv) {
         return fail("mc_context_create", st);
     }
     mc_env_map env = {};
-    if (scene.env_rgba && (st = mc_env_create(scene.env_rgba, scene.env_width, scene.env_height, scene.env_intensity, 0.f, &env)) != MC_OK) {
+    const float envRotation = o.envRotationDegrees * kPi / 180.0f;  // PT:4193
+    if (!envPixels.empty()) {
+        st = mc_env_create(envPixels.data(), envW, envH, o.envIntensity, envRotation, &env);
+        if (st == MC_OK)
+            std::printf("Environment map: %s (%dx%d), intensity %g, rotation %g deg\n", o.envPath.c_str(), envW, envH,
+                        o.envIntensity, o.envRotationDegrees);
+    } else if (scene.env_rgba) {
+        st = mc_env_create(scene.env_rgba, scene.env_width, scene.env_height,
+                           o.envIntensitySet ? o.envIntensity : scene.env_intensity, envRotation, &env);
+    }
+    if (st != MC_OK) {
         mc_context_destroy(ctx);
         mc_scene_free(&scene);
         return fail("mc_env_create", st);
+    }
+    const mc_volume_grid* grid = nullptr;
+    if (!density.empty()) {
+        mc_volume_grid header;
+        st = mc_volume_grid_create(ctx, density.data(), gridDims[0], gridDims[1], gridDims[2], gridOrigin, voxel, &grid,
+                                   &header);
+        if (st != MC_OK) {
+            mc_env_destroy(&env);
+            mc_context_destroy(ctx);
+            mc_scene_free(&scene);
+            return fail("mc_volume_grid_create", st);
+        }
+        const int media = forEachMedium([&](mc_material& m) {
+            m.density_grid = grid;
+            m.grid_max_density = header.maximum_density;
+        });
+        std::printf("volume '%s': %dx%dx%d voxels, maximum density %.3f, %d medium primitives\n", o.volumePath.c_str(),
+                    gridDims[0], gridDims[1], gridDims[2], header.maximum_density, media);
     }
 
     mc_render_params p = {};
@@ -268,6 +373,7 @@ int main(int argc, char** argv) {
         }
     }
     mc_env_destroy(&env);
+    mc_volume_grid_destroy(grid);
     mc_context_destroy(ctx);
     mc_scene_free(&scene);
     return rc;

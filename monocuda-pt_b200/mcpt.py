@@ -276,6 +276,9 @@ SIGNATURES = {
     "mc_volume_grid_destroy": (I32, [P]),
     "mc_volume_fog_sphere": (I32, [C.c_float, C.c_float, C.c_float, P, P, P]),
     "mc_volume_density": (I32, [P, P, P, I32, P]),
+    "mc_volume_file_read": (I32, [C.c_char_p, P, P, C.POINTER(C.c_float), P]),
+    "mc_volume_file_write": (I32, [C.c_char_p, P, P, C.c_float, P]),
+    "mc_pfm_read": (I32, [C.c_char_p, C.POINTER(I32), C.POINTER(I32), P]),
     "mc_server_get_stats": (I32, [P, C.POINTER(ServerStats)]),
     "mc_server_now": (C.c_double, [P]),
 }
@@ -566,6 +569,36 @@ def fog_sphere(radius, voxel_size, half_width=3.0):
     out = np.zeros((dims[2], dims[1], dims[0]), np.float32)
     check(lib.mc_volume_fog_sphere(radius, voxel_size, half_width, out.ctypes.data, dims, org))
     return out, tuple(org)
+
+
+def volume_file_write(path, density, origin, voxel_size):
+    """Writes a dense grid file (mc_volume_file_write): density (nz, ny, nx)."""
+    import numpy as np
+    d = np.ascontiguousarray(density, dtype=np.float32)
+    dims = (I32 * 3)(d.shape[2], d.shape[1], d.shape[0])
+    check(load().mc_volume_file_write(path.encode(), dims, (C.c_float * 3)(*origin), float(voxel_size), d.ctypes.data))
+
+
+def volume_file_read(path):
+    """A dense grid file: (density (nz, ny, nx) float32, origin, voxel size)."""
+    import numpy as np
+    lib = load()
+    dims, org, v = (I32 * 3)(), (C.c_float * 3)(), C.c_float()
+    check(lib.mc_volume_file_read(path.encode(), dims, org, C.byref(v), None))
+    out = np.zeros((dims[2], dims[1], dims[0]), np.float32)
+    check(lib.mc_volume_file_read(path.encode(), dims, org, C.byref(v), out.ctypes.data))
+    return out, tuple(org), v.value
+
+
+def pfm_read(path):
+    """A colour PFM as float RGBA (h, w, 4), top row first (mc_pfm_read)."""
+    import numpy as np
+    lib = load()
+    w, h = I32(), I32()
+    check(lib.mc_pfm_read(path.encode(), C.byref(w), C.byref(h), None))
+    out = np.zeros((h.value, w.value, 4), np.float32)
+    check(lib.mc_pfm_read(path.encode(), C.byref(w), C.byref(h), out.ctypes.data))
+    return out
 
 
 def volume_density(ctx, grid, d_points, n, d_out):

@@ -22,6 +22,7 @@ _SIGS = {
     "mcref_render": (I32, [P, I32, I32, I32, I32, I32, C.c_ulonglong, I32, I32, P, P]),
     "mcref_resolve": (I32, [P, I32, I32, I32, I32, C.c_float, I32, P, P, P]),
     "mcref_load_object": (I32, [C.c_char_p, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P, I32, P]),
+    "mcref_load_pfm": (I32, [C.c_char_p, P, P, P]),
 }
 _libs = {}
 

@@ -597,4 +597,16 @@ int mcref_load_object(const char* path, const mc_material* mat, float tx, float 
     return ok ? 0 : 3;
 }
 
+// loadPfmAsRgba32f (path_tracer.cu:335-368): 0 and the size (and, when rgba is
+// not NULL, the RGBA pixels) when the reference accepts the file, 3 when not.
+int mcref_load_pfm(const char* path, int* width, int* height, float* rgba) {
+    int w = 0, h = 0;
+    std::vector<float> pixels;
+    if (!loadPfmAsRgba32f(path, w, h, pixels)) return 3;
+    if (width) *width = w;
+    if (height) *height = h;
+    if (rgba) std::memcpy(rgba, pixels.data(), pixels.size() * sizeof(float));
+    return 0;
+}
+
 }  // extern "C"
