@@ -42,3 +42,24 @@ def test_fog_sphere_rejects_bad_arguments():
     org = (C.c_float * 3)()
     for r, h, b in ((0.0, 0.1, 3.0), (1.0, 0.0, 3.0), (1.0, 0.1, 0.0), (float("nan"), 0.1, 3.0), (1.0, 1e-5, 3.0)):
         assert lib.mc_volume_fog_sphere(r, h, b, None, dims, org) == 1
+
+
+def test_medium_flags_of_host_scenes():
+    """The flags DeviceScene derives on the host path, as ingestion reports
+    them: none, an isotropic medium, and one that carries a grid."""
+    boxes = mcpt.generate_scene(mcpt.SCENE_CORNELL_BOXES)
+    spheres = mcpt.generate_scene(mcpt.SCENE_CORNELL_SPHERES)
+    ico = mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=5)
+    f = mcpt._medium_flags
+    assert f(mcpt.host_triangles(boxes), boxes.triangle_count, mcpt.Triangle) == 0
+    sph = mcpt.host_spheres(spheres)
+    assert f(sph, spheres.sphere_count, mcpt.Sphere) == mcpt.MEDIUM_ANY
+    tris = mcpt.host_triangles(ico)
+    assert f(tris, ico.triangle_count, mcpt.Triangle) == mcpt.MEDIUM_ANY
+    sph[1].mat.density_grid = 0x1000  # any non-null pointer marks a grid; nothing is read through it here
+    assert f(sph, spheres.sphere_count, mcpt.Sphere) == mcpt.MEDIUM_ANY | mcpt.MEDIUM_GRID
+    sph[1].mat.density_grid = None
+    sph[0].mat.density_grid = 0x1000  # a grid on a non-medium material is ignored, as ingestion ignores it
+    assert f(sph, spheres.sphere_count, mcpt.Sphere) == mcpt.MEDIUM_ANY
+    for s in (boxes, spheres, ico):
+        mcpt.free_scene(s)
