@@ -447,6 +447,15 @@ typedef struct mc_scene_host {
 } mc_scene_host;
 
 MC_API mc_status mc_scene_generate(const mc_scene_desc* desc, mc_scene_host* out);
+/* The reference's cloud scene (buildCloudScene PT:1849-1891 and main()'s
+ * cloud camera PT:4148-4167) around a density grid: an isotropic sphere
+ * enclosing the grid's bounds (albedo 1, density scale 4, g 0.877, carrying
+ * d_grid and header->maximum_density), a ground quad 1000 below, and with
+ * sun != 0 (the reference's choice without --env) a far emissive quad in
+ * the sun's direction; 333x180, 500 spp, max depth 1000, roulette cap 0.95,
+ * the Mitsuba sensor. d_grid: from mc_volume_grid_create; header: its header. */
+MC_API mc_status mc_scene_cloud(const mc_volume_grid* d_grid, const mc_volume_grid* header, int32_t sun,
+                                mc_scene_host* out);
 MC_API mc_status mc_scene_free(mc_scene_host* scene);
 
 /* OBJ/MTL loading: loadObject (PT:2644-2859) with loadMtlFile (PT:2614-2680).

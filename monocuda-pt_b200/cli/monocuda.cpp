@@ -80,7 +80,7 @@ void usage(FILE* f) {
                  "                [--volume FILE]\n"
                  "scenes:");
     for (const auto& s : kScenes) std::fprintf(f, " %s", s.name);
-    std::fprintf(f, "\n");
+    std::fprintf(f, " cloud (with --volume)\n");
 }
 
 bool parse(int argc, char** argv, Options& o) {
@@ -208,7 +208,7 @@ int main(int argc, char** argv) {
     int kind = 0;
     for (const auto& s : kScenes)
         if (o.scene == s.name) kind = s.kind;
-    if (!kind) {
+    if (!kind && o.scene != "cloud") {
         std::fprintf(stderr, "unknown scene '%s'\n", o.scene.c_str());
         usage(stderr);
         return 2;
@@ -243,13 +243,44 @@ int main(int argc, char** argv) {
         if (vs != MC_OK) return fail("could not load volume", vs);
     }
 
-    mc_scene_desc desc = {};
-    desc.kind = kind;
-    desc.variant = o.variant;
-    desc.seed = o.sceneSeed;
+    // the cloud scene is built around the grid (buildCloudScene, PT:1849-1891)
+    const bool cloud = o.scene == "cloud";
+    if (cloud && density.empty()) {
+        std::fprintf(stderr, "the cloud scene needs a density grid: pass one with --volume FILE\n");
+        return 1;
+    }
+    mc_status st = MC_OK;
+    mc_context* ctx = nullptr;
+    if ((st = mc_context_create(0, &ctx)) != MC_OK) return fail("mc_context_create", st);
+    const mc_volume_grid* grid = nullptr;
+    mc_volume_grid header = {};
     mc_scene_host scene = {};
-    mc_status st = mc_scene_generate(&desc, &scene);
-    if (st != MC_OK) return fail("mc_scene_generate", st);
+    mc_env_map env = {};
+    auto cleanup = [&]() {
+        mc_env_destroy(&env);
+        mc_volume_grid_destroy(grid);
+        mc_context_destroy(ctx);
+        mc_scene_free(&scene);
+    };
+    if (!density.empty() &&
+        (st = mc_volume_grid_create(ctx, density.data(), gridDims[0], gridDims[1], gridDims[2], gridOrigin, voxel, &grid,
+                                    &header)) != MC_OK) {
+        cleanup();
+        return fail("mc_volume_grid_create", st);
+    }
+    if (cloud) {
+        st = mc_scene_cloud(grid, &header, envPixels.empty() ? 1 : 0, &scene);  // the sun quad without --env
+    } else {
+        mc_scene_desc desc = {};
+        desc.kind = kind;
+        desc.variant = o.variant;
+        desc.seed = o.sceneSeed;
+        st = mc_scene_generate(&desc, &scene);
+    }
+    if (st != MC_OK) {
+        cleanup();
+        return fail(cloud ? "mc_scene_cloud" : "mc_scene_generate", st);
+    }
     auto forEachMedium = [&](auto&& fn) {
         int n = 0;
         for (int i = 0; i < scene.sphere_count; i++)
@@ -262,6 +293,15 @@ int main(int argc, char** argv) {
         const float g = std::fmin(std::fmax(o.phaseG, -0.99f), 0.99f);
         forEachMedium([&](mc_material& m) { m.phase_g = g; });
     }
+    if (grid) {
+        // every medium takes the grid (PT:2509-2520)
+        const int media = forEachMedium([&](mc_material& m) {
+            m.density_grid = grid;
+            m.grid_max_density = header.maximum_density;
+        });
+        std::printf("volume '%s': %dx%dx%d voxels, maximum density %.3f, %d medium primitives\n", o.volumePath.c_str(),
+                    gridDims[0], gridDims[1], gridDims[2], header.maximum_density, media);
+    }
 
     const int W = o.width > 0 ? o.width : scene.width;
     const int H = o.height > 0 ? o.height : (o.width > 0 ? (int)((long long)scene.height * W / scene.width) : scene.height);
@@ -269,15 +309,11 @@ int main(int argc, char** argv) {
     if (W != scene.width || H != scene.height) {
         cam.image_width = W;
         cam.aspect_ratio = (float)W / (float)H;
-        if ((st = mc_camera_initialize(&cam)) != MC_OK) return fail("mc_camera_initialize", st);
+        if ((st = mc_camera_initialize(&cam)) != MC_OK) {
+            cleanup();
+            return fail("mc_camera_initialize", st);
+        }
     }
-
-    mc_context* ctx = nullptr;
-    if ((st = mc_context_create(0, &ctx)) != MC_OK) {
-        mc_scene_free(&scene);
-        return fail("mc_context_create", st);
-    }
-    mc_env_map env = {};
     const float envRotation = o.envRotationDegrees * kPi / 180.0f;  // PT:4193
     if (!envPixels.empty()) {
         st = mc_env_create(envPixels.data(), envW, envH, o.envIntensity, envRotation, &env);
@@ -289,27 +325,8 @@ int main(int argc, char** argv) {
                            o.envIntensitySet ? o.envIntensity : scene.env_intensity, envRotation, &env);
     }
     if (st != MC_OK) {
-        mc_context_destroy(ctx);
-        mc_scene_free(&scene);
+        cleanup();
         return fail("mc_env_create", st);
-    }
-    const mc_volume_grid* grid = nullptr;
-    if (!density.empty()) {
-        mc_volume_grid header;
-        st = mc_volume_grid_create(ctx, density.data(), gridDims[0], gridDims[1], gridDims[2], gridOrigin, voxel, &grid,
-                                   &header);
-        if (st != MC_OK) {
-            mc_env_destroy(&env);
-            mc_context_destroy(ctx);
-            mc_scene_free(&scene);
-            return fail("mc_volume_grid_create", st);
-        }
-        const int media = forEachMedium([&](mc_material& m) {
-            m.density_grid = grid;
-            m.grid_max_density = header.maximum_density;
-        });
-        std::printf("volume '%s': %dx%dx%d voxels, maximum density %.3f, %d medium primitives\n", o.volumePath.c_str(),
-                    gridDims[0], gridDims[1], gridDims[2], header.maximum_density, media);
     }
 
     mc_render_params p = {};
@@ -372,9 +389,6 @@ int main(int argc, char** argv) {
             }
         }
     }
-    mc_env_destroy(&env);
-    mc_volume_grid_destroy(grid);
-    mc_context_destroy(ctx);
-    mc_scene_free(&scene);
+    cleanup();
     return rc;
 }

@@ -567,6 +567,75 @@ mc_status mc_split_triangles_host(const mc_triangle* tris, int32_t n, mc_triangl
     return MC_OK;
 }
 
+mc_status mc_scene_cloud(const mc_volume_grid* d_grid, const mc_volume_grid* header, int32_t sun, mc_scene_host* out) {
+    if (!d_grid || !header || !out) return mc::set_error(MC_ERR_INVALID, "mc_scene_cloud: null argument");
+    std::memset(out, 0, sizeof(*out));
+    const HV gmin(header->world_min[0], header->world_min[1], header->world_min[2]);
+    const HV gmax(header->world_max[0], header->world_max[1], header->world_max[2]);
+    const HV center = (gmin + gmax) * 0.5f;
+    const float radius = (gmax - gmin).length() * 0.5f;
+    if (!(radius > 0.f)) return mc::set_error(MC_ERR_INVALID, "mc_scene_cloud: the grid has no extent");
+    std::vector<mc_triangle> tris;
+    std::vector<mc_sphere> sph;
+    // PT:1863-1866: an isotropic sphere around the grid (density scale 4,
+    // Henyey-Greenstein g 0.877, PT:1721-1722); the grid goes into every
+    // medium's material as main() does (PT:2509-2520)
+    mc_material cloud = make_isotropic(HV(1.f, 1.f, 1.f), 4.0f, 0.877f);
+    cloud.density_grid = d_grid;
+    cloud.grid_max_density = header->maximum_density;
+    sph.push_back(make_sphere(center, center, false, radius, cloud));
+    sph.back().center1 = mc_vec3{0.f, 0.f, 0.f};  // a stationary sphere's unused second centre, as the reference leaves it
+    // PT:1868-1872: the ground that lights the cloud's underside
+    const float extent = 20000.f, height = -1000.f;
+    add_quad(tris, HV(-extent, height, -extent), HV(extent, height, -extent), HV(extent, height, extent),
+             HV(-extent, height, extent), make_lambertian(HV(0.2f, 0.2f, 0.2f)));
+    if (sun) {
+        // PT:1874-1891: the directional sun as a far quad of matching irradiance
+        // (E = L * area / distance^2)
+        const HV toSun = -HV(-0.5826f, -0.7660f, -0.2717f);
+        const float distance = 8.f * radius;
+        const float half = 0.1f * distance;
+        const float scale = (distance * distance) / (4.f * half * half);
+        const mc_material light = make_emissive(HV(2.6f, 2.5f, 2.3f) * scale);
+        const HV c = center + toSun * distance;
+        const HV helper = (std::fabs(toSun.x) > 0.9f) ? HV(0.f, 1.f, 0.f) : HV(1.f, 0.f, 0.f);
+        const HV tangent = helper.cross(toSun).normalize() * half;
+        const HV bitangent = toSun.cross(tangent.normalize()) * half;
+        add_quad(tris, c - tangent - bitangent, c + tangent - bitangent, c + tangent + bitangent, c - tangent + bitangent,
+                 light);
+    }
+    // main()'s film and camera for the cloud (PT:4080-4084, 4113-4126, 4148-4167):
+    // the Mitsuba sensor, its horizontal field of view turned vertical, deep paths
+    const int W = 333, H = 180;
+    const float pi = 3.14159265358979323846f;
+    const float hfov = 54.43f * pi / 180.f;
+    const float aspect = (float)W / (float)H;
+    const HV from(648.064f, -82.473f, -63.856f), at(6.021f, 100.043f, -43.679f);
+    set_camera(out->camera, W, H, from, at, 2.f * std::atan(std::tan(hfov * 0.5f) / aspect) * 180.f / pi,
+               (at - from).length(), 1000, 500);
+    out->camera.up = mc_vec3{0.273f, 0.962f, -0.009f};
+    out->camera.background = mc_vec3{0.03f, 0.07f, 0.23f};
+    out->camera.rr_cap = 0.95f;
+    mc_camera_initialize(&out->camera);
+    out->width = W;
+    out->height = H;
+    out->spp = 500;
+    out->max_depth = 1000;
+    out->has_medium = MC_MEDIUM_ANY | MC_MEDIUM_GRID;
+    mc_scene_finalize_host(tris.data(), (int32_t)tris.size(), nullptr, nullptr);
+    out->triangle_count = (int32_t)tris.size();
+    out->triangles = (mc_triangle*)std::malloc(sizeof(mc_triangle) * tris.size());
+    out->sphere_count = (int32_t)sph.size();
+    out->spheres = (mc_sphere*)std::malloc(sizeof(mc_sphere) * sph.size());
+    if (!out->triangles || !out->spheres) {
+        mc_scene_free(out);
+        return mc::set_error(MC_ERR_OOM, "mc_scene_cloud: host allocation failed");
+    }
+    std::memcpy(out->triangles, tris.data(), sizeof(mc_triangle) * tris.size());
+    std::memcpy(out->spheres, sph.data(), sizeof(mc_sphere) * sph.size());
+    return MC_OK;
+}
+
 mc_status mc_scene_generate(const mc_scene_desc* desc, mc_scene_host* out) {
     if (!desc || !out) return mc::set_error(MC_ERR_INVALID, "mc_scene_generate: null argument");
     std::memset(out, 0, sizeof(*out));

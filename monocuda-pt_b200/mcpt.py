@@ -279,6 +279,7 @@ SIGNATURES = {
     "mc_volume_file_read": (I32, [C.c_char_p, P, P, C.POINTER(C.c_float), P]),
     "mc_volume_file_write": (I32, [C.c_char_p, P, P, C.c_float, P]),
     "mc_pfm_read": (I32, [C.c_char_p, C.POINTER(I32), C.POINTER(I32), P]),
+    "mc_scene_cloud": (I32, [P, C.POINTER(VolumeGrid), I32, C.POINTER(SceneHost)]),
     "mc_server_get_stats": (I32, [P, C.POINTER(ServerStats)]),
     "mc_server_now": (C.c_double, [P]),
 }

@@ -597,6 +597,34 @@ int mcref_load_object(const char* path, const mc_material* mat, float tx, float 
     return ok ? 0 : 3;
 }
 
+// setup_scene(SceneChoice::Cloud) (path_tracer.cu:2486-2524, buildCloudScene
+// 1849-1891) for a grid with these world bounds and maximum, as main() leaves
+// the globals after loading one (4066-4076): grid_pointer is only stored in
+// the medium's material. sun != 0: no --env (the sun quad is built). Copies
+// up to the capacities out; returns 0, or 3 when the scene is empty.
+int mcref_cloud_scene(const float* world_min, const float* world_max, float maximum, unsigned long long grid_pointer,
+                      int sun, mc_triangle* tris, int tri_capacity, int* tri_count, mc_sphere* spheres,
+                      int sphere_capacity, int* sphere_count) {
+    QuietStdout quiet;
+    for (int a = 0; a < 3; a++) {
+        g_volumeGrid.worldMinimum[a] = world_min[a];
+        g_volumeGrid.worldMaximum[a] = world_max[a];
+    }
+    g_volumeGrid.maximumDensity = maximum;
+    g_volumeDeviceGrid = reinterpret_cast<const nanovdb::FloatGrid*>(grid_pointer);
+    g_environmentEnabled = sun == 0;
+    g_phaseGWasSet = false;
+    hostScene scene = setup_scene(SceneChoice::Cloud);
+    g_volumeDeviceGrid = nullptr;
+    g_environmentEnabled = false;
+    const int nt = (int)scene.triangles.size(), ns = (int)scene.spheres.size();
+    if (tri_count) *tri_count = nt;
+    if (sphere_count) *sphere_count = ns;
+    for (int i = 0; i < nt && i < tri_capacity; i++) std::memcpy(&tris[i], &scene.triangles[i], sizeof(triangle));
+    for (int i = 0; i < ns && i < sphere_capacity; i++) std::memcpy(&spheres[i], &scene.spheres[i], sizeof(sphere));
+    return nt + ns > 0 ? 0 : 3;
+}
+
 // loadPfmAsRgba32f (path_tracer.cu:335-368): 0 and the size (and, when rgba is
 // not NULL, the RGBA pixels) when the reference accepts the file, 3 when not.
 int mcref_load_pfm(const char* path, int* width, int* height, float* rgba) {

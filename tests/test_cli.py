@@ -181,3 +181,19 @@ def test_cli_volume_and_phase_g_equal_library_render(tmp_path):
     mcpt.free_scene(s)
     assert st.error_flags == 0
     np.testing.assert_allclose(img.reshape(-1), acc / np.float32(2), rtol=4e-7, atol=0)
+
+
+@pytest.mark.gpu
+def test_cli_cloud_scene(tmp_path):
+    """--scene cloud --volume FILE: the reference's cloud set-up around the
+    grid renders (deep paths, roulette cap 0.95)."""
+    d, org = mcpt.fog_sphere(60.0, 4.0)
+    path = os.path.join(tmp_path, "cloud.mcvol")
+    mcpt.volume_file_write(path, d, tuple(np.asarray(org, np.float32) + np.float32([0, 100, -40])), 4.0)
+    out = os.path.join(tmp_path, "cloud.pfm")
+    r = _run("--wavefront", "--persistent", "--scene", "cloud", "--volume", path, "--width", "96", "--spp", "1",
+             "--out", out)
+    assert r.returncode == 0, r.stderr
+    assert "1 medium primitives" in r.stdout and "depth 1000" in r.stdout
+    img = _read_pfm(out)
+    assert img.shape == (51, 96, 3) and np.isfinite(img).all() and float(img.mean()) > 0

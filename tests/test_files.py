@@ -123,5 +123,7 @@ def test_cli_refuses_what_it_cannot_read(tmp_path):
     assert r.returncode == 1 and "big-endian" in r.stderr
     r = _run("--wavefront", "--volume", os.path.join(tmp_path, "missing.mcvol"))
     assert r.returncode == 1 and "volume" in r.stderr
+    r = _run("--wavefront", "--scene", "cloud")
+    assert r.returncode == 1 and "needs a density grid" in r.stderr
     r = _run("--help")
     assert r.returncode == 0 and "--env" in r.stdout and "--phase-g" in r.stdout and "--volume" in r.stdout

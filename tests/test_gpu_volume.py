@@ -253,6 +253,36 @@ def test_paths_deeper_than_the_counter_block(ctx, grid):
 
 
 
+def _fog_cloud(ctx, radius=60.0, voxel=4.0, centre=(0.0, 100.0, -40.0)):
+    d, org = mcpt.fog_sphere(radius, voxel)
+    g, h = mcpt.volume_grid_create(ctx, d, tuple(np.asarray(org, np.float32) + np.asarray(centre, np.float32)), voxel)
+    _grids.append(g)
+    return g, h
+
+
+def test_cloud_scene_image_parity(ctx):
+    """The reference's cloud scene (mc_scene_cloud: enclosing medium sphere,
+    ground, sun quad, the Mitsuba camera, max depth 1000, roulette cap 0.95)
+    around a fog-sphere grid: image and ray counts equal the reference's
+    render of the same primitives and grid."""
+    g, h = _fog_cloud(ctx)
+    s = mcpt.SceneHost()
+    mcpt.check(ctx.lib.mc_scene_cloud(g, C.byref(h), 1, C.byref(s)))
+    assert s.max_depth == 1000 and s.camera.rr_cap == np.float32(0.95)
+    W = 96
+    H = 180 * W // 333
+    mine, st = render_mine(ctx, s, W, H, 2, s.max_depth, mcpt.RNG_PHILOX, layout=mcpt.LAYOUT_WIDE4)
+    ref, rs = render_ref(s, W, H, 2, s.max_depth, 2, philox=True)
+    frac = pixel_agreement(mine, ref)
+    print("cloud: pixel agreement %.6f, rays %d+%d (reference %d+%d), depth 63+ extend %d, mean %.4f"
+          % (frac, st.extend_rays, st.shadow_rays, rs[0], rs[1], st.extend_per_depth[63], float(mine.mean())))
+    assert st.error_flags == 0 and float(mine.mean()) > 0
+    assert frac >= 0.999
+    assert abs(st.extend_rays - rs[0]) <= 0.001 * rs[0]
+    mcpt.free_scene(s)
+
+
+
 def test_release_grids(ctx):
     while _grids:
         mcpt.volume_grid_destroy(_grids.pop())

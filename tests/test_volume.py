@@ -4,6 +4,7 @@ it, the grid header's layout, and argument checks."""
 import ctypes as C
 
 import numpy as np
+import pytest
 
 import mcpt
 
@@ -63,3 +64,57 @@ def test_medium_flags_of_host_scenes():
     assert f(sph, spheres.sphere_count, mcpt.Sphere) == mcpt.MEDIUM_ANY
     for s in (boxes, spheres, ico):
         mcpt.free_scene(s)
+
+
+def _mat(m):
+    return (bytes(C.c_int32(m.type)) + bytes(C.c_int32(m.albedo.type)) + bytes(m.albedo.color_a) + bytes(m.albedo.color_b)
+            + bytes(C.c_float(m.albedo.scale)) + bytes(C.c_uint64(m.albedo.image)) + bytes(m.emitted)
+            + bytes(C.c_float(m.fuzz)) + bytes(C.c_float(m.refraction_index)) + bytes(C.c_float(m.density))
+            + bytes(C.c_float(m.phase_g)) + bytes(C.c_uint64(m.density_grid or 0)) + bytes(C.c_float(m.grid_max_density)))
+
+
+def _box(b):
+    return bytes(b.lo) + bytes(b.hi)
+
+
+@pytest.mark.parametrize("sun", [1, 0])
+def test_cloud_scene_matches_reference(sun):
+    """mc_scene_cloud against the reference's own setup_scene(Cloud)
+    (buildCloudScene and the grid-material loop, then finalizeScene), run from
+    oracle/_ref with the same grid bounds, maximum and grid pointer (only
+    stored, never read): every triangle and sphere field equal, and main()'s
+    cloud film and camera settings."""
+    import mcref
+    h = mcpt.VolumeGrid()
+    wmin, wmax = (-120.5, 10.25, -80.0), (130.75, 190.5, 60.125)
+    for a in range(3):
+        h.world_min[a], h.world_max[a] = wmin[a], wmax[a]
+    h.maximum_density = 0.873
+    grid = 0x7F00  # a stand-in device pointer: the scene only carries it
+    s = mcpt.SceneHost()
+    mcpt.check(mcpt.load().mc_scene_cloud(grid, C.byref(h), sun, C.byref(s)))
+    tris = (mcpt.Triangle * 8)()
+    sph = (mcpt.Sphere * 4)()
+    nt, ns = C.c_int32(), C.c_int32()
+    rc = mcref.load(False).mcref_cloud_scene((C.c_float * 3)(*wmin), (C.c_float * 3)(*wmax), 0.873, grid, sun,
+                                             C.addressof(tris), 8, C.byref(nt), C.addressof(sph), 4, C.byref(ns))
+    assert rc == 0 and (s.triangle_count, s.sphere_count) == (nt.value, ns.value) == (4 if sun else 2, 1)
+    mine_t, mine_s = mcpt.host_triangles(s), mcpt.host_spheres(s)
+    for i in range(nt.value):
+        assert bytes(mine_t[i])[:96] == bytes(tris[i])[:96]
+        assert _mat(mine_t[i].mat) == _mat(tris[i].mat) and _box(mine_t[i].aabb) == _box(tris[i].aabb)
+    a, b = mine_s[0], sph[0]
+    assert bytes(a.center) + bytes(a.center1) + bytes(C.c_float(a.radius)) == \
+        bytes(b.center) + bytes(b.center1) + bytes(C.c_float(b.radius))
+    assert a.is_moving == b.is_moving and _mat(a.mat) == _mat(b.mat) and _box(a.aabb) == _box(b.aabb)
+    assert a.mat.density_grid == grid and a.mat.grid_max_density == np.float32(0.873)
+    # main()'s cloud settings (PT:4080-4084, 4148-4167)
+    f32 = np.float32
+    hfov = f32(54.43) * f32(np.pi) / f32(180)
+    vfov = f32(2) * np.arctan(np.tan(hfov * f32(0.5)) / (f32(333) / f32(180))) * f32(180) / f32(np.pi)
+    assert (s.width, s.height, s.spp, s.max_depth) == (333, 180, 500, 1000)
+    assert abs(s.camera.vfov - vfov) <= 1e-5 * vfov
+    assert s.camera.rr_cap == f32(0.95) and tuple(s.camera.up.__getattribute__(k) for k in "xyz") == \
+        tuple(f32(v) for v in (0.273, 0.962, -0.009))
+    assert s.has_medium == mcpt.MEDIUM_ANY | mcpt.MEDIUM_GRID
+    mcpt.free_scene(s)
