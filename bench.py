@@ -35,7 +35,8 @@ WORKLOAD = {"workload": "displaced_icospheres", "triangles": 3932176, "width": 1
             "rng": "philox4x32-10 per (pixel, sample)", "l2": "inputs larger than L2 (BVH 252 MB + triangles 189 MB)"}
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "k_trace_displaced_icospheres.txt")
-# algorithmic bytes (roofline): node visit, primitive test, extend-ray I/O, shadow-ray I/O
+# algorithmic bytes per unit of the trace kernel: node visit (64 B binary / 128 B wide, scaled below),
+# primitive test (48 B hot record), extend-ray I/O (ray in, hit out), shadow-ray I/O (entry, time, sample update)
 NODE_BYTES, LEAF_BYTES, EXT_IO_BYTES, SHADOW_IO_BYTES = 64, 48, 48, 72
 INGEST_BYTES = 224 + 36 + 192  # per triangle: AoS record read, hot and cold records written
 

@@ -428,7 +428,7 @@ def test_megakernel_reference_agrees_with_wavefront(ctx):
 
 def test_plain_and_persistent_wavefront_identical(ctx):
     """The reference claims persistent and plain wavefront images are
-    byte-identical (README.md:23, 136); the same holds here."""
+    byte-identical (the reference project's README.md:23, 136); the same holds here."""
     s = scene(SPHERES, 0)
     a, _ = render_mine(ctx, s, 192, 192, 2, 8, mcpt.RNG_PHILOX, persistent=True, layout=mcpt.LAYOUT_WIDE4)
     b, _ = render_mine(ctx, s, 192, 192, 2, 8, mcpt.RNG_PHILOX, persistent=False, layout=mcpt.LAYOUT_WIDE4)
