@@ -457,6 +457,8 @@ struct MatInfo {
 template <class T>
 void hit_geometry(const Scene& S, int type, int prim, const V<T>& o, const V<T>& d, T t, T time, V<T>& p, V<T>& normal,
                   bool& front, V<T>& albedo, const mc_material*& mat) {
+    const T PI = (T)kPiD;
+    T u = T(0), v = T(0);  // texture coordinates of the hit
     p = o + d * t;
     if (type == 0) {
         const mc_sphere& s = S.sph[prim];
@@ -465,6 +467,9 @@ void hit_geometry(const Scene& S, int type, int prim, const V<T>& o, const V<T>&
         front = d.dot(ow) < T(0);
         normal = front ? ow : -ow;
         mat = &s.mat;
+        // PT:1505-1507 computeSphereUvFromOutwardNormal
+        u = (std::atan2(-ow.z, ow.x) + PI) / (T(2) * PI);
+        v = std::acos(std::fmin(T(1), std::fmax(T(-1), -ow.y))) / PI;
     } else {
         const mc_triangle& tr = S.tris[prim];
         V<T> v0 = vin<T>(tr.v0), v1 = vin<T>(tr.v1), v2 = vin<T>(tr.v2);
@@ -486,9 +491,21 @@ void hit_geometry(const Scene& S, int type, int prim, const V<T>& o, const V<T>&
         }
         normal = front ? sn : -sn;
         mat = &tr.mat;
+        // PT:687-695 computeTriangleUvFromHitPoint: area weights of the hit point
+        const T a2 = (v1 - v0).cross(v2 - v0).len();
+        const T w0 = (v1 - p).cross(v2 - p).len() / a2, w1 = (v0 - p).cross(v2 - p).len() / a2,
+                w2 = (v1 - p).cross(v0 - p).len() / a2;
+        u = (T)tr.uv0.x * w0 + (T)tr.uv1.x * w1 + (T)tr.uv2.x * w2;
+        v = (T)tr.uv0.y * w0 + (T)tr.uv1.y * w1 + (T)tr.uv2.y * w2;
     }
-    // only solid textures are produced by the scenes the oracle checks
-    albedo = vin<T>(mat->albedo.color_a);
+    // PT:216-234 sampleTexture: solid, or a checker of (u, v) cells; image
+    // textures are sampled by the GPU texture unit and are not restated here
+    const mc_texture& tex = mat->albedo;
+    albedo = vin<T>(tex.color_a);
+    if (tex.type == MC_TEX_CHECKER) {
+        const long long iu = (long long)std::floor(u * (T)tex.scale), iv = (long long)std::floor(v * (T)tex.scale);
+        if (((iu + iv) & 1) != 0) albedo = vin<T>(tex.color_b);
+    }
 }
 
 // mediumTransmittance (PT:2874-2898), homogeneous media only
