@@ -23,6 +23,7 @@ _SIGS = {
     "mcref_resolve": (I32, [P, I32, I32, I32, I32, C.c_float, I32, P, P, P]),
     "mcref_load_object": (I32, [C.c_char_p, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P, I32, P]),
     "mcref_load_pfm": (I32, [C.c_char_p, P, P, P]),
+    "mcref_grid_sample": (I32, [P, P, I32, P]),
     "mcref_cloud_scene": (I32, [P, P, C.c_float, C.c_uint64, I32, P, I32, P, P, I32, P]),
 }
 _libs = {}

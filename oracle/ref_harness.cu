@@ -625,6 +625,19 @@ int mcref_cloud_scene(const float* world_min, const float* world_max, float maxi
     return nt + ns > 0 ? 0 : 3;
 }
 
+// The grid reading of sampleVolumeDensity (path_tracer.cu:784-789: world to
+// index, accessor, order-1 sampler) through the nanovdb stand-in, on the host:
+// grid_bytes is a host copy of a grid (64-byte header, then the voxels).
+int mcref_grid_sample(const void* grid_bytes, const float* points, int n, float* out) {
+    const nanovdb::FloatGrid* grid = reinterpret_cast<const nanovdb::FloatGrid*>(grid_bytes);
+    for (int i = 0; i < n; i++) {
+        const nanovdb::Vec3f index = grid->worldToIndexF(nanovdb::Vec3f(points[3 * i], points[3 * i + 1], points[3 * i + 2]));
+        auto accessor = grid->tree().getAccessor();
+        out[i] = nanovdb::math::createSampler<1>(accessor)(index);
+    }
+    return 0;
+}
+
 // loadPfmAsRgba32f (path_tracer.cu:335-368): 0 and the size (and, when rgba is
 // not NULL, the RGBA pixels) when the reference accepts the file, 3 when not.
 int mcref_load_pfm(const char* path, int* width, int* height, float* rgba) {

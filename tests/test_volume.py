@@ -118,3 +118,46 @@ def test_cloud_scene_matches_reference(sun):
         tuple(f32(v) for v in (0.273, 0.962, -0.009))
     assert s.has_medium == mcpt.MEDIUM_ANY | mcpt.MEDIUM_GRID
     mcpt.free_scene(s)
+
+
+def test_oracle_grid_stand_in_reads_as_the_trilinear_restatement():
+    """The oracle's nanovdb stand-in (the grid the reference's trackers read in
+    the parity tests), called on the host through the reference's call chain
+    (PT:784-789), against a float64 restatement of the trilinear reading:
+    index point (p - origin) * (1 / voxel) in float32, 8 voxels around its floor
+    (0 outside), along z, then y, then x."""
+    import mcref
+    rng = np.random.default_rng(2)
+    nx, ny, nz = 9, 6, 7
+    d = rng.random((nz, ny, nx)).astype(np.float32) * 3
+    h = mcpt.VolumeGrid()
+    org = np.float32([-0.4, 0.25, 1.0])
+    voxel = np.float32(0.13)
+    for a in range(3):
+        h.origin[a] = org[a]
+    h.voxel_size = voxel
+    h.inv_voxel_size = np.float32(1) / voxel
+    h.dims[0], h.dims[1], h.dims[2] = nx, ny, nz
+    h.maximum_density = d.max()
+    blob = np.frombuffer(bytes(h) + d.tobytes(), np.uint8).copy()
+    pts = rng.uniform(org - 0.3, org + voxel * np.float32([nx, ny, nz]) + 0.3, (20000, 3)).astype(np.float32)
+    pts[:200] = org + voxel * rng.integers(-1, 10, (200, 3)).astype(np.float32)
+    out = np.zeros(len(pts), np.float32)
+    assert mcref.load(False).mcref_grid_sample(blob.ctypes.data, pts.ctypes.data, len(pts), out.ctypes.data) == 0
+    x = ((pts - org) * h.inv_voxel_size).astype(np.float64)
+    f = np.floor(x)
+    i = f.astype(np.int64)
+    u = x - f
+
+    def at(a, b, c):
+        ok = (a >= 0) & (b >= 0) & (c >= 0) & (a < nx) & (b < ny) & (c < nz)
+        v = np.zeros(len(a))
+        v[ok] = d[c[ok], b[ok], a[ok]]
+        return v
+
+    def lerp(a, b, w):
+        return a + w * (b - a)
+    ix, iy, iz = i[:, 0], i[:, 1], i[:, 2]
+    zs = [lerp(at(ix + a, iy + b, iz), at(ix + a, iy + b, iz + 1), u[:, 2]) for a in (0, 1) for b in (0, 1)]
+    want = lerp(lerp(zs[0], zs[1], u[:, 1]), lerp(zs[2], zs[3], u[:, 1]), u[:, 0])
+    assert np.abs(out - want).max() <= 1e-6 * 3
