@@ -283,6 +283,41 @@ def test_cloud_scene_image_parity(ctx):
 
 
 
+def test_grid_scene_in_a_batch_equals_its_single_render(ctx):
+    """A gridded scene batched with a plain one (shared waves, per-path scene
+    ids, ratio tracking on each path's own scene): both images equal their
+    single-scene renders."""
+    scenes = [gridded_spheres(ctx), mcpt.generate_scene(mcpt.SCENE_CORNELL_BOXES)]
+    devs = [mcpt.DeviceScene(mcpt.host_triangles(s), spheres=mcpt.host_spheres(s)) for s in scenes]
+    assert devs[0].view.has_medium & mcpt.MEDIUM_GRID and not devs[1].view.has_medium
+    batch = mcpt.BatchBvh(ctx, [d.view for d in devs], layout=mcpt.LAYOUT_WIDE4)
+
+    def params(s, W, spp):
+        cam = mcpt.Camera.from_buffer_copy(bytes(s.camera))
+        cam.image_width = W
+        cam.aspect_ratio = 1.0
+        mcpt.camera_initialize(cam)
+        return mcpt.render_params(cam, W, W, spp, 8, rng=mcpt.RNG_PHILOX, seed=99)
+    sizes = [(96, 3), (64, 2)]
+    accs = [torch.zeros(W * W * 3, dtype=torch.float32, device="cuda") for W, _ in sizes]
+    items = [mcpt.BatchItem(d.view, params(s, W, spp), a.data_ptr()) for d, s, a, (W, spp) in zip(devs, scenes, accs, sizes)]
+    st = batch.render(items)
+    assert st.error_flags == 0
+    batch.close()
+    for d, s, a, (W, spp) in zip(devs, scenes, accs, sizes):
+        single = mcpt.Bvh(ctx, d.view, layout=mcpt.LAYOUT_WIDE4)
+        ref = torch.zeros_like(a)
+        rs = mcpt.RenderStats()
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, single.handle, C.byref(d.view), C.byref(params(s, W, spp)),
+                                               ref.data_ptr(), C.byref(rs)))
+        single.close()
+        assert torch.equal(a, ref)
+        assert float(a.sum()) > 0
+    for s in scenes:
+        mcpt.free_scene(s)
+
+
+
 def test_release_grids(ctx):
     while _grids:
         mcpt.volume_grid_destroy(_grids.pop())
