@@ -12,6 +12,9 @@
 // per-bounce counter block, and camera/finalize loop over the path count the
 // table holds, so a wave is a fixed launch sequence (no host readback per
 // bounce as in PT:3816) that is captured once as a CUDA graph and replayed.
+// Renders deeper than the counter block (max_depth > 64) are the exception:
+// their counters form a ring, the host reads the next bounce's path count
+// every 8 bounces to end the wave early, and they are not captured.
 //
 // Compiled with --use_fast_math like the reference (CMakeLists.txt:94-96).
 #include <cuda_runtime.h>
