@@ -161,3 +161,13 @@ def test_oracle_grid_stand_in_reads_as_the_trilinear_restatement():
     zs = [lerp(at(ix + a, iy + b, iz), at(ix + a, iy + b, iz + 1), u[:, 2]) for a in (0, 1) for b in (0, 1)]
     want = lerp(lerp(zs[0], zs[1], u[:, 1]), lerp(zs[2], zs[3], u[:, 1]), u[:, 0])
     assert np.abs(out - want).max() <= 1e-6 * 3
+
+
+def test_cloud_scene_rejects_a_grid_without_extent():
+    h = mcpt.VolumeGrid()
+    for a in range(3):
+        h.world_min[a] = h.world_max[a] = 1.0
+    s = mcpt.SceneHost()
+    lib = mcpt.load()
+    assert lib.mc_scene_cloud(0x7F00, C.byref(h), 1, C.byref(s)) == 1
+    assert lib.mc_scene_cloud(None, C.byref(h), 1, C.byref(s)) == 1
