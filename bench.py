@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--refill", type=int, default=0,
                     help="trace refill threshold; 0 = the library autotuner's choice (a fixed value keeps profiles "
                          "free of the autotuner's probe launches)")
+    ap.add_argument("--resolution", default="",
+                    help="WxH instead of the workload's 1920x1080 (same view, e.g. 480x270 for small ncu captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
@@ -221,6 +223,13 @@ def run_ours(args):
     scene = mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=args.level, seed=2)
     tris = mcpt.host_triangles(scene)
     env = mcpt.host_env(scene)
+    if args.resolution:
+        rw, rh = (int(x) for x in args.resolution.lower().split("x"))
+        cam = mcpt.Camera.from_buffer_copy(bytes(scene.camera))
+        cam.image_width = rw
+        cam.aspect_ratio = rw / float(rh)
+        scene.camera = mcpt.camera_initialize(cam)
+        scene.width, scene.height = rw, rh
     ctx = mcpt.Context(local)
     ds = mcpt.DeviceScene(tris, env_rgba=env, env_intensity=scene.env_intensity, device=dev)
     layout = {"binary": mcpt.LAYOUT_BINARY, "wide4": mcpt.LAYOUT_WIDE4, "wide4q": mcpt.LAYOUT_WIDE4Q}[args.layout]
@@ -384,6 +393,9 @@ def run_ours(args):
     per_launch_s = trace_ms / max(trace_launches, 1) / 1e3
     achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     traffic = traffic_per_launch()
+    # DRAM fraction of the same launches: the captured DRAM bytes per launch
+    # over this run's mean launch duration
+    dram_gbs = traffic / per_launch_s / 1e9 if (traffic and per_launch_s > 0) else None
     value = rays_all / (ms_max / 1e3) / 1e6
     out = {
         "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
@@ -398,6 +410,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic, "kernel": "k_trace (persistent extend + shadow)",
+                     "dram_gbs": round(dram_gbs, 1) if dram_gbs else None,
+                     "dram_frac": round(dram_gbs / peak, 4) if dram_gbs else None,
                      "launches": trace_launches, "avg_launch_ms": round(trace_ms / max(trace_launches, 1), 4),
                      "trace_share": round(trace_ms / ms, 4),
                      "node_visits_per_ray": round(visits / max(rays, 1), 2),
@@ -786,47 +800,53 @@ def run_server(args):
 
 
 def run_reference(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    """The unmodified reference (oracle/_ref/libmcref.so: the reference's
+    src/path_tracer.cu compiled for sm_100a, curand XORWOW) through its own
+    renderWithWavefront with --persistent semantics, on the same scene. This
+    process loads only the reference build: the scene comes from the copy of
+    the library's seeded generator linked into that harness, not from the
+    library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
-    import mcpt
     import mcref
     if not mcref.available(False):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmcref.so was not built (needs the reference sources)"}))
         return
     ref = mcref.load(False)
-    scene = mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=args.level, seed=2)
-    tris = mcpt.host_triangles(scene)
-    env = mcpt.host_env(scene)
-    assert ref.mcref_scene_upload(C.addressof(tris), len(tris), None, 0, env.ctypes.data, scene.env_width,
+    scene = mcref.SceneHost()
+    assert ref.mcref_generate_scene(mcref.SCENE_DISPLACED_ICOSPHERES, args.level, 2, 0, C.byref(scene)) == 0
+    assert ref.mcref_scene_upload(scene.triangles, scene.triangle_count, None, 0, scene.env_rgba, scene.env_width,
                                   scene.env_height, scene.env_intensity, 0.0) == 0
     W, H, K, S = scene.width, scene.height, args.steps, args.spp_per_step
     acc = np.zeros(W * H * 3, np.float32)
     stats = np.zeros(3, np.float64)
-    cam = mcpt.Camera.from_buffer_copy(bytes(scene.camera))
+    cam = C.addressof(scene.camera)
     for _ in range(args.warmup):
-        assert ref.mcref_render(C.addressof(cam), W, H, 1, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+        assert ref.mcref_render(cam, W, H, 1, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
     clocks = Clocks(0)
     # timed: renderWithWavefront (PT:3757) itself, K steps of S samples, wavefront + persistent
-    assert ref.mcref_render(C.addressof(cam), W, H, K * S, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+    assert ref.mcref_render(cam, W, H, K * S, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
     ck = clocks.stop()
     ms = stats[2]
     # untimed replay of the same launch sequence that also reads the shadow-queue sizes
-    assert ref.mcref_render(C.addressof(cam), W, H, K * S, 8, 2, 1234, 0, 0, acc.ctypes.data, stats.ctypes.data) == 0
+    assert ref.mcref_render(cam, W, H, K * S, 8, 2, 1234, 0, 0, acc.ctypes.data, stats.ctypes.data) == 0
     rays = stats[0] + stats[1]
+    ref.mcref_free_scene(C.byref(scene))
     value = rays / (ms / 1e3) / 1e6
     out = {"metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1, "steps": K, "warmup": args.warmup,
            "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic (seeded procedural scene)", "impl": "reference",
            "config": dict(WORKLOAD, spp=K * S, spp_per_step=S, rng="curand XORWOW (the reference's own)", parallelism="1 GPU",
                           note="unmodified reference renderWithWavefront --wavefront --persistent on the B200"),
-           "cpu_baseline": {"value": round(value, 2), "unit": "Mrays/s", "cores": 1, "kind": "reference",
-                            "sample": "the full workload; the reference has no CPU implementation of the path, its own "
-                                      "CUDA build runs on the GPU driven by one host thread"},
+           "reference_run": {"kind": "reference", "device": "GPU (the reference's own CUDA build; it has no CPU "
+                                                            "implementation of the path)",
+                             "host_threads": 1, "sample": "the full workload, %d samples per pixel" % (K * S),
+                             "timing": "CUDA events around renderWithWavefront inside the harness; ray counts from "
+                                       "an untimed replay of the same launch sequence"},
            "e2e": {"value": round(value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "clocks": ck}
     print(json.dumps(out), flush=True)

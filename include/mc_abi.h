@@ -175,7 +175,9 @@ typedef struct mc_camera {
     float rr_cap;
 } mc_camera;
 
-/* PT:322-333 EnvironmentMap (g_environment). Pointers are device pointers. */
+/* PT:322-333 EnvironmentMap (g_environment). Pointers are device pointers.
+ * Maps made by mc_env_create also carry an alias table of the same texel
+ * distribution (MC_ENV_SAMPLE_ALIAS), kept by the library beside col_cdf. */
 typedef struct mc_env_map {
     uint64_t texture;           /* cudaTextureObject_t (float4, linear, wrap/clamp) */
     int32_t enabled;
@@ -273,7 +275,10 @@ typedef struct mc_render_params {
     uint64_t seed;              /* PT:4297 uses 1234 */
     int32_t intersector;        /* MC_ISECT_* */
     int32_t disable_clamp;      /* 1 = no firefly clamp (guiding MSE studies) */
-    int32_t queue_capacity;     /* 0 = width*height */
+    int32_t queue_capacity;     /* entries each extend / shadow queue holds; 0 = the wave's paths (every path
+                                   fits). Smaller values are a memory or fault-handling test: a bounce whose
+                                   queue would overflow keeps the first entries, drops the rest and the call
+                                   returns MC_ERR_QUEUE_OVERFLOW (the image is then incomplete) */
     int32_t refill_threshold;   /* idle lanes before a warp refills (PT:3400 uses 8); 0 = 8 */
     int32_t use_graph;          /* capture each sample's bounce sequence in a CUDA graph */
     int32_t instrument;         /* bit 0: count node visits / leaf tests (counting kernel variant);
@@ -282,7 +287,21 @@ typedef struct mc_render_params {
                                    states advance sample by sample): 0 = automatic (up to 16, at most about
                                    32M paths per wave), 1 = one sample per wave. Images do not depend on it:
                                    each pixel adds its samples in sample order. */
+    int32_t env_sampling;       /* MC_ENV_SAMPLE_*: how next-event estimation picks environment directions */
+    int32_t stack_entries;      /* traversal stack entries per lane: 0 = 64 (the reference's
+                                   TRAVERSAL_STACK_CAPACITY, PT:1038); 1..63 shrink the trace kernel's
+                                   shared memory; a ray that needs more ends and the call returns
+                                   MC_ERR_STACK_OVERFLOW (builds keep every 4-wide tree within 64) */
+    int32_t pad0;
 } mc_render_params;
+
+enum {
+    MC_ENV_SAMPLE_CDF = 0,      /* the reference's row/column CDF inversion (PT:433-467): four draws, two
+                                   binary searches; image parity with the reference needs this mode */
+    MC_ENV_SAMPLE_ALIAS = 1     /* Walker/Vose alias table over the texels (built by mc_env_create): four
+                                   draws, one table read; the same texel distribution, so the same expected
+                                   image, but not draw-compatible with the CDF mode */
+};
 
 #define MC_MAX_DEPTH 65536
 #define MC_MAX_DEPTH_STATS 64
@@ -316,7 +335,21 @@ MC_API mc_status mc_context_create(int device, mc_context** out);
 MC_API mc_status mc_context_destroy(mc_context* ctx);
 /* Stream (cudaStream_t) all work of this context is issued on; NULL = legacy default. */
 MC_API mc_status mc_context_set_stream(mc_context* ctx, void* stream);
+/* Waits for the context's stream; returns MC_ERR_TIMEOUT (and clears it) when a
+ * wait enqueued by mc_stream_wait_value ran out since the last call. */
 MC_API mc_status mc_context_synchronize(mc_context* ctx);
+/* Limit of the context's bounded device waits on an external flag
+ * (mc_stream_wait_value), in microseconds; 0 restores the default of 2 s. */
+MC_API mc_status mc_context_set_wait_timeout(mc_context* ctx, int64_t microseconds);
+/* Makes the context's stream wait, on the device, until *d_flag >= value: a
+ * 32-bit flag in device memory or mapped host memory that a producer outside
+ * this stream sets (the host, another stream, a peer GPU). Unlike an unbounded
+ * stream wait, the wait gives up after the context's wait timeout instead of
+ * holding the GPU: work behind it then runs, and the next
+ * mc_context_synchronize returns MC_ERR_TIMEOUT. The reference has no
+ * counterpart (it synchronises the whole device after every launch,
+ * PT:65-69). Returns once the wait is enqueued. */
+MC_API mc_status mc_stream_wait_value(mc_context* ctx, const uint32_t* d_flag, uint32_t value);
 
 /* ------------------------------------------------------------------------- */
 /* Scene helpers (host).                                                       */
@@ -517,11 +550,14 @@ MC_API mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t*
  *
  * Who needs it: a caller whose device memory is fully handed out ahead of time
  * (a render server that admits jobs up to a fixed HBM budget has nothing left
- * to allocate from at request time), a caller whose memory belongs to another
- * allocator (a caching allocator such as PyTorch's, which a direct cudaMalloc
- * would bypass and fragment), and a latency-bound loop that cannot take the
- * device-wide synchronisation cudaFree implies. This call allocates nothing:
- * no cudaMalloc/cudaFree and no allocating library routine.
+ * to allocate from at request time) and a caller whose memory belongs to
+ * another allocator (a caching allocator such as PyTorch's, which a direct
+ * cudaMalloc would bypass and fragment). This call allocates nothing: no
+ * cudaMalloc/cudaFree and no allocating library routine.
+ *
+ * Synchronisation: a call with n > 1 waits for ctx's stream to finish before
+ * it returns (it reads the device error word written by the sort's bounded
+ * waits), like mc_radix_sort_pairs.
  *
  * Scratch: a fixed device array inside the library (about 9 MiB: the
  * alternate key/value arrays for MC_SORT_STATIC_MAX_PAIRS pairs, the digit
@@ -533,9 +569,8 @@ MC_API mc_status mc_radix_sort_pairs(mc_context* ctx, uint32_t* d_keys, int32_t*
  *
  * Set-up: the first call on a device looks up that device's scratch address
  * (with the device made current for the look-up) and loads the sort kernels.
- * If that first call may happen inside a stream capture, make it earlier
- * instead: a call with n = 0 (keys and values may be NULL) does the set-up
- * and nothing else.
+ * Make that first call before any stream capture begins: a call with n = 0
+ * (keys and values may be NULL) does the set-up and nothing else.
  *
  * Overlapping calls race: every call on one device shares the one scratch
  * array, so two calls whose work overlaps in time (from two threads, or on two
@@ -749,7 +784,7 @@ typedef struct mc_server_request {
     int32_t guided;             /* render with the scene's guide (trained online) */
 } mc_server_request;
 
-enum { MC_REQ_PENDING = 0, MC_REQ_ACTIVE = 1, MC_REQ_DONE = 2, MC_REQ_RELEASED = 3 };
+enum { MC_REQ_PENDING = 0, MC_REQ_ACTIVE = 1, MC_REQ_DONE = 2, MC_REQ_RELEASED = 3, MC_REQ_CANCELLED = 4 };
 
 typedef struct mc_server_result {
     int64_t request_id;
@@ -785,6 +820,14 @@ MC_API mc_status mc_server_encode(mc_server* server, int64_t request_id, const m
                                   int64_t* bytes, float* chosen_exposure);
 /* Frees a finished request's accumulation buffer. */
 MC_API mc_status mc_server_release(mc_server* server, int64_t request_id);
+/* Cancels a pending or active request between steps (a client that went away,
+ * a deadline missed): it leaves the schedule, its accumulation buffer is freed
+ * and its memory returns to the budget at once; its state becomes
+ * MC_REQ_CANCELLED with the samples it had (spp_done). Reading or encoding it
+ * afterwards returns MC_ERR_CANCELLED. The reference has no counterpart (its
+ * only way out is exit(), PT:55-63). A request that is already done (or
+ * released) is not cancelled: MC_ERR_INVALID. */
+MC_API mc_status mc_server_cancel(mc_server* server, int64_t request_id);
 MC_API mc_status mc_server_get_stats(const mc_server* server, mc_server_stats* stats);
 /* Host seconds since the server was created (the clock of the results). */
 MC_API double mc_server_now(const mc_server* server);
@@ -827,9 +870,9 @@ MC_STATIC_ASSERT(sizeof(mc_camera) == 172, "Camera is 172 bytes");
 MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
 /* this library's own structs (bindings mirror these sizes) */
 MC_STATIC_ASSERT(sizeof(mc_guide_config) == 80, "mc_guide_config is 80 bytes");
-MC_STATIC_ASSERT(sizeof(mc_render_params) == 240, "mc_render_params is 240 bytes");
+MC_STATIC_ASSERT(sizeof(mc_render_params) == 248, "mc_render_params is 248 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_config) == 24, "mc_server_config is 24 bytes");
-MC_STATIC_ASSERT(sizeof(mc_server_request) == 256, "mc_server_request is 256 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_request) == 264, "mc_server_request is 264 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_result) == 56, "mc_server_result is 56 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_stats) == 64, "mc_server_stats is 64 bytes");
 MC_STATIC_ASSERT(sizeof(mc_image_options) == 16, "mc_image_options is 16 bytes");

@@ -9,8 +9,8 @@ Per-file flags:
   mc_render.cu, mc_resolve.cu, mc_volume.cu  -O3 --use_fast_math: the reference's release flags
                 (CMakeLists.txt:88-96), which the per-ray arithmetic must match.
   other .cu     -O3
-  mc_scene.cpp, mc_obj.cpp  g++ -O2 -ffp-contract=off (host scene, camera and OBJ
-                math as the reference's host code).
+  mc_scene.cpp, mc_scene_gen.cpp, mc_obj.cpp  g++ -O2 -ffp-contract=off (host
+                scene, camera and OBJ math as the reference's host code).
 
 Usage: python monocuda-pt_b200/build.py [-j N] [--force]
 """
@@ -43,7 +43,8 @@ UNITS = {
     "mc_resolve.cu": ["-O3", "--use_fast_math"],
     "mc_volume.cu": ["-O3", "--use_fast_math"],
 }
-HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_image.cpp": ["-O2"],
+HOST_UNITS = {"mc_scene.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"],
+              "mc_scene_gen.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_image.cpp": ["-O2"],
               "mc_obj.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "mc_files.cpp": ["-O2"]}
 
 

@@ -4,12 +4,19 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "mc_internal.h"
 
 namespace {
 thread_local char g_last_error[512] = "";
+
+// Alias tables of the environment maps made by mc_env_create, keyed by the
+// map's col_cdf pointer (the table lives in the same allocation, after it).
+std::mutex g_alias_mutex;
+std::unordered_map<const void*, const void*> g_alias_tables;
 }
 
 namespace mc {
@@ -59,6 +66,34 @@ void devbuf_free(DevBuf& b) {
     b.bytes = 0;
 }
 
+// One lane polls *flag (system-scope acquire loads, so a flag in mapped host
+// memory or a peer's memory is seen) with a back-off sleep, until it reaches
+// value or the device clock says timeout_ns have passed; then the error word
+// records the time-out and the stream moves on. Nothing else waits on this
+// kernel's lanes, and it touches no other memory.
+__global__ void k_wait_value(const uint32_t* flag, uint32_t value, long long timeout_ns, int* err) {
+    if (threadIdx.x != 0) return;
+    unsigned long long t0, now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    unsigned sleep = 32;
+    // the clock bounds the wait; the iteration count bounds it too, should
+    // the clock not advance
+    const long long maxIter = (timeout_ns >> 5) + (1ll << 20);
+    for (long long it = 0; it < maxIter; it++) {
+        uint32_t v;
+        asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v >= value) return;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if ((long long)(now - t0) > timeout_ns) {
+            atomicOr(err, MC_DEVERR_TIMEOUT);
+            return;
+        }
+        __nanosleep(sleep);
+        if (sleep < 4096) sleep <<= 1;
+    }
+    atomicOr(err, MC_DEVERR_TIMEOUT);
+}
+
 }  // namespace mc
 
 extern "C" {
@@ -102,13 +137,15 @@ mc_status mc_context_create(int device, mc_context** out) {
     ctx->device = device;
     ctx->sm_count = prop.multiProcessorCount;
     size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
-    if (cudaMalloc(&ctx->d_error, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->d_counters, counterBytes) != cudaSuccess ||
+    if (cudaMalloc(&ctx->d_error, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->d_wait_error, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_counters, counterBytes) != cudaSuccess ||
         cudaMalloc(&ctx->d_stats, (2 * MC_MAX_DEPTH_STATS + 8) * sizeof(long long)) != cudaSuccess) {
         cudaGetLastError();
         mc_context_destroy(ctx);
         return mc::set_error(MC_ERR_OOM, "mc_context_create: device allocation failed");
     }
     cudaMemset(ctx->d_error, 0, sizeof(int));
+    cudaMemset(ctx->d_wait_error, 0, sizeof(int));
     cudaMemset(ctx->d_counters, 0, counterBytes);
     *out = ctx;
     return MC_OK;
@@ -119,6 +156,7 @@ mc_status mc_context_destroy(mc_context* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream); else cudaDeviceSynchronize();
     cudaFree(ctx->d_error);
+    cudaFree(ctx->d_wait_error);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_stats);
     for (auto& b : ctx->scratch) mc::devbuf_free(b);
@@ -148,8 +186,29 @@ mc_status mc_context_set_stream(mc_context* ctx, void* stream) {
 
 mc_status mc_context_synchronize(mc_context* ctx) {
     if (!ctx) return mc::set_error(MC_ERR_INVALID, "mc_context_synchronize: null context");
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return mc::cuda_error((int)e, "cudaStreamSynchronize", __FILE__, __LINE__);
+    int flags = 0;
+    cudaError_t e = cudaMemcpyAsync(&flags, ctx->d_wait_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return mc::cuda_error((int)e, "mc_context_synchronize", __FILE__, __LINE__);
+    if (flags) {
+        if ((e = cudaMemsetAsync(ctx->d_wait_error, 0, sizeof(int), ctx->stream)) != cudaSuccess)
+            return mc::cuda_error((int)e, "mc_context_synchronize", __FILE__, __LINE__);
+        return mc::set_error(MC_ERR_TIMEOUT, "mc_stream_wait_value: the flag was not set within the wait timeout");
+    }
+    return MC_OK;
+}
+
+mc_status mc_context_set_wait_timeout(mc_context* ctx, int64_t microseconds) {
+    if (!ctx || microseconds < 0) return mc::set_error(MC_ERR_INVALID, "mc_context_set_wait_timeout: bad argument");
+    ctx->wait_timeout_ns = microseconds == 0 ? 2000000000ll : (long long)microseconds * 1000ll;
+    return MC_OK;
+}
+
+mc_status mc_stream_wait_value(mc_context* ctx, const uint32_t* d_flag, uint32_t value) {
+    if (!ctx || !d_flag) return mc::set_error(MC_ERR_INVALID, "mc_stream_wait_value: null argument");
+    mc::k_wait_value<<<1, 32, 0, ctx->stream>>>(d_flag, value, ctx->wait_timeout_ns, ctx->d_wait_error);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return mc::cuda_error((int)e, "mc_stream_wait_value", __FILE__, __LINE__);
     return MC_OK;
 }
 
@@ -198,6 +257,64 @@ mc_status mc_image_texture_destroy(uint64_t texture) {
     return MC_OK;
 }
 
+}  // extern "C"
+
+namespace mc {
+
+// Walker's alias method with Vose's linear-time construction (M. D. Vose, "A
+// linear algorithm for generating random numbers with a given distribution",
+// IEEE TSE 17(9), 1991) over the texel weights of the column CDFs: entry i =
+// (threshold, alias) with P(texel i) = (threshold_i + sum over j aliasing to i
+// of (1 - threshold_j)) / n = w_i / sum w. Built in double precision.
+void build_env_alias(const std::vector<float>& colCdf, int W, int H, std::vector<EnvAliasEntry>& table) {
+    const size_t n = (size_t)W * H;
+    table.assign(n, EnvAliasEntry{1.0f, 0});
+    std::vector<double> p(n);
+    double sum = 0.0;
+    for (int row = 0; row < H; row++) {
+        const float* cdf = &colCdf[(size_t)row * (W + 1)];
+        for (int col = 0; col < W; col++) {
+            const double w = (double)(cdf[col + 1] - cdf[col]);
+            p[(size_t)row * W + col] = w > 0.0 ? w : 0.0;
+            sum += p[(size_t)row * W + col];
+        }
+    }
+    for (size_t i = 0; i < n; i++) table[i].alias = (int32_t)i;
+    if (!(sum > 0.0)) return;
+    std::vector<uint32_t> small, large;
+    small.reserve(n);
+    large.reserve(n);
+    for (size_t i = 0; i < n; i++) {
+        p[i] = p[i] * (double)n / sum;
+        (p[i] < 1.0 ? small : large).push_back((uint32_t)i);
+    }
+    while (!small.empty() && !large.empty()) {
+        const uint32_t s = small.back(), l = large.back();
+        small.pop_back();
+        table[s].threshold = (float)p[s];
+        table[s].alias = (int32_t)l;
+        p[l] = (p[l] + p[s]) - 1.0;
+        if (p[l] < 1.0) {
+            large.pop_back();
+            small.push_back(l);
+        }
+    }
+    // leftovers (rounding) keep their own texel with certainty
+    for (uint32_t i : large) table[i] = EnvAliasEntry{1.0f, (int32_t)i};
+    for (uint32_t i : small) table[i] = EnvAliasEntry{1.0f, (int32_t)i};
+}
+
+const void* env_alias_table(const mc_env_map& env) {
+    if (!env.enabled || !env.col_cdf) return nullptr;
+    std::lock_guard<std::mutex> lock(g_alias_mutex);
+    auto it = g_alias_tables.find(env.col_cdf);
+    return it == g_alias_tables.end() ? nullptr : it->second;
+}
+
+}  // namespace mc
+
+extern "C" {
+
 mc_status mc_env_create(const float* rgba, int32_t W, int32_t H, float intensity, float rotation, mc_env_map* out) {
     if (!out) return mc::set_error(MC_ERR_INVALID, "mc_env_create: null output");
     std::memset(out, 0, sizeof(*out));
@@ -229,16 +346,35 @@ mc_status mc_env_create(const float* rgba, int32_t W, int32_t H, float intensity
         cudaFreeArray(arr);
         return mc::cuda_error((int)e, "cudaCreateTextureObject", __FILE__, __LINE__);
     }
+    std::vector<mc::EnvAliasEntry> alias;
+    mc::build_env_alias(colCdf, W, H, alias);
+    // one allocation: the column CDFs, then (16-byte aligned) the alias table
+    const size_t colBytes = colCdf.size() * sizeof(float);
+    const size_t aliasOffset = (colBytes + 15) & ~(size_t)15;
     float* dRow = nullptr; float* dCol = nullptr;
-    if (cudaMalloc(&dRow, rowCdf.size() * sizeof(float)) != cudaSuccess || cudaMalloc(&dCol, colCdf.size() * sizeof(float)) != cudaSuccess) {
+    if (cudaMalloc(&dRow, rowCdf.size() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&dCol, aliasOffset + alias.size() * sizeof(mc::EnvAliasEntry)) != cudaSuccess) {
         cudaGetLastError();
         cudaDestroyTextureObject(tex);
         cudaFreeArray(arr);
         cudaFree(dRow);
         return mc::set_error(MC_ERR_OOM, "mc_env_create: device allocation failed");
     }
-    cudaMemcpy(dRow, rowCdf.data(), rowCdf.size() * sizeof(float), cudaMemcpyHostToDevice);
-    cudaMemcpy(dCol, colCdf.data(), colCdf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    char* dAlias = reinterpret_cast<char*>(dCol) + aliasOffset;
+    if ((e = cudaMemcpy(dRow, rowCdf.data(), rowCdf.size() * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dCol, colCdf.data(), colBytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dAlias, alias.data(), alias.size() * sizeof(mc::EnvAliasEntry), cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+        cudaDestroyTextureObject(tex);
+        cudaFreeArray(arr);
+        cudaFree(dRow);
+        cudaFree(dCol);
+        return mc::cuda_error((int)e, "mc_env_create: table upload", __FILE__, __LINE__);
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_alias_mutex);
+        g_alias_tables[dCol] = dAlias;
+    }
     out->texture = (uint64_t)tex;
     out->enabled = 1;
     out->row_cdf = dRow;
@@ -257,6 +393,10 @@ mc_status mc_env_destroy(mc_env_map* env) {
         if (res.resType == cudaResourceTypeArray) cudaFreeArray(res.res.array.array);
     }
     cudaFree((void*)env->row_cdf);
+    {
+        std::lock_guard<std::mutex> lock(g_alias_mutex);
+        g_alias_tables.erase(env->col_cdf);
+    }
     cudaFree((void*)env->col_cdf);
     std::memset(env, 0, sizeof(*env));
     return MC_OK;

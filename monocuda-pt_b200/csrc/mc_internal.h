@@ -33,6 +33,17 @@ mc_status status_from_device_flags(int flags);
 void build_env_tables(const float* rgba, int W, int H, std::vector<float>& rowCdf, std::vector<float>& colCdf,
                       float& total);
 
+// One entry of an environment map's alias table: keep texel i when a uniform
+// draw is below threshold, else take texel alias.
+struct EnvAliasEntry {
+    float threshold;
+    int32_t alias;
+};
+void build_env_alias(const std::vector<float>& colCdf, int W, int H, std::vector<EnvAliasEntry>& table);
+// The device alias table of a map made by mc_env_create (EnvAliasEntry[width *
+// height]), or null for a disabled map or one the library did not create.
+const void* env_alias_table(const mc_env_map& env);
+
 // Grow-only device buffer.
 struct DevBuf {
     void* ptr = nullptr;
@@ -80,6 +91,8 @@ struct mc_context {
     cudaStream_t stream = nullptr;
     int sm_count = 0;
     int* d_error = nullptr;            // device error word
+    int* d_wait_error = nullptr;       // error word of mc_stream_wait_value (read by mc_context_synchronize)
+    long long wait_timeout_ns = 2000000000ll;  // bounded waits on external flags
     int* d_counters = nullptr;         // (MC_MAX_DEPTH_STATS+1) * MC_COUNTERS_PER_DEPTH ints
     long long* d_stats = nullptr;      // 2 * MC_MAX_DEPTH_STATS accumulated ray counts
     mc::DevBuf scratch[8];             // build / sort scratch
@@ -101,6 +114,13 @@ struct mc_context {
     unsigned long long graph_key[16] = {};  // every value the captured launches bake in
     void* staging = nullptr;             // pinned host staging for large pageable uploads
     size_t staging_bytes = 0;
+    // launch configurations measured on this context's device (occupancy of a
+    // kernel variant, its opt-in shared-memory size), filled on first use; a
+    // context is used by one host thread at a time, so these need no lock
+    int trace_blocks[128] = {};
+    int trace_blocks_smem[128] = {};     // shared-memory bytes trace_blocks[k] was measured with
+    int trace_smem_attr[128] = {};       // dynamic shared memory the variant has been opted in to
+    int shade_blocks[3] = {};            // Philox, XORWOW, guided
 };
 
 struct mc_bvh {

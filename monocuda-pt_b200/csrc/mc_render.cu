@@ -67,6 +67,7 @@ struct SceneGPU {
     uint32_t sample;
     uint32_t seedLo, seedHi;
     mc_env_map env;
+    const int2* envAlias;  // alias table of env (MC_ENV_SAMPLE_ALIAS), else null: CDF inversion
     mc_camera cam;
 };
 
@@ -130,6 +131,8 @@ struct TraceArgs {
     int* err;
     unsigned long long* counts;  // [0] node visits, [1] leaf tests (counting variant)
     int oneShot;                 // plain mode: one ray per thread, no refill
+    int stackCap;                // traversal stack entries per lane, <= MC_STACK_CAPACITY (0: all)
+    int queueCap;                // entries the extend and shadow queues hold (counts past it are clamped)
     // launches with gridded media (MC_MEDIUM_GRID): per shadow slot, the
     // distance of each medium crossing and, for back faces, the homogeneous
     // factor or the crossed primitive of a grid; rays that crossed a grid are
@@ -280,14 +283,14 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 #define MC_TRACE_MIN_BLOCKS 3
 #endif
 constexpr int kTraceThreads = 256;
-constexpr int kTraceSmem = MC_SMEM_STACK ? kTraceThreads * MC_STACK_CAPACITY * (int)sizeof(int) : 0;
 template <int ISECT, int MED, bool COUNT, int LAY, bool BATCH>
 __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
     const unsigned ltmask = lanemask_lt();
-    const int extCount = a.extCount ? *a.extCount : a.extN;
-    const int shCount = a.shCount ? *a.shCount : a.shN;
+    // a queue that overflowed holds queueCap entries (the producer flagged the overflow)
+    const int extCount = a.extCount ? min(*a.extCount, a.queueCap) : a.extN;
+    const int shCount = a.shCount ? min(*a.shCount, a.queueCap) : a.shN;
     const int total = extCount + shCount;
 #if MC_SMEM_STACK
     extern __shared__ int traceStack[];
@@ -374,8 +377,9 @@ __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(Tr
         }
         if (exhausted && __ballot_sync(kFull, has) == 0u) break;
         if (has) {
-            int r = (kind == RAY_SHADOW_ANY) ? trav_step_layout<true, ISECT, COUNT, LAY>(ts, s, stack, w, a.err, &cnt)
-                                             : trav_step_layout<false, ISECT, COUNT, LAY>(ts, s, stack, w, a.err, &cnt);
+            int r = (kind == RAY_SHADOW_ANY)
+                        ? trav_step_layout<true, ISECT, COUNT, LAY>(ts, s, stack, w, a.err, &cnt, a.stackCap)
+                        : trav_step_layout<false, ISECT, COUNT, LAY>(ts, s, stack, w, a.err, &cnt, a.stackCap);
             if (r != STEP_CONTINUE) {
                 const mc_triangle_cold* cold = a.cold0;
                 const mc_sphere* spheres = a.spheres0;
@@ -598,7 +602,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         float dist, solidPdf;
         if (envProb > 0.0f && (lightCount == 0 || rng.uniform() < envProb)) {
             float dirPdf;
-            toLight = env_sample(S.env, rng, dirPdf);
+            toLight = S.envAlias ? env_sample_alias(S.env, S.envAlias, rng, dirPdf) : env_sample(S.env, rng, dirPdf);
             lightColor = env_radiance(S.env, toLight, V3(0.f, 0.f, 0.f));
             dist = 1e30f;
             solidPdf = envProb * dirPdf;
@@ -723,7 +727,7 @@ MC_D int warp_reserve(bool want, int* counter, unsigned ltmask) {
 template <class Rng, bool GUIDED>
 __global__ void __launch_bounds__(256, GUIDED ? 2 : 4) k_shade(ShadeArgs a) {
     const unsigned ltmask = lanemask_lt();
-    const int count = *a.count;
+    const int count = min(*a.count, a.capacity);
     for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
         int q = base + threadIdx.x;
         ShadeOut out;
@@ -778,6 +782,8 @@ struct CameraArgs {
     uint32_t* draw;
     int* queue;
     int* count;
+    int capacity;  // entries the extend queue holds
+    int* err;
 };
 
 MC_D int find_scene(const WaveTable* tab, int p) {
@@ -798,7 +804,10 @@ MC_D void camera_rng_store(const CameraArgs& a, const SceneGPU& S, int p, int pi
 template <class Rng>
 __global__ void k_camera(CameraArgs a) {
     const int total = a.tab->totalPaths;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *a.count = total;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *a.count = total;
+        if (total > a.capacity) atomicOr(a.err, MC_DEVERR_QUEUE);  // the trace reads the first `capacity`
+    }
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
         int sid = a.tab->nScenes > 1 ? find_scene(a.tab, p) : 0;
         const SceneGPU& S = a.tab->scenes[sid];
@@ -1127,23 +1136,27 @@ TraceKernel trace_kernel(bool batch, int layout, bool count, int medium, int ise
 // batch launch when it carries a per-path scene map.
 void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, int layout, int medium, int isect,
                   bool persistent, int plainBlocks, bool count = false) {
-    static int occ[128] = {0};
-    static bool attr[128] = {false};
     TraceArgs t = t0;
     t.oneShot = persistent ? 0 : 1;
+    if (t.stackCap <= 0 || t.stackCap > MC_STACK_CAPACITY) t.stackCap = MC_STACK_CAPACITY;
+    // the shared-memory stack holds stackCap entries per lane
+    const int smem = MC_SMEM_STACK ? kTraceThreads * t.stackCap * (int)sizeof(int) : 0;
     const bool batch = t.sceneOf != nullptr;
     TraceKernel fn = trace_kernel(batch, layout, count, medium, isect);
     const int key = medium + 3 * (isect ? 1 : 0) + 6 * (count ? 1 : 0) + 12 * (batch ? 1 : 0) + 24 * layout;  // < 72
-    if (kTraceSmem > 48 * 1024 && !attr[key]) {
-        cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kTraceSmem);
-        attr[key] = true;
+    if (smem > 48 * 1024 && ctx->trace_smem_attr[key] < smem) {
+        cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        ctx->trace_smem_attr[key] = smem;
     }
     int blocks = std::max(1, plainBlocks);
     if (persistent) {
-        if (!occ[key]) occ[key] = occupancy_blocks((const void*)fn, ctx->sm_count, kTraceSmem);
-        blocks = occ[key];
+        if (!ctx->trace_blocks[key] || ctx->trace_blocks_smem[key] != smem) {
+            ctx->trace_blocks[key] = occupancy_blocks((const void*)fn, ctx->sm_count, smem);
+            ctx->trace_blocks_smem[key] = smem;
+        }
+        blocks = ctx->trace_blocks[key];
     }
-    fn<<<blocks, kTraceThreads, kTraceSmem, stream>>>(t);
+    fn<<<blocks, kTraceThreads, smem, stream>>>(t);
 }
 
 }  // namespace
@@ -1253,6 +1266,7 @@ static SceneGPU scene_gpu(mc_context* ctx, const mc_bvh* shared, const WaveItem&
     g.lightCount = it.view->light_count;
     g.hasMedium = it.view->has_medium;
     g.env = it.view->env;
+    g.envAlias = it.p->env_sampling == MC_ENV_SAMPLE_ALIAS ? static_cast<const int2*>(env_alias_table(g.env)) : nullptr;
     g.cam = it.p->camera;
     g.W = it.p->width;
     g.H = it.p->height;
@@ -1319,11 +1333,11 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         if (!ctx->own_stream) MC_CUDA(cudaStreamCreate(&ctx->own_stream));
         stream = ctx->own_stream;
     }
-    static int shadeBlocks[2] = {0, 0};
+    int* shadeBlocks = ctx->shade_blocks;
     if (!shadeBlocks[0]) shadeBlocks[0] = occupancy_blocks((const void*)k_shade<PhiloxRng, false>, ctx->sm_count);
     if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng, false>, ctx->sm_count);
-    static int guidedBlocks = 0;
-    if (guide && !guidedBlocks) guidedBlocks = occupancy_blocks((const void*)k_shade<PhiloxRng, true>, ctx->sm_count);
+    if (guide && !shadeBlocks[2]) shadeBlocks[2] = occupancy_blocks((const void*)k_shade<PhiloxRng, true>, ctx->sm_count);
+    const int guidedBlocks = shadeBlocks[2];
     const int plainBlocks = (2 * capacity + 255) / 256;
     const int loopBlocks = ctx->sm_count * 8;
     const WaveTable* dtab = (const WaveTable*)ctx->d_table;
@@ -1336,6 +1350,11 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ca.tr = w.tr; ca.tg = w.tg; ca.tb = w.tb; ca.sr = w.sr; ca.sg = w.sg; ca.sb = w.sb;
     ca.spec = w.spec; ca.pdf = w.pdf; ca.draw = w.draw; ca.queue = w.queue[0];
     ca.count = ctx->d_counters;
+    // entries each queue may hold: the wave's paths, or fewer when the caller
+    // asked for a smaller queue (the excess is dropped and reported as overflow)
+    const int queueCap = p0.queue_capacity > 0 ? std::min(p0.queue_capacity, capacity) : capacity;
+    ca.capacity = queueCap;
+    ca.err = ctx->d_error;
 
     ShadeArgs sa;
     std::memset(&sa, 0, sizeof(sa));
@@ -1346,7 +1365,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     sa.spec = w.spec; sa.pdf = w.pdf; sa.draw = w.draw; sa.hits = w.hits;
     sa.sox = w.sox; sa.soy = w.soy; sa.soz = w.soz; sa.sdx = w.sdx; sa.sdy = w.sdy; sa.sdz = w.sdz; sa.smax = w.smax;
     sa.scr = w.scr; sa.scg = w.scg; sa.scb = w.scb; sa.spath = w.spath;
-    sa.capacity = w.capacity;
+    sa.capacity = queueCap;
     sa.err = ctx->d_error;
 
     TraceArgs ta;
@@ -1359,6 +1378,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.scr = w.scr; ta.scg = w.scg; ta.scb = w.scb; ta.spath = w.spath;
     ta.sr = w.sr; ta.sg = w.sg; ta.sb = w.sb;
     ta.err = ctx->d_error;
+    ta.queueCap = queueCap;
+    ta.stackCap = p0.stack_entries;
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
     if (sameScene) {
@@ -1653,6 +1674,13 @@ mc_status check_params(const mc_render_params* p, const mc_scene_view* v) {
     if (p->max_depth < 0 || p->max_depth > MC_MAX_DEPTH) return set_error(MC_ERR_INVALID, "render: max_depth must be in [0, %d]", MC_MAX_DEPTH);
     if (p->rng != MC_RNG_PHILOX && p->rng != MC_RNG_XORWOW) return set_error(MC_ERR_INVALID, "render: unknown rng mode");
     if (p->intersector != MC_ISECT_REFERENCE && p->intersector != MC_ISECT_WATERTIGHT) return set_error(MC_ERR_INVALID, "render: unknown intersector");
+    if (p->queue_capacity < 0) return set_error(MC_ERR_INVALID, "render: queue_capacity must be >= 0");
+    if (p->stack_entries < 0 || p->stack_entries > MC_STACK_CAPACITY)
+        return set_error(MC_ERR_INVALID, "render: stack_entries must be in [0, %d]", MC_STACK_CAPACITY);
+    if (p->env_sampling != MC_ENV_SAMPLE_CDF && p->env_sampling != MC_ENV_SAMPLE_ALIAS)
+        return set_error(MC_ERR_INVALID, "render: unknown environment sampling mode");
+    if (p->env_sampling == MC_ENV_SAMPLE_ALIAS && v->env.enabled && !env_alias_table(v->env))
+        return set_error(MC_ERR_INVALID, "render: alias sampling needs an environment map made by mc_env_create");
     if (v->light_count > 0 && !v->lights) return set_error(MC_ERR_INVALID, "render: null light array");
     if (v->triangle_count > 0 && !v->tri_cold) return set_error(MC_ERR_INVALID, "render: null cold triangle array");
     return MC_OK;
@@ -1743,8 +1771,6 @@ mc_status mc_render_wavefront(mc_context* ctx, const mc_bvh* bvh, const mc_scene
     if (bvh->nseg != 1) return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: a batch BVH renders with mc_render_batch");
     if (scene->sphere_count + scene->triangle_count != bvh->n) return mc::set_error(MC_ERR_INVALID, "render: the BVH was built for another scene");
     int pixels = params->width * params->height;
-    if (params->queue_capacity > 0 && params->queue_capacity < pixels)
-        return mc::set_error(MC_ERR_INVALID, "mc_render_wavefront: queue capacity below width*height");
     if (params->rng == MC_RNG_XORWOW && (!ctx->rng_ready || ctx->rng_pixels < pixels || ctx->rng_seed != params->seed)) {
         if ((st = mc::rng_reset(ctx, pixels, params->seed)) != MC_OK) return st;
     }

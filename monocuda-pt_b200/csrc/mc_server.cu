@@ -327,6 +327,7 @@ mc_status mc_server_read(mc_server* s, int64_t request_id, float* host_rgb) {
     auto it = s->requests.find(request_id);
     if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_read: unknown request %lld", (long long)request_id);
     const ServerRequest& r = it->second;
+    if (r.state == MC_REQ_CANCELLED) return mc::set_error(MC_ERR_CANCELLED, "mc_server_read: request %lld was cancelled", (long long)request_id);
     if (!r.accum) return mc::set_error(MC_ERR_INVALID, "mc_server_read: request %lld holds no image", (long long)request_id);
     const size_t bytes = (size_t)r.params.width * r.params.height * 3 * sizeof(float);
     cudaError_t e = cudaMemcpyAsync(host_rgb, r.accum, bytes, cudaMemcpyDeviceToHost, s->ctx->stream);
@@ -342,6 +343,7 @@ mc_status mc_server_encode(mc_server* s, int64_t request_id, const mc_image_opti
     auto it = s->requests.find(request_id);
     if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_encode: unknown request %lld", (long long)request_id);
     const ServerRequest& r = it->second;
+    if (r.state == MC_REQ_CANCELLED) return mc::set_error(MC_ERR_CANCELLED, "mc_server_encode: request %lld was cancelled", (long long)request_id);
     if (!r.accum) return mc::set_error(MC_ERR_INVALID, "mc_server_encode: request %lld holds no image", (long long)request_id);
     if (r.done <= 0) return mc::set_error(MC_ERR_INVALID, "mc_server_encode: request %lld has no samples yet", (long long)request_id);
     return mc_image_encode(s->ctx, r.accum, r.params.width, r.params.height, r.done, opts, out, bytes, chosen_exposure);
@@ -352,11 +354,36 @@ mc_status mc_server_release(mc_server* s, int64_t request_id) {
     auto it = s->requests.find(request_id);
     if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_release: unknown request %lld", (long long)request_id);
     ServerRequest& r = it->second;
+    if (r.state == MC_REQ_CANCELLED) return MC_OK;  // its memory went back when it was cancelled
     if (r.state != MC_REQ_DONE) return mc::set_error(MC_ERR_INVALID, "mc_server_release: request %lld is not done", (long long)request_id);
     cudaFree(r.accum);
     r.accum = nullptr;
     r.state = MC_REQ_RELEASED;
     s->used -= r.bytes;
+    return MC_OK;
+}
+
+mc_status mc_server_cancel(mc_server* s, int64_t request_id) {
+    if (!s) return mc::set_error(MC_ERR_INVALID, "mc_server_cancel: null server");
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return mc::set_error(MC_ERR_NOT_FOUND, "mc_server_cancel: unknown request %lld", (long long)request_id);
+    ServerRequest& r = it->second;
+    if (r.state == MC_REQ_PENDING) {
+        s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r.id), s->pending.end());
+    } else if (r.state == MC_REQ_ACTIVE) {
+        s->active.erase(std::remove(s->active.begin(), s->active.end(), r.id), s->active.end());
+        // steps are synchronous, so no launch of this request is in flight;
+        // cudaFree would wait for one all the same
+        cudaFree(r.accum);
+        r.accum = nullptr;
+        s->used -= r.bytes;
+    } else {
+        return mc::set_error(r.state == MC_REQ_CANCELLED ? MC_ERR_CANCELLED : MC_ERR_INVALID,
+                             "mc_server_cancel: request %lld is %s", (long long)request_id,
+                             r.state == MC_REQ_CANCELLED ? "already cancelled" : "done");
+    }
+    r.state = MC_REQ_CANCELLED;
+    r.done_s = s->now();
     return MC_OK;
 }
 

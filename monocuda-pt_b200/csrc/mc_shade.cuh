@@ -96,6 +96,26 @@ MC_D V3 env_sample(const mc_env_map& env, Rng& rng, float& pdf) {
     return env_direction(env, u, v);
 }
 
+// Environment direction from the map's alias table (MC_ENV_SAMPLE_ALIAS):
+// texel i = floor(u0 * n), kept when u1 < its threshold, else its alias; then
+// the point inside the texel and the density as in env_sample. Four draws,
+// one table read instead of two binary searches; the same texel distribution
+// w / total_weight as the CDFs (Walker/Vose alias method). alias: int2 per
+// texel (threshold as float bits, alias index).
+template <class Rng>
+MC_D V3 env_sample_alias(const mc_env_map& env, const int2* __restrict__ alias, Rng& rng, float& pdf) {
+    const int n = env.width * env.height;
+    int i = min((int)(rng.uniform() * (float)n), n - 1);
+    const int2 e = __ldg(alias + i);
+    if (!(rng.uniform() < __int_as_float(e.x))) i = e.y;
+    const int row = i / env.width;
+    const int col = i - row * env.width;
+    float u = (col + rng.uniform()) / env.width;
+    float v = (row + rng.uniform()) / env.height;
+    pdf = env_texel_pdf(env, row, col, sinf(v * MC_PI));
+    return env_direction(env, u, v);
+}
+
 // PT:498-509 random_unit_vector (rejection in the cube)
 template <class Rng>
 MC_D V3 random_unit_vector(Rng& rng) {

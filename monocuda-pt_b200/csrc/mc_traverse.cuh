@@ -95,9 +95,11 @@ struct TravCount {
     int leaves = 0;
 };
 
+// cap: stack entries available to the lane (at most MC_STACK_CAPACITY); a push
+// beyond it ends the ray and sets MC_DEVERR_STACK.
 template <bool ANY, int ISECT, bool COUNT = false, class Stack = LocalStack>
 MC_D int trav_step(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
-                   TravCount* cnt = nullptr) {
+                   TravCount* cnt, int cap) {
     const float4* nd = sc.nodes + (long long)s.node * 4;
     float4 a = ldg4(nd + 0), b = ldg4(nd + 1), c = ldg4(nd + 2), d = ldg4(nd + 3);
     int lref = __float_as_int(d.x), rref = __float_as_int(d.y);
@@ -137,7 +139,7 @@ MC_D int trav_step(const TraceScene& sc, TravState& s, const Stack& stack, const
         s.node = stack[s.sp];
     } else {
         if (tL && tR) {
-            if (s.sp >= MC_STACK_CAPACITY) {
+            if (s.sp >= cap) {
                 atomicOr(err, MC_DEVERR_STACK);
                 return STEP_DONE;
             }
@@ -196,7 +198,7 @@ MC_D float q_scale(unsigned exps, int axis) {
 // leaf tests and the rank rule decide the hit as with exact boxes).
 template <bool ANY, int ISECT, bool COUNT = false, class Stack = LocalStack, bool QUANT = false>
 MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
-                    TravCount* cnt = nullptr) {
+                    TravCount* cnt, int cap) {
     float4 lx, ly, lz, hx, hy, hz, rf;
     if (QUANT) {
         const float4* nd = sc.nodes + (long long)s.node * 4;
@@ -282,7 +284,7 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, cons
     }
     // push the farther ones (farthest first), continue with the nearest
     int extra = (k1 != INFINITY) + (k2 != INFINITY) + (k3 != INFINITY);
-    if (s.sp + extra > MC_STACK_CAPACITY) {
+    if (s.sp + extra > cap) {
         atomicOr(err, MC_DEVERR_STACK);
         return STEP_DONE;
     }
@@ -296,10 +298,10 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, cons
 // LAY: MC_BVH_LAYOUT_BINARY, _WIDE4 or _WIDE4Q.
 template <bool ANY, int ISECT, bool COUNT, int LAY, class Stack>
 MC_D int trav_step_layout(const TraceScene& sc, TravState& s, const Stack& stack, const WatertightRay& w, int* err,
-                          TravCount* cnt) {
-    if (LAY == MC_BVH_LAYOUT_WIDE4Q) return trav_step4<ANY, ISECT, COUNT, Stack, true>(sc, s, stack, w, err, cnt);
-    if (LAY == MC_BVH_LAYOUT_WIDE4) return trav_step4<ANY, ISECT, COUNT, Stack, false>(sc, s, stack, w, err, cnt);
-    return trav_step<ANY, ISECT, COUNT, Stack>(sc, s, stack, w, err, cnt);
+                          TravCount* cnt, int cap) {
+    if (LAY == MC_BVH_LAYOUT_WIDE4Q) return trav_step4<ANY, ISECT, COUNT, Stack, true>(sc, s, stack, w, err, cnt, cap);
+    if (LAY == MC_BVH_LAYOUT_WIDE4) return trav_step4<ANY, ISECT, COUNT, Stack, false>(sc, s, stack, w, err, cnt, cap);
+    return trav_step<ANY, ISECT, COUNT, Stack>(sc, s, stack, w, err, cnt, cap);
 }
 
 // The hit record fields a leaf slot stands for.

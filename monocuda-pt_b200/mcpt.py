@@ -19,6 +19,7 @@ MAT_LAMBERTIAN, MAT_DIELECTRIC, MAT_CONDUCTOR, MAT_EMISSIVE, MAT_ISOTROPIC = 0, 
 TEX_SOLID, TEX_CHECKER, TEX_IMAGE = 0, 1, 2
 RNG_PHILOX, RNG_XORWOW = 0, 1
 ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
+ENV_SAMPLE_CDF, ENV_SAMPLE_ALIAS = 0, 1
 TRACE_PLAIN = 0x100
 LAYOUT_BINARY, LAYOUT_WIDE4, LAYOUT_WIDE4Q = 0, 1, 2
 BUILDER_CLUSTERED, BUILDER_LBVH = 0, 1
@@ -27,7 +28,7 @@ IMAGE_RGB8, IMAGE_RGB_F32, IMAGE_PFM, IMAGE_PNG = 0, 1, 2, 3
 SCENE_CORNELL_BOXES, SCENE_DISPLACED_ICOSPHERES, SCENE_BATCH_MEMBER, SCENE_GUIDING_ROOM = 1, 2, 3, 4
 SCENE_CORNELL_SPHERES = 5
 MAX_DEPTH_STATS = 64
-REQ_PENDING, REQ_ACTIVE, REQ_DONE, REQ_RELEASED = 0, 1, 2, 3
+REQ_PENDING, REQ_ACTIVE, REQ_DONE, REQ_RELEASED, REQ_CANCELLED = 0, 1, 2, 3, 4
 SORT_STATIC_MAX_PAIRS = 1 << 20
 GUIDE_PARAM_COUNT = 20200
 GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_OUTPUTS, GUIDE_LOBES = 144, 64, 40, 8
@@ -139,7 +140,8 @@ class RenderParams(C.Structure):
                 ("first_sample", C.c_int32), ("max_depth", C.c_int32), ("persistent", C.c_int32), ("rng", C.c_int32),
                 ("seed", C.c_uint64), ("intersector", C.c_int32), ("disable_clamp", C.c_int32),
                 ("queue_capacity", C.c_int32), ("refill_threshold", C.c_int32), ("use_graph", C.c_int32),
-                ("instrument", C.c_int32), ("samples_per_wave", C.c_int32)]
+                ("instrument", C.c_int32), ("samples_per_wave", C.c_int32), ("env_sampling", C.c_int32),
+                ("stack_entries", C.c_int32), ("pad0", C.c_int32)]
 
 
 class GuideConfig(C.Structure):
@@ -202,8 +204,8 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, VolumeGrid: 64, GuideConfig: 80, RenderParams: 240,
-         ServerConfig: 24, ServerRequest: 256, ServerResult: 56, ServerStats: 64}
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, VolumeGrid: 64, GuideConfig: 80, RenderParams: 248,
+         ServerConfig: 24, ServerRequest: 264, ServerResult: 56, ServerStats: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
 
@@ -218,6 +220,8 @@ SIGNATURES = {
     "mc_context_destroy": (I32, [P]),
     "mc_context_set_stream": (I32, [P, P]),
     "mc_context_synchronize": (I32, [P]),
+    "mc_context_set_wait_timeout": (I32, [P, C.c_int64]),
+    "mc_stream_wait_value": (I32, [P, P, C.c_uint32]),
     "mc_camera_initialize": (I32, [C.POINTER(Camera)]),
     "mc_scene_finalize_host": (I32, [P, I32, P, C.POINTER(I32)]),
     "mc_split_triangles_host": (I32, [P, I32, P, P]),
@@ -259,6 +263,7 @@ SIGNATURES = {
     "mc_server_step": (I32, [P, C.POINTER(I32)]),
     "mc_server_get_result": (I32, [P, C.c_int64, C.POINTER(ServerResult)]),
     "mc_server_release": (I32, [P, C.c_int64]),
+    "mc_server_cancel": (I32, [P, C.c_int64]),
     "mc_server_read": (I32, [P, C.c_int64, P]),
     "mc_server_encode": (I32, [P, C.c_int64, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64), C.POINTER(C.c_float)]),
     "mc_image_encode": (I32, [P, P, I32, I32, I32, C.POINTER(ImageOptions), P, C.POINTER(C.c_int64),
@@ -698,7 +703,7 @@ def make_camera(width, height, look_from, look_at, vfov, focus, max_depth=8, spp
 
 def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RNG_PHILOX, seed=1234, first_sample=0,
                   intersector=ISECT_REFERENCE, disable_clamp=False, refill_threshold=0, use_graph=False, instrument=0,
-                  samples_per_wave=0):
+                  samples_per_wave=0, env_sampling=0, queue_capacity=0, stack_entries=0):
     p = RenderParams()
     p.camera = camera
     p.width, p.height, p.spp, p.first_sample, p.max_depth = width, height, spp, first_sample, max_depth
@@ -707,11 +712,13 @@ def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RN
     p.seed = seed
     p.intersector = intersector
     p.disable_clamp = 1 if disable_clamp else 0
-    p.queue_capacity = 0
+    p.queue_capacity = queue_capacity
     p.refill_threshold = refill_threshold
     p.use_graph = 1 if use_graph else 0
     p.instrument = instrument
     p.samples_per_wave = samples_per_wave
+    p.env_sampling = env_sampling
+    p.stack_entries = stack_entries
     return p
 
 
@@ -827,6 +834,9 @@ class Server:
 
     def release(self, rid):
         check(self.lib.mc_server_release(self.handle, rid))
+
+    def cancel(self, rid):
+        check(self.lib.mc_server_cancel(self.handle, rid))
 
     def stats(self):
         st = ServerStats()

@@ -3,6 +3,8 @@
 imported by tests/, by tests/golden/make_golden.py and by bench.py's
 reference arm. Built by oracle/Makefile (needs the reference sources); the
 built .so files travel with the repository snapshot, the sources do not.
+The harness also carries the library's seeded scene generator
+(mcref_generate_scene), so the reference arm needs nothing else.
 """
 import ctypes as C
 import os
@@ -23,10 +25,24 @@ _SIGS = {
     "mcref_resolve": (I32, [P, I32, I32, I32, I32, C.c_float, I32, P, P, P]),
     "mcref_load_object": (I32, [C.c_char_p, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P, I32, P]),
     "mcref_load_pfm": (I32, [C.c_char_p, P, P, P]),
+    "mcref_generate_scene": (I32, [I32, I32, C.c_ulonglong, I32, P]),
+    "mcref_free_scene": (I32, [P]),
     "mcref_grid_sample": (I32, [P, P, I32, P]),
     "mcref_cloud_scene": (I32, [P, P, C.c_float, C.c_uint64, I32, P, I32, P, P, I32, P]),
 }
 _libs = {}
+
+# mc_scene_host (include/mc_abi.h) with the camera as its 172 raw bytes: the
+# reference arm of the benchmark reads the seeded scenes through the harness
+# without the library's Python binding.
+SCENE_DISPLACED_ICOSPHERES = 2
+
+
+class SceneHost(C.Structure):
+    _fields_ = [("triangles", P), ("triangle_count", I32), ("spheres", P), ("sphere_count", I32),
+                ("camera", C.c_float * 43), ("width", I32), ("height", I32), ("spp", I32), ("max_depth", I32),
+                ("has_medium", I32), ("env_rgba", P), ("env_width", I32), ("env_height", I32),
+                ("env_intensity", C.c_float)]
 
 
 def path(philox=False):

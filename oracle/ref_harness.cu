@@ -26,6 +26,15 @@
 #include <fcntl.h>
 #include "../include/mc_abi.h"
 
+// The library's seeded synthetic scenes, from its host-only generator source
+// (monocuda-pt_b200/csrc/mc_scene_gen.cpp, linked into this harness by
+// oracle/Makefile): the reference renders byte-identical scenes without the
+// library being loaded.
+namespace mc_gen {
+const char* generate(const mc_scene_desc* desc, mc_scene_host* out, mc_status* status);
+void free_scene(mc_scene_host* s);
+}
+
 static_assert(sizeof(triangle) == sizeof(mc_triangle), "triangle layout");
 static_assert(sizeof(triangle_hot) == sizeof(mc_triangle_hot), "triangle_hot layout");
 static_assert(sizeof(triangle_cold) == sizeof(mc_triangle_cold), "triangle_cold layout");
@@ -647,6 +656,29 @@ int mcref_load_pfm(const char* path, int* width, int* height, float* rgba) {
     if (width) *width = w;
     if (height) *height = h;
     if (rgba) std::memcpy(rgba, pixels.data(), pixels.size() * sizeof(float));
+    return 0;
+}
+
+// One of the library's seeded synthetic scenes (mc_scene_generate's kinds and
+// arguments), host arrays released by mcref_free_scene. Returns 0 or the
+// library's status code.
+int mcref_generate_scene(int kind, int variant, unsigned long long seed, int triangle_target, mc_scene_host* out) {
+    mc_scene_desc d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = kind;
+    d.variant = variant;
+    d.seed = seed;
+    d.triangle_target = triangle_target;
+    mc_status st = MC_OK;
+    if (mc_gen::generate(&d, out, &st)) {
+        mc_gen::free_scene(out);
+        return (int)st;
+    }
+    return 0;
+}
+
+int mcref_free_scene(mc_scene_host* s) {
+    mc_gen::free_scene(s);
     return 0;
 }
 

@@ -10,7 +10,7 @@ oracle's compile-only stubs).
                                               #   set, small Philox-mode images
 
 Scenes come from the library's seeded generator (host code); the fixtures hold
-the reference's outputs for them. tests/test_oracle_golden.py checks the CPU
+the reference's outputs for them. tests/test_cpu.py checks the CPU
 oracle against these files; the GPU tests compare the CUDA path against the
 reference build directly.
 """

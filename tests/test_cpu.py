@@ -291,6 +291,33 @@ def test_scene_generators_are_deterministic_and_sized():
         mcpt.free_scene(s)
 
 
+@pytest.mark.skipif(not mcref.available(False), reason="oracle/_ref not built (needs the reference sources)")
+@pytest.mark.parametrize("kind,variant,seed", [(mcpt.SCENE_CORNELL_BOXES, 0, 0), (mcpt.SCENE_DISPLACED_ICOSPHERES, 5, 2),
+                                               (mcpt.SCENE_BATCH_MEMBER, 3, 3), (mcpt.SCENE_GUIDING_ROOM, 0, 4),
+                                               (mcpt.SCENE_CORNELL_SPHERES, 0, 2)])
+def test_reference_harness_generates_the_library_scenes(kind, variant, seed):
+    """The benchmark's reference arm reads its scene through the harness's copy
+    of the generator (no library loaded there): the same bytes as the library's."""
+    a = mcpt.generate_scene(kind, variant=variant, seed=seed)
+    b = mcref.SceneHost()
+    assert mcref.load(False).mcref_generate_scene(kind, variant, seed, 0, C.byref(b)) == 0
+    try:
+        assert b.triangle_count == a.triangle_count and b.sphere_count == a.sphere_count
+        assert C.string_at(b.triangles, 224 * b.triangle_count) == bytes(mcpt.host_triangles(a))
+        if a.sphere_count:
+            assert C.string_at(b.spheres, 160 * b.sphere_count) == C.string_at(a.spheres, 160 * a.sphere_count)
+        assert bytes(b.camera) == bytes(a.camera)
+        assert (b.width, b.height, b.spp, b.max_depth, b.has_medium) == (a.width, a.height, a.spp, a.max_depth,
+                                                                         a.has_medium)
+        assert (b.env_width, b.env_height, b.env_intensity) == (a.env_width, a.env_height, a.env_intensity)
+        if a.env_width:
+            nb = 16 * a.env_width * a.env_height
+            assert C.string_at(b.env_rgba, nb) == C.string_at(C.cast(a.env_rgba, C.c_void_p), nb)
+    finally:
+        mcref.load(False).mcref_free_scene(C.byref(b))
+        mcpt.free_scene(a)
+
+
 def test_primary_rays_helper_matches_camera():
     s = mcpt.generate_scene(mcpt.SCENE_CORNELL_BOXES)
     r = primary_rays(s.camera, 8, 8)

@@ -400,7 +400,7 @@ def test_image_parity_philox(ctx, kind, variant, W, H, spp, layout):
     frac = pixel_agreement(mine, ref)
     print("philox layout %d scene %d: pixel agreement %.6f, identical %.6f, rays %d+%d (reference %d+%d)"
           % (layout, kind, frac, np.mean(np.all(mine == ref, axis=2)), st.extend_rays, st.shadow_rays, rs[0], rs[1]))
-    assert frac >= 0.999
+    assert frac == 1.0
     assert abs(st.extend_rays - rs[0]) <= 0.001 * rs[0]
 
 
@@ -412,7 +412,7 @@ def test_image_parity_xorwow_unmodified(ctx, kind):
     ref, _ = render_ref(s, 256, 256, 2, 8, 2, philox=False, unmodified=1)
     frac = pixel_agreement(mine, ref)
     print("xorwow scene %d pixel agreement %.6f" % (kind, frac))
-    assert frac >= 0.999
+    assert frac == 1.0
 
 
 def test_megakernel_reference_agrees_with_wavefront(ctx):
