@@ -72,6 +72,10 @@ def parse():
     ap.add_argument("--guide-chunk", type=int, default=8)
     ap.add_argument("--guide-lr", type=float, default=1e-3)
     ap.add_argument("--guide-steps", type=int, default=4, help="Adam steps per sample, each on 65536 records")
+    ap.add_argument("--guide-vertices", type=int, default=0,
+                    help="diffuse vertices per path that train the guide (0 = the library default, 3)")
+    ap.add_argument("--guide-dir", default="normal", choices=["normal", "ray"],
+                    help="direction input of the guide: the face normal or the arriving ray's direction")
     ap.add_argument("--mlp-items", type=int, default=1 << 20)
     ap.add_argument("--server-rates", type=float, nargs="+", default=[1, 4, 16, 64], help="arrival rates (requests/s)")
     ap.add_argument("--server-requests", type=int, default=64,
@@ -597,8 +601,9 @@ def run_guiding(args):
     # the guided one with the timed guide's configuration
     tmp = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
     render(tmp, chunk, 999999)
+    gdir = mcpt.GUIDE_DIR_NORMAL if args.guide_dir == "normal" else mcpt.GUIDE_DIR_RAY
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
-                            train_steps=args.guide_steps)
+                            train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir)
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -624,7 +629,7 @@ def run_guiding(args):
     target = plain_curve[-1][2]
     # guided, trained online from scratch
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
-                       train_steps=args.guide_steps)
+                       train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir)
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -658,6 +663,7 @@ def run_guiding(args):
            "target_rmse": round(target, 6), "plain_spp": args.guide_plain_spp, "plain_ms": round(plain_ms, 1),
            "guided_ms_to_target": round(reached, 1) if reached is not None else None,
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
+           "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve,

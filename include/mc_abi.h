@@ -665,11 +665,13 @@ MC_API mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_
 /* Flat FP32 parameter vector: W1[64][144] b1[64] W2[64][64] b2[64] W3[64][64]
  * b3[64] W4[40][64] b4[40] (W[out][in], row-major). */
 #define MC_GUIDE_PARAM_COUNT 20200
-/* Per query: x, y, z, dx, dy, dz (world position, ray direction). */
+/* Per query: x, y, z, dx, dy, dz (world position, the direction input: a
+ * unit normal or ray direction, mc_guide_config.direction_input). */
 #define MC_GUIDE_QUERY_FLOATS 6
-/* Per training record: position, ray direction at the vertex, the sampled
- * next direction, and the record's weight (the radiance estimate carried back
- * through that direction divided by its sampling density, a luminance). */
+/* Per training record: position, the direction input at the vertex, the
+ * sampled next direction, and the record's weight (the radiance estimate
+ * carried back through that direction divided by its sampling density, a
+ * luminance). */
 #define MC_GUIDE_RECORD_FLOATS 10
 /* Per query output: lobe weights[8] (sum 1), unit means[8][3], kappa[8]. */
 #define MC_GUIDE_MIXTURE_FLOATS 40
@@ -685,7 +687,18 @@ typedef struct mc_guide_config {
     float guide_fraction;       /* one-sample MIS mix: probability of sampling the guide; 0 = 0.5 */
     int32_t train_steps;        /* Adam steps per sample in guided renders, each on its own
                                    batch_capacity records of that sample; 0 = 1 */
+    int32_t train_vertices;     /* guided renders: diffuse vertices per path that give training records,
+                                   the first ones along the path (1..MC_GUIDE_MAX_TRAIN_VERTICES); 0 = 3 */
+    int32_t direction_input;    /* MC_GUIDE_DIR_*: the direction the guided renderer feeds the network */
 } mc_guide_config;
+
+#define MC_GUIDE_MAX_TRAIN_VERTICES 4
+enum {
+    MC_GUIDE_DIR_NORMAL = 0,    /* the vertex's geometric normal, turned to face the arriving ray: the
+                                   incident light of a diffuse vertex depends on where it is and which way
+                                   it faces, not on the direction it is seen from */
+    MC_GUIDE_DIR_RAY = 1        /* the arriving ray's direction */
+};
 
 MC_API mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_guide** out);
 MC_API mc_status mc_guide_destroy(mc_guide* guide);
@@ -706,9 +719,12 @@ MC_API int32_t mc_guide_steps(const mc_guide* guide);
 /* Guided wavefront render: at diffuse vertices the next direction comes from
  * the guide with probability guide_fraction and from the cosine BSDF
  * otherwise, weighted by the mixed density (one-sample MIS, unbiased); NEE's
- * MIS weights use the same mixed density. With train != 0 every sample's
- * primary vertices become training records and the guide takes one Adam step
- * after each sample. Needs the counter-based RNG and a single-scene BVH. */
+ * MIS weights use the same mixed density. With train != 0 the first
+ * train_vertices diffuse vertices of every path become training records
+ * (weight: the light that arrived through the sampled direction, excluding
+ * the vertex's own NEE, over the throughput that reached the vertex and the
+ * direction's density) and the guide takes train_steps Adam steps per sample.
+ * Needs the counter-based RNG and a single-scene BVH. */
 MC_API mc_status mc_render_guided(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
                                   const mc_render_params* params, mc_guide* guide, int32_t train, float* d_accum,
                                   mc_render_stats* stats);

@@ -93,11 +93,49 @@ struct GuideInferArgs {
     int capacity;
     const float* queries;                   // API: n x 6
     const int* queue;                       // render: path per slot
-    const float *ox, *oy, *oz, *dx, *dy, *dz;
+    const float *ox, *oy, *oz, *dx, *dy, *dz, *time;
     const mc_packed_hit* hits;
+    const mc_triangle_hot* hot;             // render with MC_GUIDE_DIR_NORMAL: the hit primitives
+    const mc_sphere* spheres;
+    int dirNormal;
     float* mix;
     int* err;
 };
+
+// Geometric normal of the hit primitive, turned to face the arriving ray d
+// (the shade kernel's face normal: e1 x e2 for a triangle, centre to hit point
+// for a sphere at the ray's time).
+__device__ __forceinline__ void face_normal(const GuideInferArgs& a, int type, int idx, float t, float time, float px,
+                                            float py, float pz, float dx, float dy, float dz, float* n) {
+    float nx, ny, nz;
+    if (type == 1) {
+        const float* v = reinterpret_cast<const float*>(a.hot + idx);
+        const float e1x = v[3] - v[0], e1y = v[4] - v[1], e1z = v[5] - v[2];
+        const float e2x = v[6] - v[0], e2y = v[7] - v[1], e2z = v[8] - v[2];
+        nx = e1y * e2z - e1z * e2y;
+        ny = e1z * e2x - e1x * e2z;
+        nz = e1x * e2y - e1y * e2x;
+    } else {
+        const mc_sphere& sp = a.spheres[idx];
+        float cx = sp.center.x, cy = sp.center.y, cz = sp.center.z;
+        if (sp.is_moving) {
+            cx = cx + (sp.center1.x - cx) * time;
+            cy = cy + (sp.center1.y - cy) * time;
+            cz = cz + (sp.center1.z - cz) * time;
+        }
+        nx = px - cx; ny = py - cy; nz = pz - cz;
+    }
+    const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+    if (!(len > 0.f)) {
+        n[0] = -dx; n[1] = -dy; n[2] = -dz;
+        return;
+    }
+    nx = nx / len; ny = ny / len; nz = nz / len;
+    if (dx * nx + dy * ny + dz * nz >= 0.f) {
+        nx = -nx; ny = -ny; nz = -nz;
+    }
+    n[0] = nx; n[1] = ny; n[2] = nz;
+}
 
 struct GuideTrainArgs {
     const bf16* blob;
@@ -296,6 +334,11 @@ __global__ void __launch_bounds__(128) k_guide_infer(GuideInferArgs a) {
                 const float t = h.w ? __int_as_float(h.x) : 0.f;
                 dx = a.dx[p]; dy = a.dy[p]; dz = a.dz[p];
                 px = a.ox[p] + dx * t; py = a.oy[p] + dy * t; pz = a.oz[p] + dz * t;
+                if (a.dirNormal && h.w) {
+                    float nrm[3];
+                    face_normal(a, h.y, h.z, t, a.time[p], px, py, pz, dx, dy, dz, nrm);
+                    dx = nrm[0]; dy = nrm[1]; dz = nrm[2];
+                }
                 out = p;
             } else {
                 const float* Q = a.queries + (size_t)q * 6;
@@ -652,13 +695,12 @@ void init_params(std::vector<float>& p, uint64_t seed) {
     fill(oW4, kOut, kHid, 0.1);
 }
 
-bool g_attr_done = false;
-
-mc_status set_attrs() {
-    if (g_attr_done) return MC_OK;
+// The kernels' opt-in shared-memory sizes, once per context (per device).
+mc_status set_attrs(mc_context* ctx) {
+    if (ctx->guide_attrs_set) return MC_OK;
     MC_CUDA(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
     MC_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
-    g_attr_done = true;
+    ctx->guide_attrs_set = true;
     return MC_OK;
 }
 
@@ -688,7 +730,7 @@ void fill_box(const mc_guide* g, Args& a) {
 
 mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n, const int* count, int offset,
                        int capacity, int stepCap, const float* scale, int* gridOut) {
-    mc_status st = set_attrs();
+    mc_status st = set_attrs(g->ctx);
     if (st != MC_OK) return st;
     GuideTrainArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -743,7 +785,7 @@ mc_status guide_reserve_paths(mc_guide* g, int paths) {
     g->mixtures = g->records = g->nee0 = nullptr;
     g->mixture_capacity = g->record_capacity = 0;
     if (cudaMalloc(&g->mixtures, (size_t)paths * kOut * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&g->records, (size_t)paths * 12 * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&g->records, (size_t)paths * g->cfg.train_vertices * 16 * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&g->nee0, (size_t)paths * 3 * sizeof(float)) != cudaSuccess) {
         cudaGetLastError();
         return set_error(MC_ERR_OOM, "guide: allocation of per-path buffers failed");
@@ -754,8 +796,9 @@ mc_status guide_reserve_paths(mc_guide* g, int paths) {
 
 mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
                             const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
-                            const float* dz, const mc_packed_hit* hits, float* mixtures) {
-    mc_status st = set_attrs();
+                            const float* dz, const float* time, const mc_packed_hit* hits, const mc_triangle_hot* hot,
+                            const mc_sphere* spheres, float* mixtures) {
+    mc_status st = set_attrs(g->ctx);
     if (st != MC_OK) return st;
     GuideInferArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -765,8 +808,11 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
     a.count = count;
     a.capacity = capacity;
     a.queue = queue;
-    a.ox = ox; a.oy = oy; a.oz = oz; a.dx = dx; a.dy = dy; a.dz = dz;
+    a.ox = ox; a.oy = oy; a.oz = oz; a.dx = dx; a.dy = dy; a.dz = dz; a.time = time;
     a.hits = hits;
+    a.hot = hot;
+    a.spheres = spheres;
+    a.dirNormal = g->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
     a.mix = mixtures;
     a.err = g->ctx->d_error;
     k_guide_infer<<<2 * g->ctx->sm_count, kTile, kInferSmem, s>>>(a);
@@ -833,6 +879,12 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     if (g->cfg.batch_capacity <= 0) g->cfg.batch_capacity = 65536;
     if (g->cfg.train_steps <= 0) g->cfg.train_steps = 1;
     if (!(g->cfg.guide_fraction > 0.f && g->cfg.guide_fraction < 1.f)) g->cfg.guide_fraction = 0.5f;
+    if (g->cfg.train_vertices <= 0) g->cfg.train_vertices = 3;
+    if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1) {
+        delete g;
+        return mc::set_error(MC_ERR_INVALID, "mc_guide_create: train_vertices above %d or unknown direction_input",
+                             MC_GUIDE_MAX_TRAIN_VERTICES);
+    }
     const size_t P = (size_t)kParams * sizeof(float);
     bool okAlloc = cudaMalloc(&g->master, P) == cudaSuccess && cudaMalloc(&g->adam_m, P) == cudaSuccess &&
                    cudaMalloc(&g->adam_v, P) == cudaSuccess && cudaMalloc(&g->blob, (size_t)kBlob * 2) == cudaSuccess &&
@@ -905,7 +957,7 @@ mc_status mc_guide_set_params(mc_guide* g, const float* params) {
 mc_status mc_guide_infer(mc_guide* g, const float* d_queries, int32_t n, float* d_mixtures) {
     if (!g || n < 0 || (n > 0 && (!d_queries || !d_mixtures))) return mc::set_error(MC_ERR_INVALID, "mc_guide_infer: bad argument");
     if (n == 0) return MC_OK;
-    mc_status st = set_attrs();
+    mc_status st = set_attrs(g->ctx);
     if (st != MC_OK) return st;
     mc_context* ctx = g->ctx;
     MC_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));

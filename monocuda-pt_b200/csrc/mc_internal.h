@@ -121,6 +121,7 @@ struct mc_context {
     int trace_blocks_smem[128] = {};     // shared-memory bytes trace_blocks[k] was measured with
     int trace_smem_attr[128] = {};       // dynamic shared memory the variant has been opted in to
     int shade_blocks[3] = {};            // Philox, XORWOW, guided
+    bool guide_attrs_set = false;        // the guide kernels' shared-memory opt-in is done
 };
 
 struct mc_bvh {
@@ -210,9 +211,12 @@ mc_status check_params(const mc_render_params* p, const mc_scene_view* v);
 mc_status bvh_depth(mc_bvh* bvh);
 mc_status context_counters(mc_context* ctx);
 // Guide kernels driven by device-side counts (guided renders).
+// Inputs of a queued path: its hit point and, per the guide's direction_input,
+// the face normal of the hit primitive (hot, spheres, time) or the ray direction.
 mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
                             const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
-                            const float* dz, const mc_packed_hit* hits, float* mixtures);
+                            const float* dz, const float* time, const mc_packed_hit* hits, const mc_triangle_hot* hot,
+                            const mc_sphere* spheres, float* mixtures);
 // `steps` Adam steps, each on the next min(stepRecords, cfg.batch_capacity)
 // of the records (stepRecords <= 0: cfg.batch_capacity).
 mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps,

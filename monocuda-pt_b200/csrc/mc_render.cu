@@ -418,15 +418,26 @@ struct ShadeArgs {
     int capacity;
     int* err;
     // guided shading: per-path mixtures of this bounce, the guide's share of
-    // the one-sample MIS, and the primary-vertex training records
+    // the one-sample MIS, the training records of the first recSlots diffuse
+    // vertices of each path, and the direction the guide is fed
     const float* mix;
     float guideFrac;
     float* rec;
+    int recSlots;
+    int dirNormal;
 };
 
-// Per-path training record of the primary vertex: position, ray direction,
-// sampled direction, weight, valid flag, MIS remainder of depth-1 emission.
-constexpr int kRecFloats = 12;
+// Training record of a diffuse vertex (recSlots per path, slot = depth):
+// [0..2] position, [3..5] direction input (face normal or ray direction),
+// [6..8] sampled direction, [9] mean throughput that reached the vertex,
+// [10] valid (the sampled direction was traced), [11] MIS remainder of the
+// emission that direction found, [12] mean sample radiance not carried by
+// that direction (everything before the vertex plus its own NEE).
+constexpr int kRecFloats = 16;
+
+MC_D float* rec_slot(const ShadeArgs& a, int p, int depth) {
+    return a.rec + ((size_t)p * a.recSlots + depth) * kRecFloats;
+}
 
 struct ShadeOut {
     bool next;
@@ -488,9 +499,9 @@ MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w) {
 // NEE's side of the MIS carries instead is kept in the record's spare slot and
 // added to its weight. Without it a broad early guide, whose density is tiny
 // next to the light's, would never be pulled toward a small light.
-MC_D void train_remainder(const ShadeArgs& a, int p, const V3& L, float w) {
-    if (w >= 1.0f) return;
-    float* r = a.rec + (size_t)p * kRecFloats;
+MC_D void train_remainder(const ShadeArgs& a, int p, int depth, const V3& L, float w) {
+    if (w >= 1.0f || depth < 1 || depth > a.recSlots) return;
+    float* r = rec_slot(a, p, depth - 1);
     if (r[10] == 0.0f) return;
     r[11] = (L.x + L.y + L.z) * (1.0f / 3.0f) * (1.0f - w);
 }
@@ -507,6 +518,12 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
     int ptype = hraw.y, pidx = hraw.z, didHit = hraw.w;
     const V3 background = v3(S.cam.background);
     const int lightCount = S.lightCount;
+    if (GUIDED && a.rec && depth >= 1 && depth <= a.recSlots) {
+        // the previous vertex's direction was traced: what the sample holds now
+        // (including that vertex's NEE) did not come through it
+        float* r = rec_slot(a, p, depth - 1);
+        if (r[10] != 0.0f) r[12] = (cs.x + cs.y + cs.z) * (1.0f / 3.0f);
+    }
     if (!didHit) {
         V3 missDir(a.dx[p], a.dy[p], a.dz[p]);
         float envW = 1.0f;
@@ -515,7 +532,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             envW = power_heuristic(a.pdf[p], envProb * env_direction_pdf(S.env, missDir));
         const V3 envL = throughput * env_radiance(S.env, missDir, background);
         cs = cs + envL * envW;
-        if (GUIDED && a.rec && depth == 1) train_remainder(a, p, envL, envW);
+        if (GUIDED && a.rec) train_remainder(a, p, depth, envL, envW);
         a.sr[p] = cs.x;
         a.sg[p] = cs.y;
         a.sb[p] = cs.z;
@@ -527,6 +544,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
     float rayTime = a.time[p];
     V3 hitPoint = o + inDir * hitT;
     V3 hitNormal;
+    V3 faceNormal;  // geometric normal facing the arriving ray (the guide's direction input)
     bool frontFace;
     float hitU, hitV;
     V3 tv0, tv1, tv2;
@@ -536,6 +554,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         V3 outward = (hitPoint - c).normalize();
         frontFace = inDir.dot(outward) < 0.0f;
         hitNormal = frontFace ? outward : -outward;
+        faceNormal = hitNormal;
         V2 uv = sphere_uv(outward);
         hitU = uv.x;
         hitV = uv.y;
@@ -549,6 +568,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         frontFace = inDir.dot(nrm) < 0.0f;
         V3 shading = triangle_shading_normal(tv0, tv1, tv2, v3(cd.n0), v3(cd.n1), v3(cd.n2), hitPoint, nrm);
         hitNormal = frontFace ? shading : -shading;
+        faceNormal = frontFace ? nrm : -nrm;
         V2 uv = triangle_uv(tv0, tv1, tv2, V2(cd.uv0.x, cd.uv0.y), V2(cd.uv1.x, cd.uv1.y), V2(cd.uv2.x, cd.uv2.y), hitPoint);
         hitU = uv.x;
         hitV = uv.y;
@@ -565,7 +585,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             emissionWeight = power_heuristic(a.pdf[p], lightPdf);
         }
         cs = cs + throughput * mat.emitted * emissionWeight;
-        if (GUIDED && a.rec && depth == 1) train_remainder(a, p, throughput * mat.emitted, emissionWeight);
+        if (GUIDED && a.rec) train_remainder(a, p, depth, throughput * mat.emitted, emissionWeight);
         a.sr[p] = cs.x;
         a.sg[p] = cs.y;
         a.sb[p] = cs.z;
@@ -573,6 +593,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
     }
     Rng rng;
     rng_load<Rng>(a, S, p, rng);
+    const V3 tPre = throughput;  // what reached this vertex (training records of guided renders)
     V3 scatterOrigin = hitPoint;
     if (mat.type == MC_MAT_ISOTROPIC) {
         float sd;
@@ -677,11 +698,14 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
                     }
                     guidedPdf = guided_pdf(m, a.guideFrac, hitNormal, nd);
                     throughput = throughput * ((c / MC_PI) / guidedPdf);
-                    if (a.rec && depth == 0) {
-                        float* r = a.rec + (size_t)p * kRecFloats;
+                    if (a.rec && depth < a.recSlots && depth + 1 < S.maxDepth) {
+                        // the direction is traced next: a training record of this vertex
+                        float* r = rec_slot(a, p, depth);
+                        const V3 din = a.dirNormal ? faceNormal : inDir;
                         r[0] = scatterOrigin.x; r[1] = scatterOrigin.y; r[2] = scatterOrigin.z;
-                        r[3] = inDir.x; r[4] = inDir.y; r[5] = inDir.z;
+                        r[3] = din.x; r[4] = din.y; r[5] = din.z;
                         r[6] = nd.x; r[7] = nd.y; r[8] = nd.z;
+                        r[9] = (tPre.x + tPre.y + tPre.z) * (1.0f / 3.0f);
                         r[10] = 1.0f;
                     }
                 } else {
@@ -738,8 +762,13 @@ __global__ void __launch_bounds__(256, GUIDED ? 2 : 4) k_shade(ShadeArgs a) {
             p = a.queue[q];
             const SceneGPU& S = a.tab->scenes[scene_of(a.tab, a.sceneOf, p)];
             if (GUIDED && a.rec && a.depth == 0) {
-                a.rec[(size_t)p * kRecFloats + 10] = 0.0f;
-                a.rec[(size_t)p * kRecFloats + 11] = 0.0f;
+                // every path of the wave passes here first: its record slots start empty
+                for (int k = 0; k < a.recSlots; k++) {
+                    float* r = rec_slot(a, p, k);
+                    r[10] = 0.0f;
+                    r[11] = 0.0f;
+                    r[12] = 0.0f;
+                }
             }
             shade_path<Rng, GUIDED>(a, S, p, out);
         }
@@ -867,35 +896,40 @@ __global__ void k_finalize(const WaveTable* tab, const float* sr, const float* s
     }
 }
 
-// A guided wave's training batch holds its records in (sample, pixel) order:
-// sample j of every pixel before sample j + 1 of any, so that an Adam step on
-// a pixel count of records sees about one sample of the whole image, as with
-// one sample per wave, and the batch (and so the trained guide) is the same
-// on every run. Entry v of that order is sample v / totalPixels of wave pixel
-// v % totalPixels. When the wave has more paths than the batch holds, only
-// entries with (pixel + sample + recPhase) % recStride == 0 are kept, the host
-// rotating recPhase between waves, so that records come from the whole image.
-// A kept entry is a record when its path has a primary-vertex record of
-// positive, finite weight: the sample without the primary vertex's NEE (the
-// radiance carried back through the sampled direction over that direction's
-// density).
+// A guided wave's training batch holds its records in (sample, vertex,
+// pixel) order: sample j of every pixel before sample j + 1 of any, so that
+// an Adam step on a pixel count of records sees about one sample of the
+// whole image, as with one sample per wave, and the batch (and so the
+// trained guide) is the same on every run. Entry v of that order is vertex
+// slot (v / P) % R of sample v / (P R) of wave pixel v % P (P pixels, R record
+// slots per path). When the wave has more entries than the batch holds, only
+// entries with (pixel + sample R + slot + recPhase) % recStride == 0 are kept,
+// the host rotating recPhase between waves, so that records come from the
+// whole image and every depth. A kept entry is a record when its slot holds a
+// record of positive, finite weight: the mean sample radiance that arrived
+// through the sampled direction (the sample minus what it held before that
+// direction was traced, plus the MIS remainder of emission the direction
+// found) over the mean throughput that reached the vertex. The primary
+// vertex's NEE goes to its own buffer, so the sample holds none of it.
 constexpr int kRecThreads = 256;
 constexpr int kRecTileChunks = 8;
 constexpr int kRecTile = kRecThreads * kRecTileChunks;  // entries per tile
 
-MC_D bool rec_entry(const WaveTable* tab, long long v, int recStride, int recPhase, const float* sr, const float* sg,
-                    const float* sb, const float* rec, int* path, float* weight) {
+MC_D bool rec_entry(const WaveTable* tab, long long v, int recSlots, int recStride, int recPhase, const float* sr,
+                    const float* sg, const float* sb, const float* rec, const float** out, float* weight) {
     const int pixels = tab->totalPixels;
-    const int j = (int)(v / pixels);
-    const int u = (int)(v - (long long)j * pixels);
-    if ((u + j + recPhase) % recStride != 0) return false;
+    const long long js = v / pixels;
+    const int u = (int)(v - js * pixels);
+    const int j = (int)(js / recSlots);
+    const int k = (int)(js - (long long)j * recSlots);
+    if ((u + j * recSlots + k + recPhase) % recStride != 0) return false;
     const SceneGPU& S = tab->scenes[tab->nScenes > 1 ? find_scene_by_pixel(tab, u) : 0];
     if (j >= S.pathStride) return false;
     const int p = S.pathOffset + (u - S.pixelOffset) * S.pathStride + j;
-    const float* r = rec + (size_t)p * kRecFloats;
-    if (r[10] == 0.0f) return false;
-    const float w = (sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) + r[11];
-    *path = p;
+    const float* r = rec + ((size_t)p * recSlots + k) * kRecFloats;
+    if (r[10] == 0.0f || !(r[9] > 0.0f)) return false;
+    const float w = ((sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) - r[12] + r[11]) / r[9];
+    *out = r;
     *weight = w;
     return w > 0.0f && w < 1e30f;
 }
@@ -907,7 +941,7 @@ __global__ void __launch_bounds__(kRecThreads) k_finalize_guided(const WaveTable
                                                                  const float* sr, const float* sg, const float* sb,
                                                                  const float* nr, const float* ng, const float* nb,
                                                                  const float* rec, int* tileCounts, long long entries,
-                                                                 int recStride, int recPhase) {
+                                                                 int recSlots, int recStride, int recPhase) {
     // the image: each pixel adds its samples of the wave in sample order
     const int pixels = tab->totalPixels;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < pixels; u += gridDim.x * blockDim.x) {
@@ -935,9 +969,10 @@ __global__ void __launch_bounds__(kRecThreads) k_finalize_guided(const WaveTable
         int c = 0;
         for (int i = 0; i < kRecTileChunks; i++) {
             const long long v = (long long)t * kRecTile + i * kRecThreads + threadIdx.x;
-            int p;
+            const float* r;
             float w;
-            c += __syncthreads_count(v < entries && rec_entry(tab, v, recStride, recPhase, sr, sg, sb, rec, &p, &w));
+            c += __syncthreads_count(v < entries &&
+                                     rec_entry(tab, v, recSlots, recStride, recPhase, sr, sg, sb, rec, &r, &w));
         }
         if (threadIdx.x == 0) tileCounts[t] = c;
     }
@@ -983,8 +1018,8 @@ __global__ void __launch_bounds__(1024) k_rec_scan(int* tileCounts, int tiles, i
 // first slot (k_rec_scan) plus the kept entries before it in the tile.
 __global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab, const float* sr, const float* sg,
                                                            const float* sb, const float* rec, const int* tileFirst,
-                                                           long long entries, int recStride, int recPhase, float* batch,
-                                                           int capacity) {
+                                                           long long entries, int recSlots, int recStride, int recPhase,
+                                                           float* batch, int capacity) {
     __shared__ int warpCount[kRecThreads / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned ltmask = lanemask_lt();
@@ -993,9 +1028,9 @@ __global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab,
         int next = tileFirst[t];
         for (int i = 0; i < kRecTileChunks; i++) {
             const long long v = (long long)t * kRecTile + i * kRecThreads + threadIdx.x;
-            int p = 0;
+            const float* r = nullptr;
             float w = 0.f;
-            const bool e = v < entries && rec_entry(tab, v, recStride, recPhase, sr, sg, sb, rec, &p, &w);
+            const bool e = v < entries && rec_entry(tab, v, recSlots, recStride, recPhase, sr, sg, sb, rec, &r, &w);
             const unsigned m = __ballot_sync(kFull, e);
             if (lane == 0) warpCount[wid] = __popc(m);
             __syncthreads();
@@ -1007,7 +1042,6 @@ __global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab,
             }
             const int slot = before + __popc(m & ltmask);
             if (e && slot < capacity) {
-                const float* r = rec + (size_t)p * kRecFloats;
                 float* b = batch + (size_t)slot * MC_GUIDE_RECORD_FLOATS;
                 for (int k = 0; k < 9; k++) b[k] = r[k];
                 b[9] = w;
@@ -1425,7 +1459,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         if ((st = guide_reserve_batch(guide, guide->cfg.batch_capacity * guide->cfg.train_steps * maxR)) != MC_OK) return st;
         long long pixelsAll = 0;
         for (int i = 0; i < n; i++) pixelsAll += (long long)items[i].p->width * items[i].p->height;
-        if ((st = guide_reserve_tiles(guide, (int)((pixelsAll * maxR + kRecTile - 1) / kRecTile))) != MC_OK) return st;
+        if ((st = guide_reserve_tiles(guide, (int)((pixelsAll * maxR * guide->cfg.train_vertices + kRecTile - 1) /
+                                                   kRecTile))) != MC_OK)
+            return st;
     }
     // the launch sequence of one wave (device table already holds the wave)
     float* nee0[3] = {nullptr, nullptr, nullptr};
@@ -1483,7 +1519,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             }
             if (guide) {
                 mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], slot(d) + 0, capacity,
-                                                 w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.hits, guide->mixtures);
+                                                 w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.time, w.hits,
+                                                 items[0].view->tri_hot, items[0].view->spheres, guide->mixtures);
                 if (gs != MC_OK) return gs;
                 launches++;
             }
@@ -1504,6 +1541,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 sd.mix = guide->mixtures;
                 sd.guideFrac = guide->cfg.guide_fraction;
                 sd.rec = train ? guide->records : nullptr;
+                sd.recSlots = guide->cfg.train_vertices;
+                sd.dirNormal = guide->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
                 k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
             } else if (philox) {
                 k_shade<PhiloxRng, false><<<shadeBlocks[0], 256, 0, stream>>>(sd);
@@ -1520,15 +1559,17 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             }
         }
         if (guide) {
-            const long long entries = train ? (long long)waveR * wavePixels : 0;
+            const int slots = guide->cfg.train_vertices;
+            const long long entries = train ? (long long)slots * waveR * wavePixels : 0;
             k_finalize_guided<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1],
                                                                       nee0[2], train ? guide->records : nullptr,
-                                                                      guide->rec_tiles, entries, recStride, recPhase);
+                                                                      guide->rec_tiles, entries, slots, recStride,
+                                                                      recPhase);
             if (train) {
                 const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
                 k_rec_scan<<<1, 1024, 0, stream>>>(guide->rec_tiles, tiles, guide->batch_count);
                 k_rec_write<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, w.sr, w.sg, w.sb, guide->records, guide->rec_tiles,
-                                                                    entries, recStride, recPhase, guide->batch,
+                                                                    entries, slots, recStride, recPhase, guide->batch,
                                                                     guide->cfg.batch_capacity * guide->cfg.train_steps *
                                                                         waveR);
                 launches += 2;
@@ -1625,7 +1666,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         wavePixels = pix;
         if (guide) {
             const long long cap = (long long)guide->cfg.batch_capacity * guide->cfg.train_steps * waveR;
-            recStride = (int)std::max(1ll, (off + cap - 1) / cap);
+            const long long entries = (long long)guide->cfg.train_vertices * off;
+            recStride = (int)std::max(1ll, (entries + cap - 1) / cap);
             recPhase = wv % recStride;
         }
         h->pad1 = 0;

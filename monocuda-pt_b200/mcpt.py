@@ -20,6 +20,7 @@ TEX_SOLID, TEX_CHECKER, TEX_IMAGE = 0, 1, 2
 RNG_PHILOX, RNG_XORWOW = 0, 1
 ISECT_REFERENCE, ISECT_WATERTIGHT = 0, 1
 ENV_SAMPLE_CDF, ENV_SAMPLE_ALIAS = 0, 1
+GUIDE_DIR_NORMAL, GUIDE_DIR_RAY = 0, 1
 TRACE_PLAIN = 0x100
 LAYOUT_BINARY, LAYOUT_WIDE4, LAYOUT_WIDE4Q = 0, 1, 2
 BUILDER_CLUSTERED, BUILDER_LBVH = 0, 1
@@ -147,7 +148,8 @@ class RenderParams(C.Structure):
 class GuideConfig(C.Structure):
     _fields_ = [("bounds", AABB), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
-                ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("_pad", C.c_int32 * 3)]
+                ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("train_vertices", C.c_int32),
+                ("direction_input", C.c_int32), ("_pad", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -727,7 +729,7 @@ class Guide:
     BF16 tensor-core inference and training."""
 
     def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5,
-                 train_steps=1):
+                 train_steps=1, train_vertices=0, direction_input=0):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = GuideConfig()
@@ -738,6 +740,8 @@ class Guide:
         cfg.batch_capacity = batch_capacity
         cfg.guide_fraction = guide_fraction
         cfg.train_steps = train_steps
+        cfg.train_vertices = train_vertices
+        cfg.direction_input = direction_input
         self.config = cfg
         h = P()
         check(self.lib.mc_guide_create(ctx.handle, C.byref(cfg), C.byref(h)))
