@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--resolution", default="",
                     help="WxH instead of the workload's 1920x1080 (same view, e.g. 480x270 for small ncu captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-1m", action="store_true",
+                    help="skip the second, ~1M-triangle line (level-7 icospheres, 983,056 triangles)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
                     help="warm-up and timed steps only (for ncu captures); prints the timed line without extras")
@@ -216,6 +218,52 @@ def cpu_baseline(scene, args):
                       % (rows, W, spp, threads, dt, int(rays))}
 
 
+def level_variant(ctx, level, steps, warmup, spp_per_step):
+    """Mrays/s of the same workload with level-L icospheres (L = 7: 3 x 327,680
+    triangles, the ~1M-triangle reading of the scene), device-timed like the
+    headline: scene resident, autotuned refill, K frames of spp_per_step."""
+    import torch
+
+    import mcpt
+    scene = mcpt.generate_scene(mcpt.SCENE_DISPLACED_ICOSPHERES, variant=level, seed=2)
+    tris = mcpt.host_triangles(scene)
+    ds = mcpt.DeviceScene(tris, env_rgba=mcpt.host_env(scene), env_intensity=scene.env_intensity)
+    bvh = mcpt.Bvh(ctx, ds.view, layout=mcpt.LAYOUT_WIDE4, builder=mcpt.BUILDER_CLUSTERED)
+    W, H = scene.width, scene.height
+    acc = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    tuned = mcpt.render_params(scene.camera, W, H, spp_per_step, 8, persistent=True, rng=mcpt.RNG_PHILOX, seed=1234)
+    mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
+    st = mcpt.RenderStats()
+
+    def step(i):
+        p = mcpt.render_params(scene.camera, W, H, spp_per_step, 8, persistent=bool(tuned.persistent),
+                               rng=mcpt.RNG_PHILOX, seed=1234, first_sample=i * spp_per_step,
+                               refill_threshold=tuned.refill_threshold, samples_per_wave=tuned.samples_per_wave,
+                               trace_threads=tuned.trace_threads, stack_entries=tuned.stack_entries)
+        mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), acc.data_ptr(),
+                                               C.byref(st)))
+        return st.extend_rays + st.shadow_rays
+    for i in range(warmup):
+        step(1000 + i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rays = sum(step(i) for i in range(steps))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"workload": "displaced_icospheres level %d" % level, "triangles": int(len(tris)), "steps": steps,
+           "spp_per_step": spp_per_step, "value": round(rays / (ms / 1e3) / 1e6, 2), "unit": "Mrays/s",
+           "ms_per_step": round(ms / steps, 3),
+           "autotuned": {"refill_threshold": int(tuned.refill_threshold), "trace_threads": int(tuned.trace_threads) or 256,
+                         "stack_entries": int(tuned.stack_entries) or 64,
+                         "samples_per_wave": int(tuned.samples_per_wave) or "automatic"}}
+    bvh.close()
+    ds.close()
+    mcpt.free_scene(scene)
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -255,7 +303,9 @@ def run_ours(args):
     def params(step, instrument=0):
         return mcpt.render_params(scene.camera, W, H, S, 8, persistent=bool(tuned.persistent), rng=mcpt.RNG_PHILOX,
                                   seed=1234, first_sample=step * S, instrument=instrument,
-                                  refill_threshold=tuned.refill_threshold, samples_per_wave=args.samples_per_wave)
+                                  refill_threshold=tuned.refill_threshold,
+                                  samples_per_wave=args.samples_per_wave or tuned.samples_per_wave,
+                                  trace_threads=tuned.trace_threads, stack_entries=tuned.stack_entries)
 
     st = mcpt.RenderStats()
     for s in warm_samples:
@@ -406,7 +456,10 @@ def run_ours(args):
         "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "config": dict(WORKLOAD, spp=K * S * world, spp_per_step=S, bvh_layout=args.layout, bvh_builder=args.builder,
-                       autotuned={"persistent": int(tuned.persistent), "refill_threshold": int(tuned.refill_threshold)},
+                       autotuned={"persistent": int(tuned.persistent), "refill_threshold": int(tuned.refill_threshold),
+                                  "samples_per_wave": int(tuned.samples_per_wave) or "automatic",
+                                  "trace_threads": int(tuned.trace_threads) or 256,
+                                  "stack_entries": int(tuned.stack_entries) or 64, "graph": int(tuned.use_graph)},
                        parallelism="replicas x%d + final all-reduce" % world if world > 1 else "1 GPU",
                        samples_per_wave=args.samples_per_wave or "automatic",
                        samples_per_sec=round(W * H * K * S * world / (ms_max / 1e3), 1),
@@ -433,6 +486,8 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": ck,
     }
+    if not args.no_1m and args.level == 8 and world == 1:
+        out["workload_1m"] = level_variant(ctx, 7, K, Wm, S)
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(scene, args)
     print(json.dumps(out), flush=True)
@@ -843,6 +898,22 @@ def run_reference(args):
     rays = stats[0] + stats[1]
     ref.mcref_free_scene(C.byref(scene))
     value = rays / (ms / 1e3) / 1e6
+    variant = None
+    if not args.no_1m and args.level == 8:
+        # the ~1M-triangle reading of the scene (level-7 icospheres), fewer samples
+        v = mcref.SceneHost()
+        assert ref.mcref_generate_scene(mcref.SCENE_DISPLACED_ICOSPHERES, 7, 2, 0, C.byref(v)) == 0
+        assert ref.mcref_scene_upload(v.triangles, v.triangle_count, None, 0, v.env_rgba, v.env_width, v.env_height,
+                                      v.env_intensity, 0.0) == 0
+        vspp = 4 * S
+        vcam = C.addressof(v.camera)
+        assert ref.mcref_render(vcam, W, H, 1, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+        assert ref.mcref_render(vcam, W, H, vspp, 8, 2, 1234, 0, 1, acc.ctypes.data, stats.ctypes.data) == 0
+        vms = stats[2]
+        assert ref.mcref_render(vcam, W, H, vspp, 8, 2, 1234, 0, 0, acc.ctypes.data, stats.ctypes.data) == 0
+        variant = {"workload": "displaced_icospheres level 7", "triangles": int(v.triangle_count), "spp": vspp,
+                   "value": round((stats[0] + stats[1]) / (vms / 1e3) / 1e6, 2), "unit": "Mrays/s"}
+        ref.mcref_free_scene(C.byref(v))
     out = {"metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1, "steps": K, "warmup": args.warmup,
            "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic (seeded procedural scene)", "impl": "reference",
@@ -855,6 +926,8 @@ def run_reference(args):
                                        "an untimed replay of the same launch sequence"},
            "e2e": {"value": round(value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "clocks": ck}
+    if variant:
+        out["workload_1m"] = variant
     print(json.dumps(out), flush=True)
 
 

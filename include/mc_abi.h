@@ -292,7 +292,10 @@ typedef struct mc_render_params {
                                    TRAVERSAL_STACK_CAPACITY, PT:1038); 1..63 shrink the trace kernel's
                                    shared memory; a ray that needs more ends and the call returns
                                    MC_ERR_STACK_OVERFLOW (builds keep every 4-wide tree within 64) */
-    int32_t pad0;
+    int32_t trace_threads;      /* trace block size: 0 or 256 (the default), or 128 (7 resident blocks per SM
+                                   when the stack's shared memory allows: single-scene renders without
+                                   density grids, reference intersector; other launches keep 256).
+                                   Images do not depend on it */
 } mc_render_params;
 
 enum {
@@ -638,11 +641,16 @@ MC_API mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_
 /* Reset the per-pixel XORWOW states (PT:2865-2871 init_rng_kernel). */
 MC_API mc_status mc_rng_reset(mc_context* ctx, int32_t width, int32_t height, uint64_t seed);
 
-/* Sets params' trace variant (persistent), refill_threshold and use_graph to
- * the fastest for the first wave that rendering params traces (its size,
- * samples per wave and spp as given), timed on this scene and BVH. Cached per
- * (device, layout, scene size class, wave size class); the image does not
- * depend on the choice. budget_ms bounds the tuning time (0 = 2000). */
+/* Sets params' launch configuration to the fastest found by timing real
+ * waves of this render on this scene and BVH: the trace variant (persistent
+ * or plain) and refill_threshold; the trace block shape (trace_threads 256,
+ * or 128 with stack_entries cut to what the 4-wide tree can need, 3 per
+ * level, when that lets 7 blocks share an SM); the queue capacity, as
+ * samples_per_wave (a wave's queues hold width x height x samples_per_wave
+ * entries: the automatic choice, or twice it while spp and about 64M paths
+ * allow; compared per sample); and use_graph. Cached per (device, layout,
+ * scene size class, image size class, spp class); the image does not depend
+ * on any choice. budget_ms bounds the tuning time (0 = 2000). */
 MC_API mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene,
                              mc_render_params* params, int32_t budget_ms);
 

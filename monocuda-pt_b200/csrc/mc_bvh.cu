@@ -1558,6 +1558,7 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         release();
         // a visit pushes at most 3 siblings: the traversal stack must hold 3 per level
         greedy = n == 0 && 3 * levels <= MC_STACK_CAPACITY;
+        bvh->wide_levels = greedy ? levels : -1;
         if (!greedy && tree) {
             cudaFree(rootOf);
             return MC_ERR_UNSUPPORTED;

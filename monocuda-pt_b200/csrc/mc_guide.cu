@@ -56,10 +56,19 @@ constexpr int iW1 = 0;
 constexpr int iW2 = iW1 + kHid * kIn * 2;
 constexpr int iW3 = iW2 + kHid * kHid * 2;
 constexpr int iW4 = iW3 + kHid * kHid * 2;
-constexpr int iE = iW4 + kOutPad * kHid * 2;
-constexpr int iH = iE + kTile * kIn * 2;
-constexpr int iBias = iH + kTile * kHid * 2;
-constexpr int kInferSmem = iBias + (3 * kHid + kOutPad) * 4;
+// kInferGroups warpgroups per CTA share one copy of the weights; each has its
+// own tile buffer (the encoded inputs X0, then in place each hidden layer's
+// activations once the MMA that read the previous contents has finished) and
+// its own 64 TMEM columns, so while one group waits on its MMA the others run
+// their epilogues.
+constexpr int kInferGroups = 4;
+constexpr int iBias = iW4 + kOutPad * kHid * 2;
+constexpr int iTiles = iBias + (3 * kHid + kOutPad) * 4 + 64;  // 64: keeps the tile buffers 128-byte aligned
+constexpr int kInferTileBytes = kTile * kIn * 2;
+constexpr int kInferSmem = iTiles + kInferGroups * kInferTileBytes;
+static_assert(iTiles % 128 == 0 && kInferTileBytes % 128 == 0, "operand buffers must stay aligned");
+static_assert(kTile * kHid * 2 <= kInferTileBytes, "the activations fit the input buffer");
+static_assert(kInferSmem <= 232448, "inference CTA exceeds the shared memory of one CTA");
 // training
 constexpr int tW1 = 0;
 constexpr int tW2 = tW1 + kHid * kIn * 2;
@@ -82,7 +91,7 @@ static_assert(kTile * kIn * 2 <= 160 * kTile * 2, "X0 must fit the transposed bu
 
 // TMEM columns of the training kernel
 constexpr uint32_t cR = 0, cG1 = 64, cG2 = 224, cG3 = 304, cG4 = 384, kTrainCols = 512;
-constexpr uint32_t kInferCols = 64;
+constexpr uint32_t kInferCols = 64 * kInferGroups;
 
 struct GuideInferArgs {
     const bf16* blob;
@@ -193,9 +202,34 @@ __device__ __forceinline__ void load_bias(float* sb, const float* master) {
     }
 }
 
-// TMEM address of column c of this warp's 32-lane slice.
+// TMEM address of column c of this warp's 32-lane slice (warp w of a
+// warpgroup reads lanes 32 (w % 4) .. 32 (w % 4) + 31).
 __device__ __forceinline__ uint32_t tcol(uint32_t base, uint32_t c) {
-    return base + ((uint32_t)(threadIdx.x & ~31) << 16) + c;
+    return base + ((uint32_t)(threadIdx.x & 96) << 16) + c;
+}
+
+// Barrier of the 128 threads of warpgroup g (named barrier 1 + g).
+__device__ __forceinline__ void wg_sync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+
+__device__ __forceinline__ void wg_sync_operands(int g) {
+    fence_async_smem();
+    fence_before_sync();
+    wg_sync(g);
+    fence_after_sync();
+}
+
+// The group's first thread waits for its committed MMAs; the group learns the outcome.
+__device__ __forceinline__ bool wg_wait_mma(int g, uint64_t* bar, uint32_t& phase, int* sFlag, int* err) {
+    if ((threadIdx.x & 127) == 0) {
+        bool ok = mbar_wait(bar, phase, kWaitLimit);
+        *sFlag = ok ? 0 : 1;
+        if (!ok) atomicOr(err, MC_DEVERR_TIMEOUT);
+    }
+    wg_sync(g);
+    fence_after_sync();
+    if (*sFlag) return false;
+    phase ^= 1u;
+    return true;
 }
 
 // Encodes one query row into the K-major X0 operand.
@@ -297,16 +331,16 @@ __device__ __forceinline__ void store_bf16(unsigned char* base, uint32_t off, fl
 // ---------------------------------------------------------------------------
 // Inference
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_guide_infer(GuideInferArgs a) {
+__global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInferArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bars[kInferGroups];
     __shared__ uint32_t tbase;
-    __shared__ int sFlag;
-    const int tid = threadIdx.x, row = tid;
+    __shared__ int sFlags[kInferGroups];
+    const int tid = threadIdx.x, g = tid >> 7, row = tid & 127;
     if ((tid >> 5) == 0) tmem_alloc(&tbase, kInferCols);
-    if (tid == 0) {
-        mbar_init(&bar, 1);
-        sFlag = 0;
+    if (tid < kInferGroups) {
+        mbar_init(&bars[tid], 1);
+        sFlags[tid] = 0;
     }
     load_kmaj(sm + iW1, a.blob + bW1, kHid, kIn);
     load_kmaj(sm + iW2, a.blob + bW2, kHid, kHid);
@@ -315,13 +349,18 @@ __global__ void __launch_bounds__(128) k_guide_infer(GuideInferArgs a) {
     float* sb = reinterpret_cast<float*>(sm + iBias);
     load_bias(sb, a.master);
     sync_operands();
-    const uint32_t R = tbase;
+    const uint32_t R = tbase + 64u * (uint32_t)g;
     const uint32_t s0 = smem_u32(sm);
+    const uint32_t sX = s0 + iTiles + (uint32_t)g * kInferTileBytes;
+    unsigned char* bufX = sm + iTiles + g * kInferTileBytes;
+    uint64_t* bar = &bars[g];
+    int* sFlag = &sFlags[g];
     const uint32_t id64 = idesc_bf16(128, kHid), id48 = idesc_bf16(128, kOutPad);
     const int n = a.count ? min(*a.count, a.capacity) : a.n;
     uint32_t phase = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile * kTile < n; tile += gridDim.x) {
+    // the groups take tiles in turn; from here on a group synchronises only itself
+    for (int tile = blockIdx.x * kInferGroups + g; tile * kTile < n; tile += gridDim.x * kInferGroups) {
         const int q = tile * kTile + row;
         const bool valid = q < n;
         float coord[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -350,34 +389,34 @@ __global__ void __launch_bounds__(128) k_guide_infer(GuideInferArgs a) {
             coord[2] = (pz - a.loz) * a.invz;
             coord[3] = dx; coord[4] = dy; coord[5] = dz;
         }
-        encode_row(sm + iE, row, coord);
-        sync_operands();
-        if (tid == 0) {
-            gemm_k(R, s0 + iE, s0 + iW1, kIn, id64, 0);
-            commit(&bar);
+        encode_row(bufX, row, coord);
+        wg_sync_operands(g);
+        if (row == 0) {
+            gemm_k(R, sX, s0 + iW1, kIn, id64, 0);
+            commit(bar);
         }
-        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        epi_hidden(R, sb, sm + iH, row);
-        sync_operands();
-        if (tid == 0) {
-            gemm_k(R, s0 + iH, s0 + iW2, kHid, id64, 0);
-            commit(&bar);
+        if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
+        epi_hidden(R, sb, bufX, row);  // the MMA that read X0 is done: H1 goes in its place
+        wg_sync_operands(g);
+        if (row == 0) {
+            gemm_k(R, sX, s0 + iW2, kHid, id64, 0);
+            commit(bar);
         }
-        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        epi_hidden(R, sb + kHid, sm + iH, row);
-        sync_operands();
-        if (tid == 0) {
-            gemm_k(R, s0 + iH, s0 + iW3, kHid, id64, 0);
-            commit(&bar);
+        if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
+        epi_hidden(R, sb + kHid, bufX, row);
+        wg_sync_operands(g);
+        if (row == 0) {
+            gemm_k(R, sX, s0 + iW3, kHid, id64, 0);
+            commit(bar);
         }
-        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        epi_hidden(R, sb + 2 * kHid, sm + iH, row);
-        sync_operands();
-        if (tid == 0) {
-            gemm_k(R, s0 + iH, s0 + iW4, kHid, id48, 0);
-            commit(&bar);
+        if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
+        epi_hidden(R, sb + 2 * kHid, bufX, row);
+        wg_sync_operands(g);
+        if (row == 0) {
+            gemm_k(R, sX, s0 + iW4, kHid, id48, 0);
+            commit(bar);
         }
-        if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
+        if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
         float y[kOutPad];
         tmem_ld16(tcol(R, 0), y);
         tmem_ld16(tcol(R, 16), y + 16);
@@ -389,10 +428,11 @@ __global__ void __launch_bounds__(128) k_guide_infer(GuideInferArgs a) {
             float4* dst = reinterpret_cast<float4*>(a.mix + (size_t)out * kOut);
             for (int i = 0; i < kOut / 4; i++) dst[i] = make_float4(m[4 * i], m[4 * i + 1], m[4 * i + 2], m[4 * i + 3]);
         }
+        // the next tile's operand barrier (fenced) orders these TMEM reads before its MMA
     }
     fence_before_sync();
     __syncthreads();
-    if (!ok && tid == 0) mbar_wait(&bar, phase, kWaitLimit);  // let an overdue MMA finish before TMEM goes back
+    if (!ok && row == 0) mbar_wait(bar, phase, kWaitLimit);  // let an overdue MMA finish before TMEM goes back
     __syncthreads();
     if ((tid >> 5) == 0) tmem_dealloc(tbase, kInferCols);
 }
@@ -815,7 +855,7 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
     a.dirNormal = g->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
     a.mix = mixtures;
     a.err = g->ctx->d_error;
-    k_guide_infer<<<2 * g->ctx->sm_count, kTile, kInferSmem, s>>>(a);
+    k_guide_infer<<<g->ctx->sm_count, kTile * kInferGroups, kInferSmem, s>>>(a);
     MC_CUDA(cudaGetLastError());
     return MC_OK;
 }
@@ -971,7 +1011,8 @@ mc_status mc_guide_infer(mc_guide* g, const float* d_queries, int32_t n, float* 
     a.mix = d_mixtures;
     a.err = ctx->d_error;
     int tiles = (n + kTile - 1) / kTile;
-    k_guide_infer<<<std::min(tiles, 2 * ctx->sm_count), kTile, kInferSmem, ctx->stream>>>(a);
+    k_guide_infer<<<std::min((tiles + kInferGroups - 1) / kInferGroups, ctx->sm_count), kTile * kInferGroups, kInferSmem,
+                    ctx->stream>>>(a);
     MC_CUDA(cudaGetLastError());
     return flags_of(ctx);
 }

@@ -155,38 +155,44 @@ mc_status mc_render_host(mc_context* ctx, const mc_triangle* tris, int32_t n_tri
     return st;
 }
 
-// Picks the trace variant (persistent or plain), the refill threshold and CUDA
-// graph replay by timing the first wave that a render of these params traces
-// (full resolution, the wave's samples per pixel, the scene's own BVH): every
-// candidate once untimed, then three timed rounds taken in turn, each
-// candidate keeping its fastest time. Results are cached per (device, layout,
-// scene size class, wave size class): later calls in the same class return at
-// once. None of the choices changes the image. budget_ms bounds the tuning
-// time (0 = 2000); candidates not timed by then are not chosen.
+// Picks the launch configuration by timing real waves of this render (full
+// resolution, the scene's own BVH), in stages: the trace variant and refill
+// threshold; the trace block shape and stack; the samples per wave (the queue
+// capacity); CUDA graph replay. In each stage every candidate runs once
+// untimed, then up to three timed rounds in turn, each keeping its fastest
+// time per sample. Results are cached per (device, layout, scene size class,
+// image size class, spp class): later calls in the same class return at once.
+// None of the choices changes the image. budget_ms bounds the tuning time
+// (0 = 2000); stages not reached by then keep their defaults.
 mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* scene, mc_render_params* params, int32_t budget_ms) {
     if (!ctx || !bvh || !scene || !params) return mc::set_error(MC_ERR_INVALID, "mc_autotune: null argument");
     if (params->width < 1 || params->height < 1) return mc::set_error(MC_ERR_INVALID, "mc_autotune: empty image");
     if (budget_ms <= 0) budget_ms = 2000;
-    struct Choice { int persistent, refill, graph; };
+    struct Choice { int persistent, refill, graph, spw, threads, stack; };
     static std::mutex mu;
-    static std::map<std::array<long long, 4>, Choice> cache;
+    static std::map<std::array<long long, 5>, Choice> cache;
     auto log2c = [](long long v) { int b = 0; while (v > 1) { v >>= 1; b++; } return (long long)b; };
     const int k = mc::wave_samples(params);
     const long long pixels = (long long)params->width * params->height;
-    const std::array<long long, 4> key = {(long long)ctx->device, (long long)bvh->layout, log2c(bvh->n), log2c(pixels * k)};
+    const std::array<long long, 5> key = {(long long)ctx->device, (long long)bvh->layout, log2c(bvh->n), log2c(pixels),
+                                          log2c(std::max(1, params->spp))};
+    auto apply = [&](const Choice& c) {
+        params->persistent = c.persistent;
+        params->refill_threshold = c.refill;
+        params->use_graph = c.graph;
+        params->samples_per_wave = c.spw;
+        params->trace_threads = c.threads;
+        params->stack_entries = c.stack;
+    };
     {
         std::lock_guard<std::mutex> lock(mu);
         auto it = cache.find(key);
         if (it != cache.end()) {
-            params->persistent = it->second.persistent;
-            params->refill_threshold = it->second.refill;
-            params->use_graph = it->second.graph;
+            apply(it->second);
             return MC_OK;
         }
     }
     mc_render_params probe = *params;
-    probe.spp = k;
-    probe.samples_per_wave = k;
     probe.first_sample = 0;
     probe.instrument = 0;
     float* dAcc = nullptr;
@@ -194,23 +200,27 @@ mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* s
         cudaGetLastError();
         return mc::set_error(MC_ERR_OOM, "mc_autotune: allocation failed");
     }
-    std::vector<Choice> cands = {{1, 8, 0}, {1, 4, 0}, {1, 12, 0}, {1, 16, 0}, {1, 24, 0}, {0, 8, 0}};
     auto t0 = std::chrono::steady_clock::now();
     auto elapsed = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
+    // one wave of c.spw samples; *ms: host time per sample
     auto run = [&](const Choice& c, float* ms) -> mc_status {
         probe.persistent = c.persistent;
         probe.refill_threshold = c.refill;
         probe.use_graph = c.graph;
+        probe.spp = c.spw;
+        probe.samples_per_wave = c.spw;
+        probe.trace_threads = c.threads;
+        probe.stack_entries = c.stack;
         mc_render_stats rs;
         auto a = std::chrono::steady_clock::now();
         mc_status st = mc_render_wavefront(ctx, bvh, scene, &probe, dAcc, &rs);
         if (cudaDeviceSynchronize() != cudaSuccess && st == MC_OK) st = mc::set_error(MC_ERR_CUDA, "mc_autotune: render failed");
-        if (ms) *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - a).count();
+        if (ms) *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - a).count() / c.spw;
         return st;
     };
-    // warm-up of every candidate (kernel loads, buffers, graph capture), then timed rounds
-    auto tune = [&](std::vector<Choice>& cs, std::vector<float>& best) -> mc_status {
-        best.assign(cs.size(), 1e30f);
+    // every candidate once (kernel loads, buffers, graph capture), then timed rounds; returns the fastest
+    auto tune = [&](const std::vector<Choice>& cs, size_t* bestIdx) -> mc_status {
+        std::vector<float> best(cs.size(), 1e30f);
         for (const Choice& c : cs) {
             mc_status st = run(c, nullptr);
             if (st != MC_OK) return st;
@@ -223,27 +233,55 @@ mc_status mc_autotune(mc_context* ctx, const mc_bvh* bvh, const mc_scene_view* s
                 best[i] = std::min(best[i], ms);
             }
         }
+        size_t b = 0;
+        for (size_t i = 1; i < cs.size(); i++)
+            if (best[i] < best[b]) b = i;
+        *bestIdx = best[b] < 1e30f ? b : 0;
         return MC_OK;
     };
-    std::vector<float> best;
-    mc_status st = tune(cands, best);
-    Choice bestC = {params->persistent, params->refill_threshold > 0 ? params->refill_threshold : 8, params->use_graph};
-    if (st == MC_OK) {
-        size_t b = 0;
-        for (size_t i = 1; i < cands.size(); i++)
-            if (best[i] < best[b]) b = i;
-        if (best[b] < 1e30f) bestC = cands[b];
-        // graph replay of the winner against the winner as launched
-        std::vector<Choice> pair = {bestC, bestC};
-        pair[1].graph = 1;
-        std::vector<float> bp;
-        if ((st = tune(pair, bp)) == MC_OK && bp[1] < bp[0]) bestC = pair[1];
+    Choice bestC = {params->persistent, params->refill_threshold > 0 ? params->refill_threshold : 8, params->use_graph,
+                    k, 256, 0};
+    mc_status st = MC_OK;
+    size_t b = 0;
+    // 1: persistence and refill threshold
+    std::vector<Choice> cands;
+    for (int r : {8, 4, 12, 16, 24}) cands.push_back({1, r, 0, k, 256, 0});
+    cands.push_back({0, 8, 0, k, 256, 0});
+    if ((st = tune(cands, &b)) == MC_OK) bestC = cands[b];
+    // 2: 128-thread blocks with the stack the 4-wide tree needs (3 entries per
+    // level, rounded up to 8): 7 blocks per SM fit in shared memory up to 56
+    // entries (persistent renders of wide layouts without density grids)
+    const int need = bvh->wide_levels > 0 ? ((3 * bvh->wide_levels + 7) / 8) * 8 : 999;
+    if (st == MC_OK && elapsed() < budget_ms && bestC.persistent && bvh->layout != MC_BVH_LAYOUT_BINARY && need <= 56 &&
+        !(scene->has_medium & MC_MEDIUM_GRID) && params->intersector == MC_ISECT_REFERENCE) {
+        Choice small = bestC;
+        small.threads = 128;
+        small.stack = need;
+        std::vector<Choice> pair = {bestC, small};
+        if ((st = tune(pair, &b)) == MC_OK) bestC = pair[b];
+    }
+    // 3: queue capacity (samples per wave): the automatic choice against twice it
+    const long long maxPaths = 64ll << 20;
+    if (st == MC_OK && elapsed() < budget_ms && params->rng == MC_RNG_PHILOX && params->samples_per_wave == 0 &&
+        2 * k <= params->spp && pixels * 2 * k <= maxPaths) {
+        Choice twice = bestC;
+        twice.spw = 2 * k;
+        std::vector<Choice> pair = {bestC, twice};
+        if ((st = tune(pair, &b)) == MC_OK) bestC = pair[b];
+    }
+    // 4: graph replay of the winner against the winner as launched
+    if (st == MC_OK && elapsed() < budget_ms) {
+        Choice g = bestC;
+        g.graph = 1;
+        std::vector<Choice> pair = {bestC, g};
+        if ((st = tune(pair, &b)) == MC_OK) bestC = pair[b];
     }
     cudaFree(dAcc);
     if (st != MC_OK) return st;
-    params->persistent = bestC.persistent;
-    params->refill_threshold = bestC.refill;
-    params->use_graph = bestC.graph;
+    // an explicit samples_per_wave of the caller stays as it was
+    if (params->samples_per_wave != 0) bestC.spw = params->samples_per_wave;
+    else if (bestC.spw == k) bestC.spw = 0;
+    apply(bestC);
     std::lock_guard<std::mutex> lock(mu);
     cache[key] = bestC;
     return MC_OK;

@@ -117,9 +117,9 @@ struct mc_context {
     // launch configurations measured on this context's device (occupancy of a
     // kernel variant, its opt-in shared-memory size), filled on first use; a
     // context is used by one host thread at a time, so these need no lock
-    int trace_blocks[128] = {};
-    int trace_blocks_smem[128] = {};     // shared-memory bytes trace_blocks[k] was measured with
-    int trace_smem_attr[128] = {};       // dynamic shared memory the variant has been opted in to
+    int trace_blocks[144] = {};
+    int trace_blocks_smem[144] = {};     // shared-memory bytes trace_blocks[k] was measured with
+    int trace_smem_attr[144] = {};       // dynamic shared memory the variant has been opted in to
     int shade_blocks[3] = {};            // Philox, XORWOW, guided
     bool guide_attrs_set = false;        // the guide kernels' shared-memory opt-in is done
 };
@@ -142,6 +142,7 @@ struct mc_bvh {
     void* prims = nullptr;             // leaf-ordered primitive records, 48 B each
     void* wide_nodes = nullptr;        // 4-wide nodes, 128 B each (layout MC_BVH_LAYOUT_WIDE4)
     long long wide_count = 0;
+    int wide_levels = -1;              // levels of the greedy 4-wide tree (a ray's stack holds <= 3 per level), -1 unknown
     void* wide_prims = nullptr;        // primitive records in reference visit (rank) order
     // reference representation (optional)
     uint32_t* codes = nullptr;

@@ -132,6 +132,7 @@ struct TraceArgs {
     unsigned long long* counts;  // [0] node visits, [1] leaf tests (counting variant)
     int oneShot;                 // plain mode: one ray per thread, no refill
     int stackCap;                // traversal stack entries per lane, <= MC_STACK_CAPACITY (0: all)
+    int threads;                 // block size asked for: 128 or 256 (0: 256)
     int queueCap;                // entries the extend and shadow queues hold (counts past it are clamped)
     // launches with gridded media (MC_MEDIUM_GRID): per shadow slot, the
     // distance of each medium crossing and, for back faces, the homogeneous
@@ -279,12 +280,16 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 // BATCH: rays of several scenes share the launch; each lane reads its ray's
 // scene from the wave table. A single-scene launch reads the scene from the
 // kernel parameters instead, which costs no registers.
+// THREADS: 256 (3 resident blocks of up to 85 registers, the default) or 128
+// (7 resident blocks of up to 73 registers: 28 warps per SM instead of 24
+// when the traversal stack is short enough for 7 blocks' shared memory; a
+// variant the autotuner may pick for single-scene launches).
 #ifndef MC_TRACE_MIN_BLOCKS
 #define MC_TRACE_MIN_BLOCKS 3
 #endif
 constexpr int kTraceThreads = 256;
-template <int ISECT, int MED, bool COUNT, int LAY, bool BATCH>
-__global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
+template <int ISECT, int MED, bool COUNT, int LAY, bool BATCH, int THREADS = kTraceThreads>
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? MC_TRACE_MIN_BLOCKS : 7) k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
     const unsigned ltmask = lanemask_lt();
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(kTraceThreads, MC_TRACE_MIN_BLOCKS) k_trace(Tr
     const int total = extCount + shCount;
 #if MC_SMEM_STACK
     extern __shared__ int traceStack[];
-    const SharedStack<kTraceThreads> stack{traceStack + threadIdx.x};
+    const SharedStack<THREADS> stack{traceStack + threadIdx.x};
 #else
     int stackMem[MC_STACK_CAPACITY];
     const LocalStack stack{stackMem};
@@ -1142,9 +1147,9 @@ __global__ void k_init_xorwow(curandState* states, int pixels, unsigned long lon
     if (p < pixels) curand_init(seed, p, 0, &states[p]);  // PT:2870
 }
 
-int occupancy_blocks(const void* fn, int sms, size_t smem = 0) {
+int occupancy_blocks(const void* fn, int sms, size_t smem = 0, int threads = 256) {
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
     if (per < 1) per = 1;
     return per * sms;
 }
@@ -1162,6 +1167,14 @@ TraceKernel trace_kernel(bool batch, int layout, bool count, int medium, int ise
                                                      {MC_TK(0, true), MC_TK(1, true), MC_TK(2, true)}};
     return table[batch ? 1 : 0][layout][count ? 1 : 0][medium][isect ? 1 : 0];
 }
+// The 128-thread variant, compiled for single-scene launches of the reference
+// intersector without counters or density grids; [layout][medium kind].
+TraceKernel trace_kernel_128(int layout, int medium) {
+    static const TraceKernel table[3][2] = {{k_trace<0, 0, false, 0, false, 128>, k_trace<0, 1, false, 0, false, 128>},
+                                            {k_trace<0, 0, false, 1, false, 128>, k_trace<0, 1, false, 1, false, 128>},
+                                            {k_trace<0, 0, false, 2, false, 128>, k_trace<0, 1, false, 2, false, 128>}};
+    return table[layout][medium];
+}
 
 // Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
 // pull rays from the work counter. Plain (PT:3376-3397): the same kernel with
@@ -1173,24 +1186,29 @@ void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, int
     TraceArgs t = t0;
     t.oneShot = persistent ? 0 : 1;
     if (t.stackCap <= 0 || t.stackCap > MC_STACK_CAPACITY) t.stackCap = MC_STACK_CAPACITY;
-    // the shared-memory stack holds stackCap entries per lane
-    const int smem = MC_SMEM_STACK ? kTraceThreads * t.stackCap * (int)sizeof(int) : 0;
     const bool batch = t.sceneOf != nullptr;
-    TraceKernel fn = trace_kernel(batch, layout, count, medium, isect);
-    const int key = medium + 3 * (isect ? 1 : 0) + 6 * (count ? 1 : 0) + 12 * (batch ? 1 : 0) + 24 * layout;  // < 72
+    // the 128-thread variant where it is compiled, else 256 threads
+    const bool small = t.threads == 128 && !batch && !count && isect == 0 && medium < 2;
+    const int threads = small ? 128 : kTraceThreads;
+    // the shared-memory stack holds stackCap entries per lane
+    const int smem = MC_SMEM_STACK ? threads * t.stackCap * (int)sizeof(int) : 0;
+    TraceKernel fn = small ? trace_kernel_128(layout, medium) : trace_kernel(batch, layout, count, medium, isect);
+    const int key = medium + 3 * (isect ? 1 : 0) + 6 * (count ? 1 : 0) + 12 * (batch ? 1 : 0) + 24 * layout +
+                    72 * (small ? 1 : 0);  // < 144
     if (smem > 48 * 1024 && ctx->trace_smem_attr[key] < smem) {
         cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         ctx->trace_smem_attr[key] = smem;
     }
-    int blocks = std::max(1, plainBlocks);
+    // plain launches: one ray per thread (plainBlocks counts 256-thread blocks)
+    int blocks = std::max(1, small ? 2 * plainBlocks : plainBlocks);
     if (persistent) {
         if (!ctx->trace_blocks[key] || ctx->trace_blocks_smem[key] != smem) {
-            ctx->trace_blocks[key] = occupancy_blocks((const void*)fn, ctx->sm_count, smem);
+            ctx->trace_blocks[key] = occupancy_blocks((const void*)fn, ctx->sm_count, smem, threads);
             ctx->trace_blocks_smem[key] = smem;
         }
         blocks = ctx->trace_blocks[key];
     }
-    fn<<<blocks, kTraceThreads, smem, stream>>>(t);
+    fn<<<blocks, threads, smem, stream>>>(t);
 }
 
 }  // namespace
@@ -1414,6 +1432,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.err = ctx->d_error;
     ta.queueCap = queueCap;
     ta.stackCap = p0.stack_entries;
+    ta.threads = p0.trace_threads;
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
     if (sameScene) {
@@ -1719,6 +1738,8 @@ mc_status check_params(const mc_render_params* p, const mc_scene_view* v) {
     if (p->queue_capacity < 0) return set_error(MC_ERR_INVALID, "render: queue_capacity must be >= 0");
     if (p->stack_entries < 0 || p->stack_entries > MC_STACK_CAPACITY)
         return set_error(MC_ERR_INVALID, "render: stack_entries must be in [0, %d]", MC_STACK_CAPACITY);
+    if (p->trace_threads != 0 && p->trace_threads != 128 && p->trace_threads != 256)
+        return set_error(MC_ERR_INVALID, "render: trace_threads must be 0, 128 or 256");
     if (p->env_sampling != MC_ENV_SAMPLE_CDF && p->env_sampling != MC_ENV_SAMPLE_ALIAS)
         return set_error(MC_ERR_INVALID, "render: unknown environment sampling mode");
     if (p->env_sampling == MC_ENV_SAMPLE_ALIAS && v->env.enabled && !env_alias_table(v->env))
@@ -1842,12 +1863,21 @@ mc_status mc_render_batch(mc_context* ctx, const mc_bvh* bvh, const mc_batch_ite
                               bvh->layout != MC_BVH_LAYOUT_BINARY ? bvh->wide_roots[i] : bvh->bin_roots[i], i};
     }
     if (capacity >= (1ll << 30)) return mc::set_error(MC_ERR_INVALID, "mc_render_batch: too many paths per wave");
-    // samples per wave: an item's own setting, else one for all items that
-    // keeps a wave within about 32M paths (at most 16)
-    const long long autoSpw = std::max(1ll, std::min(16ll, (32ll << 20) / std::max(1ll, capacity)));
+    // samples per wave: an item's own setting, else balanced so that the
+    // batch's paths fill W waves of about 32M paths each and every item ends
+    // within those W waves: item i traces ceil(spp_i / W) samples per wave
+    // (at least 1, at most 16). An item with many samples then shares every
+    // wave instead of trailing alone through small waves after the others
+    // finished; images do not depend on it (each pixel adds its samples in
+    // sample order).
+    long long totalPaths = 0;
+    for (int i = 0; i < count; i++)
+        totalPaths += (long long)items[i].params.width * items[i].params.height * std::max(1, items[i].params.spp);
+    const long long waves = std::max(1ll, (totalPaths + (32ll << 20) - 1) / (32ll << 20));
     for (int i = 0; i < count; i++) {
         const int want = items[i].params.samples_per_wave;
-        its[i].spw = want > 0 ? want : want == 0 ? (int)autoSpw : 1;
+        const long long balanced = std::max(1ll, std::min(16ll, (std::max(1, items[i].params.spp) + waves - 1) / waves));
+        its[i].spw = want > 0 ? want : want == 0 ? (int)balanced : 1;
         if ((long long)items[i].params.width * items[i].params.height * its[i].spw >= (1ll << 30)) its[i].spw = 1;
     }
     return mc::render_items(ctx, bvh, its.data(), count, use_graph != 0, stats);

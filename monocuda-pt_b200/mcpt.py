@@ -142,7 +142,7 @@ class RenderParams(C.Structure):
                 ("seed", C.c_uint64), ("intersector", C.c_int32), ("disable_clamp", C.c_int32),
                 ("queue_capacity", C.c_int32), ("refill_threshold", C.c_int32), ("use_graph", C.c_int32),
                 ("instrument", C.c_int32), ("samples_per_wave", C.c_int32), ("env_sampling", C.c_int32),
-                ("stack_entries", C.c_int32), ("pad0", C.c_int32)]
+                ("stack_entries", C.c_int32), ("trace_threads", C.c_int32)]
 
 
 class GuideConfig(C.Structure):
@@ -705,7 +705,7 @@ def make_camera(width, height, look_from, look_at, vfov, focus, max_depth=8, spp
 
 def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RNG_PHILOX, seed=1234, first_sample=0,
                   intersector=ISECT_REFERENCE, disable_clamp=False, refill_threshold=0, use_graph=False, instrument=0,
-                  samples_per_wave=0, env_sampling=0, queue_capacity=0, stack_entries=0):
+                  samples_per_wave=0, env_sampling=0, queue_capacity=0, stack_entries=0, trace_threads=0):
     p = RenderParams()
     p.camera = camera
     p.width, p.height, p.spp, p.first_sample, p.max_depth = width, height, spp, first_sample, max_depth
@@ -721,6 +721,7 @@ def render_params(camera, width, height, spp, max_depth, persistent=True, rng=RN
     p.samples_per_wave = samples_per_wave
     p.env_sampling = env_sampling
     p.stack_entries = stack_entries
+    p.trace_threads = trace_threads
     return p
 
 
