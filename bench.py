@@ -59,6 +59,11 @@ def parse():
                          "free of the autotuner's probe launches)")
     ap.add_argument("--resolution", default="",
                     help="WxH instead of the workload's 1920x1080 (same view, e.g. 480x270 for small ncu captures)")
+    ap.add_argument("--trace-threads", type=int, default=0,
+                    help="trace block size 128 or 256 (0 = the autotuner's choice, or 256 with a fixed --refill)")
+    ap.add_argument("--stack-entries", type=int, default=0,
+                    help="traversal stack entries per lane (0 = the autotuner's choice, or 64 with a fixed --refill; "
+                         "-1 = what the 4-wide tree can need, 3 per level)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-1m", action="store_true",
                     help="skip the second, ~1M-triangle line (level-7 icospheres, 983,056 triangles)")
@@ -79,7 +84,10 @@ def parse():
     ap.add_argument("--guide-dir", default="normal", choices=["normal", "ray"],
                     help="direction input of the guide: the face normal or the arriving ray's direction")
     ap.add_argument("--mlp-items", type=int, default=1 << 20)
-    ap.add_argument("--server-rates", type=float, nargs="+", default=[1, 4, 16, 64], help="arrival rates (requests/s)")
+    ap.add_argument("--server-rates", type=float, nargs="+", default=[1, 2, 4, 8, 16, 32, 64],
+                    help="arrival rates (requests/s)")
+    ap.add_argument("--server-repeats", type=int, default=3,
+                    help="runs of each rate's trace (the schedule depends on host timing); medians and ranges reported")
     ap.add_argument("--server-requests", type=int, default=64,
                     help="requests per arrival rate (at most; max(24, 16 x rate) at low rates)")
     ap.add_argument("--server-sps", type=int, default=16, help="samples per server step")
@@ -299,6 +307,14 @@ def run_ours(args):
                                refill_threshold=args.refill, samples_per_wave=args.samples_per_wave)
     if args.refill <= 0:
         mcpt.check(ctx.lib.mc_autotune(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(tuned), 4000))
+    if args.trace_threads:
+        tuned.trace_threads = args.trace_threads
+    if args.stack_entries > 0:
+        tuned.stack_entries = args.stack_entries
+    elif args.stack_entries < 0:
+        # what the 4-wide tree can need: 3 entries per level, rounded up to 8
+        lv = bvh.info().wide_levels
+        tuned.stack_entries = min(64, ((3 * lv + 7) // 8) * 8) if lv > 0 else 0
 
     def params(step, instrument=0):
         return mcpt.render_params(scene.camera, W, H, S, 8, persistent=bool(tuned.persistent), rng=mcpt.RNG_PHILOX,
@@ -456,6 +472,7 @@ def run_ours(args):
         "ms_per_step": round(ms_max / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "config": dict(WORKLOAD, spp=K * S * world, spp_per_step=S, bvh_layout=args.layout, bvh_builder=args.builder,
+                       bvh_wide_levels=int(bvh.info().wide_levels),
                        autotuned={"persistent": int(tuned.persistent), "refill_threshold": int(tuned.refill_threshold),
                                   "samples_per_wave": int(tuned.samples_per_wave) or "automatic",
                                   "trace_threads": int(tuned.trace_threads) or 256,
@@ -708,6 +725,27 @@ def run_guiding(args):
                 reached = g_ms
             break
     steps = guide.steps()
+    # where a guided wave's time goes: one more chunk with every launch timed
+    # by phase (instrument bit 1; untimed above), and the same for plain
+    split = {}
+    for name, g in (("guided", guide), ("plain", None)):
+        st = mcpt.RenderStats()
+        p = params(chunk, 40_000_000)
+        p.instrument = 2
+        tmp.zero_()
+        torch.cuda.synchronize()
+        if g is None:
+            mcpt.check(ctx.lib.mc_render_wavefront(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), tmp.data_ptr(),
+                                                   C.byref(st)))
+        else:
+            mcpt.check(ctx.lib.mc_render_guided(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), g.handle, 1,
+                                                tmp.data_ptr(), C.byref(st)))
+        per = 1.0 / chunk
+        split[name] = {"ms_per_spp": round(st.render_ms * per, 3), "trace": round(st.trace_ms * per, 3),
+                       "shade": round(st.shade_ms * per, 3), "guide_inference": round(st.guide_infer_ms * per, 3),
+                       "guide_training": round(st.guide_train_ms * per, 3)}
+        split[name]["other"] = round(split[name]["ms_per_spp"] - sum(v for k, v in split[name].items()
+                                                                     if k != "ms_per_spp"), 3)
 
     mlp = mlp_throughput(ctx, guide)
     guide.close()
@@ -721,7 +759,7 @@ def run_guiding(args):
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
-           "plain_curve": plain_curve, "guided_curve": g_curve,
+           "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,
            "mlp": mlp,
            "data": "synthetic (seeded procedural room)", "dtype": "bf16 MLP / f32 tracer"}
     print(json.dumps(out), flush=True)
@@ -830,22 +868,35 @@ def run_server(args):
     warm = [(0.0, k, 256, 256, 1, k % 2 == 0) for k in range(len(scenes))]
     serve(warm)
     baseline([(0.0, k, 256, 256, 1, False) for k in range(len(scenes))])
+    def summary(runs):
+        # runs: [(latencies, mrays)] of repeats -> median and range of p50, p99, Mrays/s
+        cols = {"p50_s": [pct(l, 0.5) for l, _ in runs], "p99_s": [pct(l, 0.99) for l, _ in runs],
+                "mrays": [m for _, m in runs]}
+        out = {}
+        for k, v in cols.items():
+            nd = 1 if k == "mrays" else 4
+            out[k] = round(statistics.median(v), nd)
+            out[k + "_range"] = [round(min(v), nd), round(max(v), nd)]
+        return out
+
     points = []
     for rate in args.server_rates:
         # the same trace for a rate whatever else is swept; fewer requests at low
         # rates, where the arrivals themselves take wall-clock time
         n_req = max(24, min(args.server_requests, int(16 * rate)))
         tr = trace(rate, n_req, 5 + int(round(rate * 1000)))
-        lat, mr = serve(tr)
         plain_tr = [(t, k, W, H, spp, False) for t, k, W, H, spp, _ in tr]
-        plat, pmr = serve(plain_tr)
-        blat, bmr = baseline(tr)
-        points.append({"lambda_per_s": rate, "requests": len(tr), "guided_requests": sum(1 for x in tr if x[5]),
-                       "p50_s": round(pct(lat, 0.5), 4), "p99_s": round(pct(lat, 0.99), 4), "mrays": round(mr, 1),
-                       "plain_only_p50_s": round(pct(plat, 0.5), 4), "plain_only_p99_s": round(pct(plat, 0.99), 4),
-                       "plain_only_mrays": round(pmr, 1),
-                       "baseline_p50_s": round(pct(blat, 0.5), 4), "baseline_p99_s": round(pct(blat, 0.99), 4),
-                       "baseline_mrays": round(bmr, 1)})
+        mixed, plain, base = [], [], []
+        for _ in range(max(1, args.server_repeats)):
+            mixed.append(serve(tr))
+            plain.append(serve(plain_tr))
+            base.append(baseline(tr))
+        point = {"lambda_per_s": rate, "requests": len(tr), "guided_requests": sum(1 for x in tr if x[5]),
+                 "repeats": len(mixed)}
+        point.update(summary(mixed))
+        point.update({"plain_only_" + k: v for k, v in summary(plain).items()})
+        point.update({"baseline_" + k: v for k, v in summary(base).items()})
+        points.append(point)
     st = srv.stats()
     out = {"metric": "served-render p50/p99 latency", "unit": "s", "higher_is_better": False, "n_gpus": 1,
            "workload": "render_server", "scenes": len(scenes),

@@ -247,6 +247,8 @@ typedef struct mc_bvh_info {
     int64_t node_bytes;         /* bytes of the traversal node array */
     int64_t prim_bytes;         /* bytes of the leaf-ordered triangle stream */
     mc_aabb scene_bounds;
+    int32_t wide_levels;        /* levels of the 4-wide tree; a ray's traversal stack holds at most
+                                   3 entries per level (0: binary layout or not known) */
 } mc_bvh_info;
 
 enum {
@@ -282,7 +284,8 @@ typedef struct mc_render_params {
     int32_t refill_threshold;   /* idle lanes before a warp refills (PT:3400 uses 8); 0 = 8 */
     int32_t use_graph;          /* capture each sample's bounce sequence in a CUDA graph */
     int32_t instrument;         /* bit 0: count node visits / leaf tests (counting kernel variant);
-                                   bit 1: time every trace launch with CUDA events on the context stream */
+                                   bit 1: time every trace, shade and guide launch with CUDA events on the
+                                   context stream */
     int32_t samples_per_wave;   /* samples traced together in one wave (counter-based RNG only; the XORWOW
                                    states advance sample by sample): 0 = automatic (up to 16, at most about
                                    32M paths per wave), 1 = one sample per wave. Images do not depend on it:
@@ -321,6 +324,9 @@ typedef struct mc_render_stats {
     int32_t trace_launches;     /* trace launches timed */
     int32_t kernel_launches;    /* library kernels launched by the call */
     int32_t error_flags;        /* device error word (MC_ERR_* bits) */
+    float shade_ms;             /* summed device time of the shade launches (instrument bit 1) */
+    float guide_infer_ms;       /* guided renders: guide inference launches (instrument bit 1) */
+    float guide_train_ms;       /* guided renders: record compaction and Adam steps (instrument bit 1) */
 } mc_render_stats;
 
 /* ------------------------------------------------------------------------- */

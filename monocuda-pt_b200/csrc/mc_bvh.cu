@@ -1915,6 +1915,7 @@ mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info) {
                                                              : bvh->node_bytes;
     info->prim_bytes = (long long)bvh->n * 48;
     info->scene_bounds = bvh->bounds;
+    info->wide_levels = bvh->layout != MC_BVH_LAYOUT_BINARY && bvh->wide_levels > 0 ? bvh->wide_levels : 0;
     return MC_OK;
 }
 

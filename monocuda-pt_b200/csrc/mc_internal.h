@@ -182,6 +182,7 @@ namespace mc {
 struct RenderTiming {
     float ms = 0.f;
     float trace_ms = 0.f;
+    float shade_ms = 0.f, infer_ms = 0.f, train_ms = 0.f;
     int trace_launches = 0;
     int kernel_launches = 0;
 };

@@ -1462,7 +1462,19 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     int* C = ctx->d_counters;
     const size_t counterBytes = (size_t)(MC_MAX_DEPTH_STATS + 1) * MC_COUNTERS_PER_DEPTH * sizeof(int);
     std::vector<cudaEvent_t> traceEvents;
-    auto traceEvent = [&]() {
+    // instrument bit 1: CUDA events around each timed launch, by phase
+    // (0 trace, 1 shade, 2 guide inference, 3 guide training with its record compaction)
+    std::vector<int> phaseOf;
+    auto phaseBegin = [&](int phase) {
+        if (!timeTrace) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, stream);
+        traceEvents.push_back(e);
+        phaseOf.push_back(phase);
+    };
+    auto phaseEnd = [&]() {
+        if (!timeTrace) return;
         cudaEvent_t e;
         cudaEventCreate(&e);
         cudaEventRecord(e, stream);
@@ -1521,9 +1533,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 t.sr = nee0[0]; t.sg = nee0[1]; t.sb = nee0[2];
             }
             if (grid && d > 0) MC_CUDA(cudaMemsetAsync(ta.vdefer, 0, sizeof(int), stream));
-            if (timeTrace) traceEvent();
+            phaseBegin(0);
             launch_trace(ctx, stream, t, layout, grid ? 2 : medium ? 1 : 0, isect, persistent, plainBlocks, countVisits);
-            if (timeTrace) traceEvent();
+            phaseEnd();
             launches++;
             if (grid && d > 0) {
                 RatioArgs r = ra;
@@ -1537,9 +1549,11 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 break;
             }
             if (guide) {
+                phaseBegin(2);
                 mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], slot(d) + 0, capacity,
                                                  w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.time, w.hits,
                                                  items[0].view->tri_hot, items[0].view->spheres, guide->mixtures);
+                phaseEnd();
                 if (gs != MC_OK) return gs;
                 launches++;
             }
@@ -1562,11 +1576,17 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 sd.rec = train ? guide->records : nullptr;
                 sd.recSlots = guide->cfg.train_vertices;
                 sd.dirNormal = guide->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
+                phaseBegin(1);
                 k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
+                phaseEnd();
             } else if (philox) {
+                phaseBegin(1);
                 k_shade<PhiloxRng, false><<<shadeBlocks[0], 256, 0, stream>>>(sd);
+                phaseEnd();
             } else {
+                phaseBegin(1);
                 k_shade<XorwowRng, false><<<shadeBlocks[1], 256, 0, stream>>>(sd);
+                phaseEnd();
             }
             launches++;
             if (deep && (d & 7) == 7 && d + 1 < maxD) {
@@ -1585,12 +1605,14 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                                                                       guide->rec_tiles, entries, slots, recStride,
                                                                       recPhase);
             if (train) {
+                phaseBegin(3);
                 const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
                 k_rec_scan<<<1, 1024, 0, stream>>>(guide->rec_tiles, tiles, guide->batch_count);
                 k_rec_write<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, w.sr, w.sg, w.sb, guide->records, guide->rec_tiles,
                                                                     entries, slots, recStride, recPhase, guide->batch,
                                                                     guide->cfg.batch_capacity * guide->cfg.train_steps *
                                                                         waveR);
+                phaseEnd();
                 launches += 2;
             }
         } else {
@@ -1602,9 +1624,11 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         if (guide && train) {
             // as many Adam steps per sample, on as many records each, as with
             // one sample per wave (a sample holds at most a record per pixel)
+            phaseBegin(3);
             mc_status gs = guide_train_device(guide, stream, guide->batch, guide->batch_count,
                                               guide->cfg.batch_capacity * guide->cfg.train_steps * waveR,
                                               guide->cfg.train_steps * waveR, wavePixels);
+            phaseEnd();
             if (gs != MC_OK) return gs;
             launches += 4 * guide->cfg.train_steps * waveR;
         }
@@ -1716,9 +1740,12 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         for (size_t i = 0; i + 1 < traceEvents.size(); i += 2) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, traceEvents[i], traceEvents[i + 1]);
-            if (tm) {
-                tm->trace_ms += ms;
-                tm->trace_launches++;
+            if (!tm) continue;
+            switch (phaseOf[i / 2]) {
+                case 0: tm->trace_ms += ms; tm->trace_launches++; break;
+                case 1: tm->shade_ms += ms; break;
+                case 2: tm->infer_ms += ms; break;
+                default: tm->train_ms += ms; break;
             }
         }
         for (cudaEvent_t e : traceEvents) cudaEventDestroy(e);
@@ -1768,6 +1795,9 @@ static mc_status finish_stats(mc_context* ctx, const RenderTiming& tm, long long
         stats->paths = paths;
         stats->render_ms = tm.ms;
         stats->trace_ms = tm.trace_ms;
+        stats->shade_ms = tm.shade_ms;
+        stats->guide_infer_ms = tm.infer_ms;
+        stats->guide_train_ms = tm.train_ms;
         stats->trace_launches = tm.trace_launches;
         stats->kernel_launches = tm.kernel_launches;
         stats->error_flags = flags;

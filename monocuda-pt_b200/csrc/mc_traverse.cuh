@@ -24,6 +24,12 @@
 #ifndef MC_SMEM_STACK
 #define MC_SMEM_STACK 1
 #endif
+// 4-wide steps: start fetching the next node (the nearest hit internal child,
+// else the top of the stack) into L1 before the leaf children are intersected,
+// so its latency overlaps theirs (1), or not (0).
+#ifndef MC_PREFETCH_NEXT
+#define MC_PREFETCH_NEXT 0
+#endif
 
 namespace mc {
 
@@ -226,6 +232,25 @@ MC_D int trav_step4(const TraceScene& sc, TravState& s, const Stack& stack, cons
     slab4(s.r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, s.tmax, tn[2], hit[2]);
     slab4(s.r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, s.tmax, tn[3], hit[3]);
     if (COUNT) cnt->visits++;
+#if MC_PREFETCH_NEXT
+    {
+        // the next node does not depend on the leaf tests below: the hit flags
+        // are taken against the distance before them, as in the choice further down
+        float kn = INFINITY;
+        int vn = -1;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (hit[c] && ref[c] >= 0 && ref[c] != MC_WIDE_EMPTY && tn[c] < kn) {
+                kn = tn[c];
+                vn = ref[c];
+            }
+        if (vn < 0 && s.sp > 0) vn = stack[s.sp - 1];
+        if (vn >= 0) {
+            const float4* nn = sc.nodes + (long long)vn * (QUANT ? 4 : 8);
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(nn));
+        }
+    }
+#endif
     // leaf children first
 #if MC_LEAF_LOOP
     // one loop over this lane's hit leaf children: a warp runs as many

@@ -133,7 +133,8 @@ class BvhBuildOpts(C.Structure):
 
 class BvhInfo(C.Structure):
     _fields_ = [("primitive_count", C.c_int32), ("internal_count", C.c_int32), ("depth", C.c_int32),
-                ("layout", C.c_int32), ("node_bytes", C.c_int64), ("prim_bytes", C.c_int64), ("scene_bounds", AABB)]
+                ("layout", C.c_int32), ("node_bytes", C.c_int64), ("prim_bytes", C.c_int64), ("scene_bounds", AABB),
+                ("wide_levels", C.c_int32)]
 
 
 class RenderParams(C.Structure):
@@ -186,7 +187,8 @@ class RenderStats(C.Structure):
     _fields_ = [("extend_rays", C.c_int64), ("shadow_rays", C.c_int64), ("paths", C.c_int64),
                 ("extend_per_depth", C.c_int64 * MAX_DEPTH_STATS), ("shadow_per_depth", C.c_int64 * MAX_DEPTH_STATS),
                 ("node_visits", C.c_int64), ("leaf_tests", C.c_int64), ("render_ms", C.c_float), ("trace_ms", C.c_float),
-                ("trace_launches", C.c_int32), ("kernel_launches", C.c_int32), ("error_flags", C.c_int32)]
+                ("trace_launches", C.c_int32), ("kernel_launches", C.c_int32), ("error_flags", C.c_int32),
+                ("shade_ms", C.c_float), ("guide_infer_ms", C.c_float), ("guide_train_ms", C.c_float)]
 
 
 class BatchItem(C.Structure):
