@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--guide-steps", type=int, default=4, help="Adam steps per sample, each on 65536 records")
     ap.add_argument("--guide-vertices", type=int, default=0,
                     help="diffuse vertices per path that train the guide (0 = the library default, 3)")
+    ap.add_argument("--guide-depth", type=int, default=0,
+                    help="bounces that sample the guide (0 = all; deeper vertices sample the cosine lobe alone)")
     ap.add_argument("--guide-dir", default="normal", choices=["normal", "ray"],
                     help="direction input of the guide: the face normal or the arriving ray's direction")
     ap.add_argument("--mlp-items", type=int, default=1 << 20)
@@ -675,7 +677,8 @@ def run_guiding(args):
     render(tmp, chunk, 999999)
     gdir = mcpt.GUIDE_DIR_NORMAL if args.guide_dir == "normal" else mcpt.GUIDE_DIR_RAY
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
-                            train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir)
+                            train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
+                            guided_depth=args.guide_depth)
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -701,7 +704,8 @@ def run_guiding(args):
     target = plain_curve[-1][2]
     # guided, trained online from scratch
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
-                       train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir)
+                       train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
+                       guided_depth=args.guide_depth)
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -757,6 +761,7 @@ def run_guiding(args):
            "guided_ms_to_target": round(reached, 1) if reached is not None else None,
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
+           "guided_depth": args.guide_depth or "all",
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,

@@ -704,6 +704,9 @@ typedef struct mc_guide_config {
     int32_t train_vertices;     /* guided renders: diffuse vertices per path that give training records,
                                    the first ones along the path (1..MC_GUIDE_MAX_TRAIN_VERTICES); 0 = 3 */
     int32_t direction_input;    /* MC_GUIDE_DIR_*: the direction the guided renderer feeds the network */
+    int32_t guided_depth;       /* guided renders: bounces whose diffuse vertices sample the guide (the network
+                                   runs only for those); deeper vertices sample the cosine lobe alone. 0 = all;
+                                   never below train_vertices + 1 when training */
 } mc_guide_config;
 
 #define MC_GUIDE_MAX_TRAIN_VERTICES 4

@@ -920,6 +920,7 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     if (g->cfg.train_steps <= 0) g->cfg.train_steps = 1;
     if (!(g->cfg.guide_fraction > 0.f && g->cfg.guide_fraction < 1.f)) g->cfg.guide_fraction = 0.5f;
     if (g->cfg.train_vertices <= 0) g->cfg.train_vertices = 3;
+    if (g->cfg.guided_depth < 0) g->cfg.guided_depth = 0;
     if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1) {
         delete g;
         return mc::set_error(MC_ERR_INVALID, "mc_guide_create: train_vertices above %d or unknown direction_input",

@@ -287,9 +287,13 @@ MC_D bool finish_ray(const TraceArgs& a, const TraceScene& ts, const mc_triangle
 #ifndef MC_TRACE_MIN_BLOCKS
 #define MC_TRACE_MIN_BLOCKS 3
 #endif
+#ifndef MC_TRACE128_MIN_BLOCKS
+#define MC_TRACE128_MIN_BLOCKS 7
+#endif
 constexpr int kTraceThreads = 256;
 template <int ISECT, int MED, bool COUNT, int LAY, bool BATCH, int THREADS = kTraceThreads>
-__global__ void __launch_bounds__(THREADS, THREADS == 256 ? MC_TRACE_MIN_BLOCKS : 7) k_trace(TraceArgs a) {
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? MC_TRACE_MIN_BLOCKS : MC_TRACE128_MIN_BLOCKS)
+    k_trace(TraceArgs a) {
     TravCount cnt;
     const int lane = threadIdx.x & 31;
     const unsigned ltmask = lanemask_lt();
@@ -1502,6 +1506,10 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         nee0[2] = guide->nee0 + 2 * (size_t)capacity;
     }
     auto slot = [&](int d) { return C + (deep ? d % kRingSlots : d) * MC_COUNTERS_PER_DEPTH; };
+    // guided renders: the bounces that sample the guide (training needs the
+    // record slots' next bounce in the guided shade as well)
+    int guidedDepth = guide ? guide->cfg.guided_depth : 0;
+    if (guide && train && guidedDepth > 0) guidedDepth = std::max(guidedDepth, guide->cfg.train_vertices + 1);
     auto enqueue_wave = [&]() -> mc_status {
         MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, stream));
         if (guide) {
@@ -1548,7 +1556,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 dEnd = d;
                 break;
             }
-            if (guide) {
+            // bounces past the guided depth shade with the cosine lobe alone: no inference
+            const bool guidedBounce = guide && (guidedDepth == 0 || d < guidedDepth);
+            if (guidedBounce) {
                 phaseBegin(2);
                 mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], slot(d) + 0, capacity,
                                                  w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.time, w.hits,
@@ -1570,7 +1580,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
             sd.nextQueue = w.queue[(d + 1) & 1];
             sd.nextCount = slot(d + 1) + 0;
             sd.shCount = slot(d) + 1;
-            if (guide) {
+            if (guidedBounce) {
                 sd.mix = guide->mixtures;
                 sd.guideFrac = guide->cfg.guide_fraction;
                 sd.rec = train ? guide->records : nullptr;

@@ -150,7 +150,7 @@ class GuideConfig(C.Structure):
     _fields_ = [("bounds", AABB), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
                 ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("train_vertices", C.c_int32),
-                ("direction_input", C.c_int32), ("_pad", C.c_int32)]
+                ("direction_input", C.c_int32), ("guided_depth", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -732,7 +732,7 @@ class Guide:
     BF16 tensor-core inference and training."""
 
     def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5,
-                 train_steps=1, train_vertices=0, direction_input=0):
+                 train_steps=1, train_vertices=0, direction_input=0, guided_depth=0):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = GuideConfig()
@@ -745,6 +745,7 @@ class Guide:
         cfg.train_steps = train_steps
         cfg.train_vertices = train_vertices
         cfg.direction_input = direction_input
+        cfg.guided_depth = guided_depth
         self.config = cfg
         h = P()
         check(self.lib.mc_guide_create(ctx.handle, C.byref(cfg), C.byref(h)))
