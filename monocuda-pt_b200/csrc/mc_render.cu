@@ -497,9 +497,15 @@ MC_D MatView load_material(const mc_material& m) {
 
 // Density of the guided direction sampler at a diffuse vertex: the cosine
 // lobe with probability 1 - frac, the guide's mixture with probability frac.
+// The guide's directions below the surface are folded up (mirrored in the
+// tangent plane), so none is lost to a zero BSDF: the guide's density at w
+// above the surface is q(w) + q(w') with w' the mirror image of w; below it is 0.
 MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w) {
-    float c = fmaxf(n.dot(w), 0.0f);
-    return (1.0f - frac) * (c / MC_PI) + frac * guide::mixture_pdf(m, w.x, w.y, w.z);
+    const float c = n.dot(w);
+    if (!(c > 0.0f)) return 0.0f;
+    const V3 r = w - n * (2.0f * c);
+    return (1.0f - frac) * (c / MC_PI) +
+           frac * (guide::mixture_pdf(m, w.x, w.y, w.z) + guide::mixture_pdf(m, r.x, r.y, r.z));
 }
 
 // Guided renders: a primary-vertex record must see all the light that arrives
@@ -516,8 +522,11 @@ MC_D void train_remainder(const ShadeArgs& a, int p, int depth, const V3& L, flo
 }
 
 // PT:3470-3696 shadeKernel for one path. GUIDED: diffuse vertices sample the
-// next direction by one-sample MIS of the cosine lobe and the guide.
-template <class Rng, bool GUIDED>
+// next direction by one-sample MIS of the cosine lobe and the guide. ALIAS:
+// scenes with an alias table draw environment directions from it; the
+// variant without it compiles the reference's CDF sampling on its own, so
+// the image-parity path keeps exactly the reference's instruction sequence.
+template <class Rng, bool GUIDED, bool ALIAS = false>
 MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out) {
     const int depth = a.depth;
     V3 throughput(a.tr[p], a.tg[p], a.tb[p]);
@@ -632,7 +641,8 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
         float dist, solidPdf;
         if (envProb > 0.0f && (lightCount == 0 || rng.uniform() < envProb)) {
             float dirPdf;
-            toLight = S.envAlias ? env_sample_alias(S.env, S.envAlias, rng, dirPdf) : env_sample(S.env, rng, dirPdf);
+            if (ALIAS && S.envAlias) toLight = env_sample_alias(S.env, S.envAlias, rng, dirPdf);
+            else toLight = env_sample(S.env, rng, dirPdf);
             lightColor = env_radiance(S.env, toLight, V3(0.f, 0.f, 0.f));
             dist = 1e30f;
             solidPdf = envProb * dirPdf;
@@ -697,6 +707,8 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
                         float d3[3];
                         guide::mixture_sample(m, u0, u1, u2, d3);
                         nd = V3(d3[0], d3[1], d3[2]);
+                        const float below = nd.dot(hitNormal);
+                        if (below < 0.0f) nd = nd - hitNormal * (2.0f * below);  // folded up (guided_pdf)
                     } else {
                         nd = lambertian_scatter(hitNormal, rng);
                     }
@@ -757,7 +769,7 @@ MC_D int warp_reserve(bool want, int* counter, unsigned ltmask) {
 // 4 resident blocks (64 registers, a few spills) beat 2 blocks of 113
 // registers by 5 %: shading waits on scattered loads (hit, material, light,
 // texture) and more warps hide more of that latency.
-template <class Rng, bool GUIDED>
+template <class Rng, bool GUIDED, bool ALIAS = false>
 __global__ void __launch_bounds__(256, GUIDED ? 2 : 4) k_shade(ShadeArgs a) {
     const unsigned ltmask = lanemask_lt();
     const int count = min(*a.count, a.capacity);
@@ -779,7 +791,7 @@ __global__ void __launch_bounds__(256, GUIDED ? 2 : 4) k_shade(ShadeArgs a) {
                     r[12] = 0.0f;
                 }
             }
-            shade_path<Rng, GUIDED>(a, S, p, out);
+            shade_path<Rng, GUIDED, ALIAS>(a, S, p, out);
         }
         int ns = warp_reserve(out.shadow, a.shCount, ltmask);
         if (out.shadow) {
@@ -1394,6 +1406,10 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     if (!shadeBlocks[1]) shadeBlocks[1] = occupancy_blocks((const void*)k_shade<XorwowRng, false>, ctx->sm_count);
     if (guide && !shadeBlocks[2]) shadeBlocks[2] = occupancy_blocks((const void*)k_shade<PhiloxRng, true>, ctx->sm_count);
     const int guidedBlocks = shadeBlocks[2];
+    // the alias-sampling shade variant when some item asked for it (items
+    // without an alias table still sample by CDF inside it)
+    bool alias = false;
+    for (int i = 0; i < n; i++) alias = alias || items[i].p->env_sampling == MC_ENV_SAMPLE_ALIAS;
     const int plainBlocks = (2 * capacity + 255) / 256;
     const int loopBlocks = ctx->sm_count * 8;
     const WaveTable* dtab = (const WaveTable*)ctx->d_table;
@@ -1587,15 +1603,18 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 sd.recSlots = guide->cfg.train_vertices;
                 sd.dirNormal = guide->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
                 phaseBegin(1);
-                k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
+                if (alias) k_shade<PhiloxRng, true, true><<<guidedBlocks, 256, 0, stream>>>(sd);
+                else k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
                 phaseEnd();
             } else if (philox) {
                 phaseBegin(1);
-                k_shade<PhiloxRng, false><<<shadeBlocks[0], 256, 0, stream>>>(sd);
+                if (alias) k_shade<PhiloxRng, false, true><<<shadeBlocks[0], 256, 0, stream>>>(sd);
+                else k_shade<PhiloxRng, false><<<shadeBlocks[0], 256, 0, stream>>>(sd);
                 phaseEnd();
             } else {
                 phaseBegin(1);
-                k_shade<XorwowRng, false><<<shadeBlocks[1], 256, 0, stream>>>(sd);
+                if (alias) k_shade<XorwowRng, false, true><<<shadeBlocks[1], 256, 0, stream>>>(sd);
+                else k_shade<XorwowRng, false><<<shadeBlocks[1], 256, 0, stream>>>(sd);
                 phaseEnd();
             }
             launches++;

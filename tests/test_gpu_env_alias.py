@@ -61,10 +61,15 @@ def tiles(img):
     return img.reshape(4, H // 4, 4, W // 4, 3).mean(axis=(1, 3)).reshape(16, 3)
 
 
-def agree(a, b, k):
+def agree(a, b, k, rel=0.0):
+    """Means within k standard errors, plus `rel` of the mean: a tile that
+    sees only the sky has no variance, and the oracle's restatement of the
+    texture unit's bilinear filtering agrees with it to about 1e-4, not bit
+    for bit."""
     se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
     diff = np.abs(a.mean(0) - b.mean(0))
-    return diff / np.maximum(se, 1e-12), bool(np.all(diff <= k * se + 1e-7))
+    tol = k * se + rel * np.abs(b.mean(0)) + 1e-7
+    return diff / np.maximum(se, 1e-12), bool(np.all(diff <= tol))
 
 
 def test_alias_sampling_converges_to_cdf_sampling_and_the_fp64_oracle(sky_scene):
@@ -82,12 +87,12 @@ def test_alias_sampling_converges_to_cdf_sampling_and_the_fp64_oracle(sky_scene)
         ref.append(acc.reshape(H, W, 3) / SPP)
     orc.orc_scene_destroy(h)
     ref = np.array(ref)
-    for name, other in (("cdf", cdf), ("fp64 oracle", ref)):
-        z, ok = agree(alias.mean(axis=(1, 2)), other.mean(axis=(1, 2)), 3.0)
+    for name, other, rel in (("cdf", cdf, 0.0), ("fp64 oracle", ref, 1e-3)):
+        z, ok = agree(alias.mean(axis=(1, 2)), other.mean(axis=(1, 2)), 3.0, rel)
         print("alias vs %s: means %s vs %s, diff/se %s" % (name, alias.mean(axis=(0, 1, 2)),
                                                           other.mean(axis=(0, 1, 2)), z))
         assert ok, name
-        tz, tok = agree(np.array([tiles(g) for g in alias]), np.array([tiles(r) for r in other]), 4.0)
+        tz, tok = agree(np.array([tiles(g) for g in alias]), np.array([tiles(r) for r in other]), 4.0, rel)
         print("  worst tile diff/se %.2f" % float(tz.max()))
         assert tok, name
     # the sky carries light into the image: a render without it is darker
