@@ -81,6 +81,9 @@ def parse():
     ap.add_argument("--guide-steps", type=int, default=4, help="Adam steps per sample, each on 65536 records")
     ap.add_argument("--guide-vertices", type=int, default=0,
                     help="diffuse vertices per path that train the guide (0 = the library default, 3)")
+    ap.add_argument("--guide-pretrain-spp", type=int, default=0,
+                    help="diagnostic: train the guide on this many untimed samples first (the headline trains from "
+                         "scratch inside the timed region)")
     ap.add_argument("--guide-depth", type=int, default=0,
                     help="bounces that sample the guide (0 = all; deeper vertices sample the cosine lobe alone)")
     ap.add_argument("--guide-dir", default="normal", choices=["normal", "ray"],
@@ -709,6 +712,8 @@ def run_guiding(args):
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
+    for c in range(0, args.guide_pretrain_spp, chunk):
+        render(tmp, chunk, 50_000_000 + c, guide, 1)
     acc = torch.zeros_like(tmp)
     g_ms, g_curve, reached, rays_g = 0.0, [], None, 0
     spp = 0
@@ -760,6 +765,7 @@ def run_guiding(args):
            "target_rmse": round(target, 6), "plain_spp": args.guide_plain_spp, "plain_ms": round(plain_ms, 1),
            "guided_ms_to_target": round(reached, 1) if reached is not None else None,
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
+           "pretrain_spp": args.guide_pretrain_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
            "guided_depth": args.guide_depth or "all",
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
