@@ -107,6 +107,7 @@ struct GuideInferArgs {
     const mc_triangle_hot* hot;             // render with MC_GUIDE_DIR_NORMAL: the hit primitives
     const mc_sphere* spheres;
     int dirNormal;
+    int stride;                             // > 1: one query per `stride` queue slots (the first of each run)
     float* mix;
     int* err;
 };
@@ -356,7 +357,8 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
     uint64_t* bar = &bars[g];
     int* sFlag = &sFlags[g];
     const uint32_t id64 = idesc_bf16(128, kHid), id48 = idesc_bf16(128, kOutPad);
-    const int n = a.count ? min(*a.count, a.capacity) : a.n;
+    const int nSlots = a.count ? min(*a.count, a.capacity) : a.n;
+    const int n = a.stride > 1 ? (nSlots + a.stride - 1) / a.stride : nSlots;
     uint32_t phase = 0;
     bool ok = true;
     // the groups take tiles in turn; from here on a group synchronises only itself
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
         if (valid) {
             float px, py, pz, dx, dy, dz;
             if (a.queue) {
-                const int p = a.queue[q];
+                const int p = a.queue[a.stride > 1 ? q * a.stride : q];
                 const int4 h = reinterpret_cast<const int4*>(a.hits)[p];
                 const float t = h.w ? __int_as_float(h.x) : 0.f;
                 dx = a.dx[p]; dy = a.dy[p]; dz = a.dz[p];
@@ -837,7 +839,7 @@ mc_status guide_reserve_paths(mc_guide* g, int paths) {
 mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
                             const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
                             const float* dz, const float* time, const mc_packed_hit* hits, const mc_triangle_hot* hot,
-                            const mc_sphere* spheres, float* mixtures) {
+                            const mc_sphere* spheres, float* mixtures, int stride) {
     mc_status st = set_attrs(g->ctx);
     if (st != MC_OK) return st;
     GuideInferArgs a;
@@ -853,6 +855,7 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
     a.hot = hot;
     a.spheres = spheres;
     a.dirNormal = g->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
+    a.stride = stride;
     a.mix = mixtures;
     a.err = g->ctx->d_error;
     k_guide_infer<<<g->ctx->sm_count, kTile * kInferGroups, kInferSmem, s>>>(a);

@@ -215,10 +215,12 @@ mc_status context_counters(mc_context* ctx);
 // Guide kernels driven by device-side counts (guided renders).
 // Inputs of a queued path: its hit point and, per the guide's direction_input,
 // the face normal of the hit primitive (hot, spheres, time) or the ray direction.
+// stride > 1: only every stride-th queue slot is queried (the first sample of
+// each pixel of a pixel-major wave at bounce 0; its samples share the mixture).
 mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const int* count, int capacity,
                             const float* ox, const float* oy, const float* oz, const float* dx, const float* dy,
                             const float* dz, const float* time, const mc_packed_hit* hits, const mc_triangle_hot* hot,
-                            const mc_sphere* spheres, float* mixtures);
+                            const mc_sphere* spheres, float* mixtures, int stride = 1);
 // `steps` Adam steps, each on the next min(stepRecords, cfg.batch_capacity)
 // of the records (stepRecords <= 0: cfg.batch_capacity).
 mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, const int* count, int capacity, int steps,

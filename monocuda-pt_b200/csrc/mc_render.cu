@@ -434,6 +434,7 @@ struct ShadeArgs {
     float* rec;
     int recSlots;
     int dirNormal;
+    int mixShare;     // bounce 0 of a single-item pixel-major wave: the pixel's samples read its first path's mixture
 };
 
 // Training record of a diffuse vertex (recSlots per path, slot = depth):
@@ -443,6 +444,14 @@ struct ShadeArgs {
 // emission that direction found, [12] mean sample radiance not carried by
 // that direction (everything before the vertex plus its own NEE).
 constexpr int kRecFloats = 16;
+
+// The path whose mixture a path samples: itself, or at a shared bounce 0 the
+// first sample of its pixel (the samples of a pixel start with the same
+// primary ray; any mixture is a valid proposal, so sharing keeps the estimator
+// unbiased whatever the hits).
+MC_D int mix_path(const ShadeArgs& a, const SceneGPU& S, int p) {
+    return a.mixShare ? p - (p - S.pathOffset) % S.pathStride : p;
+}
 
 MC_D float* rec_slot(const ShadeArgs& a, int p, int depth) {
     return a.rec + ((size_t)p * a.recSlots + depth) * kRecFloats;
@@ -664,7 +673,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             float phasePdf = hg_phase_pdf(inDir.dot(toLight), mat.g);
             float scatterPdf = iso ? phasePdf : lambertian_cosine_pdf(cosS);
             if (GUIDED && !iso && mat.type == MC_MAT_LAMBERTIAN)
-                scatterPdf = guided_pdf(a.mix + (size_t)p * guide::kOut, a.guideFrac, hitNormal, toLight);
+                scatterPdf = guided_pdf(a.mix + (size_t)mix_path(a, S, p) * guide::kOut, a.guideFrac, hitNormal, toLight);
             float scatterValue = iso ? phasePdf : cosS / MC_PI;
             float neeW = power_heuristic(solidPdf, scatterPdf);
             V3 contribution = throughput * lightColor * (scatterValue / solidPdf) * neeW;
@@ -701,7 +710,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             case MC_MAT_LAMBERTIAN:
             default:
                 if (GUIDED) {
-                    const float* m = a.mix + (size_t)p * guide::kOut;
+                    const float* m = a.mix + (size_t)mix_path(a, S, p) * guide::kOut;
                     if (rng.uniform() < a.guideFrac) {
                         float u0 = rng.uniform(), u1 = rng.uniform(), u2 = rng.uniform();
                         float d3[3];
@@ -1525,6 +1534,9 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     // guided renders: the bounces that sample the guide (training needs the
     // record slots' next bounce in the guided shade as well)
     int guidedDepth = guide ? guide->cfg.guided_depth : 0;
+    // one image per wave: at bounce 0 the samples of a pixel (neighbouring
+    // paths, the same primary ray) share one inference
+    const bool shareMix = guide && n == 1;
     if (guide && train && guidedDepth > 0) guidedDepth = std::max(guidedDepth, guide->cfg.train_vertices + 1);
     auto enqueue_wave = [&]() -> mc_status {
         MC_CUDA(cudaMemsetAsync(C, 0, counterBytes, stream));
@@ -1578,7 +1590,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 phaseBegin(2);
                 mc_status gs = guide_infer_paths(guide, stream, w.queue[d & 1], slot(d) + 0, capacity,
                                                  w.ox, w.oy, w.oz, w.dx, w.dy, w.dz, w.time, w.hits,
-                                                 items[0].view->tri_hot, items[0].view->spheres, guide->mixtures);
+                                                 items[0].view->tri_hot, items[0].view->spheres, guide->mixtures,
+                                                 d == 0 && shareMix ? waveR : 1);
                 phaseEnd();
                 if (gs != MC_OK) return gs;
                 launches++;
@@ -1602,6 +1615,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 sd.rec = train ? guide->records : nullptr;
                 sd.recSlots = guide->cfg.train_vertices;
                 sd.dirNormal = guide->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
+                sd.mixShare = d == 0 && shareMix ? 1 : 0;
                 phaseBegin(1);
                 if (alias) k_shade<PhiloxRng, true, true><<<guidedBlocks, 256, 0, stream>>>(sd);
                 else k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
