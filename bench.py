@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--guide-pretrain-spp", type=int, default=0,
                     help="diagnostic: train the guide on this many untimed samples first (the headline trains from "
                          "scratch inside the timed region)")
+    ap.add_argument("--guide-weight-cap", type=float, default=0.0,
+                    help="training: cap of a record's share of a step's weight, in units of 1 / records (0 = none)")
     ap.add_argument("--guide-depth", type=int, default=0,
                     help="bounces that sample the guide (0 = all; deeper vertices sample the cosine lobe alone)")
     ap.add_argument("--guide-dir", default="normal", choices=["normal", "ray"],
@@ -681,7 +683,7 @@ def run_guiding(args):
     gdir = mcpt.GUIDE_DIR_NORMAL if args.guide_dir == "normal" else mcpt.GUIDE_DIR_RAY
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
                             train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
-                            guided_depth=args.guide_depth)
+                            guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap)
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -708,7 +710,7 @@ def run_guiding(args):
     # guided, trained online from scratch
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
                        train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
-                       guided_depth=args.guide_depth)
+                       guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap)
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -767,7 +769,7 @@ def run_guiding(args):
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
            "pretrain_spp": args.guide_pretrain_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
-           "guided_depth": args.guide_depth or "all",
+           "guided_depth": args.guide_depth or "all", "weight_cap": args.guide_weight_cap,
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,

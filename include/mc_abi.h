@@ -707,6 +707,11 @@ typedef struct mc_guide_config {
     int32_t guided_depth;       /* guided renders: bounces whose diffuse vertices sample the guide (the network
                                    runs only for those); deeper vertices sample the cosine lobe alone. 0 = all;
                                    never below train_vertices + 1 when training */
+    float weight_cap;           /* guided renders' training: a record's share of its step's normalized weight
+                                   is capped at weight_cap / (records in the step), so a few rare bright paths
+                                   cannot take over a step (0 = no cap). The estimator stays unbiased: only
+                                   the proposal the guide learns changes */
+    int32_t pad0, pad1, pad2;
 } mc_guide_config;
 
 #define MC_GUIDE_MAX_TRAIN_VERTICES 4
@@ -902,7 +907,7 @@ MC_STATIC_ASSERT(sizeof(mc_packed_hit) == 16, "PackedHit is 16 bytes");
 MC_STATIC_ASSERT(sizeof(mc_camera) == 172, "Camera is 172 bytes");
 MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
 /* this library's own structs (bindings mirror these sizes) */
-MC_STATIC_ASSERT(sizeof(mc_guide_config) == 80, "mc_guide_config is 80 bytes");
+MC_STATIC_ASSERT(sizeof(mc_guide_config) == 96, "mc_guide_config is 96 bytes");
 MC_STATIC_ASSERT(sizeof(mc_render_params) == 248, "mc_render_params is 248 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_config) == 24, "mc_server_config is 24 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_request) == 264, "mc_server_request is 264 bytes");

@@ -158,6 +158,7 @@ struct GuideTrainArgs {
     int capacity;                           // records the batch holds
     int stepCap;                            // records one step takes
     const float* scale;
+    float weightCap;                        // > 0: a record's normalized weight is at most weightCap / n
     float* partials;
     double* loss;
     int* err;
@@ -531,7 +532,8 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
             for (int k = 0; k < kOut; k++) y[k] += sb[3 * kHid + k];
             float dy[kOutPad];
             for (int k = kOut; k < kOutPad; k++) dy[k] = 0.f;
-            const float W = valid ? rec[9] * scale : 0.f;
+            float W = valid ? rec[9] * scale : 0.f;
+            if (a.weightCap > 0.f && n > 0) W = fminf(W, a.weightCap / (float)n);
             float nx = rec[6], ny = rec[7], nz = rec[8];
             lossAcc += loss_grad(y, nx, ny, nz, W, dy);
             for (int c = 0; c < kOutPad; c += 8)
@@ -771,7 +773,7 @@ void fill_box(const mc_guide* g, Args& a) {
 }
 
 mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n, const int* count, int offset,
-                       int capacity, int stepCap, const float* scale, int* gridOut) {
+                       int capacity, int stepCap, const float* scale, int* gridOut, float weightCap = 0.f) {
     mc_status st = set_attrs(g->ctx);
     if (st != MC_OK) return st;
     GuideTrainArgs a;
@@ -786,6 +788,7 @@ mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n,
     a.capacity = capacity;
     a.stepCap = stepCap;
     a.scale = scale;
+    a.weightCap = weightCap;
     a.partials = g->partials;
     a.loss = g->loss;
     a.err = g->ctx->d_error;
@@ -898,7 +901,7 @@ mc_status guide_train_device(mc_guide* g, cudaStream_t s, const float* records, 
         k_guide_weight_scale<<<1, 1024, 0, s>>>(r, 0, count, off, capacity, B, g->scale);
         MC_CUDA(cudaGetLastError());
         int grid = 0;
-        mc_status st = launch_train(g, s, r, 0, count, off, capacity, B, g->scale, &grid);
+        mc_status st = launch_train(g, s, r, 0, count, off, capacity, B, g->scale, &grid, g->cfg.weight_cap);
         if (st != MC_OK) return st;
         if ((st = adam_step(g, s, grid)) != MC_OK) return st;
     }
@@ -924,6 +927,7 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     if (!(g->cfg.guide_fraction > 0.f && g->cfg.guide_fraction < 1.f)) g->cfg.guide_fraction = 0.5f;
     if (g->cfg.train_vertices <= 0) g->cfg.train_vertices = 3;
     if (g->cfg.guided_depth < 0) g->cfg.guided_depth = 0;
+    if (!(g->cfg.weight_cap >= 0.f)) g->cfg.weight_cap = 0.f;
     if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1) {
         delete g;
         return mc::set_error(MC_ERR_INVALID, "mc_guide_create: train_vertices above %d or unknown direction_input",

@@ -150,7 +150,8 @@ class GuideConfig(C.Structure):
     _fields_ = [("bounds", AABB), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
                 ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("train_vertices", C.c_int32),
-                ("direction_input", C.c_int32), ("guided_depth", C.c_int32)]
+                ("direction_input", C.c_int32), ("guided_depth", C.c_int32), ("weight_cap", C.c_float),
+                ("_pad", C.c_int32 * 3)]
 
 
 class ServerConfig(C.Structure):
@@ -208,7 +209,7 @@ class SceneHost(C.Structure):
 
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
-         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, VolumeGrid: 64, GuideConfig: 80, RenderParams: 248,
+         Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, VolumeGrid: 64, GuideConfig: 96, RenderParams: 248,
          ServerConfig: 24, ServerRequest: 264, ServerResult: 56, ServerStats: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
@@ -732,7 +733,7 @@ class Guide:
     BF16 tensor-core inference and training."""
 
     def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5,
-                 train_steps=1, train_vertices=0, direction_input=0, guided_depth=0):
+                 train_steps=1, train_vertices=0, direction_input=0, guided_depth=0, weight_cap=0.0):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = GuideConfig()
@@ -746,6 +747,7 @@ class Guide:
         cfg.train_vertices = train_vertices
         cfg.direction_input = direction_input
         cfg.guided_depth = guided_depth
+        cfg.weight_cap = weight_cap
         self.config = cfg
         h = P()
         check(self.lib.mc_guide_create(ctx.handle, C.byref(cfg), C.byref(h)))
