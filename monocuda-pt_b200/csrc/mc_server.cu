@@ -217,6 +217,21 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
     std::vector<mc::WaveItem> items;
     std::vector<long long> ids;
     params.reserve(chosen.size());
+    // the step's plain requests on one scene: single-scene trace launches, which
+    // can take the 128-thread block shape with the stack that scene's tree needs
+    long long plainScene = -1;
+    bool oneScene = true;
+    for (long long id : chosen) {
+        const ServerRequest& r = s->requests[id];
+        if (r.guided) continue;
+        if (plainScene < 0) plainScene = r.scene;
+        else if (plainScene != r.scene) oneScene = false;
+    }
+    int stackNeed = 0;
+    if (oneScene && plainScene >= 0) {
+        const int lv = s->scenes[(size_t)plainScene].bvh->wide_levels;
+        if (lv > 0) stackNeed = ((3 * lv + 7) / 8) * 8;
+    }
     for (long long id : chosen) {
         ServerRequest& r = s->requests[id];
         if (r.guided) continue;
@@ -225,6 +240,15 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
         p.spp = std::min(sps, r.params.spp - r.done);
         p.use_graph = 0;
         p.instrument = 0;
+        // launch shape (the image does not depend on it): the refill threshold
+        // and block shape the autotuner picks for large scenes, unless the
+        // request set its own
+        if (p.refill_threshold <= 0) p.refill_threshold = 16;
+        if (p.trace_threads == 0 && stackNeed > 0 && stackNeed <= 56 && p.stack_entries == 0 &&
+            p.intersector == MC_ISECT_REFERENCE) {
+            p.trace_threads = 128;
+            p.stack_entries = stackNeed;
+        }
         params.push_back(p);
         ids.push_back(id);
     }
