@@ -65,6 +65,8 @@ def parse():
                     help="traversal stack entries per lane (0 = the autotuner's choice, or 64 with a fixed --refill; "
                          "-1 = what the 4-wide tree can need, 3 per level)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batch and guiding summaries that the default 1-GPU line carries")
     ap.add_argument("--no-1m", action="store_true",
                     help="skip the second, ~1M-triangle line (level-7 icospheres, 983,056 triangles)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -512,6 +514,20 @@ def run_ours(args):
     }
     if not args.no_1m and args.level == 8 and world == 1:
         out["workload_1m"] = level_variant(ctx, 7, K, Wm, S)
+    if not args.no_extras and args.level == 8 and world == 1 and not args.resolution:
+        # the other workloads of the scope table, summarised in the same line:
+        # the 64-scene batch against sequential renders, guided vs plain time
+        # to plain's 64-spp RMSE on the aperture room (with the guide MLP's
+        # kernel throughput)
+        b = run_batch(args, emit=False)
+        out["batch"] = {k: b[k] for k in ("value", "unit", "triangles", "build_ms", "render_ms", "sequential_mrays",
+                                          "speedup_vs_sequential")}
+        g = run_guiding(args, emit=False)
+        out["guiding"] = {k: g[k] for k in ("metric", "value", "unit", "target_rmse", "plain_ms", "guided_ms_to_target",
+                                            "guided_spp", "phase_split_ms")}
+        out["guiding"]["mlp"] = {k: g["mlp"][k] for k in ("infer_queries_per_s", "infer_tflops", "infer_frac",
+                                                          "train_records_per_s", "train_tflops", "train_frac",
+                                                          "peak_tflops")}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(scene, args)
     print(json.dumps(out), flush=True)
@@ -519,7 +535,7 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
-def run_batch(args):
+def run_batch(args, emit=True):
     """64 seeded scenes (log-normal triangle counts, median 50k, clipped to
     [1k, 2M]; resolutions from {256^2, 512^2, 1024^2}; spp from {4, 16, 64}):
     one batched BVH build and one batched, graph-replayed render, against
@@ -577,7 +593,9 @@ def run_batch(args):
            "sequential_ms": round(seq_ms, 2), "sequential_mrays": round(seq_rays / (seq_ms / 1e3) / 1e6, 2),
            "speedup_vs_sequential": round(seq_ms / (build_ms + render_ms), 3), "generation_s": round(gen_s, 1),
            "graph": True, "layout": "wide4"}
-    print(json.dumps(out), flush=True)
+    if emit:
+        print(json.dumps(out), flush=True)
+    return out
 
 
 def mlp_throughput(ctx, guide, n=1 << 20):
@@ -632,7 +650,7 @@ def run_mlp(args):
     guide.close()
 
 
-def run_guiding(args):
+def run_guiding(args, emit=True):
     """Time to a fixed RMSE, guided vs plain wavefront, on the aperture room
     (about 200k triangles, 1024x1024, light only through a 0.2 x 0.2 hole).
     The target RMSE is plain wavefront's at --guide-plain-spp; the guided
@@ -775,7 +793,9 @@ def run_guiding(args):
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,
            "mlp": mlp,
            "data": "synthetic (seeded procedural room)", "dtype": "bf16 MLP / f32 tracer"}
-    print(json.dumps(out), flush=True)
+    if emit:
+        print(json.dumps(out), flush=True)
+    return out
 
 
 def run_server(args):
