@@ -108,6 +108,7 @@ struct GuideInferArgs {
     const mc_sphere* spheres;
     int dirNormal;
     int stride;                             // > 1: one query per `stride` queue slots (the first of each run)
+    int renderLayout;                       // mixtures of kMixRender floats (with the lobe constants) instead of kOut
     float* mix;
     int* err;
 };
@@ -426,10 +427,20 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
         tmem_ld16(tcol(R, 32), y + 32);
         if (valid) {
             for (int k = 0; k < kOut; k++) y[k] += sb[3 * kHid + k];
-            float m[kOut];
+            float m[kMixRender];
             raw_to_mixture(y, m);
-            float4* dst = reinterpret_cast<float4*>(a.mix + (size_t)out * kOut);
-            for (int i = 0; i < kOut / 4; i++) dst[i] = make_float4(m[4 * i], m[4 * i + 1], m[4 * i + 2], m[4 * i + 3]);
+            if (a.renderLayout) {
+#pragma unroll
+                for (int k = 0; k < kLobes; k++) {
+                    const float kap = m[32 + k];
+                    // log(kappa / (2 pi (1 - exp(-2 kappa)))) - kappa; expm1f keeps small kappa exact
+                    const float ln = logf(kap) - 1.83787706641f - logf(-expm1f(-2.0f * kap)) - kap;
+                    m[40 + k] = m[k] > 0.0f ? logf(m[k]) + ln : -INFINITY;
+                }
+            }
+            const int stride = a.renderLayout ? kMixRender : kOut;
+            float4* dst = reinterpret_cast<float4*>(a.mix + (size_t)out * stride);
+            for (int i = 0; i < stride / 4; i++) dst[i] = make_float4(m[4 * i], m[4 * i + 1], m[4 * i + 2], m[4 * i + 3]);
         }
         // the next tile's operand barrier (fenced) orders these TMEM reads before its MMA
     }
@@ -829,7 +840,7 @@ mc_status guide_reserve_paths(mc_guide* g, int paths) {
     cudaFree(g->nee0);
     g->mixtures = g->records = g->nee0 = nullptr;
     g->mixture_capacity = g->record_capacity = 0;
-    if (cudaMalloc(&g->mixtures, (size_t)paths * kOut * sizeof(float)) != cudaSuccess ||
+    if (cudaMalloc(&g->mixtures, (size_t)paths * kMixRender * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&g->records, (size_t)paths * g->cfg.train_vertices * 16 * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&g->nee0, (size_t)paths * 3 * sizeof(float)) != cudaSuccess) {
         cudaGetLastError();
@@ -859,6 +870,7 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
     a.spheres = spheres;
     a.dirNormal = g->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
     a.stride = stride;
+    a.renderLayout = 1;
     a.mix = mixtures;
     a.err = g->ctx->d_error;
     k_guide_infer<<<g->ctx->sm_count, kTile * kInferGroups, kInferSmem, s>>>(a);
