@@ -89,7 +89,8 @@ def parse():
     ap.add_argument("--guide-weight-cap", type=float, default=0.0,
                     help="training: cap of a record's share of a step's weight, in units of 1 / records (0 = none)")
     ap.add_argument("--guide-depth", type=int, default=0,
-                    help="bounces that sample the guide (0 = all; deeper vertices sample the cosine lobe alone)")
+                    help="bounces that sample the guide (0 = the library default, 4; deeper vertices sample the cosine "
+                         "lobe alone)")
     ap.add_argument("--guide-dir", default="normal", choices=["normal", "ray"],
                     help="direction input of the guide: the face normal or the arriving ray's direction")
     ap.add_argument("--mlp-items", type=int, default=1 << 20)
@@ -101,6 +102,8 @@ def parse():
                     help="requests per arrival rate (at most; max(24, 16 x rate) at low rates)")
     ap.add_argument("--server-sps", type=int, default=16, help="samples per server step")
     ap.add_argument("--server-wave-paths", type=int, default=0, help="paths per server wave (0 = 4M)")
+    ap.add_argument("--server-scene-waves", action="store_true",
+                    help="each step renders each scene's plain requests in a wave of their own")
     return ap.parse_args()
 
 
@@ -787,7 +790,7 @@ def run_guiding(args, emit=True):
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
            "pretrain_spp": args.guide_pretrain_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
-           "guided_depth": args.guide_depth or "all", "weight_cap": args.guide_weight_cap,
+           "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap,
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,
@@ -820,7 +823,8 @@ def run_server(args):
     for s in scenes:
         env = mcpt.host_env(s) if s.env_width > 0 else None
         devs.append(mcpt.DeviceScene(mcpt.host_triangles(s), env_rgba=env, env_intensity=s.env_intensity))
-    srv = mcpt.Server(ctx, samples_per_step=args.server_sps, wave_paths=args.server_wave_paths)
+    srv = mcpt.Server(ctx, samples_per_step=args.server_sps, wave_paths=args.server_wave_paths,
+                      flags=mcpt.SERVER_SCENE_WAVES if args.server_scene_waves else 0)
     sids = [srv.add_scene(d) for d in devs]
     bvhs = [mcpt.Bvh(ctx, d.view, layout=mcpt.LAYOUT_WIDE4) for d in devs]
     sizes = [(256, 256), (512, 512), (1024, 1024), (1920, 1080)]
@@ -935,7 +939,7 @@ def run_server(args):
            "workload": "render_server", "scenes": len(scenes),
            "scene_triangles": [int(s.triangle_count) for s in scenes], "budget_gb": st.budget_bytes / 1e9,
            "resident_scene_gb": round(st.scene_bytes / 1e9, 3), "samples_per_step": args.server_sps,
-           "wave_paths": args.server_wave_paths or 4194304,
+           "wave_paths": args.server_wave_paths or 4194304, "scene_waves": bool(args.server_scene_waves),
            "points": points, "data": "synthetic (seeded scenes and request trace)",
            "baseline": "plain per-request wavefront tracer, one request at a time in arrival order"}
     print(json.dumps(out), flush=True)

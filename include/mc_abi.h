@@ -705,8 +705,8 @@ typedef struct mc_guide_config {
                                    the first ones along the path (1..MC_GUIDE_MAX_TRAIN_VERTICES); 0 = 3 */
     int32_t direction_input;    /* MC_GUIDE_DIR_*: the direction the guided renderer feeds the network */
     int32_t guided_depth;       /* guided renders: bounces whose diffuse vertices sample the guide (the network
-                                   runs only for those); deeper vertices sample the cosine lobe alone. 0 = all;
-                                   never below train_vertices + 1 when training */
+                                   runs only for those); deeper vertices sample the cosine lobe alone. 0 = 4;
+                                   never below train_vertices + 1 when training; MC_MAX_DEPTH = every bounce */
     float weight_cap;           /* guided renders' training: a record's share of its step's normalized weight
                                    is capped at weight_cap / (records in the step), so a few rare bright paths
                                    cannot take over a step (0 = no cap). The estimator stays unbiased: only
@@ -814,7 +814,13 @@ typedef struct mc_server_config {
     int64_t wave_paths;         /* paths a step renders per sample: the oldest active request,
                                    then the ones with the least remaining work while they fit;
                                    0 = 4194304 */
+    int32_t flags;              /* MC_SERVER_* */
+    int32_t pad0;
 } mc_server_config;
+
+/* A step renders the plain requests of each scene in a wave of their own
+ * (single-scene trace launches) instead of one wave shared by every scene. */
+#define MC_SERVER_SCENE_WAVES 1
 
 typedef struct mc_server_request {
     int64_t scene_id;
@@ -909,7 +915,7 @@ MC_STATIC_ASSERT(sizeof(mc_env_map) == 56, "EnvironmentMap is 56 bytes");
 /* this library's own structs (bindings mirror these sizes) */
 MC_STATIC_ASSERT(sizeof(mc_guide_config) == 96, "mc_guide_config is 96 bytes");
 MC_STATIC_ASSERT(sizeof(mc_render_params) == 248, "mc_render_params is 248 bytes");
-MC_STATIC_ASSERT(sizeof(mc_server_config) == 24, "mc_server_config is 24 bytes");
+MC_STATIC_ASSERT(sizeof(mc_server_config) == 32, "mc_server_config is 32 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_request) == 264, "mc_server_request is 264 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_result) == 56, "mc_server_result is 56 bytes");
 MC_STATIC_ASSERT(sizeof(mc_server_stats) == 64, "mc_server_stats is 64 bytes");

@@ -18,10 +18,6 @@ constexpr int kIn = MC_GUIDE_INPUTS;     // 144
 constexpr int kHid = MC_GUIDE_HIDDEN;    // 64
 constexpr int kOut = MC_GUIDE_OUTPUTS;   // 40
 constexpr int kOutPad = 48;              // output rows padded to a multiple of 16
-// Mixture record of guided renders: the 40 API floats (weights, unit means,
-// kappa) then, per lobe, c = log(weight) + log(kappa / (2 pi (1 - exp(-2 kappa))))
-// - kappa, so the density is sum over lobes of exp(c + kappa mean . w).
-constexpr int kMixRender = 48;
 constexpr int kLobes = MC_GUIDE_LOBES;   // 8
 constexpr int kFreqs = 12;
 
@@ -93,18 +89,6 @@ MC_GD float mixture_pdf(const float* m, float wx, float wy, float wz) {
     for (int k = 0; k < kLobes; k++) {
         float c = m[8 + 3 * k] * wx + m[9 + 3 * k] * wy + m[10 + 3 * k] * wz;
         q += m[k] * vmf_pdf(m[32 + k], c);
-    }
-    return q;
-}
-
-// The same density from a render mixture record (kMixRender floats): one
-// exponential per lobe, no division.
-MC_GD float mixture_pdf_render(const float* m, float wx, float wy, float wz) {
-    float q = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kLobes; k++) {
-        const float c = m[8 + 3 * k] * wx + m[9 + 3 * k] * wy + m[10 + 3 * k] * wz;
-        q += expf(m[40 + k] + m[32 + k] * c);
     }
     return q;
 }

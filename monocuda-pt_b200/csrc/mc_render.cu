@@ -514,7 +514,7 @@ MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w) {
     if (!(c > 0.0f)) return 0.0f;
     const V3 r = w - n * (2.0f * c);
     return (1.0f - frac) * (c / MC_PI) +
-           frac * (guide::mixture_pdf_render(m, w.x, w.y, w.z) + guide::mixture_pdf_render(m, r.x, r.y, r.z));
+           frac * (guide::mixture_pdf(m, w.x, w.y, w.z) + guide::mixture_pdf(m, r.x, r.y, r.z));
 }
 
 // Guided renders: a primary-vertex record must see all the light that arrives
@@ -673,7 +673,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             float phasePdf = hg_phase_pdf(inDir.dot(toLight), mat.g);
             float scatterPdf = iso ? phasePdf : lambertian_cosine_pdf(cosS);
             if (GUIDED && !iso && mat.type == MC_MAT_LAMBERTIAN)
-                scatterPdf = guided_pdf(a.mix + (size_t)mix_path(a, S, p) * guide::kMixRender, a.guideFrac, hitNormal, toLight);
+                scatterPdf = guided_pdf(a.mix + (size_t)mix_path(a, S, p) * guide::kOut, a.guideFrac, hitNormal, toLight);
             float scatterValue = iso ? phasePdf : cosS / MC_PI;
             float neeW = power_heuristic(solidPdf, scatterPdf);
             V3 contribution = throughput * lightColor * (scatterValue / solidPdf) * neeW;
@@ -710,7 +710,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             case MC_MAT_LAMBERTIAN:
             default:
                 if (GUIDED) {
-                    const float* m = a.mix + (size_t)mix_path(a, S, p) * guide::kMixRender;
+                    const float* m = a.mix + (size_t)mix_path(a, S, p) * guide::kOut;
                     if (rng.uniform() < a.guideFrac) {
                         float u0 = rng.uniform(), u1 = rng.uniform(), u2 = rng.uniform();
                         float d3[3];

@@ -212,55 +212,56 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
         chosen.push_back(id);
         paths += px;
     }
-    // plain requests of every scene share the waves
-    std::vector<mc_render_params> params;
-    std::vector<mc::WaveItem> items;
-    std::vector<long long> ids;
-    params.reserve(chosen.size());
-    // the step's plain requests on one scene: single-scene trace launches, which
-    // can take the 128-thread block shape with the stack that scene's tree needs
-    long long plainScene = -1;
-    bool oneScene = true;
+    // plain requests: every scene's in one shared wave (the trace looks up each
+    // ray's scene), or with MC_SERVER_SCENE_WAVES one wave per scene (single-scene
+    // trace launches, which can take the 128-thread block shape with the stack
+    // that scene's tree needs)
+    std::map<long long, std::vector<long long>> plainGroups;
+    const bool sceneWaves = (s->cfg.flags & MC_SERVER_SCENE_WAVES) != 0;
     for (long long id : chosen) {
         const ServerRequest& r = s->requests[id];
         if (r.guided) continue;
-        if (plainScene < 0) plainScene = r.scene;
-        else if (plainScene != r.scene) oneScene = false;
+        plainGroups[sceneWaves ? r.scene : -1].push_back(id);
     }
-    int stackNeed = 0;
-    if (oneScene && plainScene >= 0) {
-        const int lv = s->scenes[(size_t)plainScene].bvh->wide_levels;
-        if (lv > 0) stackNeed = ((3 * lv + 7) / 8) * 8;
-    }
-    for (long long id : chosen) {
-        ServerRequest& r = s->requests[id];
-        if (r.guided) continue;
-        mc_render_params p = r.params;
-        p.first_sample = r.params.first_sample + r.done;
-        p.spp = std::min(sps, r.params.spp - r.done);
-        p.use_graph = 0;
-        p.instrument = 0;
-        // launch shape (the image does not depend on it): the refill threshold
-        // and block shape the autotuner picks for large scenes, unless the
-        // request set its own
-        if (p.refill_threshold <= 0) p.refill_threshold = 16;
-        if (p.trace_threads == 0 && stackNeed > 0 && stackNeed <= 56 && p.stack_entries == 0 &&
-            p.intersector == MC_ISECT_REFERENCE) {
-            p.trace_threads = 128;
-            p.stack_entries = stackNeed;
+    for (auto& grp : plainGroups) {
+        const std::vector<long long>& ids = grp.second;
+        long long oneScene = s->requests[ids[0]].scene;
+        for (long long id : ids)
+            if (s->requests[id].scene != oneScene) oneScene = -1;
+        int stackNeed = 0;
+        if (oneScene >= 0) {
+            const int lv = s->scenes[(size_t)oneScene].bvh->wide_levels;
+            if (lv > 0) stackNeed = ((3 * lv + 7) / 8) * 8;
         }
-        params.push_back(p);
-        ids.push_back(id);
-    }
-    for (size_t i = 0; i < ids.size(); i++) {
-        ServerRequest& r = s->requests[ids[i]];
-        const ServerScene& sc = s->scenes[(size_t)r.scene];
-        mc::WaveItem it{&sc.view, &params[i], r.accum, sc.bvh->wide_roots[0], 0};
-        it.bvh = sc.bvh;
-        it.spw = params[i].spp;  // the step's samples in one wave, pixel-major
-        items.push_back(it);
-    }
-    if (!items.empty()) {
+        std::vector<mc_render_params> params;
+        std::vector<mc::WaveItem> items;
+        params.reserve(ids.size());
+        for (long long id : ids) {
+            ServerRequest& r = s->requests[id];
+            mc_render_params p = r.params;
+            p.first_sample = r.params.first_sample + r.done;
+            p.spp = std::min(sps, r.params.spp - r.done);
+            p.use_graph = 0;
+            p.instrument = 0;
+            // launch shape (the image does not depend on it): the refill threshold
+            // and block shape the autotuner picks for large scenes, unless the
+            // request set its own
+            if (p.refill_threshold <= 0) p.refill_threshold = 16;
+            if (p.trace_threads == 0 && stackNeed > 0 && stackNeed <= 56 && p.stack_entries == 0 &&
+                p.intersector == MC_ISECT_REFERENCE) {
+                p.trace_threads = 128;
+                p.stack_entries = stackNeed;
+            }
+            params.push_back(p);
+        }
+        for (size_t i = 0; i < ids.size(); i++) {
+            ServerRequest& r = s->requests[ids[i]];
+            const ServerScene& sc = s->scenes[(size_t)r.scene];
+            mc::WaveItem it{&sc.view, &params[i], r.accum, sc.bvh->wide_roots[0], 0};
+            it.bvh = sc.bvh;
+            it.spw = params[i].spp;  // the step's samples in one wave, pixel-major
+            items.push_back(it);
+        }
         mc_render_stats rs;
         st = mc::render_items(s->ctx, items[0].bvh, items.data(), (int)items.size(), false, &rs);
         if (st != MC_OK) return st;

@@ -156,7 +156,10 @@ class GuideConfig(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_active", C.c_int32), ("samples_per_step", C.c_int32),
-                ("wave_paths", C.c_int64)]
+                ("wave_paths", C.c_int64), ("flags", C.c_int32), ("pad0", C.c_int32)]
+
+
+SERVER_SCENE_WAVES = 1
 
 
 class ServerRequest(C.Structure):
@@ -210,7 +213,7 @@ class SceneHost(C.Structure):
 
 SIZES = {Vec3: 12, AABB: 32, Texture: 40, Material: 96, Triangle: 224, TriangleHot: 36, TriangleCold: 192,
          Sphere: 160, Light: 64, BvhNode: 64, PackedHit: 16, Camera: 172, EnvMap: 56, VolumeGrid: 64, GuideConfig: 96, RenderParams: 248,
-         ServerConfig: 24, ServerRequest: 264, ServerResult: 56, ServerStats: 64}
+         ServerConfig: 32, ServerRequest: 264, ServerResult: 56, ServerStats: 64}
 for _t, _s in SIZES.items():
     assert C.sizeof(_t) == _s, (_t.__name__, C.sizeof(_t), _s)
 
@@ -793,10 +796,10 @@ class Server:
     """The render server (mc_server_*): resident scenes, HBM-budget admission,
     shared waves for all active requests."""
 
-    def __init__(self, ctx, budget_bytes=0, max_active=0, samples_per_step=0, wave_paths=0):
+    def __init__(self, ctx, budget_bytes=0, max_active=0, samples_per_step=0, wave_paths=0, flags=0):
         self.ctx = ctx
         self.lib = ctx.lib
-        cfg = ServerConfig(budget_bytes, max_active, samples_per_step, wave_paths)
+        cfg = ServerConfig(budget_bytes, max_active, samples_per_step, wave_paths, flags, 0)
         h = P()
         check(self.lib.mc_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
         self.handle = h
