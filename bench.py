@@ -86,6 +86,8 @@ def parse():
     ap.add_argument("--guide-pretrain-spp", type=int, default=0,
                     help="diagnostic: train the guide on this many untimed samples first (the headline trains from "
                          "scratch inside the timed region)")
+    ap.add_argument("--guide-fold", action="store_true",
+                    help="mirror guide directions below the surface up instead of ending those paths")
     ap.add_argument("--guide-weight-cap", type=float, default=0.0,
                     help="training: cap of a record's share of a step's weight, in units of 1 / records (0 = none)")
     ap.add_argument("--guide-depth", type=int, default=0,
@@ -704,7 +706,8 @@ def run_guiding(args, emit=True):
     gdir = mcpt.GUIDE_DIR_NORMAL if args.guide_dir == "normal" else mcpt.GUIDE_DIR_RAY
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
                             train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
-                            guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap)
+                            guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
+                            fold_below=args.guide_fold)
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -731,7 +734,8 @@ def run_guiding(args, emit=True):
     # guided, trained online from scratch
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
                        train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
-                       guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap)
+                       guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
+                       fold_below=args.guide_fold)
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -790,7 +794,7 @@ def run_guiding(args, emit=True):
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
            "pretrain_spp": args.guide_pretrain_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
-           "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap,
+           "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap, "fold_below": bool(args.guide_fold),
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,

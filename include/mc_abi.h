@@ -711,7 +711,9 @@ typedef struct mc_guide_config {
                                    is capped at weight_cap / (records in the step), so a few rare bright paths
                                    cannot take over a step (0 = no cap). The estimator stays unbiased: only
                                    the proposal the guide learns changes */
-    int32_t pad0, pad1, pad2;
+    int32_t fold_below;         /* guided renders: the guide's directions below the surface are mirrored up
+                                   (the density counts both) instead of ending the path; 0 = off */
+    int32_t pad1, pad2;
 } mc_guide_config;
 
 #define MC_GUIDE_MAX_TRAIN_VERTICES 4

@@ -435,6 +435,7 @@ struct ShadeArgs {
     int recSlots;
     int dirNormal;
     int mixShare;     // bounce 0 of a single-item pixel-major wave: the pixel's samples read its first path's mixture
+    int fold;         // guide directions below the surface are mirrored up (guided_pdf)
 };
 
 // Training record of a diffuse vertex (recSlots per path, slot = depth):
@@ -506,10 +507,16 @@ MC_D MatView load_material(const mc_material& m) {
 
 // Density of the guided direction sampler at a diffuse vertex: the cosine
 // lobe with probability 1 - frac, the guide's mixture with probability frac.
-// The guide's directions below the surface are folded up (mirrored in the
-// tangent plane), so none is lost to a zero BSDF: the guide's density at w
-// above the surface is q(w) + q(w') with w' the mirror image of w; below it is 0.
-MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w) {
+// fold: the guide's directions below the surface are folded up (mirrored in
+// the tangent plane), so none is lost to a zero BSDF: the guide's density at w
+// above the surface is then q(w) + q(w') with w' the mirror image of w, and 0
+// below. Without folding a guide direction below the surface ends the path
+// (its BSDF is zero): cheaper per sample, noisier while the guide is young.
+MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w, bool fold) {
+    if (!fold) {
+        const float c = fmaxf(n.dot(w), 0.0f);
+        return (1.0f - frac) * (c / MC_PI) + frac * guide::mixture_pdf(m, w.x, w.y, w.z);
+    }
     const float c = n.dot(w);
     if (!(c > 0.0f)) return 0.0f;
     const V3 r = w - n * (2.0f * c);
@@ -673,7 +680,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             float phasePdf = hg_phase_pdf(inDir.dot(toLight), mat.g);
             float scatterPdf = iso ? phasePdf : lambertian_cosine_pdf(cosS);
             if (GUIDED && !iso && mat.type == MC_MAT_LAMBERTIAN)
-                scatterPdf = guided_pdf(a.mix + (size_t)mix_path(a, S, p) * guide::kOut, a.guideFrac, hitNormal, toLight);
+                scatterPdf = guided_pdf(a.mix + (size_t)mix_path(a, S, p) * guide::kOut, a.guideFrac, hitNormal, toLight, a.fold != 0);
             float scatterValue = iso ? phasePdf : cosS / MC_PI;
             float neeW = power_heuristic(solidPdf, scatterPdf);
             V3 contribution = throughput * lightColor * (scatterValue / solidPdf) * neeW;
@@ -717,7 +724,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
                         guide::mixture_sample(m, u0, u1, u2, d3);
                         nd = V3(d3[0], d3[1], d3[2]);
                         const float below = nd.dot(hitNormal);
-                        if (below < 0.0f) nd = nd - hitNormal * (2.0f * below);  // folded up (guided_pdf)
+                        if (a.fold && below < 0.0f) nd = nd - hitNormal * (2.0f * below);  // folded up (guided_pdf)
                     } else {
                         nd = lambertian_scatter(hitNormal, rng);
                     }
@@ -726,7 +733,7 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
                         survives = false;  // below the surface: the BSDF is zero
                         break;
                     }
-                    guidedPdf = guided_pdf(m, a.guideFrac, hitNormal, nd);
+                    guidedPdf = guided_pdf(m, a.guideFrac, hitNormal, nd, a.fold != 0);
                     throughput = throughput * ((c / MC_PI) / guidedPdf);
                     if (a.rec && depth < a.recSlots && depth + 1 < S.maxDepth) {
                         // the direction is traced next: a training record of this vertex
@@ -1619,6 +1626,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 sd.recSlots = guide->cfg.train_vertices;
                 sd.dirNormal = guide->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
                 sd.mixShare = d == 0 && shareMix ? 1 : 0;
+                sd.fold = guide->cfg.fold_below ? 1 : 0;
                 phaseBegin(1);
                 if (alias) k_shade<PhiloxRng, true, true><<<guidedBlocks, 256, 0, stream>>>(sd);
                 else k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
