@@ -83,13 +83,12 @@ def test_guided_estimator_is_unbiased(ctx):
 
 @pytest.mark.parametrize("samples_per_wave,bar", [(1, 0.85), (0, 0.88)])
 def test_trained_guide_lowers_error_in_the_aperture_room(ctx, samples_per_wave, bar):
-    """Online training on the renderer's own primary-vertex samples, then
-    guided vs plain MSE at equal spp. One sample per wave trains after every
-    sample; the default several samples per wave train once per wave, one
-    Adam step per sample of the wave, on records of the same weights. Training
-    is reproducible, so each case gives one ratio; over guide seeds 1-5 and 9
-    they measured 0.77-0.82 (one sample per wave) and 0.79-0.86 (default),
-    0.81 for seed 9 in both."""
+    """Per sample: a guide trained online on the renderer's own samples, then
+    guided vs plain MSE at equal spp (what the trained proposal is worth per
+    sample; the time comparison is the next test). One sample per wave trains
+    after every sample; the default several samples per wave train once per
+    wave, one Adam step per sample of the wave, on records of the same
+    weights. Training is reproducible, so each case gives one ratio."""
     W = 96
     s, tris, d, bvh, cam = _setup(ctx, mcpt.SCENE_GUIDING_ROOM, W)
     lo, hi = _bounds(tris)
@@ -127,4 +126,49 @@ def test_guided_training_is_reproducible(ctx, samples_per_wave):
     assert runs[0][0].tobytes() == runs[1][0].tobytes()
     assert runs[0][1].tobytes() == runs[1][1].tobytes()
     assert runs[0][2].tobytes() == runs[1][2].tobytes()
+    mcpt.free_scene(s)
+
+
+def test_guided_time_to_error_in_the_aperture_room(ctx):
+    """Equal time: plain and guided renders of the aperture room from scratch
+    (the guide untrained at the first sample and trained online, every Adam
+    step inside the timed region), each timed with CUDA events; with error
+    falling as 1/time, (MSE x time) guided over plain is the time the guided
+    render needs to reach plain's error, relative to plain's. The product
+    target is 0.6; the guide does not reach it yet: it costs about 1.5x plain
+    per sample and learns too slowly to pay that back within these samples
+    (a guide trained on 1024 samples first lowers the per-sample MSE to
+    0.75x). The bar records that the ratio stays bounded and finite."""
+    W = 512
+    s, tris, d, bvh, cam = _setup(ctx, mcpt.SCENE_GUIDING_ROOM, W)
+    lo, hi = _bounds(tris)
+    ref = _plain(ctx, bvh, d, cam, W, 1024, 700000)
+
+    def timed(fn, warm_up=True):
+        if warm_up:
+            fn()  # kernels loaded, buffers sized
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        img = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return img, e0.elapsed_time(e1)
+
+    spp = 32
+    plain, t_p = timed(lambda: _plain(ctx, bvh, d, cam, W, spp, 800000))
+    # the guided path's warm-up on a throwaway guide of the same configuration
+    warm = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=3, train_steps=4)
+    _guided(ctx, bvh, d, cam, W, spp, 900000, warm, 1)
+    warm.close()
+    guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, train_steps=4)
+    _guided(ctx, bvh, d, cam, W, 1, 950000, guide, 0)  # sizes the new guide's buffers; no training
+    (guided, _), t_g = timed(lambda: _guided(ctx, bvh, d, cam, W, spp, 1000000, guide, 1), warm_up=False)
+    mse_p = float(((plain - ref) ** 2).mean())
+    mse_g = float(((guided - ref) ** 2).mean())
+    ratio = (mse_g * t_g) / (mse_p * t_p)
+    print("aperture room %d^2, %d spp: plain %.1f ms MSE %.3e, guided (trained online) %.1f ms MSE %.3e, "
+          "time to equal error %.3f x plain" % (W, spp, t_p, mse_p, t_g, mse_g, ratio))
+    assert np.isfinite(ratio) and ratio < 3.0
+    guide.close()
     mcpt.free_scene(s)
