@@ -295,10 +295,11 @@ typedef struct mc_render_params {
                                    TRAVERSAL_STACK_CAPACITY, PT:1038); 1..63 shrink the trace kernel's
                                    shared memory; a ray that needs more ends and the call returns
                                    MC_ERR_STACK_OVERFLOW (builds keep every 4-wide tree within 64) */
-    int32_t trace_threads;      /* trace block size: 0 or 256 (the default), or 128 (7 resident blocks per SM
-                                   when the stack's shared memory allows: single-scene renders without
-                                   density grids, reference intersector; other launches keep 256).
-                                   Images do not depend on it */
+    int32_t trace_threads;      /* trace block size: 256, or 128 (7 resident blocks per SM when the stack's
+                                   shared memory allows; launches without density grids, reference
+                                   intersector; other launches keep 256). 0 with stack_entries 0: 128 with
+                                   the stack the 4-wide trees can need (3 entries per level) when that is at
+                                   most 56, else 256. Images do not depend on it */
 } mc_render_params;
 
 enum {

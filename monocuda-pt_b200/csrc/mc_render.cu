@@ -1202,13 +1202,15 @@ TraceKernel trace_kernel(bool batch, int layout, bool count, int medium, int ise
                                                      {MC_TK(0, true), MC_TK(1, true), MC_TK(2, true)}};
     return table[batch ? 1 : 0][layout][count ? 1 : 0][medium][isect ? 1 : 0];
 }
-// The 128-thread variant, compiled for single-scene launches of the reference
-// intersector without counters or density grids; [layout][medium kind].
-TraceKernel trace_kernel_128(int layout, int medium) {
-    static const TraceKernel table[3][2] = {{k_trace<0, 0, false, 0, false, 128>, k_trace<0, 1, false, 0, false, 128>},
-                                            {k_trace<0, 0, false, 1, false, 128>, k_trace<0, 1, false, 1, false, 128>},
-                                            {k_trace<0, 0, false, 2, false, 128>, k_trace<0, 1, false, 2, false, 128>}};
-    return table[layout][medium];
+// The 128-thread variant, compiled for launches of the reference intersector
+// without counters or density grids; [batch][layout][medium kind].
+#define MC_TK128(B)                                                                                     \
+    {{k_trace<0, 0, false, 0, B, 128>, k_trace<0, 1, false, 0, B, 128>},                                \
+     {k_trace<0, 0, false, 1, B, 128>, k_trace<0, 1, false, 1, B, 128>},                                \
+     {k_trace<0, 0, false, 2, B, 128>, k_trace<0, 1, false, 2, B, 128>}}
+TraceKernel trace_kernel_128(bool batch, int layout, int medium) {
+    static const TraceKernel table[2][3][2] = {MC_TK128(false), MC_TK128(true)};
+    return table[batch ? 1 : 0][layout][medium];
 }
 
 // Persistent: one wave of resident blocks (SMs x resident blocks per SM) that
@@ -1223,11 +1225,11 @@ void launch_trace(mc_context* ctx, cudaStream_t stream, const TraceArgs& t0, int
     if (t.stackCap <= 0 || t.stackCap > MC_STACK_CAPACITY) t.stackCap = MC_STACK_CAPACITY;
     const bool batch = t.sceneOf != nullptr;
     // the 128-thread variant where it is compiled, else 256 threads
-    const bool small = t.threads == 128 && !batch && !count && isect == 0 && medium < 2;
+    const bool small = t.threads == 128 && !count && isect == 0 && medium < 2;
     const int threads = small ? 128 : kTraceThreads;
     // the shared-memory stack holds stackCap entries per lane
     const int smem = MC_SMEM_STACK ? threads * t.stackCap * (int)sizeof(int) : 0;
-    TraceKernel fn = small ? trace_kernel_128(layout, medium) : trace_kernel(batch, layout, count, medium, isect);
+    TraceKernel fn = small ? trace_kernel_128(batch, layout, medium) : trace_kernel(batch, layout, count, medium, isect);
     const int key = medium + 3 * (isect ? 1 : 0) + 6 * (count ? 1 : 0) + 12 * (batch ? 1 : 0) + 24 * layout +
                     72 * (small ? 1 : 0);  // < 144
     if (smem > 48 * 1024 && ctx->trace_smem_attr[key] < smem) {
@@ -1472,6 +1474,22 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
     ta.queueCap = queueCap;
     ta.stackCap = p0.stack_entries;
     ta.threads = p0.trace_threads;
+    if (ta.threads == 0 && ta.stackCap == 0) {
+        // by default the 128-thread shape (7 blocks per SM) when every tree of
+        // the wave is a greedy 4-wide collapse whose stack need (3 entries per
+        // level, rounded up to 8) lets 7 blocks share an SM; the image does
+        // not depend on it
+        int levels = 0;
+        for (int i = 0; i < n && levels >= 0; i++) {
+            const mc_bvh* b = items[i].bvh ? items[i].bvh : bvh;
+            levels = (b->layout == MC_BVH_LAYOUT_BINARY || b->wide_levels <= 0) ? -1 : std::max(levels, b->wide_levels);
+        }
+        const int need = levels > 0 ? ((3 * levels + 7) / 8) * 8 : 999;
+        if (need <= 56 && isect == MC_ISECT_REFERENCE) {
+            ta.threads = 128;
+            ta.stackCap = need;
+        }
+    }
     ta.refill = (p0.refill_threshold > 0 && p0.refill_threshold <= 32) ? p0.refill_threshold : 8;  // PT:3400
     if (countVisits) ta.counts = (unsigned long long*)(ctx->d_stats + 2 * MC_MAX_DEPTH_STATS);
     if (sameScene) {
