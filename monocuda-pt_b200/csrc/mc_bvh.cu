@@ -1102,6 +1102,16 @@ mc_status radix_sort_pairs_static(mc_context* ctx, uint32_t* keys, int32_t* vals
     return MC_OK;
 }
 
+// Build buffers come from the device's stream-ordered pool (pool_alloc): they
+// are taken and returned in stream order, without a device-wide wait.
+template <class T>
+static bool palloc(mc_context* ctx, T** p, size_t bytes) {
+    void* v = nullptr;
+    const bool ok = pool_alloc(ctx, &v, bytes) == MC_OK;
+    *p = (T*)v;
+    return ok;
+}
+
 mc_status bvh_depth(mc_bvh* bvh) {
     if (bvh->depth >= 0) return MC_OK;
     if (bvh->n == 1) {
@@ -1110,13 +1120,13 @@ mc_status bvh_depth(mc_bvh* bvh) {
     }
     mc_context* ctx = bvh->ctx;
     int* d;
-    MC_CUDA(cudaMalloc(&d, sizeof(int)));
+    if (!palloc(ctx, &d, sizeof(int))) return MC_ERR_OOM;
     MC_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx->stream));
     k_leaf_depth<<<grid_for(bvh->n, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, bvh->n, bvh->ni, d);
     int h = 0;
     MC_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     MC_CUDA(cudaStreamSynchronize(ctx->stream));
-    cudaFree(d);
+    pool_free(ctx, d);
     bvh->depth = h;
     return MC_OK;
 }
@@ -1411,7 +1421,7 @@ static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg,
     const size_t bytes = (size_t)NI * 64 + 2 * (size_t)N * 4 + 4 * (size_t)N * 16 + (size_t)N * 4 + 2 * (size_t)N * 8 +
                          (size_t)(nbMax + 1) * 8 + 32 + 16 * 16;  // + the 16-byte rounding of each part
     char* mem = nullptr;
-    if (cudaMalloc(&mem, bytes) != cudaSuccess) {
+    if (!palloc(ctx, &mem, bytes)) {
         cudaGetLastError();
         return set_error(MC_ERR_OOM, "mc_bvh_build: clustering scratch allocation failed");
     }
@@ -1426,7 +1436,7 @@ static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg,
     int2* sums = (int2*)take((size_t)(nbMax + 1) * 8);
     int2* total = (int2*)take(32);  // the round's totals, then [2..3] as ints: clusters, next node id
     auto fail = [&](mc_status s) {
-        cudaFree(mem);
+        pool_free(ctx, mem);
         tree.nodes = nullptr;
         return s;
     };
@@ -1507,20 +1517,20 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         int4* internal = nullptr;  // per frontier node: its internal slots
         int* blockTotals = nullptr;
         auto release = [&]() {
-            cudaFree(front[0]);
-            cudaFree(front[1]);
-            cudaFree(cnt);
-            cudaFree(internal);
-            cudaFree(blockTotals);
+            pool_free(ctx, front[0]);
+            pool_free(ctx, front[1]);
+            pool_free(ctx, cnt);
+            pool_free(ctx, internal);
+            pool_free(ctx, blockTotals);
         };
-        if (cudaMalloc(&rootOf, (size_t)NI * sizeof(int)) != cudaSuccess ||
-            cudaMalloc(&front[0], (size_t)NI * sizeof(int)) != cudaSuccess ||
-            cudaMalloc(&front[1], (size_t)NI * sizeof(int)) != cudaSuccess || cudaMalloc(&cnt, 4 * sizeof(int)) != cudaSuccess ||
-            cudaMalloc(&internal, (size_t)NI * sizeof(int4)) != cudaSuccess ||
-            cudaMalloc(&blockTotals, (size_t)(grid_for(NI, kBlock) + 1) * sizeof(int)) != cudaSuccess) {
+        if (!palloc(ctx, &rootOf, (size_t)NI * sizeof(int)) ||
+            !palloc(ctx, &front[0], (size_t)NI * sizeof(int)) ||
+            !palloc(ctx, &front[1], (size_t)NI * sizeof(int)) || !palloc(ctx, &cnt, 4 * sizeof(int)) ||
+            !palloc(ctx, &internal, (size_t)NI * sizeof(int4)) ||
+            !palloc(ctx, &blockTotals, (size_t)(grid_for(NI, kBlock) + 1) * sizeof(int))) {
             cudaGetLastError();
             release();
-            cudaFree(rootOf);
+            pool_free(ctx, rootOf);
             return set_error(MC_ERR_OOM, "mc_bvh_build: wide-collapse scratch allocation failed");
         }
         MC_CUDA(cudaMemsetAsync(wideId, 0xFF, (size_t)NI * sizeof(int), ctx->stream));
@@ -1541,7 +1551,7 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
             if (n < 0 || (long long)idBase + n > NI) {
                 // more wide nodes than internal nodes: not a binary tree over these leaves
                 release();
-                cudaFree(rootOf);
+                pool_free(ctx, rootOf);
                 return set_error(MC_ERR_INVALID, "mc_bvh_build: the collapse found %d nodes past %d", n, idBase);
             }
             idBase += n;
@@ -1552,7 +1562,7 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         int flags = 0;
         if ((st = flags_now(ctx, &flags)) != MC_OK || flags) {
             release();
-            cudaFree(rootOf);
+            pool_free(ctx, rootOf);
             return st != MC_OK ? st : status_from_device_flags(flags);
         }
         release();
@@ -1560,11 +1570,11 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         greedy = n == 0 && 3 * levels <= MC_STACK_CAPACITY;
         bvh->wide_levels = greedy ? levels : -1;
         if (!greedy && tree) {
-            cudaFree(rootOf);
+            pool_free(ctx, rootOf);
             return MC_ERR_UNSUPPORTED;
         }
         if (!greedy) {
-            cudaFree(rootOf);
+            pool_free(ctx, rootOf);
             rootOf = nullptr;
             MC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
             k_wide_select<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>(bvh->parents, dSeg, nseg, NI, wideId, counter,
@@ -1574,13 +1584,13 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
     }
     int flags = 0;
     if ((st = flags_now(ctx, &flags)) != MC_OK || flags) {
-        cudaFree(rootOf);
+        pool_free(ctx, rootOf);
         return st != MC_OK ? st : status_from_device_flags(flags);
     }
-    if (cudaMalloc(&bvh->wide_nodes, (size_t)count * 128) != cudaSuccess ||
-        cudaMalloc(&bvh->wide_prims, (size_t)N * 48) != cudaSuccess) {
+    if (!palloc(ctx, &bvh->wide_nodes, (size_t)count * 128) ||
+        !palloc(ctx, &bvh->wide_prims, (size_t)N * 48)) {
         cudaGetLastError();
-        cudaFree(rootOf);
+        pool_free(ctx, rootOf);
         return set_error(MC_ERR_OOM, "mc_bvh_build: wide-node allocation failed");
     }
     bvh->wide_roots.assign(nseg, 0);
@@ -1589,7 +1599,7 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
                                                                               rank, count, (float4*)bvh->wide_nodes);
         for (int s = 0; s < nseg; s++) bvh->wide_roots[s] = s;
         MC_CUDA(cudaStreamSynchronize(ctx->stream));
-        cudaFree(rootOf);
+        pool_free(ctx, rootOf);
     } else if (NI > 0) {
         k_wide_fill<<<grid_for(NI, kBlock), kBlock, 0, ctx->stream>>>((const float4*)bvh->nodes, wideId, rank, NI,
                                                                      (float4*)bvh->wide_nodes);
@@ -1642,6 +1652,7 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
 
     mc_bvh* bvh = new mc_bvh();
     bvh->ctx = ctx;
+    bvh->device = ctx->device;
     bvh->n = N;
     bvh->ni = NI;
     bvh->ns = nseg == 1 ? views[0].sphere_count : 0;
@@ -1651,18 +1662,18 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
     auto fail = [&](mc_status s) { mc_bvh_free(bvh); return s; };
 
     long long nodesCount = std::max(1, NI);
-    if (cudaMalloc(&bvh->nodes, (size_t)nodesCount * 64) != cudaSuccess ||
-        cudaMalloc(&bvh->prims, (size_t)N * 48) != cudaSuccess ||
-        cudaMalloc(&bvh->codes, (size_t)N * 4) != cudaSuccess ||
-        cudaMalloc(&bvh->ids, (size_t)N * 4) != cudaSuccess ||
-        cudaMalloc(&bvh->types, (size_t)N * 4) != cudaSuccess ||
-        cudaMalloc(&bvh->parents, (size_t)(NI + N) * 4 + 8) != cudaSuccess) {
+    if (!palloc(ctx, &bvh->nodes, (size_t)nodesCount * 64) ||
+        !palloc(ctx, &bvh->prims, (size_t)N * 48) ||
+        !palloc(ctx, &bvh->codes, (size_t)N * 4) ||
+        !palloc(ctx, &bvh->ids, (size_t)N * 4) ||
+        !palloc(ctx, &bvh->types, (size_t)N * 4) ||
+        !palloc(ctx, &bvh->parents, (size_t)(NI + N) * 4 + 8)) {
         cudaGetLastError();
         return fail(set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (n=%d)", N));
     }
     if (o.keep_reference_nodes) {
-        if (cudaMalloc(&bvh->ref_internal, (size_t)nodesCount * sizeof(mc_bvh_node)) != cudaSuccess ||
-            cudaMalloc(&bvh->ref_leaves, (size_t)N * sizeof(mc_bvh_node)) != cudaSuccess) {
+        if (!palloc(ctx, &bvh->ref_internal, (size_t)nodesCount * sizeof(mc_bvh_node)) ||
+            !palloc(ctx, &bvh->ref_leaves, (size_t)N * sizeof(mc_bvh_node))) {
             cudaGetLastError();
             return fail(set_error(MC_ERR_OOM, "mc_bvh_build: device allocation failed (reference nodes)"));
         }
@@ -1723,15 +1734,14 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
             // the sort needs its own two scratch arrays: reuse the node buffer (>= N-1 ints) is not enough, so allocate
             uint32_t* altK = nullptr;
             int32_t* altV = nullptr;
-            if (cudaMalloc(&altK, (size_t)N * 4) != cudaSuccess || cudaMalloc(&altV, (size_t)N * 4) != cudaSuccess) {
+            if (!palloc(ctx, &altK, (size_t)N * 4) || !palloc(ctx, &altV, (size_t)N * 4)) {
                 cudaGetLastError();
-                cudaFree(altK);
+                pool_free(ctx, altK);
                 return fail(set_error(MC_ERR_OOM, "mc_bvh_build_batch: sort scratch allocation failed"));
             }
             st = radix_sort_pairs(ctx, segKeys, order, altK, altV, N, bits);
-            cudaStreamSynchronize(ctx->stream);
-            cudaFree(altK);
-            cudaFree(altV);
+            pool_free(ctx, altK);
+            pool_free(ctx, altV);
             if (st != MC_OK) return fail(st);
             k_gather_u32<<<grid_for(N, kBlock), kBlock, 0, ctx->stream>>>(codesRef, order, N, bvh->codes, ctx->d_error);
         }
@@ -1781,14 +1791,14 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
             st = build_ploc(ctx, bvh, dSeg, nseg, order, boundsRef, tree);
             if (st == MC_OK) {
                 st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot, tree.nodes, &tree.roots);
-                cudaFree(tree.nodes);
+                pool_free(ctx, tree.nodes);
                 if (st == MC_OK) bvh->builder = MC_BVH_BUILDER_CLUSTERED;
             }
             if (st != MC_OK && st != MC_ERR_UNSUPPORTED) return fail(st);
         }
         if (st == MC_ERR_UNSUPPORTED) {
-            if (bvh->wide_nodes) cudaFree(bvh->wide_nodes);
-            if (bvh->wide_prims) cudaFree(bvh->wide_prims);
+            if (bvh->wide_nodes) pool_free(ctx, bvh->wide_nodes);
+            if (bvh->wide_prims) pool_free(ctx, bvh->wide_prims);
             bvh->wide_nodes = bvh->wide_prims = nullptr;
             if ((st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot)) != MC_OK) return fail(st);
             bvh->builder = MC_BVH_BUILDER_LBVH;
@@ -1796,17 +1806,17 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
     }
     if (o.layout == MC_BVH_LAYOUT_WIDE4Q) {
         void* q = nullptr;
-        if (cudaMalloc(&q, (size_t)bvh->wide_count * 64) != cudaSuccess) {
+        if (!palloc(ctx, &q, (size_t)bvh->wide_count * 64)) {
             cudaGetLastError();
             return fail(set_error(MC_ERR_OOM, "mc_bvh_build: quantised-node allocation failed"));
         }
         k_quantize_wide<<<grid_for((int)bvh->wide_count, kBlock), kBlock, 0, ctx->stream>>>(
             (const float4*)bvh->wide_nodes, (int)bvh->wide_count, (float4*)q);
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
-            cudaFree(q);
+            pool_free(ctx, q);
             return fail(cuda_error(cudaGetLastError(), "mc_bvh_build (quantise)", __FILE__, __LINE__));
         }
-        cudaFree(bvh->wide_nodes);
+        pool_free(ctx, bvh->wide_nodes);
         bvh->wide_nodes = q;
         bvh->layout = MC_BVH_LAYOUT_WIDE4Q;
     }
@@ -1888,16 +1898,15 @@ mc_status mc_bvh_build_batch(mc_context* ctx, const mc_scene_view* scenes, int32
 
 mc_status mc_bvh_free(mc_bvh* bvh) {
     if (!bvh) return MC_OK;
-    cudaFree(bvh->nodes);
-    cudaFree(bvh->prims);
-    cudaFree(bvh->wide_nodes);
-    cudaFree(bvh->wide_prims);
-    cudaFree(bvh->codes);
-    cudaFree(bvh->ids);
-    cudaFree(bvh->types);
-    cudaFree(bvh->parents);
-    cudaFree(bvh->ref_internal);
-    cudaFree(bvh->ref_leaves);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != bvh->device) cudaSetDevice(bvh->device);
+    // work on any stream may still read the tree (cudaFree would wait for the device too)
+    cudaDeviceSynchronize();
+    void* bufs[] = {bvh->nodes, bvh->prims, bvh->wide_nodes, bvh->wide_prims, bvh->codes,
+                    bvh->ids, bvh->types, bvh->parents, bvh->ref_internal, bvh->ref_leaves};
+    for (void* b : bufs) mc::pool_release(b);
+    if (prev >= 0 && prev != bvh->device) cudaSetDevice(prev);
     delete bvh;
     return MC_OK;
 }

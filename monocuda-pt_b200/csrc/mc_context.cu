@@ -66,6 +66,67 @@ void devbuf_free(DevBuf& b) {
     b.bytes = 0;
 }
 
+// One stream-ordered memory pool per device for the BVH build's buffers. It
+// keeps what is freed (release threshold: never), so a build after the first
+// takes its memory without a driver allocation; plain cudaMalloc / cudaFree
+// pairs per build cost from well under a millisecond to hundreds of
+// milliseconds each. The pools live as long as the process: a tree may
+// outlive the context that built it.
+namespace {
+std::mutex g_pool_mutex;
+std::unordered_map<int, cudaMemPool_t> g_pools;
+}
+
+static cudaMemPool_t device_pool(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    auto it = g_pools.find(device);
+    if (it != g_pools.end()) return it->second;
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[device] = pool;
+    return pool;
+}
+
+mc_status pool_alloc(mc_context* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    cudaMemPool_t pool = device_pool(ctx->device);
+    if (!pool) return set_error(MC_ERR_CUDA, "device %d: memory pool creation failed", ctx->device);
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes < 256 ? 256 : bytes, pool, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return set_error(MC_ERR_OOM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return MC_OK;
+}
+
+void pool_free(mc_context* ctx, void* p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+// For a caller that has made the pool's device current and waited for the
+// work that reads p.
+void pool_release(void* p) {
+    if (p) cudaFreeAsync(p, 0);
+}
+
+void pool_trim(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    auto it = g_pools.find(device);
+    if (it != g_pools.end()) cudaMemPoolTrimTo(it->second, 0);
+}
+
 // One lane polls *flag (system-scope acquire loads, so a flag in mapped host
 // memory or a peer's memory is seen) with a back-off sleep, until it reaches
 // value or the device clock says timeout_ns have passed; then the error word
@@ -174,6 +235,8 @@ mc_status mc_context_destroy(mc_context* ctx) {
     if (ctx->h_tables) cudaFreeHost(ctx->h_tables);
     cudaFree(ctx->scene_of);
     if (ctx->staging) cudaFreeHost(ctx->staging);
+    // the pool keeps the trees still alive; what it holds unused goes back
+    mc::pool_trim(ctx->device);
     delete ctx;
     return MC_OK;
 }

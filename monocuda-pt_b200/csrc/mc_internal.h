@@ -51,6 +51,11 @@ struct DevBuf {
 };
 mc_status devbuf_reserve(DevBuf& b, size_t bytes);
 void devbuf_free(DevBuf& b);
+// stream-ordered allocations from the device's pool (BVH build buffers)
+mc_status pool_alloc(mc_context* ctx, void** p, size_t bytes);
+void pool_free(mc_context* ctx, void* p);  // ordered after the work queued on ctx's stream
+void pool_release(void* p);                // device current and its readers finished
+void pool_trim(int device);                // hands the pool's unused memory back
 
 // Copies `bytes` of host memory to the device; complete when the call returns.
 // Large copies from pageable memory go through the context's pinned staging
@@ -126,6 +131,7 @@ struct mc_context {
 
 struct mc_bvh {
     mc_context* ctx = nullptr;
+    int device = 0;
     int n = 0, ns = 0, nt = 0;
     int ni = 0;                        // internal binary nodes over all segments
     int nseg = 1;                      // scenes in this build (a batch build has several)
