@@ -4,22 +4,29 @@
 // 8-lobe vMF mixture). Every layer is a tcgen05.mma (kind::f16, BF16 operands
 // from shared memory, FP32 accumulators in tensor memory) over a tile of 128
 // queries, issued by one thread; the 128 threads of the CTA each own one
-// query row for the epilogues (TMEM -> registers -> bias/ReLU -> BF16 ->
-// shared memory as the next layer's operand).
+// query row for the epilogues (TMEM -> registers -> ReLU -> BF16 -> shared
+// memory as the next layer's operand). Each bias is folded into its layer's
+// MMA (a [1, 1, 0...] column block on the activations against a
+// [hi, lo, 0...] block on the weights), so a forward epilogue is one
+// ReLU-and-convert instruction per pair of columns.
 //
 // Training (one kernel, forward + backward per tile of 128 records):
-//   forward   Z_l = H_{l-1} W_l^T + b_l          (A = activations, B = W_l)
+//   forward   Z_l = [H_{l-1} | 1 1 0..] Wb_l^T   (A = activations, B = Wb_l)
 //   loss      -w log q(next) of the vMF mixture, gradient dY per row (FP32)
-//   backward  dH_{l-1} = dZ_l W_l                (A = dZ_l, B = W_l^T copy)
-//             dW_l += dZ_l^T [H_{l-1} | 1]       (A = dZ_l^T, rows padded to
-//                                                 128; B = H^T plus a row of
-//                                                 ones, so the last column is
-//                                                 the bias gradient)
-// The weight gradients accumulate in tensor memory over all tiles a CTA
-// processes (464 of the 512 columns) and are written once per CTA as FP32
-// partials; the Adam kernel sums the partials in a fixed order
-// (deterministic) and updates FP32 master weights, from which the BF16
-// operand copies are regenerated.
+//   backward  dH_{l-1} = dZ_l W_l                (A = dZ_l, B = Wb_l read
+//                                                 MN-major)
+//             dW_l += dZ_l^T [H_{l-1} | 1 1 0..] (A = the dZ_l rows read
+//                                                 MN-major as 128 output
+//                                                 rows, the upper ones zero;
+//                                                 B = the activation rows read
+//                                                 MN-major; the first ones
+//                                                 column gives the bias
+//                                                 gradient)
+// Reading the stored rows MN-major replaces every transposed copy. The weight
+// gradients accumulate in tensor memory over all tiles a CTA processes (464
+// of the 512 columns) and are written once per CTA as FP32 partials; the Adam
+// kernel sums the partials in a fixed order (deterministic) and updates FP32
+// master weights, from which the BF16 operands are regenerated.
 //
 // Compiled without fast math: the encoding and the loss are compared with an
 // FP64 restatement.
@@ -51,43 +58,41 @@ constexpr int kTile = 128;
 constexpr long long kWaitLimit = 1ll << 20;
 
 // ---- shared-memory layouts (bytes) ----
-// inference
+// inference (bias-folded operands: inputs of kInK and kHidK columns)
 constexpr int iW1 = 0;
-constexpr int iW2 = iW1 + kHid * kIn * 2;
-constexpr int iW3 = iW2 + kHid * kHid * 2;
-constexpr int iW4 = iW3 + kHid * kHid * 2;
+constexpr int iW2 = iW1 + kHid * kInK * 2;
+constexpr int iW3 = iW2 + kHid * kHidK * 2;
+constexpr int iW4 = iW3 + kHid * kHidK * 2;
 // kInferGroups warpgroups per CTA share one copy of the weights; each has its
 // own tile buffer (the encoded inputs X0, then in place each hidden layer's
 // activations once the MMA that read the previous contents has finished) and
 // its own 64 TMEM columns, so while one group waits on its MMA the others run
 // their epilogues.
 constexpr int kInferGroups = 4;
-constexpr int iBias = iW4 + kOutPad * kHid * 2;
-constexpr int iTiles = iBias + (3 * kHid + kOutPad) * 4 + 64;  // 64: keeps the tile buffers 128-byte aligned
-constexpr int kInferTileBytes = kTile * kIn * 2;
+constexpr int iTiles = iW4 + kOutPad * kHidK * 2;
+constexpr int kInferTileBytes = kTile * kInK * 2;
 constexpr int kInferSmem = iTiles + kInferGroups * kInferTileBytes;
 static_assert(iTiles % 128 == 0 && kInferTileBytes % 128 == 0, "operand buffers must stay aligned");
-static_assert(kTile * kHid * 2 <= kInferTileBytes, "the activations fit the input buffer");
-static_assert(kInferSmem <= 232448, "inference CTA exceeds the shared memory of one CTA");
-// training
+static_assert(kTile * kHidK * 2 <= kInferTileBytes, "the activations fit the input buffer");
+static_assert(kInferSmem <= 232448 - 1024, "inference CTA exceeds the shared memory of one CTA");
+// training: the inference operands (bias-folded weights, encoded inputs and
+// activations with their bias blocks), plus the gradient rows
 constexpr int tW1 = 0;
-constexpr int tW2 = tW1 + kHid * kIn * 2;
-constexpr int tW3 = tW2 + kHid * kHid * 2;
-constexpr int tW4 = tW3 + kHid * kHid * 2;
-constexpr int tW2t = tW4 + kOutPad * kHid * 2;
-constexpr int tW3t = tW2t + kHid * kHid * 2;
-constexpr int tW4t = tW3t + kHid * kHid * 2;
-constexpr int tE = tW4t + kHid * kOutPad * 2;           // X0 (128 x 144) or X0^T + ones row (160 x 128)
-constexpr int tH1 = tE + 160 * kTile * 2;
-constexpr int tH2 = tH1 + kTile * kHid * 2;
-constexpr int tH3 = tH2 + kTile * kHid * 2;
-constexpr int tHt = tH3 + kTile * kHid * 2;             // H^T + ones row (80 x 128)
-constexpr int tD = tHt + 80 * kTile * 2;                // dZ (128 x 64) or dY (128 x 48)
-constexpr int tDt = tD + kTile * kHid * 2;              // dZ^T padded to 128 rows (128 x 128)
-constexpr int tBias = tDt + kTile * kTile * 2;
-constexpr int kTrainSmem = tBias + (3 * kHid + kOutPad) * 4;
-static_assert(kTrainSmem <= 232448, "training tile exceeds the shared memory of one CTA");
-static_assert(kTile * kIn * 2 <= 160 * kTile * 2, "X0 must fit the transposed buffer");
+constexpr int tW2 = tW1 + kHid * kInK * 2;
+constexpr int tW3 = tW2 + kHid * kHidK * 2;
+constexpr int tW4 = tW3 + kHid * kHidK * 2;
+constexpr int kDCols = 128;                             // gradient rows: dY or dZ in 0..63, zeros above
+constexpr int tD = tW4 + kOutPad * kHidK * 2;
+constexpr int tX = tD + kTile * kDCols * 2;             // encoded inputs + bias block (128 x 160)
+constexpr int tH1 = tX + kTile * kInK * 2;              // activations + bias block (128 x 80)
+constexpr int tH2 = tH1 + kTile * kHidK * 2;
+constexpr int tH3 = tH2 + kTile * kHidK * 2;
+// The MN-major reads span the whole of each buffer; a buffer is followed by
+// at least 9 KB more of the allocation (the tail after tH3), which an MN-major
+// read with its two descriptor strides exchanged would also stay inside.
+constexpr int kTrainSmem = tH3 + kTile * kHidK * 2 + 9216;
+static_assert(tD % 128 == 0 && tX % 128 == 0 && tH1 % 128 == 0, "operand buffers must stay aligned");
+static_assert(kTrainSmem <= 232448 - 1024, "training tile exceeds the shared memory of one CTA");
 
 // TMEM columns of the training kernel
 constexpr uint32_t cR = 0, cG1 = 64, cG2 = 224, cG3 = 304, cG4 = 384, kTrainCols = 512;
@@ -140,7 +145,8 @@ __device__ __forceinline__ void face_normal(const GuideInferArgs& a, int type, i
         n[0] = -dx; n[1] = -dy; n[2] = -dz;
         return;
     }
-    nx = nx / len; ny = ny / len; nz = nz / len;
+    const float r = 1.0f / len;
+    nx = nx * r; ny = ny * r; nz = nz * r;
     if (dx * nx + dy * ny + dz * nz >= 0.f) {
         nx = -nx; ny = -ny; nz = -nz;
     }
@@ -193,17 +199,6 @@ __device__ __forceinline__ void load_kmaj(unsigned char* dst, const bf16* src, i
     }
 }
 
-__device__ __forceinline__ void load_bias(float* sb, const float* master) {
-    for (int i = threadIdx.x; i < 3 * kHid + kOutPad; i += blockDim.x) {
-        float v = 0.f;
-        if (i < kHid) v = master[oB1 + i];
-        else if (i < 2 * kHid) v = master[oB2 + i - kHid];
-        else if (i < 3 * kHid) v = master[oB3 + i - 2 * kHid];
-        else if (i - 3 * kHid < kOut) v = master[oB4 + i - 3 * kHid];
-        sb[i] = v;
-    }
-}
-
 // TMEM address of column c of this warp's 32-lane slice (warp w of a
 // warpgroup reads lanes 32 (w % 4) .. 32 (w % 4) + 31).
 __device__ __forceinline__ uint32_t tcol(uint32_t base, uint32_t c) {
@@ -234,27 +229,46 @@ __device__ __forceinline__ bool wg_wait_mma(int g, uint64_t* bar, uint32_t& phas
     return true;
 }
 
-// Encodes one query row into the K-major X0 operand.
-__device__ __forceinline__ void encode_row(unsigned char* sE, int row, const float* coord6) {
-#pragma unroll 1
-    for (int ch = 0; ch < kIn / 8; ch++) {
-        float f[8];
-        encode_chunk(coord6, ch, f);
-        *reinterpret_cast<uint4*>(sE + kmaj_off(row, ch * 8, kIn)) = pack8_bf16(f);
-    }
+// The bias block [1, 1, 0, ...] of a bias-folded operand row (columns k0..k0+15).
+__device__ __forceinline__ void store_bias_block(unsigned char* s, int row, int k0, int K) {
+    *reinterpret_cast<uint4*>(s + kmaj_off(row, k0, K)) = make_uint4(0x3F803F80u, 0u, 0u, 0u);  // bf16 1.0 twice
+    *reinterpret_cast<uint4*>(s + kmaj_off(row, k0 + 8, K)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// Hidden-layer epilogue: 64 accumulator columns + bias, ReLU, BF16 row.
-__device__ __forceinline__ void epi_hidden(uint32_t tR, const float* bias, unsigned char* sOut, int row) {
-#pragma unroll 1
-    for (int c = 0; c < kHid; c += 16) {
-        float v[16];
-        tmem_ld16(tcol(tR, c), v);
+// Encodes one query row into a K-major X0 operand of K columns (kIn, or kInK
+// with the bias block after the inputs).
+__device__ __forceinline__ void encode_row(unsigned char* sE, int row, const float* coord6, int K) {
 #pragma unroll
-        for (int j = 0; j < 16; j++) v[j] = fmaxf(v[j] + bias[c + j], 0.0f);
-        *reinterpret_cast<uint4*>(sOut + kmaj_off(row, c, kHid)) = pack8_bf16(v);
-        *reinterpret_cast<uint4*>(sOut + kmaj_off(row, c + 8, kHid)) = pack8_bf16(v + 8);
+    for (int c = 0; c < 6; c++) {
+        float f[24];
+        encode_coord(coord6[c], f);
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            *reinterpret_cast<uint4*>(sE + kmaj_off(row, 24 * c + 8 * j, K)) = pack8_bf16(f + 8 * j);
     }
+    if (K == kInK) store_bias_block(sE, row, kIn, K);
+}
+
+// Hidden-layer epilogue of the bias-folded network: 64 accumulator columns
+// (bias included), ReLU and BF16 in one conversion, written as the next
+// layer's operand row with its bias block.
+__device__ __forceinline__ void epi_relu(uint32_t tR, unsigned char* sOut, int row) {
+#pragma unroll
+    for (int c = 0; c < kHid; c += 32) {
+        uint32_t v[32];
+        tmem_ld32(tcol(tR, c), v);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t* w = v + 8 * q;
+            uint4 u;
+            u.x = relu_bf16x2(__uint_as_float(w[0]), __uint_as_float(w[1]));
+            u.y = relu_bf16x2(__uint_as_float(w[2]), __uint_as_float(w[3]));
+            u.z = relu_bf16x2(__uint_as_float(w[4]), __uint_as_float(w[5]));
+            u.w = relu_bf16x2(__uint_as_float(w[6]), __uint_as_float(w[7]));
+            *reinterpret_cast<uint4*>(sOut + kmaj_off(row, c + 8 * q, kHidK)) = u;
+        }
+    }
+    store_bias_block(sOut, row, kHid, kHidK);
 }
 
 // Raw outputs -> mixture (weights, unit means, kappa).
@@ -268,13 +282,15 @@ __device__ __forceinline__ void raw_to_mixture(const float* y, float* m) {
         m[k] = expf(y[k] - mx);
         s += m[k];
     }
+    const float invS = 1.0f / s;
 #pragma unroll
     for (int k = 0; k < kLobes; k++) {
-        m[k] = m[k] / s;
+        m[k] = m[k] * invS;
         float a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
         float len = sqrtf(a * a + b * b + c * c);
         if (len > 1e-20f) {
-            m[8 + 3 * k] = a / len; m[9 + 3 * k] = b / len; m[10 + 3 * k] = c / len;
+            const float r = 1.0f / len;
+            m[8 + 3 * k] = a * r; m[9 + 3 * k] = b * r; m[10 + 3 * k] = c * r;
         } else {
             m[8 + 3 * k] = 0.f; m[9 + 3 * k] = 0.f; m[10 + 3 * k] = 1.f;
         }
@@ -326,10 +342,6 @@ __device__ float loss_grad(const float* y, float wx, float wy, float wz, float W
     return W != 0.f ? -W * logf(q) : 0.f;
 }
 
-__device__ __forceinline__ void store_bf16(unsigned char* base, uint32_t off, float v) {
-    *reinterpret_cast<bf16*>(base + off) = __float2bfloat16_rn(v);
-}
-
 // ---------------------------------------------------------------------------
 // Inference
 // ---------------------------------------------------------------------------
@@ -344,12 +356,10 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
         mbar_init(&bars[tid], 1);
         sFlags[tid] = 0;
     }
-    load_kmaj(sm + iW1, a.blob + bW1, kHid, kIn);
-    load_kmaj(sm + iW2, a.blob + bW2, kHid, kHid);
-    load_kmaj(sm + iW3, a.blob + bW3, kHid, kHid);
-    load_kmaj(sm + iW4, a.blob + bW4, kOutPad, kHid);
-    float* sb = reinterpret_cast<float*>(sm + iBias);
-    load_bias(sb, a.master);
+    load_kmaj(sm + iW1, a.blob + bI1, kHid, kInK);
+    load_kmaj(sm + iW2, a.blob + bI2, kHid, kHidK);
+    load_kmaj(sm + iW3, a.blob + bI3, kHid, kHidK);
+    load_kmaj(sm + iW4, a.blob + bI4, kOutPad, kHidK);
     sync_operands();
     const uint32_t R = tbase + 64u * (uint32_t)g;
     const uint32_t s0 = smem_u32(sm);
@@ -392,40 +402,43 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
             coord[2] = (pz - a.loz) * a.invz;
             coord[3] = dx; coord[4] = dy; coord[5] = dz;
         }
-        encode_row(bufX, row, coord);
+        encode_row(bufX, row, coord, kInK);
         wg_sync_operands(g);
         if (row == 0) {
-            gemm_k(R, sX, s0 + iW1, kIn, id64, 0);
+            gemm_k(R, sX, s0 + iW1, kInK, id64, 0);
             commit(bar);
         }
         if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
-        epi_hidden(R, sb, bufX, row);  // the MMA that read X0 is done: H1 goes in its place
+        epi_relu(R, bufX, row);  // the MMA that read X0 is done: H1 goes in its place
         wg_sync_operands(g);
         if (row == 0) {
-            gemm_k(R, sX, s0 + iW2, kHid, id64, 0);
+            gemm_k(R, sX, s0 + iW2, kHidK, id64, 0);
             commit(bar);
         }
         if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
-        epi_hidden(R, sb + kHid, bufX, row);
+        epi_relu(R, bufX, row);
         wg_sync_operands(g);
         if (row == 0) {
-            gemm_k(R, sX, s0 + iW3, kHid, id64, 0);
+            gemm_k(R, sX, s0 + iW3, kHidK, id64, 0);
             commit(bar);
         }
         if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
-        epi_hidden(R, sb + 2 * kHid, bufX, row);
+        epi_relu(R, bufX, row);
         wg_sync_operands(g);
         if (row == 0) {
-            gemm_k(R, sX, s0 + iW4, kHid, id48, 0);
+            gemm_k(R, sX, s0 + iW4, kHidK, id48, 0);
             commit(bar);
         }
         if (!(ok = wg_wait_mma(g, bar, phase, sFlag, a.err))) break;
         float y[kOutPad];
-        tmem_ld16(tcol(R, 0), y);
-        tmem_ld16(tcol(R, 16), y + 16);
+        {
+            uint32_t v[32];
+            tmem_ld32(tcol(R, 0), v);
+#pragma unroll
+            for (int k = 0; k < 32; k++) y[k] = __uint_as_float(v[k]);
+        }
         tmem_ld16(tcol(R, 32), y + 32);
         if (valid) {
-            for (int k = 0; k < kOut; k++) y[k] += sb[3 * kHid + k];
             float m[kOut];
             raw_to_mixture(y, m);
             float4* dst = reinterpret_cast<float4*>(a.mix + (size_t)out * kOut);
@@ -443,6 +456,24 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
 // ---------------------------------------------------------------------------
 // Training: forward + loss + backward, weight gradients accumulated in TMEM
 // ---------------------------------------------------------------------------
+// dZ = dH * relu'(Z) for one row: 64 accumulator columns, kept where the
+// stored activation is positive, BF16 into columns 0..63 of the gradient row.
+__device__ __forceinline__ void relu_grad(uint32_t tR, const unsigned char* sH, unsigned char* sD, int row) {
+#pragma unroll
+    for (int c = 0; c < kHid; c += 32) {
+        uint32_t v[32];
+        tmem_ld32(tcol(tR, c), v);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            float h[8], g[8];
+            unpack8_bf16(*reinterpret_cast<const uint4*>(sH + kmaj_off(row, c + 8 * q, kHidK)), h);
+#pragma unroll
+            for (int j = 0; j < 8; j++) g[j] = h[j] > 0.f ? __uint_as_float(v[8 * q + j]) : 0.f;
+            *reinterpret_cast<uint4*>(sD + kmaj_off(row, c + 8 * q, kDCols)) = pack8_bf16(g);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint64_t bar;
@@ -454,29 +485,27 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
         mbar_init(&bar, 1);
         sFlag = 0;
     }
-    load_kmaj(sm + tW1, a.blob + bW1, kHid, kIn);
-    load_kmaj(sm + tW2, a.blob + bW2, kHid, kHid);
-    load_kmaj(sm + tW3, a.blob + bW3, kHid, kHid);
-    load_kmaj(sm + tW4, a.blob + bW4, kOutPad, kHid);
-    load_kmaj(sm + tW2t, a.blob + bW2t, kHid, kHid);
-    load_kmaj(sm + tW3t, a.blob + bW3t, kHid, kHid);
-    load_kmaj(sm + tW4t, a.blob + bW4t, kHid, kOutPad);
-    float* sb = reinterpret_cast<float*>(sm + tBias);
-    load_bias(sb, a.master);
-    // constant operand rows: the ones row (bias gradient) and zero padding
-    for (int i = tid; i < 16 * kTile; i += blockDim.x) {
-        const int r = i / kTile, c = i % kTile;
-        const float v = r == 0 ? 1.f : 0.f;
-        store_bf16(sm + tE, kmaj_off(kIn + r, c, kTile), v);
-        store_bf16(sm + tHt, kmaj_off(kHid + r, c, kTile), v);
-    }
-    for (int i = tid; i < 64 * kTile; i += blockDim.x) store_bf16(sm + tDt, kmaj_off(64 + i / kTile, i % kTile, kTile), 0.f);
+    // the bias-folded forward weights; read MN-major they are also the data
+    // gradients' B operands (W instead of a transposed copy)
+    load_kmaj(sm + tW1, a.blob + bI1, kHid, kInK);
+    load_kmaj(sm + tW2, a.blob + bI2, kHid, kHidK);
+    load_kmaj(sm + tW3, a.blob + bI3, kHid, kHidK);
+    load_kmaj(sm + tW4, a.blob + bI4, kOutPad, kHidK);
+    // columns 64..127 of the gradient rows stay zero: the weight-gradient MMAs
+    // read them as output units 64..127 of an M = 128 tile
+    for (int i = tid; i < kTile * 8; i += blockDim.x)
+        *reinterpret_cast<uint4*>(sm + tD + kmaj_off(i >> 3, kHid + 8 * (i & 7), kDCols)) = make_uint4(0u, 0u, 0u, 0u);
     sync_operands();
 
     const uint32_t T = tbase;
     const uint32_t s0 = smem_u32(sm);
     const uint32_t id64 = idesc_bf16(128, kHid), id48 = idesc_bf16(128, kOutPad);
-    const uint32_t id80 = idesc_bf16(128, 80), id160 = idesc_bf16(128, 160);
+    // data gradients dH = dZ W: A = gradient rows (K-major over outputs), B = W read MN-major
+    const uint32_t idData = id64 | kMajorB_MN;
+    // weight gradients dW += dZ^T [H | 1 1 0..]: both operands read MN-major, K = the tile's records
+    const uint32_t idW80 = idesc_bf16(128, kHidK) | kMajorA_MN | kMajorB_MN;
+    const uint32_t idW160 = idesc_bf16(128, kInK) | kMajorA_MN | kMajorB_MN;
+    const Operand gradRows = kmajor(s0 + tD, kDCols), gradCols = mnmajor(s0 + tD, kDCols);
     const int n = a.count ? max(0, min(min(*a.count, a.capacity) - a.offset, a.stepCap)) : a.n;
     const float scale = a.scale ? *a.scale : 1.0f;
     uint32_t phase = 0;
@@ -494,111 +523,81 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
         coord[2] = (rec[2] - a.loz) * a.invz;
         coord[3] = rec[3]; coord[4] = rec[4]; coord[5] = rec[5];
         if (!valid) for (int i = 0; i < 6; i++) coord[i] = 0.f;
-        encode_row(sm + tE, row, coord);
+        encode_row(sm + tX, row, coord, kInK);
         sync_operands();
-        // ---- forward ----
+        // ---- forward (biases folded into the MMAs) ----
         if (tid == 0) {
-            gemm_k(T + cR, s0 + tE, s0 + tW1, kIn, id64, 0);
+            gemm_k(T + cR, s0 + tX, s0 + tW1, kInK, id64, 0);
             commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        epi_hidden(T + cR, sb, sm + tH1, row);
+        epi_relu(T + cR, sm + tH1, row);
         sync_operands();
         if (tid == 0) {
-            gemm_k(T + cR, s0 + tH1, s0 + tW2, kHid, id64, 0);
+            gemm_k(T + cR, s0 + tH1, s0 + tW2, kHidK, id64, 0);
             commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        epi_hidden(T + cR, sb + kHid, sm + tH2, row);
+        epi_relu(T + cR, sm + tH2, row);
         sync_operands();
         if (tid == 0) {
-            gemm_k(T + cR, s0 + tH2, s0 + tW3, kHid, id64, 0);
+            gemm_k(T + cR, s0 + tH2, s0 + tW3, kHidK, id64, 0);
             commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        epi_hidden(T + cR, sb + 2 * kHid, sm + tH3, row);
+        epi_relu(T + cR, sm + tH3, row);
         sync_operands();
         if (tid == 0) {
-            gemm_k(T + cR, s0 + tH3, s0 + tW4, kHid, id48, 0);
+            gemm_k(T + cR, s0 + tH3, s0 + tW4, kHidK, id48, 0);
             commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
-        // ---- loss and dY ----
+        // ---- loss and dY (columns kOut..63 zero) ----
         {
             float y[kOutPad];
-            tmem_ld16(tcol(T + cR, 0), y);
-            tmem_ld16(tcol(T + cR, 16), y + 16);
+            {
+                uint32_t v[32];
+                tmem_ld32(tcol(T + cR, 0), v);
+#pragma unroll
+                for (int k = 0; k < 32; k++) y[k] = __uint_as_float(v[k]);
+            }
             tmem_ld16(tcol(T + cR, 32), y + 32);
-            for (int k = 0; k < kOut; k++) y[k] += sb[3 * kHid + k];
-            float dy[kOutPad];
-            for (int k = kOut; k < kOutPad; k++) dy[k] = 0.f;
+            float dy[kHid];
+            for (int k = kOut; k < kHid; k++) dy[k] = 0.f;
             float W = valid ? rec[9] * scale : 0.f;
             if (a.weightCap > 0.f && n > 0) W = fminf(W, a.weightCap / (float)n);
-            float nx = rec[6], ny = rec[7], nz = rec[8];
-            lossAcc += loss_grad(y, nx, ny, nz, W, dy);
-            for (int c = 0; c < kOutPad; c += 8)
-                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c, kOutPad)) = pack8_bf16(dy + c);
-            for (int o = 0; o < kHid; o++) store_bf16(sm + tDt, kmaj_off(o, row, kTile), o < kOut ? dy[o] : 0.f);
-        }
-        // H3^T
-        for (int c = 0; c < kHid; c += 8) {
-            float h[8];
-            unpack8_bf16(*reinterpret_cast<const uint4*>(sm + tH3 + kmaj_off(row, c, kHid)), h);
-            for (int j = 0; j < 8; j++) store_bf16(sm + tHt, kmaj_off(c + j, row, kTile), h[j]);
+            lossAcc += loss_grad(y, rec[6], rec[7], rec[8], W, dy);
+#pragma unroll
+            for (int c = 0; c < kHid; c += 8)
+                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c, kDCols)) = pack8_bf16(dy + c);
         }
         sync_operands();
         if (tid == 0) {
-            gemm_k(T + cR, s0 + tD, s0 + tW4t, kOutPad, id64, 0);            // dH3 = dY W4
-            gemm_k(T + cG4, s0 + tDt, s0 + tHt, kTile, id80, done > 0);      // dW4 | db4
+            gemm_op(T + cR, gradRows, mnmajor(s0 + tW4, kHidK), kOutPad, idData, 0);          // dH3 = dY W4
+            gemm_op(T + cG4, gradCols, mnmajor(s0 + tH3, kHidK), kTile, idW80, done > 0);     // dW4 | db4
             commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
         // ---- layers 3, 2: dZ = dH * relu'(Z), then the next data / weight gradients ----
         const int hOff[3] = {tH3, tH2, tH1};
-        const int wtOff[2] = {tW3t, tW2t};
+        const int wOff[2] = {tW3, tW2};
         const uint32_t gOff[2] = {cG3, cG2};
         for (int l = 0; l < 2; l++) {
-            for (int c = 0; c < kHid; c += 16) {
-                float v[16], h[16];
-                tmem_ld16(tcol(T + cR, c), v);
-                unpack8_bf16(*reinterpret_cast<const uint4*>(sm + hOff[l] + kmaj_off(row, c, kHid)), h);
-                unpack8_bf16(*reinterpret_cast<const uint4*>(sm + hOff[l] + kmaj_off(row, c + 8, kHid)), h + 8);
-                for (int j = 0; j < 16; j++) v[j] = h[j] > 0.f ? v[j] : 0.f;
-                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c, kHid)) = pack8_bf16(v);
-                *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c + 8, kHid)) = pack8_bf16(v + 8);
-                for (int j = 0; j < 16; j++) store_bf16(sm + tDt, kmaj_off(c + j, row, kTile), v[j]);
-            }
-            for (int c = 0; c < kHid; c += 8) {
-                float h[8];
-                unpack8_bf16(*reinterpret_cast<const uint4*>(sm + hOff[l + 1] + kmaj_off(row, c, kHid)), h);
-                for (int j = 0; j < 8; j++) store_bf16(sm + tHt, kmaj_off(c + j, row, kTile), h[j]);
-            }
+            relu_grad(T + cR, sm + hOff[l], sm + tD, row);
             sync_operands();
             if (tid == 0) {
-                gemm_k(T + cR, s0 + tD, s0 + wtOff[l], kHid, id64, 0);
-                gemm_k(T + gOff[l], s0 + tDt, s0 + tHt, kTile, id80, done > 0);
+                gemm_op(T + cR, gradRows, mnmajor(s0 + wOff[l], kHidK), kHid, idData, 0);
+                gemm_op(T + gOff[l], gradCols, mnmajor(s0 + hOff[l + 1], kHidK), kTile, idW80, done > 0);
                 commit(&bar);
             }
             if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
         }
         if (!ok) break;
-        // ---- layer 1: dZ1 and dW1 | db1 against X0^T ----
-        for (int c = 0; c < kHid; c += 16) {
-            float v[16], h[16];
-            tmem_ld16(tcol(T + cR, c), v);
-            unpack8_bf16(*reinterpret_cast<const uint4*>(sm + tH1 + kmaj_off(row, c, kHid)), h);
-            unpack8_bf16(*reinterpret_cast<const uint4*>(sm + tH1 + kmaj_off(row, c + 8, kHid)), h + 8);
-            for (int j = 0; j < 16; j++) store_bf16(sm + tDt, kmaj_off(c + j, row, kTile), h[j] > 0.f ? v[j] : 0.f);
-        }
-        __syncthreads();  // every thread is done with the X0 operand layout before it is overwritten
-        for (int ch = 0; ch < kIn / 8; ch++) {
-            float f[8];
-            encode_chunk(coord, ch, f);
-            for (int j = 0; j < 8; j++) store_bf16(sm + tE, kmaj_off(ch * 8 + j, row, kTile), f[j]);
-        }
+        // ---- layer 1: dZ1, then dW1 | db1 against the encoded inputs ----
+        relu_grad(T + cR, sm + tH1, sm + tD, row);
         sync_operands();
         if (tid == 0) {
-            gemm_k(T + cG1, s0 + tDt, s0 + tE, kTile, id160, done > 0);
+            gemm_op(T + cG1, gradCols, mnmajor(s0 + tX, kInK), kTile, idW160, done > 0);
             commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase, &sFlag, a.err))) break;
@@ -649,26 +648,28 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
 // ---------------------------------------------------------------------------
 // Parameter maintenance
 // ---------------------------------------------------------------------------
+// Bias-folded operand row element k of a layer with nin inputs: the weight,
+// then the bias as a BF16 pair (hi, lo), then zeros.
+__device__ __forceinline__ bf16 folded(const float* master, int ow, int ob, int nin, int o, int k) {
+    if (k < nin) return __float2bfloat16_rn(master[ow + o * nin + k]);
+    const float b = master[ob + o];
+    const bf16 hi = __float2bfloat16_rn(b);
+    if (k == nin) return hi;
+    if (k == nin + 1) return __float2bfloat16_rn(b - __bfloat162float(hi));
+    return __float2bfloat16_rn(0.f);
+}
+
 __global__ void k_guide_prepare(const float* master, bf16* blob) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kBlob; e += gridDim.x * blockDim.x) {
-        float v = 0.f;
-        if (e < bW2) v = master[oW1 + e];
-        else if (e < bW3) v = master[oW2 + (e - bW2)];
-        else if (e < bW4) v = master[oW3 + (e - bW3)];
-        else if (e < bW2t) {
-            int o = (e - bW4) / kHid, i = (e - bW4) % kHid;
-            v = o < kOut ? master[oW4 + o * kHid + i] : 0.f;
-        } else if (e < bW3t) {
-            int i = (e - bW2t) / kHid, o = (e - bW2t) % kHid;
-            v = master[oW2 + o * kHid + i];
-        } else if (e < bW4t) {
-            int i = (e - bW3t) / kHid, o = (e - bW3t) % kHid;
-            v = master[oW3 + o * kHid + i];
-        } else {
-            int i = (e - bW4t) / kOutPad, o = (e - bW4t) % kOutPad;
-            v = o < kOut ? master[oW4 + o * kHid + i] : 0.f;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kBlobAll; e += gridDim.x * blockDim.x) {
+        bf16 v;
+        if (e < bI2) v = folded(master, oW1, oB1, kIn, (e - bI1) / kInK, (e - bI1) % kInK);
+        else if (e < bI3) v = folded(master, oW2, oB2, kHid, (e - bI2) / kHidK, (e - bI2) % kHidK);
+        else if (e < bI4) v = folded(master, oW3, oB3, kHid, (e - bI3) / kHidK, (e - bI3) % kHidK);
+        else {
+            const int o = (e - bI4) / kHidK;
+            v = o < kOut ? folded(master, oW4, oB4, kHid, o, (e - bI4) % kHidK) : __float2bfloat16_rn(0.f);
         }
-        blob[e] = __float2bfloat16_rn(v);
+        blob[e] = v;
     }
 }
 
@@ -937,7 +938,7 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     }
     const size_t P = (size_t)kParams * sizeof(float);
     bool okAlloc = cudaMalloc(&g->master, P) == cudaSuccess && cudaMalloc(&g->adam_m, P) == cudaSuccess &&
-                   cudaMalloc(&g->adam_v, P) == cudaSuccess && cudaMalloc(&g->blob, (size_t)kBlob * 2) == cudaSuccess &&
+                   cudaMalloc(&g->adam_v, P) == cudaSuccess && cudaMalloc(&g->blob, (size_t)kBlobAll * 2) == cudaSuccess &&
                    cudaMalloc(&g->partials, (size_t)ctx->sm_count * P) == cudaSuccess &&
                    cudaMalloc(&g->scale, sizeof(float)) == cudaSuccess && cudaMalloc(&g->loss, sizeof(double)) == cudaSuccess &&
                    cudaMalloc(&g->batch, (size_t)g->cfg.batch_capacity * g->cfg.train_steps * MC_GUIDE_RECORD_FLOATS *

@@ -33,17 +33,19 @@ constexpr int oB4 = oW4 + kOut * kHid;
 constexpr int kParams = oB4 + kOut;
 static_assert(kParams == MC_GUIDE_PARAM_COUNT, "parameter layout");
 
-// BF16 weight blob (elements): forward operands W[out][in] (W4 padded to 48
-// rows) and, for the backward data gradients, transposes W^T[in][out] (W4^T
-// padded to 48 columns).
-constexpr int bW1 = 0;
-constexpr int bW2 = bW1 + kHid * kIn;
-constexpr int bW3 = bW2 + kHid * kHid;
-constexpr int bW4 = bW3 + kHid * kHid;
-constexpr int bW2t = bW4 + kOutPad * kHid;
-constexpr int bW3t = bW2t + kHid * kHid;
-constexpr int bW4t = bW3t + kHid * kHid;
-constexpr int kBlob = bW4t + kHid * kOutPad;
+// BF16 weight blob (elements): every layer's weights W[out][in] with the bias
+// folded in: each layer's input gains a 16-column block [1, 1, 0, ...] and
+// its weight rows the matching block [hi, lo, 0, ...], hi = bf16(b) and
+// lo = bf16(b - hi), so the MMA adds the bias (to about 2^-17 of it) and the
+// forward epilogues only apply ReLU. W4 is padded to 48 rows. The kernels read
+// the same rows MN-major as the backward pass's W operands (dH = dZ W).
+constexpr int kInK = kIn + 16;           // 160
+constexpr int kHidK = kHid + 16;         // 80
+constexpr int bI1 = 0;
+constexpr int bI2 = bI1 + kHid * kInK;
+constexpr int bI3 = bI2 + kHid * kHidK;
+constexpr int bI4 = bI3 + kHid * kHidK;
+constexpr int kBlobAll = bI4 + kOutPad * kHidK;
 
 // log-concentration range: kappa in [0.01, 1000]
 constexpr float kLogKappaMin = -4.60517019f;
@@ -52,27 +54,28 @@ constexpr float kTwoPi = 6.28318530718f;
 
 // Inputs: coordinate c (0..2 position in [0,1], 3..5 direction), frequency f:
 // in[24c + 2f] = sin(pi 2^f x), in[24c + 2f + 1] = cos(pi 2^f x).
-// Chunk ch (8 consecutive inputs) = coordinate ch/3, frequencies 4(ch%3)..+3.
-// The chunk's first frequency is evaluated directly, the next three by the
-// double-angle identities sin 2a = 2 sin a cos a, cos 2a = (cos a - sin a)
-// (cos a + sin a): each doubling at most doubles the absolute error, so the
-// last one is within about 1e-6 of the direct value, far below the BF16
-// spacing (2^-8) the network reads the inputs in.
-MC_GD void encode_chunk(const float* coord6, int ch, float* out8) {
-    const float x = coord6[ch / 3];
-    const int f0 = (ch % 3) * 4;
-    float s, c;
-    sincospif(x * (float)(1 << f0), &s, &c);
-    out8[0] = s;
-    out8[1] = c;
+// Frequencies 0 and 6 of a coordinate are evaluated directly, the five after
+// each by the double-angle identities sin 2a = 2 sin a cos a, cos 2a =
+// (cos a - sin a)(cos a + sin a). Squaring the unit complex number cos a +
+// i sin a doubles its error (plus one rounding), so five doublings stay
+// within about 4e-6 of the direct values, far below the BF16 spacing (2^-8
+// near 1) the network reads the inputs in.
+MC_GD void encode_coord(float x, float* out24) {
 #pragma unroll
-    for (int j = 1; j < 4; j++) {
-        const float s2 = 2.0f * s * c;
-        const float c2 = (c - s) * (c + s);
-        s = s2;
-        c = c2;
-        out8[2 * j] = s;
-        out8[2 * j + 1] = c;
+    for (int half = 0; half < 2; half++) {
+        float s, c;
+        sincospif(x * (half ? 64.0f : 1.0f), &s, &c);
+        out24[12 * half] = s;
+        out24[12 * half + 1] = c;
+#pragma unroll
+        for (int j = 1; j < 6; j++) {
+            const float s2 = 2.0f * s * c;
+            const float c2 = (c - s) * (c + s);
+            s = s2;
+            c = c2;
+            out24[12 * half + 2 * j] = s;
+            out24[12 * half + 2 * j + 1] = c;
+        }
     }
 }
 

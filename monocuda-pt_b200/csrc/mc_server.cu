@@ -59,6 +59,7 @@ long long bvh_bytes(const mc_bvh* b) {
 
 struct mc_server {
     mc_context* ctx = nullptr;
+    int device = 0;
     mc_server_config cfg;
     std::chrono::steady_clock::time_point t0;
     std::vector<ServerScene> scenes;
@@ -91,10 +92,10 @@ mc_status admit(mc_server* s) {
         ServerRequest& r = s->requests[s->pending.front()];
         if (s->used + r.bytes > s->cfg.hbm_budget_bytes) break;  // arrival order: the head waits for room
         size_t accBytes = (size_t)r.params.width * r.params.height * 3 * sizeof(float);
-        if (cudaMalloc(&r.accum, accBytes) != cudaSuccess) {
-            cudaGetLastError();
+        // from the device's stream-ordered pool: a driver allocation per
+        // request costs up to hundreds of milliseconds at random
+        if (mc::pool_alloc(s->ctx, (void**)&r.accum, accBytes) != MC_OK)
             return mc::set_error(MC_ERR_OOM, "mc_server_step: accumulation buffer allocation failed");
-        }
         cudaMemsetAsync(r.accum, 0, accBytes, s->ctx->stream);
         s->used += r.bytes;
         r.state = MC_REQ_ACTIVE;
@@ -113,6 +114,7 @@ mc_status mc_server_create(mc_context* ctx, const mc_server_config* config, mc_s
     if (!ctx || !out) return mc::set_error(MC_ERR_INVALID, "mc_server_create: null argument");
     mc_server* s = new mc_server();
     s->ctx = ctx;
+    s->device = ctx->device;
     if (config) s->cfg = *config;
     else std::memset(&s->cfg, 0, sizeof(s->cfg));
     if (s->cfg.hbm_budget_bytes <= 0) s->cfg.hbm_budget_bytes = 150ll * 1000 * 1000 * 1000;
@@ -125,11 +127,16 @@ mc_status mc_server_create(mc_context* ctx, const mc_server_config* config, mc_s
     return MC_OK;
 }
 
-// Does not touch the server's context (which may be gone already): cudaFree
-// waits for the device work that uses the buffers.
+// Does not touch the server's context (which may be gone already): the
+// accumulation buffers go back to the pool once the device's work is done.
 mc_status mc_server_destroy(mc_server* s) {
     if (!s) return MC_OK;
-    for (auto& kv : s->requests) cudaFree(kv.second.accum);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != s->device) cudaSetDevice(s->device);
+    cudaDeviceSynchronize();
+    for (auto& kv : s->requests) mc::pool_release(kv.second.accum);
+    if (prev >= 0 && prev != s->device) cudaSetDevice(prev);
     for (auto& sc : s->scenes) {
         mc_bvh_free(sc.bvh);
         mc_guide_destroy(sc.guide);
@@ -381,7 +388,7 @@ mc_status mc_server_release(mc_server* s, int64_t request_id) {
     ServerRequest& r = it->second;
     if (r.state == MC_REQ_CANCELLED) return MC_OK;  // its memory went back when it was cancelled
     if (r.state != MC_REQ_DONE) return mc::set_error(MC_ERR_INVALID, "mc_server_release: request %lld is not done", (long long)request_id);
-    cudaFree(r.accum);
+    mc::pool_free(s->ctx, r.accum);  // after the work queued on the server's stream
     r.accum = nullptr;
     r.state = MC_REQ_RELEASED;
     s->used -= r.bytes;
@@ -398,8 +405,8 @@ mc_status mc_server_cancel(mc_server* s, int64_t request_id) {
     } else if (r.state == MC_REQ_ACTIVE) {
         s->active.erase(std::remove(s->active.begin(), s->active.end(), r.id), s->active.end());
         // steps are synchronous, so no launch of this request is in flight;
-        // cudaFree would wait for one all the same
-        cudaFree(r.accum);
+        // the stream-ordered free would follow one all the same
+        mc::pool_free(s->ctx, r.accum);
         r.accum = nullptr;
         s->used -= r.bytes;
     } else {

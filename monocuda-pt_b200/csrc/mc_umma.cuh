@@ -60,6 +60,41 @@ __device__ __forceinline__ void gemm_k(uint32_t d_tmem, uint32_t sa, uint32_t sb
     }
 }
 
+// An MMA operand in shared memory, stored in the K-major layout above as a
+// matrix of rows x C columns (kmaj_off with K = C). Used with K along its
+// columns it is a K-major operand; used with K along its rows it is the same
+// bytes read as an MN-major operand (no swizzle): an 8 x 8 core matrix is 8
+// K-rows of 8 MN-consecutive elements, MN-adjacent core matrices are 128
+// bytes apart (the descriptor's stride byte offset) and K-adjacent ones C*16
+// bytes (its leading byte offset). That is how the weight gradients read the
+// activations and output gradients, and the data gradients the forward
+// weights, without transposed copies.
+struct Operand {
+    uint32_t addr, lbo, sbo, kstep;  // kstep: start-address advance per K = 16
+};
+__device__ __forceinline__ Operand kmajor(uint32_t addr, int C) { return {addr, 128u, (uint32_t)C * 16u, 256u}; }
+__device__ __forceinline__ Operand mnmajor(uint32_t addr, int C) {
+    return {addr, (uint32_t)C * 16u, 128u, 2u * (uint32_t)C * 16u};
+}
+
+__device__ __forceinline__ uint64_t smem_desc_raw(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction-descriptor bits of an MN-major A (bit 15) or B (bit 16).
+constexpr uint32_t kMajorA_MN = 1u << 15;
+constexpr uint32_t kMajorB_MN = 1u << 16;
+
+// D (+)= A * B^T over K (a multiple of 16) with operands of either major-ness
+// (the instruction descriptor's major bits must agree). One thread issues.
+__device__ __forceinline__ void gemm_op(uint32_t d_tmem, Operand A, Operand B, int K, uint32_t idesc, uint32_t acc) {
+    for (int s = 0; s < K / 16; s++) {
+        mma_bf16(d_tmem, smem_desc_raw(A.addr + A.kstep * s, A.lbo, A.sbo), smem_desc_raw(B.addr + B.kstep * s, B.lbo, B.sbo),
+                 idesc, (s > 0 || acc) ? 1u : 0u);
+    }
+}
+
 // Arrive on an mbarrier when every MMA this thread issued so far has finished.
 __device__ __forceinline__ void commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -118,6 +153,28 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
         : "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane, as raw bits.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+}
+
+// Two floats -> max(., 0) as a bf16 pair (round to nearest even), lo in the
+// low half.
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
 }
 
 // Eight floats -> eight bf16 (round to nearest even) packed in a uint4, lowest

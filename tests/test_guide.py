@@ -164,8 +164,13 @@ def test_adam_step_follows_the_gradient(ctx):
     params = _params(rng)
     g = _guide(ctx, params, learning_rate=1e-3)
     rec = _records(rng, 5000)
-    grad, _ = _oracle_grad(params, rec, 1)
+    # the step follows the kernel's own gradient (the gradient tests compare
+    # that with the oracle; a component near zero can take either sign there)
+    grad, _ = _gpu_grad(ctx, g, rec)
     grad /= rec[:, 9].astype(np.float64).sum()
+    ref, _ = _oracle_grad(params, rec, 1)
+    ref /= rec[:, 9].astype(np.float64).sum()
+    assert np.linalg.norm(grad - ref) < 2e-2 * np.linalg.norm(ref)
     d_rec = torch.from_numpy(rec).cuda()
     mcpt.check(ctx.lib.mc_guide_train(g.handle, d_rec.data_ptr(), len(rec)))
     assert g.steps() == 1
