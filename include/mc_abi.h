@@ -597,6 +597,11 @@ MC_API mc_status mc_bvh_build(mc_context* ctx, const mc_scene_view* scene, const
  * view); render it with mc_render_batch. Each scene needs >= 2 primitives. */
 MC_API mc_status mc_bvh_build_batch(mc_context* ctx, const mc_scene_view* scenes, int32_t count,
                                     const mc_bvh_build_opts* opts, mc_bvh** out);
+/* A tree's buffers and a build's temporaries come from a stream-ordered pool
+ * of the device that keeps freed memory for the next build (the process's
+ * pools outlive contexts; mc_context_destroy hands back what they hold
+ * unused). mc_bvh_free waits for the device's work, as cudaFree would, and
+ * may be called after the building context is destroyed. */
 MC_API mc_status mc_bvh_free(mc_bvh* bvh);
 MC_API mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info);
 /* Export in the reference's representation (device arrays, any may be NULL):
