@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--guide-pretrain-spp", type=int, default=0,
                     help="diagnostic: train the guide on this many untimed samples first (the headline trains from "
                          "scratch inside the timed region)")
+    ap.add_argument("--guide-anchor", type=int, default=0, choices=[0, 1],
+                    help="guiding: lobe means offset by the direction input (an untrained guide proposes around "
+                         "the normal)")
     ap.add_argument("--guide-fold", action="store_true",
                     help="mirror guide directions below the surface up instead of ending those paths")
     ap.add_argument("--guide-weight-cap", type=float, default=0.0,
@@ -711,7 +714,7 @@ def run_guiding(args, emit=True):
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
                             train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                             guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
-                            fold_below=args.guide_fold)
+                            fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor))
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -739,7 +742,7 @@ def run_guiding(args, emit=True):
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
                        train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                        guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
-                       fold_below=args.guide_fold)
+                       fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor))
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -799,6 +802,7 @@ def run_guiding(args, emit=True):
            "pretrain_spp": args.guide_pretrain_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
            "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap, "fold_below": bool(args.guide_fold),
+           "anchor_lobes": bool(args.guide_anchor),
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,

@@ -719,8 +719,17 @@ typedef struct mc_guide_config {
                                    the proposal the guide learns changes */
     int32_t fold_below;         /* guided renders: the guide's directions below the surface are mirrored up
                                    (the density counts both) instead of ending the path; 0 = off */
-    int32_t pad1, pad2;
+    int32_t anchor_lobes;       /* 1: every lobe's mean is the network's raw mean output plus
+                                   MC_GUIDE_ANCHOR times the direction input (turned away from the surface
+                                   for MC_GUIDE_DIR_RAY), normalized, and kappa starts near e: an untrained
+                                   guide proposes directions around the normal, a cosine-like lobe, instead of
+                                   a near-uniform sphere whose lower half ends paths. 0 = off (raw means) */
+    int32_t pad2;
 } mc_guide_config;
+
+/* Length of the direction-input offset added to every raw lobe mean when
+ * mc_guide_config.anchor_lobes is set. */
+#define MC_GUIDE_ANCHOR 1.5f
 
 #define MC_GUIDE_MAX_TRAIN_VERTICES 4
 enum {

@@ -113,6 +113,7 @@ struct GuideInferArgs {
     const mc_sphere* spheres;
     int dirNormal;
     int stride;                             // > 1: one query per `stride` queue slots (the first of each run)
+    float anchor;                           // anchored lobes: this times the direction input offsets every raw mean
     float* mix;
     int* err;
 };
@@ -165,6 +166,7 @@ struct GuideTrainArgs {
     int stepCap;                            // records one step takes
     const float* scale;
     float weightCap;                        // > 0: a record's normalized weight is at most weightCap / n
+    float anchor;                           // anchored lobes (GuideInferArgs::anchor)
     float* partials;
     double* loss;
     int* err;
@@ -271,8 +273,9 @@ __device__ __forceinline__ void epi_relu(uint32_t tR, unsigned char* sOut, int r
     store_bias_block(sOut, row, kHid, kHidK);
 }
 
-// Raw outputs -> mixture (weights, unit means, kappa).
-__device__ __forceinline__ void raw_to_mixture(const float* y, float* m) {
+// Raw outputs -> mixture (weights, unit means, kappa). anc: the anchor
+// offset added to every raw mean (zero for unanchored guides).
+__device__ __forceinline__ void raw_to_mixture(const float* y, const float* anc, float* m) {
     float mx = y[0];
 #pragma unroll
     for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, y[k]);
@@ -286,7 +289,7 @@ __device__ __forceinline__ void raw_to_mixture(const float* y, float* m) {
 #pragma unroll
     for (int k = 0; k < kLobes; k++) {
         m[k] = m[k] * invS;
-        float a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
+        float a = y[8 + 3 * k] + anc[0], b = y[9 + 3 * k] + anc[1], c = y[10 + 3 * k] + anc[2];
         float len = sqrtf(a * a + b * b + c * c);
         if (len > 1e-20f) {
             const float r = 1.0f / len;
@@ -298,8 +301,10 @@ __device__ __forceinline__ void raw_to_mixture(const float* y, float* m) {
     }
 }
 
-// Loss -W log q(w) of one record and its gradient w.r.t. the 40 raw outputs.
-__device__ float loss_grad(const float* y, float wx, float wy, float wz, float W, float* dy) {
+// Loss -W log q(w) of one record and its gradient w.r.t. the 40 raw outputs
+// (the anchor offset anc is a constant: a raw mean's gradient is its
+// anchored mean's).
+__device__ float loss_grad(const float* y, const float* anc, float wx, float wy, float wz, float W, float* dy) {
     float mx = y[0];
     for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, y[k]);
     float e[kLobes], s = 0.f;
@@ -312,7 +317,7 @@ __device__ float loss_grad(const float* y, float wx, float wy, float wz, float W
     float q = 0.f;
     for (int k = 0; k < kLobes; k++) {
         wk[k] = e[k] / s;
-        float a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
+        float a = y[8 + 3 * k] + anc[0], b = y[9 + 3 * k] + anc[1], c = y[10 + 3 * k] + anc[2];
         float l = sqrtf(a * a + b * b + c * c);
         if (l > 1e-20f) {
             mu[3 * k] = a / l; mu[3 * k + 1] = b / l; mu[3 * k + 2] = c / l;
@@ -440,7 +445,8 @@ __global__ void __launch_bounds__(128 * kInferGroups, 1) k_guide_infer(GuideInfe
         tmem_ld16(tcol(R, 32), y + 32);
         if (valid) {
             float m[kOut];
-            raw_to_mixture(y, m);
+            const float anc[3] = {a.anchor * coord[3], a.anchor * coord[4], a.anchor * coord[5]};
+            raw_to_mixture(y, anc, m);
             float4* dst = reinterpret_cast<float4*>(a.mix + (size_t)out * kOut);
             for (int i = 0; i < kOut / 4; i++) dst[i] = make_float4(m[4 * i], m[4 * i + 1], m[4 * i + 2], m[4 * i + 3]);
         }
@@ -566,7 +572,8 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(GuideTrainArgs a) {
             for (int k = kOut; k < kHid; k++) dy[k] = 0.f;
             float W = valid ? rec[9] * scale : 0.f;
             if (a.weightCap > 0.f && n > 0) W = fminf(W, a.weightCap / (float)n);
-            lossAcc += loss_grad(y, rec[6], rec[7], rec[8], W, dy);
+            const float anc[3] = {a.anchor * rec[3], a.anchor * rec[4], a.anchor * rec[5]};
+            lossAcc += loss_grad(y, anc, rec[6], rec[7], rec[8], W, dy);
 #pragma unroll
             for (int c = 0; c < kHid; c += 8)
                 *reinterpret_cast<uint4*>(sm + tD + kmaj_off(row, c, kDCols)) = pack8_bf16(dy + c);
@@ -726,8 +733,10 @@ struct SplitMix {
 };
 
 // He-uniform weights (bound sqrt(6 / fan_in)), the output layer scaled by 0.1,
-// zero biases (kappa starts at 1).
-void init_params(std::vector<float>& p, uint64_t seed) {
+// zero biases (kappa starts at 1). Anchored lobes start with log kappa 1
+// (kappa near e): with every mean near the direction input, the untrained
+// mixture is a lobe about as wide as the cosine's.
+void init_params(std::vector<float>& p, uint64_t seed, bool anchored) {
     SplitMix r{seed ^ 0x6A09E667F3BCC909ull};
     p.assign(kParams, 0.f);
     auto fill = [&](int off, int out, int in, double gain) {
@@ -738,6 +747,15 @@ void init_params(std::vector<float>& p, uint64_t seed) {
     fill(oW2, kHid, kHid, 1.0);
     fill(oW3, kHid, kHid, 1.0);
     fill(oW4, kOut, kHid, 0.1);
+    if (anchored)
+        for (int k = 0; k < kLobes; k++) p[oB4 + 32 + k] = 1.0f;
+}
+
+// The anchor offset's signed length: the direction input as fed (the normal
+// faces the arriving ray), or turned back for the arriving ray's direction.
+float anchor_of(const mc_guide* g) {
+    if (!g->cfg.anchor_lobes) return 0.f;
+    return g->cfg.direction_input == MC_GUIDE_DIR_RAY ? -MC_GUIDE_ANCHOR : MC_GUIDE_ANCHOR;
 }
 
 // The kernels' opt-in shared-memory sizes, once per context (per device).
@@ -790,6 +808,7 @@ mc_status launch_train(mc_guide* g, cudaStream_t s, const float* records, int n,
     a.stepCap = stepCap;
     a.scale = scale;
     a.weightCap = weightCap;
+    a.anchor = anchor_of(g);
     a.partials = g->partials;
     a.loss = g->loss;
     a.err = g->ctx->d_error;
@@ -860,6 +879,7 @@ mc_status guide_infer_paths(mc_guide* g, cudaStream_t s, const int* queue, const
     a.spheres = spheres;
     a.dirNormal = g->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
     a.stride = stride;
+    a.anchor = anchor_of(g);
     a.mix = mixtures;
     a.err = g->ctx->d_error;
     k_guide_infer<<<g->ctx->sm_count, kTile * kInferGroups, kInferSmem, s>>>(a);
@@ -931,9 +951,11 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     // 7 % less time on the aperture room (the later bounces carry little light)
     if (g->cfg.guided_depth <= 0) g->cfg.guided_depth = 4;
     if (!(g->cfg.weight_cap >= 0.f)) g->cfg.weight_cap = 0.f;
-    if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1) {
+    if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1 ||
+        g->cfg.anchor_lobes < 0 || g->cfg.anchor_lobes > 1) {
         delete g;
-        return mc::set_error(MC_ERR_INVALID, "mc_guide_create: train_vertices above %d or unknown direction_input",
+        return mc::set_error(MC_ERR_INVALID,
+                             "mc_guide_create: train_vertices above %d, unknown direction_input or anchor_lobes not 0/1",
                              MC_GUIDE_MAX_TRAIN_VERTICES);
     }
     const size_t P = (size_t)kParams * sizeof(float);
@@ -951,7 +973,7 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
         return mc::set_error(MC_ERR_OOM, "mc_guide_create: device allocation failed");
     }
     std::vector<float> p;
-    init_params(p, g->cfg.seed);
+    init_params(p, g->cfg.seed, g->cfg.anchor_lobes != 0);
     cudaMemcpy(g->master, p.data(), P, cudaMemcpyHostToDevice);
     cudaMemset(g->adam_m, 0, P);
     cudaMemset(g->adam_v, 0, P);
@@ -1019,6 +1041,7 @@ mc_status mc_guide_infer(mc_guide* g, const float* d_queries, int32_t n, float* 
     fill_box(g, a);
     a.n = n;
     a.queries = d_queries;
+    a.anchor = anchor_of(g);
     a.mix = d_mixtures;
     a.err = ctx->d_error;
     int tiles = (n + kTile - 1) / kTile;

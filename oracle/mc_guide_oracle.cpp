@@ -80,14 +80,15 @@ void forward(const double* P, const std::vector<double>& W, bool bf, Fwd& F) {
     layer(F.h3, HID, oW4, oB4, OUT, F.y, nullptr);
 }
 
-void mixture(const double* y, double* m) {
+// anc: the anchor offset added to every raw lobe mean (zero when unanchored)
+void mixture(const double* y, const double* anc, double* m) {
     double mx = y[0];
     for (int k = 1; k < LOBES; k++) mx = std::max(mx, y[k]);
     double s = 0.0;
     for (int k = 0; k < LOBES; k++) s += std::exp(y[k] - mx);
     for (int k = 0; k < LOBES; k++) {
         m[k] = std::exp(y[k] - mx) / s;
-        double a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
+        double a = y[8 + 3 * k] + anc[0], b = y[9 + 3 * k] + anc[1], c = y[10 + 3 * k] + anc[2];
         double l = std::sqrt(a * a + b * b + c * c);
         if (l > 1e-20) {
             m[8 + 3 * k] = a / l; m[9 + 3 * k] = b / l; m[10 + 3 * k] = c / l;
@@ -101,12 +102,12 @@ void mixture(const double* y, double* m) {
 double vmf(double kappa, double c) { return kappa / (2.0 * M_PI * (1.0 - std::exp(-2.0 * kappa))) * std::exp(kappa * (c - 1.0)); }
 
 // -W log q(w) and d/dy
-double loss_grad(const double* y, const double* w, double W, double* dy) {
+double loss_grad(const double* y, const double* anc, const double* w, double W, double* dy) {
     double m[OUT];
-    mixture(y, m);
+    mixture(y, anc, m);
     double len[LOBES], vk[LOBES], cs[LOBES], q = 0.0;
     for (int k = 0; k < LOBES; k++) {
-        double a = y[8 + 3 * k], b = y[9 + 3 * k], c = y[10 + 3 * k];
+        double a = y[8 + 3 * k] + anc[0], b = y[9 + 3 * k] + anc[1], c = y[10 + 3 * k] + anc[2];
         len[k] = std::sqrt(a * a + b * b + c * c);
         if (!(len[k] > 1e-20)) len[k] = 0.0;
         cs[k] = m[8 + 3 * k] * w[0] + m[9 + 3 * k] * w[1] + m[10 + 3 * k] * w[2];
@@ -137,13 +138,20 @@ std::vector<double> weights(const double* P, bool bf) {
     return W;
 }
 
+// Anchored lobes (flags bit 1; bit 2 turns the direction back): every raw
+// mean is offset by 1.5 times the direction input, FP32 products as the GPU's.
+void anchor_of(int flags, const float* dir, double* anc) {
+    const float s = (flags & 2) ? ((flags & 4) ? -1.5f : 1.5f) : 0.0f;
+    for (int j = 0; j < 3; j++) anc[j] = (double)(s * dir[j]);
+}
+
 }  // namespace
 
 extern "C" {
 
 int orc_guide_forward(const double* params, const float* queries, int n, const float* lo, const float* inv,
-                      int emulate_bf16, double* mix) {
-    const bool bf = emulate_bf16 != 0;
+                      int flags, double* mix) {
+    const bool bf = (flags & 1) != 0;
     std::vector<double> W = weights(params, bf);
     Fwd F;
     for (int i = 0; i < n; i++) {
@@ -152,14 +160,16 @@ int orc_guide_forward(const double* params, const float* queries, int n, const f
         coords(Q, Q + 3, lo, inv, c6);
         encode(c6, bf, F.x);
         forward(params, W, bf, F);
-        mixture(F.y, mix + (size_t)i * OUT);
+        double anc[3];
+        anchor_of(flags, Q + 3, anc);
+        mixture(F.y, anc, mix + (size_t)i * OUT);
     }
     return 0;
 }
 
 int orc_guide_loss_grad(const double* params, const float* records, int n, const float* lo, const float* inv,
-                        int emulate_bf16, double* grad, double* loss) {
-    const bool bf = emulate_bf16 != 0;
+                        int flags, double* grad, double* loss) {
+    const bool bf = (flags & 1) != 0;
     std::vector<double> W = weights(params, bf);
     std::memset(grad, 0, sizeof(double) * NP);
     double total = 0.0;
@@ -172,7 +182,9 @@ int orc_guide_loss_grad(const double* params, const float* records, int n, const
         forward(params, W, bf, F);
         const double w[3] = {R[6], R[7], R[8]};
         double dy[OUT];
-        total += loss_grad(F.y, w, (double)R[9], dy);
+        double anc[3];
+        anchor_of(flags, R + 3, anc);
+        total += loss_grad(F.y, anc, w, (double)R[9], dy);
         for (int o = 0; o < OUT; o++) dy[o] = rb(dy[o], bf);
         // layer 4
         double dh3[HID] = {0};

@@ -56,12 +56,14 @@ int orc_render(void* scene, const mc_camera* cam, int W, int H, int spp, int fir
 /* Guiding MLP in FP64 (mc_guide_oracle.cpp). params: MC_GUIDE_PARAM_COUNT
  * doubles; lo/inv: the guide box's low corner and 1/extent (3 floats each).
  * Forward: n queries (6 floats) -> n x 40 mixtures. Loss/gradient: n records
- * (10 floats) -> gradient (PARAM_COUNT doubles) and the loss. emulate_bf16
- * rounds the values the tensor-core kernels round. */
+ * (10 floats) -> gradient (PARAM_COUNT doubles) and the loss. flags: bit 0
+ * rounds the values the tensor-core kernels round; bit 1 anchors the lobes
+ * (every raw mean offset by 1.5 x the direction input, mc_guide_config.
+ * anchor_lobes); bit 2 with bit 1 uses -1.5 (MC_GUIDE_DIR_RAY guides). */
 int orc_guide_forward(const double* params, const float* queries, int n, const float* lo, const float* inv,
-                      int emulate_bf16, double* mix);
+                      int flags, double* mix);
 int orc_guide_loss_grad(const double* params, const float* records, int n, const float* lo, const float* inv,
-                        int emulate_bf16, double* grad, double* loss);
+                        int flags, double* grad, double* loss);
 
 /* Philox-4x32-10 block (known-answer checks). */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

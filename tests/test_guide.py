@@ -76,6 +76,27 @@ def test_oracle_gradient_matches_finite_differences():
         assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i])), (i, fd, g[i])
 
 
+def test_oracle_anchored_gradient_matches_finite_differences():
+    """Anchored lobes (every raw mean offset by 1.5 x the direction input):
+    the offset is a constant, so the gradient still matches finite
+    differences."""
+    rng = np.random.default_rng(13)
+    params = _params(rng)
+    rec = _records(rng, 12)
+    for flags in (2, 6):
+        g, loss = _oracle_grad(params, rec, flags)
+        assert np.isfinite(loss) and np.all(np.isfinite(g))
+        assert loss != _oracle_grad(params, rec, 0)[1]
+        idx = np.concatenate([rng.choice(np.arange(off, off + size), 3, replace=False) for _, off, size in BLOCKS])
+        for i in idx:
+            h = 1e-6 * max(1.0, abs(params[i]))
+            pp, pm = params.copy(), params.copy()
+            pp[i] += h
+            pm[i] -= h
+            fd = (_oracle_grad(pp, rec, flags)[1] - _oracle_grad(pm, rec, flags)[1]) / (2 * h)
+            assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i])), (flags, i, fd, g[i])
+
+
 def test_oracle_bf16_mirror_stays_close_to_fp64():
     rng = np.random.default_rng(12)
     params = _params(rng)
@@ -114,11 +135,16 @@ def _gpu_grad(ctx, g, rec):
     return d_g.cpu().numpy().astype(np.float64), loss.value
 
 
+# (anchor_lobes, direction_input) -> the oracle's anchor flags
+ANCHOR_CASES = [(False, 0, 0), (True, 0, 2), (True, 1, 6)]
+
+
 @pytest.mark.gpu
-def test_inference_matches_oracle(ctx):
+@pytest.mark.parametrize("anchor,direction,aflags", ANCHOR_CASES)
+def test_inference_matches_oracle(ctx, anchor, direction, aflags):
     rng = np.random.default_rng(21)
     params = _params(rng)
-    g = _guide(ctx, params)
+    g = _guide(ctx, params, anchor_lobes=anchor, direction_input=direction)
     n = 1000
     q = np.zeros((n, 6), np.float32)
     q[:, 0:3] = rng.uniform(-1, 1, (n, 3))
@@ -127,7 +153,7 @@ def test_inference_matches_oracle(ctx):
     dq = torch.from_numpy(q).cuda()
     mcpt.check(ctx.lib.mc_guide_infer(g.handle, dq.data_ptr(), n, out.data_ptr()))
     got = out.cpu().numpy().reshape(n, 40).astype(np.float64)
-    ref = _oracle_mix(params, q, 1)
+    ref = _oracle_mix(params, q, 1 | aflags)
     np.testing.assert_allclose(got[:, :8].sum(1), 1.0, atol=1e-5)
     # BF16 activations: an FP32-accumulation difference can flip one rounding,
     # so a few elements sit further off than the bulk
@@ -136,20 +162,21 @@ def test_inference_matches_oracle(ctx):
     assert np.quantile(dm, 0.999) < 5e-3 and dm.max() < 3e-2
     np.testing.assert_allclose(got[:, 32:40], ref[:, 32:40], rtol=2e-2)
     # the pure FP64 network is close as well (BF16 is the only approximation)
-    ref64 = _oracle_mix(params, q, 0)
+    ref64 = _oracle_mix(params, q, aflags)
     assert np.abs(got[:, :8] - ref64[:, :8]).max() < 2e-2
     g.close()
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [100, 1000, 40000])
-def test_gradient_matches_oracle(ctx, n):
+@pytest.mark.parametrize("n,anchor,direction,aflags", [(100, False, 0, 0), (1000, False, 0, 0), (40000, False, 0, 0),
+                                                       (1000, True, 0, 2), (1000, True, 1, 6)])
+def test_gradient_matches_oracle(ctx, n, anchor, direction, aflags):
     rng = np.random.default_rng(22 + n)
     params = _params(rng)
-    g = _guide(ctx, params)
+    g = _guide(ctx, params, anchor_lobes=anchor, direction_input=direction)
     rec = _records(rng, n)
     got, loss = _gpu_grad(ctx, g, rec)
-    ref, rloss = _oracle_grad(params, rec, 1)
+    ref, rloss = _oracle_grad(params, rec, 1 | aflags)
     assert abs(loss - rloss) < 1e-3 * abs(rloss) + 1e-6
     for name, off, size in BLOCKS:
         a, b = got[off:off + size], ref[off:off + size]
@@ -227,3 +254,32 @@ def test_training_learns_a_directional_target(ctx):
     assert after > before + 2.0, (before, after)
     assert after > -2.53 + 2.0, after
     g.close()
+
+
+@pytest.mark.gpu
+def test_untrained_anchored_guide_proposes_around_the_normal(ctx):
+    """An untrained anchored guide: every lobe's mean lies close to the
+    direction input (the normal the renderer feeds it) and kappa starts near
+    e, so its first samples stay mostly above the surface; an unanchored
+    guide's means point anywhere."""
+    rng = np.random.default_rng(25)
+    n = 4096
+    q = np.zeros((n, 6), np.float32)
+    q[:, 0:3] = rng.uniform(-1, 1, (n, 3))
+    q[:, 3:6] = _unit(rng, n)
+    dq = torch.from_numpy(q).cuda()
+    cos = {}
+    for anchor in (False, True):
+        g = _guide(ctx, seed=9, anchor_lobes=anchor)
+        out = torch.zeros(n * 40, dtype=torch.float32, device="cuda")
+        mcpt.check(ctx.lib.mc_guide_infer(g.handle, dq.data_ptr(), n, out.data_ptr()))
+        m = out.cpu().numpy().reshape(n, 40).astype(np.float64)
+        means = m[:, 8:32].reshape(n, 8, 3)
+        cos[anchor] = np.einsum("nkj,nj->nk", means, q[:, 3:6].astype(np.float64))
+        if anchor:
+            kap = m[:, 32:40]
+            # log kappa = 1 + the untrained output layer's spread (about 0.13)
+            assert abs(np.median(kap) / np.e - 1.0) < 0.1 and kap.min() > np.exp(0.2) and kap.max() < np.exp(1.8)
+        g.close()
+    assert cos[True].min() > 0.9, cos[True].min()
+    assert abs(cos[False].mean()) < 0.2
