@@ -18,6 +18,7 @@ Multi-GPU (torchrun): every rank renders its own K frames of the full image
 all-reduce at the end, inside the timed region.
 """
 import argparse
+import copy
 import ctypes as C
 import json
 import os
@@ -86,6 +87,7 @@ def parse():
     ap.add_argument("--guide-pretrain-spp", type=int, default=0,
                     help="diagnostic: train the guide on this many untimed samples first (the headline trains from "
                          "scratch inside the timed region)")
+    ap.add_argument("--guide-batch", type=int, default=0, help="records per Adam step (0 = the library's 65536)")
     ap.add_argument("--guide-anchor", type=int, default=0, choices=[0, 1],
                     help="guiding: lobe means offset by the direction input (an untrained guide proposes around "
                          "the normal)")
@@ -536,6 +538,16 @@ def run_ours(args):
         out["guiding"]["mlp"] = {k: g["mlp"][k] for k in ("infer_queries_per_s", "infer_tflops", "infer_frac",
                                                           "train_records_per_s", "train_tflops", "train_frac",
                                                           "peak_tflops")}
+        # the same measurement with a guide that has already trained on 1024
+        # untimed samples of the view (what a resident scene's guide reaches
+        # in the server): anchored lobes, guiding and training at the first
+        # diffuse vertex only
+        ta = copy.copy(args)
+        ta.guide_anchor, ta.guide_depth, ta.guide_vertices, ta.guide_pretrain_spp = 1, 2, 1, 1024
+        t = run_guiding(ta, emit=False, mlp=False)
+        out["guiding_trained"] = {k: t[k] for k in ("value", "unit", "target_rmse", "plain_ms", "guided_ms_to_target",
+                                                    "guided_spp", "pretrain_spp", "anchor_lobes", "guided_depth",
+                                                    "train_vertices", "phase_split_ms")}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(scene, args)
     print(json.dumps(out), flush=True)
@@ -662,12 +674,14 @@ def run_mlp(args):
     guide.close()
 
 
-def run_guiding(args, emit=True):
+def run_guiding(args, emit=True, mlp=True):
     """Time to a fixed RMSE, guided vs plain wavefront, on the aperture room
     (about 200k triangles, 1024x1024, light only through a 0.2 x 0.2 hole).
     The target RMSE is plain wavefront's at --guide-plain-spp; the guided
-    renderer starts from an untrained guide, trains online (one Adam step per
-    sample) and counts every sample and every training step in its time. The
+    renderer starts from an untrained guide (or, with --guide-pretrain-spp, one
+    trained on that many untimed samples of the view), trains online
+    (--guide-steps Adam steps per sample) and counts every sample and every
+    training step in its time. The
     reference image is a plain render at --guide-ref-spp (its own noise adds
     the same amount to both MSEs). Firefly clamp off in all three (the clamp
     biases the estimators differently). Times are CUDA events around the
@@ -714,7 +728,8 @@ def run_guiding(args, emit=True):
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
                             train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                             guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
-                            fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor))
+                            fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor),
+                            batch_capacity=args.guide_batch)
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -742,7 +757,8 @@ def run_guiding(args, emit=True):
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
                        train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                        guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
-                       fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor))
+                       fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor),
+                            batch_capacity=args.guide_batch)
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -790,7 +806,7 @@ def run_guiding(args, emit=True):
         split[name]["other"] = round(split[name]["ms_per_spp"] - sum(v for k, v in split[name].items()
                                                                      if k != "ms_per_spp"), 3)
 
-    mlp = mlp_throughput(ctx, guide)
+    mlp = mlp_throughput(ctx, guide) if mlp else None
     guide.close()
     ratio = reached / plain_ms if reached is not None else None
     out = {"metric": "time to fixed RMSE vs plain wavefront", "value": round(ratio, 4) if ratio is not None else None,
@@ -802,7 +818,7 @@ def run_guiding(args, emit=True):
            "pretrain_spp": args.guide_pretrain_spp,
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
            "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap, "fold_below": bool(args.guide_fold),
-           "anchor_lobes": bool(args.guide_anchor),
+           "anchor_lobes": bool(args.guide_anchor), "batch_records": int(guide.config.batch_capacity) or 65536,
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,

@@ -782,14 +782,20 @@ MC_D int warp_reserve(bool want, int* counter, unsigned ltmask) {
     return want ? base + __popc(m & ltmask) : -1;
 }
 
-// 4 resident blocks (64 registers, a few spills) beat 2 blocks of 113
-// registers by 5 %: shading waits on scattered loads (hit, material, light,
-// texture) and more warps hide more of that latency.
+// Shading waits on scattered loads (hit, material, light, texture), so its
+// residency trades warps against spills: 3 resident blocks (80 registers, no
+// spills in the Philox variants) render the benchmark 0.6 % faster than 4
+// blocks of 64 registers (118-byte spills), which beat 2 blocks of 113 by 5 %.
+// Guided shading: 3 blocks (80 registers, 46-byte spills) take 8 % less time
+// than 2 blocks of 127.
+#ifndef MC_SHADE_BLOCKS
+#define MC_SHADE_BLOCKS 3
+#endif
 #ifndef MC_GUIDED_SHADE_BLOCKS
-#define MC_GUIDED_SHADE_BLOCKS 2
+#define MC_GUIDED_SHADE_BLOCKS 3
 #endif
 template <class Rng, bool GUIDED, bool ALIAS = false>
-__global__ void __launch_bounds__(256, GUIDED ? MC_GUIDED_SHADE_BLOCKS : 4) k_shade(ShadeArgs a) {
+__global__ void __launch_bounds__(256, GUIDED ? MC_GUIDED_SHADE_BLOCKS : MC_SHADE_BLOCKS) k_shade(ShadeArgs a) {
     const unsigned ltmask = lanemask_lt();
     const int count = min(*a.count, a.capacity);
     for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
