@@ -88,6 +88,8 @@ def parse():
                     help="diagnostic: train the guide on this many untimed samples first (the headline trains from "
                          "scratch inside the timed region)")
     ap.add_argument("--guide-batch", type=int, default=0, help="records per Adam step (0 = the library's 65536)")
+    ap.add_argument("--guide-nee", type=int, default=0, choices=[0, 1],
+                    help="guiding: the primary vertices' shadow rays also give training records")
     ap.add_argument("--guide-anchor", type=int, default=0, choices=[0, 1],
                     help="guiding: lobe means offset by the direction input (an untrained guide proposes around "
                          "the normal)")
@@ -729,7 +731,8 @@ def run_guiding(args, emit=True, mlp=True):
                             train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                             guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
                             fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor),
-                            batch_capacity=args.guide_batch)
+                            batch_capacity=args.guide_batch,
+                            nee_records=bool(args.guide_nee))
     render(tmp, chunk, 999998, warm_guide, 1)
     render(tmp, chunk, 999990, warm_guide, 1)
     warm_guide.close()
@@ -758,7 +761,8 @@ def run_guiding(args, emit=True, mlp=True):
                        train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                        guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
                        fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor),
-                            batch_capacity=args.guide_batch)
+                            batch_capacity=args.guide_batch,
+                            nee_records=bool(args.guide_nee))
     # an untimed render without training sizes the new guide's buffers; its
     # weights stay as initialised
     render(tmp, chunk, 999997, guide, 0)
@@ -819,6 +823,7 @@ def run_guiding(args, emit=True, mlp=True):
            "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
            "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap, "fold_below": bool(args.guide_fold),
            "anchor_lobes": bool(args.guide_anchor), "batch_records": int(guide.config.batch_capacity) or 65536,
+           "nee_records": bool(args.guide_nee),
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),
            "plain_curve": plain_curve, "guided_curve": g_curve, "phase_split_ms": split,

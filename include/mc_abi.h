@@ -724,7 +724,13 @@ typedef struct mc_guide_config {
                                    for MC_GUIDE_DIR_RAY), normalized, and kappa starts near e: an untrained
                                    guide proposes directions around the normal, a cosine-like lobe, instead of
                                    a near-uniform sphere whose lower half ends paths. 0 = off (raw means) */
-    int32_t pad2;
+    int32_t nee_records;        /* 1: guided renders' training also takes a record from each primary diffuse
+                                   vertex's next-event sample (the direction to the light point, weighted by
+                                   the light it brought, times its MIS weight), and the records of that vertex's
+                                   sampled direction keep only their MIS-weighted share of the emission they
+                                   found: the two kinds together still estimate the incident light, and every
+                                   unoccluded shadow ray toward a small light becomes a training sample.
+                                   0 = off */
 } mc_guide_config;
 
 /* Length of the direction-input offset added to every raw lobe mean when

@@ -952,10 +952,11 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     if (g->cfg.guided_depth <= 0) g->cfg.guided_depth = 4;
     if (!(g->cfg.weight_cap >= 0.f)) g->cfg.weight_cap = 0.f;
     if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1 ||
-        g->cfg.anchor_lobes < 0 || g->cfg.anchor_lobes > 1) {
+        g->cfg.anchor_lobes < 0 || g->cfg.anchor_lobes > 1 || g->cfg.nee_records < 0 || g->cfg.nee_records > 1) {
         delete g;
         return mc::set_error(MC_ERR_INVALID,
-                             "mc_guide_create: train_vertices above %d, unknown direction_input or anchor_lobes not 0/1",
+                             "mc_guide_create: train_vertices above %d, unknown direction_input, or anchor_lobes or "
+                             "nee_records not 0/1",
                              MC_GUIDE_MAX_TRAIN_VERTICES);
     }
     const size_t P = (size_t)kParams * sizeof(float);

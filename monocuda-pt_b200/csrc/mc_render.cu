@@ -436,6 +436,7 @@ struct ShadeArgs {
     int dirNormal;
     int mixShare;     // bounce 0 of a single-item pixel-major wave: the pixel's samples read its first path's mixture
     int fold;         // guide directions below the surface are mirrored up (guided_pdf)
+    int neeRec;       // the primary vertex's next-event sample also gives a training record
 };
 
 // Training record of a diffuse vertex (recSlots per path, slot = depth):
@@ -443,7 +444,9 @@ struct ShadeArgs {
 // [6..8] sampled direction, [9] mean throughput that reached the vertex,
 // [10] valid (the sampled direction was traced), [11] MIS remainder of the
 // emission that direction found, [12] mean sample radiance not carried by
-// that direction (everything before the vertex plus its own NEE).
+// that direction (everything before the vertex plus its own NEE), [13..15]
+// in slot 0 with NEE records: the direction of the vertex's shadow ray (zero
+// when it cast none); the light it brought is the primary vertex's NEE buffer.
 constexpr int kRecFloats = 16;
 
 // The path whose mixture a path samples: itself, or at a shared bounce 0 the
@@ -530,8 +533,12 @@ MC_D float guided_pdf(const float* m, float frac, const V3& n, const V3& w, bool
 // NEE's side of the MIS carries instead is kept in the record's spare slot and
 // added to its weight. Without it a broad early guide, whose density is tiny
 // next to the light's, would never be pulled toward a small light.
+//
+// With NEE records (neeRec) the primary vertex's shadow rays are records of
+// their own, weighted by NEE's MIS share, so the sampled direction keeps only
+// its MIS-weighted share too: the two kinds add up to the incident light.
 MC_D void train_remainder(const ShadeArgs& a, int p, int depth, const V3& L, float w) {
-    if (w >= 1.0f || depth < 1 || depth > a.recSlots) return;
+    if (w >= 1.0f || depth < 1 || depth > a.recSlots || (a.neeRec && depth == 1)) return;
     float* r = rec_slot(a, p, depth - 1);
     if (r[10] == 0.0f) return;
     r[11] = (L.x + L.y + L.z) * (1.0f / 3.0f) * (1.0f - w);
@@ -690,6 +697,18 @@ MC_D void shade_path(const ShadeArgs& a, const SceneGPU& S, int p, ShadeOut& out
             out.smax = dist * 0.999f;
             out.contrib = contribution;
         }
+        if (GUIDED && a.rec && a.neeRec && depth == 0 && mat.type == MC_MAT_LAMBERTIAN) {
+            // the vertex fields of slot 0 (the sampled direction's record writes
+            // the same values), and the shadow ray's direction
+            float* r = rec_slot(a, p, 0);
+            const V3 din = a.dirNormal ? faceNormal : inDir;
+            r[0] = scatterOrigin.x; r[1] = scatterOrigin.y; r[2] = scatterOrigin.z;
+            r[3] = din.x; r[4] = din.y; r[5] = din.z;
+            r[9] = (tPre.x + tPre.y + tPre.z) * (1.0f / 3.0f);
+            if (out.shadow) {
+                r[13] = toLight.x; r[14] = toLight.y; r[15] = toLight.z;
+            }
+        }
     }
     bool survives = true;
     if (depth > 3) {
@@ -814,6 +833,12 @@ __global__ void __launch_bounds__(256, GUIDED ? MC_GUIDED_SHADE_BLOCKS : MC_SHAD
                     r[10] = 0.0f;
                     r[11] = 0.0f;
                     r[12] = 0.0f;
+                }
+                if (a.neeRec) {
+                    float* r = rec_slot(a, p, 0);
+                    r[13] = 0.0f;
+                    r[14] = 0.0f;
+                    r[15] = 0.0f;
                 }
             }
             shade_path<Rng, GUIDED, ALIAS>(a, S, p, out);
@@ -956,25 +981,50 @@ __global__ void k_finalize(const WaveTable* tab, const float* sr, const float* s
 // through the sampled direction (the sample minus what it held before that
 // direction was traced, plus the MIS remainder of emission the direction
 // found) over the mean throughput that reached the vertex. The primary
-// vertex's NEE goes to its own buffer, so the sample holds none of it.
+// vertex's NEE goes to its own buffer, so the sample holds none of it. With
+// NEE records each path has one more slot after its R vertex slots: the
+// primary vertex's shadow ray, a record when it reached light (its NEE buffer
+// over the throughput that reached the vertex; the sampled direction's record
+// then carries no MIS remainder).
 constexpr int kRecThreads = 256;
 constexpr int kRecTileChunks = 8;
 constexpr int kRecTile = kRecThreads * kRecTileChunks;  // entries per tile
 
-MC_D bool rec_entry(const WaveTable* tab, long long v, int recSlots, int recStride, int recPhase, const float* sr,
-                    const float* sg, const float* sb, const float* rec, const float** out, float* weight) {
+struct RecSource {
+    const float *sr, *sg, *sb;  // the wave's samples
+    const float *nr, *ng, *nb;  // the primary vertices' NEE
+    const float* rec;
+    int recSlots;               // vertex slots per path
+    int neeRec;                 // 1: one more slot per path, the primary vertex's shadow ray
+};
+
+// dirOff: where the record's direction sits in its slot (6 for a sampled
+// direction, 13 for a shadow ray).
+MC_D bool rec_entry(const WaveTable* tab, long long v, const RecSource& src, int recStride, int recPhase,
+                    const float** out, float* weight, int* dirOff) {
+    const int slots = src.recSlots + src.neeRec;
     const int pixels = tab->totalPixels;
     const long long js = v / pixels;
     const int u = (int)(v - js * pixels);
-    const int j = (int)(js / recSlots);
-    const int k = (int)(js - (long long)j * recSlots);
-    if ((u + j * recSlots + k + recPhase) % recStride != 0) return false;
+    const int j = (int)(js / slots);
+    const int k = (int)(js - (long long)j * slots);
+    if ((u + j * slots + k + recPhase) % recStride != 0) return false;
     const SceneGPU& S = tab->scenes[tab->nScenes > 1 ? find_scene_by_pixel(tab, u) : 0];
     if (j >= S.pathStride) return false;
     const int p = S.pathOffset + (u - S.pixelOffset) * S.pathStride + j;
-    const float* r = rec + ((size_t)p * recSlots + k) * kRecFloats;
-    if (r[10] == 0.0f || !(r[9] > 0.0f)) return false;
-    const float w = ((sr[p] + sg[p] + sb[p]) * (1.0f / 3.0f) - r[12] + r[11]) / r[9];
+    float w;
+    const float* r;
+    if (k == src.recSlots) {
+        r = src.rec + (size_t)p * src.recSlots * kRecFloats;
+        if (!(r[9] > 0.0f) || (r[13] == 0.0f && r[14] == 0.0f && r[15] == 0.0f)) return false;
+        w = (src.nr[p] + src.ng[p] + src.nb[p]) * (1.0f / 3.0f) / r[9];
+        *dirOff = 13;
+    } else {
+        r = src.rec + ((size_t)p * src.recSlots + k) * kRecFloats;
+        if (r[10] == 0.0f || !(r[9] > 0.0f)) return false;
+        w = ((src.sr[p] + src.sg[p] + src.sb[p]) * (1.0f / 3.0f) - r[12] + r[11]) / r[9];
+        *dirOff = 6;
+    }
     *out = r;
     *weight = w;
     return w > 0.0f && w < 1e30f;
@@ -987,7 +1037,7 @@ __global__ void __launch_bounds__(kRecThreads) k_finalize_guided(const WaveTable
                                                                  const float* sr, const float* sg, const float* sb,
                                                                  const float* nr, const float* ng, const float* nb,
                                                                  const float* rec, int* tileCounts, long long entries,
-                                                                 int recSlots, int recStride, int recPhase) {
+                                                                 int recSlots, int neeRec, int recStride, int recPhase) {
     // the image: each pixel adds its samples of the wave in sample order
     const int pixels = tab->totalPixels;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < pixels; u += gridDim.x * blockDim.x) {
@@ -1009,6 +1059,7 @@ __global__ void __launch_bounds__(kRecThreads) k_finalize_guided(const WaveTable
         acc[2] = a2;
     }
     if (!rec) return;
+    const RecSource src{sr, sg, sb, nr, ng, nb, rec, recSlots, neeRec};
     // the training records: each tile's count (k_rec_scan and k_rec_write place them)
     const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
@@ -1017,8 +1068,8 @@ __global__ void __launch_bounds__(kRecThreads) k_finalize_guided(const WaveTable
             const long long v = (long long)t * kRecTile + i * kRecThreads + threadIdx.x;
             const float* r;
             float w;
-            c += __syncthreads_count(v < entries &&
-                                     rec_entry(tab, v, recSlots, recStride, recPhase, sr, sg, sb, rec, &r, &w));
+            int dirOff;
+            c += __syncthreads_count(v < entries && rec_entry(tab, v, src, recStride, recPhase, &r, &w, &dirOff));
         }
         if (threadIdx.x == 0) tileCounts[t] = c;
     }
@@ -1062,9 +1113,8 @@ __global__ void __launch_bounds__(1024) k_rec_scan(int* tileCounts, int tiles, i
 
 // Writes each kept record to its slot in (sample, pixel) order: the tile's
 // first slot (k_rec_scan) plus the kept entries before it in the tile.
-__global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab, const float* sr, const float* sg,
-                                                           const float* sb, const float* rec, const int* tileFirst,
-                                                           long long entries, int recSlots, int recStride, int recPhase,
+__global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab, const RecSource src, const int* tileFirst,
+                                                           long long entries, int recStride, int recPhase,
                                                            float* batch, int capacity) {
     __shared__ int warpCount[kRecThreads / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1076,7 +1126,8 @@ __global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab,
             const long long v = (long long)t * kRecTile + i * kRecThreads + threadIdx.x;
             const float* r = nullptr;
             float w = 0.f;
-            const bool e = v < entries && rec_entry(tab, v, recSlots, recStride, recPhase, sr, sg, sb, rec, &r, &w);
+            int dirOff = 6;
+            const bool e = v < entries && rec_entry(tab, v, src, recStride, recPhase, &r, &w, &dirOff);
             const unsigned m = __ballot_sync(kFull, e);
             if (lane == 0) warpCount[wid] = __popc(m);
             __syncthreads();
@@ -1089,7 +1140,8 @@ __global__ void __launch_bounds__(kRecThreads) k_rec_write(const WaveTable* tab,
             const int slot = before + __popc(m & ltmask);
             if (e && slot < capacity) {
                 float* b = batch + (size_t)slot * MC_GUIDE_RECORD_FLOATS;
-                for (int k = 0; k < 9; k++) b[k] = r[k];
+                for (int k = 0; k < 6; k++) b[k] = r[k];
+                for (int k = 0; k < 3; k++) b[6 + k] = r[dirOff + k];
                 b[9] = w;
             }
             next += all;
@@ -1553,8 +1605,8 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         if ((st = guide_reserve_batch(guide, guide->cfg.batch_capacity * guide->cfg.train_steps * maxR)) != MC_OK) return st;
         long long pixelsAll = 0;
         for (int i = 0; i < n; i++) pixelsAll += (long long)items[i].p->width * items[i].p->height;
-        if ((st = guide_reserve_tiles(guide, (int)((pixelsAll * maxR * guide->cfg.train_vertices + kRecTile - 1) /
-                                                   kRecTile))) != MC_OK)
+        const long long slotsAll = guide->cfg.train_vertices + (guide->cfg.nee_records ? 1 : 0);
+        if ((st = guide_reserve_tiles(guide, (int)((pixelsAll * maxR * slotsAll + kRecTile - 1) / kRecTile))) != MC_OK)
             return st;
     }
     // the launch sequence of one wave (device table already holds the wave)
@@ -1651,6 +1703,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
                 sd.dirNormal = guide->cfg.direction_input == MC_GUIDE_DIR_NORMAL ? 1 : 0;
                 sd.mixShare = d == 0 && shareMix ? 1 : 0;
                 sd.fold = guide->cfg.fold_below ? 1 : 0;
+                sd.neeRec = train && guide->cfg.nee_records ? 1 : 0;
                 phaseBegin(1);
                 if (alias) k_shade<PhiloxRng, true, true><<<guidedBlocks, 256, 0, stream>>>(sd);
                 else k_shade<PhiloxRng, true><<<guidedBlocks, 256, 0, stream>>>(sd);
@@ -1677,17 +1730,19 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         }
         if (guide) {
             const int slots = guide->cfg.train_vertices;
-            const long long entries = train ? (long long)slots * waveR * wavePixels : 0;
+            const int neeRec = guide->cfg.nee_records ? 1 : 0;
+            const long long entries = train ? (long long)(slots + neeRec) * waveR * wavePixels : 0;
             k_finalize_guided<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, sceneOf, w.sr, w.sg, w.sb, nee0[0], nee0[1],
                                                                       nee0[2], train ? guide->records : nullptr,
-                                                                      guide->rec_tiles, entries, slots, recStride,
-                                                                      recPhase);
+                                                                      guide->rec_tiles, entries, slots, neeRec,
+                                                                      recStride, recPhase);
             if (train) {
                 phaseBegin(3);
                 const int tiles = (int)((entries + kRecTile - 1) / kRecTile);
+                const RecSource src{w.sr, w.sg, w.sb, nee0[0], nee0[1], nee0[2], guide->records, slots, neeRec};
                 k_rec_scan<<<1, 1024, 0, stream>>>(guide->rec_tiles, tiles, guide->batch_count);
-                k_rec_write<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, w.sr, w.sg, w.sb, guide->records, guide->rec_tiles,
-                                                                    entries, slots, recStride, recPhase, guide->batch,
+                k_rec_write<<<loopBlocks, kRecThreads, 0, stream>>>(dtab, src, guide->rec_tiles, entries, recStride,
+                                                                    recPhase, guide->batch,
                                                                     guide->cfg.batch_capacity * guide->cfg.train_steps *
                                                                         waveR);
                 phaseEnd();
@@ -1787,7 +1842,7 @@ mc_status run_waves(mc_context* ctx, const mc_bvh* bvh, const WaveItem* items, i
         wavePixels = pix;
         if (guide) {
             const long long cap = (long long)guide->cfg.batch_capacity * guide->cfg.train_steps * waveR;
-            const long long entries = (long long)guide->cfg.train_vertices * off;
+            const long long entries = (long long)(guide->cfg.train_vertices + (guide->cfg.nee_records ? 1 : 0)) * off;
             recStride = (int)std::max(1ll, (entries + cap - 1) / cap);
             recPhase = wv % recStride;
         }

@@ -151,7 +151,7 @@ class GuideConfig(C.Structure):
                 ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
                 ("guide_fraction", C.c_float), ("train_steps", C.c_int32), ("train_vertices", C.c_int32),
                 ("direction_input", C.c_int32), ("guided_depth", C.c_int32), ("weight_cap", C.c_float),
-                ("fold_below", C.c_int32), ("anchor_lobes", C.c_int32), ("_pad", C.c_int32)]
+                ("fold_below", C.c_int32), ("anchor_lobes", C.c_int32), ("nee_records", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -737,7 +737,7 @@ class Guide:
 
     def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5,
                  train_steps=1, train_vertices=0, direction_input=0, guided_depth=0, weight_cap=0.0, fold_below=False,
-                 anchor_lobes=False):
+                 anchor_lobes=False, nee_records=False):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = GuideConfig()
@@ -754,6 +754,7 @@ class Guide:
         cfg.weight_cap = weight_cap
         cfg.fold_below = 1 if fold_below else 0
         cfg.anchor_lobes = 1 if anchor_lobes else 0
+        cfg.nee_records = 1 if nee_records else 0
         self.config = cfg
         h = P()
         check(self.lib.mc_guide_create(ctx.handle, C.byref(cfg), C.byref(h)))
