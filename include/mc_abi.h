@@ -236,7 +236,10 @@ typedef struct mc_bvh_build_opts {
     int32_t layout;             /* MC_BVH_LAYOUT_* */
     int32_t keep_reference_nodes; /* keep PT-layout nodes for mc_bvh_export */
     int32_t builder;            /* MC_BVH_BUILDER_*: the binary tree the wide layouts collapse */
-    int32_t pad0;
+    int32_t phase_launches;     /* 1: the clustering rounds and the 4-wide collapse's levels run as one
+                                   launch per phase with host checks between them; 0: each loop runs as one
+                                   cooperative (persistent) launch where the device supports it. The same
+                                   tree either way */
 } mc_bvh_build_opts;
 
 typedef struct mc_bvh_info {
@@ -609,6 +612,12 @@ MC_API mc_status mc_bvh_get_info(const mc_bvh* bvh, mc_bvh_info* info);
  * (n-1) and leaves (n) as mc_bvh_node. Needs keep_reference_nodes for nodes. */
 MC_API mc_status mc_bvh_export(const mc_bvh* bvh, uint32_t* d_codes, int32_t* d_ids, int32_t* d_types,
                                mc_bvh_node* d_internal, mc_bvh_node* d_leaves);
+/* Copies of the arrays the traversal reads (device buffers, either may be
+ * NULL): the node array (mc_bvh_info.node_bytes bytes) and the leaf-ordered
+ * primitive records (mc_bvh_info.prim_bytes bytes), e.g. to store a built tree
+ * or to compare two builds byte for byte. No counterpart in the reference,
+ * whose traversal reads its exported node layout directly. */
+MC_API mc_status mc_bvh_export_traversal(const mc_bvh* bvh, void* d_nodes, void* d_prims);
 
 /* ------------------------------------------------------------------------- */
 /* Ray sets (a8-a15). Rays are SoA: 7 device float arrays of n entries packed  */

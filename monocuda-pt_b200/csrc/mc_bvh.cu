@@ -17,6 +17,7 @@
 // This file is compiled WITHOUT fast math and with -fmad=false: the reference
 // computes bounds and Morton codes on the host with IEEE single precision and
 // no contraction, and the codes must match bit for bit.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -652,18 +653,16 @@ __global__ void k_scatter_ids(const int* __restrict__ roots, int n, int* __restr
     if (i < n) wideId[roots[i]] = i;
 }
 
-// One level of the collapse, in three launches so that wide ids follow the
+// One level of the collapse, in three steps so that wide ids follow the
 // frontier's order (the same layout on every build: breadth first, the
 // internal children of a wide node consecutive, in slot order).
 // Count: every wide node of the frontier picks its slots, keeps its internal
-// ones in slot order and adds their number to its block's total.
-__global__ void __launch_bounds__(kBlock) k_wide_level_count(const float4* __restrict__ nodes,
-                                                             const int* __restrict__ frontier, int n, int capacity,
-                                                             const int* __restrict__ wideId, int* __restrict__ rootOf,
-                                                             int4* __restrict__ internal, int* __restrict__ blockTotals,
-                                                             int* err) {
-    __shared__ int warpSum[kBlock / 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// ones in slot order and adds their number to its tile's total (tile = kBlock
+// frontier entries, one block; warpSum: kBlock / 32 entries).
+__device__ __forceinline__ void wide_count_tile(const float4* nodes, const int* frontier, int n, int capacity,
+                                                const int* wideId, int* rootOf, int4* internal, int* blockTotals, int* err,
+                                                int tile, int* warpSum) {
+    const int i = tile * kBlock + threadIdx.x;
     int nInt = 0;
     if (i < n) {
         const int B = frontier[i];
@@ -687,21 +686,29 @@ __global__ void __launch_bounds__(kBlock) k_wide_level_count(const float4* __res
     if (threadIdx.x == 0) {
         int t = 0;
         for (int k = 0; k < kBlock / 32; k++) t += warpSum[k];
-        blockTotals[blockIdx.x] = t;
+        blockTotals[tile] = t;
     }
+    __syncthreads();  // warpSum is reused by the block's next tile
 }
 
-// Scan: exclusive prefix of the block totals by one block of 1024 threads;
-// the level's total (the next frontier's size) goes to *total.
-__global__ void __launch_bounds__(1024) k_wide_level_scan(int* blockTotals, int blocks, int* total) {
-    __shared__ int warpSums[32];
-    __shared__ int carry;
+__global__ void __launch_bounds__(kBlock) k_wide_level_count(const float4* __restrict__ nodes,
+                                                             const int* __restrict__ frontier, int n, int capacity,
+                                                             const int* __restrict__ wideId, int* __restrict__ rootOf,
+                                                             int4* __restrict__ internal, int* __restrict__ blockTotals,
+                                                             int* err) {
+    __shared__ int warpSum[kBlock / 32];
+    wide_count_tile(nodes, frontier, n, capacity, wideId, rootOf, internal, blockTotals, err, blockIdx.x, warpSum);
+}
+
+// Scan: exclusive prefix of `count` ints in place by one block (a multiple of
+// 32 threads, at most 1024; warpSums: 32 entries); the total goes to *total.
+__device__ __forceinline__ void scan_ints_block(int* v, int count, int* total, int* warpSums, int& carry) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int base = 0; base < blocks; base += 1024) {
+    for (int base = 0; base < count; base += blockDim.x) {
         const int t = base + threadIdx.x;
-        const int c = t < blocks ? blockTotals[t] : 0;
+        const int c = t < count ? v[t] : 0;
         int x = c;
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
@@ -710,7 +717,7 @@ __global__ void __launch_bounds__(1024) k_wide_level_scan(int* blockTotals, int 
         if (lane == 31) warpSums[wid] = x;
         __syncthreads();
         if (wid == 0) {
-            int s = warpSums[lane];
+            int s = lane < (int)(blockDim.x >> 5) ? warpSums[lane] : 0;
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, s, o);
                 if (lane >= o) s += y;
@@ -719,23 +726,26 @@ __global__ void __launch_bounds__(1024) k_wide_level_scan(int* blockTotals, int 
         }
         __syncthreads();
         const int before = carry + (wid > 0 ? warpSums[wid - 1] : 0) + x - c;
-        if (t < blocks) blockTotals[t] = before;
+        if (t < count) v[t] = before;
         __syncthreads();
-        if (threadIdx.x == 1023) carry = before + c;
+        if (threadIdx.x == blockDim.x - 1) carry = before + c;
         __syncthreads();
     }
     if (threadIdx.x == 0) *total = carry;
 }
 
+__global__ void __launch_bounds__(1024) k_wide_level_scan(int* blockTotals, int blocks, int* total) {
+    __shared__ int warpSums[32];
+    __shared__ int carry;
+    scan_ints_block(blockTotals, blocks, total, warpSums, carry);
+}
+
 // Write: the internal children of frontier node i take wide ids idBase + o,
 // o = (internal children of the nodes before i), and the same places of the
 // next frontier.
-__global__ void __launch_bounds__(kBlock) k_wide_level_write(const int4* __restrict__ internal, int n,
-                                                             const int* __restrict__ blockFirst, int idBase,
-                                                             int capacity, int* __restrict__ next,
-                                                             int* __restrict__ wideId, int* err) {
-    __shared__ int warpSum[kBlock / 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void wide_write_tile(const int4* internal, int n, const int* blockFirst, int idBase,
+                                                int capacity, int* next, int* wideId, int* err, int tile, int* warpSum) {
+    const int i = tile * kBlock + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int4 r = make_int4(-1, -1, -1, -1);
     if (i < n) r = internal[i];
@@ -747,7 +757,7 @@ __global__ void __launch_bounds__(kBlock) k_wide_level_write(const int4* __restr
     }
     if (lane == 31) warpSum[wid] = x;
     __syncthreads();
-    int off = blockFirst[blockIdx.x] + x - nInt;
+    int off = blockFirst[tile] + x - nInt;
     for (int k = 0; k < wid; k++) off += warpSum[k];
     const int refs[4] = {r.x, r.y, r.z, r.w};
     for (int k = 0; k < nInt; k++) {
@@ -757,6 +767,70 @@ __global__ void __launch_bounds__(kBlock) k_wide_level_write(const int4* __restr
         }
         wideId[refs[k]] = idBase + off + k;
         next[off + k] = refs[k];
+    }
+    __syncthreads();  // warpSum is reused by the block's next tile
+}
+
+__global__ void __launch_bounds__(kBlock) k_wide_level_write(const int4* __restrict__ internal, int n,
+                                                             const int* __restrict__ blockFirst, int idBase,
+                                                             int capacity, int* __restrict__ next,
+                                                             int* __restrict__ wideId, int* err) {
+    __shared__ int warpSum[kBlock / 32];
+    wide_write_tile(internal, n, blockFirst, idBase, capacity, next, wideId, err, blockIdx.x, warpSum);
+}
+
+// Every level of the collapse in one cooperative launch: the three steps of
+// a level as loops over the same tiles, a grid-wide barrier after each; all
+// blocks read the level's total from the same place after a barrier, so they
+// run the same levels. Ends when a level adds no internal node, after
+// maxLevels + 1 levels, or when the wide ids would pass the node count (error).
+struct WideLevels {
+    const float4* nodes;
+    int* front[2];
+    int nseg, capacity, maxLevels;
+    int* wideId;
+    int* rootOf;
+    int4* internal;
+    int* blockTotals;
+    int* total;
+    int* out;  // [0] levels, [1] wide nodes, [2] last frontier size, [3] 1 when the ids would pass capacity
+    int* err;
+};
+
+__global__ void __launch_bounds__(kBlock) k_wide_levels(WideLevels a) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    __shared__ int warpSum[32];
+    __shared__ int carry;
+    int n = a.nseg, idBase = a.nseg, cur = 0, levels = 0;
+    bool bad = false;
+    while (n > 0 && levels <= a.maxLevels) {
+        const int* front = cur ? a.front[1] : a.front[0];
+        int* next = cur ? a.front[0] : a.front[1];
+        const int tiles = (n + kBlock - 1) / kBlock;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x)
+            wide_count_tile(a.nodes, front, n, a.capacity, a.wideId, a.rootOf, a.internal, a.blockTotals, a.err, t,
+                            warpSum);
+        grid.sync();
+        if (blockIdx.x == 0) scan_ints_block(a.blockTotals, tiles, a.total, warpSum, carry);
+        grid.sync();
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x)
+            wide_write_tile(a.internal, n, a.blockTotals, idBase, a.capacity, next, a.wideId, a.err, t, warpSum);
+        grid.sync();
+        const int m = *a.total;  // written by block 0 before the last barrier
+        if (m < 0 || (long long)idBase + m > a.capacity) {
+            bad = true;
+            break;
+        }
+        idBase += m;
+        n = m;
+        cur = 1 - cur;
+        levels++;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out[0] = levels;
+        a.out[1] = idBase;
+        a.out[2] = n;
+        a.out[3] = bad ? 1 : 0;
     }
 }
 
@@ -1223,12 +1297,11 @@ __device__ __forceinline__ float merged_area(float4 alo, float4 ahi, float4 blo,
 
 // nn[i] = the position j != i, |i - j| <= kPlocRadius, same scene, of least
 // merged area (ties: the lower j); -1 when no cluster of its scene is near.
-__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float4* __restrict__ cbox, const int* __restrict__ nPtr,
-                                                         int* __restrict__ nn) {
-    __shared__ float4 sLo[kPlocBlock + 2 * kPlocRadius], sHi[kPlocBlock + 2 * kPlocRadius];
-    const int n = *nPtr;
-    const int b0 = blockIdx.x * kPlocBlock;
-    if (b0 >= n) return;
+// One block of kPlocBlock threads takes the positions b0 .. b0 + kPlocBlock - 1
+// through a shared window (sLo / sHi: kPlocBlock + 2 kPlocRadius entries).
+// Plain loads: the persistent rounds read what other blocks wrote earlier in
+// the same launch.
+__device__ __forceinline__ void ploc_nn_tile(const float4* cbox, int n, int b0, int* nn, float4* sLo, float4* sHi) {
     for (int t = threadIdx.x; t < kPlocBlock + 2 * kPlocRadius; t += blockDim.x) {
         const int g = b0 - kPlocRadius + t;
         if (g >= 0 && g < n) {
@@ -1241,44 +1314,55 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float4* __restrict
     }
     __syncthreads();
     const int i = b0 + threadIdx.x;
-    if (i >= n) return;
-    const int me = threadIdx.x + kPlocRadius;
-    const float4 lo = sLo[me], hi = sHi[me];
-    const int s = __float_as_int(lo.w);
-    float best = INFINITY;
-    int bj = -1;
-    for (int o = -kPlocRadius; o <= kPlocRadius; o++) {
-        const int j = i + o;
-        if (o == 0 || j < 0 || j >= n) continue;
-        const float4 l2 = sLo[me + o];
-        if (__float_as_int(l2.w) != s) continue;
-        const float a = merged_area(lo, hi, l2, sHi[me + o]);
-        if (a < best) {
-            best = a;
-            bj = j;
+    if (i < n) {
+        const int me = threadIdx.x + kPlocRadius;
+        const float4 lo = sLo[me], hi = sHi[me];
+        const int s = __float_as_int(lo.w);
+        float best = INFINITY;
+        int bj = -1;
+        for (int o = -kPlocRadius; o <= kPlocRadius; o++) {
+            const int j = i + o;
+            if (o == 0 || j < 0 || j >= n) continue;
+            const float4 l2 = sLo[me + o];
+            if (__float_as_int(l2.w) != s) continue;
+            const float a = merged_area(lo, hi, l2, sHi[me + o]);
+            if (a < best) {
+                best = a;
+                bj = j;
+            }
         }
+        nn[i] = bj;
     }
-    nn[i] = bj;
+    __syncthreads();  // the window is refilled by the block's next tile
+}
+
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float4* __restrict__ cbox, const int* __restrict__ nPtr,
+                                                         int* __restrict__ nn) {
+    __shared__ float4 sLo[kPlocBlock + 2 * kPlocRadius], sHi[kPlocBlock + 2 * kPlocRadius];
+    const int n = *nPtr;
+    const int b0 = blockIdx.x * kPlocBlock;
+    if (b0 >= n) return;
+    ploc_nn_tile(cbox, n, b0, nn, sLo, sHi);
 }
 
 // (merge, alive) per cluster: a mutual pair merges at its lower position and
 // the higher one disappears; every other cluster stays.
-__global__ void k_ploc_flags(const int* __restrict__ nn, const int* __restrict__ nPtr, int2* __restrict__ flags) {
-    const int n = *nPtr;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int j = nn[i];
-        const bool mutual = j >= 0 && nn[j] == i;
-        flags[i] = make_int2(mutual && i < j ? 1 : 0, (!mutual || i < j) ? 1 : 0);
-    }
+__device__ __forceinline__ int2 ploc_flag(const int* nn, int i) {
+    const int j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    return make_int2(mutual && i < j ? 1 : 0, (!mutual || i < j) ? 1 : 0);
 }
 
-// Exclusive scan of int2 values: per block of kPlocBlock * kScanItems items,
-// then the block sums (one block), then the offsets.
-__global__ void __launch_bounds__(kPlocBlock) k_scan2_blocks(const int2* __restrict__ in, const int* __restrict__ nPtr,
-                                                              int2* __restrict__ out, int2* __restrict__ sums) {
-    __shared__ int2 warpSum[kPlocBlock / 32];
+__global__ void k_ploc_flags(const int* __restrict__ nn, const int* __restrict__ nPtr, int2* __restrict__ flags) {
     const int n = *nPtr;
-    const long long base = ((long long)blockIdx.x * kPlocBlock + threadIdx.x) * kScanItems;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flags[i] = ploc_flag(nn, i);
+}
+
+// Exclusive scan of int2 values: per tile of kPlocBlock * kScanItems items
+// (one block of kPlocBlock threads; warpSum: kPlocBlock / 32 entries), then
+// the tile sums (one block), then the offsets.
+__device__ __forceinline__ void scan2_tile(const int2* in, int n, int tile, int2* out, int2* sums, int2* warpSum) {
+    const long long base = ((long long)tile * kPlocBlock + threadIdx.x) * kScanItems;
     int2 v[kScanItems];
     int2 acc = make_int2(0, 0);
 #pragma unroll
@@ -1311,16 +1395,23 @@ __global__ void __launch_bounds__(kPlocBlock) k_scan2_blocks(const int2* __restr
         const long long g = base + q;
         if (g < n) out[g] = make_int2(before.x + v[q].x, before.y + v[q].y);
     }
-    if (threadIdx.x == kPlocBlock - 1) sums[blockIdx.x] = make_int2(before.x + acc.x, before.y + acc.y);
+    if (threadIdx.x == kPlocBlock - 1) sums[tile] = make_int2(before.x + acc.x, before.y + acc.y);
+    __syncthreads();  // warpSum is reused by the block's next tile
 }
 
-__global__ void __launch_bounds__(1024) k_scan2_sums(int2* __restrict__ sums, int nb, int2* __restrict__ total) {
-    __shared__ int2 warpSum[32];
-    __shared__ int2 carry;
+__global__ void __launch_bounds__(kPlocBlock) k_scan2_blocks(const int2* __restrict__ in, const int* __restrict__ nPtr,
+                                                              int2* __restrict__ out, int2* __restrict__ sums) {
+    __shared__ int2 warpSum[kPlocBlock / 32];
+    scan2_tile(in, *nPtr, blockIdx.x, out, sums, warpSum);
+}
+
+// Exclusive scan of the nb tile sums in place by one block (any multiple of
+// 32 threads; warpSum: blockDim.x / 32 entries); the grand total goes to *total.
+__device__ __forceinline__ void scan2_sums_block(int2* sums, int nb, int2* total, int2* warpSum, int2& carry) {
     if (threadIdx.x == 0) carry = make_int2(0, 0);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int start = 0; start < nb; start += 1024) {
+    for (int start = 0; start < nb; start += blockDim.x) {
         const int i = start + threadIdx.x;
         const int2 x = i < nb ? sums[i] : make_int2(0, 0);
         int2 incl = x;
@@ -1341,10 +1432,16 @@ __global__ void __launch_bounds__(1024) k_scan2_sums(int2* __restrict__ sums, in
         }
         if (i < nb) sums[i] = before;
         __syncthreads();
-        if (threadIdx.x == 1023) carry = make_int2(before.x + x.x, before.y + x.y);
+        if (threadIdx.x == blockDim.x - 1) carry = make_int2(before.x + x.x, before.y + x.y);
         __syncthreads();
     }
     if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(1024) k_scan2_sums(int2* __restrict__ sums, int nb, int2* __restrict__ total) {
+    __shared__ int2 warpSum[32];
+    __shared__ int2 carry;
+    scan2_sums_block(sums, nb, total, warpSum, carry);
 }
 
 __global__ void k_scan2_add(int2* __restrict__ out, const int* __restrict__ nPtr, const int2* __restrict__ sums) {
@@ -1356,39 +1453,44 @@ __global__ void k_scan2_add(int2* __restrict__ out, const int* __restrict__ nPtr
 }
 
 // Writes the round's new internal nodes (binary layout: left box, right box,
-// references) and the compacted clusters.
+// references) and the compacted clusters. pi: cluster i's (node, cluster)
+// places among the round's merges and survivors.
+__device__ __forceinline__ void ploc_emit_one(const int* cref, const float4* cbox, const int* nn, int2 f, int2 pi, int i,
+                                              int nodeBase, int nodeCap, float4* nodes, int* crefOut, float4* cboxOut,
+                                              int* err) {
+    if (!f.y) return;
+    const int p = pi.y;
+    const float4 alo = cbox[2 * (long long)i], ahi = cbox[2 * (long long)i + 1];
+    if (f.x) {
+        const int j = nn[i];
+        const int node = nodeBase + pi.x;
+        if (node >= nodeCap) {
+            atomicOr(err, MC_DEVERR_INPUT);
+            return;
+        }
+        const float4 blo = cbox[2 * (long long)j], bhi = cbox[2 * (long long)j + 1];
+        float4* o = nodes + (long long)node * 4;
+        o[0] = make_float4(alo.x, alo.y, alo.z, ahi.x);
+        o[1] = make_float4(ahi.y, ahi.z, blo.x, blo.y);
+        o[2] = make_float4(blo.z, bhi.x, bhi.y, bhi.z);
+        o[3] = make_float4(__int_as_float(cref[i]), __int_as_float(cref[j]), 0.f, 0.f);
+        crefOut[p] = node;
+        cboxOut[2 * (long long)p] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), alo.w);
+        cboxOut[2 * (long long)p + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
+    } else {
+        crefOut[p] = cref[i];
+        cboxOut[2 * (long long)p] = alo;
+        cboxOut[2 * (long long)p + 1] = ahi;
+    }
+}
+
 __global__ void k_ploc_emit(const int* __restrict__ cref, const float4* __restrict__ cbox, const int* __restrict__ nn,
                             const int2* __restrict__ flags, const int2* __restrict__ pos, const int* __restrict__ state,
                             int nodeCap, float4* __restrict__ nodes, int* __restrict__ crefOut, float4* __restrict__ cboxOut,
                             int* __restrict__ err) {
     const int n = state[0], nodeBase = state[1];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int2 f = flags[i];
-        if (!f.y) continue;
-        const int p = pos[i].y;
-        const float4 alo = cbox[2 * (long long)i], ahi = cbox[2 * (long long)i + 1];
-        if (f.x) {
-            const int j = nn[i];
-            const int node = nodeBase + pos[i].x;
-            if (node >= nodeCap) {
-                atomicOr(err, MC_DEVERR_INPUT);
-                continue;
-            }
-            const float4 blo = cbox[2 * (long long)j], bhi = cbox[2 * (long long)j + 1];
-            float4* o = nodes + (long long)node * 4;
-            o[0] = make_float4(alo.x, alo.y, alo.z, ahi.x);
-            o[1] = make_float4(ahi.y, ahi.z, blo.x, blo.y);
-            o[2] = make_float4(blo.z, bhi.x, bhi.y, bhi.z);
-            o[3] = make_float4(__int_as_float(cref[i]), __int_as_float(cref[j]), 0.f, 0.f);
-            crefOut[p] = node;
-            cboxOut[2 * (long long)p] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), alo.w);
-            cboxOut[2 * (long long)p + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
-        } else {
-            crefOut[p] = cref[i];
-            cboxOut[2 * (long long)p] = alo;
-            cboxOut[2 * (long long)p + 1] = ahi;
-        }
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        ploc_emit_one(cref, cbox, nn, flags[i], pos[i], i, nodeBase, nodeCap, nodes, crefOut, cboxOut, err);
 }
 
 // End of a round: the cluster count and the next node id move on; a round
@@ -1404,6 +1506,83 @@ __global__ void k_ploc_advance(const int2* __restrict__ total, int* __restrict__
     state[0] = t.y;
 }
 
+// Every clustering round in one cooperative launch. A round's phases (nearest
+// neighbours, merge flags, tile scans, the scan of the tile sums by block 0,
+// emit) take the same tiles as the per-phase launches above, as grid-stride
+// loops, with a grid-wide barrier after each; every block reads the round's
+// totals from the same place after a barrier, so all blocks run the same
+// rounds and reach the same barriers, and the tree is the per-phase launches'
+// to the bit. The loop ends when every scene is one cluster, after maxRounds
+// rounds (error), or when a round merges nothing (error: the globally closest
+// pair is always mutual).
+struct PlocRounds {
+    int* cref[2];
+    float4* cbox[2];
+    int* nn;
+    int2* flags;
+    int2* pos;
+    int2* sums;
+    int2* total;
+    int* state;  // out: [0] clusters left, [1] internal nodes written, [2] buffer of the last clusters, [3] rounds
+    float4* nodes;
+    int nodeCap, nseg, N, maxRounds;
+    int* err;
+};
+
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_rounds(PlocRounds a) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    __shared__ float4 sLo[kPlocBlock + 2 * kPlocRadius], sHi[kPlocBlock + 2 * kPlocRadius];
+    __shared__ int2 warpSum[kPlocBlock / 32];
+    __shared__ int2 carry;
+    const int per = kPlocBlock * kScanItems;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int n = a.N, nodeBase = 0, cur = 0, round = 0;
+    bool failed = false;
+    while (n > a.nseg) {
+        if (round >= a.maxRounds) {
+            failed = true;
+            break;
+        }
+        const int* cref = cur ? a.cref[1] : a.cref[0];
+        const float4* cbox = cur ? a.cbox[1] : a.cbox[0];
+        int* crefOut = cur ? a.cref[0] : a.cref[1];
+        float4* cboxOut = cur ? a.cbox[0] : a.cbox[1];
+        for (int b0 = blockIdx.x * kPlocBlock; b0 < n; b0 += gridDim.x * kPlocBlock)
+            ploc_nn_tile(cbox, n, b0, a.nn, sLo, sHi);
+        grid.sync();
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+            a.flags[i] = ploc_flag(a.nn, (int)i);
+        grid.sync();
+        const int nb = (n + per - 1) / per;
+        for (int t = blockIdx.x; t < nb; t += gridDim.x) scan2_tile(a.flags, n, t, a.pos, a.sums, warpSum);
+        grid.sync();
+        if (blockIdx.x == 0) scan2_sums_block(a.sums, nb, a.total, warpSum, carry);
+        grid.sync();
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const int2 pi = a.pos[i], off = a.sums[i / per];
+            ploc_emit_one(cref, cbox, a.nn, a.flags[i], make_int2(pi.x + off.x, pi.y + off.y), (int)i, nodeBase,
+                          a.nodeCap, a.nodes, crefOut, cboxOut, a.err);
+        }
+        grid.sync();
+        const int2 t = *a.total;  // written by block 0 before the last two barriers
+        if (t.x == 0) {
+            failed = true;
+            break;
+        }
+        nodeBase += t.x;
+        n = t.y;
+        cur = 1 - cur;
+        round++;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.state[0] = n;
+        a.state[1] = nodeBase;
+        a.state[2] = cur;
+        a.state[3] = round;
+        if (failed) atomicOr(a.err, MC_DEVERR_INPUT);
+    }
+}
+
 // Builds the clustered tree into tree->nodes (NI internal nodes) and its
 // scene roots; MC_ERR_UNSUPPORTED when a scene has fewer than two primitives
 // (the caller keeps the LBVH then).
@@ -1413,7 +1592,7 @@ struct ClusterTree {
 };
 
 static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg, int nseg, const int32_t* order,
-                            const mc_aabb* bounds, ClusterTree& tree) {
+                            const mc_aabb* bounds, ClusterTree& tree, bool coop) {
     const int N = bvh->n, NI = bvh->ni;
     if (NI <= 0 || N < 2) return MC_ERR_UNSUPPORTED;
     const int per = kPlocBlock * kScanItems;
@@ -1446,9 +1625,39 @@ static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg,
     const int h0[2] = {N, 0};
     if (cudaMemcpyAsync(state, h0, sizeof(h0), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
         return fail(cuda_error(cudaGetLastError(), "mc_bvh_build (clustering)", __FILE__, __LINE__));
-    // rounds run in batches between host checks; every launch reads the
-    // cluster count from the device and is sized for the last count seen
     int n = N, nodeBase = 0, cur = 0, rounds = 0;
+    // every round in one cooperative launch where the device supports it
+    int coopAttr = 0, perSm = 0;
+    if (coop && cudaDeviceGetAttribute(&coopAttr, cudaDevAttrCooperativeLaunch, ctx->device) == cudaSuccess && coopAttr &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ploc_rounds, kPlocBlock, 0) == cudaSuccess && perSm > 0) {
+        PlocRounds pr;
+        pr.cref[0] = cref[0]; pr.cref[1] = cref[1];
+        pr.cbox[0] = cbox[0]; pr.cbox[1] = cbox[1];
+        pr.nn = nn; pr.flags = flags; pr.pos = pos; pr.sums = sums; pr.total = total; pr.state = state;
+        pr.nodes = tree.nodes;
+        pr.nodeCap = NI; pr.nseg = nseg; pr.N = N; pr.maxRounds = 4096;
+        pr.err = ctx->d_error;
+        void* args[] = {&pr};
+        const int grid = (int)std::min<long long>((long long)perSm * ctx->sm_count, (N + kPlocBlock - 1) / kPlocBlock);
+        if (cudaLaunchCooperativeKernel((const void*)k_ploc_rounds, grid, kPlocBlock, args, 0, ctx->stream) ==
+            cudaSuccess) {
+            int h[4];
+            if (cudaMemcpyAsync(h, state, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+                cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                return fail(cuda_error(cudaGetLastError(), "mc_bvh_build (clustering)", __FILE__, __LINE__));
+            int fl = 0;
+            mc_status fs = flags_now(ctx, &fl);
+            if (fs != MC_OK || fl) return fail(fs != MC_OK ? fs : status_from_device_flags(fl));
+            n = h[0];
+            nodeBase = h[1];
+            cur = h[2];
+            rounds = h[3];
+        } else {
+            cudaGetLastError();  // the per-phase launches below instead
+        }
+    }
+    // otherwise rounds in batches between host checks; every launch reads the
+    // cluster count from the device and is sized for the last count seen
     const int kBatch = 8;
     while (n > nseg) {
         if (rounds > 4096) return fail(set_error(MC_ERR_INVALID, "mc_bvh_build: clustering did not converge"));
@@ -1493,7 +1702,7 @@ static mc_status build_ploc(mc_context* ctx, const mc_bvh* bvh, const Seg* dSeg,
 // clustered tree whose greedy collapse would outgrow the traversal stack
 // returns MC_ERR_UNSUPPORTED (the caller then collapses the LBVH, which has
 // the depth-parity fallback).
-static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int nseg, int* dWideRoot,
+static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int nseg, int* dWideRoot, bool coop,
                             const float4* tree = nullptr, const std::vector<int>* roots = nullptr) {
     const int N = bvh->n, NI = bvh->ni;
     const float4* bin = tree ? tree : (const float4*)bvh->nodes;
@@ -1513,7 +1722,7 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
     if (NI > 0) {
         // surface-area-greedy collapse, level by level from the scene roots
         int* front[2] = {nullptr, nullptr};
-        int* cnt = nullptr;  // [0]: next frontier size
+        int* cnt = nullptr;  // [0]: next frontier size; [4..7]: the cooperative collapse's results
         int4* internal = nullptr;  // per frontier node: its internal slots
         int* blockTotals = nullptr;
         auto release = [&]() {
@@ -1525,7 +1734,7 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         };
         if (!palloc(ctx, &rootOf, (size_t)NI * sizeof(int)) ||
             !palloc(ctx, &front[0], (size_t)NI * sizeof(int)) ||
-            !palloc(ctx, &front[1], (size_t)NI * sizeof(int)) || !palloc(ctx, &cnt, 4 * sizeof(int)) ||
+            !palloc(ctx, &front[1], (size_t)NI * sizeof(int)) || !palloc(ctx, &cnt, 8 * sizeof(int)) ||
             !palloc(ctx, &internal, (size_t)NI * sizeof(int4)) ||
             !palloc(ctx, &blockTotals, (size_t)(grid_for(NI, kBlock) + 1) * sizeof(int))) {
             cudaGetLastError();
@@ -1539,6 +1748,43 @@ static mc_status build_wide(mc_context* ctx, mc_bvh* bvh, const Seg* dSeg, int n
         k_scatter_ids<<<grid_for(nseg, kBlock), kBlock, 0, ctx->stream>>>(front[0], nseg, wideId);
         // wide ids 0..nseg-1 are the roots; each level's children follow in frontier order
         int levels = 0, cur = 0, n = nseg, idBase = nseg;
+        // every level in one cooperative launch where the device supports it
+        int coopAttr = 0, perSm = 0;
+        if (coop && cudaDeviceGetAttribute(&coopAttr, cudaDevAttrCooperativeLaunch, ctx->device) == cudaSuccess && coopAttr &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_wide_levels, kBlock, 0) == cudaSuccess && perSm > 0) {
+            WideLevels wl;
+            wl.nodes = bin;
+            wl.front[0] = front[0];
+            wl.front[1] = front[1];
+            wl.nseg = nseg;
+            wl.capacity = NI;
+            wl.maxLevels = 4 * MC_STACK_CAPACITY;
+            wl.wideId = wideId;
+            wl.rootOf = rootOf;
+            wl.internal = internal;
+            wl.blockTotals = blockTotals;
+            wl.total = cnt;
+            wl.out = cnt + 4;
+            wl.err = ctx->d_error;
+            void* args[] = {&wl};
+            const int grid = std::max(1, std::min(perSm * ctx->sm_count, grid_for(NI, kBlock)));
+            if (cudaLaunchCooperativeKernel((const void*)k_wide_levels, grid, kBlock, args, 0, ctx->stream) ==
+                cudaSuccess) {
+                int h[4];
+                MC_CUDA(cudaMemcpyAsync(h, cnt + 4, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+                MC_CUDA(cudaStreamSynchronize(ctx->stream));
+                if (h[3]) {
+                    release();
+                    pool_free(ctx, rootOf);
+                    return set_error(MC_ERR_INVALID, "mc_bvh_build: the collapse found more nodes than internal nodes");
+                }
+                levels = h[0];
+                idBase = h[1];
+                n = h[2];
+            } else {
+                cudaGetLastError();  // the per-level launches below instead
+            }
+        }
         while (n > 0 && levels <= 4 * MC_STACK_CAPACITY) {
             const int blocks = grid_for(n, kBlock);
             k_wide_level_count<<<blocks, kBlock, 0, ctx->stream>>>(bin, front[cur], n, NI, wideId, rootOf, internal,
@@ -1782,15 +2028,16 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
         bvh->bin_roots[s] = segs[s].intOff;
     }
     if (o.layout == MC_BVH_LAYOUT_WIDE4 || o.layout == MC_BVH_LAYOUT_WIDE4Q) {
+        const bool coop = o.phase_launches == 0;
         // the wide layouts traverse the collapse of the clustered tree, or of
         // the LBVH when clustering does not apply (a one-primitive scene, a
         // collapse too deep for the stack) or the caller asks for it
         st = MC_ERR_UNSUPPORTED;
         if (o.builder == MC_BVH_BUILDER_CLUSTERED) {
             ClusterTree tree;
-            st = build_ploc(ctx, bvh, dSeg, nseg, order, boundsRef, tree);
+            st = build_ploc(ctx, bvh, dSeg, nseg, order, boundsRef, tree, coop);
             if (st == MC_OK) {
-                st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot, tree.nodes, &tree.roots);
+                st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot, coop, tree.nodes, &tree.roots);
                 pool_free(ctx, tree.nodes);
                 if (st == MC_OK) bvh->builder = MC_BVH_BUILDER_CLUSTERED;
             }
@@ -1800,7 +2047,7 @@ mc_status build_segments(mc_context* ctx, const mc_scene_view* views, int nseg, 
             if (bvh->wide_nodes) pool_free(ctx, bvh->wide_nodes);
             if (bvh->wide_prims) pool_free(ctx, bvh->wide_prims);
             bvh->wide_nodes = bvh->wide_prims = nullptr;
-            if ((st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot)) != MC_OK) return fail(st);
+            if ((st = build_wide(ctx, bvh, dSeg, nseg, dWideRoot, coop)) != MC_OK) return fail(st);
             bvh->builder = MC_BVH_BUILDER_LBVH;
         }
     }
@@ -1942,6 +2189,21 @@ mc_status mc_bvh_export(const mc_bvh* bvh, uint32_t* d_codes, int32_t* d_ids, in
             MC_CUDA(cudaMemcpyAsync(d_internal, bvh->ref_internal, (size_t)(n - 1) * sizeof(mc_bvh_node), cudaMemcpyDeviceToDevice, s));
         if (d_leaves) MC_CUDA(cudaMemcpyAsync(d_leaves, bvh->ref_leaves, (size_t)n * sizeof(mc_bvh_node), cudaMemcpyDeviceToDevice, s));
     }
+    MC_CUDA(cudaStreamSynchronize(s));
+    return MC_OK;
+}
+
+mc_status mc_bvh_export_traversal(const mc_bvh* bvh, void* d_nodes, void* d_prims) {
+    if (!bvh) return mc::set_error(MC_ERR_INVALID, "mc_bvh_export_traversal: null bvh");
+    cudaStream_t s = bvh->ctx->stream;
+    const bool wide = bvh->layout != MC_BVH_LAYOUT_BINARY;
+    const long long nodeBytes = bvh->layout == MC_BVH_LAYOUT_WIDE4    ? bvh->wide_count * 128
+                                : bvh->layout == MC_BVH_LAYOUT_WIDE4Q ? bvh->wide_count * 64
+                                                                      : bvh->node_bytes;
+    if (d_nodes && nodeBytes > 0)
+        MC_CUDA(cudaMemcpyAsync(d_nodes, wide ? bvh->wide_nodes : bvh->nodes, (size_t)nodeBytes, cudaMemcpyDeviceToDevice, s));
+    if (d_prims && bvh->n > 0)
+        MC_CUDA(cudaMemcpyAsync(d_prims, wide ? bvh->wide_prims : bvh->prims, (size_t)bvh->n * 48, cudaMemcpyDeviceToDevice, s));
     MC_CUDA(cudaStreamSynchronize(s));
     return MC_OK;
 }

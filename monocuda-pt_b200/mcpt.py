@@ -128,7 +128,7 @@ class SceneView(C.Structure):
 
 class BvhBuildOpts(C.Structure):
     _fields_ = [("permutation", C.c_void_p), ("layout", C.c_int32), ("keep_reference_nodes", C.c_int32),
-                ("builder", C.c_int32), ("pad0", C.c_int32)]
+                ("builder", C.c_int32), ("phase_launches", C.c_int32)]
 
 
 class BvhInfo(C.Structure):
@@ -244,6 +244,7 @@ SIGNATURES = {
     "mc_radix_sort_pairs_static": (I32, [P, P, P, I32, I32]),
     "mc_bvh_build": (I32, [P, C.POINTER(SceneView), C.POINTER(BvhBuildOpts), C.POINTER(P)]),
     "mc_bvh_build_batch": (I32, [P, P, I32, C.POINTER(BvhBuildOpts), C.POINTER(P)]),
+    "mc_bvh_export_traversal": (I32, [P, P, P]),
     "mc_render_batch": (I32, [P, P, P, I32, I32, C.POINTER(RenderStats)]),
     "mc_bvh_free": (I32, [P]),
     "mc_bvh_get_info": (I32, [P, C.POINTER(BvhInfo)]),
@@ -366,10 +367,11 @@ class Context:
 
 class Bvh:
     def __init__(self, ctx, view, permutation=None, layout=LAYOUT_BINARY, keep_reference_nodes=False,
-                 builder=BUILDER_CLUSTERED):
+                 builder=BUILDER_CLUSTERED, phase_launches=False):
         self.ctx = ctx
         self.lib = ctx.lib
-        opts = BvhBuildOpts(ptr(permutation), layout, 1 if keep_reference_nodes else 0, builder, 0)
+        opts = BvhBuildOpts(ptr(permutation), layout, 1 if keep_reference_nodes else 0, builder,
+                            1 if phase_launches else 0)
         h = P()
         check(self.lib.mc_bvh_build(ctx.handle, C.byref(view), C.byref(opts), C.byref(h)))
         self.handle = h
@@ -381,6 +383,11 @@ class Bvh:
 
     def export(self, codes=None, ids=None, types=None, internal=None, leaves=None):
         check(self.lib.mc_bvh_export(self.handle, ptr(codes), ptr(ids), ptr(types), ptr(internal), ptr(leaves)))
+
+    def traversal_arrays(self):
+        """The node array and the leaf-ordered primitive records the traversal
+        reads, as device uint8 tensors (mc_bvh_export_traversal)."""
+        return traversal_arrays(self.lib, self.handle)
 
     def close(self):
         if self.handle:
@@ -394,14 +401,24 @@ class Bvh:
             pass
 
 
+def traversal_arrays(lib, handle):
+    import torch
+    i = BvhInfo()
+    check(lib.mc_bvh_get_info(handle, C.byref(i)))
+    nodes = torch.empty(int(i.node_bytes), dtype=torch.uint8, device="cuda")
+    prims = torch.empty(int(i.prim_bytes), dtype=torch.uint8, device="cuda")
+    check(lib.mc_bvh_export_traversal(handle, nodes.data_ptr(), prims.data_ptr()))
+    return nodes, prims
+
+
 class BatchBvh:
     """One build over several device scenes (mc_bvh_build_batch)."""
 
-    def __init__(self, ctx, views, layout=LAYOUT_WIDE4, builder=BUILDER_CLUSTERED):
+    def __init__(self, ctx, views, layout=LAYOUT_WIDE4, builder=BUILDER_CLUSTERED, phase_launches=False):
         self.ctx = ctx
         self.lib = ctx.lib
         arr = (SceneView * len(views))(*views)
-        opts = BvhBuildOpts(None, layout, 0, builder, 0)
+        opts = BvhBuildOpts(None, layout, 0, builder, 1 if phase_launches else 0)
         h = P()
         check(self.lib.mc_bvh_build_batch(ctx.handle, C.addressof(arr), len(views), C.byref(opts), C.byref(h)))
         self.handle = h

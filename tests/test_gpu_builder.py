@@ -172,3 +172,46 @@ def test_batch_with_the_smallest_scenes(ctx):
             mcpt.BatchBvh(ctx, [one[1].view, big[1].view], layout=mcpt.LAYOUT_WIDE4, builder=b)
         assert e.value.status == 1  # MC_ERR_INVALID
     mcpt.free_scene(big[0])
+
+
+PERSISTENT_CASES = [(mcpt.SCENE_CORNELL_BOXES, 0, mcpt.LAYOUT_WIDE4), (mcpt.SCENE_CORNELL_SPHERES, 0, mcpt.LAYOUT_WIDE4),
+                    (mcpt.SCENE_DISPLACED_ICOSPHERES, 7, mcpt.LAYOUT_WIDE4),
+                    (mcpt.SCENE_DISPLACED_ICOSPHERES, 5, mcpt.LAYOUT_WIDE4Q),
+                    (mcpt.SCENE_DISPLACED_ICOSPHERES, 5, mcpt.LAYOUT_WIDE4)]
+
+
+@pytest.mark.parametrize("kind,variant,layout", PERSISTENT_CASES)
+@pytest.mark.parametrize("builder", [mcpt.BUILDER_CLUSTERED, mcpt.BUILDER_LBVH])
+def test_persistent_build_loops_give_the_same_tree(ctx, kind, variant, layout, builder):
+    """The clustering rounds and the collapse levels as one cooperative launch
+    each build, byte for byte, the tree of the launch-per-phase loops: the same
+    node array, the same leaf-ordered primitives, the same level count."""
+    s, ds = _scene(kind, variant)
+    out = []
+    for phase in (False, True):
+        bvh = mcpt.Bvh(ctx, ds.view, layout=layout, builder=builder, phase_launches=phase)
+        nodes, prims = bvh.traversal_arrays()
+        i = bvh.info()
+        out.append((nodes.cpu().numpy(), prims.cpu().numpy(), int(i.wide_levels), int(i.node_bytes)))
+        bvh.close()
+    (n0, p0, l0, b0), (n1, p1, l1, b1) = out
+    assert (l0, b0) == (l1, b1)
+    assert n0.tobytes() == n1.tobytes()
+    assert p0.tobytes() == p1.tobytes()
+    mcpt.free_scene(s)
+
+
+def test_persistent_build_loops_give_the_same_batched_trees(ctx):
+    """The same for one batched build over 24 scenes of different sizes."""
+    scenes = [mcpt.generate_scene(mcpt.SCENE_BATCH_MEMBER, variant=i, seed=3, triangle_target=2000 + 3000 * i)
+              for i in range(24)]
+    devs = [mcpt.DeviceScene(mcpt.host_triangles(s)) for s in scenes]
+    out = []
+    for phase in (False, True):
+        b = mcpt.BatchBvh(ctx, [d.view for d in devs], phase_launches=phase)
+        nodes, prims = mcpt.traversal_arrays(ctx.lib, b.handle)
+        out.append((nodes.cpu().numpy().tobytes(), prims.cpu().numpy().tobytes()))
+        b.close()
+    assert out[0] == out[1]
+    for s in scenes:
+        mcpt.free_scene(s)
