@@ -688,13 +688,9 @@ __global__ void k_guide_reduce(const float* partials, int parts, float* out) {
     }
 }
 
-#ifndef MC_GUIDE_HEAD_LR
-#define MC_GUIDE_HEAD_LR 1.0f
-#endif
-__global__ void k_guide_adam(float* master, float* m, float* v, const float* partials, int parts, float lrBase, float b1,
+__global__ void k_guide_adam(float* master, float* m, float* v, const float* partials, int parts, float lr, float b1,
                              float b2, float eps, float c1, float c2) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
-        const float lr = i >= oW4 ? lrBase * MC_GUIDE_HEAD_LR : lrBase;
         float g = 0.f;
         for (int c = 0; c < parts; c++) g += partials[(size_t)c * kParams + i];
         float mi = b1 * m[i] + (1.f - b1) * g;
