@@ -688,17 +688,60 @@ __global__ void k_guide_reduce(const float* partials, int parts, float* out) {
     }
 }
 
-__global__ void k_guide_adam(float* master, float* m, float* v, const float* partials, int parts, float lr, float b1,
-                             float b2, float eps, float c1, float c2) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
-        float g = 0.f;
-        for (int c = 0; c < parts; c++) g += partials[(size_t)c * kParams + i];
-        float mi = b1 * m[i] + (1.f - b1) * g;
-        float vi = b2 * v[i] + (1.f - b2) * g * g;
-        m[i] = mi;
-        v[i] = vi;
-        master[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+// The BF16 operand entries of parameter i (its weight, or its bias's hi / lo
+// pair) from its FP32 value, as k_guide_prepare writes them.
+__device__ __forceinline__ void fold_param(bf16* blob, int i, float x) {
+    int base, nin, nk, rel;
+    bool bias;
+    if (i < oW2) {
+        base = bI1; nin = kIn; nk = kInK; bias = i >= oB1; rel = bias ? i - oB1 : i - oW1;
+    } else if (i < oW3) {
+        base = bI2; nin = kHid; nk = kHidK; bias = i >= oB2; rel = bias ? i - oB2 : i - oW2;
+    } else if (i < oW4) {
+        base = bI3; nin = kHid; nk = kHidK; bias = i >= oB3; rel = bias ? i - oB3 : i - oW3;
+    } else {
+        base = bI4; nin = kHid; nk = kHidK; bias = i >= oB4; rel = bias ? i - oB4 : i - oW4;
     }
+    if (!bias) {
+        blob[base + (rel / nin) * nk + rel % nin] = __float2bfloat16_rn(x);
+    } else {
+        const bf16 hi = __float2bfloat16_rn(x);
+        blob[base + rel * nk + nin] = hi;
+        blob[base + rel * nk + nin + 1] = __float2bfloat16_rn(x - __bfloat162float(hi));
+    }
+}
+
+// One Adam step over the training CTAs' partial gradients. Each block takes
+// 32 parameters (one per lane); its warps sum consecutive slices of the
+// partials and the slices are added in warp order, a fixed order, so the
+// update is the same on every run. The updated parameter's BF16 operand
+// entries are written in place (the blob's constant entries were written
+// when the guide was made).
+constexpr int kAdamWarps = 8;
+__global__ void __launch_bounds__(32 * kAdamWarps) k_guide_adam(float* master, float* m, float* v, const float* partials,
+                                                                int parts, float lr, float b1, float b2, float eps,
+                                                                float c1, float c2, bf16* blob) {
+    __shared__ float slice[kAdamWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
+    const int per = (parts + kAdamWarps - 1) / kAdamWarps;
+    const int cBegin = w * per, cEnd = min(parts, cBegin + per);
+    float part = 0.f;
+    if (i < kParams)
+        for (int c = cBegin; c < cEnd; c++) part += partials[(size_t)c * kParams + i];
+    slice[w][lane] = part;
+    __syncthreads();
+    if (w != 0 || i >= kParams) return;
+    float g = 0.f;
+#pragma unroll
+    for (int k = 0; k < kAdamWarps; k++) g += slice[k][lane];
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    const float x = master[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    master[i] = x;
+    fold_param(blob, i, x);
 }
 
 // 1 / (sum of the records' weights), or 0 when the sum is not positive.
@@ -824,11 +867,12 @@ mc_status adam_step(mc_guide* g, cudaStream_t s, int parts) {
     const int t = g->steps + 1;
     const float b1 = g->cfg.beta1, b2 = g->cfg.beta2;
     const float c1 = (float)(1.0 - std::pow((double)b1, t)), c2 = (float)(1.0 - std::pow((double)b2, t));
-    k_guide_adam<<<80, 256, 0, s>>>(g->master, g->adam_m, g->adam_v, g->partials, parts, g->cfg.learning_rate, b1, b2,
-                                    g->cfg.epsilon, c1, c2);
+    k_guide_adam<<<(kParams + 31) / 32, 32 * kAdamWarps, 0, s>>>(g->master, g->adam_m, g->adam_v, g->partials, parts,
+                                                                 g->cfg.learning_rate, b1, b2, g->cfg.epsilon, c1, c2,
+                                                                 (bf16*)g->blob);
     MC_CUDA(cudaGetLastError());
     g->steps = t;
-    return prepare(g, s);
+    return MC_OK;
 }
 
 mc_status flags_of(mc_context* ctx) {

@@ -283,3 +283,27 @@ def test_untrained_anchored_guide_proposes_around_the_normal(ctx):
         g.close()
     assert cos[True].min() > 0.9, cos[True].min()
     assert abs(cos[False].mean()) < 0.2
+
+
+@pytest.mark.gpu
+def test_adam_step_refreshes_the_bf16_operands(ctx):
+    """The Adam kernel writes each updated parameter's BF16 operand entries in
+    place; they must equal what a full regeneration from the FP32 parameters
+    writes: inference after training steps equals, bit for bit, inference
+    after the same parameters are set again (which regenerates every entry)."""
+    rng = np.random.default_rng(26)
+    g = _guide(ctx, seed=11, learning_rate=3e-3, anchor_lobes=True)
+    for _ in range(5):
+        batch = torch.from_numpy(_target_records(rng, 4096)).cuda()
+        mcpt.check(ctx.lib.mc_guide_train(g.handle, batch.data_ptr(), 4096))
+    n = 2048
+    q = np.zeros((n, 6), np.float32)
+    q[:, 0:3] = rng.uniform(-1, 1, (n, 3))
+    q[:, 3:6] = _unit(rng, n)
+    dq = torch.from_numpy(q).cuda()
+    out = [torch.zeros(n * 40, dtype=torch.float32, device="cuda") for _ in range(2)]
+    mcpt.check(ctx.lib.mc_guide_infer(g.handle, dq.data_ptr(), n, out[0].data_ptr()))
+    g.set_params(g.get_params())
+    mcpt.check(ctx.lib.mc_guide_infer(g.handle, dq.data_ptr(), n, out[1].data_ptr()))
+    assert out[0].cpu().numpy().tobytes() == out[1].cpu().numpy().tobytes()
+    g.close()
