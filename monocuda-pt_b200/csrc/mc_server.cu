@@ -291,7 +291,7 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
             // a scene's guide lives as long as the scene and keeps training on
             // every guided request: the setting that lowered the error per unit
             // time most once trained (anchored lobes, first bounce guided and
-            // trained; 0.76x plain's time to plain's error on the aperture room)
+            // trained; about 0.8x plain's time to plain's error on the aperture room)
             gc.anchor_lobes = 1;
             gc.guided_depth = 2;
             gc.train_vertices = 1;
