@@ -193,7 +193,7 @@ mc_status mc_context_create(int device, mc_context** out) {
     if ((e = cudaSetDevice(device)) != cudaSuccess) return mc::cuda_error((int)e, "cudaSetDevice", __FILE__, __LINE__);
     cudaDeviceProp prop;
     if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return mc::cuda_error((int)e, "cudaGetDeviceProperties", __FILE__, __LINE__);
-    if (prop.major < 10) return mc::set_error(MC_ERR_UNSUPPORTED, "mc_context_create: device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+    if (prop.major < 10) return mc::set_error(MC_ERR_UNSUPPORTED, "mc_context_create: device %d is sm_%d%d; the library is compiled for sm_100a", device, prop.major, prop.minor);
     mc_context* ctx = new mc_context();
     ctx->device = device;
     ctx->sm_count = prop.multiProcessorCount;

@@ -4,7 +4,7 @@ the same GPU, and main()'s 8-bit encoding (PT:3060-3132, 4363-4380).
 
 Bars: with a given exposure the frame buffer floats and the 8-bit pixels are
 bit-exact. With the automatic exposure the reference adds FP32 warp sums with
-atomics in no fixed order and this build sums in FP64 in a fixed order: the
+atomics in no fixed order and the library sums in FP64 in a fixed order: the
 exposure agrees within 2e-5 relative, the floats within 1e-4 relative and
 the bytes within 1 (at least 99 % identical).
 """
