@@ -73,7 +73,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile", action="store_true",
                     help="warm-up and timed steps only (for ncu captures); prints the timed line without extras")
-    ap.add_argument("--workload", default="icospheres", choices=["icospheres", "batch", "guiding", "mlp", "server"],
+    ap.add_argument("--workload", default="icospheres",
+                    choices=["icospheres", "batch", "guiding", "guided_waves", "mlp", "server"],
                     help="icospheres: the headline single-scene workload; batch: the 64-scene batched pipeline; "
                          "guiding: guided vs plain time to a fixed RMSE on the aperture room")
     ap.add_argument("--batch-scenes", type=int, default=64)
@@ -1052,6 +1053,56 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_guided_waves(args):
+    """Guided waves with online training on the aperture room (1024x1024,
+    anchored lobes, first bounce guided and trained, 4 Adam steps per sample):
+    --steps calls of --guide-chunk samples each from a fresh guide, CUDA
+    events around each call; prints rays per second and the time per sample.
+    One untimed call on a separate guide loads the kernels first. A short,
+    fixed launch sequence for launch lists of the guided path."""
+    import numpy as np
+    import torch
+
+    import mcpt
+    ctx = mcpt.Context(0)
+    s = mcpt.generate_scene(mcpt.SCENE_GUIDING_ROOM)
+    tris = mcpt.host_triangles(s)
+    ds = mcpt.DeviceScene(tris)
+    bvh = mcpt.Bvh(ctx, ds.view, layout=mcpt.LAYOUT_WIDE4)
+    v = np.frombuffer(tris, dtype=np.uint8).reshape(len(tris), 224)[:, :36].copy().view(np.float32).reshape(-1, 3)
+    g = mcpt.Guide(ctx, v.min(0).tolist(), v.max(0).tolist(), seed=7, train_steps=4, anchor_lobes=True,
+                   guided_depth=2, train_vertices=1)
+    W, H = s.width, s.height
+    acc = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    warm = mcpt.Guide(ctx, v.min(0).tolist(), v.max(0).tolist(), seed=3, train_steps=4, anchor_lobes=True,
+                      guided_depth=2, train_vertices=1)
+    pw = mcpt.render_params(s.camera, W, H, args.guide_chunk, s.max_depth, persistent=True, rng=mcpt.RNG_PHILOX,
+                            seed=4, first_sample=999000, disable_clamp=True, refill_threshold=16)
+    mcpt.check(ctx.lib.mc_render_guided(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(pw), warm.handle, 1,
+                                        acc.data_ptr(), C.byref(mcpt.RenderStats())))
+    warm.close()
+    acc.zero_()
+    ms_total, rays = 0.0, 0
+    for c in range(args.steps):
+        p = mcpt.render_params(s.camera, W, H, args.guide_chunk, s.max_depth, persistent=True, rng=mcpt.RNG_PHILOX,
+                               seed=4, first_sample=c * args.guide_chunk, disable_clamp=True, refill_threshold=16)
+        st = mcpt.RenderStats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        mcpt.check(ctx.lib.mc_render_guided(ctx.handle, bvh.handle, C.byref(ds.view), C.byref(p), g.handle, 1,
+                                            acc.data_ptr(), C.byref(st)))
+        e1.record()
+        torch.cuda.synchronize()
+        ms_total += e0.elapsed_time(e1)
+        rays += st.extend_rays + st.shadow_rays
+    spp = args.steps * args.guide_chunk
+    print(json.dumps({"metric": "Mrays/s", "value": round(rays / (ms_total / 1e3) / 1e6, 1), "unit": "Mrays/s",
+                      "workload": "guided_waves (aperture room, 1024x1024)", "spp": spp,
+                      "ms_per_spp": round(ms_total / spp, 3), "adam_steps": g.steps(), "n_gpus": 1,
+                      "data": "synthetic (seeded procedural room)"}), flush=True)
+    g.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1060,6 +1111,8 @@ def main():
         run_batch(args)
     elif args.workload == "guiding":
         run_guiding(args)
+    elif args.workload == "guided_waves":
+        run_guided_waves(args)
     elif args.workload == "mlp":
         run_mlp(args)
     elif args.workload == "server":
