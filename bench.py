@@ -91,9 +91,9 @@ def parse():
     ap.add_argument("--guide-batch", type=int, default=0, help="records per Adam step (0 = the library's 65536)")
     ap.add_argument("--guide-nee", type=int, default=0, choices=[0, 1],
                     help="guiding: the primary vertices' shadow rays also give training records")
-    ap.add_argument("--guide-anchor", type=int, default=0, choices=[0, 1],
-                    help="guiding: lobe means offset by the direction input (an untrained guide proposes around "
-                         "the normal)")
+    ap.add_argument("--guide-anchor", type=int, default=-1, choices=[-1, 0, 1],
+                    help="guiding: lobe means offset by the direction input, so an untrained guide proposes around "
+                         "the normal (1), raw means (0), or the library default, anchored (-1)")
     ap.add_argument("--guide-fold", action="store_true",
                     help="mirror guide directions below the surface up instead of ending those paths")
     ap.add_argument("--guide-weight-cap", type=float, default=0.0,
@@ -731,7 +731,7 @@ def run_guiding(args, emit=True, mlp=True):
     warm_guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=1, learning_rate=args.guide_lr,
                             train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                             guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
-                            fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor),
+                            fold_below=args.guide_fold, anchor_lobes=None if args.guide_anchor < 0 else bool(args.guide_anchor),
                             batch_capacity=args.guide_batch,
                             nee_records=bool(args.guide_nee))
     render(tmp, chunk, 999998, warm_guide, 1)
@@ -761,7 +761,7 @@ def run_guiding(args, emit=True, mlp=True):
     guide = mcpt.Guide(ctx, lo.tolist(), hi.tolist(), seed=7, learning_rate=args.guide_lr,
                        train_steps=args.guide_steps, train_vertices=args.guide_vertices, direction_input=gdir,
                        guided_depth=args.guide_depth, weight_cap=args.guide_weight_cap,
-                       fold_below=args.guide_fold, anchor_lobes=bool(args.guide_anchor),
+                       fold_below=args.guide_fold, anchor_lobes=None if args.guide_anchor < 0 else bool(args.guide_anchor),
                             batch_capacity=args.guide_batch,
                             nee_records=bool(args.guide_nee))
     # an untimed render without training sizes the new guide's buffers; its
@@ -821,9 +821,9 @@ def run_guiding(args, emit=True, mlp=True):
            "guided_ms_to_target": round(reached, 1) if reached is not None else None,
            "guided_spp": spp, "adam_steps": steps, "learning_rate": args.guide_lr, "reference_spp": args.guide_ref_spp,
            "pretrain_spp": args.guide_pretrain_spp,
-           "train_vertices": int(guide.config.train_vertices) or 3, "direction_input": args.guide_dir,
-           "guided_depth": int(guide.config.guided_depth) or 4, "weight_cap": args.guide_weight_cap, "fold_below": bool(args.guide_fold),
-           "anchor_lobes": bool(args.guide_anchor), "batch_records": int(guide.config.batch_capacity) or 65536,
+           "train_vertices": int(guide.config.train_vertices) or 1, "direction_input": args.guide_dir,
+           "guided_depth": int(guide.config.guided_depth) or 2, "weight_cap": args.guide_weight_cap, "fold_below": bool(args.guide_fold),
+           "anchor_lobes": args.guide_anchor != 0, "batch_records": int(guide.config.batch_capacity) or 65536,
            "nee_records": bool(args.guide_nee),
            "plain_mrays": round(rays_plain / (plain_ms / 1e3) / 1e6, 1),
            "guided_mrays": round(rays_g / (g_ms / 1e3) / 1e6, 1),

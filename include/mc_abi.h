@@ -717,22 +717,24 @@ typedef struct mc_guide_config {
     int32_t train_steps;        /* Adam steps per sample in guided renders, each on its own
                                    batch_capacity records of that sample; 0 = 1 */
     int32_t train_vertices;     /* guided renders: diffuse vertices per path that give training records,
-                                   the first ones along the path (1..MC_GUIDE_MAX_TRAIN_VERTICES); 0 = 3 */
+                                   the first ones along the path (1..MC_GUIDE_MAX_TRAIN_VERTICES); 0 = 1 */
     int32_t direction_input;    /* MC_GUIDE_DIR_*: the direction the guided renderer feeds the network */
     int32_t guided_depth;       /* guided renders: bounces whose diffuse vertices sample the guide (the network
-                                   runs only for those); deeper vertices sample the cosine lobe alone. 0 = 4;
-                                   never below train_vertices + 1 when training; MC_MAX_DEPTH = every bounce */
+                                   runs only for those); deeper vertices sample the cosine lobe alone. 0 = 2
+                                   (the first bounce); never below train_vertices + 1 when training;
+                                   MC_MAX_DEPTH = every bounce */
     float weight_cap;           /* guided renders' training: a record's share of its step's normalized weight
                                    is capped at weight_cap / (records in the step), so a few rare bright paths
                                    cannot take over a step (0 = no cap). The estimator stays unbiased: only
                                    the proposal the guide learns changes */
     int32_t fold_below;         /* guided renders: the guide's directions below the surface are mirrored up
                                    (the density counts both) instead of ending the path; 0 = off */
-    int32_t anchor_lobes;       /* 1: every lobe's mean is the network's raw mean output plus
-                                   MC_GUIDE_ANCHOR times the direction input (turned away from the surface
-                                   for MC_GUIDE_DIR_RAY), normalized, and kappa starts near e: an untrained
-                                   guide proposes directions around the normal, a cosine-like lobe, instead of
-                                   a near-uniform sphere whose lower half ends paths. 0 = off (raw means) */
+    int32_t anchor_lobes;       /* MC_GUIDE_LOBES_*. Anchored (the default): every lobe's mean is the
+                                   network's raw mean output plus MC_GUIDE_ANCHOR times the direction input
+                                   (turned away from the surface for MC_GUIDE_DIR_RAY), normalized, and kappa
+                                   starts near e: an untrained guide proposes directions around the normal, a
+                                   cosine-like lobe, instead of a near-uniform sphere whose lower half ends
+                                   paths. Raw: the means are the raw outputs, normalized */
     int32_t nee_records;        /* 1: guided renders' training also takes a record from each primary diffuse
                                    vertex's next-event sample (the direction to the light point, weighted by
                                    the light it brought, times its MIS weight), and the records of that vertex's
@@ -742,9 +744,14 @@ typedef struct mc_guide_config {
                                    0 = off */
 } mc_guide_config;
 
-/* Length of the direction-input offset added to every raw lobe mean when
- * mc_guide_config.anchor_lobes is set. */
+/* Length of the direction-input offset added to every raw lobe mean of an
+ * anchored guide. */
 #define MC_GUIDE_ANCHOR 1.5f
+enum {
+    MC_GUIDE_LOBES_DEFAULT = 0, /* anchored */
+    MC_GUIDE_LOBES_ANCHORED = 1,
+    MC_GUIDE_LOBES_RAW = 2
+};
 
 #define MC_GUIDE_MAX_TRAIN_VERTICES 4
 enum {

@@ -797,7 +797,7 @@ void init_params(std::vector<float>& p, uint64_t seed, bool anchored) {
 // The anchor offset's signed length: the direction input as fed (the normal
 // faces the arriving ray), or turned back for the arriving ray's direction.
 float anchor_of(const mc_guide* g) {
-    if (!g->cfg.anchor_lobes) return 0.f;
+    if (g->cfg.anchor_lobes == MC_GUIDE_LOBES_RAW) return 0.f;
     return g->cfg.direction_input == MC_GUIDE_DIR_RAY ? -MC_GUIDE_ANCHOR : MC_GUIDE_ANCHOR;
 }
 
@@ -990,16 +990,19 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
     if (g->cfg.batch_capacity <= 0) g->cfg.batch_capacity = 65536;
     if (g->cfg.train_steps <= 0) g->cfg.train_steps = 1;
     if (!(g->cfg.guide_fraction > 0.f && g->cfg.guide_fraction < 1.f)) g->cfg.guide_fraction = 0.5f;
-    if (g->cfg.train_vertices <= 0) g->cfg.train_vertices = 3;
-    // guiding the first four bounces gave the error of guiding all of them in
-    // 7 % less time on the aperture room (the later bounces carry little light)
-    if (g->cfg.guided_depth <= 0) g->cfg.guided_depth = 4;
+    // guiding and training at the first bounce only, with anchored lobes,
+    // reached plain sampling's error in the least time on the aperture room,
+    // from scratch and with a trained guide (inference and guided shading
+    // then run for two bounces of the path)
+    if (g->cfg.train_vertices <= 0) g->cfg.train_vertices = 1;
+    if (g->cfg.guided_depth <= 0) g->cfg.guided_depth = 2;
     if (!(g->cfg.weight_cap >= 0.f)) g->cfg.weight_cap = 0.f;
     if (g->cfg.train_vertices > MC_GUIDE_MAX_TRAIN_VERTICES || g->cfg.direction_input < 0 || g->cfg.direction_input > 1 ||
-        g->cfg.anchor_lobes < 0 || g->cfg.anchor_lobes > 1 || g->cfg.nee_records < 0 || g->cfg.nee_records > 1) {
+        g->cfg.anchor_lobes < 0 || g->cfg.anchor_lobes > MC_GUIDE_LOBES_RAW || g->cfg.nee_records < 0 ||
+        g->cfg.nee_records > 1) {
         delete g;
         return mc::set_error(MC_ERR_INVALID,
-                             "mc_guide_create: train_vertices above %d, unknown direction_input, or anchor_lobes or "
+                             "mc_guide_create: train_vertices above %d, unknown direction_input or anchor_lobes, or "
                              "nee_records not 0/1",
                              MC_GUIDE_MAX_TRAIN_VERTICES);
     }
@@ -1018,7 +1021,7 @@ mc_status mc_guide_create(mc_context* ctx, const mc_guide_config* config, mc_gui
         return mc::set_error(MC_ERR_OOM, "mc_guide_create: device allocation failed");
     }
     std::vector<float> p;
-    init_params(p, g->cfg.seed, g->cfg.anchor_lobes != 0);
+    init_params(p, g->cfg.seed, g->cfg.anchor_lobes != MC_GUIDE_LOBES_RAW);
     cudaMemcpy(g->master, p.data(), P, cudaMemcpyHostToDevice);
     cudaMemset(g->adam_m, 0, P);
     cudaMemset(g->adam_v, 0, P);

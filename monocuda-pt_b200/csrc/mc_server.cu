@@ -289,12 +289,9 @@ mc_status mc_server_step(mc_server* s, int32_t* active_out) {
             gc.bounds = sc.bvh->bounds;
             gc.seed = (uint64_t)kv.first + 1;
             // a scene's guide lives as long as the scene and keeps training on
-            // every guided request: the setting that lowered the error per unit
-            // time most once trained (anchored lobes, first bounce guided and
-            // trained; about 0.8x plain's time to plain's error on the aperture room)
-            gc.anchor_lobes = 1;
-            gc.guided_depth = 2;
-            gc.train_vertices = 1;
+            // every guided request; the default guide (anchored lobes, first
+            // bounce guided and trained) is the one that reached plain's error
+            // fastest once trained (about 0.8x plain's time on the aperture room)
             if ((st = mc_guide_create(s->ctx, &gc, &sc.guide)) != MC_OK) return st;
         }
         std::vector<mc_render_params> gp;

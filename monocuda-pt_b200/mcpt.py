@@ -146,6 +146,10 @@ class RenderParams(C.Structure):
                 ("stack_entries", C.c_int32), ("trace_threads", C.c_int32)]
 
 
+GUIDE_LOBES_ANCHORED = 1
+GUIDE_LOBES_RAW = 2
+
+
 class GuideConfig(C.Structure):
     _fields_ = [("bounds", AABB), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("epsilon", C.c_float), ("seed", C.c_uint64), ("batch_capacity", C.c_int32),
@@ -754,7 +758,7 @@ class Guide:
 
     def __init__(self, ctx, bounds_lo, bounds_hi, seed=1, learning_rate=1e-3, batch_capacity=0, guide_fraction=0.5,
                  train_steps=1, train_vertices=0, direction_input=0, guided_depth=0, weight_cap=0.0, fold_below=False,
-                 anchor_lobes=False, nee_records=False):
+                 anchor_lobes=None, nee_records=False):
         self.ctx = ctx
         self.lib = ctx.lib
         cfg = GuideConfig()
@@ -770,7 +774,8 @@ class Guide:
         cfg.guided_depth = guided_depth
         cfg.weight_cap = weight_cap
         cfg.fold_below = 1 if fold_below else 0
-        cfg.anchor_lobes = 1 if anchor_lobes else 0
+        # None: the library default (anchored); True / False: anchored / raw means
+        cfg.anchor_lobes = 0 if anchor_lobes is None else (GUIDE_LOBES_ANCHORED if anchor_lobes else GUIDE_LOBES_RAW)
         cfg.nee_records = 1 if nee_records else 0
         self.config = cfg
         h = P()

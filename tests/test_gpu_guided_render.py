@@ -135,10 +135,11 @@ def test_guided_time_to_error_in_the_aperture_room(ctx):
     step inside the timed region), each timed with CUDA events; with error
     falling as 1/time, (MSE x time) guided over plain is the time the guided
     render needs to reach plain's error, relative to plain's. The product
-    target is 0.6; the guide does not reach it yet: it costs about 1.5x plain
-    per sample and learns too slowly to pay that back within these samples
-    (a guide trained on 1024 samples first lowers the per-sample MSE to
-    0.75x). The bar records that the ratio stays bounded and finite."""
+    target is 0.6; the guide does not reach it: a guided sample costs about
+    1.25x a plain one and a guide from scratch learns too slowly to pay that
+    back within these samples (a guide trained on 1024 samples first lowers
+    the per-sample MSE to about 0.6x). The bar records that the ratio stays
+    bounded and finite."""
     W = 512
     s, tris, d, bvh, cam = _setup(ctx, mcpt.SCENE_GUIDING_ROOM, W)
     lo, hi = _bounds(tris)

@@ -189,7 +189,7 @@ def test_gradient_matches_oracle(ctx, n, anchor, direction, aflags):
 def test_adam_step_follows_the_gradient(ctx):
     rng = np.random.default_rng(23)
     params = _params(rng)
-    g = _guide(ctx, params, learning_rate=1e-3)
+    g = _guide(ctx, params, learning_rate=1e-3, anchor_lobes=False)
     rec = _records(rng, 5000)
     # the step follows the kernel's own gradient (the gradient tests compare
     # that with the oracle; a component near zero can take either sign there)
@@ -239,7 +239,7 @@ def test_training_learns_a_directional_target(ctx):
     trained mixture assigns the held-out samples far more density than the
     untrained one and than uniform sampling (log(1/4pi) = -2.53)."""
     rng = np.random.default_rng(24)
-    g = _guide(ctx, seed=5, learning_rate=3e-3)
+    g = _guide(ctx, seed=5, learning_rate=3e-3, anchor_lobes=False)
     held = _target_records(rng, 4096)
 
     def mean_log_q():
